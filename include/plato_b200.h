@@ -1,0 +1,202 @@
+/*
+ * plato_b200.h -- C ABI of the B200 elliptic mechanics path.
+ *
+ * Drop-in replacement for the Plato Analyze elliptic hot path: SIMP-penalised linear
+ * elastostatics on 4-node tetrahedra (SimplexMechanics<3> + LinearTetCubRuleDegreeOne),
+ * its residual and block-CRS Jacobian, the linear solve behind Problem::solution, and the
+ * "Internal Elastic Energy" criterion (compliance) with its adjoint sensitivity dC/dz.
+ * Each entry point names the reference interface it replaces (paths relative to the
+ * reference project).
+ *
+ * Conventions (same as the reference, src/PlatoTypes.hpp:15-20 and
+ * src/ImplicitFunctors.hpp:47-89): Scalar = double, ordinals = int32, dof = 3*node + dim,
+ * connectivity cell*4 + k, coordinates node*3 + dim, control z nodal (length num_nodes).
+ * Block CRS ("CrsMatrix", src/alg/CrsMatrix.hpp:20-111): row_map over node rows (N+1),
+ * column_indices node ids sorted with the diagonal included (CreateBlockMatrix,
+ * src/ImplicitFunctors.hpp:932-1005), entries row-major per block.
+ *
+ * Pointers marked [device] are CUDA device pointers on the handle's device; [host] are host
+ * pointers.  Every function returns a plato_status; no exception crosses the ABI.  A handle
+ * is bound to one CUDA stream; calls on one handle must not run concurrently.
+ */
+#ifndef PLATO_B200_H
+#define PLATO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum plato_status {
+    PLATO_OK             = 0,
+    PLATO_BAD_INPUT      = 1, /* invalid sizes, pointers, inverted/degenerate cells, bad options */
+    PLATO_NOT_CONVERGED  = 2, /* solver hit max_iterations; outputs hold the last iterate   */
+    PLATO_NONFINITE      = 3, /* NaN/Inf met in an input or a solver scalar                 */
+    PLATO_DEVICE_TIMEOUT = 4, /* a bounded device-side wait ran out                         */
+    PLATO_CUDA_ERROR     = 5, /* CUDA runtime error; see plato_last_error                   */
+    PLATO_OUT_OF_MEMORY  = 6,
+    PLATO_NOT_SUPPORTED  = 7
+} plato_status;
+
+typedef enum plato_operator_kind {
+    PLATO_OPERATOR_ASSEMBLED   = 0, /* assembled 3x3 block CRS, FP64 SpMV                  */
+    PLATO_OPERATOR_MATRIX_FREE = 1  /* element-by-element apply recomputed from the mesh   */
+} plato_operator_kind;
+
+typedef enum plato_precision {
+    PLATO_PRECISION_FP64       = 0, /* plain FP64 Jacobi-PCG                                */
+    PLATO_PRECISION_MIXED_FP32 = 1, /* FP32 inner PCG inside FP64 iterative refinement      */
+    PLATO_PRECISION_MIXED_BF16 = 2  /* as MIXED_FP32 with the block CRS stored in BF16      */
+} plato_precision;
+
+typedef struct plato_problem plato_problem; /* opaque handle */
+
+typedef struct plato_mesh_desc {
+    int32_t        num_nodes;
+    int32_t        num_cells;
+    const double*  coords;       /* [host] num_nodes*3 */
+    const int32_t* connectivity; /* [host] num_cells*4 */
+} plato_mesh_desc;
+
+/* "Isotropic Linear Elastic" (src/IsotropicLinearElasticMaterial.cpp:86-110) */
+typedef struct plato_material {
+    double youngs_modulus;
+    double poissons_ratio;
+} plato_material;
+
+/* "Penalty Function" Type SIMP -> MSIMP (src/Simp.hpp:41-52) */
+typedef struct plato_penalty {
+    double exponent;      /* reference default 3   */
+    double minimum_value; /* reference default 1e-9 */
+} plato_penalty;
+
+/* One "Uniform" natural BC on a side set (src/NaturalBC.hpp:87-113): the side set is
+ * given as GetSideSetElements / GetSideSetLocalNodes would return it. */
+typedef struct plato_natural_bc {
+    int32_t        num_faces;
+    const int32_t* face_cells;       /* [host] owning cell of each face              */
+    const int32_t* face_local_nodes; /* [host] 3 cell-local node ordinals per face    */
+    double         vector[3];        /* traction ("Vector")                          */
+} plato_natural_bc;
+
+/* Essential BCs as the Problem holds them (mBcDofs / mBcValues, src/EssentialBCs.hpp:79-88) */
+typedef struct plato_essential_bcs {
+    int32_t        num_dofs;
+    const int32_t* dofs;   /* [host] */
+    const double*  values; /* [host] */
+} plato_essential_bcs;
+
+typedef struct plato_solver_opts {
+    double  tolerance;        /* stop on ||b - A x|| / ||b|| <= tolerance (FP64)          */
+    int32_t max_iterations;   /* total inner iterations allowed                          */
+    int32_t operator_kind;    /* plato_operator_kind                                      */
+    int32_t precision;        /* plato_precision                                          */
+    int32_t self_adjoint;     /* Problem "Self-Adjoint" (src/elliptic/Problem.hpp:116)    */
+    double  inner_tolerance;  /* mixed precision: residual reduction per refinement       */
+    int32_t max_refinements;  /* mixed precision: outer FP64 refinement steps              */
+} plato_solver_opts;
+
+typedef struct plato_problem_desc {
+    plato_mesh_desc         mesh;
+    plato_material          material;
+    plato_penalty           penalty;
+    int32_t                 num_natural_bcs;
+    const plato_natural_bc* natural_bcs;  /* [host] */
+    plato_essential_bcs     essential_bcs;
+    plato_solver_opts       solver;
+} plato_problem_desc;
+
+typedef struct plato_solve_stats {
+    int32_t iterations;        /* inner iterations summed over refinements */
+    int32_t refinements;       /* outer FP64 steps (1 for plain FP64)      */
+    double  relative_residual; /* FP64 ||b - A x|| / ||b|| at exit          */
+    int32_t converged;
+    int32_t status;            /* plato_status of the solve                */
+} plato_solve_stats;
+
+/* ---- lifetime -------------------------------------------------------------------------
+ * Replaces the construction of Elliptic::Problem + VectorFunction + the criterion
+ * (src/elliptic/Problem.hpp:99-125).  Copies mesh and BCs to the device, builds the node
+ * graph and block pattern once, precomputes the traction load vector. */
+int plato_create(const plato_problem_desc* desc, plato_problem** out);
+int plato_destroy(plato_problem* h);
+/* Last error text of a handle (or of the last failed plato_create when h is NULL). */
+const char* plato_last_error(const plato_problem* h);
+/* Bind the handle to a CUDA stream (cudaStream_t); NULL means the legacy default stream. */
+int plato_set_stream(plato_problem* h, void* cuda_stream);
+int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* opts);
+int plato_get_sizes(const plato_problem* h, int32_t* num_nodes, int32_t* num_cells,
+                    int64_t* num_blocks);
+
+/* ---- block pattern ---------------------------------------------------------------------
+ * CreateBlockMatrix (src/ImplicitFunctors.hpp:932-1005) over the node-node graph
+ * (src/EngineMesh.cpp:223-320).  Copies row_map (N+1) and column_indices (num_blocks). */
+int plato_jacobian_pattern(plato_problem* h, int32_t* row_map, int32_t* column_indices /*[device]*/);
+
+/* ---- Elliptic::VectorFunction (src/elliptic/VectorFunction.hpp) ------------------------ */
+/* value(u,z): R = K(z) u - F, :251-334 */
+int plato_vf_value(plato_problem* h, const double* u, const double* z, double* R /*[device]*/);
+/* gradient_u(u,z): 3x3 block entries on the handle's pattern, :525-615 */
+int plato_vf_gradient_u(plato_problem* h, const double* u, const double* z, double* entries);
+/* gradient_u_T(u,z): transpose assembly, :432-523 */
+int plato_vf_gradient_u_T(plato_problem* h, const double* u, const double* z, double* entries);
+/* gradient_z(u,z): (dR/dz)^T, N x 3N with 1x3 blocks on the same pattern, :618-710 */
+int plato_vf_gradient_z(plato_problem* h, const double* u, const double* z, double* entries);
+/* out += gradient_z(u,z) * lambda without forming the matrix (Problem.hpp:445-448 fused) */
+int plato_vf_gradient_z_apply(plato_problem* h, const double* u, const double* z,
+                              const double* lambda, double* out /*[device]*/);
+
+/* ---- Elliptic::PhysicsScalarFunction "Internal Elastic Energy" -------------------------
+ * (src/elliptic/PhysicsScalarFunction.hpp, src/elliptic/InternalElasticEnergy.hpp) */
+int plato_sf_value(plato_problem* h, const double* u, const double* z, double* value /*[host]*/);
+int plato_sf_gradient_u(plato_problem* h, const double* u, const double* z, double* dfdu);
+int plato_sf_gradient_z(plato_problem* h, const double* u, const double* z, double* dfdz);
+
+/* ---- helpers ----------------------------------------------------------------------------
+ * applyBlockConstraints<3> with the handle's essential BCs (src/ApplyConstraints.hpp:40-112);
+ * scale multiplies the BC values (0 for the adjoint, src/elliptic/Problem.hpp:701-713). */
+int plato_apply_constraints(plato_problem* h, double* entries, double* rhs, double scale);
+/* y += A x on the handle's pattern, blocks rows_per_block x cols_per_block (3x3 or 1x3);
+ * MatrixTimesVectorPlusVector, src/PlatoMathHelpers.hpp:78-159 */
+int plato_matvec_plus(plato_problem* h, int32_t rows_per_block, int32_t cols_per_block,
+                      const double* entries, const double* x, double* y);
+
+/* ---- AbstractSolver::solve (src/alg/PlatoAbstractSolver.hpp:38-106) ---------------------
+ * Jacobi-PCG on an assembled, constrained 3x3 block matrix: A x = b, x holds the initial
+ * guess on entry. */
+int plato_solver_solve(plato_problem* h, const double* entries, double* x, const double* b,
+                       plato_solve_stats* stats);
+
+/* ---- Elliptic::Problem (src/elliptic/Problem.hpp) --------------------------------------- */
+/* solution(z), :237-292; u [device] receives the state.  u0 (may be NULL) seeds the solve. */
+int plato_problem_solution(plato_problem* h, const double* z, const double* u0, double* u,
+                           plato_solve_stats* stats);
+/* criterionValue(z, u), :300-354 */
+int plato_problem_criterion_value(plato_problem* h, const double* z, const double* u,
+                                  double* value /*[host]*/);
+/* criterionGradient(z, u), :395-450 (self-adjoint shortcut or adjoint solve) */
+int plato_problem_criterion_gradient(plato_problem* h, const double* z, const double* u,
+                                     double* dfdz, plato_solve_stats* stats);
+/* One optimisation step on HOST buffers: z -> u, compliance value, dC/dz.  Host<->device
+ * copies are part of the call (what an MPMD ComputeSolution + ComputeCriterion +
+ * ComputeCriterionGradient sequence does, src/Analyze_App.cpp:727-1201). */
+int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host,
+                                          const double* u0_host, double* u_host,
+                                          double* value_host, double* dfdz_host,
+                                          plato_solve_stats* stats);
+
+/* ---- box mesh generator (host only; stands in for BamG, unit_tests/PlatoTestHelpers.hpp) */
+int plato_box_mesh_sizes(int32_t nx, int32_t ny, int32_t nz, int32_t* num_nodes, int32_t* num_cells);
+int plato_box_mesh_tet4(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
+                        double* coords, int32_t* connectivity);
+/* face: 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+; pass NULL outputs to get the count */
+int plato_box_nodeset(int32_t nx, int32_t ny, int32_t nz, int32_t face, int32_t* nodes,
+                      int32_t* count);
+int plato_box_sideset(int32_t nx, int32_t ny, int32_t nz, int32_t face, int32_t* cells,
+                      int32_t* local_nodes, int32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLATO_B200_H */

@@ -1,0 +1,120 @@
+"""ctypes binding of the C ABI in include/plato_b200.h.
+
+The CUDA library is required: importing this module raises if
+platoanalyze_b200/lib/libplato_b200.so is missing.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libplato_b200.so"
+
+OK, BAD_INPUT, NOT_CONVERGED, NONFINITE, DEVICE_TIMEOUT, CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED = range(8)
+STATUS_NAMES = ["OK", "BAD_INPUT", "NOT_CONVERGED", "NONFINITE", "DEVICE_TIMEOUT", "CUDA_ERROR",
+                "OUT_OF_MEMORY", "NOT_SUPPORTED"]
+
+OPERATOR_ASSEMBLED, OPERATOR_MATRIX_FREE = 0, 1
+PRECISION_FP64, PRECISION_MIXED_FP32, PRECISION_MIXED_BF16 = 0, 1, 2
+
+i32p = C.POINTER(C.c_int32)
+f64p = C.POINTER(C.c_double)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("num_nodes", C.c_int32), ("num_cells", C.c_int32),
+                ("coords", f64p), ("connectivity", i32p)]
+
+
+class Material(C.Structure):
+    _fields_ = [("youngs_modulus", C.c_double), ("poissons_ratio", C.c_double)]
+
+
+class Penalty(C.Structure):
+    _fields_ = [("exponent", C.c_double), ("minimum_value", C.c_double)]
+
+
+class NaturalBC(C.Structure):
+    _fields_ = [("num_faces", C.c_int32), ("face_cells", i32p), ("face_local_nodes", i32p),
+                ("vector", C.c_double * 3)]
+
+
+class EssentialBCs(C.Structure):
+    _fields_ = [("num_dofs", C.c_int32), ("dofs", i32p), ("values", f64p)]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int32), ("operator_kind", C.c_int32),
+                ("precision", C.c_int32), ("self_adjoint", C.c_int32), ("inner_tolerance", C.c_double),
+                ("max_refinements", C.c_int32)]
+
+
+class ProblemDesc(C.Structure):
+    _fields_ = [("mesh", MeshDesc), ("material", Material), ("penalty", Penalty),
+                ("num_natural_bcs", C.c_int32), ("natural_bcs", C.POINTER(NaturalBC)),
+                ("essential_bcs", EssentialBCs), ("solver", SolverOpts)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("refinements", C.c_int32), ("relative_residual", C.c_double),
+                ("converged", C.c_int32), ("status", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PlatoError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"{name}: {msg}")
+        self.status = status
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"CUDA library not built: {LIB_PATH} (run python -m platoanalyze_b200.build)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    sig = {
+        "plato_create": ([C.POINTER(ProblemDesc), C.POINTER(vp)], C.c_int),
+        "plato_destroy": ([vp], C.c_int),
+        "plato_last_error": ([vp], C.c_char_p),
+        "plato_set_stream": ([vp, vp], C.c_int),
+        "plato_set_solver_opts": ([vp, C.POINTER(SolverOpts)], C.c_int),
+        "plato_get_sizes": ([vp, i32p, i32p, C.POINTER(C.c_int64)], C.c_int),
+        "plato_jacobian_pattern": ([vp, vp, vp], C.c_int),
+        "plato_vf_value": ([vp, vp, vp, vp], C.c_int),
+        "plato_vf_gradient_u": ([vp, vp, vp, vp], C.c_int),
+        "plato_vf_gradient_u_T": ([vp, vp, vp, vp], C.c_int),
+        "plato_vf_gradient_z": ([vp, vp, vp, vp], C.c_int),
+        "plato_vf_gradient_z_apply": ([vp, vp, vp, vp, vp], C.c_int),
+        "plato_sf_value": ([vp, vp, vp, f64p], C.c_int),
+        "plato_sf_gradient_u": ([vp, vp, vp, vp], C.c_int),
+        "plato_sf_gradient_z": ([vp, vp, vp, vp], C.c_int),
+        "plato_apply_constraints": ([vp, vp, vp, C.c_double], C.c_int),
+        "plato_matvec_plus": ([vp, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
+        "plato_solver_solve": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_problem_solution": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_problem_criterion_value": ([vp, vp, vp, f64p], C.c_int),
+        "plato_problem_criterion_gradient": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_problem_solve_and_gradient_host": ([vp, vp, vp, vp, f64p, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_box_mesh_sizes": ([C.c_int32] * 3 + [i32p, i32p], C.c_int),
+        "plato_box_mesh_tet4": ([C.c_int32] * 3 + [C.c_double] * 3 + [vp, vp], C.c_int),
+        "plato_box_nodeset": ([C.c_int32] * 4 + [vp, i32p], C.c_int),
+        "plato_box_sideset": ([C.c_int32] * 4 + [vp, vp, i32p], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+
+def check(rc: int, handle=None) -> int:
+    if rc != OK:
+        msg = lib.plato_last_error(handle)
+        raise PlatoError(rc, msg.decode() if msg else "")
+    return rc

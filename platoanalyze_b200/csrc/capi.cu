@@ -1,0 +1,420 @@
+// C ABI entry points (declared in include/plato_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "plato_internal.cuh"
+
+namespace plato {
+int build_graph(plato_problem* h);
+int launch_internal_force(plato_problem* h, const double* u, const double* z, double* R, double scale_F);
+int launch_traction(plato_problem* h, int32_t nfaces, const int32_t* fcell, const int32_t* floc, const double t[3]);
+int launch_nodal_control_derivative(plato_problem* h, int mode, const double* u, const double* z,
+                                    const double* lam, double* cellbuf, double* out, int accumulate);
+int launch_energy(plato_problem* h, const double* u, const double* z, double* result);
+int launch_assemble_jacobian(plato_problem* h, const double* z, double* entries);
+int launch_assemble_gradient_z(plato_problem* h, const double* u, const double* z, double* entries);
+int launch_dirichlet(plato_problem* h, double* A, double* rhs, double scale);
+int launch_matvec_plus(plato_problem* h, int rb, int cb, const double* A, const double* x, double* y);
+int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
+int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, double* x, plato_solve_stats* stats);
+int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* stats);
+int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* stats);
+}  // namespace plato
+
+using namespace plato;
+
+static thread_local std::string g_create_error;
+
+int plato_fail(plato_problem* h, int status, const std::string& msg) {
+    if (h) h->last_error = msg; else g_create_error = msg;
+    return status;
+}
+
+int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
+                  cudaGetErrorString(e), what, file, line);
+    const int status = (e == cudaErrorMemoryAllocation) ? PLATO_OUT_OF_MEMORY : PLATO_CUDA_ERROR;
+    return plato_fail(h, status, buf);
+}
+
+namespace {
+
+template <typename T>
+int dmalloc(plato_problem* h, T** p, int64_t count) {
+    if (*p) return PLATO_OK;
+    const size_t bytes = size_t(count > 0 ? count : 1) * sizeof(T);
+    PLATO_CUDA(h, cudaMalloc(reinterpret_cast<void**>(p), bytes));
+    return PLATO_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+bool finite_array(const double* a, int64_t n) {
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+int check_opts(plato_problem* h, const plato_solver_opts& o) {
+    if (!(o.tolerance > 0.0) || !std::isfinite(o.tolerance))
+        return plato_fail(h, PLATO_BAD_INPUT, "solver tolerance must be a positive finite number");
+    if (o.max_iterations < 1) return plato_fail(h, PLATO_BAD_INPUT, "solver max_iterations must be >= 1");
+    if (o.operator_kind != PLATO_OPERATOR_ASSEMBLED && o.operator_kind != PLATO_OPERATOR_MATRIX_FREE)
+        return plato_fail(h, PLATO_BAD_INPUT, "unknown operator_kind");
+    if (o.precision < PLATO_PRECISION_FP64 || o.precision > PLATO_PRECISION_MIXED_BF16)
+        return plato_fail(h, PLATO_BAD_INPUT, "unknown precision");
+    return PLATO_OK;
+}
+
+#define RC(expr)                   \
+    do {                           \
+        int _rc = (expr);          \
+        if (_rc) return _rc;       \
+    } while (0)
+
+#define NEED(h, cond, msg)                                             \
+    do {                                                               \
+        if (!(h)) return PLATO_BAD_INPUT;                              \
+        if (!(cond)) return plato_fail((h), PLATO_BAD_INPUT, (msg));   \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+const char* plato_last_error(const plato_problem* h) {
+    return h ? h->last_error.c_str() : g_create_error.c_str();
+}
+
+int plato_destroy(plato_problem* h) {
+    if (!h) return PLATO_OK;
+    cudaStreamSynchronize(h->stream);
+    dfree(h->conn); dfree(h->coords); dfree(h->row_map); dfree(h->cols); dfree(h->diag);
+    dfree(h->n2c_ptr); dfree(h->n2c); dfree(h->F); dfree(h->bc_dofs); dfree(h->bc_values);
+    dfree(h->bc_mask); dfree(h->K); dfree(h->KT); dfree(h->v_r); dfree(h->v_z); dfree(h->v_p);
+    dfree(h->v_Ap); dfree(h->v_dinv); dfree(h->v_b); dfree(h->v_x); dfree(h->v_tmp);
+    dfree(h->partials); dfree(h->cellbuf); dfree(h->scal); dfree(h->red_out); dfree(h->red_ticket);
+    dfree(h->f_r); dfree(h->f_z); dfree(h->f_p); dfree(h->f_Ap); dfree(h->f_x); dfree(h->f_dinv);
+    dfree(h->f_K); dfree(h->h_K); dfree(h->f_coords); dfree(h->f_z_ctrl); dfree(h->d_z_ctrl);
+    dfree(h->d_z_in); dfree(h->d_u_out); dfree(h->d_g_out);
+    if (h->scal_host) cudaFreeHost(h->scal_host);
+    delete h;
+    return PLATO_OK;
+}
+
+int plato_create(const plato_problem_desc* d, plato_problem** out) {
+    if (!out) return plato_fail(nullptr, PLATO_BAD_INPUT, "null output handle pointer");
+    *out = nullptr;
+    if (!d) return plato_fail(nullptr, PLATO_BAD_INPUT, "null problem description");
+    const plato_mesh_desc& m = d->mesh;
+    if (m.num_nodes < 1 || m.num_cells < 1 || !m.coords || !m.connectivity)
+        return plato_fail(nullptr, PLATO_BAD_INPUT, "mesh needs num_nodes >= 1, num_cells >= 1, coords and connectivity");
+    if (int64_t(m.num_nodes) * 3 > INT32_MAX || int64_t(m.num_cells) * 4 > INT32_MAX)
+        return plato_fail(nullptr, PLATO_BAD_INPUT, "mesh too large for int32 dof / connectivity ordinals");
+    if (!finite_array(m.coords, 3 * int64_t(m.num_nodes)))
+        return plato_fail(nullptr, PLATO_BAD_INPUT, "non-finite nodal coordinate");
+    const double E = d->material.youngs_modulus, nu = d->material.poissons_ratio;
+    if (!std::isfinite(E) || !std::isfinite(nu) || nu <= -1.0 || nu >= 0.5)
+        return plato_fail(nullptr, PLATO_BAD_INPUT, "material needs finite E and -1 < nu < 0.5");
+    if (!std::isfinite(d->penalty.exponent) || !std::isfinite(d->penalty.minimum_value))
+        return plato_fail(nullptr, PLATO_BAD_INPUT, "non-finite penalty parameter");
+
+    plato_problem* h = new plato_problem();
+    h->N = m.num_nodes;
+    h->C = m.num_cells;
+    h->opts = d->solver;
+    if (int rc = check_opts(h, h->opts)) { g_create_error = h->last_error; delete h; return rc; }
+    cudaGetDevice(&h->device);
+
+    // IsotropicLinearElasticMaterial<3> constants, src/IsotropicLinearElasticMaterial.cpp:86-110
+    const double coef = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    h->material.c00 = coef * (1.0 - nu);
+    h->material.c01 = coef * nu;
+    h->material.c33 = 1.0 / 2.0 * coef * (1.0 - 2.0 * nu);
+    h->material.p = d->penalty.exponent;
+    h->material.rho_min = d->penalty.minimum_value;
+    h->material.p_int = (d->penalty.exponent >= 0.0 && d->penalty.exponent <= 16.0 &&
+                         std::floor(d->penalty.exponent) == d->penalty.exponent)
+                            ? int(d->penalty.exponent) : -1;
+
+    auto fail_create = [&](int rc) {
+        g_create_error = h->last_error;
+        plato_destroy(h);
+        return rc;
+    };
+#define CRC(expr)                          \
+    do {                                   \
+        int _rc = (expr);                  \
+        if (_rc) return fail_create(_rc);  \
+    } while (0)
+#define CCUDA(expr)                                                                 \
+    do {                                                                            \
+        cudaError_t _e = (expr);                                                    \
+        if (_e != cudaSuccess) return fail_create(plato_cuda_fail(h, _e, #expr, __FILE__, __LINE__)); \
+    } while (0)
+
+    const int64_t n = 3 * int64_t(h->N);
+    CRC(dmalloc(h, &h->conn, h->C));
+    CRC(dmalloc(h, &h->coords, n));
+    CCUDA(cudaMemcpy(h->conn, m.connectivity, sizeof(int4) * size_t(h->C), cudaMemcpyHostToDevice));
+    CCUDA(cudaMemcpy(h->coords, m.coords, sizeof(double) * size_t(n), cudaMemcpyHostToDevice));
+    CRC(build_graph(h));
+
+    // essential BCs
+    const plato_essential_bcs& bc = d->essential_bcs;
+    if (bc.num_dofs < 0 || (bc.num_dofs > 0 && (!bc.dofs || !bc.values)))
+        return fail_create(plato_fail(h, PLATO_BAD_INPUT, "essential BCs need dofs and values"));
+    std::vector<uint8_t> mask(n, 0);
+    for (int32_t i = 0; i < bc.num_dofs; ++i) {
+        if (bc.dofs[i] < 0 || bc.dofs[i] >= n)
+            return fail_create(plato_fail(h, PLATO_BAD_INPUT, "essential BC dof out of range"));
+        if (!std::isfinite(bc.values[i]))
+            return fail_create(plato_fail(h, PLATO_BAD_INPUT, "non-finite essential BC value"));
+        mask[bc.dofs[i]] = 1;
+    }
+    h->nbc = bc.num_dofs;
+    CRC(dmalloc(h, &h->bc_dofs, h->nbc));
+    CRC(dmalloc(h, &h->bc_values, h->nbc));
+    CRC(dmalloc(h, &h->bc_mask, n));
+    if (h->nbc) {
+        CCUDA(cudaMemcpy(h->bc_dofs, bc.dofs, sizeof(int32_t) * h->nbc, cudaMemcpyHostToDevice));
+        CCUDA(cudaMemcpy(h->bc_values, bc.values, sizeof(double) * h->nbc, cudaMemcpyHostToDevice));
+    }
+    CCUDA(cudaMemcpy(h->bc_mask, mask.data(), size_t(n), cudaMemcpyHostToDevice));
+
+    // work vectors and reduction scratch
+    for (double** v : {&h->F, &h->v_r, &h->v_z, &h->v_p, &h->v_Ap, &h->v_dinv, &h->v_b, &h->v_x, &h->v_tmp})
+        CRC(dmalloc(h, v, n));
+    h->partials_len = 148 * 64;
+    CRC(dmalloc(h, &h->partials, 4 * int64_t(h->partials_len)));
+    CRC(dmalloc(h, &h->cellbuf, h->C));
+    CRC(dmalloc(h, &h->scal, 1));
+    CRC(dmalloc(h, &h->red_out, 1));
+    CRC(dmalloc(h, &h->red_ticket, 1));
+    CCUDA(cudaMemset(h->red_ticket, 0, sizeof(uint32_t)));
+    CCUDA(cudaMemset(h->scal, 0, sizeof(PcgScalars)));
+    CCUDA(cudaMallocHost(reinterpret_cast<void**>(&h->scal_host), 2 * sizeof(PcgScalars)));
+
+    // external load F from the natural BCs (constant in u and z)
+    CCUDA(cudaMemset(h->F, 0, sizeof(double) * size_t(n)));
+    for (int32_t k = 0; k < d->num_natural_bcs; ++k) {
+        const plato_natural_bc& nb = d->natural_bcs[k];
+        if (nb.num_faces < 0 || (nb.num_faces > 0 && (!nb.face_cells || !nb.face_local_nodes)))
+            return fail_create(plato_fail(h, PLATO_BAD_INPUT, "natural BC needs face cells and local nodes"));
+        for (int32_t f = 0; f < nb.num_faces; ++f) {
+            if (nb.face_cells[f] < 0 || nb.face_cells[f] >= h->C)
+                return fail_create(plato_fail(h, PLATO_BAD_INPUT, "natural BC face cell out of range"));
+            for (int a = 0; a < 3; ++a)
+                if (nb.face_local_nodes[3 * int64_t(f) + a] < 0 || nb.face_local_nodes[3 * int64_t(f) + a] > 3)
+                    return fail_create(plato_fail(h, PLATO_BAD_INPUT, "natural BC local node ordinal out of range"));
+        }
+        if (nb.num_faces == 0) continue;
+        int32_t *fc = nullptr, *fl = nullptr;
+        CCUDA(cudaMalloc(&fc, sizeof(int32_t) * nb.num_faces));
+        CCUDA(cudaMalloc(&fl, sizeof(int32_t) * 3 * size_t(nb.num_faces)));
+        CCUDA(cudaMemcpy(fc, nb.face_cells, sizeof(int32_t) * nb.num_faces, cudaMemcpyHostToDevice));
+        CCUDA(cudaMemcpy(fl, nb.face_local_nodes, sizeof(int32_t) * 3 * size_t(nb.num_faces), cudaMemcpyHostToDevice));
+        const int rc = launch_traction(h, nb.num_faces, fc, fl, nb.vector);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(fc);
+        cudaFree(fl);
+        CRC(rc);
+    }
+    CCUDA(cudaStreamSynchronize(h->stream));
+#undef CRC
+#undef CCUDA
+    *out = h;
+    return PLATO_OK;
+}
+
+int plato_set_stream(plato_problem* h, void* stream) {
+    if (!h) return PLATO_BAD_INPUT;
+    h->stream = static_cast<cudaStream_t>(stream);
+    return PLATO_OK;
+}
+
+int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* o) {
+    NEED(h, o != nullptr, "null solver options");
+    RC(check_opts(h, *o));
+    h->opts = *o;
+    return PLATO_OK;
+}
+
+int plato_get_sizes(const plato_problem* h, int32_t* nn, int32_t* nc, int64_t* nb) {
+    if (!h) return PLATO_BAD_INPUT;
+    if (nn) *nn = h->N;
+    if (nc) *nc = h->C;
+    if (nb) *nb = h->nblocks;
+    return PLATO_OK;
+}
+
+int plato_jacobian_pattern(plato_problem* h, int32_t* row_map, int32_t* cols) {
+    NEED(h, row_map && cols, "null pattern output");
+    PLATO_CUDA(h, cudaMemcpyAsync(row_map, h->row_map, sizeof(int32_t) * (h->N + 1), cudaMemcpyDeviceToDevice, h->stream));
+    PLATO_CUDA(h, cudaMemcpyAsync(cols, h->cols, sizeof(int32_t) * size_t(h->nblocks), cudaMemcpyDeviceToDevice, h->stream));
+    return PLATO_OK;
+}
+
+int plato_vf_value(plato_problem* h, const double* u, const double* z, double* R) {
+    NEED(h, u && z && R, "null device pointer");
+    return launch_internal_force(h, u, z, R, -1.0);
+}
+
+int plato_vf_gradient_u(plato_problem* h, const double* u, const double* z, double* entries) {
+    NEED(h, z && entries, "null device pointer");
+    (void)u;  // linear elasticity: K does not depend on u
+    return launch_assemble_jacobian(h, z, entries);
+}
+
+int plato_vf_gradient_u_T(plato_problem* h, const double* u, const double* z, double* entries) {
+    // The closed-form isotropic element blocks satisfy K_ab = K_ba^T term by term, so the
+    // transpose assembly produces the same entries as gradient_u.
+    return plato_vf_gradient_u(h, u, z, entries);
+}
+
+int plato_vf_gradient_z(plato_problem* h, const double* u, const double* z, double* entries) {
+    NEED(h, u && z && entries, "null device pointer");
+    return launch_assemble_gradient_z(h, u, z, entries);
+}
+
+int plato_vf_gradient_z_apply(plato_problem* h, const double* u, const double* z, const double* lam, double* out) {
+    NEED(h, u && z && lam && out, "null device pointer");
+    return launch_nodal_control_derivative(h, 3, u, z, lam, h->cellbuf, out, 1);
+}
+
+int plato_sf_value(plato_problem* h, const double* u, const double* z, double* value) {
+    NEED(h, u && z && value, "null pointer");
+    RC(launch_energy(h, u, z, h->red_out));
+    PLATO_CUDA(h, cudaMemcpyAsync(value, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PLATO_OK;
+}
+
+int plato_sf_gradient_u(plato_problem* h, const double* u, const double* z, double* dfdu) {
+    NEED(h, u && z && dfdu, "null device pointer");
+    return launch_internal_force(h, u, z, dfdu, 0.0);
+}
+
+int plato_sf_gradient_z(plato_problem* h, const double* u, const double* z, double* dfdz) {
+    NEED(h, u && z && dfdz, "null device pointer");
+    return launch_nodal_control_derivative(h, 1, u, z, nullptr, h->cellbuf, dfdz, 0);
+}
+
+int plato_apply_constraints(plato_problem* h, double* entries, double* rhs, double scale) {
+    NEED(h, entries != nullptr, "null matrix entries");
+    return launch_dirichlet(h, entries, rhs, scale);
+}
+
+int plato_matvec_plus(plato_problem* h, int32_t rb, int32_t cb, const double* entries, const double* x, double* y) {
+    NEED(h, entries && x && y, "null device pointer");
+    return launch_matvec_plus(h, rb, cb, entries, x, y);
+}
+
+int plato_solver_solve(plato_problem* h, const double* entries, double* x, const double* b,
+                       plato_solve_stats* stats) {
+    NEED(h, entries && x && b, "null device pointer");
+    plato_solve_stats local{};
+    plato_solve_stats* st = stats ? stats : &local;
+    return pcg_fp64_assembled(h, entries, b, x, st);
+}
+
+int plato_problem_solution(plato_problem* h, const double* z, const double* u0, double* u,
+                           plato_solve_stats* stats) {
+    NEED(h, z && u, "null device pointer");
+    plato_solve_stats local{};
+    return solve_state(h, z, u0, u, stats ? stats : &local);
+}
+
+int plato_problem_criterion_value(plato_problem* h, const double* z, const double* u, double* value) {
+    return plato_sf_value(h, u, z, value);
+}
+
+int plato_problem_criterion_gradient(plato_problem* h, const double* z, const double* u, double* dfdz,
+                                     plato_solve_stats* stats) {
+    NEED(h, z && u && dfdz, "null device pointer");
+    plato_solve_stats local{};
+    plato_solve_stats* st = stats ? stats : &local;
+    if (h->opts.self_adjoint) {
+        // lambda = -u (src/elliptic/Problem.hpp:423-427): dfdz + (dR/dz)^T lambda fused per cell
+        st->iterations = 0; st->refinements = 0; st->relative_residual = 0.0; st->converged = 1; st->status = 0;
+        return launch_nodal_control_derivative(h, 2, u, z, nullptr, h->cellbuf, dfdz, 0);
+    }
+    // adjoint: K^T lambda = -df/du with zero-valued constraints (Problem.hpp:429-441, 701-713)
+    const int64_t n = 3 * int64_t(h->N);
+    RC(launch_internal_force(h, u, z, h->v_tmp, 0.0));
+    RC(launch_axpby(h, n, -1.0, h->v_tmp, 0.0, h->v_tmp));
+    RC(solve_adjoint(h, z, h->v_tmp, h->v_x, st));
+    return launch_nodal_control_derivative(h, 4, u, z, h->v_x, h->cellbuf, dfdz, 0);
+}
+
+int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host, const double* u0_host,
+                                          double* u_host, double* value_host, double* dfdz_host,
+                                          plato_solve_stats* stats) {
+    NEED(h, z_host != nullptr, "null control");
+    const int64_t n = 3 * int64_t(h->N);
+    RC(dmalloc(h, &h->d_z_in, h->N));
+    RC(dmalloc(h, &h->d_u_out, n));
+    RC(dmalloc(h, &h->d_g_out, h->N));
+    cudaStream_t s = h->stream;
+    PLATO_CUDA(h, cudaMemcpyAsync(h->d_z_in, z_host, sizeof(double) * h->N, cudaMemcpyHostToDevice, s));
+    const double* u0 = nullptr;
+    if (u0_host) {
+        PLATO_CUDA(h, cudaMemcpyAsync(h->d_u_out, u0_host, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        u0 = h->d_u_out;
+    }
+    plato_solve_stats local{};
+    plato_solve_stats* st = stats ? stats : &local;
+    int rc = solve_state(h, h->d_z_in, u0, h->d_u_out, st);
+    if (rc && rc != PLATO_NOT_CONVERGED) return rc;
+    const int solve_rc = rc;
+    if (value_host) RC(plato_sf_value(h, h->d_u_out, h->d_z_in, value_host));
+    if (dfdz_host) {
+        plato_solve_stats adj{};
+        RC(plato_problem_criterion_gradient(h, h->d_z_in, h->d_u_out, h->d_g_out, &adj));
+        PLATO_CUDA(h, cudaMemcpyAsync(dfdz_host, h->d_g_out, sizeof(double) * h->N, cudaMemcpyDeviceToHost, s));
+    }
+    if (u_host) PLATO_CUDA(h, cudaMemcpyAsync(u_host, h->d_u_out, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA(h, cudaStreamSynchronize(s));
+    return solve_rc;
+}
+
+}  // extern "C"
+
+namespace plato {
+
+// Problem::solution (src/elliptic/Problem.hpp:237-292), one Newton step from u = 0:
+// R = -value(0, z) = F, J = gradient_u, applyStateConstraints(J, R, 1), solve J d = R.
+int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* st) {
+    const int64_t n = 3 * int64_t(h->N);
+    RC(dmalloc(h, &h->K, 9 * h->nblocks));
+    RC(launch_assemble_jacobian(h, z, h->K));
+    PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, h->F, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    RC(launch_dirichlet(h, h->K, h->v_b, 1.0));
+    if (u0) {
+        if (u0 != u) PLATO_CUDA(h, cudaMemcpyAsync(u, u0, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        PLATO_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n, h->stream));
+    }
+    return pcg_fp64_assembled(h, h->K, h->v_b, u, st);
+}
+
+// Adjoint solve K^T lambda = rhs with zero-valued constraints.
+int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* st) {
+    const int64_t n = 3 * int64_t(h->N);
+    RC(dmalloc(h, &h->K, 9 * h->nblocks));
+    RC(launch_assemble_jacobian(h, z, h->K));
+    if (rhs != h->v_b)
+        PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    RC(launch_dirichlet(h, h->K, h->v_b, 0.0));
+    PLATO_CUDA(h, cudaMemsetAsync(lam, 0, sizeof(double) * n, h->stream));
+    return pcg_fp64_assembled(h, h->K, h->v_b, lam, st);
+}
+
+}  // namespace plato

@@ -1,0 +1,285 @@
+// Internal declarations of the B200 elliptic path: the handle, error plumbing and the
+// device-side element arithmetic shared by every kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "plato_b200.h"
+
+namespace plato {
+
+// ---------------------------------------------------------------------------------------
+// Material constants of IsotropicLinearElasticMaterial<3>
+// (src/IsotropicLinearElasticMaterial.cpp:86-110): C00 = c(1-nu), C01 = c nu,
+// C33 = 1/2 c (1-2nu), c = E/((1+nu)(1-2nu)).  Lame form: lambda = C01, mu = C33.
+struct Material {
+    double c00, c01, c33;
+    double p, rho_min;  // MSIMP exponent and minimum value (src/Simp.hpp:130-134)
+    int    p_int;       // p when it is a small non-negative integer, else -1
+};
+
+// Device pointers and sizes the element kernels read.
+struct MeshView {
+    int32_t       num_nodes;
+    int32_t       num_cells;
+    const int4*   conn;    // [num_cells]   the 4 node ids of each cell
+    const double* coords;  // [3*num_nodes] node-major xyz
+};
+
+// Node graph: block pattern plus the node -> (cell, local slot) incidence.
+struct GraphView {
+    int32_t        num_nodes;
+    int64_t        num_blocks;
+    const int32_t* row_map;   // [N+1]
+    const int32_t* cols;      // [num_blocks]
+    const int32_t* diag;      // [N] position of the diagonal block of each row
+    const int32_t* n2c_ptr;   // [N+1]
+    const int32_t* n2c;       // [4*C] cell*4 + local slot, sorted by cell within a node
+};
+
+}  // namespace plato
+
+// Work state of the Jacobi-PCG (device resident).
+struct PcgScalars {
+    double rz;       // r . z
+    double rz_new;
+    double pAp;
+    double rr;       // r . r
+    double bb;       // b . b
+    double alpha;
+    double beta;
+    double tol2;     // tol^2 * b.b
+    int32_t iter;
+    int32_t done;    // 1 once ||r|| <= tol ||b||
+    int32_t nonfinite;
+    uint32_t ticket; // last-block-done counter of the fused reductions
+};
+
+struct plato_problem {
+    int          device = 0;
+    cudaStream_t stream = nullptr;
+    std::string  last_error;
+
+    int32_t N = 0, C = 0;
+    int64_t nblocks = 0;
+
+    plato::Material material{};
+    plato_solver_opts opts{};
+
+    // mesh
+    int4*   conn = nullptr;
+    double* coords = nullptr;
+    // graph
+    int32_t* row_map = nullptr;
+    int32_t* cols = nullptr;
+    int32_t* diag = nullptr;
+    int32_t* n2c_ptr = nullptr;
+    int32_t* n2c = nullptr;
+    // loads and BCs
+    double*  F = nullptr;          // external load vector (traction), length 3N
+    int32_t  nbc = 0;
+    int32_t* bc_dofs = nullptr;
+    double*  bc_values = nullptr;
+    uint8_t* bc_mask = nullptr;    // [3N] 1 where a dof is constrained
+    // assembled operator (allocated on first use)
+    double* K = nullptr;           // 9*nblocks
+    double* KT = nullptr;          // scratch for transposed / gradient_z matrices
+    // PCG work vectors (3N each) and scalars
+    double* v_r = nullptr;
+    double* v_z = nullptr;
+    double* v_p = nullptr;
+    double* v_Ap = nullptr;
+    double* v_dinv = nullptr;
+    double* v_b = nullptr;
+    double* v_x = nullptr;
+    double* v_tmp = nullptr;
+    double* partials = nullptr;    // block partial sums of reductions
+    double* cellbuf = nullptr;     // one double per cell (per-cell quantities before a nodal sum)
+    int32_t partials_len = 0;
+    PcgScalars* scal = nullptr;    // device
+    PcgScalars* scal_host = nullptr;  // pinned mirror
+    double* red_out = nullptr;     // device scalar result of a reduction
+    uint32_t* red_ticket = nullptr;
+    // mixed-precision and matrix-free work (allocated on first use)
+    float* f_r = nullptr;
+    float* f_z = nullptr;
+    float* f_p = nullptr;
+    float* f_Ap = nullptr;
+    float* f_x = nullptr;
+    float* f_dinv = nullptr;
+    float* f_K = nullptr;          // 9*nblocks FP32 copy of the constrained matrix
+    uint16_t* h_K = nullptr;       // 9*nblocks BF16 copy
+    float* f_coords = nullptr;
+    float* f_z_ctrl = nullptr;     // nodal control in FP32 (matrix-free FP32 apply)
+    double* d_z_ctrl = nullptr;    // nodal control the operator was built for
+    int     operator_ready = 0;    // K / diag valid for d_z_ctrl
+    // host staging for the _host entry points
+    double* pinned = nullptr;
+    size_t  pinned_len = 0;
+    // device scratch for host-buffer calls
+    double* d_z_in = nullptr;
+    double* d_u_out = nullptr;
+    double* d_g_out = nullptr;
+};
+
+// ---------------------------------------------------------------------------------------
+// error plumbing
+int plato_fail(plato_problem* h, int status, const std::string& msg);
+int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const char* file, int line);
+
+#define PLATO_CUDA(h, expr)                                                          \
+    do {                                                                             \
+        cudaError_t _e = (expr);                                                     \
+        if (_e != cudaSuccess) return plato_cuda_fail((h), _e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+#define PLATO_LAUNCH_CHECK(h)                                                        \
+    do {                                                                             \
+        cudaError_t _e = cudaGetLastError();                                         \
+        if (_e != cudaSuccess) return plato_cuda_fail((h), _e, "kernel launch", __FILE__, __LINE__); \
+    } while (0)
+
+namespace plato {
+
+constexpr int kNumSMs = 148;
+
+inline int grid_for(int64_t n, int threads, int64_t max_blocks = 148 * 32) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > max_blocks) b = max_blocks;
+    return int(b);
+}
+
+// ---------------------------------------------------------------------------------------
+// device element arithmetic
+
+// Basis gradients and weighted volume of a linear tet: ComputeGradientWorkset<3>
+// (src/ImplicitFunctors.hpp:169-221) times the 1/6 cubature weight
+// (src/LinearTetCubRuleDegreeOne.hpp:72-78).  g[a][d] = d N_a / d x_d.
+template <typename T>
+struct TetGeom {
+    T g[4][3];
+    T vol;
+};
+
+template <typename T>
+__device__ __forceinline__ void tet_geometry(const T x[4][3], TetGeom<T>& G) {
+    const T j11 = x[0][0] - x[3][0], j12 = x[1][0] - x[3][0], j13 = x[2][0] - x[3][0];
+    const T j21 = x[0][1] - x[3][1], j22 = x[1][1] - x[3][1], j23 = x[2][1] - x[3][1];
+    const T j31 = x[0][2] - x[3][2], j32 = x[1][2] - x[3][2], j33 = x[2][2] - x[3][2];
+    const T c11 = j22 * j33 - j23 * j32, c12 = j13 * j32 - j12 * j33, c13 = j12 * j23 - j13 * j22;
+    const T detj = j11 * c11 + j21 * c12 + j31 * c13;
+    const T inv = T(1) / detj;
+    G.g[0][0] = c11 * inv;
+    G.g[0][1] = c12 * inv;
+    G.g[0][2] = c13 * inv;
+    G.g[1][0] = (j23 * j31 - j21 * j33) * inv;
+    G.g[1][1] = (j11 * j33 - j13 * j31) * inv;
+    G.g[1][2] = (j13 * j21 - j11 * j23) * inv;
+    G.g[2][0] = (j21 * j32 - j22 * j31) * inv;
+    G.g[2][1] = (j12 * j31 - j11 * j32) * inv;
+    G.g[2][2] = (j11 * j22 - j12 * j21) * inv;
+    G.g[3][0] = -(G.g[0][0] + G.g[1][0] + G.g[2][0]);
+    G.g[3][1] = -(G.g[0][1] + G.g[1][1] + G.g[2][1]);
+    G.g[3][2] = -(G.g[0][2] + G.g[1][2] + G.g[2][2]);
+    G.vol = fabs(detj) * (T(1) / T(6));
+}
+
+__device__ __forceinline__ void load_cell_coords(const double* __restrict__ coords, int4 n,
+                                                 double x[4][3]) {
+    const int ids[4] = {n.x, n.y, n.z, n.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const double* p = coords + 3 * (int64_t)ids[a];
+        x[a][0] = __ldg(p + 0);
+        x[a][1] = __ldg(p + 1);
+        x[a][2] = __ldg(p + 2);
+    }
+}
+
+__device__ __forceinline__ int node_of(int4 n, int a) {
+    return a == 0 ? n.x : (a == 1 ? n.y : (a == 2 ? n.z : n.w));
+}
+
+// MSIMP s(rho) = rho_min + (1 - rho_min) rho^p and its derivative (src/Simp.hpp:130-134).
+// Integer exponents use repeated products (within 2 ulp of pow).
+template <typename T>
+__device__ __forceinline__ T ipow(T r, int p) {
+    T v = T(1);
+    for (int i = 0; i < p; ++i) v *= r;
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T simp(const Material& m, T rho) {
+    const T pw = m.p_int >= 0 ? ipow(rho, m.p_int) : T(pow(double(rho), m.p));
+    return T(m.rho_min) + (T(1) - T(m.rho_min)) * pw;
+}
+
+template <typename T>
+__device__ __forceinline__ T simp_dx(const Material& m, T rho) {
+    T pw;
+    if (m.p_int >= 1) pw = ipow(rho, m.p_int - 1);
+    else if (m.p_int == 0) pw = T(0);
+    else pw = T(pow(double(rho), m.p - 1.0));
+    return (T(1) - T(m.rho_min)) * (T(m.p) * pw);
+}
+
+// Voigt strain (xx, yy, zz, yz, xz, xy) with engineering shear, Strain<3>
+// (src/Strain.hpp:70-95).
+template <typename T>
+__device__ __forceinline__ void strain_voigt(const T g[4][3], const T u[4][3], T e[6]) {
+#pragma unroll
+    for (int v = 0; v < 6; ++v) e[v] = T(0);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        e[0] += u[a][0] * g[a][0];
+        e[1] += u[a][1] * g[a][1];
+        e[2] += u[a][2] * g[a][2];
+        e[3] += u[a][2] * g[a][1] + u[a][1] * g[a][2];
+        e[4] += u[a][2] * g[a][0] + u[a][0] * g[a][2];
+        e[5] += u[a][1] * g[a][0] + u[a][0] * g[a][1];
+    }
+}
+
+// Isotropic stress sigma = C eps, LinearStress (src/LinearStress.hpp:102-120).
+template <typename T>
+__device__ __forceinline__ void stress_voigt(const Material& m, const T e[6], T s[6]) {
+    const T c00 = T(m.c00), c01 = T(m.c01), c33 = T(m.c33);
+    s[0] = e[0] * c00 + e[1] * c01 + e[2] * c01;
+    s[1] = e[0] * c01 + e[1] * c00 + e[2] * c01;
+    s[2] = e[0] * c01 + e[1] * c01 + e[2] * c00;
+    s[3] = e[3] * c33;
+    s[4] = e[4] * c33;
+    s[5] = e[5] * c33;
+}
+
+// f_a = vol * B_a^T sigma: StressDivergence<3> (src/StressDivergence.hpp:70-90) for node a.
+template <typename T>
+__device__ __forceinline__ void divergence_node(const T ga[3], const T s[6], T w, T f[3]) {
+    f[0] = w * (s[0] * ga[0] + s[5] * ga[1] + s[4] * ga[2]);
+    f[1] = w * (s[5] * ga[0] + s[1] * ga[1] + s[3] * ga[2]);
+    f[2] = w * (s[4] * ga[0] + s[3] * ga[1] + s[2] * ga[2]);
+}
+
+// 3x3 block (a,b) of the element stiffness w * B_a^T C B_b for isotropic C:
+// K_ab[i][j] = w (lambda ga_i gb_j + mu ga_j gb_i + mu (ga . gb) delta_ij).
+template <typename T>
+__device__ __forceinline__ void stiffness_block(const Material& m, const T ga[3], const T gb[3],
+                                                T w, T K[9]) {
+    const T lam = T(m.c01) * w, mu = T(m.c33) * w;
+    const T dot = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            T v = lam * ga[i] * gb[j] + mu * ga[j] * gb[i];
+            if (i == j) v += mu * dot;
+            K[3 * i + j] = v;
+        }
+}
+
+}  // namespace plato

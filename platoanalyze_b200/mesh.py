@@ -1,0 +1,59 @@
+"""Structured tet box meshes (host arrays) through the library's generator."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from .capi import check, lib
+
+X_MINUS, X_PLUS, Y_MINUS, Y_PLUS, Z_MINUS, Z_PLUS = range(6)
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+@dataclass
+class BoxMesh:
+    nx: int
+    ny: int
+    nz: int
+    lx: float
+    ly: float
+    lz: float
+    coords: np.ndarray        # (N, 3) float64
+    connectivity: np.ndarray  # (C, 4) int32
+
+    @property
+    def num_nodes(self) -> int:
+        return self.coords.shape[0]
+
+    @property
+    def num_cells(self) -> int:
+        return self.connectivity.shape[0]
+
+    def nodeset(self, face: int) -> np.ndarray:
+        cnt = C.c_int32(0)
+        check(lib.plato_box_nodeset(self.nx, self.ny, self.nz, face, None, C.byref(cnt)))
+        out = np.empty(cnt.value, dtype=np.int32)
+        check(lib.plato_box_nodeset(self.nx, self.ny, self.nz, face, _ptr(out), C.byref(cnt)))
+        return out
+
+    def sideset(self, face: int) -> tuple[np.ndarray, np.ndarray]:
+        cnt = C.c_int32(0)
+        check(lib.plato_box_sideset(self.nx, self.ny, self.nz, face, None, None, C.byref(cnt)))
+        cells = np.empty(cnt.value, dtype=np.int32)
+        local = np.empty((cnt.value, 3), dtype=np.int32)
+        check(lib.plato_box_sideset(self.nx, self.ny, self.nz, face, _ptr(cells), _ptr(local), C.byref(cnt)))
+        return cells, local
+
+
+def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0, lz: float = 1.0) -> BoxMesh:
+    nn, nc = C.c_int32(0), C.c_int32(0)
+    check(lib.plato_box_mesh_sizes(nx, ny, nz, C.byref(nn), C.byref(nc)))
+    coords = np.empty((nn.value, 3), dtype=np.float64)
+    conn = np.empty((nc.value, 4), dtype=np.int32)
+    check(lib.plato_box_mesh_tet4(nx, ny, nz, lx, ly, lz, _ptr(coords), _ptr(conn)))
+    return BoxMesh(nx, ny, nz, lx, ly, lz, coords, conn)

@@ -1,0 +1,232 @@
+"""Python mirror of the reference's elliptic interfaces over the C ABI.
+
+`EllipticProblem` owns one plato_problem handle and exposes the reference's method names:
+VectorFunction (`vf_value`, `vf_gradient_u`, `vf_gradient_u_T`, `vf_gradient_z`),
+PhysicsScalarFunction "Internal Elastic Energy" (`sf_value`, `sf_gradient_u`,
+`sf_gradient_z`) and Problem (`solution`, `criterion_value`, `criterion_gradient`).
+Device buffers are torch CUDA tensors (torch is used for memory and streams only; all
+arithmetic runs in the library's kernels).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+from .capi import check, lib
+from .mesh import BoxMesh
+
+
+def _np_ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class SolverOptions:
+    tolerance: float = 1e-10
+    max_iterations: int = 20000
+    operator_kind: int = capi.OPERATOR_ASSEMBLED
+    precision: int = capi.PRECISION_FP64
+    self_adjoint: bool = True
+    inner_tolerance: float = 1e-4
+    max_refinements: int = 50
+
+    def to_c(self) -> capi.SolverOpts:
+        return capi.SolverOpts(self.tolerance, self.max_iterations, self.operator_kind, self.precision,
+                               int(self.self_adjoint), self.inner_tolerance, self.max_refinements)
+
+
+@dataclass
+class ProblemSpec:
+    coords: np.ndarray
+    connectivity: np.ndarray
+    youngs_modulus: float = 1.0
+    poissons_ratio: float = 0.3
+    penalty_exponent: float = 3.0
+    penalty_minimum: float = 1e-9
+    tractions: list = field(default_factory=list)  # [(face_cells, face_local_nodes, (tx,ty,tz))]
+    bc_dofs: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    bc_values: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    solver: SolverOptions = field(default_factory=SolverOptions)
+
+
+def cantilever_spec(mesh: BoxMesh, traction=(0.0, -1.0, 0.0), E=1.0, nu=0.3, p=3.0, rho_min=1e-9,
+                    solver: SolverOptions | None = None) -> ProblemSpec:
+    """Box clamped on x = 0 (all three dofs), uniform traction on the x = Lx face."""
+    from .mesh import X_MINUS, X_PLUS
+    fixed = mesh.nodeset(X_MINUS)
+    dofs = (3 * fixed[:, None] + np.arange(3)[None, :]).reshape(-1).astype(np.int32)
+    cells, local = mesh.sideset(X_PLUS)
+    return ProblemSpec(mesh.coords, mesh.connectivity, E, nu, p, rho_min,
+                       [(cells, local, traction)], dofs, np.zeros(dofs.size), solver or SolverOptions())
+
+
+class EllipticProblem:
+    def __init__(self, spec: ProblemSpec, stream=None):
+        import torch  # device memory and streams only
+
+        self.torch = torch
+        self.spec = spec
+        coords = np.ascontiguousarray(spec.coords, dtype=np.float64)
+        conn = np.ascontiguousarray(spec.connectivity, dtype=np.int32)
+        self._keep = [coords, conn]
+        nbcs = (capi.NaturalBC * max(1, len(spec.tractions)))()
+        for k, (cells, local, vec) in enumerate(spec.tractions):
+            cells = np.ascontiguousarray(cells, dtype=np.int32)
+            local = np.ascontiguousarray(local, dtype=np.int32)
+            self._keep += [cells, local]
+            nbcs[k].num_faces = cells.size
+            nbcs[k].face_cells = cells.ctypes.data_as(capi.i32p)
+            nbcs[k].face_local_nodes = local.ctypes.data_as(capi.i32p)
+            nbcs[k].vector = (C.c_double * 3)(*vec)
+        dofs = np.ascontiguousarray(spec.bc_dofs, dtype=np.int32)
+        vals = np.ascontiguousarray(spec.bc_values, dtype=np.float64)
+        self._keep += [dofs, vals]
+        desc = capi.ProblemDesc()
+        desc.mesh = capi.MeshDesc(coords.shape[0], conn.shape[0], coords.ctypes.data_as(capi.f64p),
+                                  conn.ctypes.data_as(capi.i32p))
+        desc.material = capi.Material(spec.youngs_modulus, spec.poissons_ratio)
+        desc.penalty = capi.Penalty(spec.penalty_exponent, spec.penalty_minimum)
+        desc.num_natural_bcs = len(spec.tractions)
+        desc.natural_bcs = nbcs
+        desc.essential_bcs = capi.EssentialBCs(dofs.size, dofs.ctypes.data_as(capi.i32p),
+                                               vals.ctypes.data_as(capi.f64p))
+        desc.solver = spec.solver.to_c()
+        h = C.c_void_p()
+        check(lib.plato_create(C.byref(desc), C.byref(h)))
+        self.h = h
+        self.set_stream(stream if stream is not None else torch.cuda.current_stream())
+        nn, nc, nb = C.c_int32(), C.c_int32(), C.c_int64()
+        check(lib.plato_get_sizes(h, C.byref(nn), C.byref(nc), C.byref(nb)), h)
+        self.num_nodes, self.num_cells, self.num_blocks = nn.value, nc.value, nb.value
+        self.num_dofs = 3 * self.num_nodes
+
+    # -- plumbing ------------------------------------------------------------------------
+    def set_stream(self, stream) -> None:
+        self.stream = stream
+        check(lib.plato_set_stream(self.h, C.c_void_p(stream.cuda_stream)), self.h)
+
+    def set_solver(self, opts: SolverOptions) -> None:
+        o = opts.to_c()
+        check(lib.plato_set_solver_opts(self.h, C.byref(o)), self.h)
+        self.spec.solver = opts
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib.plato_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _dev(self, t):
+        assert t.is_cuda and t.is_contiguous(), "device tensors must be contiguous CUDA tensors"
+        return C.c_void_p(t.data_ptr())
+
+    def zeros(self, n, dtype=None):
+        return self.torch.zeros(n, dtype=dtype or self.torch.float64, device="cuda")
+
+    def to_dev(self, a: np.ndarray):
+        return self.torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    # -- pattern ---------------------------------------------------------------------------
+    def pattern(self):
+        rm = self.zeros(self.num_nodes + 1, self.torch.int32)
+        cols = self.zeros(self.num_blocks, self.torch.int32)
+        check(lib.plato_jacobian_pattern(self.h, self._dev(rm), self._dev(cols)), self.h)
+        return rm, cols
+
+    # -- VectorFunction ----------------------------------------------------------------------
+    def vf_value(self, u, z):
+        R = self.zeros(self.num_dofs)
+        check(lib.plato_vf_value(self.h, self._dev(u), self._dev(z), self._dev(R)), self.h)
+        return R
+
+    def vf_gradient_u(self, u, z):
+        K = self.zeros(9 * self.num_blocks)
+        check(lib.plato_vf_gradient_u(self.h, self._dev(u), self._dev(z), self._dev(K)), self.h)
+        return K
+
+    def vf_gradient_u_T(self, u, z):
+        K = self.zeros(9 * self.num_blocks)
+        check(lib.plato_vf_gradient_u_T(self.h, self._dev(u), self._dev(z), self._dev(K)), self.h)
+        return K
+
+    def vf_gradient_z(self, u, z):
+        G = self.zeros(3 * self.num_blocks)
+        check(lib.plato_vf_gradient_z(self.h, self._dev(u), self._dev(z), self._dev(G)), self.h)
+        return G
+
+    def vf_gradient_z_apply(self, u, z, lam, out):
+        check(lib.plato_vf_gradient_z_apply(self.h, self._dev(u), self._dev(z), self._dev(lam), self._dev(out)),
+              self.h)
+        return out
+
+    # -- ScalarFunction ------------------------------------------------------------------------
+    def sf_value(self, u, z) -> float:
+        v = C.c_double()
+        check(lib.plato_sf_value(self.h, self._dev(u), self._dev(z), C.byref(v)), self.h)
+        return v.value
+
+    def sf_gradient_u(self, u, z):
+        g = self.zeros(self.num_dofs)
+        check(lib.plato_sf_gradient_u(self.h, self._dev(u), self._dev(z), self._dev(g)), self.h)
+        return g
+
+    def sf_gradient_z(self, u, z):
+        g = self.zeros(self.num_nodes)
+        check(lib.plato_sf_gradient_z(self.h, self._dev(u), self._dev(z), self._dev(g)), self.h)
+        return g
+
+    # -- helpers ---------------------------------------------------------------------------------
+    def apply_constraints(self, entries, rhs, scale=1.0):
+        check(lib.plato_apply_constraints(self.h, self._dev(entries), self._dev(rhs) if rhs is not None else None,
+                                          scale), self.h)
+
+    def matvec_plus(self, rb, cb, entries, x, y):
+        check(lib.plato_matvec_plus(self.h, rb, cb, self._dev(entries), self._dev(x), self._dev(y)), self.h)
+        return y
+
+    def solver_solve(self, entries, x, b):
+        st = capi.SolveStats()
+        check(lib.plato_solver_solve(self.h, self._dev(entries), self._dev(x), self._dev(b), C.byref(st)), self.h)
+        return st.as_dict()
+
+    # -- Problem -------------------------------------------------------------------------------------
+    def solution(self, z, u0=None, raise_on_error=True):
+        u = self.zeros(self.num_dofs)
+        st = capi.SolveStats()
+        rc = lib.plato_problem_solution(self.h, self._dev(z), self._dev(u0) if u0 is not None else None,
+                                        self._dev(u), C.byref(st))
+        if raise_on_error:
+            check(rc, self.h)
+        return u, st.as_dict() | {"rc": rc}
+
+    def criterion_value(self, z, u) -> float:
+        v = C.c_double()
+        check(lib.plato_problem_criterion_value(self.h, self._dev(z), self._dev(u), C.byref(v)), self.h)
+        return v.value
+
+    def criterion_gradient(self, z, u):
+        g = self.zeros(self.num_nodes)
+        st = capi.SolveStats()
+        check(lib.plato_problem_criterion_gradient(self.h, self._dev(z), self._dev(u), self._dev(g), C.byref(st)),
+              self.h)
+        return g, st.as_dict()
+
+    def solve_and_gradient_host(self, z: np.ndarray, u0: np.ndarray | None = None, u_out=None, g_out=None):
+        """One optimisation step on host (numpy) buffers; returns (u, value, dfdz, stats)."""
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        u = u_out if u_out is not None else np.empty(self.num_dofs)
+        g = g_out if g_out is not None else np.empty(self.num_nodes)
+        v = C.c_double()
+        st = capi.SolveStats()
+        rc = lib.plato_problem_solve_and_gradient_host(self.h, _np_ptr(z), _np_ptr(u0) if u0 is not None else None,
+                                                       _np_ptr(u), C.byref(v), _np_ptr(g), C.byref(st))
+        check(rc, self.h)
+        return u, v.value, g, st.as_dict()

@@ -128,6 +128,15 @@ int plato_set_stream(plato_problem* h, void* cuda_stream);
 int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* opts);
 int plato_get_sizes(const plato_problem* h, int32_t* num_nodes, int32_t* num_cells,
                     int64_t* num_blocks);
+/* Instrumentation (no reference counterpart; the reference times phases with
+ * Teuchos::TimeMonitor, src/alg/EpetraLinearSolver.cpp:16-17).  With timing enabled, every
+ * 8th operator apply inside the solver is bracketed by CUDA events on the handle's stream;
+ * op_ms_total / op_timed is the average apply duration.  launches counts every kernel the
+ * handle has launched. */
+int plato_set_timing(plato_problem* h, int32_t enable);
+int plato_get_instrumentation(const plato_problem* h, int64_t* launches, double* op_ms_total,
+                              int64_t* op_timed);
+int plato_reset_instrumentation(plato_problem* h);
 
 /* ---- block pattern ---------------------------------------------------------------------
  * CreateBlockMatrix (src/ImplicitFunctors.hpp:932-1005) over the node-node graph

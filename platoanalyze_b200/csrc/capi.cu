@@ -105,6 +105,7 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_K); dfree(h->h_K); dfree(h->f_coords); dfree(h->f_z_ctrl); dfree(h->d_z_ctrl);
     dfree(h->d_z_in); dfree(h->d_u_out); dfree(h->d_g_out);
     if (h->scal_host) cudaFreeHost(h->scal_host);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     delete h;
     return PLATO_OK;
 }
@@ -244,6 +245,29 @@ int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* o) {
     NEED(h, o != nullptr, "null solver options");
     RC(check_opts(h, *o));
     h->opts = *o;
+    return PLATO_OK;
+}
+
+int plato_set_timing(plato_problem* h, int32_t enable) {
+    if (!h) return PLATO_BAD_INPUT;
+    h->timing = enable ? 1 : 0;
+    return PLATO_OK;
+}
+
+int plato_get_instrumentation(const plato_problem* h, int64_t* launches, double* op_ms_total,
+                              int64_t* op_timed) {
+    if (!h) return PLATO_BAD_INPUT;
+    if (launches) *launches = h->launches;
+    if (op_ms_total) *op_ms_total = h->op_ms_total;
+    if (op_timed) *op_timed = h->op_timed;
+    return PLATO_OK;
+}
+
+int plato_reset_instrumentation(plato_problem* h) {
+    if (!h) return PLATO_BAD_INPUT;
+    h->launches = 0;
+    h->op_ms_total = 0.0;
+    h->op_timed = 0;
     return PLATO_OK;
 }
 

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "plato_b200.h"
 
@@ -123,6 +124,14 @@ struct plato_problem {
     double* d_z_in = nullptr;
     double* d_u_out = nullptr;
     double* d_g_out = nullptr;
+    // instrumentation: kernel launches issued, and sampled CUDA-event timings of the
+    // solver's operator apply (every kTimingStride-th apply, events on the handle's stream)
+    int64_t launches = 0;
+    int     timing = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    int     ev_used = 0;
+    double  op_ms_total = 0.0;
+    int64_t op_timed = 0;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -138,6 +147,7 @@ int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const cha
 
 #define PLATO_LAUNCH_CHECK(h)                                                        \
     do {                                                                             \
+        (h)->launches += 1;                                                          \
         cudaError_t _e = cudaGetLastError();                                         \
         if (_e != cudaSuccess) return plato_cuda_fail((h), _e, "kernel launch", __FILE__, __LINE__); \
     } while (0)

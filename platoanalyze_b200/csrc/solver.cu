@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 32;
+constexpr int kTimingStride = 8;
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -253,6 +254,39 @@ int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, do
     return PLATO_OK;
 }
 
+
+#define RC_(expr)              \
+    do {                       \
+        int _rc = (expr);      \
+        if (_rc) return _rc;   \
+    } while (0)
+
+// Event pairs for the sampled operator timings (reused across solves).
+int timing_events(plato_problem* h, cudaEvent_t* e0, cudaEvent_t* e1) {
+    while ((int)h->ev_pool.size() < h->ev_used + 2) {
+        cudaEvent_t e;
+        PLATO_CUDA(h, cudaEventCreate(&e));
+        h->ev_pool.push_back(e);
+    }
+    *e0 = h->ev_pool[h->ev_used];
+    *e1 = h->ev_pool[h->ev_used + 1];
+    h->ev_used += 2;
+    return PLATO_OK;
+}
+
+// Adds the durations of the timed applies that belonged to executed iterations.
+int collect_timing(plato_problem* h, const std::vector<int64_t>& iters, int64_t executed) {
+    for (size_t k = 0; k < iters.size(); ++k) {
+        if (iters[k] >= executed) break;
+        float ms = 0.f;
+        PLATO_CUDA(h, cudaEventElapsedTime(&ms, h->ev_pool[2 * k], h->ev_pool[2 * k + 1]));
+        h->op_ms_total += ms;
+        h->op_timed += 1;
+    }
+    h->ev_used = 0;
+    return PLATO_OK;
+}
+
 int launch_spmv(plato_problem* h, const double* A, const double* x, double* y) {
     const int blocks = grid_for((int64_t)h->N * 32, kThreads, 148 * 16);
     k_bsr_spmv<<<blocks, kThreads, 0, h->stream>>>(h->N, h->row_map, h->cols, A, x, y, nullptr, nullptr);
@@ -285,6 +319,7 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
     PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
 
     int32_t restarts = 0;
+    int32_t iter_base = 0;
     bool keep_bb = false;
     for (;;) {
         // r = b - A x ; z = Dinv r ; p = z
@@ -295,19 +330,31 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
         PLATO_LAUNCH_CHECK(h);
         // iterate in chunks; poll the scalars of the previous chunk while the next one runs
         PcgScalars* slots = h->scal_host;
+        int64_t enqueued = 0;
+        std::vector<int64_t> timed_iters;
+        h->ev_used = 0;
         int cur = 0;
         bool have_prev = false;
         cudaEvent_t ev[2];
         PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
         PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
         for (;;) {
-            for (int k = 0; k < kChunk; ++k) {
+            for (int k = 0; k < kChunk; ++k, ++enqueued) {
+                const bool timed = h->timing && (enqueued % kTimingStride) == 0;
+                cudaEvent_t e0 = nullptr, e1 = nullptr;
+                if (timed) {
+                    RC_(timing_events(h, &e0, &e1));
+                    timed_iters.push_back(enqueued);
+                    PLATO_CUDA(h, cudaEventRecord(e0, s));
+                }
                 k_bsr_spmv<<<spmv_blocks, kThreads, 0, s>>>(h->N, h->row_map, h->cols, A, h->v_p, h->v_Ap,
                                                             h->scal, h->partials);
+                if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
                 k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_Ap, h->v_dinv, h->v_z,
                                                              h->scal, h->partials, max_it);
                 k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
             }
+            h->launches += 3 * kChunk - 1;
             PLATO_LAUNCH_CHECK(h);
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
@@ -323,6 +370,8 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
         cudaEventDestroy(ev[1]);
         PcgScalars fin;
         PLATO_CUDA(h, cudaMemcpy(&fin, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
+        RC_(collect_timing(h, timed_iters, fin.iter - iter_base));
+        iter_base = fin.iter;
         if (fin.nonfinite) {
             stats->iterations = fin.iter;
             stats->refinements = 1;

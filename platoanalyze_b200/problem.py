@@ -113,6 +113,17 @@ class EllipticProblem:
         check(lib.plato_set_solver_opts(self.h, C.byref(o)), self.h)
         self.spec.solver = opts
 
+    def set_timing(self, enable: bool) -> None:
+        check(lib.plato_set_timing(self.h, int(enable)), self.h)
+
+    def instrumentation(self) -> dict:
+        n, ms, k = C.c_int64(), C.c_double(), C.c_int64()
+        check(lib.plato_get_instrumentation(self.h, C.byref(n), C.byref(ms), C.byref(k)), self.h)
+        return {"launches": n.value, "op_ms_total": ms.value, "op_timed": k.value}
+
+    def reset_instrumentation(self) -> None:
+        check(lib.plato_reset_instrumentation(self.h), self.h)
+
     def close(self) -> None:
         if getattr(self, "h", None):
             lib.plato_destroy(self.h)

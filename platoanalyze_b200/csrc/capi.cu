@@ -18,7 +18,9 @@ int launch_assemble_gradient_z(plato_problem* h, const double* u, const double* 
 int launch_dirichlet(plato_problem* h, double* A, double* rhs, double scale);
 int launch_matvec_plus(plato_problem* h, int rb, int cb, const double* A, const double* x, double* y);
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
-int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, double* x, plato_solve_stats* stats);
+int build_sell_pattern(plato_problem* h);
+int prepare_operator(plato_problem* h, const double* crs);
+int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
 int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* stats);
 int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* stats);
 }  // namespace plato
@@ -104,6 +106,9 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_r); dfree(h->f_z); dfree(h->f_p); dfree(h->f_Ap); dfree(h->f_x); dfree(h->f_dinv);
     dfree(h->f_K); dfree(h->h_K); dfree(h->f_coords); dfree(h->f_z_ctrl); dfree(h->d_z_ctrl);
     dfree(h->d_z_in); dfree(h->d_u_out); dfree(h->d_g_out);
+    dfree(h->sell.width); dfree(h->sell.ptr); dfree(h->sell.cols);
+    dfree(h->sell64); dfree(h->sell32);
+    if (h->sell16) cudaFree(h->sell16);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     delete h;
@@ -167,6 +172,7 @@ int plato_create(const plato_problem_desc* d, plato_problem** out) {
     CCUDA(cudaMemcpy(h->conn, m.connectivity, sizeof(int4) * size_t(h->C), cudaMemcpyHostToDevice));
     CCUDA(cudaMemcpy(h->coords, m.coords, sizeof(double) * size_t(n), cudaMemcpyHostToDevice));
     CRC(build_graph(h));
+    CRC(build_sell_pattern(h));
 
     // essential BCs
     const plato_essential_bcs& bc = d->essential_bcs;
@@ -346,7 +352,8 @@ int plato_solver_solve(plato_problem* h, const double* entries, double* x, const
     NEED(h, entries && x && b, "null device pointer");
     plato_solve_stats local{};
     plato_solve_stats* st = stats ? stats : &local;
-    return pcg_fp64_assembled(h, entries, b, x, st);
+    RC(prepare_operator(h, entries));
+    return pcg_fp64(h, b, x, st);
 }
 
 int plato_problem_solution(plato_problem* h, const double* z, const double* u0, double* u,
@@ -421,12 +428,13 @@ int solve_state(plato_problem* h, const double* z, const double* u0, double* u, 
     RC(launch_assemble_jacobian(h, z, h->K));
     PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, h->F, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     RC(launch_dirichlet(h, h->K, h->v_b, 1.0));
+    RC(prepare_operator(h, h->K));
     if (u0) {
         if (u0 != u) PLATO_CUDA(h, cudaMemcpyAsync(u, u0, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     } else {
         PLATO_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n, h->stream));
     }
-    return pcg_fp64_assembled(h, h->K, h->v_b, u, st);
+    return pcg_fp64(h, h->v_b, u, st);
 }
 
 // Adjoint solve K^T lambda = rhs with zero-valued constraints.
@@ -437,8 +445,9 @@ int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* 
     if (rhs != h->v_b)
         PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     RC(launch_dirichlet(h, h->K, h->v_b, 0.0));
+    RC(prepare_operator(h, h->K));
     PLATO_CUDA(h, cudaMemsetAsync(lam, 0, sizeof(double) * n, h->stream));
-    return pcg_fp64_assembled(h, h->K, h->v_b, lam, st);
+    return pcg_fp64(h, h->v_b, lam, st);
 }
 
 }  // namespace plato

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "plato_b200.h"
+#include "sell.cuh"
 
 namespace plato {
 
@@ -124,6 +125,11 @@ struct plato_problem {
     double* d_z_in = nullptr;
     double* d_u_out = nullptr;
     double* d_g_out = nullptr;
+    // solver-private SELL-32 copy of the constrained operator (sell.cu)
+    plato::SellPattern sell{};
+    double* sell64 = nullptr;      // FP64 entries
+    float*  sell32 = nullptr;      // FP32 entries (mixed precision)
+    void*   sell16 = nullptr;      // BF16 entries (mixed precision)
     // instrumentation: kernel launches issued, and sampled CUDA-event timings of the
     // solver's operator apply (every kTimingStride-th apply, events on the handle's stream)
     int64_t launches = 0;

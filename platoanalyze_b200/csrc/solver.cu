@@ -7,111 +7,45 @@
 // confirming with the recomputed residual b - A x.
 //
 // Per iteration three kernels run back to back on the handle's stream with no host
-// round-trip: (1) block-CRS SpMV fused with the p.Ap reduction, (2) the x/r update fused
-// with the Jacobi apply and the r.z and r.r reductions, (3) the search-direction update.
-// The global scalars (alpha, beta, convergence) live in device memory; each reduction is
-// finished by the last block to arrive (ticket counter), so there is no extra launch and no
-// spin-wait.  The host polls a pinned copy of the scalars every kChunk iterations while the
-// next chunk is already queued, and every kernel returns at once after convergence.
+// round-trip: (1) SELL-32 SpMV fused with the p.Ap reduction and alpha, (2) the x/r update
+// fused with the Jacobi apply and the r.z / r.r reductions, beta and the stop test, (3) the
+// search-direction update.  The scalars live in device memory; each reduction is finished
+// by the last block to arrive (ticket counter): no extra launch, no spin-wait.  The host
+// polls a pinned copy of the scalars every kChunk iterations while the next chunk is
+// already queued, and every kernel returns at once after convergence.
 #include "plato_internal.cuh"
+#include "solver_common.cuh"
 
 namespace plato {
 
-MeshView mesh_view(const plato_problem* h);
-GraphView graph_view(const plato_problem* h);
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
+int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float* out32, void* out16,
+                       double* dinv, float* dinv32);
 
 namespace {
 
-constexpr int kThreads = 256;
 constexpr int kChunk = 32;
 constexpr int kTimingStride = 8;
 
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Sums NV per-thread values over the block; thread 0 gets the result.
-template <int NV>
-__device__ __forceinline__ void block_sum_n(double (&v)[NV], double (*sh)[32]) {
-#pragma unroll
-    for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0)
-#pragma unroll
-        for (int q = 0; q < NV; ++q) sh[q][w] = v[q];
-    __syncthreads();
-    if (w == 0) {
-        const int nw = blockDim.x >> 5;
-#pragma unroll
-        for (int q = 0; q < NV; ++q) v[q] = warp_sum(l < nw ? sh[q][l] : 0.0);
-    }
-    __syncthreads();
-}
-
-// Last-block-done: returns true in the block that finishes last; partials[NV*block + q]
-// hold every block's sums.
-template <int NV>
-__device__ __forceinline__ bool publish_partials(const double (&v)[NV], double* partials,
-                                                 unsigned int* ticket, bool* sh_last) {
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) partials[NV * blockIdx.x + q] = v[q];
-        __threadfence();
-        *sh_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    return *sh_last;
-}
-
-template <int NV>
-__device__ __forceinline__ void final_sums(double (&t)[NV], const double* partials, double (*sh)[32]) {
-    __threadfence();
-#pragma unroll
-    for (int q = 0; q < NV; ++q) t[q] = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-#pragma unroll
-        for (int q = 0; q < NV; ++q) t[q] += partials[NV * b + q];
-    block_sum_n<NV>(t, sh);
-}
-
-__device__ __forceinline__ bool finite(double v) { return isfinite(v); }
-
-// y = A x on the 3x3 block CRS, one warp per node row: lanes stream the row's 9*nb values
-// contiguously (coalesced), gather x through L2, and reduce the three row sums with
-// shuffles.  With S != nullptr the kernel also forms p.Ap (x = p, y = Ap) and alpha.
+// y = A x on the SELL copy; with S != nullptr also p.Ap (x = p, y = Ap) and alpha.
 __global__ void __launch_bounds__(kThreads)
-k_bsr_spmv(int32_t N, const int32_t* __restrict__ row_map, const int32_t* __restrict__ cols,
-           const double* __restrict__ A, const double* __restrict__ x, double* __restrict__ y,
-           PcgScalars* S, double* partials) {
+k_sell_spmv(SellView A, const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
+            PcgScalars* S, double* partials) {
     __shared__ double sh[1][32];
     __shared__ bool last;
     if (S && S->done) return;
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     double dot = 0.0;
-    for (int64_t r = warp; r < N; r += nwarps) {
-        const int32_t rs = row_map[r], re = row_map[r + 1];
-        const int64_t base = 9 * (int64_t)rs, end = 9 * (int64_t)re;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        int blk = lane / 9, ij = lane - 9 * (lane / 9);
-        for (int64_t t = base + lane; t < end; t += 32) {
-            const int i = (ij * 11) >> 5, j = ij - 3 * i;
-            const double prod = __ldg(A + t) * __ldg(x + 3 * (int64_t)__ldg(cols + rs + blk) + j);
-            a0 += (i == 0) ? prod : 0.0;
-            a1 += (i == 1) ? prod : 0.0;
-            a2 += (i == 2) ? prod : 0.0;
-            blk += 3;
-            ij += 5;
-            if (ij >= 9) { ij -= 9; ++blk; }
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < padded; r += nthreads) {
+        double a0, a1, a2;
+        sell_row<double>(A, vals, x, r, a0, a1, a2);
+        if (r < A.num_rows) {
+            y[3 * r] = a0;
+            y[3 * r + 1] = a1;
+            y[3 * r + 2] = a2;
+            if (S) dot += x[3 * r] * a0 + x[3 * r + 1] * a1 + x[3 * r + 2] * a2;
         }
-        a0 = warp_sum(a0);
-        a1 = warp_sum(a1);
-        a2 = warp_sum(a2);
-        if (lane < 3) y[3 * r + lane] = lane == 0 ? a0 : (lane == 1 ? a1 : a2);
-        if (S && lane == 0) dot += x[3 * r] * a0 + x[3 * r + 1] * a1 + x[3 * r + 2] * a2;
     }
     if (!S) return;
     double v[1] = {dot};
@@ -122,7 +56,7 @@ k_bsr_spmv(int32_t N, const int32_t* __restrict__ row_map, const int32_t* __rest
         if (threadIdx.x == 0) {
             S->pAp = t[0];
             S->alpha = S->rz / t[0];
-            if (!finite(S->alpha) || t[0] <= 0.0) { S->nonfinite = 1; S->done = 1; }
+            if (!isfinite(S->alpha) || t[0] <= 0.0) { S->nonfinite = 1; S->done = 1; }
             S->ticket = 0u;
         }
     }
@@ -158,7 +92,7 @@ k_pcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r, const do
             S->rz = t[0];
             S->rr = t[1];
             S->iter += 1;
-            if (!finite(t[0]) || !finite(t[1])) { S->nonfinite = 1; S->done = 1; }
+            if (!isfinite(t[0]) || !isfinite(t[1])) { S->nonfinite = 1; S->done = 1; }
             if (t[1] <= S->tol2 || S->iter >= max_it) S->done = 1;
             S->ticket = 0u;
         }
@@ -174,7 +108,7 @@ k_pcg_direction(int64_t n, const double* __restrict__ z, double* __restrict__ p,
         p[i] = z[i] + beta * p[i];
 }
 
-// r = b - Ax (Ax already in r_in_Ax); z = Dinv r; p = z; sums r.z, r.r, b.b -> init scalars.
+// r = b - r (r holds A x on entry); z = Dinv r; p = z; sums r.z, r.r, b.b -> start scalars.
 __global__ void __launch_bounds__(kThreads)
 k_pcg_start(int64_t n, const double* __restrict__ b, double* __restrict__ r, const double* __restrict__ dinv,
             double* __restrict__ z, double* __restrict__ p, PcgScalars* S, double* partials, double tol,
@@ -205,20 +139,10 @@ k_pcg_start(int64_t n, const double* __restrict__ b, double* __restrict__ r, con
                 S->tol2 = tol * tol * t[2];
                 S->iter = 0;
             }
-            S->nonfinite = (!finite(t[0]) || !finite(t[1]) || !finite(t[2])) ? 1 : 0;
+            S->nonfinite = (!isfinite(t[0]) || !isfinite(t[1]) || !isfinite(t[2])) ? 1 : 0;
             S->done = (t[1] <= S->tol2 || S->nonfinite) ? 1 : 0;
             S->ticket = 0u;
         }
-    }
-}
-
-__global__ void k_jacobi_from_blocks(int32_t N, const int32_t* __restrict__ diag, const double* __restrict__ A,
-                                     double* __restrict__ dinv) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3 * (int64_t)N;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = t / 3;
-        const int d = int(t - 3 * a);
-        dinv[t] = 1.0 / A[9 * (int64_t)diag[a] + 4 * d];
     }
 }
 
@@ -244,22 +168,12 @@ k_dot(int64_t n, const double* __restrict__ a, const double* __restrict__ b, dou
 
 }  // namespace
 
-// a.b into *host_result (synchronises the stream).
-int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, double* host_result) {
-    const int blocks = grid_for(n, kThreads, h->partials_len);
-    k_dot<<<blocks, kThreads, 0, h->stream>>>(n, a, b, h->partials, h->red_ticket, h->red_out);
-    PLATO_LAUNCH_CHECK(h);
-    PLATO_CUDA(h, cudaMemcpyAsync(host_result, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
-    return PLATO_OK;
+SellView sell_view(const plato_problem* h) { return SellView{h->N, h->sell.width, h->sell.ptr, h->sell.cols}; }
+
+int spmv_blocks(const plato_problem* h) {
+    const int64_t padded = ((int64_t)h->N + 31) & ~int64_t(31);
+    return grid_for(padded, kThreads, 148 * 16);
 }
-
-
-#define RC_(expr)              \
-    do {                       \
-        int _rc = (expr);      \
-        if (_rc) return _rc;   \
-    } while (0)
 
 // Event pairs for the sampled operator timings (reused across solves).
 int timing_events(plato_problem* h, cudaEvent_t* e0, cudaEvent_t* e1) {
@@ -287,35 +201,43 @@ int collect_timing(plato_problem* h, const std::vector<int64_t>& iters, int64_t 
     return PLATO_OK;
 }
 
-int launch_spmv(plato_problem* h, const double* A, const double* x, double* y) {
-    const int blocks = grid_for((int64_t)h->N * 32, kThreads, 148 * 16);
-    k_bsr_spmv<<<blocks, kThreads, 0, h->stream>>>(h->N, h->row_map, h->cols, A, x, y, nullptr, nullptr);
+// a.b into *host_result (synchronises the stream).
+int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, double* host_result) {
+    const int blocks = grid_for(n, kThreads, h->partials_len);
+    k_dot<<<blocks, kThreads, 0, h->stream>>>(n, a, b, h->partials, h->red_ticket, h->red_out);
+    PLATO_LAUNCH_CHECK(h);
+    PLATO_CUDA(h, cudaMemcpyAsync(host_result, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PLATO_OK;
+}
+
+int launch_sell_spmv(plato_problem* h, const double* vals, const double* x, double* y) {
+    k_sell_spmv<<<spmv_blocks(h), kThreads, 0, h->stream>>>(sell_view(h), vals, x, y, nullptr, nullptr);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }
 
-int launch_jacobi(plato_problem* h, const double* A, double* dinv) {
-    k_jacobi_from_blocks<<<grid_for(3 * (int64_t)h->N, kThreads), kThreads, 0, h->stream>>>(h->N, h->diag, A, dinv);
-    PLATO_LAUNCH_CHECK(h);
-    return PLATO_OK;
+// Makes the SELL copy (and Jacobi diagonal) of a constrained CRS matrix.
+int prepare_operator(plato_problem* h, const double* crs) {
+    if (!h->sell64) PLATO_CUDA(h, cudaMalloc(&h->sell64, sizeof(double) * 9 * size_t(h->sell.total_slots)));
+    return launch_crs_to_sell(h, crs, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
 }
 
-// Solves A x = b (A assembled, constrained).  x holds the initial guess.
-int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, double* x,
-                       plato_solve_stats* stats) {
+// Solves A x = b with A in h->sell64 and its inverse diagonal in h->v_dinv.  x holds the
+// initial guess on entry.
+int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
+    const double* A = h->sell64;
     const int64_t n = 3 * (int64_t)h->N;
     cudaStream_t s = h->stream;
     const double tol = h->opts.tolerance;
     const int32_t max_it = h->opts.max_iterations;
     const int vec_blocks = grid_for(n, kThreads, 148 * 16);
-    const int spmv_blocks = grid_for((int64_t)h->N * 32, kThreads, 148 * 16);
-    if (vec_blocks * 3 > h->partials_len || spmv_blocks > h->partials_len)
+    const int sp_blocks = spmv_blocks(h);
+    if (vec_blocks * 3 > 4 * h->partials_len || sp_blocks > 4 * h->partials_len)
         return plato_fail(h, PLATO_BAD_INPUT, "reduction scratch too small");
-    int rc = launch_jacobi(h, A, h->v_dinv);
-    if (rc) return rc;
+    const SellView V = sell_view(h);
 
     PcgScalars init{};
-    init.tol2 = 0.0;
     PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
 
     int32_t restarts = 0;
@@ -323,12 +245,11 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
     bool keep_bb = false;
     for (;;) {
         // r = b - A x ; z = Dinv r ; p = z
-        rc = launch_spmv(h, A, x, h->v_r);
+        int rc = launch_sell_spmv(h, A, x, h->v_r);
         if (rc) return rc;
         k_pcg_start<<<vec_blocks, kThreads, 0, s>>>(n, b, h->v_r, h->v_dinv, h->v_z, h->v_p, h->scal,
                                                      h->partials, tol, keep_bb ? 1 : 0);
         PLATO_LAUNCH_CHECK(h);
-        // iterate in chunks; poll the scalars of the previous chunk while the next one runs
         PcgScalars* slots = h->scal_host;
         int64_t enqueued = 0;
         std::vector<int64_t> timed_iters;
@@ -343,12 +264,12 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
                 const bool timed = h->timing && (enqueued % kTimingStride) == 0;
                 cudaEvent_t e0 = nullptr, e1 = nullptr;
                 if (timed) {
-                    RC_(timing_events(h, &e0, &e1));
+                    rc = timing_events(h, &e0, &e1);
+                    if (rc) return rc;
                     timed_iters.push_back(enqueued);
                     PLATO_CUDA(h, cudaEventRecord(e0, s));
                 }
-                k_bsr_spmv<<<spmv_blocks, kThreads, 0, s>>>(h->N, h->row_map, h->cols, A, h->v_p, h->v_Ap,
-                                                            h->scal, h->partials);
+                k_sell_spmv<<<sp_blocks, kThreads, 0, s>>>(V, A, h->v_p, h->v_Ap, h->scal, h->partials);
                 if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
                 k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_Ap, h->v_dinv, h->v_z,
                                                              h->scal, h->partials, max_it);
@@ -370,18 +291,19 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
         cudaEventDestroy(ev[1]);
         PcgScalars fin;
         PLATO_CUDA(h, cudaMemcpy(&fin, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
-        RC_(collect_timing(h, timed_iters, fin.iter - iter_base));
+        rc = collect_timing(h, timed_iters, fin.iter - iter_base);
+        if (rc) return rc;
         iter_base = fin.iter;
+        stats->iterations = fin.iter;
+        stats->refinements = 1;
         if (fin.nonfinite) {
-            stats->iterations = fin.iter;
-            stats->refinements = 1;
             stats->relative_residual = NAN;
             stats->converged = 0;
             stats->status = PLATO_NONFINITE;
             return plato_fail(h, PLATO_NONFINITE, "non-finite value in the conjugate-gradient recurrences");
         }
-        // true residual check: r = b - A x
-        rc = launch_spmv(h, A, x, h->v_Ap);
+        // true residual: r = b - A x
+        rc = launch_sell_spmv(h, A, x, h->v_Ap);
         if (rc) return rc;
         rc = launch_axpby(h, n, 1.0, b, 0.0, h->v_r);
         if (rc) return rc;
@@ -391,8 +313,6 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
         rc = launch_dot(h, h->v_r, h->v_r, n, &rr);
         if (rc) return rc;
         const double rel = fin.bb > 0.0 ? sqrt(rr / fin.bb) : 0.0;
-        stats->iterations = fin.iter;
-        stats->refinements = 1;
         stats->relative_residual = rel;
         if (rel <= tol || fin.bb == 0.0) {
             stats->converged = 1;
@@ -402,7 +322,7 @@ int pcg_fp64_assembled(plato_problem* h, const double* A, const double* b, doubl
         if (fin.iter >= max_it || restarts >= 3) {
             stats->converged = 0;
             stats->status = PLATO_NOT_CONVERGED;
-            return plato_fail(h, PLATO_NOT_CONVERGED, "PCG reached max_iterations without meeting the tolerance");
+            return plato_fail(h, PLATO_NOT_CONVERGED, "PCG stopped before ||b - A x|| <= tol ||b||");
         }
         // the recurrence drifted from the true residual: restart from the current x
         ++restarts;

@@ -93,8 +93,8 @@ typedef struct plato_solver_opts {
     int32_t operator_kind;    /* plato_operator_kind                                      */
     int32_t precision;        /* plato_precision                                          */
     int32_t self_adjoint;     /* Problem "Self-Adjoint" (src/elliptic/Problem.hpp:116)    */
-    double  inner_tolerance;  /* mixed precision: residual reduction per refinement       */
-    int32_t max_refinements;  /* mixed precision: outer FP64 refinement steps              */
+    double  chebyshev_ratio;  /* preconditioner interval [lambda_max/ratio, lambda_max]    */
+    int32_t chebyshev_degree; /* operator applies per preconditioner call; 0 = Jacobi      */
 } plato_solver_opts;
 
 typedef struct plato_problem_desc {
@@ -108,8 +108,8 @@ typedef struct plato_problem_desc {
 } plato_problem_desc;
 
 typedef struct plato_solve_stats {
-    int32_t iterations;        /* inner iterations summed over refinements */
-    int32_t refinements;       /* outer FP64 steps (1 for plain FP64)      */
+    int32_t iterations;        /* outer (FP64) Krylov iterations            */
+    int32_t refinements;       /* preconditioner operator applies in total */
     double  relative_residual; /* FP64 ||b - A x|| / ||b|| at exit          */
     int32_t converged;
     int32_t status;            /* plato_status of the solve                */
@@ -170,6 +170,13 @@ int plato_apply_constraints(plato_problem* h, double* entries, double* rhs, doub
  * MatrixTimesVectorPlusVector, src/PlatoMathHelpers.hpp:78-159 */
 int plato_matvec_plus(plato_problem* h, int32_t rows_per_block, int32_t cols_per_block,
                       const double* entries, const double* x, double* y);
+
+/* y = K_c(z) x with K_c the Dirichlet-constrained stiffness that Problem::solution hands to
+ * the solver (gradient_u + applyBlockConstraints, src/elliptic/Problem.hpp:262-266), applied
+ * either from the assembled block matrix (operator_kind = PLATO_OPERATOR_ASSEMBLED) or
+ * element by element without a matrix (PLATO_OPERATOR_MATRIX_FREE). */
+int plato_apply_operator(plato_problem* h, const double* z, int32_t operator_kind, const double* x,
+                         double* y /*[device]*/);
 
 /* ---- AbstractSolver::solve (src/alg/PlatoAbstractSolver.hpp:38-106) ---------------------
  * Jacobi-PCG on an assembled, constrained 3x3 block matrix: A x = b, x holds the initial

@@ -45,8 +45,8 @@ class EssentialBCs(C.Structure):
 
 class SolverOpts(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int32), ("operator_kind", C.c_int32),
-                ("precision", C.c_int32), ("self_adjoint", C.c_int32), ("inner_tolerance", C.c_double),
-                ("max_refinements", C.c_int32)]
+                ("precision", C.c_int32), ("self_adjoint", C.c_int32), ("chebyshev_ratio", C.c_double),
+                ("chebyshev_degree", C.c_int32)]
 
 
 class ProblemDesc(C.Structure):
@@ -96,6 +96,7 @@ def _load() -> C.CDLL:
         "plato_sf_gradient_z": ([vp, vp, vp, vp], C.c_int),
         "plato_apply_constraints": ([vp, vp, vp, C.c_double], C.c_int),
         "plato_matvec_plus": ([vp, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
+        "plato_apply_operator": ([vp, vp, C.c_int32, vp, vp], C.c_int),
         "plato_solver_solve": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_problem_solution": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_problem_criterion_value": ([vp, vp, vp, f64p], C.c_int),

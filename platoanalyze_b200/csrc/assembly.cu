@@ -208,6 +208,14 @@ int launch_dirichlet(plato_problem* h, double* A, double* rhs, double scale) {
     return PLATO_OK;
 }
 
+// rhs_d = scale * value_d on constrained dofs only (no matrix).
+int launch_dirichlet_rhs(plato_problem* h, double* rhs, double scale) {
+    if (h->nbc == 0) return PLATO_OK;
+    k_dirichlet_rhs<<<grid_for(h->nbc, 128), 128, 0, h->stream>>>(h->nbc, h->bc_dofs, h->bc_values, scale, rhs);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
 int launch_matvec_plus(plato_problem* h, int rb, int cb, const double* A, const double* x, double* y) {
     const int64_t n = (int64_t)h->N * rb;
     if (rb == 3 && cb == 3)

@@ -23,6 +23,16 @@ int prepare_operator(plato_problem* h, const double* crs);
 int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
 int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* stats);
 int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* stats);
+int prepare_mixed(plato_problem* h, const double* crs, const double* z);
+int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
+int matfree_rhs(plato_problem* h, double* b, double scale);
+int launch_dirichlet_rhs(plato_problem* h, double* rhs, double scale);
+int launch_ebe_apply64_unmasked(plato_problem* h, const double* x, double* y);
+int launch_masked_axpy(plato_problem* h, double a, const double* x, double* y);
+int matfree_setup(plato_problem* h, const double* z);
+int launch_ebe_apply64(plato_problem* h, const double* x, double* y, const PcgScalars* S);
+int launch_mask_copy(plato_problem* h, const double* x, double* y);
+int launch_sell_spmv(plato_problem* h, const double* vals, const double* x, double* y);
 }  // namespace plato
 
 using namespace plato;
@@ -109,6 +119,8 @@ int plato_destroy(plato_problem* h) {
     dfree(h->sell.width); dfree(h->sell.ptr); dfree(h->sell.cols);
     dfree(h->sell64); dfree(h->sell32);
     if (h->sell16) cudaFree(h->sell16);
+    dfree(h->mf_w64); dfree(h->mf_w32); dfree(h->v_q);
+    dfree(h->f_res); dfree(h->f_d0); dfree(h->f_d1); dfree(h->f_y); dfree(h->f_w);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     delete h;
@@ -185,6 +197,7 @@ int plato_create(const plato_problem_desc* d, plato_problem** out) {
         if (!std::isfinite(bc.values[i]))
             return fail_create(plato_fail(h, PLATO_BAD_INPUT, "non-finite essential BC value"));
         mask[bc.dofs[i]] = 1;
+        if (bc.values[i] != 0.0) h->bc_nonzero = 1;
     }
     h->nbc = bc.num_dofs;
     CRC(dmalloc(h, &h->bc_dofs, h->nbc));
@@ -347,13 +360,37 @@ int plato_matvec_plus(plato_problem* h, int32_t rb, int32_t cb, const double* en
     return launch_matvec_plus(h, rb, cb, entries, x, y);
 }
 
+int plato_apply_operator(plato_problem* h, const double* z, int32_t operator_kind, const double* x, double* y) {
+    NEED(h, z && x && y, "null device pointer");
+    if (operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
+        RC(matfree_setup(h, z));
+        RC(launch_ebe_apply64(h, x, y, nullptr));
+        return launch_mask_copy(h, x, y);
+    }
+    if (operator_kind != PLATO_OPERATOR_ASSEMBLED) return plato_fail(h, PLATO_BAD_INPUT, "unknown operator_kind");
+    RC(dmalloc(h, &h->K, 9 * h->nblocks));
+    RC(launch_assemble_jacobian(h, z, h->K));
+    RC(launch_dirichlet(h, h->K, nullptr, 0.0));
+    RC(prepare_operator(h, h->K));
+    return launch_sell_spmv(h, h->sell64, x, y);
+}
+
 int plato_solver_solve(plato_problem* h, const double* entries, double* x, const double* b,
                        plato_solve_stats* stats) {
     NEED(h, entries && x && b, "null device pointer");
     plato_solve_stats local{};
     plato_solve_stats* st = stats ? stats : &local;
-    RC(prepare_operator(h, entries));
-    return pcg_fp64(h, b, x, st);
+    // the matrix is given: the assembled operator is used whatever operator_kind says
+    if (h->opts.precision == PLATO_PRECISION_FP64 && h->opts.chebyshev_degree <= 0) {
+        RC(prepare_operator(h, entries));
+        return pcg_fp64(h, b, x, st);
+    }
+    const int32_t kind = h->opts.operator_kind;
+    h->opts.operator_kind = PLATO_OPERATOR_ASSEMBLED;
+    int rc = prepare_mixed(h, entries, nullptr);
+    if (!rc) rc = fcg_poly(h, b, x, st);
+    h->opts.operator_kind = kind;
+    return rc;
 }
 
 int plato_problem_solution(plato_problem* h, const double* z, const double* u0, double* u,
@@ -420,34 +457,65 @@ int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host
 
 namespace plato {
 
-// Problem::solution (src/elliptic/Problem.hpp:237-292), one Newton step from u = 0:
-// R = -value(0, z) = F, J = gradient_u, applyStateConstraints(J, R, 1), solve J d = R.
-int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* st) {
+static bool plain_method(const plato_solver_opts& o) {
+    return o.operator_kind == PLATO_OPERATOR_ASSEMBLED && o.precision == PLATO_PRECISION_FP64 &&
+           o.chebyshev_degree <= 0;
+}
+
+// Builds the constrained operator of control z and the right-hand side (rhs with the
+// Dirichlet rows/columns eliminated, values scaled by bc_scale), then solves into x (which
+// holds the initial guess).  Plain method: assembled block matrix + Jacobi-PCG.  Otherwise:
+// flexible CG with the Chebyshev preconditioner on the assembled or matrix-free operator.
+static int solve_constrained(plato_problem* h, const double* z, const double* rhs, double bc_scale, double* x,
+                             plato_solve_stats* st) {
     const int64_t n = 3 * int64_t(h->N);
+    if (rhs != h->v_b)
+        PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
+        RC(prepare_mixed(h, nullptr, z));
+        RC(matfree_rhs(h, h->v_b, bc_scale));
+        return fcg_poly(h, h->v_b, x, st);
+    }
     RC(dmalloc(h, &h->K, 9 * h->nblocks));
     RC(launch_assemble_jacobian(h, z, h->K));
-    PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, h->F, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
-    RC(launch_dirichlet(h, h->K, h->v_b, 1.0));
-    RC(prepare_operator(h, h->K));
+    RC(launch_dirichlet(h, h->K, h->v_b, bc_scale));
+    if (plain_method(h->opts)) {
+        RC(prepare_operator(h, h->K));
+        return pcg_fp64(h, h->v_b, x, st);
+    }
+    RC(prepare_mixed(h, h->K, z));
+    return fcg_poly(h, h->v_b, x, st);
+}
+
+// Problem::solution (src/elliptic/Problem.hpp:237-292), one Newton step from u = 0:
+// R = -value(0, z) = F, J = gradient_u, applyStateConstraints(J, R, 1), solve J d = R.
+// (value(0, z) = 0 - F exactly, so F is used directly.)  u0, when given, seeds the solve.
+int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* st) {
+    const int64_t n = 3 * int64_t(h->N);
     if (u0) {
         if (u0 != u) PLATO_CUDA(h, cudaMemcpyAsync(u, u0, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     } else {
         PLATO_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n, h->stream));
     }
-    return pcg_fp64(h, h->v_b, u, st);
+    return solve_constrained(h, z, h->F, 1.0, u, st);
 }
 
-// Adjoint solve K^T lambda = rhs with zero-valued constraints.
+// Adjoint solve K^T lambda = rhs with zero-valued constraints (K is symmetric).
 int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* st) {
-    const int64_t n = 3 * int64_t(h->N);
-    RC(dmalloc(h, &h->K, 9 * h->nblocks));
-    RC(launch_assemble_jacobian(h, z, h->K));
-    if (rhs != h->v_b)
-        PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
-    RC(launch_dirichlet(h, h->K, h->v_b, 0.0));
-    RC(prepare_operator(h, h->K));
-    PLATO_CUDA(h, cudaMemsetAsync(lam, 0, sizeof(double) * n, h->stream));
-    return pcg_fp64(h, h->v_b, lam, st);
+    PLATO_CUDA(h, cudaMemsetAsync(lam, 0, sizeof(double) * 3 * size_t(h->N), h->stream));
+    return solve_constrained(h, z, rhs, 0.0, lam, st);
+}
+
+// Matrix-free right-hand side: b_free -= (K g)_free for inhomogeneous values g, b_d = scale g_d.
+int matfree_rhs(plato_problem* h, double* b, double scale) {
+    if (scale != 0.0 && h->bc_nonzero) {
+        const int64_t n = 3 * int64_t(h->N);
+        PLATO_CUDA(h, cudaMemsetAsync(h->v_tmp, 0, sizeof(double) * n, h->stream));
+        RC(launch_dirichlet_rhs(h, h->v_tmp, scale));
+        RC(launch_ebe_apply64_unmasked(h, h->v_tmp, h->v_q));
+        RC(launch_masked_axpy(h, -1.0, h->v_q, b));
+    }
+    return launch_dirichlet_rhs(h, b, scale);
 }
 
 }  // namespace plato

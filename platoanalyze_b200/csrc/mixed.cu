@@ -1,0 +1,632 @@
+// Flexible CG in FP64 with a Chebyshev-Jacobi polynomial preconditioner applied in low
+// precision (the mixed-precision solve of PLATO_PRECISION_MIXED_FP32 / _MIXED_BF16, and the
+// FP64 polynomial-preconditioned variant).
+//
+// Outer method: flexible conjugate gradients with one-term A-orthogonalisation (Notay's
+// FCG(1)): q = A p, alpha = (p.r)/(p.q), x += alpha p, r -= alpha q, z = M(r),
+// beta = -(z.q)/(p.q), p = z + beta p.  Operator applications, the residual, the iterate,
+// every dot product and step length are FP64; the stop test ||r|| <= tol ||b|| is FP64 and
+// is confirmed on exit with the recomputed residual b - A x.
+//
+// Preconditioner M: `degree` steps of the Chebyshev iteration for D^-1 A on the interval
+// [lambda_max / ratio, lambda_max] from a zero initial guess (Saad, Iterative Methods for
+// Sparse Linear Systems, 2nd ed., Alg. 12.1), run on an FP32 (or BF16-stored, or
+// matrix-free FP32) copy of the operator with FP32 vectors.  Only the preconditioner sees
+// reduced precision, so it changes the iteration count, not the converged answer.
+// lambda_max comes from power iteration with a safety factor.
+//
+// Each Chebyshev step on the SELL copy is one fused kernel (gather SpMV, residual update,
+// direction and iterate update; no reductions).  The matrix-free variant scatters with
+// FP32 atomics and finishes the step in a vector kernel.
+#include <cmath>
+#include <cuda_bf16.h>
+
+#include "plato_internal.cuh"
+#include "solver_common.cuh"
+
+namespace plato {
+
+int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
+int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, double* host_result);
+int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float* out32, void* out16,
+                       double* dinv, float* dinv32);
+int launch_sell_spmv(plato_problem* h, const double* vals, const double* x, double* y);
+int launch_ebe_apply64(plato_problem* h, const double* x, double* y, const PcgScalars* S);
+int launch_ebe_apply32(plato_problem* h, const float* x, float* y, const PcgScalars* S);
+int launch_mask_copy(plato_problem* h, const double* x, double* y);
+int matfree_setup(plato_problem* h, const double* z);
+SellView sell_view(const plato_problem* h);
+int spmv_blocks(const plato_problem* h);
+int timing_events(plato_problem* h, cudaEvent_t* e0, cudaEvent_t* e1);
+int collect_timing(plato_problem* h, const std::vector<int64_t>& iters, int64_t executed);
+
+namespace {
+
+constexpr int kChunk = 16;
+constexpr int kTimingStride = 8;
+
+enum InnerKind { INNER_SELL64 = 0, INNER_SELL32 = 1, INNER_SELL16 = 2, INNER_EBE32 = 3, INNER_EBE64 = 4 };
+
+struct ChebCoef {
+    float c0;      // first step: d = c0 Dinv r
+    float c1[64];  // step k: d_k = c1[k] d_(k-1) + c2[k] Dinv res
+    float c2[64];
+};
+
+// ---- outer operator: q = A p, then p.q -> alpha = (p.r)/(p.q) ------------------------------
+
+__device__ __forceinline__ void finish_pq(PcgScalars* S, double pq) {
+    S->pAp = pq;
+    S->alpha = S->rz / pq;
+    if (!isfinite(S->alpha) || pq <= 0.0) { S->nonfinite = 1; S->done = 1; }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_fcg_sell_apply(SellView A, const double* __restrict__ vals, const double* __restrict__ p, double* __restrict__ q,
+                 PcgScalars* S, double* partials) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S->done) return;
+    double dot = 0.0;
+    const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < padded; r += (int64_t)gridDim.x * blockDim.x) {
+        double a0, a1, a2;
+        sell_row<double>(A, vals, p, r, a0, a1, a2);
+        if (r < A.num_rows) {
+            q[3 * r] = a0;
+            q[3 * r + 1] = a1;
+            q[3 * r + 2] = a2;
+            dot += p[3 * r] * a0 + p[3 * r + 1] * a1 + p[3 * r + 2] * a2;
+        }
+    }
+    double v[1] = {dot};
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            finish_pq(S, t[0]);
+            S->ticket = 0u;
+        }
+    }
+}
+
+// After a matrix-free apply: constrained rows of q take p (identity rows), then p.q.
+__global__ void __launch_bounds__(kThreads)
+k_fcg_mask_dot(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ p, double* __restrict__ q,
+               PcgScalars* S, double* partials) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S->done) return;
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double qi = q[i];
+        if (mask[i]) { qi = p[i]; q[i] = qi; }
+        v[0] += p[i] * qi;
+    }
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            finish_pq(S, t[0]);
+            S->ticket = 0u;
+        }
+    }
+}
+
+// x += alpha p; r -= alpha q; r.r and the stop test; starts the preconditioner:
+// res = r (FP32), d = c0 Dinv r, y = d.
+__global__ void __launch_bounds__(kThreads)
+k_fcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+             const double* __restrict__ q, const float* __restrict__ dinv32, float* __restrict__ res,
+             float* __restrict__ d, float* __restrict__ y, float c0, PcgScalars* S, double* partials,
+             int32_t max_it) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S->done) return;
+    const double alpha = S->alpha;
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        v[0] += ri * ri;
+        const float rf = float(ri);
+        const float di = c0 * dinv32[i] * rf;
+        res[i] = rf;
+        d[i] = di;
+        y[i] = di;
+    }
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            S->rr = t[0];
+            S->iter += 1;
+            if (!isfinite(t[0])) { S->nonfinite = 1; S->done = 1; }
+            if (t[0] <= S->tol2 || S->iter >= max_it) S->done = 1;
+            S->ticket = 0u;
+        }
+    }
+}
+
+// One Chebyshev step on a SELL copy (entries TV): w = A d_cur, res -= w,
+// d_next = c1 d_cur + c2 Dinv res, y += d_next.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_cheb_sell(SellView A, const void* __restrict__ vals, const float* __restrict__ dinv32, float* __restrict__ res,
+            const float* __restrict__ dcur, float* __restrict__ dnext, float* __restrict__ y, float c1, float c2,
+            const PcgScalars* S) {
+    if (S->done) return;
+    const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < padded; r += (int64_t)gridDim.x * blockDim.x) {
+        float w0, w1, w2;
+        if (KIND == INNER_SELL16)
+            sell_row_bf16(A, static_cast<const __nv_bfloat16*>(vals), dcur, r, w0, w1, w2);
+        else if (KIND == INNER_SELL32)
+            sell_row<float>(A, static_cast<const float*>(vals), dcur, r, w0, w1, w2);
+        else {
+            double a0, a1, a2;
+            sell_row<double>(A, static_cast<const double*>(vals), dcur, r, a0, a1, a2);
+            w0 = float(a0); w1 = float(a1); w2 = float(a2);
+        }
+        if (r < A.num_rows) {
+            const float w[3] = {w0, w1, w2};
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int64_t k = 3 * r + i;
+                const float rs = res[k] - w[i];
+                res[k] = rs;
+                const float dn = c1 * dcur[k] + c2 * dinv32[k] * rs;
+                dnext[k] = dn;
+                y[k] += dn;
+            }
+        }
+    }
+}
+
+// Chebyshev step after a matrix-free apply (w holds P A P d_cur; constrained rows are identity).
+__global__ void __launch_bounds__(kThreads)
+k_cheb_vec(int64_t n, const uint8_t* __restrict__ mask, const float* __restrict__ w, const float* __restrict__ dinv32,
+           float* __restrict__ res, const float* __restrict__ dcur, float* __restrict__ dnext, float* __restrict__ y,
+           float c1, float c2, const PcgScalars* S) {
+    if (S->done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = mask[i] ? dcur[i] : w[i];
+        const float rs = res[i] - wi;
+        res[i] = rs;
+        const float dn = c1 * dcur[i] + c2 * dinv32[i] * rs;
+        dnext[i] = dn;
+        y[i] += dn;
+    }
+}
+
+// z = y (widened), z.q -> beta = -(z.q)/(p.q); then p = z + beta p and p.r in k_fcg_direction.
+__global__ void __launch_bounds__(kThreads)
+k_fcg_zq(int64_t n, const float* __restrict__ y, double* __restrict__ z, const double* __restrict__ q,
+         PcgScalars* S, double* partials, int first) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S->done) return;
+    if (first) {  // initial direction: only widen z = y
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            z[i] = double(y[i]);
+        return;
+    }
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double zi = double(y[i]);
+        z[i] = zi;
+        v[0] += zi * q[i];
+    }
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            S->zq = t[0];
+            S->beta = -t[0] / S->pAp;
+            if (!isfinite(S->beta)) { S->nonfinite = 1; S->done = 1; }
+            S->ticket = 0u;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_fcg_direction(int64_t n, const double* __restrict__ z, double* __restrict__ p, const double* __restrict__ r,
+                PcgScalars* S, double* partials, int first) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S->done) return;
+    const double beta = first ? 0.0 : S->beta;
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double pi = z[i] + beta * (first ? 0.0 : p[i]);
+        p[i] = pi;
+        v[0] += pi * r[i];
+    }
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            S->rz = t[0];  // p.r
+            if (!isfinite(t[0])) { S->nonfinite = 1; S->done = 1; }
+            S->ticket = 0u;
+        }
+    }
+}
+
+// r = b - A x (A x in r on entry), r.r and b.b; starts the preconditioner like k_fcg_update.
+__global__ void __launch_bounds__(kThreads)
+k_fcg_start(int64_t n, const double* __restrict__ b, double* __restrict__ r, const float* __restrict__ dinv32,
+            float* __restrict__ res, float* __restrict__ d, float* __restrict__ y, float c0, PcgScalars* S,
+            double* partials, double tol, int keep_bb) {
+    __shared__ double sh[2][32];
+    __shared__ bool last;
+    double v[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ri = b[i] - r[i];
+        r[i] = ri;
+        v[0] += ri * ri;
+        v[1] += b[i] * b[i];
+        const float rf = float(ri);
+        const float di = c0 * dinv32[i] * rf;
+        res[i] = rf;
+        d[i] = di;
+        y[i] = di;
+    }
+    block_sum_n<2>(v, sh);
+    if (publish_partials<2>(v, partials, &S->ticket, &last)) {
+        double t[2];
+        final_sums<2>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            S->rr = t[0];
+            if (!keep_bb) {
+                S->bb = t[1];
+                S->tol2 = tol * tol * t[1];
+                S->iter = 0;
+            }
+            S->nonfinite = (!isfinite(t[0]) || !isfinite(t[1])) ? 1 : 0;
+            S->done = (t[0] <= S->tol2 || S->nonfinite) ? 1 : 0;
+            S->ticket = 0u;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_power_step(int64_t n, const uint8_t* __restrict__ mask, const float* __restrict__ v, const float* __restrict__ w,
+             const float* __restrict__ dinv32, double* partials, unsigned int* ticket, double* out) {
+    // out[0] = v.(A v), out[1] = v.(D v), out[2] = |Dinv A v|^2
+    __shared__ double sh[3][32];
+    __shared__ bool last;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = (mask && mask[i]) ? v[i] : w[i];
+        s[0] += double(v[i]) * wi;
+        s[1] += double(v[i]) * v[i] / dinv32[i];
+        const double t = double(dinv32[i]) * wi;
+        s[2] += t * t;
+    }
+    block_sum_n<3>(s, sh);
+    if (publish_partials<3>(s, partials, ticket, &last)) {
+        double t[3];
+        final_sums<3>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
+            *ticket = 0u;
+        }
+    }
+}
+
+__global__ void k_power_next(int64_t n, const uint8_t* __restrict__ mask, const float* __restrict__ v,
+                             const float* __restrict__ w, const float* __restrict__ dinv32, float scale,
+                             float* __restrict__ vn) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float wi = (mask && mask[i]) ? v[i] : w[i];
+        vn[i] = scale * dinv32[i] * wi;
+    }
+}
+
+__global__ void k_power_init(int64_t n, float* __restrict__ v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t h = uint32_t(i) * 2654435761u;
+        h ^= h >> 15;
+        h *= 2246822519u;
+        h ^= h >> 13;
+        v[i] = float(h & 0xffffff) / float(0x1000000) + 0.5f;
+    }
+}
+
+int inner_kind(const plato_problem* h) {
+    const plato_solver_opts& o = h->opts;
+    if (o.operator_kind == PLATO_OPERATOR_MATRIX_FREE)
+        return o.precision == PLATO_PRECISION_FP64 ? INNER_EBE64 : INNER_EBE32;
+    if (o.precision == PLATO_PRECISION_MIXED_BF16) return INNER_SELL16;
+    if (o.precision == PLATO_PRECISION_MIXED_FP32) return INNER_SELL32;
+    return INNER_SELL64;
+}
+
+}  // namespace
+
+// Inner SELL product for the power iteration (plain w = A d, FP32 out).
+namespace {
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_sell_apply32(SellView A, const void* __restrict__ vals, const float* __restrict__ x, float* __restrict__ y) {
+    const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < padded; r += (int64_t)gridDim.x * blockDim.x) {
+        float w0, w1, w2;
+        if (KIND == INNER_SELL16)
+            sell_row_bf16(A, static_cast<const __nv_bfloat16*>(vals), x, r, w0, w1, w2);
+        else if (KIND == INNER_SELL32)
+            sell_row<float>(A, static_cast<const float*>(vals), x, r, w0, w1, w2);
+        else {
+            double a0, a1, a2;
+            sell_row<double>(A, static_cast<const double*>(vals), x, r, a0, a1, a2);
+            w0 = float(a0); w1 = float(a1); w2 = float(a2);
+        }
+        if (r < A.num_rows) {
+            y[3 * r] = w0;
+            y[3 * r + 1] = w1;
+            y[3 * r + 2] = w2;
+        }
+    }
+}
+}  // namespace
+
+static const void* inner_vals(const plato_problem* h, int kind) {
+    if (kind == INNER_SELL16) return h->sell16;
+    if (kind == INNER_SELL32) return h->sell32;
+    return h->sell64;
+}
+
+static int apply_inner_plain(plato_problem* h, int kind, const float* x, float* y) {
+    if (kind == INNER_EBE32 || kind == INNER_EBE64) return launch_ebe_apply32(h, x, y, nullptr);
+    const SellView V = sell_view(h);
+    const void* vals = inner_vals(h, kind);
+    const int B = spmv_blocks(h);
+    if (kind == INNER_SELL16) k_sell_apply32<INNER_SELL16><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
+    else if (kind == INNER_SELL32) k_sell_apply32<INNER_SELL32><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
+    else k_sell_apply32<INNER_SELL64><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+// lambda_max of Dinv A (inner operator) by power iteration; returns the Rayleigh quotient.
+static int estimate_lambda_max(plato_problem* h, int kind, int steps, double* lmax) {
+    const int64_t n = 3 * (int64_t)h->N;
+    const int VB = grid_for(n, kThreads, 148 * 16);
+    const uint8_t* mask = (kind == INNER_EBE32 || kind == INNER_EBE64) ? h->bc_mask : nullptr;
+    k_power_init<<<VB, kThreads, 0, h->stream>>>(n, h->f_d0);
+    PLATO_LAUNCH_CHECK(h);
+    double host[3] = {0, 0, 0};
+    double lam = 0.0;
+    float scale = 1.0f;
+    for (int it = 0; it < steps; ++it) {
+        int rc = apply_inner_plain(h, kind, h->f_d0, h->f_w);
+        if (rc) return rc;
+        k_power_step<<<VB, kThreads, 0, h->stream>>>(n, mask, h->f_d0, h->f_w, h->f_dinv, h->partials, h->red_ticket,
+                                                     h->red_out);
+        PLATO_LAUNCH_CHECK(h);
+        PLATO_CUDA(h, cudaMemcpyAsync(host, h->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+        lam = host[0] / host[1];
+        scale = float(1.0 / std::sqrt(host[2] / double(n)));
+        if (!std::isfinite(lam) || !std::isfinite(scale))
+            return plato_fail(h, PLATO_NONFINITE, "power iteration for the Chebyshev interval failed");
+        k_power_next<<<VB, kThreads, 0, h->stream>>>(n, mask, h->f_d0, h->f_w, h->f_dinv, scale, h->f_d1);
+        PLATO_LAUNCH_CHECK(h);
+        std::swap(h->f_d0, h->f_d1);
+    }
+    *lmax = lam;
+    return PLATO_OK;
+}
+
+// Chebyshev coefficients for `degree` steps on [lmax/ratio, lmax].
+static ChebCoef chebyshev(double lmax, double ratio, int degree) {
+    ChebCoef c{};
+    const double lmin = lmax / ratio;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    c.c0 = float(1.0 / theta);
+    for (int k = 1; k < degree && k < 64; ++k) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        c.c1[k] = float(rn * rho);
+        c.c2[k] = float(2.0 * rn / delta);
+        rho = rn;
+    }
+    return c;
+}
+
+// Prepares the operators for a polynomial-preconditioned solve with control z (assembled
+// path: h->K holds the constrained CRS matrix).
+int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
+    const int64_t n = 3 * (int64_t)h->N;
+    for (float** v : {&h->f_res, &h->f_d0, &h->f_d1, &h->f_y, &h->f_w, &h->f_dinv})
+        if (!*v) PLATO_CUDA(h, cudaMalloc(v, sizeof(float) * n));
+    if (!h->v_q) PLATO_CUDA(h, cudaMalloc(&h->v_q, sizeof(double) * n));
+    const int kind = inner_kind(h);
+    if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) return matfree_setup(h, z);
+    const size_t slots = 9 * size_t(h->sell.total_slots);
+    if (!h->sell64) PLATO_CUDA(h, cudaMalloc(&h->sell64, sizeof(double) * slots));
+    float* o32 = nullptr;
+    void* o16 = nullptr;
+    if (kind == INNER_SELL32) {
+        if (!h->sell32) PLATO_CUDA(h, cudaMalloc(&h->sell32, sizeof(float) * slots));
+        o32 = h->sell32;
+    } else if (kind == INNER_SELL16) {
+        if (!h->sell16) PLATO_CUDA(h, cudaMalloc(&h->sell16, sizeof(__nv_bfloat16) * slots));
+        o16 = h->sell16;
+    }
+    return launch_crs_to_sell(h, crs, h->sell64, o32, o16, h->v_dinv, h->f_dinv);
+}
+
+// Flexible CG with the Chebyshev preconditioner: A x = b, x holds the initial guess.
+int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
+    const int64_t n = 3 * (int64_t)h->N;
+    cudaStream_t s = h->stream;
+    const double tol = h->opts.tolerance;
+    const int32_t max_it = h->opts.max_iterations;
+    const int degree = h->opts.chebyshev_degree < 1 ? 1 : (h->opts.chebyshev_degree > 64 ? 64 : h->opts.chebyshev_degree);
+    const int kind = inner_kind(h);
+    const bool mf = h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE;
+    const int VB = grid_for(n, kThreads, 148 * 16);
+    const int SB = spmv_blocks(h);
+    const SellView V = sell_view(h);
+
+    double lmax = 0.0;
+    int rc = estimate_lambda_max(h, kind, 20, &lmax);
+    if (rc) return rc;
+    const double safety = kind == INNER_SELL16 ? 1.15 : 1.10;
+    const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree);
+
+    auto outer_apply = [&](const double* in, double* out) -> int {
+        if (mf) {
+            int r2 = launch_ebe_apply64(h, in, out, nullptr);
+            if (r2) return r2;
+            return launch_mask_copy(h, in, out);
+        }
+        return launch_sell_spmv(h, h->sell64, in, out);
+    };
+    auto precondition = [&](float c0_unused) -> int {
+        (void)c0_unused;
+        float* dcur = h->f_d0;
+        float* dnext = h->f_d1;
+        for (int k = 1; k < degree; ++k) {
+            if (mf) {
+                int r2 = launch_ebe_apply32(h, dcur, h->f_w, h->scal);
+                if (r2) return r2;
+                k_cheb_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, h->f_w, h->f_dinv, h->f_res, dcur, dnext, h->f_y,
+                                                   cc.c1[k], cc.c2[k], h->scal);
+            } else if (kind == INNER_SELL16) {
+                k_cheb_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+            } else if (kind == INNER_SELL32) {
+                k_cheb_sell<INNER_SELL32><<<SB, kThreads, 0, s>>>(V, h->sell32, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+            } else {
+                k_cheb_sell<INNER_SELL64><<<SB, kThreads, 0, s>>>(V, h->sell64, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+            }
+            PLATO_LAUNCH_CHECK(h);
+            std::swap(dcur, dnext);
+        }
+        return PLATO_OK;
+    };
+
+    PcgScalars init{};
+    PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
+    int32_t restarts = 0, iter_base = 0;
+    bool keep_bb = false;
+    int64_t precond_applies = 0;
+    for (;;) {
+        // r = b - A x; z = M r; p = z; p.r
+        rc = outer_apply(x, h->v_r);
+        if (rc) return rc;
+        k_fcg_start<<<VB, kThreads, 0, s>>>(n, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, h->scal,
+                                             h->partials, tol, keep_bb ? 1 : 0);
+        PLATO_LAUNCH_CHECK(h);
+        rc = precondition(cc.c0);
+        if (rc) return rc;
+        k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, h->v_z, h->v_q, h->scal, h->partials, 1);
+        k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 1);
+        h->launches += 1;
+        PLATO_LAUNCH_CHECK(h);
+
+        PcgScalars* slots = h->scal_host;
+        int64_t enqueued = 0;
+        std::vector<int64_t> timed_iters;
+        h->ev_used = 0;
+        int cur = 0;
+        bool have_prev = false;
+        cudaEvent_t ev[2];
+        PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+        PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        for (;;) {
+            for (int k = 0; k < kChunk; ++k, ++enqueued) {
+                const bool timed = h->timing && (enqueued % kTimingStride) == 0;
+                cudaEvent_t e0 = nullptr, e1 = nullptr;
+                if (timed) {
+                    rc = timing_events(h, &e0, &e1);
+                    if (rc) return rc;
+                    timed_iters.push_back(enqueued);
+                    PLATO_CUDA(h, cudaEventRecord(e0, s));
+                }
+                if (mf) {
+                    rc = launch_ebe_apply64(h, h->v_p, h->v_q, h->scal);
+                    if (rc) return rc;
+                    k_fcg_mask_dot<<<VB, kThreads, 0, s>>>(n, h->bc_mask, h->v_p, h->v_q, h->scal, h->partials);
+                } else {
+                    k_fcg_sell_apply<<<SB, kThreads, 0, s>>>(V, h->sell64, h->v_p, h->v_q, h->scal, h->partials);
+                }
+                if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
+                k_fcg_update<<<VB, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_q, h->f_dinv, h->f_res, h->f_d0,
+                                                     h->f_y, cc.c0, h->scal, h->partials, max_it);
+                h->launches += 2;
+                rc = precondition(cc.c0);
+                if (rc) return rc;
+                k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, h->v_z, h->v_q, h->scal, h->partials, 0);
+                k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 0);
+                h->launches += 1;
+                PLATO_LAUNCH_CHECK(h);
+            }
+            PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
+            PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
+            if (have_prev) {
+                PLATO_CUDA(h, cudaEventSynchronize(ev[cur ^ 1]));
+                if (slots[cur ^ 1].done) break;
+            }
+            have_prev = true;
+            cur ^= 1;
+        }
+        PLATO_CUDA(h, cudaStreamSynchronize(s));
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        PcgScalars fin;
+        PLATO_CUDA(h, cudaMemcpy(&fin, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
+        rc = collect_timing(h, timed_iters, fin.iter - iter_base);
+        if (rc) return rc;
+        precond_applies += int64_t(fin.iter - iter_base + 1) * (degree - 1);
+        iter_base = fin.iter;
+        stats->iterations = fin.iter;
+        stats->refinements = int32_t(precond_applies);
+        if (fin.nonfinite) {
+            stats->relative_residual = NAN;
+            stats->converged = 0;
+            stats->status = PLATO_NONFINITE;
+            return plato_fail(h, PLATO_NONFINITE, "non-finite value or loss of positivity in flexible CG");
+        }
+        // true residual r = b - A x
+        rc = outer_apply(x, h->v_q);
+        if (rc) return rc;
+        rc = launch_axpby(h, n, 1.0, b, 0.0, h->v_r);
+        if (rc) return rc;
+        rc = launch_axpby(h, n, -1.0, h->v_q, 1.0, h->v_r);
+        if (rc) return rc;
+        double rr = 0.0;
+        rc = launch_dot(h, h->v_r, h->v_r, n, &rr);
+        if (rc) return rc;
+        const double rel = fin.bb > 0.0 ? std::sqrt(rr / fin.bb) : 0.0;
+        stats->relative_residual = rel;
+        if (rel <= tol || fin.bb == 0.0) {
+            stats->converged = 1;
+            stats->status = PLATO_OK;
+            return PLATO_OK;
+        }
+        if (fin.iter >= max_it || restarts >= 3) {
+            stats->converged = 0;
+            stats->status = PLATO_NOT_CONVERGED;
+            return plato_fail(h, PLATO_NOT_CONVERGED, "flexible CG stopped before ||b - A x|| <= tol ||b||");
+        }
+        ++restarts;
+        keep_bb = true;
+        PcgScalars cont = fin;
+        cont.done = 0;
+        PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &cont, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
+    }
+}
+
+}  // namespace plato

@@ -54,6 +54,7 @@ struct PcgScalars {
     double alpha;
     double beta;
     double tol2;     // tol^2 * b.b
+    double zq;       // flexible CG: z_(k+1) . A p_k
     int32_t iter;
     int32_t done;    // 1 once ||r|| <= tol ||b||
     int32_t nonfinite;
@@ -86,6 +87,7 @@ struct plato_problem {
     int32_t* bc_dofs = nullptr;
     double*  bc_values = nullptr;
     uint8_t* bc_mask = nullptr;    // [3N] 1 where a dof is constrained
+    int      bc_nonzero = 0;       // some essential BC value is nonzero
     // assembled operator (allocated on first use)
     double* K = nullptr;           // 9*nblocks
     double* KT = nullptr;          // scratch for transposed / gradient_z matrices
@@ -130,6 +132,15 @@ struct plato_problem {
     double* sell64 = nullptr;      // FP64 entries
     float*  sell32 = nullptr;      // FP32 entries (mixed precision)
     void*   sell16 = nullptr;      // BF16 entries (mixed precision)
+    // matrix-free operator data (matfree.cu) and mixed-precision work vectors (mixed.cu)
+    double* mf_w64 = nullptr;      // per-cell SIMP weight s(rho_e), FP64
+    float*  mf_w32 = nullptr;      // same, FP32
+    double* v_q = nullptr;         // A p of the flexible CG
+    float*  f_res = nullptr;       // Chebyshev residual
+    float*  f_d0 = nullptr;        // Chebyshev directions (double buffered)
+    float*  f_d1 = nullptr;
+    float*  f_y = nullptr;         // preconditioner output
+    float*  f_w = nullptr;         // inner operator output
     // instrumentation: kernel launches issued, and sampled CUDA-event timings of the
     // solver's operator apply (every kTimingStride-th apply, events on the handle's stream)
     int64_t launches = 0;

@@ -30,12 +30,12 @@ class SolverOptions:
     operator_kind: int = capi.OPERATOR_ASSEMBLED
     precision: int = capi.PRECISION_FP64
     self_adjoint: bool = True
-    inner_tolerance: float = 1e-4
-    max_refinements: int = 50
+    chebyshev_ratio: float = 30.0
+    chebyshev_degree: int = 0
 
     def to_c(self) -> capi.SolverOpts:
         return capi.SolverOpts(self.tolerance, self.max_iterations, self.operator_kind, self.precision,
-                               int(self.self_adjoint), self.inner_tolerance, self.max_refinements)
+                               int(self.self_adjoint), self.chebyshev_ratio, self.chebyshev_degree)
 
 
 @dataclass
@@ -201,6 +201,12 @@ class EllipticProblem:
 
     def matvec_plus(self, rb, cb, entries, x, y):
         check(lib.plato_matvec_plus(self.h, rb, cb, self._dev(entries), self._dev(x), self._dev(y)), self.h)
+        return y
+
+    def apply_operator(self, z, x, operator_kind=capi.OPERATOR_ASSEMBLED):
+        """y = K_c(z) x, K_c the Dirichlet-constrained stiffness (assembled or matrix-free)."""
+        y = self.zeros(self.num_dofs)
+        check(lib.plato_apply_operator(self.h, self._dev(z), operator_kind, self._dev(x), self._dev(y)), self.h)
         return y
 
     def solver_solve(self, entries, x, b):

@@ -26,7 +26,7 @@ static plato_problem_desc cube_desc(std::vector<double>& coords, std::vector<int
     d.mesh = {nn, nc, coords.data(), conn.data()};
     d.material = {1.0e6, 0.3};
     d.penalty = {1.0, 0.0};
-    d.solver = {1e-10, 10000, PLATO_OPERATOR_ASSEMBLED, PLATO_PRECISION_FP64, 1, 1e-4, 50};
+    d.solver = {1e-10, 10000, PLATO_OPERATOR_ASSEMBLED, PLATO_PRECISION_FP64, 1, 30.0, 0};
     return d;
 }
 
@@ -77,7 +77,7 @@ int main() {
         d.num_natural_bcs = 1;
         d.natural_bcs = &load;
         d.essential_bcs = {int32_t(bcd.size()), bcd.data(), bcv.data()};
-        d.solver = {1e-12, 10000, PLATO_OPERATOR_ASSEMBLED, PLATO_PRECISION_FP64, 1, 1e-4, 50};
+        d.solver = {1e-12, 10000, PLATO_OPERATOR_ASSEMBLED, PLATO_PRECISION_FP64, 1, 30.0, 0};
         auto cant = std::make_shared<Model>(d);
         Elliptic::Problem problem(cant);
         ScalarVector zc(std::vector<double>(size_t(nn), 0.5));

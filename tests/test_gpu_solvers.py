@@ -1,0 +1,116 @@
+"""Matrix-free operator and the polynomial-preconditioned / mixed-precision solvers.
+
+The FP64 plain method is the oracle-checked reference (tests/test_gpu_parity.py).  Every
+other solver configuration must reach the same FP64 tolerance (the stop test is always the
+FP64 residual) and land within 1e-8 of the CPU oracle's solution; reduced precision may
+only change the iteration count.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+from oracle import Oracle
+from platoanalyze_b200 import capi
+from platoanalyze_b200.problem import EllipticProblem, ProblemSpec, SolverOptions
+from platoanalyze_b200.workloads import cantilever, splitmix_uniform
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = {
+    "fp64_cheb8": SolverOptions(precision=capi.PRECISION_FP64, chebyshev_degree=8),
+    "fp32_cheb8": SolverOptions(precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=8),
+    "bf16_cheb8": SolverOptions(precision=capi.PRECISION_MIXED_BF16, chebyshev_degree=8),
+    "mf_fp64_jacobi": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE, precision=capi.PRECISION_FP64,
+                                    chebyshev_degree=1),
+    "mf_fp32_cheb8": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE, precision=capi.PRECISION_MIXED_FP32,
+                                   chebyshev_degree=8),
+}
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def setup():
+    spec = cantilever(20, 10, 10, SolverOptions(tolerance=1e-10))
+    z = splitmix_uniform(spec.coords.shape[0], 0x5EED0003)
+    prob = EllipticProblem(spec)
+    orc = Oracle.from_spec(spec)
+    uo, _ = orc.solution(z, tol=1e-12)
+    go = orc.criterion_gradient(z, uo)
+    return spec, z, prob, orc, uo, go
+
+
+def constrained_matvec(orc, z, x):
+    K = orc.vf_gradient_u(np.zeros(3 * orc.N), z)
+    rhs = np.zeros(3 * orc.N)
+    orc.apply_constraints(K, rhs, 0.0)
+    return orc.matvec_plus(3, 3, K, x, np.zeros(3 * orc.N))
+
+
+@pytest.mark.parametrize("kind", [capi.OPERATOR_ASSEMBLED, capi.OPERATOR_MATRIX_FREE])
+def test_operator_apply_matches_oracle(setup, kind):
+    spec, z, prob, orc, *_ = setup
+    x = np.sin(np.arange(3 * orc.N) * 0.7)
+    y = host(prob.apply_operator(prob.to_dev(z), prob.to_dev(x), kind))
+    ref = constrained_matvec(orc, z, x)
+    assert rel_l2(y, ref) <= 1e-12, rel_l2(y, ref)
+
+
+def test_matrix_free_on_perturbed_mesh():
+    from test_gpu_parity import perturbed_mesh
+    coords, conn = perturbed_mesh(5, 4, 4, 3)
+    fixed = np.where(coords[:, 0] < 1e-12)[0]
+    dofs = (3 * fixed[:, None] + np.arange(3)).ravel().astype(np.int32)
+    spec = ProblemSpec(coords, conn, 1.7, 0.21, 3.0, 1e-9, [], dofs, np.linspace(0, 1e-3, dofs.size))
+    prob, orc = EllipticProblem(spec), Oracle.from_spec(spec)
+    z = splitmix_uniform(coords.shape[0], 5)
+    x = np.cos(np.arange(3 * coords.shape[0]))
+    y = host(prob.apply_operator(prob.to_dev(z), prob.to_dev(x), capi.OPERATOR_MATRIX_FREE))
+    assert rel_l2(y, constrained_matvec(orc, z, x)) <= 1e-12
+
+
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_solver_configuration_reaches_fp64_answer(setup, name):
+    spec, z, prob, orc, uo, go = setup
+    opts = CONFIGS[name]
+    opts.tolerance = 1e-10
+    prob.set_solver(opts)
+    try:
+        zd = prob.to_dev(z)
+        u, st = prob.solution(zd)
+        g, _ = prob.criterion_gradient(zd, u)
+    finally:
+        prob.set_solver(SolverOptions(tolerance=1e-10))
+    assert st["converged"] == 1 and st["relative_residual"] <= 1e-10, st
+    assert rel_l2(host(u), uo) <= 1e-8, rel_l2(host(u), uo)
+    assert rel_l2(host(g), go) <= 1e-8, rel_l2(host(g), go)
+
+
+def test_chebyshev_reduces_outer_iterations(setup):
+    spec, z, prob, *_ = setup
+    zd = prob.to_dev(z)
+    _, plain = prob.solution(zd)
+    prob.set_solver(SolverOptions(tolerance=1e-10, precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=8))
+    try:
+        _, poly = prob.solution(zd)
+    finally:
+        prob.set_solver(SolverOptions(tolerance=1e-10))
+    assert poly["iterations"] * 3 < plain["iterations"], (poly, plain)
+
+
+def test_inhomogeneous_dirichlet_matrix_free_matches_assembled():
+    spec = cantilever(6, 3, 3, SolverOptions(tolerance=1e-11))
+    spec.bc_values = np.linspace(-1e-3, 2e-3, spec.bc_dofs.size)
+    z = splitmix_uniform(spec.coords.shape[0], 17)
+    orc = Oracle.from_spec(spec)
+    uo, _ = orc.solution(z, tol=1e-13)
+    for opts in (SolverOptions(tolerance=1e-11),
+                 SolverOptions(tolerance=1e-11, operator_kind=capi.OPERATOR_MATRIX_FREE,
+                               precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=6)):
+        spec.solver = opts
+        prob = EllipticProblem(spec)
+        u, st = prob.solution(prob.to_dev(z))
+        assert st["converged"] == 1
+        assert rel_l2(host(u), uo) <= 1e-8

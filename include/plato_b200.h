@@ -94,7 +94,9 @@ typedef struct plato_solver_opts {
     int32_t precision;        /* plato_precision                                          */
     int32_t self_adjoint;     /* Problem "Self-Adjoint" (src/elliptic/Problem.hpp:116)    */
     double  chebyshev_ratio;  /* preconditioner interval [lambda_max/ratio, lambda_max]    */
-    int32_t chebyshev_degree; /* operator applies per preconditioner call; 0 = Jacobi      */
+    int32_t chebyshev_degree; /* Chebyshev steps per preconditioner call (it applies the
+                                 operator degree-1 times); 0 with FP64 + assembled = the
+                                 plain Jacobi-PCG, 1 = Jacobi inside flexible CG           */
 } plato_solver_opts;
 
 typedef struct plato_problem_desc {

@@ -566,36 +566,44 @@ int oracle_pcg_jacobi(int32_t N, const int32_t* row_map, const int32_t* cols, co
         st->converged = 1;
         return 0;
     }
+    /* Stop when the iterated residual meets tol (AztecOO's AZ_r0 test); then recompute
+     * b - A x.  In FP64 that cannot be evaluated much below eps ||A|| ||x|| / ||b||, so the
+     * solve is accepted when the true residual is within 10 tol, and otherwise restarted
+     * from the current iterate (fresh search direction), at most 3 times. */
     double rz = dot(r.data(), zv.data(), n);
     double rnorm = std::sqrt(dot(r.data(), r.data(), n));
-    int32_t it = 0;
-    while (it < max_it && rnorm / bnorm > tol) {
-        apply(p.data(), Ap.data());
-        const double alpha = rz / dot(p.data(), Ap.data(), n);
+    int32_t it = 0, restarts = 0;
+    double true_rel = rnorm / bnorm;
+    for (;;) {
+        bool breakdown = false;
+        while (it < max_it && rnorm / bnorm > tol) {
+            apply(p.data(), Ap.data());
+            const double pAp = dot(p.data(), Ap.data(), n);
+            if (!(pAp > 0.0) || !std::isfinite(pAp)) { breakdown = true; break; }
+            const double alpha = rz / pAp;
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; zv[i] = dinv[i] * r[i]; }
-        ++it;
-        rnorm = std::sqrt(dot(r.data(), r.data(), n));
-        if (rnorm / bnorm <= tol) {
-            /* confirm with the true residual; continue from it if the recurrence drifted */
-            apply(x, Ap.data());
-#pragma omp parallel for schedule(static)
-            for (int64_t i = 0; i < n; ++i) { r[i] = b[i] - Ap[i]; zv[i] = dinv[i] * r[i]; }
+            for (int64_t i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; zv[i] = dinv[i] * r[i]; }
+            ++it;
             rnorm = std::sqrt(dot(r.data(), r.data(), n));
-            if (rnorm / bnorm <= tol) break;
+            const double rz_new = dot(r.data(), zv.data(), n);
+            const double beta = rz_new / rz;
+            rz = rz_new;
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < n; ++i) p[i] = zv[i] + beta * p[i];
         }
-        const double rz_new = dot(r.data(), zv.data(), n);
-        const double beta = rz_new / rz;
-        rz = rz_new;
+        apply(x, Ap.data());
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < n; ++i) p[i] = zv[i] + beta * p[i];
+        for (int64_t i = 0; i < n; ++i) { r[i] = b[i] - Ap[i]; zv[i] = dinv[i] * r[i]; p[i] = zv[i]; }
+        true_rel = std::sqrt(dot(r.data(), r.data(), n)) / bnorm;
+        const bool met = (rnorm / bnorm <= tol || breakdown) && true_rel <= 10.0 * tol;
+        if (met || true_rel <= tol || it >= max_it || restarts >= 3) break;
+        ++restarts;
+        rz = dot(r.data(), zv.data(), n);
+        rnorm = true_rel * bnorm;
     }
-    apply(x, Ap.data());
-#pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - Ap[i];
     st->iterations = it;
-    st->relative_residual = std::sqrt(dot(r.data(), r.data(), n)) / bnorm;
-    st->converged = st->relative_residual <= tol ? 1 : 0;
+    st->relative_residual = true_rel;
+    st->converged = true_rel <= 10.0 * tol ? 1 : 0;
     return st->converged ? 0 : 1;
 }
 

@@ -611,7 +611,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         if (rc) return rc;
         const double rel = fin.bb > 0.0 ? std::sqrt(rr / fin.bb) : 0.0;
         stats->relative_residual = rel;
-        if (rel <= tol || fin.bb == 0.0) {
+        // same acceptance as the plain PCG: recurrence met, true residual within 10x of tol
+        const bool recurrence_met = fin.rr <= fin.tol2;
+        if (fin.bb == 0.0 || rel <= tol || (recurrence_met && rel <= 10.0 * tol)) {
             stats->converged = 1;
             stats->status = PLATO_OK;
             return PLATO_OK;

@@ -48,6 +48,9 @@ int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const cha
     char buf[512];
     std::snprintf(buf, sizeof buf, "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
                   cudaGetErrorString(e), what, file, line);
+    // clear the runtime's last-error slot so a later launch check does not report this
+    // (non-sticky) error again; sticky errors persist in the context regardless
+    (void)cudaGetLastError();
     const int status = (e == cudaErrorMemoryAllocation) ? PLATO_OUT_OF_MEMORY : PLATO_CUDA_ERROR;
     return plato_fail(h, status, buf);
 }
@@ -216,7 +219,7 @@ int plato_create(const plato_problem_desc* d, plato_problem** out) {
     CRC(dmalloc(h, &h->partials, 4 * int64_t(h->partials_len)));
     CRC(dmalloc(h, &h->cellbuf, h->C));
     CRC(dmalloc(h, &h->scal, 1));
-    CRC(dmalloc(h, &h->red_out, 1));
+    CRC(dmalloc(h, &h->red_out, 4));  // up to 4 reduction results (power iteration uses 3)
     CRC(dmalloc(h, &h->red_ticket, 1));
     CCUDA(cudaMemset(h->red_ticket, 0, sizeof(uint32_t)));
     CCUDA(cudaMemset(h->scal, 0, sizeof(PcgScalars)));

@@ -204,6 +204,27 @@ int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host
                                           double* value_host, double* dfdz_host,
                                           plato_solve_stats* stats);
 
+/* ---- allocation-free compliance value ---------------------------------------------------
+ * No counterpart in the reference.  Same value as plato_sf_value (internal elastic energy,
+ * 1/2 u^T K(z) u over the cells) for callers that cannot allocate device memory when they
+ * need it (their device memory belongs to another allocator's pool, or they must not risk
+ * the implicit synchronisation of cudaMalloc/cudaFree).  No handle: connectivity
+ * (num_cells*4 int32, 16-byte aligned), coords (num_nodes*3), u (num_nodes*3) and z
+ * (num_nodes) are caller-owned [device] arrays; value is a [device] double written on
+ * cuda_stream (NULL = legacy stream), readable after the caller synchronises that stream.
+ * The call allocates nothing: its reduction scratch is a static device array of 65,536 block
+ * partial sums (512 KiB, held by every GPU that loads the library until exit), so num_cells is
+ * limited to 16,777,216; larger meshes get PLATO_BAD_INPUT.  The first call on a device looks
+ * up the scratch address on the current device; make that first call before any stream
+ * capture.  Every call shares the one scratch array, which keeps the last call's contents:
+ * calls whose kernels overlap on the GPU (different streams, or different host threads on
+ * one device) race and must be serialised by the caller.  Errors read through
+ * plato_last_error(NULL). */
+int plato_sf_value_noalloc(int32_t num_nodes, int32_t num_cells, const int32_t* connectivity,
+                           const double* coords, const double* u, const double* z,
+                           const plato_material* material, const plato_penalty* penalty,
+                           double* value, void* cuda_stream);
+
 /* ---- box mesh generator (host only; stands in for BamG, unit_tests/PlatoTestHelpers.hpp) */
 int plato_box_mesh_sizes(int32_t nx, int32_t ny, int32_t nz, int32_t* num_nodes, int32_t* num_cells);
 int plato_box_mesh_tet4(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,

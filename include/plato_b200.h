@@ -164,6 +164,13 @@ int plato_sf_value(plato_problem* h, const double* u, const double* z, double* v
 int plato_sf_gradient_u(plato_problem* h, const double* u, const double* z, double* dfdu);
 int plato_sf_gradient_z(plato_problem* h, const double* u, const double* z, double* dfdz);
 
+/* ---- Geometric "Volume" criterion (src/geometric/Volume.hpp:83-110) --------------------
+ * V(z) = sum_e |det J_e| / 6 * s_v(rho_e) with the criterion's own penalty s_v (MSIMP
+ * parameters; exponent 1 and minimum 0 give the material volume sum_e vol_e rho_e), and
+ * dV/dz on the nodes (GeometryScalarFunction::gradient_z, SFad<4> control derivative). */
+int plato_volume_value(plato_problem* h, const double* z, const plato_penalty* penalty, double* value /*[host]*/);
+int plato_volume_gradient_z(plato_problem* h, const double* z, const plato_penalty* penalty, double* dvdz);
+
 /* ---- helpers ----------------------------------------------------------------------------
  * applyBlockConstraints<3> with the handle's essential BCs (src/ApplyConstraints.hpp:40-112);
  * scale multiplies the BC values (0 for the adjoint, src/elliptic/Problem.hpp:701-713). */

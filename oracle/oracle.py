@@ -60,6 +60,8 @@ def _load() -> C.CDLL:
         "oracle_problem_criterion_gradient": ([P, vp, vp, C.c_int32, C.c_double, C.c_int32, vp,
                                                C.POINTER(OracleStats)], C.c_int),
         "oracle_num_threads": ([], C.c_int),
+        "oracle_volume_value": ([P, vp, C.c_double, C.c_double], C.c_double),
+        "oracle_volume_gradient_z": ([P, vp, C.c_double, C.c_double, vp], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -206,6 +208,14 @@ class Oracle:
         lib.oracle_problem_criterion_gradient(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)),
                                               _p(np.ascontiguousarray(u, np.float64)), int(self_adjoint), tol,
                                               max_it, _p(g), C.byref(st))
+        return g
+
+    def volume_value(self, z, p=1.0, m=0.0) -> float:
+        return lib.oracle_volume_value(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)), p, m)
+
+    def volume_gradient_z(self, z, p=1.0, m=0.0):
+        g = np.empty(self.N)
+        lib.oracle_volume_gradient_z(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)), p, m, _p(g))
         return g
 
     @staticmethod

@@ -490,6 +490,48 @@ void oracle_sf_gradient_z(const oracle_problem* P, const double* u, const double
     }
 }
 
+/* Geometric Volume criterion, src/geometric/Volume.hpp:83-110: ComputeCellVolume<3>
+ * (src/ImplicitFunctors.hpp:292-315, |det J|) times the cubature weight, weighted by the
+ * criterion's penalty of the cell density (ApplyWeighting); summed over cells.  The gradient
+ * is the SFad<4> control derivative vol * s'(rho) * 1/4 scattered to the cell's nodes. */
+static double cell_volume(const oracle_problem* P, int32_t c) {
+    const int32_t* n = P->connectivity + 4 * (int64_t)c;
+    auto X = [&](int a, int d) { return P->coords[3 * (int64_t)n[a] + d]; };
+    double j11 = X(0, 0) - X(3, 0), j12 = X(1, 0) - X(3, 0), j13 = X(2, 0) - X(3, 0);
+    double j21 = X(0, 1) - X(3, 1), j22 = X(1, 1) - X(3, 1), j23 = X(2, 1) - X(3, 1);
+    double j31 = X(0, 2) - X(3, 2), j32 = X(1, 2) - X(3, 2), j33 = X(2, 2) - X(3, 2);
+    double detj = j11 * j22 * j33 + j12 * j23 * j31 + j13 * j21 * j32
+                - j11 * j23 * j32 - j12 * j21 * j33 - j13 * j22 * j31;
+    return std::fabs(detj) * cub_weight(3);
+}
+
+double oracle_volume_value(const oracle_problem* P, const double* z, double p, double m) {
+    oracle_problem Q = *P;
+    Q.penalty_exponent = p;
+    Q.penalty_minimum = m;
+    double total = 0.0;
+#pragma omp parallel for reduction(+ : total) schedule(static)
+    for (int32_t c = 0; c < P->num_cells; ++c) {
+        double v = cell_volume(P, c);
+        v *= msimp(&Q, cell_density(z, P->connectivity + 4 * (int64_t)c));
+        total += v;
+    }
+    return total;
+}
+
+void oracle_volume_gradient_z(const oracle_problem* P, const double* z, double p, double m, double* dvdz) {
+    oracle_problem Q = *P;
+    Q.penalty_exponent = p;
+    Q.penalty_minimum = m;
+    std::fill(dvdz, dvdz + (int64_t)P->num_nodes, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int32_t c = 0; c < P->num_cells; ++c) {
+        const int32_t* nd = P->connectivity + 4 * (int64_t)c;
+        const double val = cell_volume(P, c) * (msimp_dx(&Q, cell_density(z, nd)) * (1.0 / kNodesPerCell));
+        for (int k = 0; k < 4; ++k) atomic_add(&dvdz[nd[k]], val);
+    }
+}
+
 /* applyBlockConstraints<3>, src/ApplyConstraints.hpp:40-112 (both loops). */
 void oracle_apply_block_constraints(int32_t num_node_rows, const int32_t* row_map,
                                     const int32_t* cols, double* entries, double* rhs,

@@ -73,6 +73,10 @@ double oracle_sf_value(const oracle_problem* P, const double* u, const double* z
 void   oracle_sf_gradient_u(const oracle_problem* P, const double* u, const double* z, double* dfdu);
 void   oracle_sf_gradient_z(const oracle_problem* P, const double* u, const double* z, double* dfdz);
 
+/* Geometric "Volume" criterion with its own MSIMP penalty (exponent p, minimum m). */
+double oracle_volume_value(const oracle_problem* P, const double* z, double p, double m);
+void   oracle_volume_gradient_z(const oracle_problem* P, const double* z, double p, double m, double* dvdz);
+
 /* helpers */
 void oracle_apply_block_constraints(int32_t num_node_rows, const int32_t* row_map,
                                     const int32_t* column_indices, double* entries, double* rhs,

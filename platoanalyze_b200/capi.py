@@ -97,6 +97,8 @@ def _load() -> C.CDLL:
         "plato_apply_constraints": ([vp, vp, vp, C.c_double], C.c_int),
         "plato_matvec_plus": ([vp, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
         "plato_apply_operator": ([vp, vp, C.c_int32, vp, vp], C.c_int),
+        "plato_volume_value": ([vp, vp, C.POINTER(Penalty), f64p], C.c_int),
+        "plato_volume_gradient_z": ([vp, vp, C.POINTER(Penalty), vp], C.c_int),
         "plato_solver_solve": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_problem_solution": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_problem_criterion_value": ([vp, vp, vp, f64p], C.c_int),

@@ -33,6 +33,8 @@ int matfree_setup(plato_problem* h, const double* z);
 int launch_ebe_apply64(plato_problem* h, const double* x, double* y, const PcgScalars* S);
 int launch_mask_copy(plato_problem* h, const double* x, double* y);
 int launch_sell_spmv(plato_problem* h, const double* vals, const double* x, double* y);
+int launch_volume(plato_problem* h, const Material& pen, const double* z, double* result);
+int launch_volume_gradient(plato_problem* h, const Material& pen, const double* z, double* dvdz);
 }  // namespace plato
 
 using namespace plato;
@@ -351,6 +353,30 @@ int plato_sf_gradient_u(plato_problem* h, const double* u, const double* z, doub
 int plato_sf_gradient_z(plato_problem* h, const double* u, const double* z, double* dfdz) {
     NEED(h, u && z && dfdz, "null device pointer");
     return launch_nodal_control_derivative(h, 1, u, z, nullptr, h->cellbuf, dfdz, 0);
+}
+
+static Material volume_penalty(const plato_penalty* p) {
+    Material m{};
+    m.p = p->exponent;
+    m.rho_min = p->minimum_value;
+    m.p_int = (p->exponent >= 0.0 && p->exponent <= 16.0 && std::floor(p->exponent) == p->exponent)
+                  ? int(p->exponent) : -1;
+    return m;
+}
+
+int plato_volume_value(plato_problem* h, const double* z, const plato_penalty* penalty, double* value) {
+    NEED(h, z && penalty && value, "null pointer");
+    NEED(h, std::isfinite(penalty->exponent) && std::isfinite(penalty->minimum_value), "non-finite penalty");
+    RC(launch_volume(h, volume_penalty(penalty), z, h->red_out));
+    PLATO_CUDA(h, cudaMemcpyAsync(value, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PLATO_OK;
+}
+
+int plato_volume_gradient_z(plato_problem* h, const double* z, const plato_penalty* penalty, double* dvdz) {
+    NEED(h, z && penalty && dvdz, "null pointer");
+    NEED(h, std::isfinite(penalty->exponent) && std::isfinite(penalty->minimum_value), "non-finite penalty");
+    return launch_volume_gradient(h, volume_penalty(penalty), z, dvdz);
 }
 
 int plato_apply_constraints(plato_problem* h, double* entries, double* rhs, double scale) {

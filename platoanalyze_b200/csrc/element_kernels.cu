@@ -170,6 +170,54 @@ __global__ void __launch_bounds__(kThreads) k_energy_sum(MeshView m, Material ma
     }
 }
 
+// Geometric "Volume" criterion (src/geometric/Volume.hpp:83-110): cell volume |det J| / 6
+// weighted by the criterion's own penalty s_v(rho) (ApplyWeighting); GRAD = 1 gives the
+// derivative with respect to one nodal control, vol s_v'(rho) / 4.
+template <int GRAD>
+__device__ __forceinline__ double cell_volume_quantity(const MeshView& m, const Material& pen,
+                                                       const double* __restrict__ z, int64_t c) {
+    CellState cs;
+    load_cell(m, z, c, cs);
+    return GRAD ? cs.G.vol * simp_dx(pen, cs.rho) * 0.25 : cs.G.vol * simp(pen, cs.rho);
+}
+
+__global__ void __launch_bounds__(kThreads) k_volume_sum(MeshView m, Material pen, const double* __restrict__ z,
+                                                         double* __restrict__ partials,
+                                                         unsigned int* __restrict__ ticket,
+                                                         double* __restrict__ result) {
+    __shared__ double sh[32];
+    __shared__ bool last;
+    double v = 0.0;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < m.num_cells;
+         c += (int64_t)gridDim.x * blockDim.x)
+        v += cell_volume_quantity<0>(m, pen, z, c);
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v;
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double t = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) t += partials[b];
+        t = block_sum(t, sh);
+        if (threadIdx.x == 0) {
+            *result = t;
+            *ticket = 0u;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_volume_cell_grad(MeshView m, Material pen,
+                                                               const double* __restrict__ z,
+                                                               double* __restrict__ out) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < m.num_cells;
+         c += (int64_t)gridDim.x * blockDim.x)
+        out[c] = cell_volume_quantity<1>(m, pen, z, c);
+}
+
 // Traction load F: SurfaceLoadIntegral<3> (src/SurfaceLoadIntegral.hpp:97-150) with the
 // triangle degree-one rule (weight 1/2, basis 1/3 each), area from
 // CalculateSurfaceArea<3> (src/SurfaceIntegralUtilities.hpp:217-227).
@@ -250,6 +298,22 @@ int launch_nodal_control_derivative(plato_problem* h, int mode, const double* u,
     }
     PLATO_LAUNCH_CHECK(h);
     k_node_sum<<<grid_for(h->N, kThreads), kThreads, 0, h->stream>>>(graph_view(h), cellbuf, out, accumulate);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+// Volume criterion value into *result (device scalar) and its nodal gradient.
+int launch_volume(plato_problem* h, const Material& pen, const double* z, double* result) {
+    const int G = grid_for(h->C, kThreads, h->partials_len);
+    k_volume_sum<<<G, kThreads, 0, h->stream>>>(mesh_view(h), pen, z, h->partials, h->red_ticket, result);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+int launch_volume_gradient(plato_problem* h, const Material& pen, const double* z, double* dvdz) {
+    k_volume_cell_grad<<<grid_for(h->C, kThreads), kThreads, 0, h->stream>>>(mesh_view(h), pen, z, h->cellbuf);
+    PLATO_LAUNCH_CHECK(h);
+    k_node_sum<<<grid_for(h->N, kThreads), kThreads, 0, h->stream>>>(graph_view(h), h->cellbuf, dvdz, 0);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -203,6 +203,17 @@ class EllipticProblem:
         check(lib.plato_matvec_plus(self.h, rb, cb, self._dev(entries), self._dev(x), self._dev(y)), self.h)
         return y
 
+    def volume_value(self, z, exponent=1.0, minimum=0.0) -> float:
+        """Geometric Volume criterion sum_e vol_e s_v(rho_e) (penalty exponent 1, minimum 0 by default)."""
+        v, pen = C.c_double(), capi.Penalty(exponent, minimum)
+        check(lib.plato_volume_value(self.h, self._dev(z), C.byref(pen), C.byref(v)), self.h)
+        return v.value
+
+    def volume_gradient_z(self, z, exponent=1.0, minimum=0.0):
+        g, pen = self.zeros(self.num_nodes), capi.Penalty(exponent, minimum)
+        check(lib.plato_volume_gradient_z(self.h, self._dev(z), C.byref(pen), self._dev(g)), self.h)
+        return g
+
     def apply_operator(self, z, x, operator_kind=capi.OPERATOR_ASSEMBLED):
         """y = K_c(z) x, K_c the Dirichlet-constrained stiffness (assembled or matrix-free)."""
         y = self.zeros(self.num_dofs)

@@ -256,3 +256,13 @@ def test_bad_connectivity_rejected():
     conn[0, 0] = m.num_nodes  # out of range
     with pytest.raises(capi.PlatoError):
         EllipticProblem(ProblemSpec(m.coords, conn))
+
+
+def test_volume_criterion(small):
+    spec, prob, orc, z = small
+    zd = prob.to_dev(z)
+    for p, m in ((1.0, 0.0), (3.0, 1e-3)):
+        v = prob.volume_value(zd, p, m)
+        assert abs(v - orc.volume_value(z, p, m)) <= TOL * abs(v)
+        close(host(prob.volume_gradient_z(zd, p, m)), orc.volume_gradient_z(z, p, m))
+    assert prob.volume_value(prob.to_dev(np.ones(orc.N)), 1.0, 0.0) == pytest.approx(2.0, rel=1e-13)

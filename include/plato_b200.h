@@ -97,6 +97,11 @@ typedef struct plato_solver_opts {
     int32_t chebyshev_degree; /* Chebyshev steps per preconditioner call (it applies the
                                  operator degree-1 times); 0 with FP64 + assembled = the
                                  plain Jacobi-PCG, 1 = Jacobi inside flexible CG           */
+    int32_t coarse_cells[3];  /* two-level preconditioner: coarse box grid of
+                                 coarse_cells[0] x [1] x [2] cells over the mesh bounding
+                                 box (trilinear coarse space, Galerkin coarse operator);
+                                 {0,0,0} = none.  Needs every element inside one coarse
+                                 cell (box meshes with divisible cell counts)             */
 } plato_solver_opts;
 
 typedef struct plato_problem_desc {

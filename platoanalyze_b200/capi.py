@@ -46,7 +46,7 @@ class EssentialBCs(C.Structure):
 class SolverOpts(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int32), ("operator_kind", C.c_int32),
                 ("precision", C.c_int32), ("self_adjoint", C.c_int32), ("chebyshev_ratio", C.c_double),
-                ("chebyshev_degree", C.c_int32)]
+                ("chebyshev_degree", C.c_int32), ("coarse_cells", C.c_int32 * 3)]
 
 
 class ProblemDesc(C.Structure):

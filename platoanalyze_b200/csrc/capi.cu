@@ -24,6 +24,7 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
 int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* stats);
 int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* stats);
 int prepare_mixed(plato_problem* h, const double* crs, const double* z);
+int prepare_coarse(plato_problem* h, const double* z);
 int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
 int matfree_rhs(plato_problem* h, double* b, double scale);
 int launch_dirichlet_rhs(plato_problem* h, double* rhs, double scale);
@@ -128,6 +129,7 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_res); dfree(h->f_d0); dfree(h->f_d1); dfree(h->f_y); dfree(h->f_w);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    coarse_release(h);
     delete h;
     return PLATO_OK;
 }
@@ -153,6 +155,16 @@ int plato_create(const plato_problem_desc* d, plato_problem** out) {
     h->N = m.num_nodes;
     h->C = m.num_cells;
     h->opts = d->solver;
+    for (int dd = 0; dd < 3; ++dd) {
+        h->bbox_min[dd] = m.coords[dd];
+        h->bbox_max[dd] = m.coords[dd];
+    }
+    for (int64_t p = 1; p < m.num_nodes; ++p)
+        for (int dd = 0; dd < 3; ++dd) {
+            const double v = m.coords[3 * p + dd];
+            if (v < h->bbox_min[dd]) h->bbox_min[dd] = v;
+            if (v > h->bbox_max[dd]) h->bbox_max[dd] = v;
+        }
     if (int rc = check_opts(h, h->opts)) { g_create_error = h->last_error; delete h; return rc; }
     cudaGetDevice(&h->device);
 
@@ -416,6 +428,7 @@ int plato_solver_solve(plato_problem* h, const double* entries, double* x, const
     }
     const int32_t kind = h->opts.operator_kind;
     h->opts.operator_kind = PLATO_OPERATOR_ASSEMBLED;
+    h->coarse.active = 0;  // the coarse operator needs the control, which this entry point lacks
     int rc = prepare_mixed(h, entries, nullptr);
     if (!rc) rc = fcg_poly(h, b, x, st);
     h->opts.operator_kind = kind;
@@ -488,7 +501,7 @@ namespace plato {
 
 static bool plain_method(const plato_solver_opts& o) {
     return o.operator_kind == PLATO_OPERATOR_ASSEMBLED && o.precision == PLATO_PRECISION_FP64 &&
-           o.chebyshev_degree <= 0;
+           o.chebyshev_degree <= 0 && o.coarse_cells[0] <= 0;
 }
 
 // Builds the constrained operator of control z and the right-hand side (rhs with the
@@ -500,8 +513,10 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
     const int64_t n = 3 * int64_t(h->N);
     if (rhs != h->v_b)
         PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    h->coarse.active = 0;
     if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
         RC(prepare_mixed(h, nullptr, z));
+        RC(prepare_coarse(h, z));
         RC(matfree_rhs(h, h->v_b, bc_scale));
         return fcg_poly(h, h->v_b, x, st);
     }
@@ -513,6 +528,7 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         return pcg_fp64(h, h->v_b, x, st);
     }
     RC(prepare_mixed(h, h->K, z));
+    RC(prepare_coarse(h, z));
     return fcg_poly(h, h->v_b, x, st);
 }
 

@@ -1,0 +1,545 @@
+// Two-level preconditioner: trilinear coarse space on a box grid and its Galerkin operator.
+//
+// Coarse space Z (3N x 3Nc): a box grid of nc[0] x nc[1] x nc[2] cells over the mesh
+// bounding box; fine dof (p, d) = sum over the 8 corners J of p's cell of phi_J(x_p) U_(J,d),
+// phi_J trilinear; constrained fine dofs are masked out (P Z), so the coarse space never
+// moves a clamped dof.  The coarse operator is exactly Galerkin, E = (PZ)^T K (PZ), assembled
+// element by element: with every element inside one coarse cell, the coarse basis restricted
+// to an element is the linear interpolant of its nodal values, whose gradient is
+// G_J^(d) = sum_a m_(a,d) phi_J(x_a) grad N_a, so E gets
+// vol s(rho) (lambda G_J^(i)_i G_L^(j)_j + mu G_J^(i)_j G_L^(j)_i + mu delta_ij G_J^(i).G_L^(i))
+// from each element (the isotropic block formula with coarse gradients).
+//
+// Per solve: one CTA per coarse cell accumulates its 24x24 block over its elements (batches
+// staged in shared memory, each thread owning a few entries in registers), then E is
+// factored (blocked Cholesky, 32x32 tiles) and inverted explicitly (E^-1 = L^-T L^-1), so a
+// coarse solve in the iteration is one dense matrix-vector product.
+// Per preconditioner call: restriction (one CTA per coarse node gathers its support through
+// the per-cell node lists, deterministic), y_c = E^-1 r_c (warp per row), prolongation.
+#include <cub/cub.cuh>
+
+#include "plato_internal.cuh"
+
+namespace plato {
+
+GraphView graph_view(const plato_problem* h);
+
+namespace {
+
+constexpr int kTile = 32;
+constexpr int kBatch = 64;
+
+struct CoarseView {
+    int nc0, nc1, nc2;
+    double x0, y0, z0, hx, hy, hz;
+};
+
+__host__ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ void cell_of(const CoarseView& cv, double x, double y, double z, int& cx, int& cy,
+                                        int& cz) {
+    cx = clampi(int(floor((x - cv.x0) / cv.hx)), 0, cv.nc0 - 1);
+    cy = clampi(int(floor((y - cv.y0) / cv.hy)), 0, cv.nc1 - 1);
+    cz = clampi(int(floor((z - cv.z0) / cv.hz)), 0, cv.nc2 - 1);
+}
+
+__device__ __forceinline__ int cell_id(const CoarseView& cv, int cx, int cy, int cz) {
+    return (cx * cv.nc1 + cy) * cv.nc2 + cz;
+}
+
+__device__ __forceinline__ int coarse_node(const CoarseView& cv, int ix, int iy, int iz) {
+    return (ix * (cv.nc1 + 1) + iy) * (cv.nc2 + 1) + iz;
+}
+
+// trilinear weight of corner (bx,by,bz) at local coordinates (u,v,w)
+__device__ __forceinline__ double corner_weight(int b, double u, double v, double w) {
+    return ((b & 4) ? u : 1.0 - u) * ((b & 2) ? v : 1.0 - v) * ((b & 1) ? w : 1.0 - w);
+}
+
+__global__ void k_node_keys(int32_t N, const double* __restrict__ coords, CoarseView cv, uint32_t* __restrict__ key,
+                            int32_t* __restrict__ val, int32_t* __restrict__ count) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        int cx, cy, cz;
+        cell_of(cv, coords[3 * p], coords[3 * p + 1], coords[3 * p + 2], cx, cy, cz);
+        const int c = cell_id(cv, cx, cy, cz);
+        key[p] = uint32_t(c);
+        val[p] = int32_t(p);
+        atomicAdd(&count[c], 1);
+    }
+}
+
+// cell of an element = cell of its centroid; flags elements with a node outside that cell
+__global__ void k_elem_keys(int32_t C, const int4* __restrict__ conn, const double* __restrict__ coords, CoarseView cv,
+                            uint32_t* __restrict__ key, int32_t* __restrict__ val, int32_t* __restrict__ count,
+                            int32_t* __restrict__ bad) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < C; e += (int64_t)gridDim.x * blockDim.x) {
+        const int4 n = conn[e];
+        double x[4][3];
+        load_cell_coords(coords, n, x);
+        double c[3] = {0, 0, 0};
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) c[d] += 0.25 * x[a][d];
+        int cx, cy, cz;
+        cell_of(cv, c[0], c[1], c[2], cx, cy, cz);
+        const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
+        const double hh[3] = {cv.hx, cv.hy, cv.hz};
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) {
+                const double t = (x[a][d] - lo[d]) / hh[d];
+                if (t < -1e-9 || t > 1.0 + 1e-9) atomicExch(bad, 1);
+            }
+        const int cid = cell_id(cv, cx, cy, cz);
+        key[e] = uint32_t(cid);
+        val[e] = int32_t(e);
+        atomicAdd(&count[cid], 1);
+    }
+}
+
+// E (n x n, row-major) += Galerkin contribution of every element; one CTA per coarse cell.
+__global__ void __launch_bounds__(256)
+k_galerkin(CoarseView cv, const int32_t* __restrict__ elem_ptr, const int32_t* __restrict__ elem_list,
+           const int4* __restrict__ conn, const double* __restrict__ coords, const double* __restrict__ z,
+           Material mat, const uint8_t* __restrict__ mask, int n, double* __restrict__ E) {
+    __shared__ double Gs[kBatch][3][8][3];
+    __shared__ double ws[kBatch];
+    const int ncells = cv.nc0 * cv.nc1 * cv.nc2;
+    const double lam = mat.c01, mu = mat.c33;
+    for (int cell = blockIdx.x; cell < ncells; cell += gridDim.x) {
+        const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
+        const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
+        double acc[3] = {0.0, 0.0, 0.0};
+        const int e0 = elem_ptr[cell], e1 = elem_ptr[cell + 1];
+        for (int base = e0; base < e1; base += kBatch) {
+            if (threadIdx.x < kBatch) {
+                const int k = threadIdx.x;
+                double w = 0.0;
+                if (base + k < e1) {
+                    const int e = elem_list[base + k];
+                    const int4 nd = conn[e];
+                    double x[4][3];
+                    load_cell_coords(coords, nd, x);
+                    TetGeom<double> G;
+                    tet_geometry(x, G);
+                    const double rho = (z[nd.x] + z[nd.y] + z[nd.z] + z[nd.w]) * 0.25;
+                    w = G.vol * simp(mat, rho);
+                    const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
+                    double loc[4][3];
+                    for (int a = 0; a < 4; ++a) {
+                        loc[a][0] = (x[a][0] - lo[0]) / cv.hx;
+                        loc[a][1] = (x[a][1] - lo[1]) / cv.hy;
+                        loc[a][2] = (x[a][2] - lo[2]) / cv.hz;
+                    }
+                    for (int d = 0; d < 3; ++d)
+                        for (int J = 0; J < 8; ++J) {
+                            double gj[3] = {0.0, 0.0, 0.0};
+                            for (int a = 0; a < 4; ++a) {
+                                if (mask[3 * (int64_t)ids[a] + d]) continue;
+                                const double wa = corner_weight(J, loc[a][0], loc[a][1], loc[a][2]);
+                                gj[0] += wa * G.g[a][0];
+                                gj[1] += wa * G.g[a][1];
+                                gj[2] += wa * G.g[a][2];
+                            }
+                            Gs[k][d][J][0] = gj[0];
+                            Gs[k][d][J][1] = gj[1];
+                            Gs[k][d][J][2] = gj[2];
+                        }
+                }
+                ws[k] = w;
+            }
+            __syncthreads();
+            const int nb = min(kBatch, e1 - base);
+            for (int s = 0; s < 3; ++s) {
+                const int t = threadIdx.x + 256 * s;
+                if (t >= 576) break;
+                const int r = t / 24, c = t - 24 * (t / 24);
+                const int J = r / 3, i = r - 3 * (r / 3), L = c / 3, j = c - 3 * (c / 3);
+                double a = 0.0;
+                for (int k = 0; k < nb; ++k) {
+                    const double* Gi = Gs[k][i][J];
+                    const double* Gj = Gs[k][j][L];
+                    double v = lam * Gi[i] * Gj[j] + mu * Gi[j] * Gj[i];
+                    if (i == j) v += mu * (Gi[0] * Gj[0] + Gi[1] * Gj[1] + Gi[2] * Gj[2]);
+                    a += ws[k] * v;
+                }
+                acc[s] += a;
+            }
+            __syncthreads();
+        }
+        for (int s = 0; s < 3; ++s) {
+            const int t = threadIdx.x + 256 * s;
+            if (t >= 576) break;
+            const int r = t / 24, c = t - 24 * (t / 24);
+            const int J = r / 3, i = r - 3 * (r / 3), L = c / 3, j = c - 3 * (c / 3);
+            const int gJ = coarse_node(cv, cx + ((J >> 2) & 1), cy + ((J >> 1) & 1), cz + (J & 1));
+            const int gL = coarse_node(cv, cx + ((L >> 2) & 1), cy + ((L >> 1) & 1), cz + (L & 1));
+            if (acc[s] != 0.0) atomicAdd(&E[(int64_t)(3 * gJ + i) * n + 3 * gL + j], acc[s]);
+        }
+    }
+}
+
+// Zero rows/columns (coarse dofs whose basis vanishes after masking) get a unit diagonal.
+__global__ void k_regularize(int n, double* __restrict__ E) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        if (!(E[(int64_t)k * n + k] > 0.0)) E[(int64_t)k * n + k] = 1.0;
+}
+
+// ---- blocked Cholesky (lower, in place) --------------------------------------------------
+
+__global__ void k_chol_diag(int n, double* __restrict__ A, int kb, int32_t* __restrict__ bad) {
+    __shared__ double T[kTile][kTile + 1];
+    const int r0 = kb * kTile, m = min(kTile, n - r0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (tx < m && ty < m) T[ty][tx] = A[(int64_t)(r0 + ty) * n + r0 + tx];
+    __syncthreads();
+    for (int k = 0; k < m; ++k) {
+        if (tx == 0 && ty == 0) {
+            const double d = T[k][k];
+            if (!(d > 0.0)) { atomicExch(bad, 1); T[k][k] = 1.0; }
+            else T[k][k] = sqrt(d);
+        }
+        __syncthreads();
+        if (tx == 0 && ty > k && ty < m) T[ty][k] /= T[k][k];
+        __syncthreads();
+        if (ty > k && tx > k && tx <= ty && ty < m) T[ty][tx] -= T[ty][k] * T[tx][k];
+        __syncthreads();
+    }
+    if (tx < m && ty < m) A[(int64_t)(r0 + ty) * n + r0 + tx] = (tx <= ty) ? T[ty][tx] : 0.0;
+}
+
+// A[ib,kb] <- A[ib,kb] L_kk^-T for every block row ib > kb (one CTA per block row)
+__global__ void k_chol_panel(int n, double* __restrict__ A, int kb) {
+    __shared__ double L[kTile][kTile + 1];
+    __shared__ double X[kTile][kTile + 1];
+    const int ib = kb + 1 + blockIdx.x;
+    const int r0 = ib * kTile, c0 = kb * kTile;
+    const int mr = min(kTile, n - r0), mc = min(kTile, n - c0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (tx < mc && ty < mc) L[ty][tx] = A[(int64_t)(c0 + ty) * n + c0 + tx];
+    if (tx < mc && ty < mr) X[ty][tx] = A[(int64_t)(r0 + ty) * n + c0 + tx];
+    __syncthreads();
+    // row ty solves x L^T = a: x_c = (a_c - sum_{k<c} x_k L_ck) / L_cc
+    if (tx == 0 && ty < mr)
+        for (int c = 0; c < mc; ++c) {
+            double s = X[ty][c];
+            for (int k = 0; k < c; ++k) s -= X[ty][k] * L[c][k];
+            X[ty][c] = s / L[c][c];
+        }
+    __syncthreads();
+    if (tx < mc && ty < mr) A[(int64_t)(r0 + ty) * n + c0 + tx] = X[ty][tx];
+}
+
+// trailing update A[ib,jb] -= A[ib,kb] A[jb,kb]^T for kb < jb <= ib
+__global__ void k_chol_update(int n, double* __restrict__ A, int kb, int nblk) {
+    __shared__ double P[kTile][kTile + 1];
+    __shared__ double Q[kTile][kTile + 1];
+    const int rem = nblk - kb - 1;
+    // blockIdx.x enumerates (ib, jb) with jb <= ib in the trailing triangle
+    int idx = blockIdx.x, ib = 0;
+    while (idx >= ib + 1) { idx -= ib + 1; ++ib; }
+    const int jb = idx;
+    if (ib >= rem) return;
+    const int gi = kb + 1 + ib, gj = kb + 1 + jb;
+    const int r0 = gi * kTile, s0 = gj * kTile, c0 = kb * kTile;
+    const int mr = min(kTile, n - r0), ms = min(kTile, n - s0), mc = min(kTile, n - c0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    P[ty][tx] = (ty < mr && tx < mc) ? A[(int64_t)(r0 + ty) * n + c0 + tx] : 0.0;
+    Q[ty][tx] = (ty < ms && tx < mc) ? A[(int64_t)(s0 + ty) * n + c0 + tx] : 0.0;
+    __syncthreads();
+    if (ty < mr && tx < ms) {
+        double s = 0.0;
+        for (int k = 0; k < mc; ++k) s += P[ty][k] * Q[tx][k];
+        A[(int64_t)(r0 + ty) * n + s0 + tx] -= s;
+    }
+}
+
+// X = L^-1 by column blocks (one CTA per column block cb); L lower in A.
+__global__ void k_tri_inverse(int n, const double* __restrict__ A, double* __restrict__ X, int nblk) {
+    __shared__ double L[kTile][kTile + 1];
+    __shared__ double T[kTile][kTile + 1];
+    __shared__ double Y[kTile][kTile + 1];
+    const int cb = blockIdx.x;
+    const int c0 = cb * kTile, mc = min(kTile, n - c0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int ib = 0; ib < cb; ++ib) {  // strictly above the diagonal block: zero
+        const int r0 = ib * kTile, mr = min(kTile, n - r0);
+        if (ty < mr && tx < mc) X[(int64_t)(r0 + ty) * n + c0 + tx] = 0.0;
+    }
+    for (int ib = cb; ib < nblk; ++ib) {
+        const int r0 = ib * kTile, mr = min(kTile, n - r0);
+        // T = I[ib,cb] - sum_{kb=cb}^{ib-1} L[ib,kb] X[kb,cb]
+        double t = (ib == cb && tx == ty) ? 1.0 : 0.0;
+        for (int kb = cb; kb < ib; ++kb) {
+            const int k0 = kb * kTile, mk = min(kTile, n - k0);
+            __syncthreads();
+            L[ty][tx] = (ty < mr && tx < mk) ? A[(int64_t)(r0 + ty) * n + k0 + tx] : 0.0;
+            Y[ty][tx] = (ty < mk && tx < mc) ? X[(int64_t)(k0 + ty) * n + c0 + tx] : 0.0;
+            __syncthreads();
+            for (int k = 0; k < mk; ++k) t -= L[ty][k] * Y[k][tx];
+        }
+        __syncthreads();
+        T[ty][tx] = t;
+        L[ty][tx] = (ty < mr && tx < mr) ? A[(int64_t)(r0 + ty) * n + r0 + tx] : 0.0;
+        __syncthreads();
+        // forward substitution L_ii Z = T, column tx
+        if (ty == 0 && tx < mc)
+            for (int r = 0; r < mr; ++r) {
+                double s = T[r][tx];
+                for (int k = 0; k < r; ++k) s -= L[r][k] * T[k][tx];
+                T[r][tx] = s / L[r][r];
+            }
+        __syncthreads();
+        if (ty < mr && tx < mc) X[(int64_t)(r0 + ty) * n + c0 + tx] = T[ty][tx];
+    }
+}
+
+// Einv = X^T X for X = L^-1 (lower): Einv[ib,jb] = sum_{kb >= max(ib,jb)} X[kb,ib]^T X[kb,jb]
+__global__ void k_gram(int n, const double* __restrict__ X, double* __restrict__ Einv, int nblk) {
+    __shared__ double P[kTile][kTile + 1];
+    __shared__ double Q[kTile][kTile + 1];
+    const int ib = blockIdx.y, jb = blockIdx.x;
+    const int r0 = ib * kTile, s0 = jb * kTile;
+    const int mr = min(kTile, n - r0), ms = min(kTile, n - s0);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    double acc = 0.0;
+    for (int kb = max(ib, jb); kb < nblk; ++kb) {
+        const int k0 = kb * kTile, mk = min(kTile, n - k0);
+        __syncthreads();
+        P[ty][tx] = (ty < mk && tx < mr) ? X[(int64_t)(k0 + ty) * n + r0 + tx] : 0.0;
+        Q[ty][tx] = (ty < mk && tx < ms) ? X[(int64_t)(k0 + ty) * n + s0 + tx] : 0.0;
+        __syncthreads();
+        for (int k = 0; k < mk; ++k) acc += P[k][ty] * Q[k][tx];
+    }
+    if (ty < mr && tx < ms) Einv[(int64_t)(r0 + ty) * n + s0 + tx] = acc;
+}
+
+// ---- per-iteration kernels ----------------------------------------------------------------
+
+// rc[(J,d)] = sum_p phi_J(x_p) m_(p,d) v[(p,d)] (one CTA per coarse node, deterministic)
+__global__ void __launch_bounds__(256)
+k_restrict(CoarseView cv, const int32_t* __restrict__ node_ptr, const int32_t* __restrict__ node_list,
+           const double* __restrict__ coords, const uint8_t* __restrict__ mask, const float* __restrict__ v,
+           double* __restrict__ rc, const PcgScalars* S) {
+    __shared__ double sh[3][8];
+    if (S && S->done) return;
+    const int ncn = (cv.nc0 + 1) * (cv.nc1 + 1) * (cv.nc2 + 1);
+    for (int J = blockIdx.x; J < ncn; J += gridDim.x) {
+        const int iz = J % (cv.nc2 + 1), iy = (J / (cv.nc2 + 1)) % (cv.nc1 + 1), ix = J / ((cv.nc1 + 1) * (cv.nc2 + 1));
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < 8; ++b) {
+            const int cx = ix - ((b >> 2) & 1), cy = iy - ((b >> 1) & 1), cz = iz - (b & 1);
+            if (cx < 0 || cy < 0 || cz < 0 || cx >= cv.nc0 || cy >= cv.nc1 || cz >= cv.nc2) continue;
+            const int cell = cell_id(cv, cx, cy, cz);
+            const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
+            for (int q = node_ptr[cell] + threadIdx.x; q < node_ptr[cell + 1]; q += blockDim.x) {
+                const int64_t p = node_list[q];
+                const double wgt = corner_weight(b, (coords[3 * p] - lo[0]) / cv.hx,
+                                                 (coords[3 * p + 1] - lo[1]) / cv.hy, (coords[3 * p + 2] - lo[2]) / cv.hz);
+                for (int d = 0; d < 3; ++d)
+                    if (!mask[3 * p + d]) s[d] += wgt * double(v[3 * p + d]);
+            }
+        }
+        for (int d = 0; d < 3; ++d)
+            for (int o = 16; o > 0; o >>= 1) s[d] += __shfl_xor_sync(0xffffffffu, s[d], o);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0)
+            for (int d = 0; d < 3; ++d) sh[d][w] = s[d];
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double t = 0.0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[threadIdx.x][k];
+            rc[3 * J + threadIdx.x] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// yc = Einv rc (warp per row)
+__global__ void k_coarse_gemv(int n, const double* __restrict__ Einv, const double* __restrict__ rc,
+                              double* __restrict__ yc, const PcgScalars* S) {
+    if (S && S->done) return;
+    const int lane = threadIdx.x & 31;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
+        double s = 0.0;
+        for (int c = lane; c < n; c += 32) s += Einv[(int64_t)row * n + c] * rc[c];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) yc[row] = s;
+    }
+}
+
+// y[(p,d)] (+)= m_(p,d) sum_J phi_J(x_p) yc[(J,d)]
+__global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ coords, const uint8_t* __restrict__ mask,
+                          const double* __restrict__ yc, float* __restrict__ y, int accumulate, const PcgScalars* S) {
+    if (S && S->done) return;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+        const double x = coords[3 * p], yy = coords[3 * p + 1], zz = coords[3 * p + 2];
+        int cx, cy, cz;
+        cell_of(cv, x, yy, zz, cx, cy, cz);
+        const double u = (x - (cv.x0 + cx * cv.hx)) / cv.hx, v = (yy - (cv.y0 + cy * cv.hy)) / cv.hy,
+                     w = (zz - (cv.z0 + cz * cv.hz)) / cv.hz;
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < 8; ++b) {
+            const double wgt = corner_weight(b, u, v, w);
+            const int J = coarse_node(cv, cx + ((b >> 2) & 1), cy + ((b >> 1) & 1), cz + (b & 1));
+            s[0] += wgt * yc[3 * J];
+            s[1] += wgt * yc[3 * J + 1];
+            s[2] += wgt * yc[3 * J + 2];
+        }
+        for (int d = 0; d < 3; ++d) {
+            const float val = mask[3 * p + d] ? 0.f : float(s[d]);
+            y[3 * p + d] = accumulate ? y[3 * p + d] + val : val;
+        }
+    }
+}
+
+}  // namespace
+
+static CoarseView coarse_view(const plato_problem* h) {
+    const CoarseSpace& c = h->coarse;
+    return CoarseView{c.nc[0], c.nc[1], c.nc[2], c.x0[0], c.x0[1], c.x0[2], c.h[0], c.h[1], c.h[2]};
+}
+
+static int csr_by_key(plato_problem* h, int64_t count, uint32_t* keys, int32_t* vals, int32_t* hist, int nkeys,
+                      int32_t** ptr_out, int32_t** list_out) {
+    cudaStream_t s = h->stream;
+    uint32_t* k2 = nullptr;
+    int32_t* v2 = nullptr;
+    PLATO_CUDA(h, cudaMallocAsync(&k2, sizeof(uint32_t) * count, s));
+    PLATO_CUDA(h, cudaMalloc(&v2, sizeof(int32_t) * count));
+    PLATO_CUDA(h, cudaMalloc(ptr_out, sizeof(int32_t) * (nkeys + 1)));
+    size_t tb = 0, tb2 = 0;
+    PLATO_CUDA(h, cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, k2, vals, v2, count, 0, 32, s));
+    PLATO_CUDA(h, cub::DeviceScan::ExclusiveSum(nullptr, tb2, hist, *ptr_out, nkeys + 1, s));
+    void* tmp = nullptr;
+    PLATO_CUDA(h, cudaMallocAsync(&tmp, tb > tb2 ? tb : tb2, s));
+    PLATO_CUDA(h, cub::DeviceRadixSort::SortPairs(tmp, tb, keys, k2, vals, v2, count, 0, 32, s));
+    PLATO_CUDA(h, cub::DeviceScan::ExclusiveSum(tmp, tb2, hist, *ptr_out, nkeys + 1, s));
+    PLATO_CUDA(h, cudaFreeAsync(tmp, s));
+    PLATO_CUDA(h, cudaFreeAsync(k2, s));
+    *list_out = v2;
+    return PLATO_OK;
+}
+
+// Mesh-level setup for the requested coarse grid (once per grid size).
+int coarse_setup_mesh(plato_problem* h) {
+    CoarseSpace& c = h->coarse;
+    const int* want = h->opts.coarse_cells;
+    if (c.ready && c.nc[0] == want[0] && c.nc[1] == want[1] && c.nc[2] == want[2]) return PLATO_OK;
+    coarse_release(h);
+    for (int d = 0; d < 3; ++d) {
+        if (want[d] < 1 || want[d] > 64) return plato_fail(h, PLATO_BAD_INPUT, "coarse_cells must be in [1, 64]");
+        c.nc[d] = want[d];
+        c.x0[d] = h->bbox_min[d];
+        c.h[d] = (h->bbox_max[d] - h->bbox_min[d]) / want[d];
+        if (!(c.h[d] > 0.0)) return plato_fail(h, PLATO_BAD_INPUT, "degenerate mesh bounding box");
+    }
+    c.ncells = c.nc[0] * c.nc[1] * c.nc[2];
+    c.nnodes = (c.nc[0] + 1) * (c.nc[1] + 1) * (c.nc[2] + 1);
+    c.ndof = 3 * c.nnodes;
+    if (c.ndof > 6144) return plato_fail(h, PLATO_BAD_INPUT, "coarse grid too large for the dense coarse solve");
+    cudaStream_t s = h->stream;
+    const CoarseView cv = coarse_view(h);
+    const int T = 256;
+    uint32_t* keys = nullptr;
+    int32_t *vals = nullptr, *hist = nullptr, *bad = nullptr;
+    const int64_t mx = h->C > h->N ? h->C : h->N;
+    PLATO_CUDA(h, cudaMallocAsync(&keys, sizeof(uint32_t) * mx, s));
+    PLATO_CUDA(h, cudaMallocAsync(&vals, sizeof(int32_t) * mx, s));
+    PLATO_CUDA(h, cudaMallocAsync(&hist, sizeof(int32_t) * (c.ncells + 1), s));
+    PLATO_CUDA(h, cudaMallocAsync(&bad, sizeof(int32_t), s));
+    // nodes by cell
+    PLATO_CUDA(h, cudaMemsetAsync(hist, 0, sizeof(int32_t) * (c.ncells + 1), s));
+    k_node_keys<<<grid_for(h->N, T), T, 0, s>>>(h->N, h->coords, cv, keys, vals, hist);
+    PLATO_LAUNCH_CHECK(h);
+    int rc = csr_by_key(h, h->N, keys, vals, hist, c.ncells, &c.node_ptr, &c.node_list);
+    if (rc) return rc;
+    // elements by cell (+ the every-element-in-one-cell check)
+    PLATO_CUDA(h, cudaMemsetAsync(hist, 0, sizeof(int32_t) * (c.ncells + 1), s));
+    PLATO_CUDA(h, cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
+    k_elem_keys<<<grid_for(h->C, T), T, 0, s>>>(h->C, h->conn, h->coords, cv, keys, vals, hist, bad);
+    PLATO_LAUNCH_CHECK(h);
+    rc = csr_by_key(h, h->C, keys, vals, hist, c.ncells, &c.elem_ptr, &c.elem_list);
+    if (rc) return rc;
+    int32_t bad_h = 0;
+    PLATO_CUDA(h, cudaMemcpyAsync(&bad_h, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA(h, cudaStreamSynchronize(s));
+    PLATO_CUDA(h, cudaFreeAsync(keys, s));
+    PLATO_CUDA(h, cudaFreeAsync(vals, s));
+    PLATO_CUDA(h, cudaFreeAsync(hist, s));
+    PLATO_CUDA(h, cudaFreeAsync(bad, s));
+    if (bad_h)
+        return plato_fail(h, PLATO_BAD_INPUT,
+                          "coarse grid does not align with the mesh: an element straddles two coarse cells");
+    const size_t nn = size_t(c.ndof) * c.ndof;
+    PLATO_CUDA(h, cudaMalloc(&c.E, sizeof(double) * nn));
+    PLATO_CUDA(h, cudaMalloc(&c.Einv, sizeof(double) * nn));
+    PLATO_CUDA(h, cudaMalloc(&c.rc, sizeof(double) * c.ndof));
+    PLATO_CUDA(h, cudaMalloc(&c.yc, sizeof(double) * c.ndof));
+    PLATO_CUDA(h, cudaMalloc(&c.flag, sizeof(int32_t)));
+    c.ready = 1;
+    return PLATO_OK;
+}
+
+void coarse_release(plato_problem* h) {
+    CoarseSpace& c = h->coarse;
+    for (int32_t** p : {&c.node_ptr, &c.node_list, &c.elem_ptr, &c.elem_list, &c.flag})
+        if (*p) { cudaFree(*p); *p = nullptr; }
+    for (double** p : {&c.E, &c.Einv, &c.rc, &c.yc})
+        if (*p) { cudaFree(*p); *p = nullptr; }
+    c.ready = 0;
+}
+
+// Per-solve setup: Galerkin operator of control z, Cholesky, explicit inverse.
+int coarse_setup_operator(plato_problem* h, const double* z) {
+    CoarseSpace& c = h->coarse;
+    cudaStream_t s = h->stream;
+    const int n = c.ndof;
+    const size_t nn = size_t(n) * n;
+    PLATO_CUDA(h, cudaMemsetAsync(c.E, 0, sizeof(double) * nn, s));
+    k_galerkin<<<grid_for(c.ncells, 1, 148 * 8), 256, 0, s>>>(coarse_view(h), c.elem_ptr, c.elem_list, h->conn,
+                                                               h->coords, z, h->material, h->bc_mask, n, c.E);
+    PLATO_LAUNCH_CHECK(h);
+    k_regularize<<<grid_for(n, 256), 256, 0, s>>>(n, c.E);
+    PLATO_LAUNCH_CHECK(h);
+    PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
+    const int nblk = (n + kTile - 1) / kTile;
+    const dim3 tb(kTile, kTile);
+    for (int kb = 0; kb < nblk; ++kb) {
+        k_chol_diag<<<1, tb, 0, s>>>(n, c.E, kb, c.flag);
+        const int rem = nblk - kb - 1;
+        if (rem > 0) {
+            k_chol_panel<<<rem, tb, 0, s>>>(n, c.E, kb);
+            k_chol_update<<<rem * (rem + 1) / 2, tb, 0, s>>>(n, c.E, kb, nblk);
+        }
+    }
+    h->launches += 3 * nblk;
+    PLATO_LAUNCH_CHECK(h);
+    // X = L^-1 into the rc-independent scratch (Einv used as X first, then overwritten)
+    double* X = nullptr;
+    PLATO_CUDA(h, cudaMallocAsync(&X, sizeof(double) * nn, s));
+    k_tri_inverse<<<nblk, tb, 0, s>>>(n, c.E, X, nblk);
+    PLATO_LAUNCH_CHECK(h);
+    k_gram<<<dim3(nblk, nblk), tb, 0, s>>>(n, X, c.Einv, nblk);
+    PLATO_LAUNCH_CHECK(h);
+    PLATO_CUDA(h, cudaFreeAsync(X, s));
+    int32_t bad = 0;
+    PLATO_CUDA(h, cudaMemcpyAsync(&bad, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA(h, cudaStreamSynchronize(s));
+    if (bad) return plato_fail(h, PLATO_NONFINITE, "coarse operator is not positive definite");
+    return PLATO_OK;
+}
+
+// y (FP32) = / += Z E^-1 Z^T v (v FP32); kernels return at once after convergence.
+int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S) {
+    CoarseSpace& c = h->coarse;
+    cudaStream_t s = h->stream;
+    const CoarseView cv = coarse_view(h);
+    k_restrict<<<grid_for(c.nnodes, 1, 148 * 8), 256, 0, s>>>(cv, c.node_ptr, c.node_list, h->coords, h->bc_mask, v,
+                                                               c.rc, S);
+    k_coarse_gemv<<<grid_for(int64_t(c.ndof) * 32, 256, 148 * 8), 256, 0, s>>>(c.ndof, c.Einv, c.rc, c.yc, S);
+    k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, y, accumulate, S);
+    h->launches += 2;
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+}  // namespace plato

@@ -203,6 +203,53 @@ k_cheb_vec(int64_t n, const uint8_t* __restrict__ mask, const float* __restrict_
     }
 }
 
+// res -= A x on a SELL copy (FP32 vectors).
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_res_sub_sell(SellView A, const void* __restrict__ vals, const float* __restrict__ x, float* __restrict__ res,
+               const PcgScalars* S) {
+    if (S->done) return;
+    const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < padded; r += (int64_t)gridDim.x * blockDim.x) {
+        float w0, w1, w2;
+        if (KIND == INNER_SELL16)
+            sell_row_bf16(A, static_cast<const __nv_bfloat16*>(vals), x, r, w0, w1, w2);
+        else if (KIND == INNER_SELL32)
+            sell_row<float>(A, static_cast<const float*>(vals), x, r, w0, w1, w2);
+        else {
+            double a0, a1, a2;
+            sell_row<double>(A, static_cast<const double*>(vals), x, r, a0, a1, a2);
+            w0 = float(a0); w1 = float(a1); w2 = float(a2);
+        }
+        if (r < A.num_rows) {
+            res[3 * r] -= w0;
+            res[3 * r + 1] -= w1;
+            res[3 * r + 2] -= w2;
+        }
+    }
+}
+
+// res -= P A P x + (I - P) x after a matrix-free apply into w.
+__global__ void __launch_bounds__(kThreads)
+k_res_sub_vec(int64_t n, const uint8_t* __restrict__ mask, const float* __restrict__ x, const float* __restrict__ w,
+              float* __restrict__ res, const PcgScalars* S) {
+    if (S->done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        res[i] -= mask[i] ? x[i] : w[i];
+}
+
+// First Chebyshev step of a sweep that adds to y: d = c0 Dinv res, y += d.
+__global__ void __launch_bounds__(kThreads)
+k_cheb_first(int64_t n, float c0, const float* __restrict__ dinv32, const float* __restrict__ res,
+             float* __restrict__ d, float* __restrict__ y, const PcgScalars* S) {
+    if (S->done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float di = c0 * dinv32[i] * res[i];
+        d[i] = di;
+        y[i] += di;
+    }
+}
+
 // z = y (widened), z.q -> beta = -(z.q)/(p.q); then p = z + beta p and p.r in k_fcg_direction.
 __global__ void __launch_bounds__(kThreads)
 k_fcg_zq(int64_t n, const float* __restrict__ y, double* __restrict__ z, const double* __restrict__ q,
@@ -464,6 +511,17 @@ int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
     return launch_crs_to_sell(h, crs, h->sell64, o32, o16, h->v_dinv, h->f_dinv);
 }
 
+// Two-level preconditioner data for control z (mesh buckets once, Galerkin operator per solve).
+int prepare_coarse(plato_problem* h, const double* z) {
+    if (h->opts.coarse_cells[0] <= 0 || !z) return PLATO_OK;
+    int rc = coarse_setup_mesh(h);
+    if (rc) return rc;
+    rc = coarse_setup_operator(h, z);
+    if (rc) return rc;
+    h->coarse.active = 1;
+    return PLATO_OK;
+}
+
 // Flexible CG with the Chebyshev preconditioner: A x = b, x holds the initial guess.
 int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
     const int64_t n = 3 * (int64_t)h->N;
@@ -491,8 +549,25 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         }
         return launch_sell_spmv(h, h->sell64, in, out);
     };
-    auto precondition = [&](float c0_unused) -> int {
-        (void)c0_unused;
+    const bool coarse = h->coarse.active != 0;
+    // res -= A_inner xin (FP32)
+    auto inner_apply_sub = [&](const float* xin) -> int {
+        if (mf) {
+            int r2 = launch_ebe_apply32(h, xin, h->f_w, h->scal);
+            if (r2) return r2;
+            k_res_sub_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, xin, h->f_w, h->f_res, h->scal);
+        } else if (kind == INNER_SELL16) {
+            k_res_sub_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, xin, h->f_res, h->scal);
+        } else if (kind == INNER_SELL32) {
+            k_res_sub_sell<INNER_SELL32><<<SB, kThreads, 0, s>>>(V, h->sell32, xin, h->f_res, h->scal);
+        } else {
+            k_res_sub_sell<INNER_SELL64><<<SB, kThreads, 0, s>>>(V, h->sell64, xin, h->f_res, h->scal);
+        }
+        PLATO_LAUNCH_CHECK(h);
+        return PLATO_OK;
+    };
+    float* dlast = h->f_d0;
+    auto chebyshev_steps = [&]() -> int {
         float* dcur = h->f_d0;
         float* dnext = h->f_d1;
         for (int k = 1; k < degree; ++k) {
@@ -514,7 +589,26 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             PLATO_LAUNCH_CHECK(h);
             std::swap(dcur, dnext);
         }
+        dlast = dcur;
         return PLATO_OK;
+    };
+    // M(r) with r in f_res (FP32) and, from the update kernel, d0 = c0 Dinv r, y = d0 already
+    // written.  Without a coarse space M = the Chebyshev sweep S.  With it, the balancing
+    // two-level form M = C + (I - CA) S (I - AC), C = Z E^-1 Z^T:
+    //   y = C r; res = r - A y; y += S(res); res -= A s; y += C res.
+    auto precondition = [&](float c0) -> int {
+        if (!coarse) return chebyshev_steps();
+        int r2 = coarse_apply(h, h->f_res, h->f_y, 0, h->scal);
+        if (r2) return r2;
+        r2 = inner_apply_sub(h->f_y);
+        if (r2) return r2;
+        k_cheb_first<<<VB, kThreads, 0, s>>>(n, c0, h->f_dinv, h->f_res, h->f_d0, h->f_y, h->scal);
+        PLATO_LAUNCH_CHECK(h);
+        r2 = chebyshev_steps();
+        if (r2) return r2;
+        r2 = inner_apply_sub(dlast);
+        if (r2) return r2;
+        return coarse_apply(h, h->f_res, h->f_y, 1, h->scal);
     };
 
     PcgScalars init{};

@@ -61,6 +61,25 @@ struct PcgScalars {
     uint32_t ticket; // last-block-done counter of the fused reductions
 };
 
+// Two-level preconditioner state (coarse.cu).
+struct CoarseSpace {
+    int      nc[3] = {0, 0, 0};   // coarse cells per axis
+    int      ready = 0;           // mesh-level setup done for nc
+    int      active = 0;          // operator built for the current solve
+    double   x0[3] = {0, 0, 0};   // grid origin (mesh bounding-box minimum)
+    double   h[3] = {0, 0, 0};    // coarse cell size
+    int32_t  ncells = 0, nnodes = 0, ndof = 0;
+    int32_t* node_ptr = nullptr;  // fine nodes bucketed by coarse cell (CSR)
+    int32_t* node_list = nullptr;
+    int32_t* elem_ptr = nullptr;  // elements bucketed by coarse cell (CSR)
+    int32_t* elem_list = nullptr;
+    double*  E = nullptr;         // Galerkin operator, then its Cholesky factor (ndof^2)
+    double*  Einv = nullptr;      // explicit inverse (ndof^2)
+    double*  rc = nullptr;        // restricted residual
+    double*  yc = nullptr;        // coarse correction
+    int32_t* flag = nullptr;
+};
+
 struct plato_problem {
     int          device = 0;
     cudaStream_t stream = nullptr;
@@ -88,6 +107,9 @@ struct plato_problem {
     double*  bc_values = nullptr;
     uint8_t* bc_mask = nullptr;    // [3N] 1 where a dof is constrained
     int      bc_nonzero = 0;       // some essential BC value is nonzero
+    double   bbox_min[3] = {0, 0, 0};
+    double   bbox_max[3] = {0, 0, 0};
+    CoarseSpace coarse{};
     // assembled operator (allocated on first use)
     double* K = nullptr;           // 9*nblocks
     double* KT = nullptr;          // scratch for transposed / gradient_z matrices
@@ -154,6 +176,12 @@ struct plato_problem {
 // ---------------------------------------------------------------------------------------
 // error plumbing
 int plato_fail(plato_problem* h, int status, const std::string& msg);
+namespace plato {
+int coarse_setup_mesh(plato_problem* h);
+int coarse_setup_operator(plato_problem* h, const double* z);
+int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S);
+void coarse_release(plato_problem* h);
+}  // namespace plato
 int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const char* file, int line);
 
 #define PLATO_CUDA(h, expr)                                                          \

@@ -32,10 +32,12 @@ class SolverOptions:
     self_adjoint: bool = True
     chebyshev_ratio: float = 30.0
     chebyshev_degree: int = 0
+    coarse_cells: tuple = (0, 0, 0)
 
     def to_c(self) -> capi.SolverOpts:
         return capi.SolverOpts(self.tolerance, self.max_iterations, self.operator_kind, self.precision,
-                               int(self.self_adjoint), self.chebyshev_ratio, self.chebyshev_degree)
+                               int(self.self_adjoint), self.chebyshev_ratio, self.chebyshev_degree,
+                               (C.c_int32 * 3)(*self.coarse_cells))
 
 
 @dataclass

@@ -24,6 +24,13 @@ CONFIGS = {
                                     chebyshev_degree=1),
     "mf_fp32_cheb8": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE, precision=capi.PRECISION_MIXED_FP32,
                                    chebyshev_degree=8),
+    "fp32_cheb4_coarse": SolverOptions(precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4,
+                                       coarse_cells=(5, 5, 5)),
+    "bf16_cheb4_coarse": SolverOptions(precision=capi.PRECISION_MIXED_BF16, chebyshev_degree=4,
+                                       coarse_cells=(10, 5, 5)),
+    "mf_fp32_cheb4_coarse": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE,
+                                          precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4,
+                                          coarse_cells=(4, 2, 2)),
 }
 
 
@@ -98,6 +105,29 @@ def test_chebyshev_reduces_outer_iterations(setup):
     finally:
         prob.set_solver(SolverOptions(tolerance=1e-10))
     assert poly["iterations"] * 3 < plain["iterations"], (poly, plain)
+
+
+def test_coarse_space_cuts_iterations(setup):
+    spec, z, prob, *_ = setup
+    zd = prob.to_dev(z)
+    prob.set_solver(SolverOptions(tolerance=1e-10, precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4))
+    try:
+        _, one = prob.solution(zd)
+        prob.set_solver(SolverOptions(tolerance=1e-10, precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4,
+                                      coarse_cells=(10, 5, 5)))
+        _, two = prob.solution(zd)
+    finally:
+        prob.set_solver(SolverOptions(tolerance=1e-10))
+    assert two["converged"] == 1 and two["iterations"] * 2 < one["iterations"], (one, two)
+
+
+def test_coarse_grid_must_align():
+    spec = cantilever(6, 3, 3, SolverOptions(tolerance=1e-10, precision=capi.PRECISION_MIXED_FP32,
+                                             chebyshev_degree=4, coarse_cells=(4, 2, 2)))
+    prob = EllipticProblem(spec)
+    with pytest.raises(capi.PlatoError) as e:
+        prob.solution(prob.to_dev(np.full(spec.coords.shape[0], 0.5)))
+    assert e.value.status == capi.BAD_INPUT and "straddles" in str(e.value)
 
 
 def test_inhomogeneous_dirichlet_matrix_free_matches_assembled():

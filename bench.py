@@ -1,13 +1,21 @@
 """Benchmark: solve+adjoint throughput of SIMP linear-tet elastostatics on B200.
 
-One step = one optimisation unit of the reference's Elliptic::Problem: assemble K(z),
-apply the Dirichlet elimination, Jacobi-PCG to the FP64 tolerance, compliance value and
-dC/dz (self-adjoint).  Workload (default): 160 x 80 x 80 hexes x 6 tets on [0,2]x[0,1]x[0,1]
+One step = one optimisation unit of the reference's Elliptic::Problem: assemble K(z) and
+eliminate the clamped dofs, solve K u = F to the FP64 tolerance, compliance value and dC/dz
+(self-adjoint).  Workload (default): 160 x 80 x 80 hexes x 6 tets on [0,2]x[0,1]x[0,1]
 (6,144,000 tets, 3,168,963 dofs), clamped at x = 0, traction (0,-1,0) on x = 2, E = 1,
 nu = 0.3, SIMP p = 3, rho_min = 1e-9, nodal densities i.i.d. U[0.01, 1] (SplitMix64 seed
 0x5EED0002).  Synthetic data; every input and the 1.12 GB block matrix exceed the 126 MB L2.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Methods (--method):
+  two-level  (default) FP64 flexible CG; preconditioner = FP32 Chebyshev-Jacobi smoothing on
+             an FP32 copy of the matrix + Galerkin coarse correction on a 10x5x5 box grid.
+  plain      the reference's algorithm: FP64 Jacobi-PCG on the assembled block matrix.
+Both stop on the same FP64 residual test (1e-10); the line also carries the plain method's
+throughput measured in the same run, and the accuracy of the timed solution against the
+CPU oracle's own FP64 solve.
+
+    python bench.py [--gpus N --steps K --warmup W] [--method plain] [--impl reference]
 
 Prints one JSON line (rank 0).  Multi-GPU runs are independent replicas (weak scaling).
 """
@@ -30,9 +38,20 @@ sys.path.insert(0, str(ROOT))
 METRIC = "solve+adjoint/s at 3.2M DoF, 1e-8 rel err: learned-MP PCG vs plain FP64 PCG"
 UNIT = "solve+adjoint/s"
 SIZES = {"large": (160, 80, 80), "medium": (80, 40, 40), "small": (20, 10, 10)}
-# Jacobi-PCG iterations of the plain FP64 method on the large workload at tol 1e-10 (from the
-# B200 run of this bench; the GPU arm re-measures and reports its own count).
-FP64_ITERATIONS = {"large": 3634, "medium": 1834, "small": None}
+COARSE = (10, 5, 5)  # coarse box grid of the two-level method (aligned with every size above)
+# Jacobi-PCG iterations of the plain FP64 method at tol 1e-10 (measured by this bench on B200
+# and by the CPU oracle's own solve; the reference arm extrapolates its sample with them).
+FP64_ITERATIONS = {"large": 3632, "medium": 1833, "small": None}
+
+
+METHOD_TEXT = {
+    "two-level": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP32 SELL copy + "
+                  "FP64 Galerkin coarse correction on a 10x5x5 trilinear box grid"),
+    "plain": "plain FP64 Jacobi-PCG on the assembled 3x3 block matrix (the reference's algorithm)",
+    "chebyshev": "FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP32 SELL copy",
+    "bf16": "FP64 flexible CG; preconditioner: Chebyshev-Jacobi (16 steps) on a BF16-stored SELL copy",
+    "matrix-free": "FP64 flexible CG on the matrix-free operator; FP32 matrix-free Chebyshev-Jacobi (16 steps)",
+}
 
 
 def parse():
@@ -41,11 +60,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--method", default="two-level", choices=list(METHOD_TEXT))
     ap.add_argument("--size", default="large", choices=list(SIZES))
     ap.add_argument("--tol", type=float, default=1e-10)
-    ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations in the CPU sample")
+    ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations in the reference-arm sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
+
+
+def solver_options(method: str, tol: float):
+    from platoanalyze_b200.workloads import method_options
+
+    return method_options(method, tol, COARSE)
 
 
 def peaks():
@@ -108,36 +134,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-# CPU arm: the oracle (FP64 restatement of the reference path) on a bounded sample
-
-def cpu_sample(spec, z, n_iters_full, cpu_iters):
-    """Times assembly + constraints + `cpu_iters` PCG iterations + compliance + dC/dz on the
-    full mesh with the oracle, and extrapolates the PCG part to `n_iters_full` iterations."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    from oracle import Oracle
-
-    orc = Oracle.from_spec(spec)
-    orc.graph()  # pattern build is one-off setup (not part of a step)
-    t0 = time.perf_counter()
-    K = orc.vf_gradient_u(np.zeros(3 * orc.N), z)
-    rhs = np.zeros(3 * orc.N)
-    R = orc.vf_value(np.zeros(3 * orc.N), z)
-    rhs[:] = -R
-    orc.apply_constraints(K, rhs, 1.0)
-    t1 = time.perf_counter()
-    x, st = orc.pcg(K, rhs, tol=1e-300, max_it=cpu_iters)
-    t2 = time.perf_counter()
-    orc.sf_value(x, z)
-    orc.criterion_gradient(z, x, self_adjoint=True)
-    t3 = time.perf_counter()
-    per_iter = (t2 - t1) / max(1, st["iterations"])
-    unit_s = (t1 - t0) + per_iter * n_iters_full + (t3 - t2)
-    return {"value": 1.0 / unit_s, "unit": UNIT, "cores": Oracle.num_threads(), "kind": "port",
-            "sample": (f"oracle on the full mesh: assembly+constraints {t1 - t0:.2f}s, {st['iterations']} PCG "
-                       f"iterations at {per_iter * 1e3:.1f} ms each extrapolated to {n_iters_full}, "
-                       f"compliance+dC/dz {t3 - t2:.2f}s"),
-            "seconds_per_unit": unit_s}
-
+# CPU side: the oracle (FP64 restatement of the reference path, plain Jacobi-PCG)
 
 def oracle_reference(spec, z, tol):
     """Full FP64 solve + compliance + dC/dz of the problem with the CPU oracle, timed."""
@@ -162,8 +159,45 @@ def oracle_reference(spec, z, tol):
             "t_pcg": t2 - t1, "t_criterion": t3 - t2, "cores": Oracle.num_threads()}
 
 
+def cpu_sample(spec, z, n_iters_full, cpu_iters):
+    """Assembly + constraints + `cpu_iters` PCG iterations + compliance + dC/dz on the full
+    mesh with the oracle; the PCG part is extrapolated to `n_iters_full` iterations."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import Oracle
+
+    orc = Oracle.from_spec(spec)
+    orc.graph()
+    t0 = time.perf_counter()
+    K = orc.vf_gradient_u(np.zeros(3 * orc.N), z)
+    rhs = -orc.vf_value(np.zeros(3 * orc.N), z)
+    orc.apply_constraints(K, rhs, 1.0)
+    t1 = time.perf_counter()
+    x, st = orc.pcg(K, rhs, tol=1e-300, max_it=cpu_iters)
+    t2 = time.perf_counter()
+    orc.sf_value(x, z)
+    orc.criterion_gradient(z, x, self_adjoint=True)
+    t3 = time.perf_counter()
+    per_iter = (t2 - t1) / max(1, st["iterations"])
+    unit_s = (t1 - t0) + per_iter * n_iters_full + (t3 - t2)
+    return {"value": 1.0 / unit_s, "unit": UNIT, "cores": Oracle.num_threads(), "kind": "port",
+            "sample": (f"oracle on the full mesh: assembly+constraints {t1 - t0:.2f}s, {st['iterations']} PCG "
+                       f"iterations at {per_iter * 1e3:.1f} ms each extrapolated to {n_iters_full}, "
+                       f"compliance+dC/dz {t3 - t2:.2f}s")}
+
+
+def workload_config(args, spec, method):
+    nx, ny, nz = SIZES[args.size]
+    return {"workload": f"SIMP cantilever {nx}x{ny}x{nz} hexes x 6 tets on [0,2]x[0,1]x[0,1]",
+            "tets": int(spec.connectivity.shape[0]), "dofs": int(3 * spec.coords.shape[0]),
+            "density": "nodal i.i.d. U[0.01,1], SplitMix64 seed 0x5EED0002", "method": METHOD_TEXT[method],
+            "tolerance": args.tol, "adjoint": "self-adjoint (lambda = -u)",
+            "l2": "inputs larger than L2 (block matrix 1.12 GB, vectors 25 MB each)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
 def run_reference(args):
-    """--impl reference: the oracle port of the reference path on the host cores."""
+    """--impl reference: the oracle port of the reference path (plain FP64 Jacobi-PCG) on the
+    host cores, each step a bounded sample extrapolated to the full iteration count."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -184,21 +218,11 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": workload_config(args, spec),
+            "config": workload_config(args, spec, "plain"),
             "cpu_baseline": {k: vals[-1][k] for k in ("cores", "kind", "sample")} | {"value": v, "unit": UNIT},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
-
-
-def workload_config(args, spec, method="plain FP64 Jacobi-PCG, assembled 3x3 block CRS"):
-    nx, ny, nz = SIZES[args.size]
-    return {"workload": f"SIMP cantilever {nx}x{ny}x{nz} hexes x 6 tets on [0,2]x[0,1]x[0,1]",
-            "tets": int(spec.connectivity.shape[0]), "dofs": int(3 * spec.coords.shape[0]),
-            "density": "nodal i.i.d. U[0.01,1], SplitMix64 seed 0x5EED0002", "method": method,
-            "tolerance": args.tol, "adjoint": "self-adjoint (lambda = -u)",
-            "l2": "inputs larger than L2 (block matrix 1.12 GB, vectors 25 MB x 7)",
-            "parallelism": f"replicas x{args.gpus}"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -220,10 +244,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    from platoanalyze_b200.problem import EllipticProblem, SolverOptions
+    from platoanalyze_b200.problem import EllipticProblem
     from platoanalyze_b200.workloads import SEED_LARGE, cantilever, splitmix_uniform
 
-    spec = cantilever(*SIZES[args.size], SolverOptions(tolerance=args.tol, max_iterations=200000))
+    spec = cantilever(*SIZES[args.size], solver_options(args.method, args.tol))
     z = splitmix_uniform(spec.coords.shape[0], SEED_LARGE)
     prob = EllipticProblem(spec)
     zd = prob.to_dev(z)
@@ -235,75 +259,101 @@ def main():
         g, _ = prob.criterion_gradient(zd, u)
         return u, f, g, st
 
+    def timed_steps(k):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out, stats = None, []
+        for _ in range(k):
+            out = step()
+            stats.append(out[3])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), out, stats
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
 
     prob.reset_instrumentation()
     prob.set_timing(True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        iters = []
-        for _ in range(args.steps):
-            u, f, g, st = step()
-            iters.append(st["iterations"])
-        e1.record(stream)
-        torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+        ms_max, (u, f, g, _), stats = timed_steps(args.steps)
     prob.set_timing(False)
-    ms = e0.elapsed_time(e1)
     inst = prob.instrumentation()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
     value = world * args.steps / (ms_max / 1e3)
 
-    # end to end through the C ABI with host buffers (H2D z, D2H u, compliance, dC/dz)
-    z_host = np.ascontiguousarray(z)
-    u_host = np.empty(prob.num_dofs)
-    g_host = np.empty(prob.num_nodes)
+    # end to end through the C ABI with host buffers (H2D z, D2H u and dC/dz, compliance)
     u_pin = torch.empty(prob.num_dofs, dtype=torch.float64).pin_memory().numpy()
     g_pin = torch.empty(prob.num_nodes, dtype=torch.float64).pin_memory().numpy()
-    z_pin = torch.from_numpy(z_host).pin_memory().numpy()
+    z_pin = torch.from_numpy(np.ascontiguousarray(z)).pin_memory().numpy()
     prob.solve_and_gradient_host(z_pin, u_out=u_pin, g_out=g_pin)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream)
     for _ in range(args.steps):
         prob.solve_and_gradient_host(z_pin, u_out=u_pin, g_out=g_pin)
     e1.record(stream)
     torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    ms_e2e = max(e0.elapsed_time(e1), wall * 1e3)
+    ms_e2e = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
     t = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps / (float(t.item()) / 1e3)
-    del u_host, g_host
 
-    # roofline of the dominant kernel (FP64 SELL SpMV inside PCG).  Algorithmic bytes: the
-    # constrained block matrix once (9 doubles + 1 column index per block, row pointers),
-    # x gathered once and y written once.
+    # roofline: the FP64 operator apply of the Krylov loop (SELL SpMV) and, for the two-level
+    # method, the FP32 Chebyshev step that dominates its step.  Algorithmic bytes per launch:
+    # the matrix once (entries + column index per block, row pointers) and each vector stream once.
     N, B = prob.num_nodes, prob.num_blocks
-    spmv_bytes = 9 * B * 8 + B * 4 + (N + 1) * 4 + 3 * N * 8 * 2
-    avg_ms = inst["op_ms_total"] / max(1, inst["op_timed"])
     peak, peak_kind = peaks()
-    achieved = spmv_bytes / (avg_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_sell_spmv (FP64 SELL-32 block SpMV + p.Ap)", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes": spmv_bytes, "avg_launch_ms": avg_ms,
-                "launches_timed": inst["op_timed"]}
+    spmv_bytes = 9 * B * 8 + B * 4 + (N + 1) * 4 + 3 * N * 8 * 2
+    spmv_ms = inst["op_ms_total"] / max(1, inst["op_timed"])
+    rl_spmv = {"bound": "hbm", "kernel": "k_sell_spmv / k_fcg_sell_apply (FP64 SELL-32 SpMV + p.Ap)",
+               "achieved": spmv_bytes / (spmv_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+               "frac": spmv_bytes / (spmv_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+               "algorithmic_bytes": spmv_bytes, "avg_launch_ms": spmv_ms, "launches_timed": inst["op_timed"]}
+    roofline, roofline_other = rl_spmv, None
+    if inst["inner_timed"]:
+        cheb_bytes = 9 * B * 4 + B * 4 + (N + 1) * 4 + 7 * 3 * N * 4
+        cheb_ms = inst["inner_ms_total"] / inst["inner_timed"]
+        rl_cheb = {"bound": "hbm", "kernel": "k_cheb_sell<FP32> (FP32 SELL SpMV fused with one Chebyshev step)",
+                   "achieved": cheb_bytes / (cheb_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                   "frac": cheb_bytes / (cheb_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+                   "algorithmic_bytes": cheb_bytes, "avg_launch_ms": cheb_ms, "launches_timed": inst["inner_timed"]}
+        roofline, roofline_other = rl_cheb, rl_spmv
 
-    # accuracy against the CPU oracle's own FP64 solve of the full problem (untimed), and the
-    # CPU baseline from the same oracle run
+    rl_asm = None
+    if inst["assembly_timed"]:
+        # connectivity + coordinates + control in; block values + column indices + row map out
+        asm_bytes = 16 * prob.num_cells + 24 * N + 8 * N + 72 * B + 4 * B + 4 * (N + 1)
+        asm_ms = inst["assembly_ms_total"] / inst["assembly_timed"]
+        rl_asm = {"bound": "hbm", "kernel": "k_assemble_jacobian (K(z) block-CRS assembly, warp per block row)",
+                  "achieved": asm_bytes / (asm_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                  "frac": asm_bytes / (asm_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+                  "algorithmic_bytes": asm_bytes, "avg_launch_ms": asm_ms, "launches_timed": inst["assembly_timed"]}
+
+    # the plain FP64 GPU method on the same problem, same run (comparison only)
+    plain = None
+    if args.method != "plain":
+        prob.set_solver(solver_options("plain", args.tol))
+        step()
+        ms_plain, _, pstats = timed_steps(2)
+        plain = {"value": world * 2 / (ms_plain / 1e3), "ms_per_step": ms_plain / 2,
+                 "pcg_iterations": [s["iterations"] for s in pstats]}
+        prob.set_solver(solver_options(args.method, args.tol))
+
+    # accuracy against the CPU oracle's own FP64 solve of the full problem (untimed); the same
+    # oracle run is the CPU baseline (all host threads)
     cpu, accuracy = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref = oracle_reference(spec, z, args.tol)
@@ -315,16 +365,22 @@ def main():
                     "vs": f"CPU FP64 oracle solve of the same problem ({ref['iterations']} PCG iterations, "
                           f"relres {ref['relative_residual']:.2e})"}
         cpu = {"value": 1.0 / ref["seconds"], "unit": UNIT, "cores": ref["cores"], "kind": "port",
-               "sample": (f"full oracle solve+adjoint of the same workload on the host: assembly+constraints "
-                          f"{ref['t_assembly']:.2f}s, {ref['iterations']} PCG iterations {ref['t_pcg']:.2f}s, "
-                          f"compliance+dC/dz {ref['t_criterion']:.2f}s")}
+               "sample": (f"full oracle solve+adjoint of the same workload on the host (plain FP64 Jacobi-PCG): "
+                          f"assembly+constraints {ref['t_assembly']:.2f}s, {ref['iterations']} PCG iterations "
+                          f"{ref['t_pcg']:.2f}s, compliance+dC/dz {ref['t_criterion']:.2f}s")}
 
+    cfg = workload_config(args, spec, args.method) | {
+        "krylov_iterations": [s["iterations"] for s in stats],
+        "preconditioner_operator_applies": [s["refinements"] for s in stats],
+        "relative_residual": [s["relative_residual"] for s in stats]}
+    if plain:
+        cfg["plain_fp64_gpu"] = plain
+        cfg["speedup_vs_plain_fp64_gpu"] = value / plain["value"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args, spec) | {"pcg_iterations": iters},
-            "accuracy": accuracy,
-            "roofline": roofline, "cpu_baseline": cpu,
+            "scaling": "weak", "vs_baseline": None, "dtype": {"plain": "f64", "bf16": "f64+bf16"}.get(args.method, "f64+f32"),
+            "data": "synthetic", "config": cfg, "accuracy": accuracy, "roofline": roofline,
+            "roofline_fp64_spmv": roofline_other, "roofline_assembly": rl_asm, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N,
                     "d2h_bytes_per_step": 8 * (3 * N + N) + 8},
             "gpu_launches": inst["launches"], "clocks": clk.summary()}

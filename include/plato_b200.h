@@ -144,6 +144,11 @@ int plato_set_timing(plato_problem* h, int32_t enable);
 int plato_get_instrumentation(const plato_problem* h, int64_t* launches, double* op_ms_total,
                               int64_t* op_timed);
 int plato_reset_instrumentation(plato_problem* h);
+/* Sampled CUDA-event time of one kernel class inside the solvers: kind 0 = the FP64 operator
+ * apply of the Krylov loop, kind 1 = the first Chebyshev step of the low-precision
+ * preconditioner (one step = one preconditioner-operator apply fused with its update),
+ * kind 2 = the Jacobian assembly of each assembled solve. */
+int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
 
 /* ---- block pattern ---------------------------------------------------------------------
  * CreateBlockMatrix (src/ImplicitFunctors.hpp:932-1005) over the node-node graph

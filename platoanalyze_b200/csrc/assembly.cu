@@ -4,23 +4,23 @@
 // The reference assembles cell by cell with one FP64 atomic per entry and finds each entry
 // by a linear search of its row (assemble_jacobian_fad, src/Assembly.hpp:1374-1438;
 // BlockMatrixEntryOrdinal, src/ImplicitFunctors.hpp:730-766).  Here the assembly is
-// node-centric: one warp owns one block row, its lanes walk the row node's incident cells,
-// each lane computes the four 3x3 blocks K_ab of its cell in closed form
-// (w B_a^T C B_b), and the row is accumulated in shared memory and written once, coalesced.
-// No global atomics; every value is written exactly once.
+// node-centric: one warp owns one block row and writes it exactly once, coalesced, with no
+// global atomics.
+//
+// K(z) (k_assemble_jacobian): the lanes take the row node's incident cells, one cell each,
+// and compute its gradients and weight w = vol s(rho) once.  The isotropic block of a cell is
+//   K_ab = w (lambda g_a g_b^T + mu g_b g_a^T + mu (g_a . g_b) I),
+// so each block of the row is K = lambda M + mu M^T + mu tr(M) I with M = sum_cells w g_a g_b^T.
+// Lanes then switch roles: the contributions are bucketed by block slot with __match_any_sync
+// (no atomics), each lane owns one off-diagonal block and sums its M in registers, and the
+// diagonal block (every incident cell contributes) is a warp butterfly reduction.
 #include "plato_internal.cuh"
 
 namespace plato {
 namespace {
 
 constexpr int kWarpsPerBlock = 8;
-constexpr int kMaxRowBlocks = 64;  // rows with more blocks take the global-atomic path
-
-template <int BS>
-struct RowSmem {
-    int32_t cols[kMaxRowBlocks];
-    double  acc[kMaxRowBlocks * BS];
-};
+constexpr int kMaxRowBlocks = 64;  // (dR/dz)^T rows with more blocks take the global-atomic path
 
 __device__ __forceinline__ int find_slot(const int32_t* cols, int n, int32_t node) {
     // rows are sorted: binary search
@@ -32,13 +32,181 @@ __device__ __forceinline__ int find_slot(const int32_t* cols, int n, int32_t nod
     return lo;
 }
 
-// MODE 0: K(z) 3x3 blocks.  MODE 1: (dR/dz)^T 1x3 blocks: entry (a, (b,d)) =
-// sum over cells of dR_(b,d)/dz_a = vol s'(rho)/4 (B_b^T sigma0(u))_d.
-template <int MODE>
+// ---- K(z) -----------------------------------------------------------------------------------
+
+constexpr int kJacWarps = 4;
+constexpr int kFastCells = 32;   // rows with at most this many incident cells and blocks use the
+constexpr int kFastBlocks = 32;  // register path; larger rows accumulate with global atomics
+
+struct JacRowSmem {
+    int32_t cols[kFastBlocks];
+    int32_t count[kFastBlocks];                // contributions bucketed into each block slot
+    uint8_t rec[kFastCells][kFastBlocks];      // [k][slot] = lane * 4 + local node of the k-th one
+    double  wga[kFastCells][3];                // w g_a of each incident cell (a = the row node)
+    double  g[kFastCells][12];                 // the 4 gradients of each cell; reused for the output
+};
+static_assert(9 * kFastBlocks <= 12 * kFastCells, "output staging must fit in the gradient area");
+
+// Rows beyond the fast-path limits: every lane walks cells and adds its four blocks with
+// global FP64 atomics into the zeroed row (general meshes with high-valence nodes).
+__device__ __noinline__ void jacobian_row_atomic(const MeshView& m, const GraphView& g, const Material& mat,
+                                                 const double* __restrict__ z, double* __restrict__ entries,
+                                                 int64_t row, int lane) {
+    const int32_t rs = g.row_map[row], nbk = g.row_map[row + 1] - rs;
+    for (int64_t t = lane; t < (int64_t)nbk * 9; t += 32) entries[9 * (int64_t)rs + t] = 0.0;
+    __syncwarp();
+    for (int32_t k = g.n2c_ptr[row] + lane; k < g.n2c_ptr[row + 1]; k += 32) {
+        const int32_t packed = g.n2c[k];
+        const int32_t c = packed >> 2, la = packed & 3;
+        const int4 n = m.conn[c];
+        double x[4][3];
+        load_cell_coords(m.coords, n, x);
+        TetGeom<double> G;
+        tet_geometry(x, G);
+        const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+        const double w = G.vol * simp(mat, rho);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            double Kb[9];
+            stiffness_block(mat, G.g[la], G.g[b], w, Kb);
+            const int slot = find_slot(g.cols + rs, nbk, node_of(n, b));
+#pragma unroll
+            for (int q = 0; q < 9; ++q) atomicAdd(&entries[9 * ((int64_t)rs + slot) + q], Kb[q]);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kJacWarps * 32, 5)
+k_assemble_jacobian(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
+                    double* __restrict__ entries) {
+    __shared__ JacRowSmem sm[kJacWarps];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    JacRowSmem& S = sm[wib];
+    const double c01 = mat.c01, c33 = mat.c33;
+    const int64_t warps_total = (int64_t)gridDim.x * kJacWarps;
+    for (int64_t row = blockIdx.x * (int64_t)kJacWarps + wib; row < g.num_nodes; row += warps_total) {
+        const int32_t rs = g.row_map[row];
+        const int nbk = g.row_map[row + 1] - rs;
+        const int32_t ks = g.n2c_ptr[row];
+        const int ncell = g.n2c_ptr[row + 1] - ks;
+        if (nbk > kFastBlocks || ncell > kFastCells) {  // warp-uniform
+            jacobian_row_atomic(m, g, mat, z, entries, row, lane);
+            continue;
+        }
+        if (lane < nbk) {
+            S.cols[lane] = g.cols[rs + lane];
+            S.count[lane] = 0;
+        }
+        __syncwarp();
+
+        // 1. one incident cell per lane: gradients, weight, diagonal contribution w g_a g_a^T
+        const bool active = lane < ncell;
+        int4 n = make_int4(0, 0, 0, 0);
+        int la = -1;
+        double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz yz xz xy
+        if (active) {
+            const int32_t packed = g.n2c[ks + lane];
+            la = packed & 3;
+            n = m.conn[packed >> 2];
+            double x[4][3];
+            load_cell_coords(m.coords, n, x);
+            TetGeom<double> G;
+            tet_geometry(x, G);
+            const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+            const double w = G.vol * simp(mat, rho);
+            double ga[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) ga[i] = la == 0 ? G.g[0][i] : la == 1 ? G.g[1][i] : la == 2 ? G.g[2][i] : G.g[3][i];
+            const double a0 = w * ga[0], a1 = w * ga[1], a2 = w * ga[2];
+            S.wga[lane][0] = a0;
+            S.wga[lane][1] = a1;
+            S.wga[lane][2] = a2;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) S.g[lane][3 * b + i] = G.g[b][i];
+            d[0] = a0 * ga[0]; d[1] = a1 * ga[1]; d[2] = a2 * ga[2];
+            d[3] = a1 * ga[2]; d[4] = a0 * ga[2]; d[5] = a0 * ga[1];
+        }
+
+        // 2. bucket the off-diagonal contributions (cell, local node b) by block slot
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int key = (active && b != la) ? find_slot(S.cols, nbk, node_of(n, b)) : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const int rank = __popc(peers & below);
+            if (key >= 0) S.rec[S.count[key] + rank][key] = uint8_t(lane * 4 + b);
+            __syncwarp();
+            if (key >= 0 && rank == 0) S.count[key] += __popc(peers);
+            __syncwarp();
+        }
+
+        // 3. diagonal block: butterfly sum of the incident cells' w g_a g_a^T
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) d[q] += __shfl_xor_sync(0xffffffffu, d[q], off);
+
+        // 4. lane = block slot: M = sum w g_a g_b^T, K = lambda M + mu M^T + mu tr(M) I
+        const int dslot = g.diag[row] - rs;
+        double K[9];
+        if (lane < nbk) {
+            double M[9];
+            if (lane == dslot) {
+                M[0] = d[0]; M[4] = d[1]; M[8] = d[2];
+                M[5] = M[7] = d[3];
+                M[2] = M[6] = d[4];
+                M[1] = M[3] = d[5];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) M[q] = 0.0;
+                const int cnt = S.count[lane];
+                for (int r = 0; r < cnt; ++r) {
+                    const int code = S.rec[r][lane];
+                    const int c = code >> 2, b = code & 3;
+                    const double a[3] = {S.wga[c][0], S.wga[c][1], S.wga[c][2]};
+                    const double gb[3] = {S.g[c][3 * b], S.g[c][3 * b + 1], S.g[c][3 * b + 2]};
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) M[3 * i + j] = fma(a[i], gb[j], M[3 * i + j]);
+                }
+            }
+            const double tr = c33 * (M[0] + M[4] + M[8]);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) K[3 * i + j] = c01 * M[3 * i + j] + c33 * M[3 * j + i] + (i == j ? tr : 0.0);
+        }
+        __syncwarp();  // every read of S.g is done before it becomes the output stage
+        double* out = &S.g[0][0];
+        if (lane < nbk)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) out[9 * lane + q] = K[q];
+        __syncwarp();
+        double* dst = entries + 9 * (int64_t)rs;
+        for (int q = lane; q < 9 * nbk; q += 32) dst[q] = out[q];
+        __syncwarp();
+    }
+}
+
+// ---- (dR/dz)^T --------------------------------------------------------------------------------
+
+template <int BS>
+struct RowSmem {
+    int32_t cols[kMaxRowBlocks];
+    double  acc[kMaxRowBlocks * BS];
+};
+
+// (dR/dz)^T with 1x3 blocks: entry (a, (b,d)) = sum over cells of dR_(b,d)/dz_a
+// = vol s'(rho)/4 (B_b^T sigma0(u))_d.  Lanes take the row node's cells and accumulate the
+// four 1x3 blocks of each in shared memory.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
-k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
-                const double* __restrict__ u, double* __restrict__ entries) {
-    constexpr int BS = (MODE == 0) ? 9 : 3;
+k_assemble_dRdz_rows(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
+                     const double* __restrict__ u, double* __restrict__ entries) {
+    constexpr int BS = 3;
     __shared__ RowSmem<BS> sm[kWarpsPerBlock];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     RowSmem<BS>& S = sm[wib];
@@ -57,55 +225,35 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
         const int32_t ks = g.n2c_ptr[row], ke = g.n2c_ptr[row + 1];
         for (int32_t k = ks + lane; k < ke; k += 32) {
             const int32_t packed = g.n2c[k];
-            const int32_t c = packed >> 2, la = packed & 3;
+            const int32_t c = packed >> 2;
             const int4 n = m.conn[c];
             double x[4][3];
             load_cell_coords(m.coords, n, x);
             TetGeom<double> G;
             tet_geometry(x, G);
             const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
-            const double* ga = G.g[la];
-            if (MODE == 0) {
-                const double w = G.vol * simp(mat, rho);
+            double ue[4][3], e[6], s[6];
+            const int ids[4] = {n.x, n.y, n.z, n.w};
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    double Kb[9];
-                    stiffness_block(mat, ga, G.g[b], w, Kb);
-                    const int32_t nb = node_of(n, b);
-                    if (fast) {
-                        const int slot = find_slot(S.cols, nbk, nb);
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
-                        for (int q = 0; q < 9; ++q) atomicAdd(&S.acc[9 * slot + q], Kb[q]);
-                    } else {
-                        const int slot = find_slot(g.cols + rs, nbk, nb);
+                for (int d = 0; d < 3; ++d) ue[a][d] = __ldg(u + 3 * (int64_t)ids[a] + d);
+            strain_voigt(G.g, ue, e);
+            stress_voigt(mat, e, s);
+            const double w = G.vol * simp_dx(mat, rho) * 0.25;
 #pragma unroll
-                        for (int q = 0; q < 9; ++q) atomicAdd(&entries[9 * ((int64_t)rs + slot) + q], Kb[q]);
-                    }
-                }
-            } else {
-                double ue[4][3], e[6], s[6];
-                const int ids[4] = {n.x, n.y, n.z, n.w};
+            for (int b = 0; b < 4; ++b) {
+                double f[3];
+                divergence_node(G.g[b], s, w, f);
+                const int32_t nb = ids[b];
+                if (fast) {
+                    const int slot = find_slot(S.cols, nbk, nb);
 #pragma unroll
-                for (int a = 0; a < 4; ++a)
+                    for (int q = 0; q < 3; ++q) atomicAdd(&S.acc[3 * slot + q], f[q]);
+                } else {
+                    const int slot = find_slot(g.cols + rs, nbk, nb);
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) ue[a][d] = __ldg(u + 3 * (int64_t)ids[a] + d);
-                strain_voigt(G.g, ue, e);
-                stress_voigt(mat, e, s);
-                const double w = G.vol * simp_dx(mat, rho) * 0.25;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    double f[3];
-                    divergence_node(G.g[b], s, w, f);
-                    const int32_t nb = ids[b];
-                    if (fast) {
-                        const int slot = find_slot(S.cols, nbk, nb);
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) atomicAdd(&S.acc[3 * slot + q], f[q]);
-                    } else {
-                        const int slot = find_slot(g.cols + rs, nbk, nb);
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) atomicAdd(&entries[3 * ((int64_t)rs + slot) + q], f[q]);
-                    }
+                    for (int q = 0; q < 3; ++q) atomicAdd(&entries[3 * ((int64_t)rs + slot) + q], f[q]);
                 }
             }
         }
@@ -181,17 +329,17 @@ MeshView mesh_view(const plato_problem* h);
 GraphView graph_view(const plato_problem* h);
 
 int launch_assemble_jacobian(plato_problem* h, const double* z, double* entries) {
-    const int blocks = grid_for(h->N, kWarpsPerBlock, 148 * 64);
-    k_assemble_rows<0><<<blocks, kWarpsPerBlock * 32, 0, h->stream>>>(mesh_view(h), graph_view(h),
-                                                                       h->material, z, nullptr, entries);
+    const int blocks = grid_for(h->N, kJacWarps, 148 * 5 * 8);
+    k_assemble_jacobian<<<blocks, kJacWarps * 32, 0, h->stream>>>(mesh_view(h), graph_view(h), h->material, z,
+                                                                  entries);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }
 
 int launch_assemble_gradient_z(plato_problem* h, const double* u, const double* z, double* entries) {
     const int blocks = grid_for(h->N, kWarpsPerBlock, 148 * 64);
-    k_assemble_rows<1><<<blocks, kWarpsPerBlock * 32, 0, h->stream>>>(mesh_view(h), graph_view(h),
-                                                                       h->material, z, u, entries);
+    k_assemble_dRdz_rows<<<blocks, kWarpsPerBlock * 32, 0, h->stream>>>(mesh_view(h), graph_view(h), h->material,
+                                                                         z, u, entries);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

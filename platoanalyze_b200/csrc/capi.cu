@@ -129,6 +129,8 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_res); dfree(h->f_d0); dfree(h->f_d1); dfree(h->f_y); dfree(h->f_w);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->asm_ev)
+        if (e) cudaEventDestroy(e);
     coarse_release(h);
     delete h;
     return PLATO_OK;
@@ -299,11 +301,24 @@ int plato_get_instrumentation(const plato_problem* h, int64_t* launches, double*
     return PLATO_OK;
 }
 
+int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count) {
+    if (!h || !ms_total || !count) return PLATO_BAD_INPUT;
+    if (kind == 0) { *ms_total = h->op_ms_total; *count = h->op_timed; }
+    else if (kind == 1) { *ms_total = h->inner_ms_total; *count = h->inner_timed; }
+    else if (kind == 2) { *ms_total = h->asm_ms_total; *count = h->asm_timed; }
+    else return PLATO_BAD_INPUT;
+    return PLATO_OK;
+}
+
 int plato_reset_instrumentation(plato_problem* h) {
     if (!h) return PLATO_BAD_INPUT;
     h->launches = 0;
     h->op_ms_total = 0.0;
     h->op_timed = 0;
+    h->inner_ms_total = 0.0;
+    h->inner_timed = 0;
+    h->asm_ms_total = 0.0;
+    h->asm_timed = 0;
     return PLATO_OK;
 }
 
@@ -521,15 +536,30 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         return fcg_poly(h, h->v_b, x, st);
     }
     RC(dmalloc(h, &h->K, 9 * h->nblocks));
+    if (h->timing) {
+        for (cudaEvent_t& e : h->asm_ev)
+            if (!e) PLATO_CUDA(h, cudaEventCreate(&e));
+        PLATO_CUDA(h, cudaEventRecord(h->asm_ev[0], h->stream));
+    }
     RC(launch_assemble_jacobian(h, z, h->K));
+    if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[1], h->stream));
     RC(launch_dirichlet(h, h->K, h->v_b, bc_scale));
+    int rc;
     if (plain_method(h->opts)) {
         RC(prepare_operator(h, h->K));
-        return pcg_fp64(h, h->v_b, x, st);
+        rc = pcg_fp64(h, h->v_b, x, st);
+    } else {
+        RC(prepare_mixed(h, h->K, z));
+        RC(prepare_coarse(h, z));
+        rc = fcg_poly(h, h->v_b, x, st);
     }
-    RC(prepare_mixed(h, h->K, z));
-    RC(prepare_coarse(h, z));
-    return fcg_poly(h, h->v_b, x, st);
+    if (h->timing) {  // the solver has synchronised the stream
+        float ms = 0.f;
+        PLATO_CUDA(h, cudaEventElapsedTime(&ms, h->asm_ev[0], h->asm_ev[1]));
+        h->asm_ms_total += ms;
+        h->asm_timed += 1;
+    }
+    return rc;
 }
 
 // Problem::solution (src/elliptic/Problem.hpp:237-292), one Newton step from u = 0:

@@ -10,12 +10,14 @@
 // vol s(rho) (lambda G_J^(i)_i G_L^(j)_j + mu G_J^(i)_j G_L^(j)_i + mu delta_ij G_J^(i).G_L^(i))
 // from each element (the isotropic block formula with coarse gradients).
 //
-// Per solve: one CTA per coarse cell accumulates its 24x24 block over its elements (batches
-// staged in shared memory, each thread owning a few entries in registers), then E is
+// Per solve: the elements of each coarse cell are split over about eight CTAs per SM; each
+// CTA stages batches of elements' coarse gradients in shared memory and sums its share of
+// the cell's symmetric 24x24 block (upper triangle) in registers, then adds it to E.  E is
 // factored (blocked Cholesky, 32x32 tiles) and inverted explicitly (E^-1 = L^-T L^-1), so a
 // coarse solve in the iteration is one dense matrix-vector product.
-// Per preconditioner call: restriction (one CTA per coarse node gathers its support through
-// the per-cell node lists, deterministic), y_c = E^-1 r_c (warp per row), prolongation.
+// Per preconditioner call: restriction in two deterministic passes (per-cell partial sums by
+// split CTAs, then a fixed-order sum per coarse dof), y_c = E^-1 r_c (warp per row),
+// prolongation (thread per fine node).
 #include <cub/cub.cuh>
 
 #include "plato_internal.cuh"
@@ -27,7 +29,8 @@ GraphView graph_view(const plato_problem* h);
 namespace {
 
 constexpr int kTile = 32;
-constexpr int kBatch = 64;
+constexpr int kBatch = 32;     // elements staged per Galerkin batch (8 threads each)
+constexpr int kThreadsPerCta = 256;
 
 struct CoarseView {
     int nc0, nc1, nc2;
@@ -95,85 +98,102 @@ __global__ void k_elem_keys(int32_t C, const int4* __restrict__ conn, const doub
     }
 }
 
-// E (n x n, row-major) += Galerkin contribution of every element; one CTA per coarse cell.
-__global__ void __launch_bounds__(256)
-k_galerkin(CoarseView cv, const int32_t* __restrict__ elem_ptr, const int32_t* __restrict__ elem_list,
+// Upper-triangle entry t (row-major) of a 24x24 matrix -> (r, c), r <= c.
+__device__ __forceinline__ void upper_entry(int t, int& r, int& c) {
+    r = 0;
+    while (t >= 24 - r) { t -= 24 - r; ++r; }
+    c = r + t;
+}
+
+// E (n x n, row-major) += Galerkin contribution of every element.  CTA (cell, split) takes a
+// contiguous share of the coarse cell's elements in batches of kBatch: eight threads per
+// element (one corner J each) stage its coarse gradients G_J^(i) and Q_(J,i) = w G_J^(i) in
+// shared memory, then each thread sums one or two of the 300 upper-triangle entries of the
+// cell's symmetric 24x24 block over the batch in registers; the sums are added to E (and
+// mirrored) once per CTA.
+__global__ void __launch_bounds__(kThreadsPerCta)
+k_galerkin(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, const int32_t* __restrict__ elem_list,
            const int4* __restrict__ conn, const double* __restrict__ coords, const double* __restrict__ z,
            Material mat, const uint8_t* __restrict__ mask, int n, double* __restrict__ E) {
     __shared__ double Gs[kBatch][3][8][3];
-    __shared__ double ws[kBatch];
-    const int ncells = cv.nc0 * cv.nc1 * cv.nc2;
+    __shared__ double Qs[kBatch][3][8][3];
     const double lam = mat.c01, mu = mat.c33;
-    for (int cell = blockIdx.x; cell < ncells; cell += gridDim.x) {
-        const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
-        const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
-        double acc[3] = {0.0, 0.0, 0.0};
-        const int e0 = elem_ptr[cell], e1 = elem_ptr[cell + 1];
-        for (int base = e0; base < e1; base += kBatch) {
-            if (threadIdx.x < kBatch) {
-                const int k = threadIdx.x;
-                double w = 0.0;
-                if (base + k < e1) {
-                    const int e = elem_list[base + k];
-                    const int4 nd = conn[e];
-                    double x[4][3];
-                    load_cell_coords(coords, nd, x);
-                    TetGeom<double> G;
-                    tet_geometry(x, G);
-                    const double rho = (z[nd.x] + z[nd.y] + z[nd.z] + z[nd.w]) * 0.25;
-                    w = G.vol * simp(mat, rho);
-                    const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
-                    double loc[4][3];
-                    for (int a = 0; a < 4; ++a) {
-                        loc[a][0] = (x[a][0] - lo[0]) / cv.hx;
-                        loc[a][1] = (x[a][1] - lo[1]) / cv.hy;
-                        loc[a][2] = (x[a][2] - lo[2]) / cv.hz;
-                    }
-                    for (int d = 0; d < 3; ++d)
-                        for (int J = 0; J < 8; ++J) {
-                            double gj[3] = {0.0, 0.0, 0.0};
-                            for (int a = 0; a < 4; ++a) {
-                                if (mask[3 * (int64_t)ids[a] + d]) continue;
-                                const double wa = corner_weight(J, loc[a][0], loc[a][1], loc[a][2]);
-                                gj[0] += wa * G.g[a][0];
-                                gj[1] += wa * G.g[a][1];
-                                gj[2] += wa * G.g[a][2];
-                            }
-                            Gs[k][d][J][0] = gj[0];
-                            Gs[k][d][J][1] = gj[1];
-                            Gs[k][d][J][2] = gj[2];
-                        }
+    const int cell = blockIdx.x / split, part = blockIdx.x - cell * split;
+    const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
+    const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
+    const int q0 = elem_ptr[cell], q1 = elem_ptr[cell + 1];
+    const int chunk = (q1 - q0 + split - 1) / split;
+    const int e0 = q0 + part * chunk, e1 = min(q1, e0 + chunk);
+    int R[2], Cc[2];
+    const int nent = threadIdx.x + kThreadsPerCta < 300 ? 2 : 1;
+    upper_entry(threadIdx.x, R[0], Cc[0]);
+    R[1] = Cc[1] = 0;
+    if (nent == 2) upper_entry(threadIdx.x + kThreadsPerCta, R[1], Cc[1]);
+    double acc[2] = {0.0, 0.0};
+    const int k = threadIdx.x >> 3, J = threadIdx.x & 7;  // staging: element k of the batch, corner J
+    for (int base = e0; base < e1; base += kBatch) {
+        if (base + k < e1) {
+            const int4 nd = conn[elem_list[base + k]];
+            double x[4][3];
+            load_cell_coords(coords, nd, x);
+            TetGeom<double> G;
+            tet_geometry(x, G);
+            const double rho = (z[nd.x] + z[nd.y] + z[nd.z] + z[nd.w]) * 0.25;
+            const double w = G.vol * simp(mat, rho);
+            const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
+            double wa[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+                wa[a] = corner_weight(J, (x[a][0] - lo[0]) / cv.hx, (x[a][1] - lo[1]) / cv.hy, (x[a][2] - lo[2]) / cv.hz);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double gj[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    if (mask[3 * (int64_t)ids[a] + d]) continue;
+                    gj[0] += wa[a] * G.g[a][0];
+                    gj[1] += wa[a] * G.g[a][1];
+                    gj[2] += wa[a] * G.g[a][2];
                 }
-                ws[k] = w;
-            }
-            __syncthreads();
-            const int nb = min(kBatch, e1 - base);
-            for (int s = 0; s < 3; ++s) {
-                const int t = threadIdx.x + 256 * s;
-                if (t >= 576) break;
-                const int r = t / 24, c = t - 24 * (t / 24);
-                const int J = r / 3, i = r - 3 * (r / 3), L = c / 3, j = c - 3 * (c / 3);
-                double a = 0.0;
-                for (int k = 0; k < nb; ++k) {
-                    const double* Gi = Gs[k][i][J];
-                    const double* Gj = Gs[k][j][L];
-                    double v = lam * Gi[i] * Gj[j] + mu * Gi[j] * Gj[i];
-                    if (i == j) v += mu * (Gi[0] * Gj[0] + Gi[1] * Gj[1] + Gi[2] * Gj[2]);
-                    a += ws[k] * v;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    Gs[k][d][J][t] = gj[t];
+                    Qs[k][d][J][t] = w * gj[t];
                 }
-                acc[s] += a;
             }
-            __syncthreads();
         }
-        for (int s = 0; s < 3; ++s) {
-            const int t = threadIdx.x + 256 * s;
-            if (t >= 576) break;
-            const int r = t / 24, c = t - 24 * (t / 24);
-            const int J = r / 3, i = r - 3 * (r / 3), L = c / 3, j = c - 3 * (c / 3);
-            const int gJ = coarse_node(cv, cx + ((J >> 2) & 1), cy + ((J >> 1) & 1), cz + (J & 1));
-            const int gL = coarse_node(cv, cx + ((L >> 2) & 1), cy + ((L >> 1) & 1), cz + (L & 1));
-            if (acc[s] != 0.0) atomicAdd(&E[(int64_t)(3 * gJ + i) * n + 3 * gL + j], acc[s]);
+        __syncthreads();
+        const int nb = min(kBatch, e1 - base);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            if (s >= nent) break;
+            const int Jr = R[s] / 3, i = R[s] - 3 * Jr, L = Cc[s] / 3, j = Cc[s] - 3 * L;
+            double a = 0.0;
+            if (i == j) {
+                for (int e = 0; e < nb; ++e) {
+                    const double* Qi = Qs[e][i][Jr];
+                    const double* Gj = Gs[e][j][L];
+                    a += (lam + mu) * Qi[i] * Gj[i] + mu * (Qi[0] * Gj[0] + Qi[1] * Gj[1] + Qi[2] * Gj[2]);
+                }
+            } else {
+                for (int e = 0; e < nb; ++e) {
+                    const double* Qi = Qs[e][i][Jr];
+                    const double* Gj = Gs[e][j][L];
+                    a += lam * Qi[i] * Gj[j] + mu * Qi[j] * Gj[i];
+                }
+            }
+            acc[s] += a;
         }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        if (s >= nent || acc[s] == 0.0) continue;
+        const int Jr = R[s] / 3, i = R[s] - 3 * Jr, L = Cc[s] / 3, j = Cc[s] - 3 * L;
+        const int gJ = coarse_node(cv, cx + ((Jr >> 2) & 1), cy + ((Jr >> 1) & 1), cz + (Jr & 1));
+        const int gL = coarse_node(cv, cx + ((L >> 2) & 1), cy + ((L >> 1) & 1), cz + (L & 1));
+        atomicAdd(&E[(int64_t)(3 * gJ + i) * n + 3 * gL + j], acc[s]);
+        if (R[s] != Cc[s]) atomicAdd(&E[(int64_t)(3 * gL + j) * n + 3 * gJ + i], acc[s]);
     }
 }
 
@@ -314,42 +334,72 @@ __global__ void k_gram(int n, const double* __restrict__ X, double* __restrict__
 
 // ---- per-iteration kernels ----------------------------------------------------------------
 
-// rc[(J,d)] = sum_p phi_J(x_p) m_(p,d) v[(p,d)] (one CTA per coarse node, deterministic)
-__global__ void __launch_bounds__(256)
-k_restrict(CoarseView cv, const int32_t* __restrict__ node_ptr, const int32_t* __restrict__ node_list,
-           const double* __restrict__ coords, const uint8_t* __restrict__ mask, const float* __restrict__ v,
-           double* __restrict__ rc, const PcgScalars* S) {
-    __shared__ double sh[3][8];
+// Restriction rc[(J,d)] = sum_p phi_J(x_p) m_(p,d) v[(p,d)], deterministic, in two passes.
+// Pass 1: CTA (cell, split) sums over its share of the coarse cell's fine nodes the 24 values
+// phi_b(x_p) m_(p,d) v[(p,d)] (corner b of the cell, component d) into part[CTA][24].
+__global__ void __launch_bounds__(kThreadsPerCta)
+k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
+                 const int32_t* __restrict__ node_list, const double* __restrict__ coords,
+                 const uint8_t* __restrict__ mask, const float* __restrict__ v, double* __restrict__ part,
+                 const PcgScalars* S) {
+    __shared__ double sh[kThreadsPerCta / 32][24];
+    if (S && S->done) return;
+    const int cell = blockIdx.x / split, piece = blockIdx.x - cell * split;
+    const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
+    const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
+    const int q0 = node_ptr[cell], q1 = node_ptr[cell + 1];
+    const int chunk = (q1 - q0 + split - 1) / split;
+    const int a0 = q0 + piece * chunk, a1 = min(q1, a0 + chunk);
+    double s[24];
+#pragma unroll
+    for (int t = 0; t < 24; ++t) s[t] = 0.0;
+    for (int q = a0 + threadIdx.x; q < a1; q += kThreadsPerCta) {
+        const int64_t p = node_list[q];
+        const double u = (coords[3 * p] - lo[0]) / cv.hx, vv = (coords[3 * p + 1] - lo[1]) / cv.hy,
+                     w = (coords[3 * p + 2] - lo[2]) / cv.hz;
+        double val[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) val[d] = mask[3 * p + d] ? 0.0 : double(v[3 * p + d]);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const double wgt = corner_weight(b, u, vv, w);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s[3 * b + d] += wgt * val[d];
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 24; ++t)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[t] += __shfl_xor_sync(0xffffffffu, s[t], o);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < 24; ++t) sh[wid][t] = s[t];
+    __syncthreads();
+    if (threadIdx.x < 24) {
+        double t = 0.0;
+        for (int k = 0; k < kThreadsPerCta / 32; ++k) t += sh[k][threadIdx.x];
+        part[(int64_t)blockIdx.x * 24 + threadIdx.x] = t;
+    }
+}
+
+// Pass 2: rc[(J,d)] = sum over the <= 8 cells around coarse node J (J is corner b of the cell)
+// and over their splits, in a fixed order.
+__global__ void k_restrict_sum(CoarseView cv, int split, const double* __restrict__ part, double* __restrict__ rc,
+                               const PcgScalars* S) {
     if (S && S->done) return;
     const int ncn = (cv.nc0 + 1) * (cv.nc1 + 1) * (cv.nc2 + 1);
-    for (int J = blockIdx.x; J < ncn; J += gridDim.x) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * ncn; t += gridDim.x * blockDim.x) {
+        const int J = t / 3, d = t - 3 * J;
         const int iz = J % (cv.nc2 + 1), iy = (J / (cv.nc2 + 1)) % (cv.nc1 + 1), ix = J / ((cv.nc1 + 1) * (cv.nc2 + 1));
-        double s[3] = {0.0, 0.0, 0.0};
+        double sum = 0.0;
         for (int b = 0; b < 8; ++b) {
             const int cx = ix - ((b >> 2) & 1), cy = iy - ((b >> 1) & 1), cz = iz - (b & 1);
             if (cx < 0 || cy < 0 || cz < 0 || cx >= cv.nc0 || cy >= cv.nc1 || cz >= cv.nc2) continue;
-            const int cell = cell_id(cv, cx, cy, cz);
-            const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
-            for (int q = node_ptr[cell] + threadIdx.x; q < node_ptr[cell + 1]; q += blockDim.x) {
-                const int64_t p = node_list[q];
-                const double wgt = corner_weight(b, (coords[3 * p] - lo[0]) / cv.hx,
-                                                 (coords[3 * p + 1] - lo[1]) / cv.hy, (coords[3 * p + 2] - lo[2]) / cv.hz);
-                for (int d = 0; d < 3; ++d)
-                    if (!mask[3 * p + d]) s[d] += wgt * double(v[3 * p + d]);
-            }
+            const double* pc = part + (int64_t)cell_id(cv, cx, cy, cz) * split * 24 + 3 * b + d;
+            for (int k = 0; k < split; ++k) sum += pc[24 * k];
         }
-        for (int d = 0; d < 3; ++d)
-            for (int o = 16; o > 0; o >>= 1) s[d] += __shfl_xor_sync(0xffffffffu, s[d], o);
-        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        if (l == 0)
-            for (int d = 0; d < 3; ++d) sh[d][w] = s[d];
-        __syncthreads();
-        if (threadIdx.x < 3) {
-            double t = 0.0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[threadIdx.x][k];
-            rc[3 * J + threadIdx.x] = t;
-        }
-        __syncthreads();
+        rc[t] = sum;
     }
 }
 
@@ -472,6 +522,11 @@ int coarse_setup_mesh(plato_problem* h) {
     const size_t nn = size_t(c.ndof) * c.ndof;
     PLATO_CUDA(h, cudaMalloc(&c.E, sizeof(double) * nn));
     PLATO_CUDA(h, cudaMalloc(&c.Einv, sizeof(double) * nn));
+    // splits of each coarse cell's node / element lists so that the restriction and the
+    // Galerkin sum run about 8 CTAs per SM
+    c.rsplit = clampi((148 * 8 + c.ncells - 1) / c.ncells, 1, 64);
+    c.gsplit = clampi((148 * 8 + c.ncells - 1) / c.ncells, 1, 64);
+    PLATO_CUDA(h, cudaMalloc(&c.rpart, sizeof(double) * 24 * c.ncells * c.rsplit));
     PLATO_CUDA(h, cudaMalloc(&c.rc, sizeof(double) * c.ndof));
     PLATO_CUDA(h, cudaMalloc(&c.yc, sizeof(double) * c.ndof));
     PLATO_CUDA(h, cudaMalloc(&c.flag, sizeof(int32_t)));
@@ -483,7 +538,7 @@ void coarse_release(plato_problem* h) {
     CoarseSpace& c = h->coarse;
     for (int32_t** p : {&c.node_ptr, &c.node_list, &c.elem_ptr, &c.elem_list, &c.flag})
         if (*p) { cudaFree(*p); *p = nullptr; }
-    for (double** p : {&c.E, &c.Einv, &c.rc, &c.yc})
+    for (double** p : {&c.E, &c.Einv, &c.rc, &c.yc, &c.rpart})
         if (*p) { cudaFree(*p); *p = nullptr; }
     c.ready = 0;
 }
@@ -495,8 +550,8 @@ int coarse_setup_operator(plato_problem* h, const double* z) {
     const int n = c.ndof;
     const size_t nn = size_t(n) * n;
     PLATO_CUDA(h, cudaMemsetAsync(c.E, 0, sizeof(double) * nn, s));
-    k_galerkin<<<grid_for(c.ncells, 1, 148 * 8), 256, 0, s>>>(coarse_view(h), c.elem_ptr, c.elem_list, h->conn,
-                                                               h->coords, z, h->material, h->bc_mask, n, c.E);
+    k_galerkin<<<c.ncells * c.gsplit, kThreadsPerCta, 0, s>>>(coarse_view(h), c.gsplit, c.elem_ptr, c.elem_list,
+                                                               h->conn, h->coords, z, h->material, h->bc_mask, n, c.E);
     PLATO_LAUNCH_CHECK(h);
     k_regularize<<<grid_for(n, 256), 256, 0, s>>>(n, c.E);
     PLATO_LAUNCH_CHECK(h);
@@ -533,11 +588,12 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
     CoarseSpace& c = h->coarse;
     cudaStream_t s = h->stream;
     const CoarseView cv = coarse_view(h);
-    k_restrict<<<grid_for(c.nnodes, 1, 148 * 8), 256, 0, s>>>(cv, c.node_ptr, c.node_list, h->coords, h->bc_mask, v,
-                                                               c.rc, S);
+    k_restrict_cells<<<c.ncells * c.rsplit, kThreadsPerCta, 0, s>>>(cv, c.rsplit, c.node_ptr, c.node_list, h->coords,
+                                                                      h->bc_mask, v, c.rpart, S);
+    k_restrict_sum<<<grid_for(c.ndof, 256), 256, 0, s>>>(cv, c.rsplit, c.rpart, c.rc, S);
     k_coarse_gemv<<<grid_for(int64_t(c.ndof) * 32, 256, 148 * 8), 256, 0, s>>>(c.ndof, c.Einv, c.rc, c.yc, S);
     k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, y, accumulate, S);
-    h->launches += 2;
+    h->launches += 3;
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -567,10 +567,19 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         return PLATO_OK;
     };
     float* dlast = h->f_d0;
+    std::vector<int64_t> timed_iters;  // timing records of the current pass (see collect_timing)
+    int64_t inner_record = -1;  // >= 0: time the first step of this sweep (record 2*iter+1)
     auto chebyshev_steps = [&]() -> int {
         float* dcur = h->f_d0;
         float* dnext = h->f_d1;
         for (int k = 1; k < degree; ++k) {
+            cudaEvent_t t0 = nullptr, t1 = nullptr;
+            if (k == 1 && inner_record >= 0) {
+                int r2 = timing_events(h, &t0, &t1);
+                if (r2) return r2;
+                timed_iters.push_back(inner_record);
+                PLATO_CUDA(h, cudaEventRecord(t0, s));
+            }
             if (mf) {
                 int r2 = launch_ebe_apply32(h, dcur, h->f_w, h->scal);
                 if (r2) return r2;
@@ -587,6 +596,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                                                                   h->f_y, cc.c1[k], cc.c2[k], h->scal);
             }
             PLATO_LAUNCH_CHECK(h);
+            if (t1) PLATO_CUDA(h, cudaEventRecord(t1, s));
             std::swap(dcur, dnext);
         }
         dlast = dcur;
@@ -632,7 +642,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
 
         PcgScalars* slots = h->scal_host;
         int64_t enqueued = 0;
-        std::vector<int64_t> timed_iters;
+        timed_iters.clear();
         h->ev_used = 0;
         int cur = 0;
         bool have_prev = false;
@@ -646,7 +656,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 if (timed) {
                     rc = timing_events(h, &e0, &e1);
                     if (rc) return rc;
-                    timed_iters.push_back(enqueued);
+                    timed_iters.push_back(2 * enqueued);
                     PLATO_CUDA(h, cudaEventRecord(e0, s));
                 }
                 if (mf) {
@@ -660,7 +670,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 k_fcg_update<<<VB, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_q, h->f_dinv, h->f_res, h->f_d0,
                                                      h->f_y, cc.c0, h->scal, h->partials, max_it);
                 h->launches += 2;
+                inner_record = timed ? 2 * enqueued + 1 : -1;
                 rc = precondition(cc.c0);
+                inner_record = -1;
                 if (rc) return rc;
                 k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, h->v_z, h->v_q, h->scal, h->partials, 0);
                 k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 0);

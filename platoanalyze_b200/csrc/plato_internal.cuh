@@ -75,6 +75,8 @@ struct CoarseSpace {
     int32_t* elem_list = nullptr;
     double*  E = nullptr;         // Galerkin operator, then its Cholesky factor (ndof^2)
     double*  Einv = nullptr;      // explicit inverse (ndof^2)
+    int32_t  rsplit = 1, gsplit = 1;  // CTAs per coarse cell in the restriction / Galerkin sum
+    double*  rpart = nullptr;     // restriction partial sums (ncells * rsplit * 24)
     double*  rc = nullptr;        // restricted residual
     double*  yc = nullptr;        // coarse correction
     int32_t* flag = nullptr;
@@ -171,6 +173,11 @@ struct plato_problem {
     int     ev_used = 0;
     double  op_ms_total = 0.0;
     int64_t op_timed = 0;
+    double  inner_ms_total = 0.0;  // preconditioner operator step (mixed-precision solver)
+    int64_t inner_timed = 0;
+    cudaEvent_t asm_ev[2] = {nullptr, nullptr};  // Jacobian assembly of the solve path
+    double  asm_ms_total = 0.0;
+    int64_t asm_timed = 0;
 };
 
 // ---------------------------------------------------------------------------------------

@@ -191,14 +191,21 @@ int timing_events(plato_problem* h, cudaEvent_t* e0, cudaEvent_t* e1) {
     return PLATO_OK;
 }
 
-// Adds the durations of the timed applies that belonged to executed iterations.
+// Adds the durations of the timed applies that belonged to executed iterations.  Each
+// record is 2 * iteration + class (0 = outer FP64 operator, 1 = preconditioner operator
+// step), in the order the event pairs were taken.
 int collect_timing(plato_problem* h, const std::vector<int64_t>& iters, int64_t executed) {
     for (size_t k = 0; k < iters.size(); ++k) {
-        if (iters[k] >= executed) break;
+        if ((iters[k] >> 1) >= executed) break;
         float ms = 0.f;
         PLATO_CUDA(h, cudaEventElapsedTime(&ms, h->ev_pool[2 * k], h->ev_pool[2 * k + 1]));
-        h->op_ms_total += ms;
-        h->op_timed += 1;
+        if (iters[k] & 1) {
+            h->inner_ms_total += ms;
+            h->inner_timed += 1;
+        } else {
+            h->op_ms_total += ms;
+            h->op_timed += 1;
+        }
     }
     h->ev_used = 0;
     return PLATO_OK;
@@ -269,7 +276,7 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 if (timed) {
                     rc = timing_events(h, &e0, &e1);
                     if (rc) return rc;
-                    timed_iters.push_back(enqueued);
+                    timed_iters.push_back(2 * enqueued);
                     PLATO_CUDA(h, cudaEventRecord(e0, s));
                 }
                 k_sell_spmv<<<sp_blocks, kThreads, 0, s>>>(V, A, h->v_p, h->v_Ap, h->scal, h->partials);

@@ -121,7 +121,12 @@ class EllipticProblem:
     def instrumentation(self) -> dict:
         n, ms, k = C.c_int64(), C.c_double(), C.c_int64()
         check(lib.plato_get_instrumentation(self.h, C.byref(n), C.byref(ms), C.byref(k)), self.h)
-        return {"launches": n.value, "op_ms_total": ms.value, "op_timed": k.value}
+        out = {"launches": n.value, "op_ms_total": ms.value, "op_timed": k.value}
+        for kind, name in ((1, "inner"), (2, "assembly")):
+            t, c = C.c_double(), C.c_int64()
+            check(lib.plato_get_kernel_timing(self.h, kind, C.byref(t), C.byref(c)), self.h)
+            out[name + "_ms_total"], out[name + "_timed"] = t.value, c.value
+        return out
 
     def reset_instrumentation(self) -> None:
         check(lib.plato_reset_instrumentation(self.h), self.h)

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from . import capi
 from .mesh import box_mesh
 from .problem import ProblemSpec, SolverOptions, cantilever_spec
 
@@ -44,3 +45,35 @@ def large_problem(solver: SolverOptions | None = None, n: tuple[int, int, int] =
     spec = cantilever(*n, solver)
     z = splitmix_uniform(spec.coords.shape[0], SEED_LARGE)
     return spec, z
+
+
+COARSE_BOX = (10, 5, 5)  # coarse box grid of the two-level method (aligns with 20k x 10k x 10k hex grids)
+
+METHODS = ("two-level", "plain", "chebyshev", "bf16", "matrix-free")
+
+
+def method_options(method: str, tol: float = 1e-10, coarse=COARSE_BOX) -> SolverOptions:
+    """Solver options of the named method; every method stops on the same FP64 residual test.
+
+    plain        FP64 Jacobi-PCG on the assembled block matrix (the reference's algorithm)
+    two-level    FP64 flexible CG; FP32 Chebyshev(8)-Jacobi on an FP32 copy of the matrix plus
+                 a Galerkin coarse correction on a trilinear box grid
+    chebyshev    the same without the coarse correction
+    bf16         BF16-stored matrix, Chebyshev(16)-Jacobi, no coarse correction
+    matrix-free  FP32 element-by-element operator, Chebyshev(16)-Jacobi, no coarse correction
+    """
+    if method == "plain":
+        return SolverOptions(tolerance=tol, max_iterations=200000)
+    if method == "two-level":
+        return SolverOptions(tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP32,
+                             chebyshev_degree=8, chebyshev_ratio=30.0, coarse_cells=tuple(coarse))
+    if method == "chebyshev":
+        return SolverOptions(tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP32,
+                             chebyshev_degree=8, chebyshev_ratio=30.0)
+    if method == "bf16":
+        return SolverOptions(tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_BF16,
+                             chebyshev_degree=16)
+    if method == "matrix-free":
+        return SolverOptions(tolerance=tol, max_iterations=200000, operator_kind=capi.OPERATOR_MATRIX_FREE,
+                             precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=16)
+    raise ValueError(f"unknown method {method!r}; one of {METHODS}")

@@ -245,6 +245,38 @@ def test_iteration_limit_reports_not_converged():
     assert st["rc"] == capi.NOT_CONVERGED and st["iterations"] == 3
 
 
+def fan_mesh(k):
+    """Tets (0, pole, ring_j, ring_j+1) around a vertical axis through node 0, above and below
+    the ring: node 0 has 2k cells and k + 3 blocks, each pole k cells."""
+    t = 2 * np.pi * np.arange(k) / k
+    ring = np.stack([np.cos(t), np.sin(t), 0.1 * np.sin(3 * t)], axis=1)
+    coords = np.vstack([[0.0, 0.0, 0.0], [0.1, 0.0, 1.0], [0.0, 0.1, -1.0], ring])
+    cells = []
+    for j in range(k):
+        a, b = 3 + j, 3 + (j + 1) % k
+        cells.append([0, 1, a, b])
+        cells.append([0, 2, b, a])
+    return coords, np.asarray(cells, dtype=np.int32)
+
+
+@pytest.mark.parametrize("k", [12, 20, 40])
+def test_high_valence_rows(k):
+    """Rows with more than 32 incident cells or blocks take the atomic assembly path; rows
+    below the limits the register path.  Both must match the oracle."""
+    coords, conn = fan_mesh(k)
+    spec = ProblemSpec(coords, conn, 1.7, 0.31, 3.0, 1e-9)
+    prob, orc = EllipticProblem(spec), Oracle.from_spec(spec)
+    z = splitmix_uniform(coords.shape[0], 7 + k)
+    u = np.cos(np.arange(3 * coords.shape[0]) * 0.7)
+    ud, zd = prob.to_dev(u), prob.to_dev(z)
+    rm, cols = orc.graph()
+    rmg, colsg = (host(t) for t in prob.pattern())
+    assert np.array_equal(rmg, rm) and np.array_equal(colsg, cols)
+    close(host(prob.vf_gradient_u(ud, zd)), orc.vf_gradient_u(u, z))
+    close(host(prob.vf_gradient_z(ud, zd)), orc.vf_gradient_z(u, z))
+    close(host(prob.vf_value(ud, zd)), orc.vf_value(u, z))
+
+
 def test_bad_connectivity_rejected():
     m = box_mesh(2, 2, 2)
     conn = m.connectivity.copy()

@@ -242,6 +242,28 @@ int plato_sf_value_noalloc(int32_t num_nodes, int32_t num_cells, const int32_t* 
                            const plato_material* material, const plato_penalty* penalty,
                            double* value, void* cuda_stream);
 
+/* ---- batches of independent problems (no reference counterpart: the reference builds one
+ * Elliptic::Problem per design and load case, src/elliptic/Problem.hpp:80-140) -----------
+ * plato_create_batch returns ONE handle over the disjoint union of `count` problems: member
+ * s's nodes, cells, essential-BC dofs and traction faces follow those of members 0..s-1
+ * (plato_batch_info gives the offsets).  Every entry point above then acts on the union:
+ * vectors are the members' vectors concatenated, the block pattern is block diagonal, and
+ * the solves (problem_solution, the adjoint, solver_solve) run every member to its own stop
+ * test ||r_s|| <= tol ||b_s|| in one batched flexible CG (one launch per stage for all
+ * members; Chebyshev-Jacobi preconditioner of solver.chebyshev_degree, Jacobi when it is 0).
+ * Members must share material and penalty; the solver options are descs[0].solver; the
+ * matrix-free operator and the coarse space are PLATO_NOT_SUPPORTED for batches.  The
+ * aggregate statistics of a solve carry the maximum iterations and relative residual. */
+int plato_create_batch(int32_t count, const plato_problem_desc* descs, plato_problem** out);
+/* count (1 for a single problem) and the member offsets node_offsets[count+1],
+ * cell_offsets[count+1] (either may be NULL) */
+int plato_batch_info(const plato_problem* h, int32_t* count, int32_t* node_offsets, int32_t* cell_offsets);
+/* per-member statistics of the last solve on a batch handle: stats[count] (host) */
+int plato_batch_last_stats(const plato_problem* h, plato_solve_stats* stats);
+/* per-member criterion values (internal elastic energy, PhysicsScalarFunction::value for
+ * each member) into values[count] [device]; synchronises the handle's stream */
+int plato_batch_criterion_values(plato_problem* h, const double* z, const double* u, double* values);
+
 /* ---- box mesh generator (host only; stands in for BamG, unit_tests/PlatoTestHelpers.hpp) */
 int plato_box_mesh_sizes(int32_t nx, int32_t ny, int32_t nz, int32_t* num_nodes, int32_t* num_cells);
 int plato_box_mesh_tet4(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,

@@ -107,6 +107,10 @@ def _load() -> C.CDLL:
         "plato_problem_solve_and_gradient_host": ([vp, vp, vp, vp, f64p, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_sf_value_noalloc": ([C.c_int32, C.c_int32, vp, vp, vp, vp, C.POINTER(Material), C.POINTER(Penalty),
                                     vp, vp], C.c_int),
+        "plato_create_batch": ([C.c_int32, C.POINTER(ProblemDesc), C.POINTER(vp)], C.c_int),
+        "plato_batch_info": ([vp, i32p, i32p, i32p], C.c_int),
+        "plato_batch_last_stats": ([vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_batch_criterion_values": ([vp, vp, vp, vp], C.c_int),
         "plato_box_mesh_sizes": ([C.c_int32] * 3 + [i32p, i32p], C.c_int),
         "plato_box_mesh_tet4": ([C.c_int32] * 3 + [C.c_double] * 3 + [vp, vp], C.c_int),
         "plato_box_nodeset": ([C.c_int32] * 4 + [vp, i32p], C.c_int),

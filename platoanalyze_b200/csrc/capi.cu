@@ -132,6 +132,7 @@ int plato_destroy(plato_problem* h) {
     for (cudaEvent_t e : h->asm_ev)
         if (e) cudaEventDestroy(e);
     coarse_release(h);
+    batch_release(h);
     delete h;
     return PLATO_OK;
 }
@@ -282,6 +283,8 @@ int plato_set_stream(plato_problem* h, void* stream) {
 int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* o) {
     NEED(h, o != nullptr, "null solver options");
     RC(check_opts(h, *o));
+    if (h->batch.nseg > 0 && (o->operator_kind != PLATO_OPERATOR_ASSEMBLED || o->coarse_cells[0] > 0))
+        return plato_fail(h, PLATO_NOT_SUPPORTED, "batched solves use the assembled operator without a coarse space");
     h->opts = *o;
     return PLATO_OK;
 }
@@ -437,6 +440,10 @@ int plato_solver_solve(plato_problem* h, const double* entries, double* x, const
     plato_solve_stats local{};
     plato_solve_stats* st = stats ? stats : &local;
     // the matrix is given: the assembled operator is used whatever operator_kind says
+    if (h->batch.nseg > 0) {
+        RC(prepare_mixed(h, entries, nullptr));
+        return fcg_batch(h, b, x, st);
+    }
     if (h->opts.precision == PLATO_PRECISION_FP64 && h->opts.chebyshev_degree <= 0) {
         RC(prepare_operator(h, entries));
         return pcg_fp64(h, b, x, st);
@@ -545,7 +552,10 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
     if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[1], h->stream));
     RC(launch_dirichlet(h, h->K, h->v_b, bc_scale));
     int rc;
-    if (plain_method(h->opts)) {
+    if (h->batch.nseg > 0) {  // member-wise flexible CG over the union (Jacobi when no degree is set)
+        RC(prepare_mixed(h, h->K, z));
+        rc = fcg_batch(h, h->v_b, x, st);
+    } else if (plain_method(h->opts)) {
         RC(prepare_operator(h, h->K));
         rc = pcg_fp64(h, h->v_b, x, st);
     } else {

@@ -318,11 +318,47 @@ int launch_volume_gradient(plato_problem* h, const Material& pen, const double* 
     return PLATO_OK;
 }
 
+// Internal elastic energy of each member of a batch: CTA (member, piece) sums its share of
+// the member's cells, then one thread per member adds the pieces in order (deterministic).
+__global__ void __launch_bounds__(kThreads) k_energy_pieces(MeshView m, Material mat, const double* __restrict__ u,
+                                                            const double* __restrict__ z,
+                                                            const int32_t* __restrict__ cell_off,
+                                                            double* __restrict__ pieces) {
+    __shared__ double sh[32];
+    const int s = blockIdx.x / kEnergySplit, piece = blockIdx.x - s * kEnergySplit;
+    const int64_t c0 = cell_off[s], c1 = cell_off[s + 1];
+    const int64_t len = (c1 - c0 + kEnergySplit - 1) / kEnergySplit;
+    const int64_t a = c0 + piece * len, e = a + len < c1 ? a + len : c1;
+    double v = 0.0;
+    for (int64_t c = a + threadIdx.x; c < e; c += blockDim.x) v += cell_quantity<0>(m, mat, u, z, nullptr, c);
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) pieces[blockIdx.x] = v;
+}
+
+__global__ void k_sum_pieces(int32_t nseg, const double* __restrict__ pieces, double* __restrict__ values) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (int k = 0; k < kEnergySplit; ++k) t += pieces[(int64_t)s * kEnergySplit + k];
+        values[s] = t;
+    }
+}
+
 // Internal elastic energy into *result (device scalar).
 int launch_energy(plato_problem* h, const double* u, const double* z, double* result) {
     const int G = grid_for(h->C, kThreads, h->partials_len);
     k_energy_sum<<<G, kThreads, 0, h->stream>>>(mesh_view(h), h->material, u, z, h->partials,
                                                  h->red_ticket, result);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+// Energy of every batch member into values[nseg] (device).
+int launch_energy_segments(plato_problem* h, const double* u, const double* z, double* values) {
+    const int nseg = h->batch.nseg;
+    k_energy_pieces<<<nseg * kEnergySplit, kThreads, 0, h->stream>>>(mesh_view(h), h->material, u, z,
+                                                                      h->batch.cell_off_d, h->batch.values);
+    PLATO_LAUNCH_CHECK(h);
+    k_sum_pieces<<<grid_for(nseg, 128), 128, 0, h->stream>>>(nseg, h->batch.values, values);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -18,6 +18,7 @@
 // Each Chebyshev step on the SELL copy is one fused kernel (gather SpMV, residual update,
 // direction and iterate update; no reductions).  The matrix-free variant scatters with
 // FP32 atomics and finishes the step in a vector kernel.
+#include <algorithm>
 #include <cmath>
 #include <cuda_bf16.h>
 
@@ -735,6 +736,399 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         cont.done = 0;
         PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &cont, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
     }
+}
+
+// ---- batched flexible CG ------------------------------------------------------------------
+//
+// A batch is the disjoint union of independent problems, so its operator is block diagonal
+// and every member's Krylov recurrence only needs member-wise dot products.  The segmented
+// kernels below run one CTA per tile of at most kThreads rows of one member; each reduction
+// publishes per-tile partials and the last tile of a member to finish (per-member ticket)
+// sums that member's partials in tile order (deterministic) and updates its scalars.  Tiles
+// of converged members return at once.  The Chebyshev preconditioner kernels are row-local
+// and run over the whole union; the batch-wide PcgScalars::done is set when every member is
+// done and stops them.
+
+namespace {
+
+struct BatchView {
+    int32_t        nseg;
+    const int32_t* cta_seg;
+    const int32_t* cta_row0;
+    const int32_t* cta_row1;
+    const int32_t* seg_cta0;
+    SegScalars*    S;
+    PcgScalars*    G;
+    int32_t*       ndone;
+    double*        partials;
+};
+
+template <int NV>
+__device__ __forceinline__ bool seg_publish(const BatchView& B, int s, double (&v)[NV], double (*sh)[32],
+                                            bool* sh_last) {
+    block_sum_n<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) B.partials[NV * blockIdx.x + q] = v[q];
+        __threadfence();
+        const unsigned tiles = unsigned(B.seg_cta0[s + 1] - B.seg_cta0[s]);
+        *sh_last = atomicAdd(&B.S[s].ticket, 1u) == tiles - 1u;
+    }
+    __syncthreads();
+    return *sh_last;
+}
+
+template <int NV>
+__device__ __forceinline__ void seg_final(const BatchView& B, int s, double (&t)[NV], double (*sh)[32]) {
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) t[q] = 0.0;
+    for (int c = B.seg_cta0[s] + threadIdx.x; c < B.seg_cta0[s + 1]; c += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) t[q] += B.partials[NV * c + q];
+    block_sum_n<NV>(t, sh);
+}
+
+// thread 0 of a member's last tile, when the member turns done
+__device__ __forceinline__ void seg_mark_done(const BatchView& B) {
+    if (atomicAdd(B.ndone, 1) + 1 == B.nseg) B.G->done = 1;
+}
+
+// r = b - A x (A x in r on entry), r.r and b.b per member; starts the preconditioner.
+// accept scales the stop test (1 on the first pass, the true-residual slack on restarts).
+__global__ void __launch_bounds__(kThreads)
+k_bfcg_start(BatchView B, const double* __restrict__ b, double* __restrict__ r, const float* __restrict__ dinv32,
+             float* __restrict__ res, float* __restrict__ d, float* __restrict__ y, float c0, double tol,
+             int keep_bb, double accept) {
+    __shared__ double sh[2][32];
+    __shared__ bool last;
+    const int s = B.cta_seg[blockIdx.x];
+    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (row < B.cta_row1[blockIdx.x]) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * row + i;
+            const double ri = b[k] - r[k];
+            r[k] = ri;
+            v[0] += ri * ri;
+            v[1] += b[k] * b[k];
+            const float rf = float(ri);
+            const float di = c0 * dinv32[k] * rf;
+            res[k] = rf;
+            d[k] = di;
+            y[k] = di;
+        }
+    }
+    if (seg_publish<2>(B, s, v, sh, &last)) {
+        double t[2];
+        seg_final<2>(B, s, t, sh);
+        if (threadIdx.x == 0) {
+            SegScalars& S = B.S[s];
+            S.rr = t[0];
+            if (!keep_bb) {
+                S.bb = t[1];
+                S.tol2 = tol * tol * t[1];
+                S.iter = 0;
+            }
+            S.nonfinite = (!isfinite(t[0]) || !isfinite(t[1])) ? 1 : 0;
+            S.done = (t[0] <= accept * accept * S.tol2 || S.nonfinite) ? 1 : 0;
+            if (S.done) seg_mark_done(B);
+            S.ticket = 0u;
+        }
+    }
+}
+
+// q = A p (FP64 SELL rows of the tile), p.q per member -> alpha = (p.r)/(p.q)
+__global__ void __launch_bounds__(kThreads)
+k_bfcg_apply(BatchView B, SellView A, const double* __restrict__ vals, const double* __restrict__ p,
+             double* __restrict__ q) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    const int s = B.cta_seg[blockIdx.x];
+    if (B.S[s].done) return;
+    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
+    double v[1] = {0.0};
+    if (row < B.cta_row1[blockIdx.x]) {
+        double a0, a1, a2;
+        sell_row<double>(A, vals, p, row, a0, a1, a2);
+        q[3 * row] = a0;
+        q[3 * row + 1] = a1;
+        q[3 * row + 2] = a2;
+        v[0] = p[3 * row] * a0 + p[3 * row + 1] * a1 + p[3 * row + 2] * a2;
+    }
+    if (seg_publish<1>(B, s, v, sh, &last)) {
+        double t[1];
+        seg_final<1>(B, s, t, sh);
+        if (threadIdx.x == 0) {
+            SegScalars& S = B.S[s];
+            S.pq = t[0];
+            S.alpha = S.pr / t[0];
+            if (!isfinite(S.alpha) || t[0] <= 0.0) {
+                S.nonfinite = 1;
+                S.done = 1;
+                seg_mark_done(B);
+            }
+            S.ticket = 0u;
+        }
+    }
+}
+
+// x += alpha p; r -= alpha q; r.r and the member's stop test; starts the preconditioner.
+// Tiles of converged members clear their preconditioner vectors instead.
+__global__ void __launch_bounds__(kThreads)
+k_bfcg_update(BatchView B, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+              const double* __restrict__ q, const float* __restrict__ dinv32, float* __restrict__ res,
+              float* __restrict__ d, float* __restrict__ y, float c0, int32_t max_it) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    const int s = B.cta_seg[blockIdx.x];
+    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
+    const bool in = row < B.cta_row1[blockIdx.x];
+    if (B.S[s].done) {
+        if (in)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) res[3 * row + i] = d[3 * row + i] = y[3 * row + i] = 0.f;
+        return;
+    }
+    const double alpha = B.S[s].alpha;
+    double v[1] = {0.0};
+    if (in) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * row + i;
+            x[k] += alpha * p[k];
+            const double ri = r[k] - alpha * q[k];
+            r[k] = ri;
+            v[0] += ri * ri;
+            const float rf = float(ri);
+            const float di = c0 * dinv32[k] * rf;
+            res[k] = rf;
+            d[k] = di;
+            y[k] = di;
+        }
+    }
+    if (seg_publish<1>(B, s, v, sh, &last)) {
+        double t[1];
+        seg_final<1>(B, s, t, sh);
+        if (threadIdx.x == 0) {
+            SegScalars& S = B.S[s];
+            S.rr = t[0];
+            S.iter += 1;
+            if (!isfinite(t[0])) S.nonfinite = 1;
+            if (S.nonfinite || t[0] <= S.tol2 || S.iter >= max_it) {
+                S.done = 1;
+                seg_mark_done(B);
+            }
+            S.ticket = 0u;
+        }
+    }
+}
+
+// z = y (widened); z.q per member -> beta = -(z.q)/(p.q).  first: only z = y.
+__global__ void __launch_bounds__(kThreads)
+k_bfcg_zq(BatchView B, const float* __restrict__ y, double* __restrict__ z, const double* __restrict__ q, int first) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    const int s = B.cta_seg[blockIdx.x];
+    if (B.S[s].done) return;
+    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
+    const bool in = row < B.cta_row1[blockIdx.x];
+    double v[1] = {0.0};
+    if (in)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * row + i;
+            const double zi = double(y[k]);
+            z[k] = zi;
+            if (!first) v[0] += zi * q[k];
+        }
+    if (first) return;
+    if (seg_publish<1>(B, s, v, sh, &last)) {
+        double t[1];
+        seg_final<1>(B, s, t, sh);
+        if (threadIdx.x == 0) {
+            SegScalars& S = B.S[s];
+            S.zq = t[0];
+            S.beta = -t[0] / S.pq;
+            if (!isfinite(S.beta)) {
+                S.nonfinite = 1;
+                S.done = 1;
+                seg_mark_done(B);
+            }
+            S.ticket = 0u;
+        }
+    }
+}
+
+// p = z + beta p; p.r per member.
+__global__ void __launch_bounds__(kThreads)
+k_bfcg_direction(BatchView B, const double* __restrict__ z, double* __restrict__ p, const double* __restrict__ r,
+                 int first) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    const int s = B.cta_seg[blockIdx.x];
+    if (B.S[s].done) return;
+    const double beta = first ? 0.0 : B.S[s].beta;
+    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
+    double v[1] = {0.0};
+    if (row < B.cta_row1[blockIdx.x])
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * row + i;
+            const double pi = z[k] + (first ? 0.0 : beta * p[k]);
+            p[k] = pi;
+            v[0] += pi * r[k];
+        }
+    if (seg_publish<1>(B, s, v, sh, &last)) {
+        double t[1];
+        seg_final<1>(B, s, t, sh);
+        if (threadIdx.x == 0) {
+            SegScalars& S = B.S[s];
+            S.pr = t[0];
+            if (!isfinite(t[0])) {
+                S.nonfinite = 1;
+                S.done = 1;
+                seg_mark_done(B);
+            }
+            S.ticket = 0u;
+        }
+    }
+}
+
+}  // namespace
+
+// Batched flexible CG with the Chebyshev-Jacobi preconditioner on the assembled union
+// operator (SELL copies prepared by prepare_mixed); x holds the initial guess.  Every member
+// stops on its own residual test ||r_s|| <= tol ||b_s||, confirmed with its recomputed true
+// residual; per-member statistics go to h->batch.last, the aggregate to *stats.
+int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
+    BatchState& bt = h->batch;
+    const int64_t n = 3 * (int64_t)h->N;
+    cudaStream_t s = h->stream;
+    const double tol = h->opts.tolerance;
+    const int32_t max_it = h->opts.max_iterations;
+    const int degree = h->opts.chebyshev_degree < 1 ? 1 : (h->opts.chebyshev_degree > 64 ? 64 : h->opts.chebyshev_degree);
+    const int kind = inner_kind(h);
+    const int VB = grid_for(n, kThreads, 148 * 16);
+    const int SB = spmv_blocks(h);
+    const SellView V = sell_view(h);
+    const int T = bt.ncta;
+    const BatchView BV{bt.nseg, bt.cta_seg, bt.cta_row0, bt.cta_row1, bt.seg_cta0, bt.S, h->scal, bt.ndone,
+                       bt.partials};
+
+    double lmax = 0.0;
+    int rc = estimate_lambda_max(h, kind, 20, &lmax);
+    if (rc) return rc;
+    const double safety = kind == INNER_SELL16 ? 1.15 : 1.10;
+    const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree);
+
+    auto chebyshev_steps = [&]() -> int {
+        float* dcur = h->f_d0;
+        float* dnext = h->f_d1;
+        for (int k = 1; k < degree; ++k) {
+            if (kind == INNER_SELL16)
+                k_cheb_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+            else if (kind == INNER_SELL32)
+                k_cheb_sell<INNER_SELL32><<<SB, kThreads, 0, s>>>(V, h->sell32, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+            else
+                k_cheb_sell<INNER_SELL64><<<SB, kThreads, 0, s>>>(V, h->sell64, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+            PLATO_LAUNCH_CHECK(h);
+            std::swap(dcur, dnext);
+        }
+        return PLATO_OK;
+    };
+
+    PcgScalars init{};
+    PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
+    PLATO_CUDA(h, cudaMemsetAsync(bt.S, 0, sizeof(SegScalars) * bt.nseg, s));
+    constexpr int kMaxPasses = 4;  // first pass + restarts from the true residual
+    constexpr double kSlack = 10.0;
+    int64_t precond_applies = 0;
+    cudaEvent_t ev[2];
+    PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    auto destroy_events = [&]() { cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]); };
+    int pass = 0;
+    for (;; ++pass) {
+        // r = b - A x; members whose (true) residual passes are done
+        PLATO_CUDA(h, cudaMemsetAsync(bt.ndone, 0, sizeof(int32_t), s));
+        PLATO_CUDA(h, cudaMemsetAsync(&h->scal->done, 0, sizeof(int32_t), s));
+        rc = launch_sell_spmv(h, h->sell64, x, h->v_r);
+        if (rc) { destroy_events(); return rc; }
+        k_bfcg_start<<<T, kThreads, 0, s>>>(BV, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, tol,
+                                             pass > 0 ? 1 : 0, pass > 0 ? kSlack : 1.0);
+        PLATO_LAUNCH_CHECK(h);
+        PcgScalars* slots = h->scal_host;
+        PLATO_CUDA(h, cudaMemcpyAsync(&slots[0], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
+        PLATO_CUDA(h, cudaStreamSynchronize(s));
+        if (slots[0].done || pass == kMaxPasses - 1) break;
+        // z = M r, p = z, p.r
+        rc = chebyshev_steps();
+        if (rc) { destroy_events(); return rc; }
+        k_bfcg_zq<<<T, kThreads, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 1);
+        k_bfcg_direction<<<T, kThreads, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 1);
+        h->launches += 2;
+        PLATO_LAUNCH_CHECK(h);
+        int cur = 0;
+        bool have_prev = false;
+        for (;;) {
+            for (int k = 0; k < kChunk; ++k) {
+                k_bfcg_apply<<<T, kThreads, 0, s>>>(BV, V, h->sell64, h->v_p, h->v_q);
+                k_bfcg_update<<<T, kThreads, 0, s>>>(BV, x, h->v_r, h->v_p, h->v_q, h->f_dinv, h->f_res, h->f_d0,
+                                                      h->f_y, cc.c0, max_it);
+                h->launches += 2;
+                rc = chebyshev_steps();
+                if (rc) { destroy_events(); return rc; }
+                k_bfcg_zq<<<T, kThreads, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 0);
+                k_bfcg_direction<<<T, kThreads, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 0);
+                h->launches += 2;
+                PLATO_LAUNCH_CHECK(h);
+                precond_applies += degree - 1;
+            }
+            PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
+            PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
+            if (have_prev) {
+                PLATO_CUDA(h, cudaEventSynchronize(ev[cur ^ 1]));
+                if (slots[cur ^ 1].done) break;
+            }
+            have_prev = true;
+            cur ^= 1;
+        }
+        PLATO_CUDA(h, cudaStreamSynchronize(s));
+    }
+    destroy_events();
+    PLATO_CUDA(h, cudaMemcpyAsync(bt.S_host, bt.S, sizeof(SegScalars) * bt.nseg, cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA(h, cudaStreamSynchronize(s));
+    bt.last.assign(bt.nseg, plato_solve_stats{});
+    plato_solve_stats agg{};
+    agg.converged = 1;
+    agg.status = PLATO_OK;
+    for (int m = 0; m < bt.nseg; ++m) {
+        const SegScalars& S = bt.S_host[m];
+        plato_solve_stats& st = bt.last[m];
+        st.iterations = S.iter;
+        st.refinements = int32_t(precond_applies);
+        st.relative_residual = S.bb > 0.0 ? std::sqrt(S.rr / S.bb) : 0.0;
+        const bool ok = !S.nonfinite && S.done && (S.bb == 0.0 || st.relative_residual <= kSlack * tol) &&
+                        (S.iter < max_it || st.relative_residual <= tol);
+        st.converged = ok ? 1 : 0;
+        st.status = S.nonfinite ? PLATO_NONFINITE : (ok ? PLATO_OK : PLATO_NOT_CONVERGED);
+        agg.iterations = std::max(agg.iterations, st.iterations);
+        agg.relative_residual = std::max(agg.relative_residual, S.nonfinite ? NAN : st.relative_residual);
+        if (!ok) agg.converged = 0;
+        if (st.status != PLATO_OK && agg.status != PLATO_NONFINITE) agg.status = st.status;
+    }
+    agg.refinements = int32_t(precond_applies);
+    *stats = agg;
+    if (agg.status == PLATO_NONFINITE)
+        return plato_fail(h, PLATO_NONFINITE, "non-finite value or loss of positivity in a batch member's solve");
+    if (agg.status != PLATO_OK)
+        return plato_fail(h, PLATO_NOT_CONVERGED, "a batch member stopped before ||b - A x|| <= tol ||b||");
+    return PLATO_OK;
 }
 
 }  // namespace plato

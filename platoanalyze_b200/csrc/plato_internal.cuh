@@ -61,6 +61,42 @@ struct PcgScalars {
     uint32_t ticket; // last-block-done counter of the fused reductions
 };
 
+// Per-problem Krylov state of a batched solve (one entry per member problem).
+struct SegScalars {
+    double pr;       // p . r
+    double pq;       // p . A p
+    double alpha;
+    double beta;
+    double zq;       // z . A p
+    double rr;       // r . r
+    double bb;       // b . b
+    double tol2;     // tol^2 * b.b
+    int32_t iter;
+    int32_t done;
+    int32_t nonfinite;
+    uint32_t ticket; // last-CTA-done counter of the member's reductions
+};
+
+// Batch of independent problems stored as one disjoint-union mesh (batch.cu).  Member s owns
+// node rows [node_off[s], node_off[s+1]) and cells [cell_off[s], cell_off[s+1]); the
+// segmented solver kernels run one CTA per tile of at most 256 rows of one member.
+struct BatchState {
+    int32_t  nseg = 0;                 // 0 for a single problem
+    std::vector<int32_t> node_off, cell_off;
+    int32_t  ncta = 0;
+    int32_t* cta_seg = nullptr;        // [ncta] member of each tile
+    int32_t* cta_row0 = nullptr;       // [ncta] first row of each tile
+    int32_t* cta_row1 = nullptr;       // [ncta] one past its last row
+    int32_t* seg_cta0 = nullptr;       // [nseg+1] first tile of each member
+    int32_t* cell_off_d = nullptr;     // [nseg+1] on the device
+    SegScalars* S = nullptr;           // [nseg] device
+    SegScalars* S_host = nullptr;      // [nseg] pinned
+    int32_t* ndone = nullptr;          // members done (device)
+    double*  partials = nullptr;       // [2*ncta]
+    double*  values = nullptr;         // [nseg * kEnergySplit] criterion partial sums
+    std::vector<plato_solve_stats> last;  // per-member statistics of the last solve
+};
+
 // Two-level preconditioner state (coarse.cu).
 struct CoarseSpace {
     int      nc[3] = {0, 0, 0};   // coarse cells per axis
@@ -178,6 +214,7 @@ struct plato_problem {
     cudaEvent_t asm_ev[2] = {nullptr, nullptr};  // Jacobian assembly of the solve path
     double  asm_ms_total = 0.0;
     int64_t asm_timed = 0;
+    BatchState batch{};
 };
 
 // ---------------------------------------------------------------------------------------
@@ -188,6 +225,10 @@ int coarse_setup_mesh(plato_problem* h);
 int coarse_setup_operator(plato_problem* h, const double* z);
 int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S);
 void coarse_release(plato_problem* h);
+void batch_release(plato_problem* h);
+int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
+constexpr int kEnergySplit = 32;  // CTAs per member in the batched criterion sum
+int launch_energy_segments(plato_problem* h, const double* u, const double* z, double* values);
 }  // namespace plato
 int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const char* file, int line);
 

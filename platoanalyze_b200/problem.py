@@ -65,45 +65,92 @@ def cantilever_spec(mesh: BoxMesh, traction=(0.0, -1.0, 0.0), E=1.0, nu=0.3, p=3
                        [(cells, local, traction)], dofs, np.zeros(dofs.size), solver or SolverOptions())
 
 
+def _problem_desc(spec: ProblemSpec, keep: list) -> capi.ProblemDesc:
+    """C description of a problem; the arrays it points to are appended to `keep`."""
+    coords = np.ascontiguousarray(spec.coords, dtype=np.float64)
+    conn = np.ascontiguousarray(spec.connectivity, dtype=np.int32)
+    keep += [coords, conn]
+    nbcs = (capi.NaturalBC * max(1, len(spec.tractions)))()
+    keep.append(nbcs)
+    for k, (cells, local, vec) in enumerate(spec.tractions):
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        local = np.ascontiguousarray(local, dtype=np.int32)
+        keep += [cells, local]
+        nbcs[k].num_faces = cells.size
+        nbcs[k].face_cells = cells.ctypes.data_as(capi.i32p)
+        nbcs[k].face_local_nodes = local.ctypes.data_as(capi.i32p)
+        nbcs[k].vector = (C.c_double * 3)(*vec)
+    dofs = np.ascontiguousarray(spec.bc_dofs, dtype=np.int32)
+    vals = np.ascontiguousarray(spec.bc_values, dtype=np.float64)
+    keep += [dofs, vals]
+    desc = capi.ProblemDesc()
+    desc.mesh = capi.MeshDesc(coords.shape[0], conn.shape[0], coords.ctypes.data_as(capi.f64p),
+                              conn.ctypes.data_as(capi.i32p))
+    desc.material = capi.Material(spec.youngs_modulus, spec.poissons_ratio)
+    desc.penalty = capi.Penalty(spec.penalty_exponent, spec.penalty_minimum)
+    desc.num_natural_bcs = len(spec.tractions)
+    desc.natural_bcs = nbcs
+    desc.essential_bcs = capi.EssentialBCs(dofs.size, dofs.ctypes.data_as(capi.i32p), vals.ctypes.data_as(capi.f64p))
+    desc.solver = spec.solver.to_c()
+    return desc
+
+
 class EllipticProblem:
-    def __init__(self, spec: ProblemSpec, stream=None):
+    """Elliptic::Problem with its VectorFunction and compliance criterion on one GPU.
+
+    EllipticProblem.batch(specs) builds one handle over several independent problems (their
+    disjoint union); node_offsets / cell_offsets locate each member in the union's vectors.
+    """
+
+    def __init__(self, spec: ProblemSpec, stream=None, _batch: list | None = None):
         import torch  # device memory and streams only
 
         self.torch = torch
         self.spec = spec
-        coords = np.ascontiguousarray(spec.coords, dtype=np.float64)
-        conn = np.ascontiguousarray(spec.connectivity, dtype=np.int32)
-        self._keep = [coords, conn]
-        nbcs = (capi.NaturalBC * max(1, len(spec.tractions)))()
-        for k, (cells, local, vec) in enumerate(spec.tractions):
-            cells = np.ascontiguousarray(cells, dtype=np.int32)
-            local = np.ascontiguousarray(local, dtype=np.int32)
-            self._keep += [cells, local]
-            nbcs[k].num_faces = cells.size
-            nbcs[k].face_cells = cells.ctypes.data_as(capi.i32p)
-            nbcs[k].face_local_nodes = local.ctypes.data_as(capi.i32p)
-            nbcs[k].vector = (C.c_double * 3)(*vec)
-        dofs = np.ascontiguousarray(spec.bc_dofs, dtype=np.int32)
-        vals = np.ascontiguousarray(spec.bc_values, dtype=np.float64)
-        self._keep += [dofs, vals]
-        desc = capi.ProblemDesc()
-        desc.mesh = capi.MeshDesc(coords.shape[0], conn.shape[0], coords.ctypes.data_as(capi.f64p),
-                                  conn.ctypes.data_as(capi.i32p))
-        desc.material = capi.Material(spec.youngs_modulus, spec.poissons_ratio)
-        desc.penalty = capi.Penalty(spec.penalty_exponent, spec.penalty_minimum)
-        desc.num_natural_bcs = len(spec.tractions)
-        desc.natural_bcs = nbcs
-        desc.essential_bcs = capi.EssentialBCs(dofs.size, dofs.ctypes.data_as(capi.i32p),
-                                               vals.ctypes.data_as(capi.f64p))
-        desc.solver = spec.solver.to_c()
+        self._keep = []
         h = C.c_void_p()
-        check(lib.plato_create(C.byref(desc), C.byref(h)))
+        if _batch is None:
+            desc = _problem_desc(spec, self._keep)
+            check(lib.plato_create(C.byref(desc), C.byref(h)))
+        else:
+            descs = (capi.ProblemDesc * len(_batch))()
+            for k, sp in enumerate(_batch):
+                descs[k] = _problem_desc(sp, self._keep)
+            check(lib.plato_create_batch(len(_batch), descs, C.byref(h)))
         self.h = h
         self.set_stream(stream if stream is not None else torch.cuda.current_stream())
         nn, nc, nb = C.c_int32(), C.c_int32(), C.c_int64()
         check(lib.plato_get_sizes(h, C.byref(nn), C.byref(nc), C.byref(nb)), h)
         self.num_nodes, self.num_cells, self.num_blocks = nn.value, nc.value, nb.value
         self.num_dofs = 3 * self.num_nodes
+        cnt = C.c_int32()
+        check(lib.plato_batch_info(h, C.byref(cnt), None, None), h)
+        self.count = cnt.value
+        self.node_offsets = np.zeros(self.count + 1, np.int32)
+        self.cell_offsets = np.zeros(self.count + 1, np.int32)
+        check(lib.plato_batch_info(h, None, self.node_offsets.ctypes.data_as(capi.i32p),
+                                   self.cell_offsets.ctypes.data_as(capi.i32p)), h)
+
+    @classmethod
+    def batch(cls, specs: list, stream=None) -> "EllipticProblem":
+        """One handle over independent problems (shared material and penalty; solver options of
+        specs[0]); solves run every member to its own tolerance in one batched flexible CG."""
+        return cls(specs[0], stream, _batch=list(specs))
+
+    def member_slices(self, dofs_per_node: int = 3):
+        """Slices of member s in union node vectors with dofs_per_node entries per node."""
+        o = self.node_offsets
+        return [slice(dofs_per_node * int(o[s]), dofs_per_node * int(o[s + 1])) for s in range(self.count)]
+
+    def batch_last_stats(self) -> list:
+        st = (capi.SolveStats * self.count)()
+        check(lib.plato_batch_last_stats(self.h, st), self.h)
+        return [x.as_dict() for x in st]
+
+    def batch_criterion_values(self, z, u) -> np.ndarray:
+        v = self.zeros(self.count)
+        check(lib.plato_batch_criterion_values(self.h, self._dev(z), self._dev(u), self._dev(v)), self.h)
+        return v.cpu().numpy()
 
     # -- plumbing ------------------------------------------------------------------------
     def set_stream(self, stream) -> None:

@@ -16,6 +16,8 @@ from .problem import ProblemSpec, SolverOptions, cantilever_spec
 
 SEED_LARGE = 0x5EED0002
 SEED_MIXED = 0x5EED0003
+SEED_BATCH = 0x5EED0004
+BATCH_SIZES = (16, 24, 32, 48, 64)
 
 
 def splitmix_uniform(n: int, seed: int, lo: float = 0.01, hi: float = 1.0) -> np.ndarray:
@@ -77,3 +79,39 @@ def method_options(method: str, tol: float = 1e-10, coarse=COARSE_BOX) -> Solver
         return SolverOptions(tolerance=tol, max_iterations=200000, operator_kind=capi.OPERATOR_MATRIX_FREE,
                              precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=16)
     raise ValueError(f"unknown method {method!r}; one of {METHODS}")
+
+
+def grf_density(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), corr: float = 0.1,
+                rng: np.random.Generator | None = None) -> np.ndarray:
+    """Nodal density on the (nx+1)(ny+1)(nz+1) box-mesh nodes (z fastest): a stationary
+    Gaussian random field with covariance exp(-r^2 / (2 corr^2)), sampled by filtering white
+    noise in Fourier space (spectral density exp(-|k|^2 corr^2 / 2)), standardised to zero
+    mean and unit variance, passed through the logistic function and clipped to [0.01, 1]."""
+    rng = rng or np.random.default_rng(0)
+    shape = (nx + 1, ny + 1, nz + 1)
+    h = [lengths[0] / nx, lengths[1] / ny, lengths[2] / nz]
+    noise = rng.standard_normal(shape)
+    k = np.meshgrid(*[2 * np.pi * np.fft.fftfreq(m, d=hh) for m, hh in zip(shape, h)], indexing="ij")
+    k2 = k[0] ** 2 + k[1] ** 2 + k[2] ** 2
+    field = np.real(np.fft.ifftn(np.fft.fftn(noise) * np.exp(-0.25 * k2 * corr * corr)))
+    field = (field - field.mean()) / max(field.std(), 1e-300)
+    return np.clip(1.0 / (1.0 + np.exp(-field)), 0.01, 1.0).reshape(-1)
+
+
+def batch_workload(count: int = 64, seed: int = SEED_BATCH, sizes=BATCH_SIZES,
+                   solver: SolverOptions | None = None):
+    """Independent cantilevers n x n/2 x n/2 hexes x 6 tets on [0,2]x[0,1]x[0,1], n drawn
+    uniformly from `sizes`; density from grf_density; traction on the x = 2 face with a
+    direction uniform on the unit sphere and magnitude 1.  Returns (specs, densities, ns)."""
+    rng = np.random.default_rng(seed)
+    specs, zs, ns = [], [], []
+    for _ in range(count):
+        n = int(rng.choice(np.asarray(sizes)))
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        mesh = box_mesh(n, n // 2, n // 2, 2.0, 1.0, 1.0)
+        specs.append(cantilever_spec(mesh, traction=tuple(float(v) for v in d), E=1.0, nu=0.3, p=3.0,
+                                     rho_min=1e-9, solver=solver))
+        zs.append(grf_density(n, n // 2, n // 2, rng=rng))
+        ns.append(n)
+    return specs, zs, ns

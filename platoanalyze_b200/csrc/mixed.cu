@@ -996,6 +996,38 @@ k_bfcg_direction(BatchView B, const double* __restrict__ z, double* __restrict__
     }
 }
 
+// One Chebyshev step over the tiles of members still iterating (converged members' rows
+// are skipped): w = A d_cur, res -= w, d_next = c1 d_cur + c2 Dinv res, y += d_next.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads)
+k_bcheb_sell(BatchView B, SellView A, const void* __restrict__ vals, const float* __restrict__ dinv32,
+             float* __restrict__ res, const float* __restrict__ dcur, float* __restrict__ dnext, float* __restrict__ y,
+             float c1, float c2) {
+    if (B.S[B.cta_seg[blockIdx.x]].done) return;
+    const int64_t r = B.cta_row0[blockIdx.x] + threadIdx.x;
+    if (r >= B.cta_row1[blockIdx.x]) return;
+    float w0, w1, w2;
+    if (KIND == INNER_SELL16)
+        sell_row_bf16(A, static_cast<const __nv_bfloat16*>(vals), dcur, r, w0, w1, w2);
+    else if (KIND == INNER_SELL32)
+        sell_row<float>(A, static_cast<const float*>(vals), dcur, r, w0, w1, w2);
+    else {
+        double a0, a1, a2;
+        sell_row<double>(A, static_cast<const double*>(vals), dcur, r, a0, a1, a2);
+        w0 = float(a0); w1 = float(a1); w2 = float(a2);
+    }
+    const float w[3] = {w0, w1, w2};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int64_t k = 3 * r + i;
+        const float rs = res[k] - w[i];
+        res[k] = rs;
+        const float dn = c1 * dcur[k] + c2 * dinv32[k] * rs;
+        dnext[k] = dn;
+        y[k] += dn;
+    }
+}
+
 }  // namespace
 
 // Batched flexible CG with the Chebyshev-Jacobi preconditioner on the assembled union
@@ -1010,8 +1042,6 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
     const int32_t max_it = h->opts.max_iterations;
     const int degree = h->opts.chebyshev_degree < 1 ? 1 : (h->opts.chebyshev_degree > 64 ? 64 : h->opts.chebyshev_degree);
     const int kind = inner_kind(h);
-    const int VB = grid_for(n, kThreads, 148 * 16);
-    const int SB = spmv_blocks(h);
     const SellView V = sell_view(h);
     const int T = bt.ncta;
     const BatchView BV{bt.nseg, bt.cta_seg, bt.cta_row0, bt.cta_row1, bt.seg_cta0, bt.S, h->scal, bt.ndone,
@@ -1028,14 +1058,14 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         float* dnext = h->f_d1;
         for (int k = 1; k < degree; ++k) {
             if (kind == INNER_SELL16)
-                k_cheb_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
-                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                k_bcheb_sell<INNER_SELL16><<<T, kThreads, 0, s>>>(BV, V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k]);
             else if (kind == INNER_SELL32)
-                k_cheb_sell<INNER_SELL32><<<SB, kThreads, 0, s>>>(V, h->sell32, h->f_dinv, h->f_res, dcur, dnext,
-                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                k_bcheb_sell<INNER_SELL32><<<T, kThreads, 0, s>>>(BV, V, h->sell32, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k]);
             else
-                k_cheb_sell<INNER_SELL64><<<SB, kThreads, 0, s>>>(V, h->sell64, h->f_dinv, h->f_res, dcur, dnext,
-                                                                  h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                k_bcheb_sell<INNER_SELL64><<<T, kThreads, 0, s>>>(BV, V, h->sell64, h->f_dinv, h->f_res, dcur, dnext,
+                                                                  h->f_y, cc.c1[k], cc.c2[k]);
             PLATO_LAUNCH_CHECK(h);
             std::swap(dcur, dnext);
         }

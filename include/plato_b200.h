@@ -264,6 +264,59 @@ int plato_batch_last_stats(const plato_problem* h, plato_solve_stats* stats);
  * each member) into values[count] [device]; synchronises the handle's stream */
 int plato_batch_criterion_values(plato_problem* h, const double* z, const double* u, double* values);
 
+/* Problem::solution with an initial guess improved on a subspace (no reference counterpart;
+ * the learned warm start uses it).  W holds k <= 8 columns of 3N values [device]; after the
+ * operator is assembled and constrained, the iterate x (u0, or zero) becomes x + P W c with
+ * (W^T P K P W) c = W^T P (b - K x) (P zeroes the constrained dofs): the minimiser of the
+ * energy error over x + span(P W).  The correction is dropped (x kept) when the Gram matrix
+ * is not positive definite or ||b - K x|| would become non-finite or grow more than 10x; the
+ * solve then runs to the usual tolerance.  *residual_ratio (may be NULL) receives ||b - K x||
+ * after / before the correction (1 when it was dropped).  Single problems on the assembled
+ * operator only. */
+int plato_problem_solution_subspace(plato_problem* h, const double* z, const double* u0, const double* W, int32_t k,
+                                    double* u, plato_solve_stats* stats, double* residual_ratio);
+
+/* ---- learned warm start (no reference counterpart) -------------------------------------
+ * A 3-level 3D U-Net (16-32-64 channels; 3x3x3 convolutions with ReLU, 2x2x2 average pooling,
+ * nearest upsampling, skip concatenation, 1x1x1 head) on the nodes of an n0 x n1 x n2 box
+ * node grid (zero-padded to multiples of 4).  Input: 8 FP32 features per node
+ * [batch][n0][n1][n2][8]; output: 9 FP32 values per node [batch][n0][n1][n2][9].  BF16
+ * tensor-core kernels with FP32 accumulation for every convolution, forward and backward;
+ * FP32 parameters trained with Adam.  All array arguments are [device]; work is issued on the
+ * network's stream; errors read through plato_unet_last_error(). */
+typedef struct plato_unet plato_unet;
+int plato_unet_create(const int32_t nodes[3], int32_t max_batch, plato_unet** out);
+int plato_unet_destroy(plato_unet* net);
+int plato_unet_set_stream(plato_unet* net, void* cuda_stream);
+const char* plato_unet_last_error(void);
+int plato_unet_num_params(const plato_unet* net, int64_t* count);
+/* parameters: per layer, weights [taps][cout][cin] then bias [cout]; setting them resets Adam */
+int plato_unet_set_params(plato_unet* net, const float* params);
+int plato_unet_get_params(const plato_unet* net, float* params);
+int plato_unet_forward(plato_unet* net, int32_t batch, const float* input, float* output);
+/* mean squared error against target [batch][n0][n1][n2][9] and the parameter gradient (kept
+ * for plato_unet_adam_step; also copied to grads when non-NULL); *loss is a [host] double */
+int plato_unet_loss_and_gradients(plato_unet* net, int32_t batch, const float* input, const float* target,
+                                  double* loss, float* grads);
+int plato_unet_adam_step(plato_unet* net, float learning_rate, int32_t step);
+/* network input for a box design: the 8 features per node of the net_nodes grid (density
+ * interpolated trilinearly from the src_nodes grid's nodal z, loaded-face and clamped-face
+ * masks at the two x ends, normalised coordinates, density cubed, zero) into features [device] */
+int plato_unet_features(const int32_t src_nodes[3], const double* z, const int32_t net_nodes[3], float* features,
+                        void* cuda_stream);
+/* the 3 subspace columns W [3][3 * dst nodes] (column d = predicted response to a unit
+ * traction along axis d, trilinear from the network output [net nodes][9]) */
+int plato_unet_subspace(const int32_t net_nodes[3], const float* output, const int32_t dst_nodes[3], double* W,
+                        void* cuda_stream);
+/* `passes` 7-point averaging passes (each node becomes the mean of itself and its face
+ * neighbours) over FP32 data [nodes][channels] in place; scratch holds as many floats */
+int plato_box_smooth(const int32_t nodes[3], int32_t channels, int32_t passes, float* data, float* scratch,
+                     void* cuda_stream);
+/* trilinear resampling of `channels` FP64 values per node between two node grids spanning the
+ * same box (nodes ordered z fastest) */
+int plato_box_resample(const int32_t src_nodes[3], const int32_t dst_nodes[3], int32_t channels, const double* src,
+                       double* dst, void* cuda_stream);
+
 /* ---- box mesh generator (host only; stands in for BamG, unit_tests/PlatoTestHelpers.hpp) */
 int plato_box_mesh_sizes(int32_t nx, int32_t ny, int32_t nz, int32_t* num_nodes, int32_t* num_cells);
 int plato_box_mesh_tet4(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,

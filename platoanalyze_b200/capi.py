@@ -111,6 +111,21 @@ def _load() -> C.CDLL:
         "plato_batch_info": ([vp, i32p, i32p, i32p], C.c_int),
         "plato_batch_last_stats": ([vp, C.POINTER(SolveStats)], C.c_int),
         "plato_batch_criterion_values": ([vp, vp, vp, vp], C.c_int),
+        "plato_problem_solution_subspace": ([vp, vp, vp, vp, C.c_int32, vp, C.POINTER(SolveStats), f64p], C.c_int),
+        "plato_unet_create": ([i32p, C.c_int32, C.POINTER(vp)], C.c_int),
+        "plato_unet_destroy": ([vp], C.c_int),
+        "plato_unet_set_stream": ([vp, vp], C.c_int),
+        "plato_unet_last_error": ([], C.c_char_p),
+        "plato_unet_num_params": ([vp, C.POINTER(C.c_int64)], C.c_int),
+        "plato_unet_set_params": ([vp, vp], C.c_int),
+        "plato_unet_get_params": ([vp, vp], C.c_int),
+        "plato_unet_forward": ([vp, C.c_int32, vp, vp], C.c_int),
+        "plato_unet_loss_and_gradients": ([vp, C.c_int32, vp, vp, f64p, vp], C.c_int),
+        "plato_unet_adam_step": ([vp, C.c_float, C.c_int32], C.c_int),
+        "plato_unet_features": ([i32p, vp, i32p, vp, vp], C.c_int),
+        "plato_unet_subspace": ([i32p, vp, i32p, vp, vp], C.c_int),
+        "plato_box_smooth": ([i32p, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
+        "plato_box_resample": ([i32p, i32p, C.c_int32, vp, vp, vp], C.c_int),
         "plato_box_mesh_sizes": ([C.c_int32] * 3 + [i32p, i32p], C.c_int),
         "plato_box_mesh_tet4": ([C.c_int32] * 3 + [C.c_double] * 3 + [vp, vp], C.c_int),
         "plato_box_nodeset": ([C.c_int32] * 4 + [vp, i32p], C.c_int),

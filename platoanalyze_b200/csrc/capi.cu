@@ -133,6 +133,7 @@ int plato_destroy(plato_problem* h) {
         if (e) cudaEventDestroy(e);
     coarse_release(h);
     batch_release(h);
+    if (h->ritz_scratch) cudaFree(h->ritz_scratch);
     delete h;
     return PLATO_OK;
 }
@@ -464,6 +465,23 @@ int plato_problem_solution(plato_problem* h, const double* z, const double* u0, 
     return solve_state(h, z, u0, u, stats ? stats : &local);
 }
 
+int plato_problem_solution_subspace(plato_problem* h, const double* z, const double* u0, const double* W, int32_t k,
+                                    double* u, plato_solve_stats* stats, double* residual_ratio) {
+    NEED(h, z && u, "null device pointer");
+    NEED(h, k >= 0 && k <= 8 && (k == 0 || W), "subspace needs 0 <= k <= 8 columns");
+    if (k > 0 && (h->batch.nseg > 0 || h->opts.operator_kind != PLATO_OPERATOR_ASSEMBLED))
+        return plato_fail(h, PLATO_NOT_SUPPORTED, "subspace initial guesses need a single problem on the assembled operator");
+    plato_solve_stats local{};
+    h->ritz_W = W;
+    h->ritz_k = k;
+    h->ritz_rel_gain = 1.0;
+    const int rc = solve_state(h, z, u0, u, stats ? stats : &local);
+    h->ritz_W = nullptr;
+    h->ritz_k = 0;
+    if (residual_ratio) *residual_ratio = h->ritz_rel_gain;
+    return rc;
+}
+
 int plato_problem_criterion_value(plato_problem* h, const double* z, const double* u, double* value) {
     return plato_sf_value(h, u, z, value);
 }
@@ -557,10 +575,12 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         rc = fcg_batch(h, h->v_b, x, st);
     } else if (plain_method(h->opts)) {
         RC(prepare_operator(h, h->K));
+        RC(ritz_guess(h, h->v_b, x));
         rc = pcg_fp64(h, h->v_b, x, st);
     } else {
         RC(prepare_mixed(h, h->K, z));
         RC(prepare_coarse(h, z));
+        RC(ritz_guess(h, h->v_b, x));
         rc = fcg_poly(h, h->v_b, x, st);
     }
     if (h->timing) {  // the solver has synchronised the stream

@@ -215,6 +215,12 @@ struct plato_problem {
     double  asm_ms_total = 0.0;
     int64_t asm_timed = 0;
     BatchState batch{};
+    // subspace initial guess (ritz.cu): columns set for the duration of one solution call
+    const double* ritz_W = nullptr;
+    int32_t ritz_k = 0;
+    double* ritz_scratch = nullptr;
+    size_t  ritz_scratch_len = 0;
+    double  ritz_rel_gain = 1.0;   // ||r|| after / before the last subspace correction (1: not used)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -227,6 +233,7 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
 void coarse_release(plato_problem* h);
 void batch_release(plato_problem* h);
 int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
+int ritz_guess(plato_problem* h, const double* b, double* x);
 constexpr int kEnergySplit = 32;  // CTAs per member in the batched criterion sum
 int launch_energy_segments(plato_problem* h, const double* u, const double* z, double* values);
 }  // namespace plato

@@ -1,0 +1,990 @@
+// Learned warm start: a 3-level 3D U-Net (16-32-64 channels) on the nodes of a box mesh,
+// trained and evaluated with hand-written BF16 tensor-core kernels (no reference
+// counterpart: Plato Analyze has no learned component).
+//
+// Tensors are channels-last (b, d, h, w, c) with a one-voxel zero halo on every side, so a
+// 3x3x3 convolution with zero padding reads its neighbours without bounds checks; kernels
+// only ever write interior voxels.  Activations are BF16, activation gradients FP32,
+// parameters FP32 (Adam) with BF16 copies for the tensor cores.
+//
+//  * Convolution (forward and data gradient): implicit GEMM, M = voxels, N = output
+//    channels, K = taps x input channels, mma.sync.m16n8k16 BF16 -> FP32; each warp owns
+//    32 voxels x all output channels; A fragments are gathered straight from the haloed
+//    tensor (pairs of channels are 32-bit words), B fragments from the weights laid out
+//    [tap][out][in].  Bias, ReLU and FP32 accumulation are fused in the epilogue.  The data
+//    gradient is the same convolution with flipped, transposed weights.
+//  * Weight gradient: GEMM over voxels, M = output channels, N = input channels, K =
+//    voxels; a CTA stages 64-voxel tiles of the masked output gradient and of the shifted
+//    input in shared memory and feeds the tensor cores with ldmatrix.trans; partial sums
+//    are added to the FP32 gradient with atomics.
+//  * 2x2x2 average pooling, nearest upsampling, the ReLU gradient mask, the loss and Adam
+//    are element-wise kernels.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "plato_b200.h"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+std::string g_unet_error;
+
+int fail(int status, const std::string& msg) {
+    g_unet_error = msg;
+    return status;
+}
+
+#define UCUDA(expr)                                                                               \
+    do {                                                                                          \
+        cudaError_t _e = (expr);                                                                  \
+        if (_e != cudaSuccess) {                                                                  \
+            (void)cudaGetLastError();                                                             \
+            return fail(_e == cudaErrorMemoryAllocation ? PLATO_OUT_OF_MEMORY : PLATO_CUDA_ERROR, \
+                        std::string("CUDA error ") + cudaGetErrorName(_e) + " in " #expr);        \
+        }                                                                                         \
+    } while (0)
+
+#define ULAUNCH()                                                                              \
+    do {                                                                                       \
+        cudaError_t _e = cudaGetLastError();                                                   \
+        if (_e != cudaSuccess)                                                                 \
+            return fail(PLATO_CUDA_ERROR, std::string("kernel launch failed: ") + cudaGetErrorName(_e)); \
+    } while (0)
+
+// A channel slice [c0, c0 + C) of a haloed channels-last tensor with ld channels per voxel.
+struct TView {
+    void*   p;
+    int32_t ld, c0;
+    int32_t B, D, H, W;  // interior extents
+};
+
+__host__ __device__ __forceinline__ int64_t halo_index(const TView& t, int64_t v) {
+    const int64_t x = v % t.W;
+    int64_t r = v / t.W;
+    const int64_t y = r % t.H;
+    r /= t.H;
+    const int64_t z = r % t.D;
+    const int64_t b = r / t.D;
+    return ((b * (t.D + 2) + z + 1) * (t.H + 2) + y + 1) * (t.W + 2) + x + 1;
+}
+
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t ld32(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// ---- convolution: forward and data gradient ---------------------------------------------
+// out[v][co] (+)= act(bias[co] + sum_t sum_ci W[t][co][ci] in[v + o_t][ci]); TAPS = 27
+// (3x3x3, zero padding) or 1.  COUTP = COUT rounded up to 8 (weights padded with zeros).
+constexpr int kConvWarps = 4;
+constexpr int kMT = 2;  // 16-voxel m-tiles per warp
+
+template <int CIN, int COUT, int TAPS, bool RELU, bool OUT_F32, bool ACCUM>
+__global__ void __launch_bounds__(kConvWarps * 32)
+k_conv(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TView out, int64_t nvox) {
+    static_assert(CIN % 16 == 0, "input channels must be a multiple of 16");
+    constexpr int COUTP = (COUT + 7) / 8 * 8;
+    constexpr int NT = COUTP / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tig = lane & 3;
+    const int64_t vbase = (int64_t(blockIdx.x) * kConvWarps + warp) * (16 * kMT);
+    if (vbase >= nvox) return;
+    const bf16* __restrict__ ip = static_cast<const bf16*>(in.p);
+    // haloed voxel offsets of the rows this lane touches (rows g and g+8 of each m-tile)
+    int64_t rowoff[kMT][2];
+    bool rowok[kMT][2];
+#pragma unroll
+    for (int m = 0; m < kMT; ++m)
+#pragma unroll
+        for (int hlf = 0; hlf < 2; ++hlf) {
+            const int64_t v = vbase + 16 * m + g + 8 * hlf;
+            rowok[m][hlf] = v < nvox;
+            rowoff[m][hlf] = (rowok[m][hlf] ? halo_index(in, v) : 0) * in.ld + in.c0 + 2 * tig;
+        }
+    float acc[kMT][NT][4];
+#pragma unroll
+    for (int m = 0; m < kMT; ++m)
+#pragma unroll
+        for (int n = 0; n < NT; ++n)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[m][n][q] = 0.f;
+    const int64_t sy = in.W + 2, sz = int64_t(in.H + 2) * (in.W + 2);
+    for (int t = 0; t < TAPS; ++t) {
+        int64_t o = 0;
+        if (TAPS == 27) o = ((t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1)) * in.ld;
+        const bf16* __restrict__ wt = Wt + int64_t(t) * COUTP * CIN;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; ++kc) {
+            uint32_t a[kMT][4];
+#pragma unroll
+            for (int m = 0; m < kMT; ++m) {
+                const bf16* r0 = ip + rowoff[m][0] + o + 16 * kc;
+                const bf16* r1 = ip + rowoff[m][1] + o + 16 * kc;
+                a[m][0] = rowok[m][0] ? ld32(r0) : 0u;
+                a[m][1] = rowok[m][1] ? ld32(r1) : 0u;
+                a[m][2] = rowok[m][0] ? ld32(r0 + 8) : 0u;
+                a[m][3] = rowok[m][1] ? ld32(r1 + 8) : 0u;
+            }
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                const bf16* wp = wt + (8 * n + g) * CIN + 16 * kc + 2 * tig;
+                const uint32_t b0 = ld32(wp), b1 = ld32(wp + 8);
+#pragma unroll
+                for (int m = 0; m < kMT; ++m) mma16816(acc[m][n], a[m], b0, b1);
+            }
+        }
+    }
+    // epilogue: rows g / g+8, columns 8n + 2 tig + {0, 1}
+#pragma unroll
+    for (int m = 0; m < kMT; ++m)
+#pragma unroll
+        for (int hlf = 0; hlf < 2; ++hlf) {
+            const int64_t v = vbase + 16 * m + g + 8 * hlf;
+            if (v >= nvox) continue;
+            const int64_t base = halo_index(out, v) * out.ld + out.c0;
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                const int c = 8 * n + 2 * tig;
+                if (c >= COUT) continue;
+                float y0 = acc[m][n][2 * hlf], y1 = acc[m][n][2 * hlf + 1];
+                if (bias) {
+                    y0 += bias[c];
+                    if (c + 1 < COUT) y1 += bias[c + 1];
+                }
+                if (RELU) {
+                    y0 = fmaxf(y0, 0.f);
+                    y1 = fmaxf(y1, 0.f);
+                }
+                if (OUT_F32) {
+                    float* op = static_cast<float*>(out.p) + base + c;
+                    if (ACCUM) {
+                        op[0] += y0;
+                        if (c + 1 < COUT) op[1] += y1;
+                    } else {
+                        op[0] = y0;
+                        if (c + 1 < COUT) op[1] = y1;
+                    }
+                } else {
+                    *reinterpret_cast<uint32_t*>(static_cast<bf16*>(out.p) + base + c) = pack_bf16(y0, y1);
+                }
+            }
+        }
+}
+
+// ---- weight gradient --------------------------------------------------------------------
+// dW[t][co][ci] += sum_v dy[v][co] x[v + o_t][ci]; grid (voxel chunks, TAPS).
+constexpr int kWgVox = 64;    // voxels per shared-memory tile
+constexpr int kWgTiles = 8;   // tiles per CTA
+
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const bf16* p) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2_t(uint32_t& r0, uint32_t& r1, const bf16* p) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+
+template <int CIN, int COUT, int TAPS>
+__global__ void __launch_bounds__(128)
+k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t nvox) {
+    static_assert(COUT % 16 == 0 && CIN % 8 == 0, "channel counts");
+    constexpr int LDY = COUT + 8, LDX = CIN + 8;  // padded rows: 16-byte aligned, no bank conflicts
+    constexpr int TILES = (COUT / 16) * (CIN / 8);
+    constexpr int PER = (TILES + 3) / 4;
+    __shared__ __align__(16) bf16 sy[kWgVox * LDY];
+    __shared__ __align__(16) bf16 sx[kWgVox * LDX];
+    const int t = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t sz = int64_t(x.H + 2) * (x.W + 2), syy = x.W + 2;
+    const int64_t o = TAPS == 27 ? ((t / 9 - 1) * sz + ((t / 3) % 3 - 1) * syy + (t % 3 - 1)) : 0;
+    float acc[PER][4];
+#pragma unroll
+    for (int k = 0; k < PER; ++k)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[k][q] = 0.f;
+    const bf16* __restrict__ yp = static_cast<const bf16*>(dy.p);
+    const bf16* __restrict__ xp = static_cast<const bf16*>(x.p);
+    for (int tile = 0; tile < kWgTiles; ++tile) {
+        const int64_t v0 = (int64_t(blockIdx.x) * kWgTiles + tile) * kWgVox;
+        if (v0 >= nvox) break;
+        // stage: 16-byte vectors of 8 channels
+        for (int q = threadIdx.x; q < kWgVox * (COUT / 8); q += blockDim.x) {
+            const int r = q / (COUT / 8), c8 = q % (COUT / 8);
+            const int64_t v = v0 + r;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (v < nvox) val = *reinterpret_cast<const uint4*>(yp + halo_index(dy, v) * dy.ld + dy.c0 + 8 * c8);
+            *reinterpret_cast<uint4*>(sy + r * LDY + 8 * c8) = val;
+        }
+        for (int q = threadIdx.x; q < kWgVox * (CIN / 8); q += blockDim.x) {
+            const int r = q / (CIN / 8), c8 = q % (CIN / 8);
+            const int64_t v = v0 + r;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (v < nvox)
+                val = *reinterpret_cast<const uint4*>(xp + (halo_index(x, v) + o) * x.ld + x.c0 + 8 * c8);
+            *reinterpret_cast<uint4*>(sx + r * LDX + 8 * c8) = val;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < kWgVox / 16; ++ks) {
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int tid = warp + 4 * k;
+                if (tid >= TILES) break;
+                const int m0 = 16 * (tid / (CIN / 8)), n0 = 8 * (tid % (CIN / 8));
+                // A = dy^T (rows co, cols voxel): matrices (m0, k0), (m0+8, k0), (m0, k0+8), (m0+8, k0+8)
+                const int mat = lane >> 3, rr = lane & 7;
+                const int krow = 16 * ks + rr + ((mat & 2) ? 8 : 0);
+                const int mcol = m0 + ((mat & 1) ? 8 : 0);
+                uint32_t a[4];
+                ldsm_x4_t(a, sy + krow * LDY + mcol);
+                // B = x (rows voxel, cols ci): matrices (k0, n0), (k0+8, n0)
+                const int krow2 = 16 * ks + (lane & 7) + ((lane >> 3) & 1) * 8;
+                uint32_t b0, b1;
+                ldsm_x2_t(b0, b1, sx + krow2 * LDX + n0);
+                mma16816(acc[k], a, b0, b1);
+            }
+        }
+        __syncthreads();
+    }
+    const int g = lane >> 2, tig = lane & 3;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int tid = warp + 4 * k;
+        if (tid >= TILES) break;
+        const int m0 = 16 * (tid / (CIN / 8)), n0 = 8 * (tid % (CIN / 8));
+        float* w = dW + int64_t(t) * cout_real * CIN;  // rows past the real output channels are padding
+        if (m0 + g < cout_real) {
+            atomicAdd(w + (m0 + g) * CIN + n0 + 2 * tig, acc[k][0]);
+            atomicAdd(w + (m0 + g) * CIN + n0 + 2 * tig + 1, acc[k][1]);
+        }
+        if (m0 + g + 8 < cout_real) {
+            atomicAdd(w + (m0 + g + 8) * CIN + n0 + 2 * tig, acc[k][2]);
+            atomicAdd(w + (m0 + g + 8) * CIN + n0 + 2 * tig + 1, acc[k][3]);
+        }
+    }
+}
+
+// ---- element-wise kernels ---------------------------------------------------------------
+
+// masked output gradient (BF16, plain ld = C): m = dy * [y > 0] (relu) or dy
+__global__ void k_grad_mask(TView dy, TView y, int relu, bf16* __restrict__ m, int C, int64_t nvox) {
+    const int64_t total = nvox * C;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C;
+        const int c = int(i - v * C);
+        const int64_t hv = halo_index(dy, v);
+        float val = static_cast<const float*>(dy.p)[hv * dy.ld + dy.c0 + c];
+        if (relu && !(__bfloat162float(static_cast<const bf16*>(y.p)[hv * y.ld + y.c0 + c]) > 0.f)) val = 0.f;
+        m[hv * C + c] = __float2bfloat16(val);
+    }
+}
+
+// db[c] += sum_v m[v][c] for c < count (m haloed, ld channels per voxel)
+__global__ void k_bias_grad(const bf16* __restrict__ m, TView shape, int ld, int count, float* __restrict__ db,
+                            int64_t nvox) {
+    for (int c = threadIdx.x; c < count; c += blockDim.x) {
+        float s = 0.f;
+        for (int64_t v = blockIdx.x; v < nvox; v += gridDim.x) s += __bfloat162float(m[halo_index(shape, v) * ld + c]);
+        atomicAdd(db + c, s);
+    }
+}
+
+// 2x2x2 average pooling: out (extents of the coarse grid) from in (twice as fine)
+__global__ void k_pool(TView in, TView out, int C) {
+    const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C;
+        const int c = int(i - v * C);
+        const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
+        const int64_t b = v / (int64_t(out.W) * out.H * out.D);
+        float s = 0.f;
+        for (int q = 0; q < 8; ++q) {
+            const int64_t fv = ((b * in.D + 2 * z + (q >> 2)) * in.H + 2 * y + ((q >> 1) & 1)) * in.W + 2 * x + (q & 1);
+            s += __bfloat162float(static_cast<const bf16*>(in.p)[halo_index(in, fv) * in.ld + in.c0 + c]);
+        }
+        static_cast<bf16*>(out.p)[halo_index(out, v) * out.ld + out.c0 + c] = __float2bfloat16(0.125f * s);
+    }
+}
+
+// pooling gradient: din[fine] += dout[coarse] / 8 (FP32 gradients)
+__global__ void k_pool_grad(TView dout, TView din, int C) {
+    const int64_t nv = int64_t(din.B) * din.D * din.H * din.W;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C;
+        const int c = int(i - v * C);
+        const int x = int(v % din.W), y = int((v / din.W) % din.H), z = int((v / (int64_t(din.W) * din.H)) % din.D);
+        const int64_t b = v / (int64_t(din.W) * din.H * din.D);
+        const int64_t cv = ((b * dout.D + z / 2) * dout.H + y / 2) * dout.W + x / 2;
+        static_cast<float*>(din.p)[halo_index(din, v) * din.ld + din.c0 + c] +=
+            0.125f * static_cast<const float*>(dout.p)[halo_index(dout, cv) * dout.ld + dout.c0 + c];
+    }
+}
+
+// nearest upsampling: out[fine] = in[coarse]
+__global__ void k_upsample(TView in, TView out, int C) {
+    const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C;
+        const int c = int(i - v * C);
+        const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
+        const int64_t b = v / (int64_t(out.W) * out.H * out.D);
+        const int64_t cv = ((b * in.D + z / 2) * in.H + y / 2) * in.W + x / 2;
+        static_cast<bf16*>(out.p)[halo_index(out, v) * out.ld + out.c0 + c] =
+            static_cast<const bf16*>(in.p)[halo_index(in, cv) * in.ld + in.c0 + c];
+    }
+}
+
+// upsampling gradient: din[coarse] = sum of the 8 fine dout
+__global__ void k_upsample_grad(TView dout, TView din, int C) {
+    const int64_t nv = int64_t(din.B) * din.D * din.H * din.W;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C;
+        const int c = int(i - v * C);
+        const int x = int(v % din.W), y = int((v / din.W) % din.H), z = int((v / (int64_t(din.W) * din.H)) % din.D);
+        const int64_t b = v / (int64_t(din.W) * din.H * din.D);
+        float s = 0.f;
+        for (int q = 0; q < 8; ++q) {
+            const int64_t fv = ((b * dout.D + 2 * z + (q >> 2)) * dout.H + 2 * y + ((q >> 1) & 1)) * dout.W + 2 * x + (q & 1);
+            s += static_cast<const float*>(dout.p)[halo_index(dout, fv) * dout.ld + dout.c0 + c];
+        }
+        static_cast<float*>(din.p)[halo_index(din, v) * din.ld + din.c0 + c] = s;
+    }
+}
+
+// network input: plain FP32 [B][n0][n1][n2][8] nodes -> haloed BF16 (16 channels, 8..15 zero)
+__global__ void k_pack_input(const float* __restrict__ src, int n0, int n1, int n2, TView in) {
+    const int64_t nv = int64_t(in.B) * n0 * n1 * n2;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * 8; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / 8;
+        const int c = int(i - v * 8);
+        const int x = int(v % n2), y = int((v / n2) % n1), z = int((v / (int64_t(n2) * n1)) % n0);
+        const int64_t b = v / (int64_t(n2) * n1 * n0);
+        const int64_t pv = ((b * in.D + z) * in.H + y) * in.W + x;
+        static_cast<bf16*>(in.p)[halo_index(in, pv) * in.ld + c] = __float2bfloat16(src[i]);
+    }
+}
+
+// network output: haloed FP32 (ld 16, 9 channels) -> plain FP32 [B][n0][n1][n2][9]
+__global__ void k_unpack_output(TView out, int n0, int n1, int n2, float* __restrict__ dst) {
+    const int64_t nv = int64_t(out.B) * n0 * n1 * n2;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * 9; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / 9;
+        const int c = int(i - v * 9);
+        const int x = int(v % n2), y = int((v / n2) % n1), z = int((v / (int64_t(n2) * n1)) % n0);
+        const int64_t b = v / (int64_t(n2) * n1 * n0);
+        const int64_t pv = ((b * out.D + z) * out.H + y) * out.W + x;
+        dst[i] = static_cast<const float*>(out.p)[halo_index(out, pv) * out.ld + c];
+    }
+}
+
+// mean squared error over the node region and its gradient (zero on padding voxels)
+__global__ void k_loss(TView out, const float* __restrict__ tgt, int n0, int n1, int n2, TView dout,
+                       double* __restrict__ loss) {
+    const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
+    const double inv = 1.0 / (double(out.B) * n0 * n1 * n2 * 9);
+    double local = 0.0;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * 16; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / 16;
+        const int c = int(i - v * 16);
+        const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
+        const int64_t b = v / (int64_t(out.W) * out.H * out.D);
+        const int64_t hv = halo_index(out, v);
+        float gval = 0.f;
+        if (c < 9 && z < n0 && y < n1 && x < n2) {
+            const float d = static_cast<const float*>(out.p)[hv * out.ld + c] -
+                            tgt[(((b * n0 + z) * n1 + y) * n2 + x) * 9 + c];
+            local += double(d) * d;
+            gval = float(2.0 * inv) * d;
+        }
+        static_cast<bf16*>(dout.p)[hv * dout.ld + c] = __float2bfloat16(gval);
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * inv);
+}
+
+// Adam (Kingma & Ba) on the FP32 parameters
+__global__ void k_adam(int64_t n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// BF16 copies of a layer's weights: forward [t][co][ci] and data-gradient [t'][ci][co]
+// with t' = taps - 1 - t (flipped kernel, transposed channels)
+__global__ void k_pack_weights(const float* __restrict__ w, int taps, int cout, int coutp, int cin,
+                               bf16* __restrict__ wf, bf16* __restrict__ wb, int cinp_b) {
+    const int64_t n = int64_t(taps) * coutp * cin;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int ci = int(i % cin);
+        const int co = int((i / cin) % coutp);
+        const int t = int(i / (int64_t(cin) * coutp));
+        const float val = co < cout ? w[(int64_t(t) * cout + co) * cin + ci] : 0.f;
+        wf[i] = __float2bfloat16(val);
+        if (wb && co < cinp_b) wb[(int64_t(taps - 1 - t) * cin + ci) * cinp_b + co] = __float2bfloat16(val);
+    }
+}
+
+// trilinear interpolation on a box node grid (nodes z fastest) at fractional index (fx, fy, fz)
+__device__ __forceinline__ void trilinear_setup(double f, int s, int& i0, double& u) {
+    i0 = min(int(floor(f)), s > 1 ? s - 2 : 0);
+    u = f - i0;
+}
+
+// trilinear resampling between two node grids spanning the same box (nodes z fastest)
+__global__ void k_box_resample(int s0, int s1, int s2, int d0, int d1, int d2, int C, const double* __restrict__ src,
+                               double* __restrict__ dst) {
+    const int64_t n = int64_t(d0) * d1 * d2;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int k = int(i % d2), j = int((i / d2) % d1), l = int(i / (int64_t(d2) * d1));
+        int x0, y0, z0;
+        double ux, uy, uz;
+        trilinear_setup(d0 > 1 ? double(l) * (s0 - 1) / (d0 - 1) : 0.0, s0, x0, ux);
+        trilinear_setup(d1 > 1 ? double(j) * (s1 - 1) / (d1 - 1) : 0.0, s1, y0, uy);
+        trilinear_setup(d2 > 1 ? double(k) * (s2 - 1) / (d2 - 1) : 0.0, s2, z0, uz);
+        for (int c = 0; c < C; ++c) {
+            double s = 0.0;
+            for (int q = 0; q < 8; ++q) {
+                const int xx = min(x0 + (q >> 2), s0 - 1), yy = min(y0 + ((q >> 1) & 1), s1 - 1), zz = min(z0 + (q & 1), s2 - 1);
+                const double w = ((q >> 2) ? ux : 1.0 - ux) * (((q >> 1) & 1) ? uy : 1.0 - uy) * ((q & 1) ? uz : 1.0 - uz);
+                s += w * src[((int64_t(xx) * s1 + yy) * s2 + zz) * C + c];
+            }
+            dst[i * C + c] = s;
+        }
+    }
+}
+
+// network features of a box design on the network's node grid, from the nodal density of a
+// (possibly finer) box node grid: 0 density (trilinear), 1 loaded face x = max, 2 clamped face
+// x = 0, 3..5 normalised node coordinates, 6 density cubed (the SIMP stiffness scale), 7 zero
+__global__ void k_features(int s0, int s1, int s2, const double* __restrict__ z, int n0, int n1, int n2,
+                           float* __restrict__ feat) {
+    const int64_t n = int64_t(n0) * n1 * n2;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int k = int(i % n2), j = int((i / n2) % n1), l = int(i / (int64_t(n2) * n1));
+        int x0, y0, z0;
+        double ux, uy, uz;
+        trilinear_setup(n0 > 1 ? double(l) * (s0 - 1) / (n0 - 1) : 0.0, s0, x0, ux);
+        trilinear_setup(n1 > 1 ? double(j) * (s1 - 1) / (n1 - 1) : 0.0, s1, y0, uy);
+        trilinear_setup(n2 > 1 ? double(k) * (s2 - 1) / (n2 - 1) : 0.0, s2, z0, uz);
+        double d = 0.0;
+        for (int q = 0; q < 8; ++q) {
+            const int xx = min(x0 + (q >> 2), s0 - 1), yy = min(y0 + ((q >> 1) & 1), s1 - 1), zz = min(z0 + (q & 1), s2 - 1);
+            d += ((q >> 2) ? ux : 1.0 - ux) * (((q >> 1) & 1) ? uy : 1.0 - uy) * ((q & 1) ? uz : 1.0 - uz) *
+                 z[(int64_t(xx) * s1 + yy) * s2 + zz];
+        }
+        float* f = feat + 8 * i;
+        f[0] = float(d);
+        f[1] = l == n0 - 1 ? 1.f : 0.f;
+        f[2] = l == 0 ? 1.f : 0.f;
+        f[3] = n0 > 1 ? float(l) / float(n0 - 1) : 0.f;
+        f[4] = n1 > 1 ? float(j) / float(n1 - 1) : 0.f;
+        f[5] = n2 > 1 ? float(k) / float(n2 - 1) : 0.f;
+        f[6] = float(d * d * d);
+        f[7] = 0.f;
+    }
+}
+
+// subspace columns on a (possibly finer) box node grid from the network output: column d
+// (d = load direction) at node p, component c = trilinear interpolation of output channel 3d + c
+__global__ void k_subspace(int n0, int n1, int n2, const float* __restrict__ out9, int d0, int d1, int d2,
+                           double* __restrict__ W) {
+    const int64_t n = int64_t(d0) * d1 * d2;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int k = int(i % d2), j = int((i / d2) % d1), l = int(i / (int64_t(d2) * d1));
+        int x0, y0, z0;
+        double ux, uy, uz;
+        trilinear_setup(d0 > 1 ? double(l) * (n0 - 1) / (d0 - 1) : 0.0, n0, x0, ux);
+        trilinear_setup(d1 > 1 ? double(j) * (n1 - 1) / (d1 - 1) : 0.0, n1, y0, uy);
+        trilinear_setup(d2 > 1 ? double(k) * (n2 - 1) / (d2 - 1) : 0.0, n2, z0, uz);
+        double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int q = 0; q < 8; ++q) {
+            const int xx = min(x0 + (q >> 2), n0 - 1), yy = min(y0 + ((q >> 1) & 1), n1 - 1), zz = min(z0 + (q & 1), n2 - 1);
+            const double w = ((q >> 2) ? ux : 1.0 - ux) * (((q >> 1) & 1) ? uy : 1.0 - uy) * ((q & 1) ? uz : 1.0 - uz);
+            const float* o = out9 + ((int64_t(xx) * n1 + yy) * n2 + zz) * 9;
+            for (int c = 0; c < 9; ++c) acc[c] += w * double(o[c]);
+        }
+        for (int dcol = 0; dcol < 3; ++dcol)
+            for (int c = 0; c < 3; ++c) W[dcol * 3 * n + 3 * i + c] = acc[3 * dcol + c];
+    }
+}
+
+// one 7-point averaging pass over a box node grid (C values per node): each node becomes the
+// mean of itself and its face neighbours inside the grid
+__global__ void k_box_smooth(int n0, int n1, int n2, int C, const float* __restrict__ in, float* __restrict__ out) {
+    const int64_t n = int64_t(n0) * n1 * n2;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n * C; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C;
+        const int k = int(v % n2), j = int((v / n2) % n1), l = int(v / (int64_t(n2) * n1));
+        float s = in[i];
+        int cnt = 1;
+        const int64_t sx = int64_t(n1) * n2 * C, sy = int64_t(n2) * C;
+        if (l > 0) { s += in[i - sx]; ++cnt; }
+        if (l < n0 - 1) { s += in[i + sx]; ++cnt; }
+        if (j > 0) { s += in[i - sy]; ++cnt; }
+        if (j < n1 - 1) { s += in[i + sy]; ++cnt; }
+        if (k > 0) { s += in[i - C]; ++cnt; }
+        if (k < n2 - 1) { s += in[i + C]; ++cnt; }
+        out[i] = s / float(cnt);
+    }
+}
+
+int blocks_for(int64_t n, int threads, int64_t cap = 148 * 32) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    return int(b < cap ? b : cap);
+}
+
+// ---- the network ------------------------------------------------------------------------
+
+struct Layer {
+    int cin, cout, taps, relu;
+    int64_t w_off, b_off;     // offsets in the FP32 parameter vector
+    bf16* wf = nullptr;       // [taps][coutp][cin]
+    bf16* wb = nullptr;       // [taps][cin][coutp_b] (data gradient)
+    int coutp() const { return (cout + 7) / 8 * 8; }
+};
+
+}  // namespace
+
+struct plato_unet {
+    cudaStream_t stream = nullptr;
+    int n[3] = {0, 0, 0};        // node grid
+    int g0[3] = {0, 0, 0};       // padded level-0 grid (multiples of 4)
+    int max_batch = 0;
+    std::vector<Layer> layers;   // e0a e0b e1a e1b e2a e2b d1a d1b d0a d0b head
+    int64_t nparams = 0;
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    // activations (BF16, haloed) and gradients (FP32, haloed)
+    bf16 *in = nullptr, *x0a = nullptr, *cat0 = nullptr, *p1 = nullptr, *x1a = nullptr, *cat1 = nullptr,
+         *p2 = nullptr, *x2a = nullptr, *x2b = nullptr, *x1c = nullptr, *x1d = nullptr, *x0c = nullptr, *x0d = nullptr;
+    float* out = nullptr;
+    float *dx0a = nullptr, *dcat0 = nullptr, *dp1 = nullptr, *dx1a = nullptr, *dcat1 = nullptr, *dp2 = nullptr,
+          *dx2a = nullptr, *dx2b = nullptr, *dx1c = nullptr, *dx1d = nullptr, *dx0c = nullptr, *dx0d = nullptr;
+    bf16* mbuf = nullptr;        // masked output gradient (BF16), also the head's gradient
+    double* loss_d = nullptr;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+int64_t halo_elems(const int* g, int B, int C) { return int64_t(B) * (g[0] + 2) * (g[1] + 2) * (g[2] + 2) * C; }
+
+TView tv(void* p, int ld, int c0, int B, const int* g) { return TView{p, ld, c0, B, g[0], g[1], g[2]}; }
+
+template <typename T>
+int alloc(plato_unet* u, T** p, int64_t count) {
+    UCUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * size_t(count > 0 ? count : 1)));
+    u->allocs.push_back(*p);
+    UCUDA(cudaMemset(*p, 0, sizeof(T) * size_t(count > 0 ? count : 1)));
+    return PLATO_OK;
+}
+
+// launch helpers (dispatch on the layer's channel counts)
+template <int CIN, int COUT, int TAPS, bool RELU, bool F32, bool ACC>
+int conv_launch(cudaStream_t s, TView in, const bf16* w, const float* b, TView out, int64_t nvox) {
+    const int64_t per = kConvWarps * 16 * kMT;
+    k_conv<CIN, COUT, TAPS, RELU, F32, ACC><<<int((nvox + per - 1) / per), kConvWarps * 32, 0, s>>>(in, w, b, out, nvox);
+    ULAUNCH();
+    return PLATO_OK;
+}
+
+int conv_forward(cudaStream_t s, const Layer& L, TView in, TView out, const float* bias, int64_t nvox) {
+    const int c = L.cin, o = L.cout;
+    if (L.taps == 1) return conv_launch<16, 9, 1, false, true, false>(s, in, L.wf, bias, out, nvox);
+#define FWD(CI, CO) \
+    if (c == CI && o == CO) return conv_launch<CI, CO, 27, true, false, false>(s, in, L.wf, bias, out, nvox);
+    FWD(16, 16) FWD(16, 32) FWD(32, 32) FWD(32, 64) FWD(64, 64) FWD(96, 32) FWD(48, 16)
+#undef FWD
+    return fail(PLATO_NOT_SUPPORTED, "no forward convolution for these channel counts");
+}
+
+// data gradient into an FP32 tensor (write, or accumulate)
+int conv_data_grad(cudaStream_t s, const Layer& L, TView dy, TView dx, int64_t nvox, bool accumulate) {
+    const int c = L.cout, o = L.cin;  // roles swap
+    if (L.taps == 1) {
+        if (accumulate) return conv_launch<16, 16, 1, false, true, true>(s, dy, L.wb, nullptr, dx, nvox);
+        return conv_launch<16, 16, 1, false, true, false>(s, dy, L.wb, nullptr, dx, nvox);
+    }
+#define BWD(CI, CO)                                                                                       \
+    if (c == CI && o == CO) {                                                                             \
+        if (accumulate) return conv_launch<CI, CO, 27, false, true, true>(s, dy, L.wb, nullptr, dx, nvox); \
+        return conv_launch<CI, CO, 27, false, true, false>(s, dy, L.wb, nullptr, dx, nvox);               \
+    }
+    BWD(16, 16) BWD(32, 16) BWD(32, 32) BWD(64, 32) BWD(64, 64) BWD(32, 96) BWD(16, 48)
+#undef BWD
+    return fail(PLATO_NOT_SUPPORTED, "no data-gradient convolution for these channel counts");
+}
+
+template <int CIN, int COUT, int TAPS>
+int wgrad_launch(cudaStream_t s, TView x, TView dy, float* dW, int cout_real, int64_t nvox) {
+    const int64_t per = int64_t(kWgVox) * kWgTiles;
+    const dim3 grid(unsigned((nvox + per - 1) / per), TAPS);
+    k_conv_wgrad<CIN, COUT, TAPS><<<grid, 128, 0, s>>>(x, dy, dW, cout_real, nvox);
+    ULAUNCH();
+    return PLATO_OK;
+}
+
+int conv_weight_grad(cudaStream_t s, const Layer& L, TView x, TView dy, float* dW, int64_t nvox) {
+    const int c = L.cin, o = L.coutp() < 16 ? 16 : L.coutp();
+    if (L.taps == 1) return wgrad_launch<16, 16, 1>(s, x, dy, dW, L.cout, nvox);
+#define WG(CI, CO) \
+    if (c == CI && o == CO) return wgrad_launch<CI, CO, 27>(s, x, dy, dW, L.cout, nvox);
+    WG(16, 16) WG(16, 32) WG(32, 32) WG(32, 64) WG(64, 64) WG(96, 32) WG(48, 16)
+#undef WG
+    return fail(PLATO_NOT_SUPPORTED, "no weight-gradient kernel for these channel counts");
+}
+
+#define URC(expr)                    \
+    do {                             \
+        int _rc = (expr);            \
+        if (_rc) return _rc;         \
+    } while (0)
+
+int pack_all_weights(plato_unet* u) {
+    for (Layer& L : u->layers) {
+        const int64_t n = int64_t(L.taps) * L.coutp() * L.cin;
+        const int cinp_b = L.taps == 1 ? 16 : L.coutp();
+        k_pack_weights<<<blocks_for(n, 256), 256, 0, u->stream>>>(u->params + L.w_off, L.taps, L.cout, L.coutp(), L.cin,
+                                                                 L.wf, L.wb, cinp_b);
+        ULAUNCH();
+    }
+    return PLATO_OK;
+}
+
+int forward(plato_unet* u, int B, const float* input) {
+    cudaStream_t s = u->stream;
+    const int* G0 = u->g0;
+    const int G1[3] = {G0[0] / 2, G0[1] / 2, G0[2] / 2};
+    const int G2[3] = {G1[0] / 2, G1[1] / 2, G1[2] / 2};
+    const int64_t n0 = int64_t(B) * G0[0] * G0[1] * G0[2], n1 = int64_t(B) * G1[0] * G1[1] * G1[2],
+                  n2 = int64_t(B) * G2[0] * G2[1] * G2[2];
+    const std::vector<Layer>& L = u->layers;
+    auto bias = [&](int k) { return u->params + L[k].b_off; };
+    const int64_t nn = int64_t(B) * u->n[0] * u->n[1] * u->n[2];
+    k_pack_input<<<blocks_for(nn * 8, 256), 256, 0, s>>>(input, u->n[0], u->n[1], u->n[2], tv(u->in, 16, 0, B, G0));
+    ULAUNCH();
+    URC(conv_forward(s, L[0], tv(u->in, 16, 0, B, G0), tv(u->x0a, 16, 0, B, G0), bias(0), n0));
+    URC(conv_forward(s, L[1], tv(u->x0a, 16, 0, B, G0), tv(u->cat0, 48, 32, B, G0), bias(1), n0));
+    k_pool<<<blocks_for(n1 * 16, 256), 256, 0, s>>>(tv(u->cat0, 48, 32, B, G0), tv(u->p1, 16, 0, B, G1), 16);
+    ULAUNCH();
+    URC(conv_forward(s, L[2], tv(u->p1, 16, 0, B, G1), tv(u->x1a, 32, 0, B, G1), bias(2), n1));
+    URC(conv_forward(s, L[3], tv(u->x1a, 32, 0, B, G1), tv(u->cat1, 96, 64, B, G1), bias(3), n1));
+    k_pool<<<blocks_for(n2 * 32, 256), 256, 0, s>>>(tv(u->cat1, 96, 64, B, G1), tv(u->p2, 32, 0, B, G2), 32);
+    ULAUNCH();
+    URC(conv_forward(s, L[4], tv(u->p2, 32, 0, B, G2), tv(u->x2a, 64, 0, B, G2), bias(4), n2));
+    URC(conv_forward(s, L[5], tv(u->x2a, 64, 0, B, G2), tv(u->x2b, 64, 0, B, G2), bias(5), n2));
+    k_upsample<<<blocks_for(n1 * 64, 256), 256, 0, s>>>(tv(u->x2b, 64, 0, B, G2), tv(u->cat1, 96, 0, B, G1), 64);
+    ULAUNCH();
+    URC(conv_forward(s, L[6], tv(u->cat1, 96, 0, B, G1), tv(u->x1c, 32, 0, B, G1), bias(6), n1));
+    URC(conv_forward(s, L[7], tv(u->x1c, 32, 0, B, G1), tv(u->x1d, 32, 0, B, G1), bias(7), n1));
+    k_upsample<<<blocks_for(n0 * 32, 256), 256, 0, s>>>(tv(u->x1d, 32, 0, B, G1), tv(u->cat0, 48, 0, B, G0), 32);
+    ULAUNCH();
+    URC(conv_forward(s, L[8], tv(u->cat0, 48, 0, B, G0), tv(u->x0c, 16, 0, B, G0), bias(8), n0));
+    URC(conv_forward(s, L[9], tv(u->x0c, 16, 0, B, G0), tv(u->x0d, 16, 0, B, G0), bias(9), n0));
+    URC(conv_forward(s, L[10], tv(u->x0d, 16, 0, B, G0), tv(u->out, 16, 0, B, G0), bias(10), n0));
+    return PLATO_OK;
+}
+
+// one layer's backward: dY (FP32 slice) masked by its output -> weight and bias gradients,
+// and (write_dx) the data gradient into dx (write, or accumulate)
+int layer_backward(plato_unet* u, int k, TView dy, TView y, TView x, TView dx, bool write_dx, bool accumulate,
+                   int64_t nvox) {
+    cudaStream_t s = u->stream;
+    const Layer& L = u->layers[k];
+    const int C = L.coutp() < 16 ? 16 : L.coutp();
+    const int gdims[3] = {y.D, y.H, y.W};
+    TView m = tv(u->mbuf, C, 0, y.B, gdims);
+    if (k != int(u->layers.size()) - 1) {  // the head's masked gradient is written by the loss
+        // mbuf is reused with other grids and widths: clear it so its halo reads as zero
+        UCUDA(cudaMemsetAsync(u->mbuf, 0, sizeof(bf16) * size_t(halo_elems(gdims, y.B, C)), s));
+        k_grad_mask<<<blocks_for(nvox * L.cout, 256), 256, 0, s>>>(dy, y, L.relu, u->mbuf, C, nvox);
+        ULAUNCH();
+    }
+    URC(conv_weight_grad(s, L, x, m, u->grads + L.w_off, nvox));
+    k_bias_grad<<<256, 128, 0, s>>>(u->mbuf, m, C, L.cout, u->grads + L.b_off, nvox);
+    ULAUNCH();
+    if (write_dx) URC(conv_data_grad(s, L, m, dx, nvox, accumulate));
+    return PLATO_OK;
+}
+
+int backward(plato_unet* u, int B) {
+    cudaStream_t s = u->stream;
+    const int* G0 = u->g0;
+    const int G1[3] = {G0[0] / 2, G0[1] / 2, G0[2] / 2};
+    const int G2[3] = {G1[0] / 2, G1[1] / 2, G1[2] / 2};
+    const int64_t n0 = int64_t(B) * G0[0] * G0[1] * G0[2], n1 = int64_t(B) * G1[0] * G1[1] * G1[2],
+                  n2 = int64_t(B) * G2[0] * G2[1] * G2[2];
+    TView none{nullptr, 0, 0, B, 1, 1, 1};
+    UCUDA(cudaMemsetAsync(u->grads, 0, sizeof(float) * size_t(u->nparams), s));
+    // head (its masked gradient, BF16, is in mbuf from the loss)
+    URC(layer_backward(u, 10, none, tv(u->out, 16, 0, B, G0), tv(u->x0d, 16, 0, B, G0), tv(u->dx0d, 16, 0, B, G0),
+                       true, false, n0));
+    URC(layer_backward(u, 9, tv(u->dx0d, 16, 0, B, G0), tv(u->x0d, 16, 0, B, G0), tv(u->x0c, 16, 0, B, G0),
+                       tv(u->dx0c, 16, 0, B, G0), true, false, n0));
+    URC(layer_backward(u, 8, tv(u->dx0c, 16, 0, B, G0), tv(u->x0c, 16, 0, B, G0), tv(u->cat0, 48, 0, B, G0),
+                       tv(u->dcat0, 48, 0, B, G0), true, false, n0));
+    k_upsample_grad<<<blocks_for(n1 * 32, 256), 256, 0, s>>>(tv(u->dcat0, 48, 0, B, G0), tv(u->dx1d, 32, 0, B, G1), 32);
+    ULAUNCH();
+    URC(layer_backward(u, 7, tv(u->dx1d, 32, 0, B, G1), tv(u->x1d, 32, 0, B, G1), tv(u->x1c, 32, 0, B, G1),
+                       tv(u->dx1c, 32, 0, B, G1), true, false, n1));
+    URC(layer_backward(u, 6, tv(u->dx1c, 32, 0, B, G1), tv(u->x1c, 32, 0, B, G1), tv(u->cat1, 96, 0, B, G1),
+                       tv(u->dcat1, 96, 0, B, G1), true, false, n1));
+    k_upsample_grad<<<blocks_for(n2 * 64, 256), 256, 0, s>>>(tv(u->dcat1, 96, 0, B, G1), tv(u->dx2b, 64, 0, B, G2), 64);
+    ULAUNCH();
+    URC(layer_backward(u, 5, tv(u->dx2b, 64, 0, B, G2), tv(u->x2b, 64, 0, B, G2), tv(u->x2a, 64, 0, B, G2),
+                       tv(u->dx2a, 64, 0, B, G2), true, false, n2));
+    URC(layer_backward(u, 4, tv(u->dx2a, 64, 0, B, G2), tv(u->x2a, 64, 0, B, G2), tv(u->p2, 32, 0, B, G2),
+                       tv(u->dp2, 32, 0, B, G2), true, false, n2));
+    k_pool_grad<<<blocks_for(n1 * 32, 256), 256, 0, s>>>(tv(u->dp2, 32, 0, B, G2), tv(u->dcat1, 96, 64, B, G1), 32);
+    ULAUNCH();
+    URC(layer_backward(u, 3, tv(u->dcat1, 96, 64, B, G1), tv(u->cat1, 96, 64, B, G1), tv(u->x1a, 32, 0, B, G1),
+                       tv(u->dx1a, 32, 0, B, G1), true, false, n1));
+    URC(layer_backward(u, 2, tv(u->dx1a, 32, 0, B, G1), tv(u->x1a, 32, 0, B, G1), tv(u->p1, 16, 0, B, G1),
+                       tv(u->dp1, 16, 0, B, G1), true, false, n1));
+    k_pool_grad<<<blocks_for(n0 * 16, 256), 256, 0, s>>>(tv(u->dp1, 16, 0, B, G1), tv(u->dcat0, 48, 32, B, G0), 16);
+    ULAUNCH();
+    URC(layer_backward(u, 1, tv(u->dcat0, 48, 32, B, G0), tv(u->cat0, 48, 32, B, G0), tv(u->x0a, 16, 0, B, G0),
+                       tv(u->dx0a, 16, 0, B, G0), true, false, n0));
+    URC(layer_backward(u, 0, tv(u->dx0a, 16, 0, B, G0), tv(u->x0a, 16, 0, B, G0), tv(u->in, 16, 0, B, G0), none,
+                       false, false, n0));
+    return PLATO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* plato_unet_last_error(void) { return g_unet_error.c_str(); }
+
+int plato_unet_create(const int32_t nodes[3], int32_t max_batch, plato_unet** out) {
+    if (!out) return fail(PLATO_BAD_INPUT, "null output pointer");
+    *out = nullptr;
+    if (!nodes || max_batch < 1) return fail(PLATO_BAD_INPUT, "node grid and max_batch >= 1 required");
+    for (int d = 0; d < 3; ++d)
+        if (nodes[d] < 2 || nodes[d] > 4096) return fail(PLATO_BAD_INPUT, "node grid extents must be in [2, 4096]");
+    plato_unet* u = new plato_unet();
+    u->max_batch = max_batch;
+    for (int d = 0; d < 3; ++d) {
+        u->n[d] = nodes[d];
+        u->g0[d] = (nodes[d] + 3) / 4 * 4;
+    }
+    // layers: {cin, cout, taps, relu}
+    const int spec[11][4] = {{16, 16, 27, 1}, {16, 16, 27, 1}, {16, 32, 27, 1}, {32, 32, 27, 1}, {32, 64, 27, 1},
+                             {64, 64, 27, 1}, {96, 32, 27, 1}, {32, 32, 27, 1}, {48, 16, 27, 1}, {16, 16, 27, 1},
+                             {16, 9, 1, 0}};
+    int64_t off = 0;
+    for (auto& sp : spec) {
+        Layer L;
+        L.cin = sp[0];
+        L.cout = sp[1];
+        L.taps = sp[2];
+        L.relu = sp[3];
+        L.w_off = off;
+        off += int64_t(L.taps) * L.cout * L.cin;
+        L.b_off = off;
+        off += L.cout;
+        u->layers.push_back(L);
+    }
+    u->nparams = off;
+    auto cleanup = [&](int rc) {
+        std::string msg = g_unet_error;
+        plato_unet_destroy(u);
+        g_unet_error = msg;
+        return rc;
+    };
+#define CA(p, n)                               \
+    do {                                       \
+        int _rc = alloc(u, &(p), (n));         \
+        if (_rc) return cleanup(_rc);          \
+    } while (0)
+    for (Layer& L : u->layers) {
+        CA(L.wf, int64_t(L.taps) * L.coutp() * L.cin);
+        CA(L.wb, int64_t(L.taps) * L.cin * (L.taps == 1 ? 16 : L.coutp()));
+    }
+    CA(u->params, u->nparams);
+    CA(u->grads, u->nparams);
+    CA(u->adam_m, u->nparams);
+    CA(u->adam_v, u->nparams);
+    const int B = max_batch;
+    const int* G0 = u->g0;
+    const int G1[3] = {G0[0] / 2, G0[1] / 2, G0[2] / 2};
+    const int G2[3] = {G1[0] / 2, G1[1] / 2, G1[2] / 2};
+    CA(u->in, halo_elems(G0, B, 16));
+    CA(u->x0a, halo_elems(G0, B, 16));
+    CA(u->cat0, halo_elems(G0, B, 48));
+    CA(u->p1, halo_elems(G1, B, 16));
+    CA(u->x1a, halo_elems(G1, B, 32));
+    CA(u->cat1, halo_elems(G1, B, 96));
+    CA(u->p2, halo_elems(G2, B, 32));
+    CA(u->x2a, halo_elems(G2, B, 64));
+    CA(u->x2b, halo_elems(G2, B, 64));
+    CA(u->x1c, halo_elems(G1, B, 32));
+    CA(u->x1d, halo_elems(G1, B, 32));
+    CA(u->x0c, halo_elems(G0, B, 16));
+    CA(u->x0d, halo_elems(G0, B, 16));
+    CA(u->out, halo_elems(G0, B, 16));
+    CA(u->dx0a, halo_elems(G0, B, 16));
+    CA(u->dcat0, halo_elems(G0, B, 48));
+    CA(u->dp1, halo_elems(G1, B, 16));
+    CA(u->dx1a, halo_elems(G1, B, 32));
+    CA(u->dcat1, halo_elems(G1, B, 96));
+    CA(u->dp2, halo_elems(G2, B, 32));
+    CA(u->dx2a, halo_elems(G2, B, 64));
+    CA(u->dx2b, halo_elems(G2, B, 64));
+    CA(u->dx1c, halo_elems(G1, B, 32));
+    CA(u->dx1d, halo_elems(G1, B, 32));
+    CA(u->dx0c, halo_elems(G0, B, 16));
+    CA(u->dx0d, halo_elems(G0, B, 16));
+    CA(u->mbuf, halo_elems(G0, B, 64) > halo_elems(G1, B, 64) ? halo_elems(G0, B, 64) : halo_elems(G1, B, 64));
+    CA(u->loss_d, 1);
+#undef CA
+    *out = u;
+    return PLATO_OK;
+}
+
+int plato_unet_destroy(plato_unet* u) {
+    if (!u) return PLATO_OK;
+    if (u->stream) cudaStreamSynchronize(u->stream);
+    for (void* p : u->allocs) cudaFree(p);
+    delete u;
+    return PLATO_OK;
+}
+
+int plato_unet_set_stream(plato_unet* u, void* stream) {
+    if (!u) return fail(PLATO_BAD_INPUT, "null network");
+    u->stream = static_cast<cudaStream_t>(stream);
+    return PLATO_OK;
+}
+
+int plato_unet_num_params(const plato_unet* u, int64_t* n) {
+    if (!u || !n) return fail(PLATO_BAD_INPUT, "null argument");
+    *n = u->nparams;
+    return PLATO_OK;
+}
+
+int plato_unet_set_params(plato_unet* u, const float* params) {
+    if (!u || !params) return fail(PLATO_BAD_INPUT, "null argument");
+    UCUDA(cudaMemcpyAsync(u->params, params, sizeof(float) * size_t(u->nparams), cudaMemcpyDeviceToDevice, u->stream));
+    UCUDA(cudaMemsetAsync(u->adam_m, 0, sizeof(float) * size_t(u->nparams), u->stream));
+    UCUDA(cudaMemsetAsync(u->adam_v, 0, sizeof(float) * size_t(u->nparams), u->stream));
+    return pack_all_weights(u);
+}
+
+int plato_unet_get_params(const plato_unet* u, float* params) {
+    if (!u || !params) return fail(PLATO_BAD_INPUT, "null argument");
+    UCUDA(cudaMemcpyAsync(params, u->params, sizeof(float) * size_t(u->nparams), cudaMemcpyDeviceToDevice, u->stream));
+    return PLATO_OK;
+}
+
+int plato_unet_forward(plato_unet* u, int32_t batch, const float* input, float* output) {
+    if (!u || !input || !output) return fail(PLATO_BAD_INPUT, "null argument");
+    if (batch < 1 || batch > u->max_batch) return fail(PLATO_BAD_INPUT, "batch outside [1, max_batch]");
+    URC(forward(u, batch, input));
+    const int64_t nn = int64_t(batch) * u->n[0] * u->n[1] * u->n[2];
+    k_unpack_output<<<blocks_for(nn * 9, 256), 256, 0, u->stream>>>(tv(u->out, 16, 0, batch, u->g0), u->n[0], u->n[1],
+                                                                     u->n[2], output);
+    ULAUNCH();
+    return PLATO_OK;
+}
+
+int plato_unet_loss_and_gradients(plato_unet* u, int32_t batch, const float* input, const float* target,
+                                  double* loss, float* grads) {
+    if (!u || !input || !target) return fail(PLATO_BAD_INPUT, "null argument");
+    if (batch < 1 || batch > u->max_batch) return fail(PLATO_BAD_INPUT, "batch outside [1, max_batch]");
+    URC(forward(u, batch, input));
+    cudaStream_t s = u->stream;
+    UCUDA(cudaMemsetAsync(u->loss_d, 0, sizeof(double), s));
+    UCUDA(cudaMemsetAsync(u->mbuf, 0, sizeof(bf16) * size_t(halo_elems(u->g0, batch, 16)), s));
+    const int64_t n0 = int64_t(batch) * u->g0[0] * u->g0[1] * u->g0[2];
+    k_loss<<<blocks_for(n0 * 16, 256), 256, 0, s>>>(tv(u->out, 16, 0, batch, u->g0), target, u->n[0], u->n[1], u->n[2],
+                                                   tv(u->mbuf, 16, 0, batch, u->g0), u->loss_d);
+    ULAUNCH();
+    URC(backward(u, batch));
+    if (grads)
+        UCUDA(cudaMemcpyAsync(grads, u->grads, sizeof(float) * size_t(u->nparams), cudaMemcpyDeviceToDevice, s));
+    if (loss) {
+        UCUDA(cudaMemcpyAsync(loss, u->loss_d, sizeof(double), cudaMemcpyDeviceToHost, s));
+        UCUDA(cudaStreamSynchronize(s));
+    }
+    return PLATO_OK;
+}
+
+int plato_unet_adam_step(plato_unet* u, float lr, int32_t step) {
+    if (!u || step < 1 || !(lr > 0.f)) return fail(PLATO_BAD_INPUT, "adam needs a network, step >= 1 and lr > 0");
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, float(step)), c2 = 1.f - std::pow(b2, float(step));
+    k_adam<<<blocks_for(u->nparams, 256), 256, 0, u->stream>>>(u->nparams, u->params, u->grads, u->adam_m, u->adam_v, lr,
+                                                               b1, b2, 1e-8f, c1, c2);
+    ULAUNCH();
+    return pack_all_weights(u);
+}
+
+int plato_box_resample(const int32_t src_nodes[3], const int32_t dst_nodes[3], int32_t channels, const double* src,
+                       double* dst, void* stream) {
+    if (!src_nodes || !dst_nodes || !src || !dst || channels < 1) return fail(PLATO_BAD_INPUT, "bad resample arguments");
+    for (int d = 0; d < 3; ++d)
+        if (src_nodes[d] < 1 || dst_nodes[d] < 1) return fail(PLATO_BAD_INPUT, "node grid extents must be >= 1");
+    const int64_t n = int64_t(dst_nodes[0]) * dst_nodes[1] * dst_nodes[2];
+    k_box_resample<<<blocks_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        src_nodes[0], src_nodes[1], src_nodes[2], dst_nodes[0], dst_nodes[1], dst_nodes[2], channels, src, dst);
+    ULAUNCH();
+    return PLATO_OK;
+}
+
+int plato_unet_features(const int32_t src_nodes[3], const double* z, const int32_t net_nodes[3], float* features,
+                        void* stream) {
+    if (!src_nodes || !net_nodes || !z || !features) return fail(PLATO_BAD_INPUT, "bad feature arguments");
+    const int64_t n = int64_t(net_nodes[0]) * net_nodes[1] * net_nodes[2];
+    k_features<<<blocks_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        src_nodes[0], src_nodes[1], src_nodes[2], z, net_nodes[0], net_nodes[1], net_nodes[2], features);
+    ULAUNCH();
+    return PLATO_OK;
+}
+
+int plato_unet_subspace(const int32_t net_nodes[3], const float* output, const int32_t dst_nodes[3], double* W,
+                        void* stream) {
+    if (!net_nodes || !dst_nodes || !output || !W) return fail(PLATO_BAD_INPUT, "bad subspace arguments");
+    const int64_t n = int64_t(dst_nodes[0]) * dst_nodes[1] * dst_nodes[2];
+    k_subspace<<<blocks_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        net_nodes[0], net_nodes[1], net_nodes[2], output, dst_nodes[0], dst_nodes[1], dst_nodes[2], W);
+    ULAUNCH();
+    return PLATO_OK;
+}
+
+int plato_box_smooth(const int32_t nodes[3], int32_t channels, int32_t passes, float* data, float* scratch,
+                     void* stream) {
+    if (!nodes || !data || !scratch || channels < 1 || passes < 0) return fail(PLATO_BAD_INPUT, "bad smoothing arguments");
+    const int64_t n = int64_t(nodes[0]) * nodes[1] * nodes[2] * channels;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (int p = 0; p < passes; ++p) {
+        k_box_smooth<<<blocks_for(n, 256), 256, 0, s>>>(nodes[0], nodes[1], nodes[2], channels, data, scratch);
+        ULAUNCH();
+        UCUDA(cudaMemcpyAsync(data, scratch, sizeof(float) * size_t(n), cudaMemcpyDeviceToDevice, s));
+    }
+    return PLATO_OK;
+}
+
+}  // extern "C"

@@ -81,12 +81,11 @@ def method_options(method: str, tol: float = 1e-10, coarse=COARSE_BOX) -> Solver
     raise ValueError(f"unknown method {method!r}; one of {METHODS}")
 
 
-def grf_density(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), corr: float = 0.1,
-                rng: np.random.Generator | None = None) -> np.ndarray:
-    """Nodal density on the (nx+1)(ny+1)(nz+1) box-mesh nodes (z fastest): a stationary
-    Gaussian random field with covariance exp(-r^2 / (2 corr^2)), sampled by filtering white
-    noise in Fourier space (spectral density exp(-|k|^2 corr^2 / 2)), standardised to zero
-    mean and unit variance, passed through the logistic function and clipped to [0.01, 1]."""
+def grf_field(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), corr: float = 0.1,
+              rng: np.random.Generator | None = None) -> np.ndarray:
+    """A stationary Gaussian random field with covariance exp(-r^2 / (2 corr^2)) on the
+    (nx+1)(ny+1)(nz+1) box-mesh nodes (z fastest), sampled by filtering white noise in Fourier
+    space (spectral density exp(-|k|^2 corr^2 / 2)) and standardised to zero mean, unit variance."""
     rng = rng or np.random.default_rng(0)
     shape = (nx + 1, ny + 1, nz + 1)
     h = [lengths[0] / nx, lengths[1] / ny, lengths[2] / nz]
@@ -94,8 +93,14 @@ def grf_density(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), corr: float 
     k = np.meshgrid(*[2 * np.pi * np.fft.fftfreq(m, d=hh) for m, hh in zip(shape, h)], indexing="ij")
     k2 = k[0] ** 2 + k[1] ** 2 + k[2] ** 2
     field = np.real(np.fft.ifftn(np.fft.fftn(noise) * np.exp(-0.25 * k2 * corr * corr)))
-    field = (field - field.mean()) / max(field.std(), 1e-300)
-    return np.clip(1.0 / (1.0 + np.exp(-field)), 0.01, 1.0).reshape(-1)
+    return ((field - field.mean()) / max(field.std(), 1e-300)).reshape(-1)
+
+
+def grf_density(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), corr: float = 0.1,
+                rng: np.random.Generator | None = None) -> np.ndarray:
+    """Nodal density: grf_field passed through the logistic function and clipped to [0.01, 1]."""
+    g = grf_field(nx, ny, nz, lengths, corr, rng)
+    return np.clip(1.0 / (1.0 + np.exp(-g)), 0.01, 1.0)
 
 
 def batch_workload(count: int = 64, seed: int = SEED_BATCH, sizes=BATCH_SIZES,

@@ -9,7 +9,8 @@ nu = 0.3, SIMP p = 3, rho_min = 1e-9, nodal densities i.i.d. U[0.01, 1] (SplitMi
 
 Methods (--method):
   two-level  (default) FP64 flexible CG; preconditioner = FP32 Chebyshev-Jacobi smoothing on
-             an FP32 copy of the matrix + Galerkin coarse correction on a 10x5x5 box grid.
+             an FP32 copy of the matrix + Galerkin coarse correction on a 10x5x5 box grid
+             (A-DEF2 two-level form).
   plain      the reference's algorithm: FP64 Jacobi-PCG on the assembled block matrix.
 Both stop on the same FP64 residual test (1e-10); the line also carries the plain method's
 throughput measured in the same run, and the accuracy of the timed solution against the

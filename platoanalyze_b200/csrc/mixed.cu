@@ -239,18 +239,6 @@ k_res_sub_vec(int64_t n, const uint8_t* __restrict__ mask, const float* __restri
         res[i] -= mask[i] ? x[i] : w[i];
 }
 
-// First Chebyshev step of a sweep that adds to y: d = c0 Dinv res, y += d.
-__global__ void __launch_bounds__(kThreads)
-k_cheb_first(int64_t n, float c0, const float* __restrict__ dinv32, const float* __restrict__ res,
-             float* __restrict__ d, float* __restrict__ y, const PcgScalars* S) {
-    if (S->done) return;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float di = c0 * dinv32[i] * res[i];
-        d[i] = di;
-        y[i] += di;
-    }
-}
-
 // z = y (widened), z.q -> beta = -(z.q)/(p.q); then p = z + beta p and p.r in k_fcg_direction.
 __global__ void __launch_bounds__(kThreads)
 k_fcg_zq(int64_t n, const float* __restrict__ y, double* __restrict__ z, const double* __restrict__ q,
@@ -604,20 +592,14 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         return PLATO_OK;
     };
     // M(r) with r in f_res (FP32) and, from the update kernel, d0 = c0 Dinv r, y = d0 already
-    // written.  Without a coarse space M = the Chebyshev sweep S.  With it, the balancing
-    // two-level form M = C + (I - CA) S (I - AC), C = Z E^-1 Z^T:
-    //   y = C r; res = r - A y; y += S(res); res -= A s; y += C res.
-    auto precondition = [&](float c0) -> int {
-        if (!coarse) return chebyshev_steps();
-        int r2 = coarse_apply(h, h->f_res, h->f_y, 0, h->scal);
-        if (r2) return r2;
-        r2 = inner_apply_sub(h->f_y);
-        if (r2) return r2;
-        k_cheb_first<<<VB, kThreads, 0, s>>>(n, c0, h->f_dinv, h->f_res, h->f_d0, h->f_y, h->scal);
-        PLATO_LAUNCH_CHECK(h);
-        r2 = chebyshev_steps();
-        if (r2) return r2;
-        r2 = inner_apply_sub(dlast);
+    // written.  Without a coarse space M = the Chebyshev sweep S.  With it, the two-level form
+    // A-DEF2 (Tang, Nabben, Vuik, Erlangga, J. Sci. Comput. 39, 2009), M = (I - CA) S + C with
+    // C = Z E^-1 Z^T: s = S r; res = r - A s; y = s + C res - one coarse solve and one extra
+    // inner operator apply per call (the balancing form C + (I - CA) S (I - AC) needs two of each).
+    auto precondition = [&](float) -> int {
+        int r2 = chebyshev_steps();
+        if (r2 || !coarse) return r2;
+        r2 = inner_apply_sub(dlast);  // the sweep left res = r - A (s - d_last)
         if (r2) return r2;
         return coarse_apply(h, h->f_res, h->f_y, 1, h->scal);
     };

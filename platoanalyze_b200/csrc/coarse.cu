@@ -35,6 +35,7 @@ constexpr int kThreadsPerCta = 256;
 struct CoarseView {
     int nc0, nc1, nc2;
     double x0, y0, z0, hx, hy, hz;
+    double ihx, ihy, ihz;  // 1 / h: local coordinates of the hot kernels are (x - lo) * ih
 };
 
 __host__ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -144,7 +145,7 @@ k_galerkin(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, const
             double wa[4];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
-                wa[a] = corner_weight(J, (x[a][0] - lo[0]) / cv.hx, (x[a][1] - lo[1]) / cv.hy, (x[a][2] - lo[2]) / cv.hz);
+                wa[a] = corner_weight(J, (x[a][0] - lo[0]) * cv.ihx, (x[a][1] - lo[1]) * cv.ihy, (x[a][2] - lo[2]) * cv.ihz);
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 double gj[3] = {0.0, 0.0, 0.0};
@@ -355,8 +356,8 @@ k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
     for (int t = 0; t < 24; ++t) s[t] = 0.0;
     for (int q = a0 + threadIdx.x; q < a1; q += kThreadsPerCta) {
         const int64_t p = node_list[q];
-        const double u = (coords[3 * p] - lo[0]) / cv.hx, vv = (coords[3 * p + 1] - lo[1]) / cv.hy,
-                     w = (coords[3 * p + 2] - lo[2]) / cv.hz;
+        const double u = (coords[3 * p] - lo[0]) * cv.ihx, vv = (coords[3 * p + 1] - lo[1]) * cv.ihy,
+                     w = (coords[3 * p + 2] - lo[2]) * cv.ihz;
         double val[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) val[d] = mask[3 * p + d] ? 0.0 : double(v[3 * p + d]);
@@ -424,8 +425,8 @@ __global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ c
         const double x = coords[3 * p], yy = coords[3 * p + 1], zz = coords[3 * p + 2];
         int cx, cy, cz;
         cell_of(cv, x, yy, zz, cx, cy, cz);
-        const double u = (x - (cv.x0 + cx * cv.hx)) / cv.hx, v = (yy - (cv.y0 + cy * cv.hy)) / cv.hy,
-                     w = (zz - (cv.z0 + cz * cv.hz)) / cv.hz;
+        const double u = (x - (cv.x0 + cx * cv.hx)) * cv.ihx, v = (yy - (cv.y0 + cy * cv.hy)) * cv.ihy,
+                     w = (zz - (cv.z0 + cz * cv.hz)) * cv.ihz;
         double s[3] = {0.0, 0.0, 0.0};
         for (int b = 0; b < 8; ++b) {
             const double wgt = corner_weight(b, u, v, w);
@@ -445,7 +446,8 @@ __global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ c
 
 static CoarseView coarse_view(const plato_problem* h) {
     const CoarseSpace& c = h->coarse;
-    return CoarseView{c.nc[0], c.nc[1], c.nc[2], c.x0[0], c.x0[1], c.x0[2], c.h[0], c.h[1], c.h[2]};
+    return CoarseView{c.nc[0], c.nc[1], c.nc[2], c.x0[0], c.x0[1], c.x0[2], c.h[0], c.h[1], c.h[2],
+                      1.0 / c.h[0], 1.0 / c.h[1], 1.0 / c.h[2]};
 }
 
 static int csr_by_key(plato_problem* h, int64_t count, uint32_t* keys, int32_t* vals, int32_t* hist, int nkeys,

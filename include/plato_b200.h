@@ -317,6 +317,41 @@ int plato_box_smooth(const int32_t nodes[3], int32_t channels, int32_t passes, f
 int plato_box_resample(const int32_t src_nodes[3], const int32_t dst_nodes[3], int32_t channels, const double* src,
                        double* dst, void* cuda_stream);
 
+/* ---- Helmholtz density filter (src/helmholtz/Problem.hpp, VectorFunction.hpp,
+ * HelmholtzResidual.hpp) ------------------------------------------------------------------
+ * A filter handle over the mesh: one unknown per node, the same node pattern as the
+ * mechanics (plato_jacobian_pattern), every array [device] of num_nodes values, entries one
+ * value per block.  Solves are FP64 Jacobi-PCG to solver.tolerance (0: 1e-12) within
+ * solver.max_iterations (0: 100000); the other solver fields are ignored.  plato_destroy
+ * releases the handle. */
+typedef struct plato_helmholtz_desc {
+    plato_mesh_desc    mesh;
+    double             length_scale;         /* "Length Scale" L > 0 (HelmholtzResidual.hpp:81)     */
+    double             surface_length_scale; /* "Surface Length Scale" alpha >= 0 (:82); 0 = none   */
+    int32_t            num_surface_faces;    /* faces carrying the surface term: the exterior faces
+                                                outside the "Symmetry Plane Sides" (:197-198)       */
+    const int32_t*     surface_face_cells;       /* [host] owning cell of each face              */
+    const int32_t*     surface_face_local_nodes; /* [host] 3 cell-local node ordinals per face    */
+    plato_solver_opts  solver;
+} plato_helmholtz_desc;
+int plato_create_helmholtz(const plato_helmholtz_desc* desc, plato_problem** out);
+/* VectorFunction::value: R = K filtered - M control, K including the surface term
+ * alpha L sum over faces of (area / 9) for the face's node pairs (evaluate_boundary) */
+int plato_helmholtz_value(plato_problem* h, const double* filtered, const double* control, double* R);
+/* VectorFunction::gradient_u: K_ab = sum vol (L^2 g_a . g_b + 1/16) + the surface term
+ * (assembled once per handle) */
+int plato_helmholtz_gradient_u(plato_problem* h, double* entries);
+/* VectorFunction::gradient_z, transposed as the reference returns it: -sum vol / 16 */
+int plato_helmholtz_gradient_z(plato_problem* h, double* entries);
+/* Problem::solution (src/helmholtz/Problem.hpp:158-176): filtered = K^-1 M control */
+int plato_helmholtz_solution(plato_problem* h, const double* control, double* filtered, plato_solve_stats* stats);
+/* Problem::criterionGradient (src/helmholtz/Problem.hpp:187-208): from the criterion's
+ * derivative with respect to the filtered density to the one with respect to the control,
+ * dfdcontrol = (dR/dcontrol)^T K^-1 (-dfdfiltered) = M K^-1 dfdfiltered.  Unlike the reference,
+ * the input is not negated in place. */
+int plato_helmholtz_criterion_gradient(plato_problem* h, const double* dfdfiltered, double* dfdcontrol,
+                                       plato_solve_stats* stats);
+
 /* ---- box mesh generator (host only; stands in for BamG, unit_tests/PlatoTestHelpers.hpp) */
 int plato_box_mesh_sizes(int32_t nx, int32_t ny, int32_t nz, int32_t* num_nodes, int32_t* num_cells);
 int plato_box_mesh_tet4(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,

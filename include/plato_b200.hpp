@@ -102,6 +102,13 @@ public:
         h_.reset(h);
         check(plato_get_sizes(h, &num_nodes_, &num_cells_, &num_blocks_), h);
     }
+    // a Helmholtz density filter over the mesh (one unknown per node)
+    explicit Model(const plato_helmholtz_desc& desc) {
+        plato_problem* h = nullptr;
+        check(plato_create_helmholtz(&desc, &h), nullptr);
+        h_.reset(h);
+        check(plato_get_sizes(h, &num_nodes_, &num_cells_, &num_blocks_), h);
+    }
     plato_problem* handle() const { return h_.get(); }
     int32_t numNodes() const { return num_nodes_; }
     int32_t numCells() const { return num_cells_; }
@@ -244,4 +251,55 @@ private:
 };
 
 }  // namespace Elliptic
+
+namespace Helmholtz {
+
+// Plato::Helmholtz::VectorFunction (src/helmholtz/VectorFunction.hpp) on a filter Model.
+class VectorFunction {
+public:
+    explicit VectorFunction(std::shared_ptr<Model> m) : m_(std::move(m)) {}
+    ScalarVector value(const ScalarVector& filtered, const ScalarVector& control) const {
+        ScalarVector R(size_t(m_->numNodes()));
+        check(plato_helmholtz_value(m_->handle(), filtered.data(), control.data(), R.data()), m_->handle());
+        return R;
+    }
+    std::shared_ptr<CrsMatrix> gradient_u(const ScalarVector&, const ScalarVector&) const {
+        auto A = m_->newMatrix(1, 1);
+        check(plato_helmholtz_gradient_u(m_->handle(), A->entries.data()), m_->handle());
+        return A;
+    }
+    std::shared_ptr<CrsMatrix> gradient_z(const ScalarVector&, const ScalarVector&) const {
+        auto A = m_->newMatrix(1, 1);
+        check(plato_helmholtz_gradient_z(m_->handle(), A->entries.data()), m_->handle());
+        return A;
+    }
+
+private:
+    std::shared_ptr<Model> m_;
+};
+
+// Plato::Helmholtz::Problem (src/helmholtz/Problem.hpp:158-208).
+class Problem {
+public:
+    explicit Problem(std::shared_ptr<Model> m) : m_(std::move(m)), state_(size_t(m_->numNodes())) {}
+
+    const ScalarVector& solution(const ScalarVector& control) {
+        check(plato_helmholtz_solution(m_->handle(), control.data(), state_.data(), &last_), m_->handle());
+        return state_;
+    }
+    // the reference negates its argument in place; this one leaves it unchanged
+    ScalarVector criterionGradient(const ScalarVector& dfdfiltered) {
+        ScalarVector g(size_t(m_->numNodes()));
+        check(plato_helmholtz_criterion_gradient(m_->handle(), dfdfiltered.data(), g.data(), &last_), m_->handle());
+        return g;
+    }
+    const plato_solve_stats& lastSolveStats() const { return last_; }
+
+private:
+    std::shared_ptr<Model> m_;
+    ScalarVector state_;
+    plato_solve_stats last_{};
+};
+
+}  // namespace Helmholtz
 }  // namespace plato_b200

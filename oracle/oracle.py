@@ -31,6 +31,11 @@ class OracleStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("relative_residual", C.c_double), ("converged", C.c_int32)]
 
 
+class OracleHelmholtz(C.Structure):
+    _fields_ = [("length_scale", C.c_double), ("surface_length_scale", C.c_double), ("num_faces", C.c_int32),
+                ("face_cells", i32p), ("face_local_nodes", i32p)]
+
+
 def _build() -> None:
     if not LIB_PATH.exists():
         cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
@@ -41,6 +46,7 @@ def _load() -> C.CDLL:
     _build()
     lib = C.CDLL(str(LIB_PATH))
     P = C.POINTER(OracleProblem)
+    H = C.POINTER(OracleHelmholtz)
     vp = C.c_void_p
     sig = {
         "oracle_cell_fields": ([P, vp, vp, vp, vp, vp, vp], None),
@@ -62,6 +68,12 @@ def _load() -> C.CDLL:
         "oracle_num_threads": ([], C.c_int),
         "oracle_volume_value": ([P, vp, C.c_double, C.c_double], C.c_double),
         "oracle_volume_gradient_z": ([P, vp, C.c_double, C.c_double, vp], None),
+        "oracle_helmholtz_value": ([P, H, vp, vp, vp], None),
+        "oracle_helmholtz_gradient_u": ([P, H, vp, vp, vp], None),
+        "oracle_helmholtz_gradient_z": ([P, vp, vp, vp], None),
+        "oracle_helmholtz_solution": ([P, H, vp, vp, C.c_double, C.c_int32, C.POINTER(OracleStats)], C.c_int),
+        "oracle_helmholtz_criterion_gradient": ([P, H, vp, vp, C.c_double, C.c_int32,
+                                                 C.POINTER(OracleStats)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -217,6 +229,56 @@ class Oracle:
         g = np.empty(self.N)
         lib.oracle_volume_gradient_z(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)), p, m, _p(g))
         return g
+
+    # -- Helmholtz density filter (scalar, one value per node) ------------------------------
+    # `surface` = (alpha, face_cells, face_local_nodes): "Surface Length Scale" and its faces
+    def _helm(self, L, surface):
+        if surface is None:
+            return OracleHelmholtz(L, 0.0, 0, None, None)
+        alpha, cells, local = surface
+        cells = np.ascontiguousarray(cells, np.int32)
+        local = np.ascontiguousarray(local, np.int32)
+        self._helm_keep = (cells, local)
+        return OracleHelmholtz(L, alpha, cells.size, cells.ctypes.data_as(i32p), local.ctypes.data_as(i32p))
+
+    def helmholtz_value(self, L, filtered, control, surface=None):
+        R = np.empty(self.N)
+        H = self._helm(L, surface)
+        lib.oracle_helmholtz_value(C.byref(self.P), C.byref(H), _p(np.ascontiguousarray(filtered, np.float64)),
+                                   _p(np.ascontiguousarray(control, np.float64)), _p(R))
+        return R
+
+    def helmholtz_gradient_u(self, L, surface=None):
+        rm, cols = self.graph()
+        K = np.empty(cols.size)
+        H = self._helm(L, surface)
+        lib.oracle_helmholtz_gradient_u(C.byref(self.P), C.byref(H), _p(rm), _p(cols), _p(K))
+        return K
+
+    def helmholtz_gradient_z(self):
+        rm, cols = self.graph()
+        K = np.empty(cols.size)
+        lib.oracle_helmholtz_gradient_z(C.byref(self.P), _p(rm), _p(cols), _p(K))
+        return K
+
+    def helmholtz_solution(self, L, control, tol=1e-12, max_it=100000, surface=None):
+        f = np.empty(self.N)
+        st = OracleStats()
+        H = self._helm(L, surface)
+        lib.oracle_helmholtz_solution(C.byref(self.P), C.byref(H), _p(np.ascontiguousarray(control, np.float64)),
+                                      _p(f), tol, max_it, C.byref(st))
+        return f, {"iterations": st.iterations, "relative_residual": st.relative_residual,
+                   "converged": st.converged}
+
+    def helmholtz_criterion_gradient(self, L, dfdfiltered, tol=1e-12, max_it=100000, surface=None):
+        g = np.empty(self.N)
+        st = OracleStats()
+        H = self._helm(L, surface)
+        lib.oracle_helmholtz_criterion_gradient(C.byref(self.P), C.byref(H),
+                                                _p(np.ascontiguousarray(dfdfiltered, np.float64)), _p(g), tol, max_it,
+                                                C.byref(st))
+        return g, {"iterations": st.iterations, "relative_residual": st.relative_residual,
+                   "converged": st.converged}
 
     @staticmethod
     def num_threads() -> int:

@@ -583,18 +583,18 @@ void oracle_matvec_plus(int32_t num_node_rows, int32_t rb, int32_t cb, const int
  * (src/alg/PlatoAbstractSolver.hpp:38-106); this is the textbook method (Hestenes-
  * Stiefel CG with M = diag(A)), FP64 throughout, stopping on ||r_k||/||b|| <= tol and
  * confirming with the recomputed residual b - A x. */
-int oracle_pcg_jacobi(int32_t N, const int32_t* row_map, const int32_t* cols, const double* A,
-                      const double* b, double* x, double tol, int32_t max_it, oracle_solve_stats* st) {
-    const int64_t n = 3 * (int64_t)N;
+static int pcg_jacobi_dpn(int32_t N, int dpn, const int32_t* row_map, const int32_t* cols, const double* A,
+                          const double* b, double* x, double tol, int32_t max_it, oracle_solve_stats* st) {
+    const int64_t n = dpn * (int64_t)N;
     std::vector<double> dinv(n), r(n), zv(n), p(n), Ap(n);
 #pragma omp parallel for schedule(static)
     for (int32_t i = 0; i < N; ++i) {
         int64_t e = block_entry(row_map, cols, i, i);
-        for (int d = 0; d < 3; ++d) dinv[3 * (int64_t)i + d] = 1.0 / A[9 * e + 4 * d];
+        for (int d = 0; d < dpn; ++d) dinv[dpn * (int64_t)i + d] = 1.0 / A[dpn * dpn * e + (dpn + 1) * d];
     }
     auto apply = [&](const double* in, double* out) {
         std::fill(out, out + n, 0.0);
-        oracle_matvec_plus(N, 3, 3, row_map, cols, A, in, out);
+        oracle_matvec_plus(N, dpn, dpn, row_map, cols, A, in, out);
     };
     apply(x, Ap.data());
 #pragma omp parallel for schedule(static)
@@ -649,6 +649,11 @@ int oracle_pcg_jacobi(int32_t N, const int32_t* row_map, const int32_t* cols, co
     return st->converged ? 0 : 1;
 }
 
+int oracle_pcg_jacobi(int32_t N, const int32_t* row_map, const int32_t* cols, const double* A,
+                      const double* b, double* x, double tol, int32_t max_it, oracle_solve_stats* st) {
+    return pcg_jacobi_dpn(N, 3, row_map, cols, A, b, x, tol, max_it, st);
+}
+
 /* Problem::solution, src/elliptic/Problem.hpp:237-292 (one Newton step):
  * R = value(0, z); R *= -1; J = gradient_u; applyStateConstraints(J, R, 1);
  * solve J d = R; u = 0 + d. */
@@ -696,6 +701,142 @@ int oracle_problem_criterion_gradient(const oracle_problem* P, const double* z, 
     std::vector<double> dRdz(3 * cols.size());
     oracle_vf_gradient_z(P, u, z, rm.data(), cols.data(), dRdz.data());
     oracle_matvec_plus(P->num_nodes, 1, 3, rm.data(), cols.data(), dRdz.data(), lambda.data(), dfdz);
+    return rc;
+}
+
+/* ---- Helmholtz density filter (src/helmholtz) ------------------------------------------
+ * HelmholtzResidual::evaluate (src/helmholtz/HelmholtzResidual.hpp:103-176): per cell, with
+ * the one-point rule (basis functions 1/4 at the centroid) and vol = |det J| / 6: the flux
+ * L^2 grad(filtered) (HelmholtzFlux.hpp:32-43) is divided against the basis gradients,
+ * R_a += vol (L^2 grad(filtered) . g_a) (FluxDivergence), then the mass term
+ * R_a += N_a (filtered_gp - control_gp) vol (AddMassTerm.hpp:35-47). */
+
+/* Triangle area of a face (CalculateSurfaceArea<3>, src/SurfaceIntegralUtilities.hpp:212-227,
+ * times the degree-one triangle weight 1/2) and its three global nodes. */
+static double face_area(const oracle_problem* P, const oracle_helmholtz* H, int32_t f, int32_t id[3]) {
+    const int32_t* n = P->connectivity + 4 * (int64_t)H->face_cells[f];
+    for (int a = 0; a < 3; ++a) id[a] = n[H->face_local_nodes[3 * (int64_t)f + a]];
+    double J[2][3];
+    for (int a = 0; a < 2; ++a)
+        for (int d = 0; d < 3; ++d) J[a][d] = P->coords[3 * (int64_t)id[a] + d] - P->coords[3 * (int64_t)id[2] + d];
+    const double J23 = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    const double J31 = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+    const double J12 = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    return 0.5 * std::sqrt(J23 * J23 + J31 * J31 + J12 * J12);
+}
+
+/* evaluate_boundary (src/helmholtz/HelmholtzResidual.hpp:178-241), per face with the
+ * degree-one triangle rule (basis 1/3): filtered_face = sum_b filtered_b / 3 and
+ * R_a += alpha L filtered_face area / 3 for the face's nodes.  The reference keeps
+ * filtered_face in a per-cell slot, shared by the faces of one cell; here it is per face. */
+void oracle_helmholtz_value(const oracle_problem* P, const oracle_helmholtz* H, const double* filtered,
+                            const double* control, double* R) {
+    std::fill(R, R + P->num_nodes, 0.0);
+    const double L2 = H->length_scale * H->length_scale;
+#pragma omp parallel for schedule(static)
+    for (int32_t c = 0; c < P->num_cells; ++c) {
+        CellGeom G;
+        cell_geometry(P, c, G);
+        const int32_t* n = P->connectivity + 4 * (int64_t)c;
+        double grad[3] = {0.0, 0.0, 0.0}, fg = 0.0, cg = 0.0;
+        for (int a = 0; a < 4; ++a) {
+            for (int d = 0; d < 3; ++d) grad[d] += filtered[n[a]] * G.g[a][d];
+            fg += 0.25 * filtered[n[a]];
+            cg += 0.25 * control[n[a]];
+        }
+        double flux[3];
+        for (int d = 0; d < 3; ++d) flux[d] = L2 * grad[d];
+        double out[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) out[a] += flux[d] * G.g[a][d] * G.vol;
+        for (int a = 0; a < 4; ++a) out[a] += 0.25 * (fg - cg) * G.vol;
+        for (int a = 0; a < 4; ++a) atomic_add(&R[n[a]], out[a]);
+    }
+    if (!(H->surface_length_scale > 0.0)) return;
+    const double aL = H->surface_length_scale * H->length_scale;
+    for (int32_t f = 0; f < H->num_faces; ++f) {
+        int32_t id[3];
+        const double area = face_area(P, H, f, id);
+        double ff = 0.0;
+        for (int b = 0; b < 3; ++b) ff += filtered[id[b]] / 3.0;
+        for (int a = 0; a < 3; ++a) R[id[a]] += aL * ff * (area / 3.0);
+    }
+}
+
+/* VectorFunction::gradient_u (src/helmholtz/VectorFunction.hpp): dR_a/dfiltered_b =
+ * vol (L^2 g_a . g_b + 1/16) per cell, plus alpha L area / 9 per surface face. */
+void oracle_helmholtz_gradient_u(const oracle_problem* P, const oracle_helmholtz* H, const int32_t* row_map,
+                                 const int32_t* cols, double* entries) {
+    std::fill(entries, entries + row_map[P->num_nodes], 0.0);
+    const double L2 = H->length_scale * H->length_scale;
+#pragma omp parallel for schedule(static)
+    for (int32_t c = 0; c < P->num_cells; ++c) {
+        CellGeom G;
+        cell_geometry(P, c, G);
+        const int32_t* n = P->connectivity + 4 * (int64_t)c;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                const double v = G.vol * (L2 * (G.g[a][0] * G.g[b][0] + G.g[a][1] * G.g[b][1] + G.g[a][2] * G.g[b][2]) +
+                                          0.0625);
+                atomic_add(&entries[block_entry(row_map, cols, n[a], n[b])], v);
+            }
+    }
+    if (!(H->surface_length_scale > 0.0)) return;
+    const double aL = H->surface_length_scale * H->length_scale;
+    for (int32_t f = 0; f < H->num_faces; ++f) {
+        int32_t id[3];
+        const double area = face_area(P, H, f, id);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) entries[block_entry(row_map, cols, id[a], id[b])] += aL * (area / 3.0) / 3.0;
+    }
+}
+
+/* VectorFunction::gradient_z, transposed as the reference returns it: dR_a/dcontrol_b =
+ * -vol / 16 (the mass term; symmetric). */
+void oracle_helmholtz_gradient_z(const oracle_problem* P, const int32_t* row_map, const int32_t* cols,
+                                 double* entries) {
+    std::fill(entries, entries + row_map[P->num_nodes], 0.0);
+#pragma omp parallel for schedule(static)
+    for (int32_t c = 0; c < P->num_cells; ++c) {
+        CellGeom G;
+        cell_geometry(P, c, G);
+        const int32_t* n = P->connectivity + 4 * (int64_t)c;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) atomic_add(&entries[block_entry(row_map, cols, n[b], n[a])], -0.0625 * G.vol);
+    }
+}
+
+/* Helmholtz Problem::solution (src/helmholtz/Problem.hpp:158-176): R = value(0, control),
+ * R *= -1, J = gradient_u, solve J filtered = R from zero. */
+int oracle_helmholtz_solution(const oracle_problem* P, const oracle_helmholtz* H, const double* control,
+                              double* filtered, double tol, int32_t max_it, oracle_solve_stats* st) {
+    const int64_t N = P->num_nodes;
+    std::vector<int32_t> rm, cols;
+    build_graph(P, rm, cols);
+    std::vector<double> zero(N, 0.0), R(N), J(cols.size());
+    oracle_helmholtz_value(P, H, zero.data(), control, R.data());
+    for (auto& v : R) v *= -1.0;
+    oracle_helmholtz_gradient_u(P, H, rm.data(), cols.data(), J.data());
+    std::fill(filtered, filtered + N, 0.0);
+    return pcg_jacobi_dpn(P->num_nodes, 1, rm.data(), cols.data(), J.data(), R.data(), filtered, tol, max_it, st);
+}
+
+/* Helmholtz Problem::criterionGradient (src/helmholtz/Problem.hpp:187-208): given the
+ * criterion's derivative with respect to the filtered density g, solve J x = -g and return
+ * (dR/dcontrol)^T x (= M J^-1 g). */
+int oracle_helmholtz_criterion_gradient(const oracle_problem* P, const oracle_helmholtz* H, const double* dfdfiltered,
+                                        double* dfdcontrol, double tol, int32_t max_it, oracle_solve_stats* st) {
+    const int64_t N = P->num_nodes;
+    std::vector<int32_t> rm, cols;
+    build_graph(P, rm, cols);
+    std::vector<double> J(cols.size()), dRdz(cols.size()), rhs(N), x(N, 0.0);
+    oracle_helmholtz_gradient_u(P, H, rm.data(), cols.data(), J.data());
+    oracle_helmholtz_gradient_z(P, rm.data(), cols.data(), dRdz.data());
+    for (int64_t i = 0; i < N; ++i) rhs[i] = -dfdfiltered[i];
+    const int rc = pcg_jacobi_dpn(P->num_nodes, 1, rm.data(), cols.data(), J.data(), rhs.data(), x.data(), tol,
+                                  max_it, st);
+    std::fill(dfdcontrol, dfdcontrol + N, 0.0);
+    oracle_matvec_plus(P->num_nodes, 1, 1, rm.data(), cols.data(), dRdz.data(), x.data(), dfdcontrol);
     return rc;
 }
 

@@ -96,6 +96,30 @@ int oracle_problem_criterion_gradient(const oracle_problem* P, const double* z, 
                                       int32_t self_adjoint, double tolerance, int32_t max_iterations,
                                       double* dfdz, oracle_solve_stats* stats);
 
+/* Helmholtz density filter (src/helmholtz): "Length Scale" L, "Surface Length Scale" alpha
+ * (0 = no surface term) and the faces that carry it (the exterior faces outside the
+ * "Symmetry Plane Sides"; HelmholtzResidual.hpp evaluate_boundary). */
+typedef struct oracle_helmholtz {
+    double         length_scale;
+    double         surface_length_scale;
+    int32_t        num_faces;
+    const int32_t* face_cells;       /* owning cell of each face */
+    const int32_t* face_local_nodes; /* 3 cell-local node ordinals per face */
+} oracle_helmholtz;
+
+/* Residual, Jacobian and (dR/dcontrol)^T entries (one value per block of the node pattern),
+ * solution, and the chain rule from the filtered to the unfiltered density. */
+void oracle_helmholtz_value(const oracle_problem* P, const oracle_helmholtz* H, const double* filtered,
+                            const double* control, double* R);
+void oracle_helmholtz_gradient_u(const oracle_problem* P, const oracle_helmholtz* H, const int32_t* row_map,
+                                 const int32_t* column_indices, double* entries);
+void oracle_helmholtz_gradient_z(const oracle_problem* P, const int32_t* row_map, const int32_t* column_indices,
+                                 double* entries);
+int oracle_helmholtz_solution(const oracle_problem* P, const oracle_helmholtz* H, const double* control,
+                              double* filtered, double tolerance, int32_t max_iterations, oracle_solve_stats* stats);
+int oracle_helmholtz_criterion_gradient(const oracle_problem* P, const oracle_helmholtz* H, const double* dfdfiltered,
+                                        double* dfdcontrol, double tolerance, int32_t max_iterations,
+                                        oracle_solve_stats* stats);
 int oracle_num_threads(void);
 
 #ifdef __cplusplus

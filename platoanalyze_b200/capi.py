@@ -55,6 +55,12 @@ class ProblemDesc(C.Structure):
                 ("essential_bcs", EssentialBCs), ("solver", SolverOpts)]
 
 
+class HelmholtzDesc(C.Structure):
+    _fields_ = [("mesh", MeshDesc), ("length_scale", C.c_double), ("surface_length_scale", C.c_double),
+                ("num_surface_faces", C.c_int32), ("surface_face_cells", i32p),
+                ("surface_face_local_nodes", i32p), ("solver", SolverOpts)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("refinements", C.c_int32), ("relative_residual", C.c_double),
                 ("converged", C.c_int32), ("status", C.c_int32)]
@@ -126,6 +132,12 @@ def _load() -> C.CDLL:
         "plato_unet_subspace": ([i32p, vp, i32p, vp, vp], C.c_int),
         "plato_box_smooth": ([i32p, C.c_int32, C.c_int32, vp, vp, vp], C.c_int),
         "plato_box_resample": ([i32p, i32p, C.c_int32, vp, vp, vp], C.c_int),
+        "plato_create_helmholtz": ([C.POINTER(HelmholtzDesc), C.POINTER(vp)], C.c_int),
+        "plato_helmholtz_value": ([vp, vp, vp, vp], C.c_int),
+        "plato_helmholtz_gradient_u": ([vp, vp], C.c_int),
+        "plato_helmholtz_gradient_z": ([vp, vp], C.c_int),
+        "plato_helmholtz_solution": ([vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_helmholtz_criterion_gradient": ([vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_box_mesh_sizes": ([C.c_int32] * 3 + [i32p, i32p], C.c_int),
         "plato_box_mesh_tet4": ([C.c_int32] * 3 + [C.c_double] * 3 + [vp, vp], C.c_int),
         "plato_box_nodeset": ([C.c_int32] * 4 + [vp, i32p], C.c_int),

@@ -221,6 +221,17 @@ struct plato_problem {
     double* ritz_scratch = nullptr;
     size_t  ritz_scratch_len = 0;
     double  ritz_rel_gain = 1.0;   // ||r|| after / before the last subspace correction (1: not used)
+    // Helmholtz density filter (helmholtz.cu): physics 1, one unknown per node
+    int32_t physics = 0;           // 0 elastostatics, 1 Helmholtz filter
+    double  helm_length = 0.0;     // length scale L
+    int32_t helm_ready = 0;        // K, its SELL copy and diagonal built
+    double* helm_K = nullptr;      // one value per block of the node pattern
+    double* helm_sell = nullptr;   // SELL copy (one value per slot)
+    double* helm_dinv = nullptr;   // inverse diagonal
+    double  helm_surface = 0.0;    // surface length scale alpha (0: no surface term)
+    int32_t helm_nfaces = 0;       // faces carrying the surface term
+    int32_t* helm_fcell = nullptr; // their owning cells
+    int32_t* helm_floc = nullptr;  // 3 cell-local node ordinals per face
 };
 
 // ---------------------------------------------------------------------------------------

@@ -65,6 +65,45 @@ k_sell_spmv(SellView A, const double* __restrict__ vals, const double* __restric
     }
 }
 
+// Scalar (one value per node) y = A x on the SELL pattern: value of slot k of row 32s+l at
+// ptr_s + 32k + l; with S != nullptr also p.Ap and alpha.
+__global__ void __launch_bounds__(kThreads, 6)
+k_sell1_spmv(SellView A, const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
+             PcgScalars* S, double* partials) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S && S->done) return;
+    double dot = 0.0;
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < padded; r += nthreads) {
+        const int64_t sl = r >> 5;
+        const int l = int(r & 31);
+        const int w = __ldg(A.width + sl);
+        const int64_t base = __ldg(A.ptr + sl) + l;
+        double a = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < w; ++k) a += __ldg(vals + base + 32 * k) * __ldg(x + __ldg(A.cols + base + 32 * k));
+        if (r < A.num_rows) {
+            y[r] = a;
+            if (S) dot += x[r] * a;
+        }
+    }
+    if (!S) return;
+    double v[1] = {dot};
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            S->pAp = t[0];
+            S->alpha = S->rz / t[0];
+            if (!isfinite(S->alpha) || t[0] <= 0.0) { S->nonfinite = 1; S->done = 1; }
+            S->ticket = 0u;
+        }
+    }
+}
+
 // x += alpha p; r -= alpha Ap; z = Dinv r; then r.z, r.r -> beta and the stop test.
 __global__ void __launch_bounds__(kThreads)
 k_pcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
@@ -233,19 +272,17 @@ int prepare_operator(plato_problem* h, const double* crs) {
     return launch_crs_to_sell(h, crs, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
 }
 
-// Solves A x = b with A in h->sell64 and its inverse diagonal in h->v_dinv.  x holds the
-// initial guess on entry.
-int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
-    const double* A = h->sell64;
-    const int64_t n = 3 * (int64_t)h->N;
+// Jacobi-PCG on n unknowns with the operator apply(in, out, S) (S != nullptr: fused p.Ap and
+// alpha) and inverse diagonal dinv; x holds the initial guess on entry.
+template <class Apply>
+static int pcg_run(plato_problem* h, int64_t n, Apply apply, const double* dinv, const double* b, double* x,
+                   plato_solve_stats* stats) {
     cudaStream_t s = h->stream;
     const double tol = h->opts.tolerance;
     const int32_t max_it = h->opts.max_iterations;
     const int vec_blocks = grid_for(n, kThreads, 148 * 16);
-    const int sp_blocks = spmv_blocks(h);
-    if (vec_blocks * 3 > 4 * h->partials_len || sp_blocks > 4 * h->partials_len)
+    if (vec_blocks * 3 > 4 * h->partials_len || spmv_blocks(h) > 4 * h->partials_len)
         return plato_fail(h, PLATO_BAD_INPUT, "reduction scratch too small");
-    const SellView V = sell_view(h);
 
     PcgScalars init{};
     PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
@@ -255,9 +292,9 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     bool keep_bb = false;
     for (;;) {
         // r = b - A x ; z = Dinv r ; p = z
-        int rc = launch_sell_spmv(h, A, x, h->v_r);
+        int rc = apply(x, h->v_r, nullptr);
         if (rc) return rc;
-        k_pcg_start<<<vec_blocks, kThreads, 0, s>>>(n, b, h->v_r, h->v_dinv, h->v_z, h->v_p, h->scal,
+        k_pcg_start<<<vec_blocks, kThreads, 0, s>>>(n, b, h->v_r, dinv, h->v_z, h->v_p, h->scal,
                                                      h->partials, tol, keep_bb ? 1 : 0);
         PLATO_LAUNCH_CHECK(h);
         PcgScalars* slots = h->scal_host;
@@ -279,13 +316,14 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                     timed_iters.push_back(2 * enqueued);
                     PLATO_CUDA(h, cudaEventRecord(e0, s));
                 }
-                k_sell_spmv<<<sp_blocks, kThreads, 0, s>>>(V, A, h->v_p, h->v_Ap, h->scal, h->partials);
+                rc = apply(h->v_p, h->v_Ap, h->scal);
+                if (rc) return rc;
                 if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
-                k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_Ap, h->v_dinv, h->v_z,
+                k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_Ap, dinv, h->v_z,
                                                              h->scal, h->partials, max_it);
                 k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
             }
-            h->launches += 3 * kChunk - 1;
+            h->launches += 2 * kChunk - 1;  // the operator applies count themselves
             PLATO_LAUNCH_CHECK(h);
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
@@ -313,7 +351,7 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             return plato_fail(h, PLATO_NONFINITE, "non-finite value in the conjugate-gradient recurrences");
         }
         // true residual: r = b - A x
-        rc = launch_sell_spmv(h, A, x, h->v_Ap);
+        rc = apply(x, h->v_Ap, nullptr);
         if (rc) return rc;
         rc = launch_axpby(h, n, 1.0, b, 0.0, h->v_r);
         if (rc) return rc;
@@ -346,6 +384,40 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         cont.done = 0;
         PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &cont, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
     }
+}
+
+// Solves A x = b with A in h->sell64 and its inverse diagonal in h->v_dinv.  x holds the
+// initial guess on entry.
+int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
+    const SellView V = sell_view(h);
+    const int sp_blocks = spmv_blocks(h);
+    const double* A = h->sell64;
+    auto apply = [&](const double* in, double* out, PcgScalars* S) -> int {
+        k_sell_spmv<<<sp_blocks, kThreads, 0, h->stream>>>(V, A, in, out, S, S ? h->partials : nullptr);
+        PLATO_LAUNCH_CHECK(h);
+        return PLATO_OK;
+    };
+    return pcg_run(h, 3 * (int64_t)h->N, apply, h->v_dinv, b, x, stats);
+}
+
+// Scalar Jacobi-PCG (one unknown per node) on SELL values `vals` with inverse diagonal dinv.
+int pcg_scalar(plato_problem* h, const double* vals, const double* dinv, const double* b, double* x,
+               plato_solve_stats* stats) {
+    const SellView V = sell_view(h);
+    const int sp_blocks = spmv_blocks(h);
+    auto apply = [&](const double* in, double* out, PcgScalars* S) -> int {
+        k_sell1_spmv<<<sp_blocks, kThreads, 0, h->stream>>>(V, vals, in, out, S, S ? h->partials : nullptr);
+        PLATO_LAUNCH_CHECK(h);
+        return PLATO_OK;
+    };
+    return pcg_run(h, (int64_t)h->N, apply, dinv, b, x, stats);
+}
+
+// y = A x for a scalar SELL matrix.
+int launch_sell1_spmv(plato_problem* h, const double* vals, const double* x, double* y) {
+    k_sell1_spmv<<<spmv_blocks(h), kThreads, 0, h->stream>>>(sell_view(h), vals, x, y, nullptr, nullptr);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
 }
 
 }  // namespace plato

@@ -50,6 +50,39 @@ class BoxMesh:
         return cells, local
 
 
+    def sides(self, faces) -> tuple[np.ndarray, np.ndarray]:
+        """The faces of several box sides, concatenated: (owning cells, 3 local node ordinals)."""
+        parts = [self.sideset(f) for f in faces]
+        if not parts:
+            return np.zeros(0, np.int32), np.zeros((0, 3), np.int32)
+        return np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts])
+
+
+# cell-local node ordinals of the four faces of a tet
+TET_FACES = np.array([[0, 1, 3], [1, 2, 3], [0, 3, 2], [0, 2, 1]], dtype=np.int32)
+
+
+def exterior_faces(connectivity: np.ndarray, exclude_nodes: np.ndarray | None = None):
+    """Faces that belong to exactly one cell, as (owning cells, 3 local node ordinals), in cell
+    order.  With `exclude_nodes`, faces whose three nodes all lie in that node set are left
+    out (the complement of a side set given by its nodes, as the Helmholtz filter's surface
+    term takes it)."""
+    conn = np.ascontiguousarray(connectivity, dtype=np.int64)
+    nc = conn.shape[0]
+    tri = conn[:, TET_FACES]                      # (nc, 4, 3) global nodes
+    key = np.sort(tri.reshape(-1, 3), axis=1)
+    _, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    once = cnt[inv.reshape(-1)] == 1
+    if exclude_nodes is not None and len(exclude_nodes):
+        mark = np.zeros(int(conn.max()) + 1, dtype=bool)
+        mark[np.asarray(exclude_nodes, dtype=np.int64)] = True
+        once &= ~mark[key].all(axis=1)
+    idx = np.nonzero(once)[0]
+    cells = (idx // 4).astype(np.int32)
+    local = TET_FACES[idx % 4].astype(np.int32)
+    return cells, local
+
+
 def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0, lz: float = 1.0) -> BoxMesh:
     nn, nc = C.c_int32(0), C.c_int32(0)
     check(lib.plato_box_mesh_sizes(nx, ny, nz, C.byref(nn), C.byref(nc)))

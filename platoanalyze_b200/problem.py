@@ -312,3 +312,97 @@ class EllipticProblem:
                                                        _np_ptr(u), C.byref(v), _np_ptr(g), C.byref(st))
         check(rc, self.h)
         return u, v.value, g, st.as_dict()
+
+
+class HelmholtzFilter:
+    """Helmholtz density filter (src/helmholtz/Problem.hpp) over a tet mesh with length scale L
+    and, optionally, the surface term with multiplier alpha on `surface_faces` = (owning cells,
+    3 local node ordinals) - the exterior faces outside the symmetry planes, e.g.
+    `mesh.exterior_faces(connectivity, symmetry_nodes)`.  One unknown per node; vectors are
+    device (torch) arrays of num_nodes values."""
+
+    def __init__(self, coords, connectivity, length_scale: float, surface_length_scale: float = 0.0,
+                 surface_faces=None, tolerance: float = 1e-12, max_iterations: int = 100000, stream=None):
+        import torch
+
+        self.torch = torch
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        conn = np.ascontiguousarray(connectivity, dtype=np.int32)
+        if surface_faces is None:
+            fc, fl = np.zeros(0, np.int32), np.zeros((0, 3), np.int32)
+        else:
+            fc = np.ascontiguousarray(surface_faces[0], dtype=np.int32)
+            fl = np.ascontiguousarray(surface_faces[1], dtype=np.int32)
+        mesh = capi.MeshDesc(coords.shape[0], conn.shape[0], coords.ctypes.data_as(capi.f64p),
+                             conn.ctypes.data_as(capi.i32p))
+        opts = SolverOptions(tolerance=tolerance, max_iterations=max_iterations).to_c()
+        desc = capi.HelmholtzDesc(mesh, float(length_scale), float(surface_length_scale), fc.size,
+                                  fc.ctypes.data_as(capi.i32p), fl.ctypes.data_as(capi.i32p), opts)
+        h = C.c_void_p()
+        check(lib.plato_create_helmholtz(C.byref(desc), C.byref(h)))
+        self.h = h
+        self.length_scale = float(length_scale)
+        self.surface_length_scale = float(surface_length_scale)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        check(lib.plato_set_stream(h, C.c_void_p(self.stream.cuda_stream)), h)
+        nn, nc, nb = C.c_int32(), C.c_int32(), C.c_int64()
+        check(lib.plato_get_sizes(h, C.byref(nn), C.byref(nc), C.byref(nb)), h)
+        self.num_nodes, self.num_cells, self.num_blocks = nn.value, nc.value, nb.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib.plato_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _dev(self, t):
+        return C.c_void_p(t.data_ptr())
+
+    def to_dev(self, a):
+        return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+    def zeros(self, n, dtype=None):
+        return self.torch.zeros(n, dtype=dtype or self.torch.float64, device="cuda")
+
+    set_timing = EllipticProblem.set_timing
+    instrumentation = EllipticProblem.instrumentation
+    reset_instrumentation = EllipticProblem.reset_instrumentation
+
+    def pattern(self):
+        rm = self.zeros(self.num_nodes + 1, self.torch.int32)
+        cols = self.zeros(self.num_blocks, self.torch.int32)
+        check(lib.plato_jacobian_pattern(self.h, self._dev(rm), self._dev(cols)), self.h)
+        return rm, cols
+
+    def value(self, filtered, control):
+        R = self.zeros(self.num_nodes)
+        check(lib.plato_helmholtz_value(self.h, self._dev(filtered), self._dev(control), self._dev(R)), self.h)
+        return R
+
+    def gradient_u(self):
+        K = self.zeros(self.num_blocks)
+        check(lib.plato_helmholtz_gradient_u(self.h, self._dev(K)), self.h)
+        return K
+
+    def gradient_z(self):
+        K = self.zeros(self.num_blocks)
+        check(lib.plato_helmholtz_gradient_z(self.h, self._dev(K)), self.h)
+        return K
+
+    def solution(self, control):
+        f = self.zeros(self.num_nodes)
+        st = capi.SolveStats()
+        check(lib.plato_helmholtz_solution(self.h, self._dev(control), self._dev(f), C.byref(st)), self.h)
+        return f, st.as_dict()
+
+    def criterion_gradient(self, dfdfiltered):
+        g = self.zeros(self.num_nodes)
+        st = capi.SolveStats()
+        check(lib.plato_helmholtz_criterion_gradient(self.h, self._dev(dfdfiltered), self._dev(g), C.byref(st)),
+              self.h)
+        return g, st.as_dict()

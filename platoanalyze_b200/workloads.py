@@ -17,6 +17,7 @@ from .problem import ProblemSpec, SolverOptions, cantilever_spec
 SEED_LARGE = 0x5EED0002
 SEED_MIXED = 0x5EED0003
 SEED_BATCH = 0x5EED0004
+SEED_FILTER = 0x5EED0005
 BATCH_SIZES = (16, 24, 32, 48, 64)
 
 

@@ -1,7 +1,8 @@
 // C++ caller of the adapter (include/plato_b200.hpp), written the way the reference's
 // DerivativeTests.ElastostaticResidual3D / InternalElasticEnergy3D drive
 // VectorFunction and PhysicsScalarFunction (unit_tests/DerivativeTests.cpp:257-634), plus a
-// Problem::solution / criterionValue / criterionGradient sequence on a small cantilever.
+// Problem::solution / criterionValue / criterionGradient sequence on a small cantilever,
+// and Helmholtz::Problem / VectorFunction on the same mesh.
 // Prints "key: values..." lines; tests/test_gpu_adapter.py compares them with the golds.
 #include <cstdio>
 #include <vector>
@@ -89,6 +90,28 @@ int main() {
         std::printf("compliance: %.17g\n", f);
         print("state", state.to_host(), 3 * size_t(nn));
         print("dcdz", g, size_t(nn));
+
+        // ---- Helmholtz filter on the same mesh, surface term on the x = 2 side ------------
+        plato_helmholtz_desc hd{};
+        hd.mesh = d.mesh;
+        hd.length_scale = 0.2;
+        hd.surface_length_scale = 0.5;
+        hd.num_surface_faces = nface;
+        hd.surface_face_cells = fc.data();
+        hd.surface_face_local_nodes = fl.data();
+        hd.solver.tolerance = 1e-13;
+        auto filter = std::make_shared<Model>(hd);
+        Helmholtz::Problem hp(filter);
+        std::vector<double> ctl(static_cast<size_t>(nn)), w(static_cast<size_t>(nn));
+        for (int32_t i = 0; i < nn; ++i) {
+            ctl[i] = 0.25 + 0.5 * ((i * 7919) % 101) / 100.0;
+            w[i] = 1.0 + 0.01 * (i % 13);
+        }
+        ScalarVector ctl_d(ctl), w_d(w);
+        print("filtered", hp.solution(ctl_d).to_host(), size_t(nn));
+        print("filter_gradient", hp.criterionGradient(w_d).to_host(), size_t(nn));
+        Helmholtz::VectorFunction hvf(filter);
+        print("filter_jacobian", hvf.gradient_u(ctl_d, ctl_d)->entries.to_host(), size_t(filter->numBlocks()));
 
         // error path: an exception carries the status
         try {

@@ -56,3 +56,21 @@ def test_adapter_problem_matches_oracle(output):
     assert rel_l2(vals(output["dcdz"]), orc.criterion_gradient(z, u)) <= 1e-11
     assert "converged 1" in output["solve"]
     assert output["error_path"] == "status 1"
+
+
+def test_adapter_helmholtz_matches_oracle(output):
+    from platoanalyze_b200.mesh import X_PLUS, box_mesh
+
+    m = box_mesh(6, 3, 3, 2.0, 1.0, 1.0)
+    orc = Oracle(m.coords, m.connectivity)
+    n = m.num_nodes
+    i = np.arange(n)
+    control = 0.25 + 0.5 * ((i * 7919) % 101) / 100.0
+    w = 1.0 + 0.01 * (i % 13)
+    cells, local = m.sideset(X_PLUS)
+    S = (0.5, cells, local)
+    fo, _ = orc.helmholtz_solution(0.2, control, tol=1e-14, surface=S)
+    go, _ = orc.helmholtz_criterion_gradient(0.2, w, tol=1e-14, surface=S)
+    assert rel_l2(vals(output["filtered"]), fo) <= 1e-10
+    assert rel_l2(vals(output["filter_gradient"]), go) <= 1e-10
+    assert rel_l2(vals(output["filter_jacobian"]), orc.helmholtz_gradient_u(0.2, surface=S)) <= 1e-13

@@ -203,6 +203,13 @@ int plato_apply_operator(plato_problem* h, const double* z, int32_t operator_kin
 int plato_solver_solve(plato_problem* h, const double* entries, double* x, const double* b,
                        plato_solve_stats* stats);
 
+/* ---- two-level preconditioner diagnostics (no reference counterpart) ------------------
+ * The Galerkin coarse operator E = (PZ)^T K(z) (PZ) of the solver options' coarse grid
+ * (Z trilinear on the box grid, P masking the constrained dofs; a dof whose column
+ * vanishes gets a unit diagonal) and the E^-1 the preconditioner applies, both [host]
+ * row-major ndof x ndof.  With E and Einv NULL only *ndof is set.  z [device]. */
+int plato_coarse_operator(plato_problem* h, const double* z, int32_t* ndof, double* E, double* Einv);
+
 /* ---- Elliptic::Problem (src/elliptic/Problem.hpp) --------------------------------------- */
 /* solution(z), :237-292; u [device] receives the state.  u0 (may be NULL) seeds the solve. */
 int plato_problem_solution(plato_problem* h, const double* z, const double* u0, double* u,
@@ -351,6 +358,71 @@ int plato_helmholtz_solution(plato_problem* h, const double* control, double* fi
  * the input is not negated in place. */
 int plato_helmholtz_criterion_gradient(plato_problem* h, const double* dfdfiltered, double* dfdcontrol,
                                        plato_solve_stats* stats);
+
+/* ---- MPMD application (src/Analyze_App.hpp, src/Analyze_App.cpp; Plato::Application) --
+ * The reference's Analyze application driven by PlatoEngine: an input deck (Teuchos
+ * ParameterList XML: "Input Mesh", "Physics", "PDE Constraint", "Spatial Model", "Material
+ * Models", "Elliptic" > "Penalty Function", "Criteria", "Natural Boundary Conditions",
+ * "Essential Boundary Conditions", "Linear Solver", "Self-Adjoint"; for the filter
+ * "Parameters" > "Length Scale", "Surface Length Scale", "Symmetry Plane Sides") and an
+ * operations file (<Operation> elements: Function, Name, Criterion, Target, ProblemDefinition,
+ * Output > Argument/ArgumentName, Parameter > ArgumentName/Target/InitialValue).
+ * Functions built: ComputeSolution, ComputeCriterion, ComputeCriterionValue,
+ * ComputeCriterionGradient, ApplyHelmholtz, ApplyHelmholtzGradient, UpdateProblem.
+ * "Input Mesh" = an Exodus II file (plato_mesh_file_open; relative to base_dir) or
+ * "box:NX,NY,NZ[:LX,LY,LZ]" (generated; node and side sets x-, x+, y-, y+, z-, z+).
+ * Shared data crosses as host arrays: fields of num_nodes values, values of one. */
+typedef struct plato_app plato_app;
+typedef enum plato_data_layout {
+    PLATO_LAYOUT_SCALAR_FIELD     = 0, /* nodal field ("Topology", gradients, state components) */
+    PLATO_LAYOUT_SCALAR_VALUE     = 1, /* one number (criterion value minus its Target)         */
+    PLATO_LAYOUT_SCALAR_PARAMETER = 2  /* operation parameter; context = the operation's Name    */
+} plato_data_layout;
+/* MPMD_App constructor + initialize (src/Analyze_App.cpp:301-366).  input_config and
+ * operations are XML text (first non-blank character '<') or file names, relative to
+ * base_dir (may be NULL).  On failure *out is NULL and plato_app_last_error(NULL) says why. */
+int plato_app_create(const char* input_config, const char* operations, const char* base_dir, plato_app** out);
+/* Host-only check of a deck and operations file: parses both, generates the mesh, resolves
+ * every problem definition (material, penalties, boundary conditions against the mesh's
+ * sets, criteria, solver) and each operation's criterion, without touching the GPU.
+ * message (may be NULL) receives the first error, truncated to capacity. */
+int plato_app_validate(const char* input_config, const char* operations, const char* base_dir, char* message,
+                       int64_t capacity);
+/* The deck as parsed, one "name (type) = value" line per parameter, sublists indented;
+ * *needed = bytes including the terminator (call with text NULL to size the buffer). */
+int plato_deck_to_text(const char* input_config, char* text, int64_t capacity, int64_t* needed);
+int plato_app_destroy(plato_app* app);
+const char* plato_app_last_error(const plato_app* app);
+int plato_app_num_nodes(const plato_app* app, int32_t* num_nodes);
+/* MPMD_App::compute (src/Analyze_App.cpp:566-590) */
+int plato_app_compute(plato_app* app, const char* operation);
+/* MPMD_App::importDataT (src/Analyze_App.hpp:181-195): "Topology" (or "Solution") fields,
+ * operation parameters (context = operation name) */
+int plato_app_import(plato_app* app, const char* name, int32_t layout, const char* context, const double* data,
+                     int64_t count);
+/* MPMD_App::exportDataT (src/Analyze_App.hpp:287-312): criterion values and gradients by
+ * their ArgumentName, "Topology", state components ("displacement X" / "Y" / "Z",
+ * "filtered density") */
+int plato_app_export(plato_app* app, const char* name, int32_t layout, double* data, int64_t count);
+
+/* ---- Exodus II mesh files (the reference's "Input Mesh"; src/EngineMesh.cpp,
+ * src/OmegaHMesh.cpp) --------------------------------------------------------------------
+ * Host-only reader of netCDF classic encodings (CDF-1, CDF-2, CDF-5; a netCDF-4/HDF5 file is
+ * refused): coordinates, the 4-node tetrahedral element blocks in order, node sets and side
+ * sets with their names (else "nodelist_<id>" / "sideset_<id>").  Indices are 0-based on
+ * output; a side becomes its cell and 3 cell-local node ordinals (Exodus tetrahedron sides
+ * 1: (1,2,4), 2: (2,3,4), 3: (1,4,3), 4: (1,3,2)).  Call a getter with NULL arrays to size. */
+typedef struct plato_mesh_file plato_mesh_file;
+int plato_mesh_file_open(const char* path, plato_mesh_file** out);
+const char* plato_mesh_file_last_error(void);
+int plato_mesh_file_close(plato_mesh_file* m);
+int plato_mesh_file_info(const plato_mesh_file* m, int32_t* num_nodes, int32_t* num_cells, int32_t* num_node_sets,
+                         int32_t* num_side_sets);
+int plato_mesh_file_mesh(const plato_mesh_file* m, double* coords /*[host] 3N*/, int32_t* connectivity /*[host] 4C*/);
+int plato_mesh_file_node_set(const plato_mesh_file* m, int32_t index, char* name, int64_t name_capacity,
+                             int32_t* nodes, int32_t* count);
+int plato_mesh_file_side_set(const plato_mesh_file* m, int32_t index, char* name, int64_t name_capacity,
+                             int32_t* cells, int32_t* local_nodes /*3 per face*/, int32_t* count);
 
 /* ---- box mesh generator (host only; stands in for BamG, unit_tests/PlatoTestHelpers.hpp) */
 int plato_box_mesh_sizes(int32_t nx, int32_t ny, int32_t nz, int32_t* num_nodes, int32_t* num_cells);

@@ -56,7 +56,7 @@ def build_library(verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     LIB.parent.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    headers = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(INCLUDE.glob("*.h"))
     jobs = []
     objs = []
     for src in sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp")):

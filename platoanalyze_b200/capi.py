@@ -11,6 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libplato_b200.so"
 
 OK, BAD_INPUT, NOT_CONVERGED, NONFINITE, DEVICE_TIMEOUT, CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED = range(8)
+LAYOUT_SCALAR_FIELD, LAYOUT_SCALAR_VALUE, LAYOUT_SCALAR_PARAMETER = range(3)
 STATUS_NAMES = ["OK", "BAD_INPUT", "NOT_CONVERGED", "NONFINITE", "DEVICE_TIMEOUT", "CUDA_ERROR",
                 "OUT_OF_MEMORY", "NOT_SUPPORTED"]
 
@@ -138,6 +139,23 @@ def _load() -> C.CDLL:
         "plato_helmholtz_gradient_z": ([vp, vp], C.c_int),
         "plato_helmholtz_solution": ([vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_helmholtz_criterion_gradient": ([vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_app_create": ([C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(vp)], C.c_int),
+        "plato_app_destroy": ([vp], C.c_int),
+        "plato_app_last_error": ([vp], C.c_char_p),
+        "plato_app_num_nodes": ([vp, i32p], C.c_int),
+        "plato_app_compute": ([vp, C.c_char_p], C.c_int),
+        "plato_app_import": ([vp, C.c_char_p, C.c_int32, C.c_char_p, vp, C.c_int64], C.c_int),
+        "plato_app_export": ([vp, C.c_char_p, C.c_int32, vp, C.c_int64], C.c_int),
+        "plato_app_validate": ([C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64], C.c_int),
+        "plato_deck_to_text": ([C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+        "plato_coarse_operator": ([vp, vp, i32p, vp, vp], C.c_int),
+        "plato_mesh_file_open": ([C.c_char_p, C.POINTER(vp)], C.c_int),
+        "plato_mesh_file_last_error": ([], C.c_char_p),
+        "plato_mesh_file_close": ([vp], C.c_int),
+        "plato_mesh_file_info": ([vp, i32p, i32p, i32p, i32p], C.c_int),
+        "plato_mesh_file_mesh": ([vp, vp, vp], C.c_int),
+        "plato_mesh_file_node_set": ([vp, C.c_int32, C.c_char_p, C.c_int64, vp, i32p], C.c_int),
+        "plato_mesh_file_side_set": ([vp, C.c_int32, C.c_char_p, C.c_int64, vp, vp, i32p], C.c_int),
         "plato_box_mesh_sizes": ([C.c_int32] * 3 + [i32p, i32p], C.c_int),
         "plato_box_mesh_tet4": ([C.c_int32] * 3 + [C.c_double] * 3 + [vp, vp], C.c_int),
         "plato_box_nodeset": ([C.c_int32] * 4 + [vp, i32p], C.c_int),

@@ -134,7 +134,7 @@ int plato_destroy(plato_problem* h) {
     coarse_release(h);
     batch_release(h);
     if (h->ritz_scratch) cudaFree(h->ritz_scratch);
-    dfree(h->helm_K); dfree(h->helm_sell); dfree(h->helm_dinv); dfree(h->helm_fcell); dfree(h->helm_floc);
+    dfree(h->helm_K); dfree(h->helm_sell); dfree(h->helm_D); dfree(h->helm_Dsell); dfree(h->helm_dinv); dfree(h->helm_fcell); dfree(h->helm_floc);
     delete h;
     return PLATO_OK;
 }

@@ -11,10 +11,13 @@
 // from each element (the isotropic block formula with coarse gradients).
 //
 // Per solve: the elements of each coarse cell are split over about eight CTAs per SM; each
-// CTA stages batches of elements' coarse gradients in shared memory and sums its share of
-// the cell's symmetric 24x24 block (upper triangle) in registers, then adds it to E.  E is
+// CTA stages batches of elements' coarse gradients in shared memory and accumulates its
+// share of the cell's symmetric 24x24 block in registers (as a rank-k update of the
+// gradients for the elements whose nodes are free or fully clamped, entry by entry for the
+// rest), then adds it to E.  E is
 // factored (blocked Cholesky, 32x32 tiles) and inverted explicitly (E^-1 = L^-T L^-1), so a
-// coarse solve in the iteration is one dense matrix-vector product.
+// coarse solve in the iteration is one dense matrix-vector product.  Each diagonal tile's
+// inverse is formed as the tile is factored, so the panels and the inverse are tile products.
 // Per preconditioner call: restriction in two deterministic passes (per-cell partial sums by
 // split CTAs, then a fixed-order sum per coarse dof), y_c = E^-1 r_c (warp per row),
 // prolongation (thread per fine node).
@@ -72,10 +75,12 @@ __global__ void k_node_keys(int32_t N, const double* __restrict__ coords, Coarse
     }
 }
 
-// cell of an element = cell of its centroid; flags elements with a node outside that cell
+// cell of an element = cell of its centroid; flags elements with a node outside that cell.
+// key = 2 cell + 1 when some node of the element has its three dofs constrained unalike
+// (those take the general Galerkin kernel), 2 cell otherwise.
 __global__ void k_elem_keys(int32_t C, const int4* __restrict__ conn, const double* __restrict__ coords, CoarseView cv,
-                            uint32_t* __restrict__ key, int32_t* __restrict__ val, int32_t* __restrict__ count,
-                            int32_t* __restrict__ bad) {
+                            const uint8_t* __restrict__ mask, uint32_t* __restrict__ key, int32_t* __restrict__ val,
+                            int32_t* __restrict__ count, int32_t* __restrict__ bad) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < C; e += (int64_t)gridDim.x * blockDim.x) {
         const int4 n = conn[e];
         double x[4][3];
@@ -92,10 +97,16 @@ __global__ void k_elem_keys(int32_t C, const int4* __restrict__ conn, const doub
                 const double t = (x[a][d] - lo[d]) / hh[d];
                 if (t < -1e-9 || t > 1.0 + 1e-9) atomicExch(bad, 1);
             }
-        const int cid = cell_id(cv, cx, cy, cz);
-        key[e] = uint32_t(cid);
+        const int ids[4] = {n.x, n.y, n.z, n.w};
+        int mixed = 0;
+        for (int a = 0; a < 4; ++a) {
+            const uint8_t* m = mask + 3 * (int64_t)ids[a];
+            mixed |= (m[0] != m[1]) || (m[0] != m[2]);
+        }
+        const int k = 2 * cell_id(cv, cx, cy, cz) + mixed;
+        key[e] = uint32_t(k);
         val[e] = int32_t(e);
-        atomicAdd(&count[cid], 1);
+        atomicAdd(&count[k], 1);
     }
 }
 
@@ -106,8 +117,141 @@ __device__ __forceinline__ void upper_entry(int t, int& r, int& c) {
     c = r + t;
 }
 
-// E (n x n, row-major) += Galerkin contribution of every element.  CTA (cell, split) takes a
-// contiguous share of the coarse cell's elements in batches of kBatch: eight threads per
+// Common path: for an element whose nodes are each either free or fully clamped, the coarse
+// gradient is one vector per corner, g_J = sum over free nodes a of phi_J(x_a) grad N_a, and
+// every entry of the cell's 24 x 24 block of E is a fixed combination of
+//   M = sum_e w_e g g^T   (g = (g_0, ..., g_7), 24 values; w_e = vol s(rho))
+// E_(J,i),(L,j) = lam M_(Ji),(Lj) + mu M_(Jj),(Li) + mu delta_ij sum_k M_(Jk),(Lk).
+// M is a symmetric rank-k update: CTA (cell, split) stages kFastBatch elements' (w, g) in
+// shared memory (one thread per element), then 250 threads accumulate the ten upper 6 x 6
+// tiles of M in registers, each over a fixed slice of the batch (25 slices); the slices are
+// summed in shared memory, the block formula applied, and the upper triangle added to E
+// (mirrored) once per CTA.
+constexpr int kFastBatch = 256;
+constexpr int kSlices = 25;
+
+__global__ void __launch_bounds__(kThreadsPerCta)
+k_galerkin_fast(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, const int32_t* __restrict__ elem_list,
+                const int4* __restrict__ conn, const double* __restrict__ coords, const double* __restrict__ z,
+                Material mat, const uint8_t* __restrict__ mask, int n, double* __restrict__ E) {
+    extern __shared__ double smem[];
+    double* Gs = smem;                       // [kFastBatch][25]: w, then g (24)
+    double* Red = smem;                      // [kSlices][10][36] after the last batch
+    double* Ms = smem + kSlices * 10 * 36;   // [24][24]
+    const double lam = mat.c01, mu = mat.c33;
+    const int cell = blockIdx.x / split, part = blockIdx.x - cell * split;
+    const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
+    const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
+    const int q0 = elem_ptr[2 * cell], q1 = elem_ptr[2 * cell + 1];
+    const int chunk = (q1 - q0 + split - 1) / split;
+    const int e0 = q0 + part * chunk, e1 = min(q1, e0 + chunk);
+    const int tid = threadIdx.x;
+    // tile t of the upper 4 x 4 grid of 6 x 6 tiles: (ti, tj), ti <= tj
+    const int tile = tid % 10, slice = tid / 10;
+    int ti = 0, tj = tile;
+    while (tj >= 4 - ti) { tj -= 4 - ti; ++ti; }
+    tj += ti;
+    double acc[36];
+#pragma unroll
+    for (int q = 0; q < 36; ++q) acc[q] = 0.0;
+    for (int base = e0; base < e1; base += kFastBatch) {
+        const int nb = min(kFastBatch, e1 - base);
+        if (tid < nb) {
+            const int4 nd = conn[elem_list[base + tid]];
+            double x[4][3];
+            load_cell_coords(coords, nd, x);
+            TetGeom<double> G;
+            tet_geometry(x, G);
+            const double rho = (z[nd.x] + z[nd.y] + z[nd.z] + z[nd.w]) * 0.25;
+            double* row = Gs + tid * 25;
+            row[0] = G.vol * simp(mat, rho);
+            const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
+            double uvw[4][3];
+            bool freeN[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                uvw[a][0] = (x[a][0] - lo[0]) * cv.ihx;
+                uvw[a][1] = (x[a][1] - lo[1]) * cv.ihy;
+                uvw[a][2] = (x[a][2] - lo[2]) * cv.ihz;
+                freeN[a] = mask[3 * (int64_t)ids[a]] == 0;
+            }
+#pragma unroll
+            for (int J = 0; J < 8; ++J) {
+                double gj[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    if (!freeN[a]) continue;
+                    const double wa = corner_weight(J, uvw[a][0], uvw[a][1], uvw[a][2]);
+                    gj[0] += wa * G.g[a][0];
+                    gj[1] += wa * G.g[a][1];
+                    gj[2] += wa * G.g[a][2];
+                }
+                row[1 + 3 * J] = gj[0];
+                row[2 + 3 * J] = gj[1];
+                row[3 + 3 * J] = gj[2];
+            }
+        }
+        __syncthreads();
+        if (slice < kSlices) {
+            for (int e = slice; e < nb; e += kSlices) {
+                const double* row = Gs + e * 25;
+                const double w = row[0];
+                double a[6], b[6];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    a[q] = w * row[1 + 6 * ti + q];
+                    b[q] = row[1 + 6 * tj + q];
+                }
+#pragma unroll
+                for (int r = 0; r < 6; ++r)
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) acc[6 * r + c] += a[r] * b[c];
+            }
+        }
+        __syncthreads();
+    }
+    if (e0 >= e1) return;  // uniform across the CTA: nothing staged, nothing to add
+    if (slice < kSlices)
+#pragma unroll
+        for (int q = 0; q < 36; ++q) Red[(slice * 10 + tile) * 36 + q] = acc[q];
+    __syncthreads();
+    // M (full 24 x 24) from the slice sums of the upper tiles
+    for (int t = tid; t < 360; t += blockDim.x) {
+        const int tl = t / 36, q = t - 36 * tl;
+        double sum = 0.0;
+        for (int sl = 0; sl < kSlices; ++sl) sum += Red[(sl * 10 + tl) * 36 + q];
+        int a0 = 0, b0 = tl;
+        while (b0 >= 4 - a0) { b0 -= 4 - a0; ++a0; }
+        b0 += a0;
+        if (a0 == b0 && q / 6 > q % 6) continue;  // a diagonal tile's lower half mirrors its upper
+        const int r = 6 * a0 + q / 6, c = 6 * b0 + q % 6;
+        Ms[r * 24 + c] = sum;
+        Ms[c * 24 + r] = sum;
+    }
+    __syncthreads();
+    // upper triangle of the cell's E block
+    for (int t = tid; t < 300; t += blockDim.x) {
+        int R, Cc;
+        upper_entry(t, R, Cc);
+        const int Jr = R / 3, i = R - 3 * Jr, L = Cc / 3, j = Cc - 3 * L;
+        double v = lam * Ms[(3 * Jr + i) * 24 + 3 * L + j] + mu * Ms[(3 * Jr + j) * 24 + 3 * L + i];
+        if (i == j)
+            v += mu * (Ms[(3 * Jr) * 24 + 3 * L] + Ms[(3 * Jr + 1) * 24 + 3 * L + 1] + Ms[(3 * Jr + 2) * 24 + 3 * L + 2]);
+        if (v == 0.0) continue;
+        const int gJ = coarse_node(cv, cx + ((Jr >> 2) & 1), cy + ((Jr >> 1) & 1), cz + (Jr & 1));
+        const int gL = coarse_node(cv, cx + ((L >> 2) & 1), cy + ((L >> 1) & 1), cz + (L & 1));
+        atomicAdd(&E[(int64_t)(3 * gJ + i) * n + 3 * gL + j], v);
+        if (R != Cc) atomicAdd(&E[(int64_t)(3 * gL + j) * n + 3 * gJ + i], v);
+    }
+}
+
+constexpr size_t kFastSmem = sizeof(double) * (kSlices * 10 * 36 + 24 * 24);
+static_assert(kSlices * 10 * 36 >= kFastBatch * 25, "reduction area must cover the staging area");
+
+// General path, for elements with a node whose dofs are constrained unalike (a roller): the
+// coarse gradient then depends on the component, G_J^(d) = sum_a m_(a,d) phi_J(x_a) grad N_a.
+// E (n x n, row-major) += their Galerkin contribution.  CTA (cell, split) takes a
+// contiguous share of the coarse cell's such elements in batches of kBatch: eight threads per
 // element (one corner J each) stage its coarse gradients G_J^(i) and Q_(J,i) = w G_J^(i) in
 // shared memory, then each thread sums one or two of the 300 upper-triangle entries of the
 // cell's symmetric 24x24 block over the batch in registers; the sums are added to E (and
@@ -122,9 +266,10 @@ k_galerkin(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, const
     const int cell = blockIdx.x / split, part = blockIdx.x - cell * split;
     const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
     const double lo[3] = {cv.x0 + cx * cv.hx, cv.y0 + cy * cv.hy, cv.z0 + cz * cv.hz};
-    const int q0 = elem_ptr[cell], q1 = elem_ptr[cell + 1];
+    const int q0 = elem_ptr[2 * cell + 1], q1 = elem_ptr[2 * cell + 2];
     const int chunk = (q1 - q0 + split - 1) / split;
     const int e0 = q0 + part * chunk, e1 = min(q1, e0 + chunk);
+    if (e0 >= e1) return;
     int R[2], Cc[2];
     const int nent = threadIdx.x + kThreadsPerCta < 300 ? 2 : 1;
     upper_entry(threadIdx.x, R[0], Cc[0]);
@@ -206,11 +351,16 @@ __global__ void k_regularize(int n, double* __restrict__ E) {
 
 // ---- blocked Cholesky (lower, in place) --------------------------------------------------
 
-__global__ void k_chol_diag(int n, double* __restrict__ A, int kb, int32_t* __restrict__ bad) {
+// Factors the diagonal block kb in place (L_kk) and writes its inverse L_kk^-1 to D[kb]
+// (a 32 x 32 lower-triangular tile): the panel and the explicit inverse then need only tile
+// products, no substitution.
+__global__ void k_chol_diag(int n, double* __restrict__ A, int kb, double* __restrict__ D, int32_t* __restrict__ bad) {
     __shared__ double T[kTile][kTile + 1];
+    __shared__ double W[kTile][kTile + 1];
     const int r0 = kb * kTile, m = min(kTile, n - r0);
     const int tx = threadIdx.x, ty = threadIdx.y;
     if (tx < m && ty < m) T[ty][tx] = A[(int64_t)(r0 + ty) * n + r0 + tx];
+    W[ty][tx] = (tx == ty) ? 1.0 : 0.0;
     __syncthreads();
     for (int k = 0; k < m; ++k) {
         if (tx == 0 && ty == 0) {
@@ -224,29 +374,32 @@ __global__ void k_chol_diag(int n, double* __restrict__ A, int kb, int32_t* __re
         if (ty > k && tx > k && tx <= ty && ty < m) T[ty][tx] -= T[ty][k] * T[tx][k];
         __syncthreads();
     }
+    // W = L^-1 row by row: row r is final once divided by L_rr, then leaves the rows below
+    for (int r = 0; r < m; ++r) {
+        if (ty == r && tx <= r) W[r][tx] /= T[r][r];
+        __syncthreads();
+        if (ty > r && ty < m && tx <= r) W[ty][tx] -= T[ty][r] * W[r][tx];
+        __syncthreads();
+    }
     if (tx < m && ty < m) A[(int64_t)(r0 + ty) * n + r0 + tx] = (tx <= ty) ? T[ty][tx] : 0.0;
+    D[(int64_t)kb * kTile * kTile + ty * kTile + tx] = (tx < m && ty < m && tx <= ty) ? W[ty][tx] : 0.0;
 }
 
 // A[ib,kb] <- A[ib,kb] L_kk^-T for every block row ib > kb (one CTA per block row)
-__global__ void k_chol_panel(int n, double* __restrict__ A, int kb) {
-    __shared__ double L[kTile][kTile + 1];
+__global__ void k_chol_panel(int n, double* __restrict__ A, int kb, const double* __restrict__ D) {
+    __shared__ double Dk[kTile][kTile + 1];
     __shared__ double X[kTile][kTile + 1];
     const int ib = kb + 1 + blockIdx.x;
     const int r0 = ib * kTile, c0 = kb * kTile;
     const int mr = min(kTile, n - r0), mc = min(kTile, n - c0);
     const int tx = threadIdx.x, ty = threadIdx.y;
-    if (tx < mc && ty < mc) L[ty][tx] = A[(int64_t)(c0 + ty) * n + c0 + tx];
-    if (tx < mc && ty < mr) X[ty][tx] = A[(int64_t)(r0 + ty) * n + c0 + tx];
+    Dk[ty][tx] = D[(int64_t)kb * kTile * kTile + ty * kTile + tx];
+    X[ty][tx] = (tx < mc && ty < mr) ? A[(int64_t)(r0 + ty) * n + c0 + tx] : 0.0;
     __syncthreads();
-    // row ty solves x L^T = a: x_c = (a_c - sum_{k<c} x_k L_ck) / L_cc
-    if (tx == 0 && ty < mr)
-        for (int c = 0; c < mc; ++c) {
-            double s = X[ty][c];
-            for (int k = 0; k < c; ++k) s -= X[ty][k] * L[c][k];
-            X[ty][c] = s / L[c][c];
-        }
-    __syncthreads();
-    if (tx < mc && ty < mr) A[(int64_t)(r0 + ty) * n + c0 + tx] = X[ty][tx];
+    // (X L^-T)[ty][tx] = sum_{k <= tx} X[ty][k] Linv[tx][k]
+    double s = 0.0;
+    for (int k = 0; k <= tx; ++k) s += X[ty][k] * Dk[tx][k];
+    if (tx < mc && ty < mr) A[(int64_t)(r0 + ty) * n + c0 + tx] = s;
 }
 
 // trailing update A[ib,jb] -= A[ib,kb] A[jb,kb]^T for kb < jb <= ib
@@ -273,43 +426,50 @@ __global__ void k_chol_update(int n, double* __restrict__ A, int kb, int nblk) {
     }
 }
 
-// X = L^-1 by column blocks (one CTA per column block cb); L lower in A.
-__global__ void k_tri_inverse(int n, const double* __restrict__ A, double* __restrict__ X, int nblk) {
-    __shared__ double L[kTile][kTile + 1];
-    __shared__ double T[kTile][kTile + 1];
-    __shared__ double Y[kTile][kTile + 1];
-    const int cb = blockIdx.x;
-    const int c0 = cb * kTile, mc = min(kTile, n - c0);
+// X = L^-1 by doubling: with the inverses of two adjacent diagonal blocks B1 (above) and B2
+// known, X[B2,B1] = -X[B2,B2] L[B2,B1] X[B1,B1].  Level s joins blocks of s tiles into blocks
+// of 2s, so five levels of two batched tile-product launches cover 19 tiles, and no CTA
+// carries more than s tile products (the column-by-column substitution carried up to 171).
+// X starts as its diagonal tiles D[i] = L_ii^-1 and zeros.
+__global__ void k_tri_init(int n, int nblk, const double* __restrict__ D, double* __restrict__ X) {
+    const int ib = blockIdx.y, jb = blockIdx.x;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int ib = 0; ib < cb; ++ib) {  // strictly above the diagonal block: zero
-        const int r0 = ib * kTile, mr = min(kTile, n - r0);
-        if (ty < mr && tx < mc) X[(int64_t)(r0 + ty) * n + c0 + tx] = 0.0;
+    const int r = ib * kTile + ty, c = jb * kTile + tx;
+    if (r >= n || c >= n) return;
+    X[(int64_t)r * n + c] = (ib == jb) ? D[(int64_t)ib * kTile * kTile + ty * kTile + tx] : 0.0;
+}
+
+// Level s, one CTA per output tile (pair p, row tile i of B2, column tile j of B1):
+// mode 0: T[i,j] = sum_{k in B1, k >= j} L[i,k] X[k,j];  mode 1: X[i,j] = -sum_{k in B2, k <= i} X[i,k] T[k,j]
+__global__ void k_tri_level(int n, int nblk, int s, int mode, const double* __restrict__ A, double* __restrict__ X,
+                            double* __restrict__ T) {
+    __shared__ double P[kTile][kTile + 1];
+    __shared__ double Q[kTile][kTile + 1];
+    const int per_pair = s * s;
+    const int pair = blockIdx.x / per_pair, rem = blockIdx.x - pair * per_pair;
+    const int b1 = pair * 2 * s, b2 = b1 + s;              // first tiles of B1 and B2
+    const int e1 = min(b2, nblk), e2 = min(b2 + s, nblk);  // ends
+    const int i = b2 + rem / s, j = b1 + rem % s;
+    if (b2 >= nblk || i >= e2 || j >= e1) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int r0 = i * kTile, c0 = j * kTile;
+    const int mr = min(kTile, n - r0), mc = min(kTile, n - c0);
+    const int k_lo = mode == 0 ? j : b2, k_hi = mode == 0 ? e1 : i + 1;
+    const double* left = mode == 0 ? A : X;
+    const double* right = mode == 0 ? X : T;
+    double acc = 0.0;
+    for (int kb = k_lo; kb < k_hi; ++kb) {
+        const int k0 = kb * kTile, mk = min(kTile, n - k0);
+        __syncthreads();
+        P[ty][tx] = (ty < mr && tx < mk) ? left[(int64_t)(r0 + ty) * n + k0 + tx] : 0.0;
+        Q[ty][tx] = (ty < mk && tx < mc) ? right[(int64_t)(k0 + ty) * n + c0 + tx] : 0.0;
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < kTile; ++k) acc += P[ty][k] * Q[k][tx];
     }
-    for (int ib = cb; ib < nblk; ++ib) {
-        const int r0 = ib * kTile, mr = min(kTile, n - r0);
-        // T = I[ib,cb] - sum_{kb=cb}^{ib-1} L[ib,kb] X[kb,cb]
-        double t = (ib == cb && tx == ty) ? 1.0 : 0.0;
-        for (int kb = cb; kb < ib; ++kb) {
-            const int k0 = kb * kTile, mk = min(kTile, n - k0);
-            __syncthreads();
-            L[ty][tx] = (ty < mr && tx < mk) ? A[(int64_t)(r0 + ty) * n + k0 + tx] : 0.0;
-            Y[ty][tx] = (ty < mk && tx < mc) ? X[(int64_t)(k0 + ty) * n + c0 + tx] : 0.0;
-            __syncthreads();
-            for (int k = 0; k < mk; ++k) t -= L[ty][k] * Y[k][tx];
-        }
-        __syncthreads();
-        T[ty][tx] = t;
-        L[ty][tx] = (ty < mr && tx < mr) ? A[(int64_t)(r0 + ty) * n + r0 + tx] : 0.0;
-        __syncthreads();
-        // forward substitution L_ii Z = T, column tx
-        if (ty == 0 && tx < mc)
-            for (int r = 0; r < mr; ++r) {
-                double s = T[r][tx];
-                for (int k = 0; k < r; ++k) s -= L[r][k] * T[k][tx];
-                T[r][tx] = s / L[r][r];
-            }
-        __syncthreads();
-        if (ty < mr && tx < mc) X[(int64_t)(r0 + ty) * n + c0 + tx] = T[ty][tx];
+    if (ty < mr && tx < mc) {
+        if (mode == 0) T[(int64_t)(r0 + ty) * n + c0 + tx] = acc;
+        else X[(int64_t)(r0 + ty) * n + c0 + tx] = -acc;
     }
 }
 
@@ -496,7 +656,7 @@ int coarse_setup_mesh(plato_problem* h) {
     const int64_t mx = h->C > h->N ? h->C : h->N;
     PLATO_CUDA(h, cudaMallocAsync(&keys, sizeof(uint32_t) * mx, s));
     PLATO_CUDA(h, cudaMallocAsync(&vals, sizeof(int32_t) * mx, s));
-    PLATO_CUDA(h, cudaMallocAsync(&hist, sizeof(int32_t) * (c.ncells + 1), s));
+    PLATO_CUDA(h, cudaMallocAsync(&hist, sizeof(int32_t) * (2 * c.ncells + 1), s));
     PLATO_CUDA(h, cudaMallocAsync(&bad, sizeof(int32_t), s));
     // nodes by cell
     PLATO_CUDA(h, cudaMemsetAsync(hist, 0, sizeof(int32_t) * (c.ncells + 1), s));
@@ -504,12 +664,12 @@ int coarse_setup_mesh(plato_problem* h) {
     PLATO_LAUNCH_CHECK(h);
     int rc = csr_by_key(h, h->N, keys, vals, hist, c.ncells, &c.node_ptr, &c.node_list);
     if (rc) return rc;
-    // elements by cell (+ the every-element-in-one-cell check)
-    PLATO_CUDA(h, cudaMemsetAsync(hist, 0, sizeof(int32_t) * (c.ncells + 1), s));
+    // elements by cell and kind (+ the every-element-in-one-cell check)
+    PLATO_CUDA(h, cudaMemsetAsync(hist, 0, sizeof(int32_t) * (2 * c.ncells + 1), s));
     PLATO_CUDA(h, cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
-    k_elem_keys<<<grid_for(h->C, T), T, 0, s>>>(h->C, h->conn, h->coords, cv, keys, vals, hist, bad);
+    k_elem_keys<<<grid_for(h->C, T), T, 0, s>>>(h->C, h->conn, h->coords, cv, h->bc_mask, keys, vals, hist, bad);
     PLATO_LAUNCH_CHECK(h);
-    rc = csr_by_key(h, h->C, keys, vals, hist, c.ncells, &c.elem_ptr, &c.elem_list);
+    rc = csr_by_key(h, h->C, keys, vals, hist, 2 * c.ncells, &c.elem_ptr, &c.elem_list);
     if (rc) return rc;
     int32_t bad_h = 0;
     PLATO_CUDA(h, cudaMemcpyAsync(&bad_h, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -546,38 +706,56 @@ void coarse_release(plato_problem* h) {
 }
 
 // Per-solve setup: Galerkin operator of control z, Cholesky, explicit inverse.
-int coarse_setup_operator(plato_problem* h, const double* z) {
+// E_copy (device, may be NULL) receives E before it is factored.
+int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     CoarseSpace& c = h->coarse;
     cudaStream_t s = h->stream;
     const int n = c.ndof;
     const size_t nn = size_t(n) * n;
     PLATO_CUDA(h, cudaMemsetAsync(c.E, 0, sizeof(double) * nn, s));
+    PLATO_CUDA(h, cudaFuncSetAttribute(k_galerkin_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFastSmem)));
+    k_galerkin_fast<<<c.ncells * c.gsplit, kThreadsPerCta, kFastSmem, s>>>(
+        coarse_view(h), c.gsplit, c.elem_ptr, c.elem_list, h->conn, h->coords, z, h->material, h->bc_mask, n, c.E);
+    PLATO_LAUNCH_CHECK(h);
     k_galerkin<<<c.ncells * c.gsplit, kThreadsPerCta, 0, s>>>(coarse_view(h), c.gsplit, c.elem_ptr, c.elem_list,
                                                                h->conn, h->coords, z, h->material, h->bc_mask, n, c.E);
     PLATO_LAUNCH_CHECK(h);
     k_regularize<<<grid_for(n, 256), 256, 0, s>>>(n, c.E);
     PLATO_LAUNCH_CHECK(h);
+    if (E_copy) PLATO_CUDA(h, cudaMemcpyAsync(E_copy, c.E, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
     PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
     const int nblk = (n + kTile - 1) / kTile;
     const dim3 tb(kTile, kTile);
+    // X = L^-1 and the inverse diagonal tiles D in per-solve scratch
+    double *X = nullptr, *D = nullptr;
+    PLATO_CUDA(h, cudaMallocAsync(&X, sizeof(double) * nn, s));
+    PLATO_CUDA(h, cudaMallocAsync(&D, sizeof(double) * size_t(nblk) * kTile * kTile, s));
     for (int kb = 0; kb < nblk; ++kb) {
-        k_chol_diag<<<1, tb, 0, s>>>(n, c.E, kb, c.flag);
+        k_chol_diag<<<1, tb, 0, s>>>(n, c.E, kb, D, c.flag);
         const int rem = nblk - kb - 1;
         if (rem > 0) {
-            k_chol_panel<<<rem, tb, 0, s>>>(n, c.E, kb);
+            k_chol_panel<<<rem, tb, 0, s>>>(n, c.E, kb, D);
             k_chol_update<<<rem * (rem + 1) / 2, tb, 0, s>>>(n, c.E, kb, nblk);
         }
     }
     h->launches += 3 * nblk;
     PLATO_LAUNCH_CHECK(h);
-    // X = L^-1 into the rc-independent scratch (Einv used as X first, then overwritten)
-    double* X = nullptr;
-    PLATO_CUDA(h, cudaMallocAsync(&X, sizeof(double) * nn, s));
-    k_tri_inverse<<<nblk, tb, 0, s>>>(n, c.E, X, nblk);
+    double* Tmp = nullptr;
+    PLATO_CUDA(h, cudaMallocAsync(&Tmp, sizeof(double) * nn, s));
+    k_tri_init<<<dim3(nblk, nblk), tb, 0, s>>>(n, nblk, D, X);
     PLATO_LAUNCH_CHECK(h);
+    for (int lv = 1; lv < nblk; lv *= 2) {
+        const int pairs = (nblk + 2 * lv - 1) / (2 * lv);
+        k_tri_level<<<pairs * lv * lv, tb, 0, s>>>(n, nblk, lv, 0, c.E, X, Tmp);
+        k_tri_level<<<pairs * lv * lv, tb, 0, s>>>(n, nblk, lv, 1, c.E, X, Tmp);
+        h->launches += 1;
+        PLATO_LAUNCH_CHECK(h);
+    }
+    PLATO_CUDA(h, cudaFreeAsync(Tmp, s));
     k_gram<<<dim3(nblk, nblk), tb, 0, s>>>(n, X, c.Einv, nblk);
     PLATO_LAUNCH_CHECK(h);
     PLATO_CUDA(h, cudaFreeAsync(X, s));
+    PLATO_CUDA(h, cudaFreeAsync(D, s));
     int32_t bad = 0;
     PLATO_CUDA(h, cudaMemcpyAsync(&bad, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));
@@ -601,3 +779,23 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
 }
 
 }  // namespace plato
+
+extern "C" int plato_coarse_operator(plato_problem* h, const double* z, int32_t* ndof, double* E, double* Einv) {
+    using namespace plato;
+    if (!h || !ndof) return PLATO_BAD_INPUT;
+    if (h->opts.coarse_cells[0] <= 0) return plato_fail(h, PLATO_BAD_INPUT, "no coarse grid in the solver options");
+    int rc = coarse_setup_mesh(h);
+    if (rc) return rc;
+    *ndof = h->coarse.ndof;
+    if (!E && !Einv) return PLATO_OK;
+    if (!z) return plato_fail(h, PLATO_BAD_INPUT, "null control");
+    const size_t nn = size_t(h->coarse.ndof) * h->coarse.ndof;
+    double* Ed = nullptr;
+    PLATO_CUDA(h, cudaMalloc(&Ed, sizeof(double) * nn));
+    rc = coarse_setup_operator(h, z, Ed);
+    if (!rc && E) rc = cudaMemcpy(E, Ed, sizeof(double) * nn, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : PLATO_CUDA_ERROR;
+    if (!rc && Einv)
+        rc = cudaMemcpy(Einv, h->coarse.Einv, sizeof(double) * nn, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : PLATO_CUDA_ERROR;
+    cudaFree(Ed);
+    return rc;
+}

@@ -7,17 +7,19 @@
 // K_ab = sum vol (L^2 g_a . g_b + 1/16) and M_ab = sum vol / 16 on the node pattern.
 //
 // A filter handle is a plato_problem over the mesh (same node graph and SELL pattern as the
-// mechanics) with one unknown per node.  K depends on the mesh and L only, so it is
-// assembled once per handle (warp per row, deterministic per-slot sums in cell order) and
-// kept with its SELL copy and Jacobi diagonal; each solution is a scalar Jacobi-PCG in FP64
-// (the kernels of solver.cu on one value per slot).
+// mechanics) with one unknown per node.  K and D = (dR/dcontrol)^T = -M depend on the mesh
+// and L only, so both are assembled once per handle (warp per row, deterministic per-slot
+// sums in cell order) and kept with their SELL copies and K's Jacobi diagonal.  Every call
+// is then SELL SpMVs and, for the two solves, a scalar Jacobi-PCG in FP64 (solver.cu): the
+// residual is K filtered + D control, the right-hand side of the solution -D control, the
+// chain rule D K^-1 (-dF/dfiltered).
 //
 // Surface term (evaluate_boundary, src/helmholtz/HelmholtzResidual.hpp:178-241; "Surface
 // Length Scale" alpha, default 0): on each face that carries it, with the degree-one triangle
-// rule, R_a += alpha L (area / 3) (sum_b filtered_b / 3) and K_ab += alpha L area / 9.  The
-// reference holds the face's filtered value in a per-cell slot that the faces of one cell
-// share; it is per face here.  Faces are few and the term is assembled once per handle, so
-// it adds with atomics after the deterministic cell sums.
+// rule, R_a += alpha L (area / 3) (sum_b filtered_b / 3), i.e. K_ab += alpha L area / 9.
+// The reference holds the face's filtered value in a per-cell slot that the faces of one
+// cell share; it is per face here.  Faces are few and K is assembled once per handle, so the
+// term adds with atomics after the deterministic cell sums.
 #include <cmath>
 
 #include "plato_internal.cuh"
@@ -29,64 +31,11 @@ GraphView graph_view(const plato_problem* h);
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
 int pcg_scalar(plato_problem* h, const double* vals, const double* dinv, const double* b, double* x,
                plato_solve_stats* stats);
+int launch_sell1_spmv(plato_problem* h, const double* vals, const double* x, double* y);
 
 namespace {
 
 constexpr int kThreads = 256;
-
-// R_a = sum over the node's cells of vol (L^2 grad(filtered) . g_a + (filtered_gp - control_gp) / 4),
-// cells in incidence order (deterministic)
-__global__ void __launch_bounds__(kThreads)
-k_helm_value(MeshView m, GraphView g, double L2, const double* __restrict__ filtered,
-             const double* __restrict__ control, double* __restrict__ R) {
-    for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < g.num_nodes;
-         a += (int64_t)gridDim.x * blockDim.x) {
-        double sum = 0.0;
-        for (int32_t k = g.n2c_ptr[a]; k < g.n2c_ptr[a + 1]; ++k) {
-            const int32_t packed = g.n2c[k];
-            const int la = packed & 3;
-            const int4 n = m.conn[packed >> 2];
-            double x[4][3];
-            load_cell_coords(m.coords, n, x);
-            TetGeom<double> G;
-            tet_geometry(x, G);
-            const double f[4] = {filtered[n.x], filtered[n.y], filtered[n.z], filtered[n.w]};
-            const double fg = 0.25 * (f[0] + f[1] + f[2] + f[3]);
-            const double cg = 0.25 * (control[n.x] + control[n.y] + control[n.z] + control[n.w]);
-            double grad[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) grad[d] += f[b] * G.g[b][d];
-            double ga[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) ga[d] = la == 0 ? G.g[0][d] : la == 1 ? G.g[1][d] : la == 2 ? G.g[2][d] : G.g[3][d];
-            double out = 0.0;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) out += L2 * grad[d] * ga[d] * G.vol;
-            sum += out + 0.25 * (fg - cg) * G.vol;
-        }
-        R[a] = sum;
-    }
-}
-
-// y_a = scale * (M x)_a = scale * sum over the node's cells of vol/16 * sum_b x_b
-__global__ void __launch_bounds__(kThreads)
-k_helm_mass(MeshView m, GraphView g, double scale, const double* __restrict__ x, double* __restrict__ y) {
-    for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < g.num_nodes;
-         a += (int64_t)gridDim.x * blockDim.x) {
-        double sum = 0.0;
-        for (int32_t k = g.n2c_ptr[a]; k < g.n2c_ptr[a + 1]; ++k) {
-            const int4 n = m.conn[g.n2c[k] >> 2];
-            double xc[4][3];
-            load_cell_coords(m.coords, n, xc);
-            TetGeom<double> G;
-            tet_geometry(xc, G);
-            sum += 0.0625 * G.vol * (x[n.x] + x[n.y] + x[n.z] + x[n.w]);
-        }
-        y[a] = scale * sum;
-    }
-}
 
 // One value per block of the node pattern, warp per row.  MODE 0: K_ab = sum vol (L^2 g_a.g_b
 // + 1/16); MODE 1: (dR/dcontrol)^T, -sum vol / 16.  The row's cells are staged 32 at a time
@@ -158,19 +107,6 @@ __device__ __forceinline__ double face_nodes_area(MeshView m, const int32_t* fce
     return 0.5 * sqrt(J23 * J23 + J31 * J31 + J12 * J12);
 }
 
-// R_a += aL (area / 3) filtered_face over the surface faces
-__global__ void __launch_bounds__(kThreads)
-k_helm_surface_value(MeshView m, int32_t nfaces, const int32_t* __restrict__ fcell, const int32_t* __restrict__ floc,
-                     double aL, const double* __restrict__ filtered, double* __restrict__ R) {
-    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nfaces; f += (int64_t)gridDim.x * blockDim.x) {
-        int32_t id[3];
-        const double area = face_nodes_area(m, fcell, floc, f, id);
-        const double ff = filtered[id[0]] / 3.0 + filtered[id[1]] / 3.0 + filtered[id[2]] / 3.0;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) atomicAdd(R + id[a], aL * ff * (area / 3.0));
-    }
-}
-
 // K_ab += aL area / 9 for the node pairs of each surface face (rows sorted: binary search)
 __global__ void __launch_bounds__(kThreads)
 k_helm_surface_entries(MeshView m, GraphView g, int32_t nfaces, const int32_t* __restrict__ fcell,
@@ -211,7 +147,7 @@ __global__ void k_crs_to_sell1(int32_t N, SellView A, const int32_t* __restrict_
             }
             sell[base + t] = v;
         }
-        if (threadIdx.x < 32 && 32 * s + threadIdx.x < N) {
+        if (dinv && threadIdx.x < 32 && 32 * s + threadIdx.x < N) {
             const int64_t r = 32 * s + threadIdx.x;
             dinv[r] = 1.0 / crs[diag[r]];
         }
@@ -222,11 +158,13 @@ __global__ void k_crs_to_sell1(int32_t N, SellView A, const int32_t* __restrict_
 
 SellView sell_view(const plato_problem* h);
 
-// K, its SELL copy and Jacobi diagonal (once per handle)
+// K and D = (dR/dcontrol)^T = -M, their SELL copies and K's Jacobi diagonal (once per handle)
 static int helm_prepare(plato_problem* h) {
     if (h->helm_ready) return PLATO_OK;
     if (!h->helm_K) PLATO_CUDA(h, cudaMalloc(&h->helm_K, sizeof(double) * size_t(h->nblocks)));
+    if (!h->helm_D) PLATO_CUDA(h, cudaMalloc(&h->helm_D, sizeof(double) * size_t(h->nblocks)));
     if (!h->helm_sell) PLATO_CUDA(h, cudaMalloc(&h->helm_sell, sizeof(double) * size_t(h->sell.total_slots)));
+    if (!h->helm_Dsell) PLATO_CUDA(h, cudaMalloc(&h->helm_Dsell, sizeof(double) * size_t(h->sell.total_slots)));
     if (!h->helm_dinv) PLATO_CUDA(h, cudaMalloc(&h->helm_dinv, sizeof(double) * size_t(h->N)));
     const double L2 = h->helm_length * h->helm_length;
     k_helm_rows<0><<<grid_for(h->N, 4, 148 * 32), 128, 0, h->stream>>>(mesh_view(h), graph_view(h), L2, h->helm_K);
@@ -239,6 +177,11 @@ static int helm_prepare(plato_problem* h) {
     }
     k_crs_to_sell1<<<grid_for(h->sell.nslices, 1, 148 * 16), 256, 0, h->stream>>>(
         h->N, sell_view(h), h->row_map, h->diag, h->helm_K, h->helm_sell, h->helm_dinv);
+    PLATO_LAUNCH_CHECK(h);
+    k_helm_rows<1><<<grid_for(h->N, 4, 148 * 32), 128, 0, h->stream>>>(mesh_view(h), graph_view(h), 0.0, h->helm_D);
+    PLATO_LAUNCH_CHECK(h);
+    k_crs_to_sell1<<<grid_for(h->sell.nslices, 1, 148 * 16), 256, 0, h->stream>>>(
+        h->N, sell_view(h), h->row_map, h->diag, h->helm_D, h->helm_Dsell, nullptr);
     PLATO_LAUNCH_CHECK(h);
     h->helm_ready = 1;
     return PLATO_OK;
@@ -322,15 +265,11 @@ int plato_create_helmholtz(const plato_helmholtz_desc* desc, plato_problem** out
 int plato_helmholtz_value(plato_problem* h, const double* filtered, const double* control, double* R) {
     RC(helm_check(h));
     if (!filtered || !control || !R) return plato_fail(h, PLATO_BAD_INPUT, "null device pointer");
-    k_helm_value<<<grid_for(h->N, 256), 256, 0, h->stream>>>(mesh_view(h), graph_view(h),
-                                                             h->helm_length * h->helm_length, filtered, control, R);
-    PLATO_LAUNCH_CHECK(h);
-    if (h->helm_nfaces > 0) {
-        k_helm_surface_value<<<grid_for(h->helm_nfaces, kThreads), kThreads, 0, h->stream>>>(
-            mesh_view(h), h->helm_nfaces, h->helm_fcell, h->helm_floc, h->helm_surface * h->helm_length, filtered, R);
-        PLATO_LAUNCH_CHECK(h);
-    }
-    return PLATO_OK;
+    RC(helm_prepare(h));
+    // R = K filtered + D control (D = (dR/dcontrol)^T = -M, symmetric)
+    RC(launch_sell1_spmv(h, h->helm_sell, filtered, R));
+    RC(launch_sell1_spmv(h, h->helm_Dsell, control, h->v_tmp));
+    return launch_axpby(h, h->N, 1.0, h->v_tmp, 1.0, R);
 }
 
 int plato_helmholtz_gradient_u(plato_problem* h, double* entries) {
@@ -345,8 +284,9 @@ int plato_helmholtz_gradient_u(plato_problem* h, double* entries) {
 int plato_helmholtz_gradient_z(plato_problem* h, double* entries) {
     RC(helm_check(h));
     if (!entries) return plato_fail(h, PLATO_BAD_INPUT, "null device pointer");
-    k_helm_rows<1><<<grid_for(h->N, 4, 148 * 32), 128, 0, h->stream>>>(mesh_view(h), graph_view(h), 0.0, entries);
-    PLATO_LAUNCH_CHECK(h);
+    RC(helm_prepare(h));
+    PLATO_CUDA(h, cudaMemcpyAsync(entries, h->helm_D, sizeof(double) * size_t(h->nblocks), cudaMemcpyDeviceToDevice,
+                                  h->stream));
     return PLATO_OK;
 }
 
@@ -355,9 +295,8 @@ int plato_helmholtz_solution(plato_problem* h, const double* control, double* fi
     if (!control || !filtered) return plato_fail(h, PLATO_BAD_INPUT, "null device pointer");
     plato_solve_stats local{};
     RC(helm_prepare(h));
-    // R = value(0, control); rhs = -R = M control; solve K filtered = rhs from zero
-    PLATO_CUDA(h, cudaMemsetAsync(h->v_x, 0, sizeof(double) * size_t(h->N), h->stream));
-    RC(plato_helmholtz_value(h, h->v_x, control, h->v_b));
+    // R = value(0, control) = D control; rhs = -R; solve K filtered = rhs from zero
+    RC(launch_sell1_spmv(h, h->helm_Dsell, control, h->v_b));
     RC(launch_axpby(h, h->N, -1.0, h->v_b, 0.0, h->v_b));
     PLATO_CUDA(h, cudaMemsetAsync(filtered, 0, sizeof(double) * size_t(h->N), h->stream));
     return pcg_scalar(h, h->helm_sell, h->helm_dinv, h->v_b, filtered, stats ? stats : &local);
@@ -369,13 +308,11 @@ int plato_helmholtz_criterion_gradient(plato_problem* h, const double* dfdfilter
     if (!dfdfiltered || !dfdcontrol) return plato_fail(h, PLATO_BAD_INPUT, "null device pointer");
     plato_solve_stats local{};
     RC(helm_prepare(h));
-    // solve K x = -g, then dfdcontrol = (dR/dcontrol)^T x = -M x
+    // solve K x = -g, then dfdcontrol = (dR/dcontrol)^T x = D x
     RC(launch_axpby(h, h->N, -1.0, dfdfiltered, 0.0, h->v_b));
     PLATO_CUDA(h, cudaMemsetAsync(h->v_x, 0, sizeof(double) * size_t(h->N), h->stream));
     RC(pcg_scalar(h, h->helm_sell, h->helm_dinv, h->v_b, h->v_x, stats ? stats : &local));
-    k_helm_mass<<<grid_for(h->N, 256), 256, 0, h->stream>>>(mesh_view(h), graph_view(h), -1.0, h->v_x, dfdcontrol);
-    PLATO_LAUNCH_CHECK(h);
-    return PLATO_OK;
+    return launch_sell1_spmv(h, h->helm_Dsell, h->v_x, dfdcontrol);
 }
 
 }  // extern "C"

@@ -227,6 +227,8 @@ struct plato_problem {
     int32_t helm_ready = 0;        // K, its SELL copy and diagonal built
     double* helm_K = nullptr;      // one value per block of the node pattern
     double* helm_sell = nullptr;   // SELL copy (one value per slot)
+    double* helm_D = nullptr;      // (dR/dcontrol)^T = -M, one value per block
+    double* helm_Dsell = nullptr;  // its SELL copy
     double* helm_dinv = nullptr;   // inverse diagonal
     double  helm_surface = 0.0;    // surface length scale alpha (0: no surface term)
     int32_t helm_nfaces = 0;       // faces carrying the surface term
@@ -239,7 +241,7 @@ struct plato_problem {
 int plato_fail(plato_problem* h, int status, const std::string& msg);
 namespace plato {
 int coarse_setup_mesh(plato_problem* h);
-int coarse_setup_operator(plato_problem* h, const double* z);
+int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy = nullptr);
 int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S);
 void coarse_release(plato_problem* h);
 void batch_release(plato_problem* h);

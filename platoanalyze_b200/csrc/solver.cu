@@ -9,7 +9,7 @@
 // Per iteration three kernels run back to back on the handle's stream with no host
 // round-trip: (1) SELL-32 SpMV fused with the p.Ap reduction and alpha, (2) the x/r update
 // fused with the Jacobi apply and the r.z / r.r reductions, beta and the stop test, (3) the
-// search-direction update.  The scalars live in device memory; each reduction is finished
+// search-direction update (for scalar systems folded into the next SpMV).  The scalars live in device memory; each reduction is finished
 // by the last block to arrive (ticket counter): no extra launch, no spin-wait.  The host
 // polls a pinned copy of the scalars every kChunk iterations while the next chunk is
 // already queued, and every kernel returns at once after convergence.
@@ -66,13 +66,19 @@ k_sell_spmv(SellView A, const double* __restrict__ vals, const double* __restric
 }
 
 // Scalar (one value per node) y = A x on the SELL pattern: value of slot k of row 32s+l at
-// ptr_s + 32k + l; with S != nullptr also p.Ap and alpha.
+// ptr_s + 32k + l.  With S != nullptr also p.Ap and alpha (x = p, y = Ap).  With DIR the
+// CG search direction is formed on the fly, p = z + beta p_old (beta = 0 on the first
+// step), read at every column, written for the thread's own row into p_new; this replaces a
+// separate direction kernel (same arithmetic, so the same bits).  6 blocks of 256 per SM.
+template <bool DIR>
 __global__ void __launch_bounds__(kThreads, 6)
-k_sell1_spmv(SellView A, const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
-             PcgScalars* S, double* partials) {
+k_sell1_spmv(SellView A, const double* __restrict__ vals, const double* __restrict__ x,
+             const double* __restrict__ p_old, double* __restrict__ p_new, double* __restrict__ y, PcgScalars* S,
+             double* partials) {
     __shared__ double sh[1][32];
     __shared__ bool last;
     if (S && S->done) return;
+    const double beta = DIR ? S->beta : 0.0;
     double dot = 0.0;
     const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
     const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
@@ -83,10 +89,20 @@ k_sell1_spmv(SellView A, const double* __restrict__ vals, const double* __restri
         const int64_t base = __ldg(A.ptr + sl) + l;
         double a = 0.0;
 #pragma unroll 4
-        for (int k = 0; k < w; ++k) a += __ldg(vals + base + 32 * k) * __ldg(x + __ldg(A.cols + base + 32 * k));
+        for (int k = 0; k < w; ++k) {
+            const int32_t c = __ldg(A.cols + base + 32 * k);
+            const double xc = DIR ? x[c] + beta * p_old[c] : x[c];
+            a += __ldg(vals + base + 32 * k) * xc;
+        }
         if (r < A.num_rows) {
             y[r] = a;
-            if (S) dot += x[r] * a;
+            if (DIR) {
+                const double pr = x[r] + beta * p_old[r];
+                p_new[r] = pr;
+                dot += pr * a;
+            } else if (S) {
+                dot += x[r] * a;
+            }
         }
     }
     if (!S) return;
@@ -176,6 +192,7 @@ k_pcg_start(int64_t n, const double* __restrict__ b, double* __restrict__ r, con
         if (threadIdx.x == 0) {
             S->rz = t[0];
             S->rr = t[1];
+            S->beta = 0.0;
             if (!keep_bb) {
                 S->bb = t[2];
                 S->tol2 = tol * tol * t[2];
@@ -216,6 +233,7 @@ int spmv_blocks(const plato_problem* h) {
     const int64_t padded = ((int64_t)h->N + 31) & ~int64_t(31);
     return grid_for(padded, kThreads, 148 * 16);
 }
+
 
 // Event pairs for the sampled operator timings (reused across solves).
 int timing_events(plato_problem* h, cudaEvent_t* e0, cudaEvent_t* e1) {
@@ -273,10 +291,13 @@ int prepare_operator(plato_problem* h, const double* crs) {
 }
 
 // Jacobi-PCG on n unknowns with the operator apply(in, out, S) (S != nullptr: fused p.Ap and
-// alpha) and inverse diagonal dinv; x holds the initial guess on entry.
-template <class Apply>
-static int pcg_run(plato_problem* h, int64_t n, Apply apply, const double* dinv, const double* b, double* x,
-                   plato_solve_stats* stats) {
+// alpha) and inverse diagonal dinv; x holds the initial guess on entry.  With p2 (n values)
+// the search direction is formed inside the operator instead of by its own kernel:
+// apply_dir(p_old, p_new, Ap, S) computes p_new = z + beta p_old and Ap = A p_new, and the
+// two direction buffers alternate.
+template <class Apply, class ApplyDir>
+static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir, double* p2, const double* dinv,
+                   const double* b, double* x, plato_solve_stats* stats) {
     cudaStream_t s = h->stream;
     const double tol = h->opts.tolerance;
     const int32_t max_it = h->opts.max_iterations;
@@ -294,6 +315,8 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, const double* dinv,
         // r = b - A x ; z = Dinv r ; p = z
         int rc = apply(x, h->v_r, nullptr);
         if (rc) return rc;
+        double* pbuf[2] = {h->v_p, p2};
+        int pcur = 0;
         k_pcg_start<<<vec_blocks, kThreads, 0, s>>>(n, b, h->v_r, dinv, h->v_z, h->v_p, h->scal,
                                                      h->partials, tol, keep_bb ? 1 : 0);
         PLATO_LAUNCH_CHECK(h);
@@ -316,14 +339,20 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, const double* dinv,
                     timed_iters.push_back(2 * enqueued);
                     PLATO_CUDA(h, cudaEventRecord(e0, s));
                 }
-                rc = apply(h->v_p, h->v_Ap, h->scal);
+                if (p2) {
+                    rc = apply_dir(pbuf[pcur], pbuf[pcur ^ 1], h->v_Ap, h->scal);
+                    pcur ^= 1;
+                } else {
+                    rc = apply(h->v_p, h->v_Ap, h->scal);
+                }
                 if (rc) return rc;
                 if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
-                k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_Ap, dinv, h->v_z,
+                k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, pbuf[pcur], h->v_Ap, dinv, h->v_z,
                                                              h->scal, h->partials, max_it);
-                k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
+                if (!p2) k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
             }
-            h->launches += 2 * kChunk - 1;  // the operator applies count themselves
+            // the operator applies count themselves
+            h->launches += (p2 ? kChunk : 2 * kChunk) - 1;
             PLATO_LAUNCH_CHECK(h);
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
@@ -397,25 +426,36 @@ int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         PLATO_LAUNCH_CHECK(h);
         return PLATO_OK;
     };
-    return pcg_run(h, 3 * (int64_t)h->N, apply, h->v_dinv, b, x, stats);
+    auto no_dir = [](const double*, double*, double*, PcgScalars*) -> int { return PLATO_OK; };
+    return pcg_run(h, 3 * (int64_t)h->N, apply, no_dir, nullptr, h->v_dinv, b, x, stats);
 }
 
-// Scalar Jacobi-PCG (one unknown per node) on SELL values `vals` with inverse diagonal dinv.
+// Scalar Jacobi-PCG (one unknown per node) on SELL values `vals` with inverse diagonal dinv;
+// two kernels per iteration (the search direction is formed inside the SpMV).  The second
+// direction buffer is the handle's scratch vector v_tmp (3N values, unused by this solve).
 int pcg_scalar(plato_problem* h, const double* vals, const double* dinv, const double* b, double* x,
                plato_solve_stats* stats) {
     const SellView V = sell_view(h);
     const int sp_blocks = spmv_blocks(h);
+    if (sp_blocks > 4 * h->partials_len) return plato_fail(h, PLATO_BAD_INPUT, "reduction scratch too small");
     auto apply = [&](const double* in, double* out, PcgScalars* S) -> int {
-        k_sell1_spmv<<<sp_blocks, kThreads, 0, h->stream>>>(V, vals, in, out, S, S ? h->partials : nullptr);
+        k_sell1_spmv<false><<<sp_blocks, kThreads, 0, h->stream>>>(V, vals, in, nullptr, nullptr, out, S,
+                                                                   S ? h->partials : nullptr);
         PLATO_LAUNCH_CHECK(h);
         return PLATO_OK;
     };
-    return pcg_run(h, (int64_t)h->N, apply, dinv, b, x, stats);
+    auto apply_dir = [&](const double* p_old, double* p_new, double* out, PcgScalars* S) -> int {
+        k_sell1_spmv<true><<<sp_blocks, kThreads, 0, h->stream>>>(V, vals, h->v_z, p_old, p_new, out, S, h->partials);
+        PLATO_LAUNCH_CHECK(h);
+        return PLATO_OK;
+    };
+    return pcg_run(h, (int64_t)h->N, apply, apply_dir, h->v_tmp, dinv, b, x, stats);
 }
 
 // y = A x for a scalar SELL matrix.
 int launch_sell1_spmv(plato_problem* h, const double* vals, const double* x, double* y) {
-    k_sell1_spmv<<<spmv_blocks(h), kThreads, 0, h->stream>>>(sell_view(h), vals, x, y, nullptr, nullptr);
+    k_sell1_spmv<false><<<spmv_blocks(h), kThreads, 0, h->stream>>>(sell_view(h), vals, x, nullptr, nullptr, y,
+                                                                    nullptr, nullptr);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

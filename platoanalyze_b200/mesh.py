@@ -83,6 +83,52 @@ def exterior_faces(connectivity: np.ndarray, exclude_nodes: np.ndarray | None = 
     return cells, local
 
 
+@dataclass
+class MeshFile:
+    coords: np.ndarray        # (N, 3) float64
+    connectivity: np.ndarray  # (C, 4) int32
+    node_sets: dict           # name -> 0-based nodes
+    side_sets: dict           # name -> (cells, (F, 3) local node ordinals)
+
+    @property
+    def num_nodes(self) -> int:
+        return self.coords.shape[0]
+
+
+def read_exodus(path: str) -> MeshFile:
+    """An Exodus II tetrahedral mesh in a netCDF classic encoding (CDF-1, -2 or -5)."""
+    from .capi import PlatoError
+
+    h = C.c_void_p()
+    rc = lib.plato_mesh_file_open(str(path).encode(), C.byref(h))
+    if rc != 0:
+        raise PlatoError(rc, (lib.plato_mesh_file_last_error() or b"").decode())
+    try:
+        nn, nc, nns, nss = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib.plato_mesh_file_info(h, C.byref(nn), C.byref(nc), C.byref(nns), C.byref(nss)))
+        coords = np.empty((nn.value, 3), np.float64)
+        conn = np.empty((nc.value, 4), np.int32)
+        check(lib.plato_mesh_file_mesh(h, _ptr(coords), _ptr(conn)))
+        name = C.create_string_buffer(256)
+        node_sets, side_sets = {}, {}
+        for k in range(nns.value):
+            cnt = C.c_int32()
+            check(lib.plato_mesh_file_node_set(h, k, name, 256, None, C.byref(cnt)))
+            nodes = np.empty(cnt.value, np.int32)
+            check(lib.plato_mesh_file_node_set(h, k, name, 256, _ptr(nodes), C.byref(cnt)))
+            node_sets[name.value.decode()] = nodes
+        for k in range(nss.value):
+            cnt = C.c_int32()
+            check(lib.plato_mesh_file_side_set(h, k, name, 256, None, None, C.byref(cnt)))
+            cells = np.empty(cnt.value, np.int32)
+            local = np.empty((cnt.value, 3), np.int32)
+            check(lib.plato_mesh_file_side_set(h, k, name, 256, _ptr(cells), _ptr(local), C.byref(cnt)))
+            side_sets[name.value.decode()] = (cells, local)
+        return MeshFile(coords, conn, node_sets, side_sets)
+    finally:
+        lib.plato_mesh_file_close(h)
+
+
 def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0, lz: float = 1.0) -> BoxMesh:
     nn, nc = C.c_int32(0), C.c_int32(0)
     check(lib.plato_box_mesh_sizes(nx, ny, nz, C.byref(nn), C.byref(nc)))

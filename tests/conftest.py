@@ -4,7 +4,7 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
-for p in (ROOT, ROOT / "oracle", ROOT / "tests"):
+for p in (ROOT, ROOT / "oracle", ROOT / "tests", ROOT / "tests" / "golden"):
     if str(p) not in sys.path:
         sys.path.insert(0, str(p))
 

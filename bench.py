@@ -8,9 +8,10 @@ nu = 0.3, SIMP p = 3, rho_min = 1e-9, nodal densities i.i.d. U[0.01, 1] (SplitMi
 0x5EED0002).  Synthetic data; every input and the 1.12 GB block matrix exceed the 126 MB L2.
 
 Methods (--method):
-  two-level  (default) FP64 flexible CG; preconditioner = FP32 Chebyshev-Jacobi smoothing on
-             an FP32 copy of the matrix + Galerkin coarse correction on a 10x5x5 box grid
-             (A-DEF2 two-level form).
+  two-level-fp16  (default) FP64 flexible CG; preconditioner = FP32 Chebyshev-Jacobi smoothing
+             on an FP16 copy of the Jacobi-scaled matrix D^-1/2 A D^-1/2 + Galerkin coarse
+             correction on a 10x5x5 box grid (A-DEF2 two-level form).
+  two-level  the same with an FP32 copy of the unscaled matrix.
   plain      the reference's algorithm: FP64 Jacobi-PCG on the assembled block matrix.
 Both stop on the same FP64 residual test (1e-10); the line also carries the plain method's
 throughput measured in the same run, and the accuracy of the timed solution against the
@@ -48,6 +49,9 @@ FP64_ITERATIONS = {"large": 3632, "medium": 1833, "small": None}
 METHOD_TEXT = {
     "two-level": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP32 SELL copy + "
                   "FP64 Galerkin coarse correction on a 10x5x5 trilinear box grid"),
+    "two-level-fp16": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP16 copy of the "
+                       "Jacobi-scaled matrix D^-1/2 A D^-1/2 + FP64 Galerkin coarse correction on a 10x5x5 trilinear "
+                       "box grid"),
     "plain": "plain FP64 Jacobi-PCG on the assembled 3x3 block matrix (the reference's algorithm)",
     "chebyshev": "FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP32 SELL copy",
     "bf16": "FP64 flexible CG; preconditioner: Chebyshev-Jacobi (16 steps) on a BF16-stored SELL copy",
@@ -61,7 +65,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--method", default="two-level", choices=list(METHOD_TEXT))
+    ap.add_argument("--method", default="two-level-fp16", choices=list(METHOD_TEXT))
     ap.add_argument("--size", default="large", choices=list(SIZES))
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations in the reference-arm sample")
@@ -533,9 +537,14 @@ def main():
                "algorithmic_bytes": spmv_bytes, "avg_launch_ms": spmv_ms, "launches_timed": inst["op_timed"]}
     roofline, roofline_other = rl_spmv, None
     if inst["inner_timed"]:
-        cheb_bytes = 9 * B * 4 + B * 4 + (N + 1) * 4 + 7 * 3 * N * 4
+        if args.method == "two-level-fp16":  # FP16 entries, no Jacobi diagonal stream (unit diagonal)
+            cheb_bytes = 9 * B * 2 + B * 4 + (N + 1) * 4 + 6 * 3 * N * 4
+            cheb_name = "k_sell16s<0> (FP16 Jacobi-scaled SELL SpMV fused with one Chebyshev step)"
+        else:
+            cheb_bytes = 9 * B * 4 + B * 4 + (N + 1) * 4 + 7 * 3 * N * 4
+            cheb_name = "k_cheb_sell<FP32> (FP32 SELL SpMV fused with one Chebyshev step)"
         cheb_ms = inst["inner_ms_total"] / inst["inner_timed"]
-        rl_cheb = {"bound": "hbm", "kernel": "k_cheb_sell<FP32> (FP32 SELL SpMV fused with one Chebyshev step)",
+        rl_cheb = {"bound": "hbm", "kernel": cheb_name,
                    "achieved": cheb_bytes / (cheb_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                    "frac": cheb_bytes / (cheb_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
                    "algorithmic_bytes": cheb_bytes, "avg_launch_ms": cheb_ms, "launches_timed": inst["inner_timed"]}
@@ -587,7 +596,8 @@ def main():
         cfg["speedup_vs_plain_fp64_gpu"] = value / plain["value"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": {"plain": "f64", "bf16": "f64+bf16"}.get(args.method, "f64+f32"),
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"plain": "f64", "bf16": "f64+bf16", "two-level-fp16": "f64+f32+f16"}.get(args.method, "f64+f32"),
             "data": "synthetic", "config": cfg, "accuracy": accuracy, "roofline": roofline,
             "roofline_fp64_spmv": roofline_other, "roofline_assembly": rl_asm, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N,

@@ -16,7 +16,7 @@ STATUS_NAMES = ["OK", "BAD_INPUT", "NOT_CONVERGED", "NONFINITE", "DEVICE_TIMEOUT
                 "OUT_OF_MEMORY", "NOT_SUPPORTED"]
 
 OPERATOR_ASSEMBLED, OPERATOR_MATRIX_FREE = 0, 1
-PRECISION_FP64, PRECISION_MIXED_FP32, PRECISION_MIXED_BF16 = 0, 1, 2
+PRECISION_FP64, PRECISION_MIXED_FP32, PRECISION_MIXED_BF16, PRECISION_MIXED_FP16 = 0, 1, 2, 3
 
 i32p = C.POINTER(C.c_int32)
 f64p = C.POINTER(C.c_double)

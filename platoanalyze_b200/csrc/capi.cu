@@ -86,7 +86,7 @@ int check_opts(plato_problem* h, const plato_solver_opts& o) {
     if (o.max_iterations < 1) return plato_fail(h, PLATO_BAD_INPUT, "solver max_iterations must be >= 1");
     if (o.operator_kind != PLATO_OPERATOR_ASSEMBLED && o.operator_kind != PLATO_OPERATOR_MATRIX_FREE)
         return plato_fail(h, PLATO_BAD_INPUT, "unknown operator_kind");
-    if (o.precision < PLATO_PRECISION_FP64 || o.precision > PLATO_PRECISION_MIXED_BF16)
+    if (o.precision < PLATO_PRECISION_FP64 || o.precision > PLATO_PRECISION_MIXED_FP16)
         return plato_fail(h, PLATO_BAD_INPUT, "unknown precision");
     return PLATO_OK;
 }
@@ -125,10 +125,14 @@ int plato_destroy(plato_problem* h) {
     dfree(h->sell.width); dfree(h->sell.ptr); dfree(h->sell.cols);
     dfree(h->sell64); dfree(h->sell32);
     if (h->sell16) cudaFree(h->sell16);
+    if (h->sell16s) cudaFree(h->sell16s);
+    dfree(h->f_sq); dfree(h->f_isq);
     dfree(h->mf_w64); dfree(h->mf_w32); dfree(h->v_q);
     dfree(h->f_res); dfree(h->f_d0); dfree(h->f_d1); dfree(h->f_y); dfree(h->f_w);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->poll_ev)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : h->asm_ev)
         if (e) cudaEventDestroy(e);
     coarse_release(h);

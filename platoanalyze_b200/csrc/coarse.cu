@@ -21,6 +21,8 @@
 // Per preconditioner call: restriction in two deterministic passes (per-cell partial sums by
 // split CTAs, then a fixed-order sum per coarse dof), y_c = E^-1 r_c (warp per row),
 // prolongation (thread per fine node).
+#include <mutex>
+
 #include <cub/cub.cuh>
 
 #include "plato_internal.cuh"
@@ -501,8 +503,8 @@ __global__ void k_gram(int n, const double* __restrict__ X, double* __restrict__
 __global__ void __launch_bounds__(kThreadsPerCta)
 k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
                  const int32_t* __restrict__ node_list, const double* __restrict__ coords,
-                 const uint8_t* __restrict__ mask, const float* __restrict__ v, double* __restrict__ part,
-                 const PcgScalars* S) {
+                 const uint8_t* __restrict__ mask, const float* __restrict__ v, const float* __restrict__ vscale,
+                 double* __restrict__ part, const PcgScalars* S) {
     __shared__ double sh[kThreadsPerCta / 32][24];
     if (S && S->done) return;
     const int cell = blockIdx.x / split, piece = blockIdx.x - cell * split;
@@ -520,7 +522,8 @@ k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
                      w = (coords[3 * p + 2] - lo[2]) * cv.ihz;
         double val[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) val[d] = mask[3 * p + d] ? 0.0 : double(v[3 * p + d]);
+        for (int d = 0; d < 3; ++d)
+            val[d] = mask[3 * p + d] ? 0.0 : double(vscale ? vscale[3 * p + d] * v[3 * p + d] : v[3 * p + d]);
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
             const double wgt = corner_weight(b, u, vv, w);
@@ -577,9 +580,10 @@ __global__ void k_coarse_gemv(int n, const double* __restrict__ Einv, const doub
     }
 }
 
-// y[(p,d)] (+)= m_(p,d) sum_J phi_J(x_p) yc[(J,d)]
+// y[(p,d)] (+)= yscale[(p,d)] m_(p,d) sum_J phi_J(x_p) yc[(J,d)]  (yscale may be NULL: 1)
 __global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ coords, const uint8_t* __restrict__ mask,
-                          const double* __restrict__ yc, float* __restrict__ y, int accumulate, const PcgScalars* S) {
+                          const double* __restrict__ yc, const float* __restrict__ yscale, float* __restrict__ y,
+                          int accumulate, const PcgScalars* S) {
     if (S && S->done) return;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
         const double x = coords[3 * p], yy = coords[3 * p + 1], zz = coords[3 * p + 2];
@@ -596,7 +600,7 @@ __global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ c
             s[2] += wgt * yc[3 * J + 2];
         }
         for (int d = 0; d < 3; ++d) {
-            const float val = mask[3 * p + d] ? 0.f : float(s[d]);
+            const float val = mask[3 * p + d] ? 0.f : (yscale ? yscale[3 * p + d] * float(s[d]) : float(s[d]));
             y[3 * p + d] = accumulate ? y[3 * p + d] + val : val;
         }
     }
@@ -684,6 +688,10 @@ int coarse_setup_mesh(plato_problem* h) {
     const size_t nn = size_t(c.ndof) * c.ndof;
     PLATO_CUDA(h, cudaMalloc(&c.E, sizeof(double) * nn));
     PLATO_CUDA(h, cudaMalloc(&c.Einv, sizeof(double) * nn));
+    PLATO_CUDA(h, cudaMalloc(&c.X, sizeof(double) * nn));
+    PLATO_CUDA(h, cudaMalloc(&c.T, sizeof(double) * nn));
+    const int nblk = (c.ndof + kTile - 1) / kTile;
+    PLATO_CUDA(h, cudaMalloc(&c.Dt, sizeof(double) * size_t(nblk) * kTile * kTile));
     // splits of each coarse cell's node / element lists so that the restriction and the
     // Galerkin sum run about 8 CTAs per SM
     c.rsplit = clampi((148 * 8 + c.ncells - 1) / c.ncells, 1, 64);
@@ -700,7 +708,7 @@ void coarse_release(plato_problem* h) {
     CoarseSpace& c = h->coarse;
     for (int32_t** p : {&c.node_ptr, &c.node_list, &c.elem_ptr, &c.elem_list, &c.flag})
         if (*p) { cudaFree(*p); *p = nullptr; }
-    for (double** p : {&c.E, &c.Einv, &c.rc, &c.yc, &c.rpart})
+    for (double** p : {&c.E, &c.Einv, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.rpart})
         if (*p) { cudaFree(*p); *p = nullptr; }
     c.ready = 0;
 }
@@ -713,7 +721,12 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     const int n = c.ndof;
     const size_t nn = size_t(n) * n;
     PLATO_CUDA(h, cudaMemsetAsync(c.E, 0, sizeof(double) * nn, s));
-    PLATO_CUDA(h, cudaFuncSetAttribute(k_galerkin_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFastSmem)));
+    static std::once_flag smem_once;  // per kernel and process; a driver round trip per call otherwise
+    cudaError_t attr = cudaSuccess;
+    std::call_once(smem_once, [&] {
+        attr = cudaFuncSetAttribute(k_galerkin_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFastSmem));
+    });
+    PLATO_CUDA(h, attr);
     k_galerkin_fast<<<c.ncells * c.gsplit, kThreadsPerCta, kFastSmem, s>>>(
         coarse_view(h), c.gsplit, c.elem_ptr, c.elem_list, h->conn, h->coords, z, h->material, h->bc_mask, n, c.E);
     PLATO_LAUNCH_CHECK(h);
@@ -726,10 +739,8 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
     const int nblk = (n + kTile - 1) / kTile;
     const dim3 tb(kTile, kTile);
-    // X = L^-1 and the inverse diagonal tiles D in per-solve scratch
-    double *X = nullptr, *D = nullptr;
-    PLATO_CUDA(h, cudaMallocAsync(&X, sizeof(double) * nn, s));
-    PLATO_CUDA(h, cudaMallocAsync(&D, sizeof(double) * size_t(nblk) * kTile * kTile, s));
+    // X = L^-1 and the inverse diagonal tiles D (scratch allocated with the coarse grid)
+    double *X = c.X, *D = c.Dt;
     for (int kb = 0; kb < nblk; ++kb) {
         k_chol_diag<<<1, tb, 0, s>>>(n, c.E, kb, D, c.flag);
         const int rem = nblk - kb - 1;
@@ -740,8 +751,7 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     }
     h->launches += 3 * nblk;
     PLATO_LAUNCH_CHECK(h);
-    double* Tmp = nullptr;
-    PLATO_CUDA(h, cudaMallocAsync(&Tmp, sizeof(double) * nn, s));
+    double* Tmp = c.T;
     k_tri_init<<<dim3(nblk, nblk), tb, 0, s>>>(n, nblk, D, X);
     PLATO_LAUNCH_CHECK(h);
     for (int lv = 1; lv < nblk; lv *= 2) {
@@ -751,11 +761,8 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
         h->launches += 1;
         PLATO_LAUNCH_CHECK(h);
     }
-    PLATO_CUDA(h, cudaFreeAsync(Tmp, s));
     k_gram<<<dim3(nblk, nblk), tb, 0, s>>>(n, X, c.Einv, nblk);
     PLATO_LAUNCH_CHECK(h);
-    PLATO_CUDA(h, cudaFreeAsync(X, s));
-    PLATO_CUDA(h, cudaFreeAsync(D, s));
     int32_t bad = 0;
     PLATO_CUDA(h, cudaMemcpyAsync(&bad, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));
@@ -763,16 +770,17 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     return PLATO_OK;
 }
 
-// y (FP32) = / += Z E^-1 Z^T v (v FP32); kernels return at once after convergence.
-int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S) {
+// y (FP32) = / += Z E^-1 Z^T v (v FP32); kernels return at once after convergence.  With sq
+// (the scaled mixed precision, v and y in D^1/2-scaled variables): y += sq Z E^-1 Z^T (sq v).
+int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S, const float* sq) {
     CoarseSpace& c = h->coarse;
     cudaStream_t s = h->stream;
     const CoarseView cv = coarse_view(h);
     k_restrict_cells<<<c.ncells * c.rsplit, kThreadsPerCta, 0, s>>>(cv, c.rsplit, c.node_ptr, c.node_list, h->coords,
-                                                                      h->bc_mask, v, c.rpart, S);
+                                                                      h->bc_mask, v, sq, c.rpart, S);
     k_restrict_sum<<<grid_for(c.ndof, 256), 256, 0, s>>>(cv, c.rsplit, c.rpart, c.rc, S);
     k_coarse_gemv<<<grid_for(int64_t(c.ndof) * 32, 256, 148 * 8), 256, 0, s>>>(c.ndof, c.Einv, c.rc, c.yc, S);
-    k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, y, accumulate, S);
+    k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, sq, y, accumulate, S);
     h->launches += 3;
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;

@@ -22,6 +22,8 @@
 #include <cmath>
 #include <cuda_bf16.h>
 
+#include <cuda_fp16.h>
+
 #include "plato_internal.cuh"
 #include "solver_common.cuh"
 
@@ -31,6 +33,8 @@ int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double 
 int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, double* host_result);
 int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float* out32, void* out16,
                        double* dinv, float* dinv32);
+int launch_sell_scale16(plato_problem* h, const double* sell64, const double* dinv, void* out16, float* sq,
+                        float* isq, float* ones);
 int launch_sell_spmv(plato_problem* h, const double* vals, const double* x, double* y);
 int launch_ebe_apply64(plato_problem* h, const double* x, double* y, const PcgScalars* S);
 int launch_ebe_apply32(plato_problem* h, const float* x, float* y, const PcgScalars* S);
@@ -46,7 +50,8 @@ namespace {
 constexpr int kChunk = 16;
 constexpr int kTimingStride = 8;
 
-enum InnerKind { INNER_SELL64 = 0, INNER_SELL32 = 1, INNER_SELL16 = 2, INNER_EBE32 = 3, INNER_EBE64 = 4 };
+enum InnerKind { INNER_SELL64 = 0, INNER_SELL32 = 1, INNER_SELL16 = 2, INNER_EBE32 = 3, INNER_EBE64 = 4,
+                 INNER_SELL16S = 5 };
 
 struct ChebCoef {
     float c0;      // first step: d = c0 Dinv r
@@ -120,9 +125,9 @@ k_fcg_mask_dot(int64_t n, const uint8_t* __restrict__ mask, const double* __rest
 // res = r (FP32), d = c0 Dinv r, y = d.
 __global__ void __launch_bounds__(kThreads)
 k_fcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
-             const double* __restrict__ q, const float* __restrict__ dinv32, float* __restrict__ res,
-             float* __restrict__ d, float* __restrict__ y, float c0, PcgScalars* S, double* partials,
-             int32_t max_it) {
+             const double* __restrict__ q, const float* __restrict__ dinv32, const float* __restrict__ res_scale,
+             float* __restrict__ res, float* __restrict__ d, float* __restrict__ y, float c0, PcgScalars* S,
+             double* partials, int32_t max_it) {
     __shared__ double sh[1][32];
     __shared__ bool last;
     if (S->done) return;
@@ -133,7 +138,7 @@ k_fcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r, const do
         const double ri = r[i] - alpha * q[i];
         r[i] = ri;
         v[0] += ri * ri;
-        const float rf = float(ri);
+        const float rf = res_scale ? res_scale[i] * float(ri) : float(ri);
         const float di = c0 * dinv32[i] * rf;
         res[i] = rf;
         d[i] = di;
@@ -183,6 +188,70 @@ k_cheb_sell(SellView A, const void* __restrict__ vals, const float* __restrict__
                 const float dn = c1 * dcur[k] + c2 * dinv32[k] * rs;
                 dnext[k] = dn;
                 y[k] += dn;
+            }
+        }
+    }
+}
+
+// FP16 Jacobi-scaled matrix (INNER_SELL16S), two rows per thread: rows 2m and 2m+1 of a
+// slice share each (k, q) entry pair as one __half2 and their column indices as one int2,
+// so a thread loads 4 bytes per entry load (2-byte loads would halve the bytes in flight of
+// this latency-bound loop).  Entry (k, q) of the pair at (9 ptr_s) / 2 + 16 (9k + q) + m.
+// MODE 0: Chebyshev step in scaled variables (unit diagonal): w = A^ d, res -= w,
+//         d_next = c1 d + c2 res, y += d_next;  MODE 1: res -= A^ x;  MODE 2: out = A^ x.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 4)
+k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__ x, float* __restrict__ res,
+          float* __restrict__ dnext, float* __restrict__ y, float c1, float c2, const PcgScalars* S) {
+    if (S && S->done) return;
+    const int64_t npairs = (((int64_t)A.num_rows + 31) & ~int64_t(31)) >> 1;
+    for (int64_t pr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pr < npairs;
+         pr += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t sl = pr >> 4;
+        const int m = int(pr & 15);
+        const int w = __ldg(A.width + sl);
+        const int64_t base = __ldg(A.ptr + sl);
+        const int2* __restrict__ cp = reinterpret_cast<const int2*>(A.cols + base) + m;
+        const __half2* __restrict__ vp = reinterpret_cast<const __half2*>(vals + 9 * base) + m;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+#pragma unroll 4
+        for (int k = 0; k < w; ++k) {
+            const int2 c = __ldg(cp + 16 * k);
+            const float x0 = __ldg(x + 3 * (int64_t)c.x), x1 = __ldg(x + 3 * (int64_t)c.x + 1),
+                        x2 = __ldg(x + 3 * (int64_t)c.x + 2);
+            const float z0 = __ldg(x + 3 * (int64_t)c.y), z1 = __ldg(x + 3 * (int64_t)c.y + 1),
+                        z2 = __ldg(x + 3 * (int64_t)c.y + 2);
+            const __half2* vk = vp + 144 * k;
+            float2 e[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) e[q] = __half22float2(vk[16 * q]);
+            a0 += e[0].x * x0 + e[1].x * x1 + e[2].x * x2;
+            a1 += e[3].x * x0 + e[4].x * x1 + e[5].x * x2;
+            a2 += e[6].x * x0 + e[7].x * x1 + e[8].x * x2;
+            b0 += e[0].y * z0 + e[1].y * z1 + e[2].y * z2;
+            b1 += e[3].y * z0 + e[4].y * z1 + e[5].y * z2;
+            b2 += e[6].y * z0 + e[7].y * z1 + e[8].y * z2;
+        }
+        const int64_t r0 = 32 * sl + 2 * m;
+        const float wv[6] = {a0, a1, a2, b0, b1, b2};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (r0 + h >= A.num_rows) break;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int64_t k = 3 * (r0 + h) + i;
+                const float wi = wv[3 * h + i];
+                if (MODE == 0) {
+                    const float rs = res[k] - wi;
+                    res[k] = rs;
+                    const float dn = c1 * x[k] + c2 * rs;
+                    dnext[k] = dn;
+                    y[k] += dn;
+                } else if (MODE == 1) {
+                    res[k] -= wi;
+                } else {
+                    y[k] = wi;
+                }
             }
         }
     }
@@ -239,21 +308,22 @@ k_res_sub_vec(int64_t n, const uint8_t* __restrict__ mask, const float* __restri
         res[i] -= mask[i] ? x[i] : w[i];
 }
 
-// z = y (widened), z.q -> beta = -(z.q)/(p.q); then p = z + beta p and p.r in k_fcg_direction.
+// z = y (widened; times z_scale when the preconditioner ran in scaled variables), z.q ->
+// beta = -(z.q)/(p.q); then p = z + beta p and p.r in k_fcg_direction.
 __global__ void __launch_bounds__(kThreads)
-k_fcg_zq(int64_t n, const float* __restrict__ y, double* __restrict__ z, const double* __restrict__ q,
-         PcgScalars* S, double* partials, int first) {
+k_fcg_zq(int64_t n, const float* __restrict__ y, const float* __restrict__ z_scale, double* __restrict__ z,
+         const double* __restrict__ q, PcgScalars* S, double* partials, int first) {
     __shared__ double sh[1][32];
     __shared__ bool last;
     if (S->done) return;
     if (first) {  // initial direction: only widen z = y
         for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-            z[i] = double(y[i]);
+            z[i] = double(z_scale ? z_scale[i] * y[i] : y[i]);
         return;
     }
     double v[1] = {0.0};
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double zi = double(y[i]);
+        const double zi = double(z_scale ? z_scale[i] * y[i] : y[i]);
         z[i] = zi;
         v[0] += zi * q[i];
     }
@@ -298,8 +368,8 @@ k_fcg_direction(int64_t n, const double* __restrict__ z, double* __restrict__ p,
 // r = b - A x (A x in r on entry), r.r and b.b; starts the preconditioner like k_fcg_update.
 __global__ void __launch_bounds__(kThreads)
 k_fcg_start(int64_t n, const double* __restrict__ b, double* __restrict__ r, const float* __restrict__ dinv32,
-            float* __restrict__ res, float* __restrict__ d, float* __restrict__ y, float c0, PcgScalars* S,
-            double* partials, double tol, int keep_bb) {
+            const float* __restrict__ res_scale, float* __restrict__ res, float* __restrict__ d, float* __restrict__ y,
+            float c0, PcgScalars* S, double* partials, double tol, int keep_bb) {
     __shared__ double sh[2][32];
     __shared__ bool last;
     double v[2] = {0.0, 0.0};
@@ -308,7 +378,7 @@ k_fcg_start(int64_t n, const double* __restrict__ b, double* __restrict__ r, con
         r[i] = ri;
         v[0] += ri * ri;
         v[1] += b[i] * b[i];
-        const float rf = float(ri);
+        const float rf = res_scale ? res_scale[i] * float(ri) : float(ri);
         const float di = c0 * dinv32[i] * rf;
         res[i] = rf;
         d[i] = di;
@@ -381,6 +451,7 @@ int inner_kind(const plato_problem* h) {
     if (o.operator_kind == PLATO_OPERATOR_MATRIX_FREE)
         return o.precision == PLATO_PRECISION_FP64 ? INNER_EBE64 : INNER_EBE32;
     if (o.precision == PLATO_PRECISION_MIXED_BF16) return INNER_SELL16;
+    if (o.precision == PLATO_PRECISION_MIXED_FP16) return INNER_SELL16S;
     if (o.precision == PLATO_PRECISION_MIXED_FP32) return INNER_SELL32;
     return INNER_SELL64;
 }
@@ -414,6 +485,7 @@ k_sell_apply32(SellView A, const void* __restrict__ vals, const float* __restric
 }  // namespace
 
 static const void* inner_vals(const plato_problem* h, int kind) {
+    if (kind == INNER_SELL16S) return h->sell16s;
     if (kind == INNER_SELL16) return h->sell16;
     if (kind == INNER_SELL32) return h->sell32;
     return h->sell64;
@@ -424,7 +496,10 @@ static int apply_inner_plain(plato_problem* h, int kind, const float* x, float* 
     const SellView V = sell_view(h);
     const void* vals = inner_vals(h, kind);
     const int B = spmv_blocks(h);
-    if (kind == INNER_SELL16) k_sell_apply32<INNER_SELL16><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
+    if (kind == INNER_SELL16S)
+        k_sell16s<2><<<B, kThreads, 0, h->stream>>>(V, static_cast<const __half*>(vals), x, nullptr, nullptr, y, 0.f,
+                                                    0.f, nullptr);
+    else if (kind == INNER_SELL16) k_sell_apply32<INNER_SELL16><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
     else if (kind == INNER_SELL32) k_sell_apply32<INNER_SELL32><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
     else k_sell_apply32<INNER_SELL64><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
     PLATO_LAUNCH_CHECK(h);
@@ -496,6 +571,14 @@ int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
     } else if (kind == INNER_SELL16) {
         if (!h->sell16) PLATO_CUDA(h, cudaMalloc(&h->sell16, sizeof(__nv_bfloat16) * slots));
         o16 = h->sell16;
+    } else if (kind == INNER_SELL16S) {
+        if (!h->sell16s) PLATO_CUDA(h, cudaMalloc(&h->sell16s, sizeof(__half) * slots));
+        for (float** v : {&h->f_sq, &h->f_isq})
+            if (!*v) PLATO_CUDA(h, cudaMalloc(v, sizeof(float) * n));
+        int rc = launch_crs_to_sell(h, crs, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
+        if (rc) return rc;
+        // the Jacobi diagonal of the scaled matrix is 1: f_dinv = ones
+        return launch_sell_scale16(h, h->sell64, h->v_dinv, h->sell16s, h->f_sq, h->f_isq, h->f_dinv);
     }
     return launch_crs_to_sell(h, crs, h->sell64, o32, o16, h->v_dinv, h->f_dinv);
 }
@@ -539,12 +622,18 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         return launch_sell_spmv(h, h->sell64, in, out);
     };
     const bool coarse = h->coarse.active != 0;
+    // FP16 scaled inner matrix: the preconditioner works on D^-1/2 r and returns D^1/2 z
+    const bool scaled = kind == INNER_SELL16S;
+    const float* res_scale = scaled ? h->f_isq : nullptr;
     // res -= A_inner xin (FP32)
     auto inner_apply_sub = [&](const float* xin) -> int {
         if (mf) {
             int r2 = launch_ebe_apply32(h, xin, h->f_w, h->scal);
             if (r2) return r2;
             k_res_sub_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, xin, h->f_w, h->f_res, h->scal);
+        } else if (kind == INNER_SELL16S) {
+            k_sell16s<1><<<SB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), xin, h->f_res, nullptr,
+                                                 nullptr, 0.f, 0.f, h->scal);
         } else if (kind == INNER_SELL16) {
             k_res_sub_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, xin, h->f_res, h->scal);
         } else if (kind == INNER_SELL32) {
@@ -574,6 +663,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 if (r2) return r2;
                 k_cheb_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, h->f_w, h->f_dinv, h->f_res, dcur, dnext, h->f_y,
                                                    cc.c1[k], cc.c2[k], h->scal);
+            } else if (kind == INNER_SELL16S) {
+                k_sell16s<0><<<SB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), dcur, h->f_res, dnext,
+                                                     h->f_y, cc.c1[k], cc.c2[k], h->scal);
             } else if (kind == INNER_SELL16) {
                 k_cheb_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
                                                                   h->f_y, cc.c1[k], cc.c2[k], h->scal);
@@ -601,7 +693,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         if (r2 || !coarse) return r2;
         r2 = inner_apply_sub(dlast);  // the sweep left res = r - A (s - d_last)
         if (r2) return r2;
-        return coarse_apply(h, h->f_res, h->f_y, 1, h->scal);
+        return coarse_apply(h, h->f_res, h->f_y, 1, h->scal, scaled ? h->f_sq : nullptr);
     };
 
     PcgScalars init{};
@@ -613,12 +705,12 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         // r = b - A x; z = M r; p = z; p.r
         rc = outer_apply(x, h->v_r);
         if (rc) return rc;
-        k_fcg_start<<<VB, kThreads, 0, s>>>(n, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, h->scal,
+        k_fcg_start<<<VB, kThreads, 0, s>>>(n, b, h->v_r, h->f_dinv, res_scale, h->f_res, h->f_d0, h->f_y, cc.c0, h->scal,
                                              h->partials, tol, keep_bb ? 1 : 0);
         PLATO_LAUNCH_CHECK(h);
         rc = precondition(cc.c0);
         if (rc) return rc;
-        k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, h->v_z, h->v_q, h->scal, h->partials, 1);
+        k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, res_scale, h->v_z, h->v_q, h->scal, h->partials, 1);
         k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 1);
         h->launches += 1;
         PLATO_LAUNCH_CHECK(h);
@@ -629,9 +721,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         h->ev_used = 0;
         int cur = 0;
         bool have_prev = false;
-        cudaEvent_t ev[2];
-        PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-        PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        cudaEvent_t* ev = h->poll_ev;
+        for (int e = 0; e < 2; ++e)
+            if (!ev[e]) PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
         for (;;) {
             for (int k = 0; k < kChunk; ++k, ++enqueued) {
                 const bool timed = h->timing && (enqueued % kTimingStride) == 0;
@@ -650,14 +742,14 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                     k_fcg_sell_apply<<<SB, kThreads, 0, s>>>(V, h->sell64, h->v_p, h->v_q, h->scal, h->partials);
                 }
                 if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
-                k_fcg_update<<<VB, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_q, h->f_dinv, h->f_res, h->f_d0,
+                k_fcg_update<<<VB, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_q, h->f_dinv, res_scale, h->f_res, h->f_d0,
                                                      h->f_y, cc.c0, h->scal, h->partials, max_it);
                 h->launches += 2;
                 inner_record = timed ? 2 * enqueued + 1 : -1;
                 rc = precondition(cc.c0);
                 inner_record = -1;
                 if (rc) return rc;
-                k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, h->v_z, h->v_q, h->scal, h->partials, 0);
+                k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, res_scale, h->v_z, h->v_q, h->scal, h->partials, 0);
                 k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 0);
                 h->launches += 1;
                 PLATO_LAUNCH_CHECK(h);
@@ -672,8 +764,6 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             cur ^= 1;
         }
         PLATO_CUDA(h, cudaStreamSynchronize(s));
-        cudaEventDestroy(ev[0]);
-        cudaEventDestroy(ev[1]);
         PcgScalars fin;
         PLATO_CUDA(h, cudaMemcpy(&fin, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
         rc = collect_timing(h, timed_iters, fin.iter - iter_base);
@@ -1024,6 +1114,8 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
     const int32_t max_it = h->opts.max_iterations;
     const int degree = h->opts.chebyshev_degree < 1 ? 1 : (h->opts.chebyshev_degree > 64 ? 64 : h->opts.chebyshev_degree);
     const int kind = inner_kind(h);
+    if (kind == INNER_SELL16S)
+        return plato_fail(h, PLATO_NOT_SUPPORTED, "the FP16 scaled inner precision is built for single problems");
     const SellView V = sell_view(h);
     const int T = bt.ncta;
     const BatchView BV{bt.nseg, bt.cta_seg, bt.cta_row0, bt.cta_row1, bt.seg_cta0, bt.S, h->scal, bt.ndone,
@@ -1060,17 +1152,16 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
     constexpr int kMaxPasses = 4;  // first pass + restarts from the true residual
     constexpr double kSlack = 10.0;
     int64_t precond_applies = 0;
-    cudaEvent_t ev[2];
-    PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-    auto destroy_events = [&]() { cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]); };
+    cudaEvent_t* ev = h->poll_ev;
+    for (int e = 0; e < 2; ++e)
+        if (!ev[e]) PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
     int pass = 0;
     for (;; ++pass) {
         // r = b - A x; members whose (true) residual passes are done
         PLATO_CUDA(h, cudaMemsetAsync(bt.ndone, 0, sizeof(int32_t), s));
         PLATO_CUDA(h, cudaMemsetAsync(&h->scal->done, 0, sizeof(int32_t), s));
         rc = launch_sell_spmv(h, h->sell64, x, h->v_r);
-        if (rc) { destroy_events(); return rc; }
+        if (rc) return rc;
         k_bfcg_start<<<T, kThreads, 0, s>>>(BV, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, tol,
                                              pass > 0 ? 1 : 0, pass > 0 ? kSlack : 1.0);
         PLATO_LAUNCH_CHECK(h);
@@ -1080,7 +1171,7 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         if (slots[0].done || pass == kMaxPasses - 1) break;
         // z = M r, p = z, p.r
         rc = chebyshev_steps();
-        if (rc) { destroy_events(); return rc; }
+        if (rc) return rc;
         k_bfcg_zq<<<T, kThreads, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 1);
         k_bfcg_direction<<<T, kThreads, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 1);
         h->launches += 2;
@@ -1094,7 +1185,7 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
                                                       h->f_y, cc.c0, max_it);
                 h->launches += 2;
                 rc = chebyshev_steps();
-                if (rc) { destroy_events(); return rc; }
+                if (rc) return rc;
                 k_bfcg_zq<<<T, kThreads, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 0);
                 k_bfcg_direction<<<T, kThreads, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 0);
                 h->launches += 2;
@@ -1112,7 +1203,6 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         }
         PLATO_CUDA(h, cudaStreamSynchronize(s));
     }
-    destroy_events();
     PLATO_CUDA(h, cudaMemcpyAsync(bt.S_host, bt.S, sizeof(SegScalars) * bt.nseg, cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));
     bt.last.assign(bt.nseg, plato_solve_stats{});

@@ -111,6 +111,9 @@ struct CoarseSpace {
     int32_t* elem_list = nullptr;
     double*  E = nullptr;         // Galerkin operator, then its Cholesky factor (ndof^2)
     double*  Einv = nullptr;      // explicit inverse (ndof^2)
+    double*  X = nullptr;         // L^-1 while inverting (ndof^2)
+    double*  T = nullptr;         // tile-product scratch of the inversion (ndof^2)
+    double*  Dt = nullptr;        // inverse diagonal tiles of the Cholesky factor
     int32_t  rsplit = 1, gsplit = 1;  // CTAs per coarse cell in the restriction / Galerkin sum
     double*  rpart = nullptr;     // restriction partial sums (ncells * rsplit * 24)
     double*  rc = nullptr;        // restricted residual
@@ -192,6 +195,9 @@ struct plato_problem {
     double* sell64 = nullptr;      // FP64 entries
     float*  sell32 = nullptr;      // FP32 entries (mixed precision)
     void*   sell16 = nullptr;      // BF16 entries (mixed precision)
+    void*   sell16s = nullptr;     // FP16 entries of D^-1/2 A D^-1/2 (scaled mixed precision)
+    float*  f_sq = nullptr;        // D^1/2 (scaled mixed precision)
+    float*  f_isq = nullptr;       // D^-1/2
     // matrix-free operator data (matfree.cu) and mixed-precision work vectors (mixed.cu)
     double* mf_w64 = nullptr;      // per-cell SIMP weight s(rho_e), FP64
     float*  mf_w32 = nullptr;      // same, FP32
@@ -205,6 +211,7 @@ struct plato_problem {
     // solver's operator apply (every kTimingStride-th apply, events on the handle's stream)
     int64_t launches = 0;
     int     timing = 0;
+    cudaEvent_t poll_ev[2] = {nullptr, nullptr};  // host polling of the solver scalars (made once)
     std::vector<cudaEvent_t> ev_pool;
     int     ev_used = 0;
     double  op_ms_total = 0.0;
@@ -242,7 +249,8 @@ int plato_fail(plato_problem* h, int status, const std::string& msg);
 namespace plato {
 int coarse_setup_mesh(plato_problem* h);
 int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy = nullptr);
-int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S);
+int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S,
+                 const float* sq = nullptr);
 void coarse_release(plato_problem* h);
 void batch_release(plato_problem* h);
 int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);

@@ -12,8 +12,12 @@
 // The copy is made once per solve from the constrained CRS by a per-slice shared-memory
 // transpose (both sides coalesced), which also extracts the Jacobi diagonal and can emit
 // FP32 and BF16 copies of the entries for the mixed-precision preconditioner.
+#include <mutex>
+
 #include <cub/cub.cuh>
 #include <cuda_bf16.h>
+
+#include <cuda_fp16.h>
 
 #include "plato_internal.cuh"
 #include "sell.cuh"
@@ -108,6 +112,39 @@ k_crs_to_sell(int32_t N, int32_t nslices, const int32_t* __restrict__ row_map, c
     }
 }
 
+// FP16 copy of the Jacobi-scaled matrix: entry (a, b) of block k of row r, column node c,
+// becomes A * sqrt(dinv[3r+a]) * sqrt(dinv[3c+b]) (dinv = 1 / diag, FP64), same slots as
+// the FP64 SELL copy.  Also sq = D^1/2, isq = D^-1/2 and ones (the Jacobi diagonal of the
+// scaled matrix) in FP32.
+__global__ void k_sell_scale16(int32_t N, int32_t nslices, const int32_t* __restrict__ width,
+                               const int64_t* __restrict__ ptr, const int32_t* __restrict__ cols,
+                               const double* __restrict__ sell64, const double* __restrict__ dinv,
+                               __half* __restrict__ out16, float* __restrict__ sq, float* __restrict__ isq,
+                               float* __restrict__ ones) {
+    for (int64_t s = blockIdx.x; s < nslices; s += gridDim.x) {
+        const int w = width[s];
+        const int64_t base = ptr[s];
+        for (int t = threadIdx.x; t < 9 * 32 * w; t += blockDim.x) {
+            const int l = t & 31, kq = t >> 5;
+            const int k = kq / 9, q = kq - 9 * k, a = q / 3, b = q - 3 * a;
+            const int64_t r = 32 * s + l;
+            double v = 0.0;
+            if (r < N) {
+                const int64_t c = cols[base + 32 * k + l];
+                v = sell64[9 * base + t] * sqrt(dinv[3 * r + a]) * sqrt(dinv[3 * c + b]);
+            }
+            out16[9 * base + t] = __double2half(v);
+        }
+        if (threadIdx.x < 96 && 32 * s + threadIdx.x / 3 < N) {
+            const int64_t i = 96 * s + threadIdx.x;
+            const double di = dinv[i];
+            sq[i] = float(1.0 / sqrt(di));
+            isq[i] = float(sqrt(di));
+            ones[i] = 1.0f;
+        }
+    }
+}
+
 }  // namespace
 
 int build_sell_pattern(plato_problem* h) {
@@ -160,8 +197,18 @@ int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float
     const size_t smem = size_t(9) * P.max_slice_blocks * sizeof(double);
     const int grid = grid_for(P.nslices, 1, 148 * 16);
     if (smem <= 200 * 1024) {
-        PLATO_CUDA(h, cudaFuncSetAttribute(k_crs_to_sell<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(smem > 48 * 1024 ? smem : 48 * 1024)));
+        // the attribute is per kernel and process; raise it only (a driver round trip per call otherwise)
+        static std::mutex mu;
+        static int granted = 0;
+        const int want = int(smem > 48 * 1024 ? smem : 48 * 1024);
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            if (want > granted) {
+                PLATO_CUDA(h, cudaFuncSetAttribute(k_crs_to_sell<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   want));
+                granted = want;
+            }
+        }
         k_crs_to_sell<true><<<grid, kSliceThreads, smem, h->stream>>>(
             h->N, P.nslices, h->row_map, h->diag, P.width, P.ptr, crs, out64, out32,
             static_cast<__nv_bfloat16*>(out16), dinv, dinv32);
@@ -170,6 +217,15 @@ int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float
             h->N, P.nslices, h->row_map, h->diag, P.width, P.ptr, crs, out64, out32,
             static_cast<__nv_bfloat16*>(out16), dinv, dinv32);
     }
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+int launch_sell_scale16(plato_problem* h, const double* sell64, const double* dinv, void* out16, float* sq,
+                        float* isq, float* ones) {
+    const SellPattern& P = h->sell;
+    k_sell_scale16<<<grid_for(P.nslices, 1, 148 * 16), kSliceThreads, 0, h->stream>>>(
+        h->N, P.nslices, P.width, P.ptr, P.cols, sell64, dinv, static_cast<__half*>(out16), sq, isq, ones);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -326,9 +326,9 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
         h->ev_used = 0;
         int cur = 0;
         bool have_prev = false;
-        cudaEvent_t ev[2];
-        PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-        PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        cudaEvent_t* ev = h->poll_ev;
+        for (int e = 0; e < 2; ++e)
+            if (!ev[e]) PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
         for (;;) {
             for (int k = 0; k < kChunk; ++k, ++enqueued) {
                 const bool timed = h->timing && (enqueued % kTimingStride) == 0;
@@ -364,8 +364,6 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
             cur ^= 1;
         }
         PLATO_CUDA(h, cudaStreamSynchronize(s));
-        cudaEventDestroy(ev[0]);
-        cudaEventDestroy(ev[1]);
         PcgScalars fin;
         PLATO_CUDA(h, cudaMemcpy(&fin, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
         rc = collect_timing(h, timed_iters, fin.iter - iter_base);

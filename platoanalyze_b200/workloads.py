@@ -52,7 +52,7 @@ def large_problem(solver: SolverOptions | None = None, n: tuple[int, int, int] =
 
 COARSE_BOX = (10, 5, 5)  # coarse box grid of the two-level method (aligns with 20k x 10k x 10k hex grids)
 
-METHODS = ("two-level", "plain", "chebyshev", "bf16", "matrix-free")
+METHODS = ("two-level", "two-level-fp16", "plain", "chebyshev", "bf16", "matrix-free")
 
 
 def method_options(method: str, tol: float = 1e-10, coarse=COARSE_BOX) -> SolverOptions:
@@ -61,6 +61,8 @@ def method_options(method: str, tol: float = 1e-10, coarse=COARSE_BOX) -> Solver
     plain        FP64 Jacobi-PCG on the assembled block matrix (the reference's algorithm)
     two-level    FP64 flexible CG; FP32 Chebyshev(8)-Jacobi on an FP32 copy of the matrix plus
                  a Galerkin coarse correction on a trilinear box grid
+    two-level-fp16  the same with the Chebyshev sweep on an FP16 copy of the Jacobi-scaled
+                 matrix D^-1/2 A D^-1/2
     chebyshev    the same without the coarse correction
     bf16         BF16-stored matrix, Chebyshev(16)-Jacobi, no coarse correction
     matrix-free  FP32 element-by-element operator, Chebyshev(16)-Jacobi, no coarse correction
@@ -69,6 +71,9 @@ def method_options(method: str, tol: float = 1e-10, coarse=COARSE_BOX) -> Solver
         return SolverOptions(tolerance=tol, max_iterations=200000)
     if method == "two-level":
         return SolverOptions(tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP32,
+                             chebyshev_degree=8, chebyshev_ratio=30.0, coarse_cells=tuple(coarse))
+    if method == "two-level-fp16":
+        return SolverOptions(tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP16,
                              chebyshev_degree=8, chebyshev_ratio=30.0, coarse_cells=tuple(coarse))
     if method == "chebyshev":
         return SolverOptions(tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP32,

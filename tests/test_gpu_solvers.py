@@ -28,6 +28,9 @@ CONFIGS = {
                                        coarse_cells=(5, 5, 5)),
     "bf16_cheb4_coarse": SolverOptions(precision=capi.PRECISION_MIXED_BF16, chebyshev_degree=4,
                                        coarse_cells=(10, 5, 5)),
+    "fp16s_cheb8": SolverOptions(precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8),
+    "fp16s_cheb8_coarse": SolverOptions(precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8,
+                                        coarse_cells=(10, 5, 5)),
     "mf_fp32_cheb4_coarse": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE,
                                           precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4,
                                           coarse_cells=(4, 2, 2)),

@@ -724,8 +724,11 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         cudaEvent_t* ev = h->poll_ev;
         for (int e = 0; e < 2; ++e)
             if (!ev[e]) PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
+        ChunkPlanner plan;
+        plan.full = kChunk;
+        int32_t chunk = kChunk;
         for (;;) {
-            for (int k = 0; k < kChunk; ++k, ++enqueued) {
+            for (int k = 0; k < chunk; ++k, ++enqueued) {
                 const bool timed = h->timing && (enqueued % kTimingStride) == 0;
                 cudaEvent_t e0 = nullptr, e1 = nullptr;
                 if (timed) {
@@ -756,9 +759,11 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             }
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
+            const int32_t queued = chunk;  // behind the polled state: this chunk
             if (have_prev) {
                 PLATO_CUDA(h, cudaEventSynchronize(ev[cur ^ 1]));
                 if (slots[cur ^ 1].done) break;
+                chunk = plan.next(slots[cur ^ 1], queued);
             }
             have_prev = true;
             cur ^= 1;

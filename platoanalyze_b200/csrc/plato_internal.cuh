@@ -2,6 +2,8 @@
 // device-side element arithmetic shared by every kernel.
 #pragma once
 
+#include <cmath>
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -59,6 +61,32 @@ struct PcgScalars {
     int32_t done;    // 1 once ||r|| <= tol ||b||
     int32_t nonfinite;
     uint32_t ticket; // last-block-done counter of the fused reductions
+};
+
+// Size of the next chunk of Krylov iterations the host enqueues while the previous one runs.
+// Every iteration enqueued after convergence still launches its kernels (they return at
+// once), so near the end the chunks shrink to what the observed residual decay predicts:
+// polled state s (its iteration count and r.r), `in_flight` iterations already queued
+// behind it.  Early or irregular decay keeps the full chunk.
+struct ChunkPlanner {
+    int32_t full = 16;
+    int32_t last_iter = -1;
+    double  last_rr = 0.0;
+    int32_t next(const PcgScalars& st, int32_t in_flight) {
+        int32_t size = full;
+        if (last_iter >= 0 && st.iter > last_iter && st.rr > 0.0 && last_rr > 0.0 && st.tol2 > 0.0) {
+            const double rate = std::pow(st.rr / last_rr, 1.0 / double(st.iter - last_iter));
+            if (rate > 0.0 && rate < 0.999) {
+                const double left = std::log(st.tol2 / st.rr) / std::log(rate);  // iterations still needed
+                const double after = left - double(in_flight);
+                if (after <= 0.0) size = 2;
+                else if (after + 2.0 < double(full)) size = int32_t(after) + 2;
+            }
+        }
+        last_iter = st.iter;
+        last_rr = st.rr;
+        return size;
+    }
 };
 
 // Per-problem Krylov state of a batched solve (one entry per member problem).

@@ -329,8 +329,11 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
         cudaEvent_t* ev = h->poll_ev;
         for (int e = 0; e < 2; ++e)
             if (!ev[e]) PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
+        ChunkPlanner plan;
+        plan.full = kChunk;
+        int32_t chunk = kChunk;
         for (;;) {
-            for (int k = 0; k < kChunk; ++k, ++enqueued) {
+            for (int k = 0; k < chunk; ++k, ++enqueued) {
                 const bool timed = h->timing && (enqueued % kTimingStride) == 0;
                 cudaEvent_t e0 = nullptr, e1 = nullptr;
                 if (timed) {
@@ -352,13 +355,15 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
                 if (!p2) k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
             }
             // the operator applies count themselves
-            h->launches += (p2 ? kChunk : 2 * kChunk) - 1;
+            h->launches += (p2 ? chunk : 2 * chunk) - 1;
             PLATO_LAUNCH_CHECK(h);
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));
+            const int32_t queued = chunk;
             if (have_prev) {
                 PLATO_CUDA(h, cudaEventSynchronize(ev[cur ^ 1]));
                 if (slots[cur ^ 1].done) break;
+                chunk = plan.next(slots[cur ^ 1], queued);
             }
             have_prev = true;
             cur ^= 1;

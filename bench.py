@@ -10,7 +10,7 @@ nu = 0.3, SIMP p = 3, rho_min = 1e-9, nodal densities i.i.d. U[0.01, 1] (SplitMi
 Methods (--method):
   two-level-fp16  (default) FP64 flexible CG; preconditioner = FP32 Chebyshev-Jacobi smoothing
              on an FP16 copy of the Jacobi-scaled matrix D^-1/2 A D^-1/2 + Galerkin coarse
-             correction on a 10x5x5 box grid (A-DEF2 two-level form).
+             correction on a 16x8x8 box grid (A-DEF2 two-level form).
   two-level  the same with an FP32 copy of the unscaled matrix.
   plain      the reference's algorithm: FP64 Jacobi-PCG on the assembled block matrix.
 Both stop on the same FP64 residual test (1e-10); the line also carries the plain method's
@@ -40,17 +40,18 @@ sys.path.insert(0, str(ROOT))
 METRIC = "solve+adjoint/s at 3.2M DoF, 1e-8 rel err: learned-MP PCG vs plain FP64 PCG"
 UNIT = "solve+adjoint/s"
 SIZES = {"large": (160, 80, 80), "medium": (80, 40, 40), "small": (20, 10, 10)}
-COARSE = (10, 5, 5)  # coarse box grid of the two-level method (aligned with every size above)
+# coarse box grid of the two-level method: coarse cells of 10^3 hexes (16x8x8 on 160x80x80,
+# 4131 coarse dofs), see workloads.coarse_grid
 # Jacobi-PCG iterations of the plain FP64 method at tol 1e-10 (measured by this bench on B200
 # and by the CPU oracle's own solve; the reference arm extrapolates its sample with them).
 FP64_ITERATIONS = {"large": 3632, "medium": 1833, "small": None}
 
 
 METHOD_TEXT = {
-    "two-level": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP32 SELL copy + "
-                  "FP64 Galerkin coarse correction on a 10x5x5 trilinear box grid"),
-    "two-level-fp16": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP16 copy of the "
-                       "Jacobi-scaled matrix D^-1/2 A D^-1/2 + FP64 Galerkin coarse correction on a 10x5x5 trilinear "
+    "two-level": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (10 steps on [lmax/200, lmax]) on an FP32 SELL copy + "
+                  "FP64 Galerkin coarse correction on a 16x8x8 trilinear box grid"),
+    "two-level-fp16": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (10 steps on [lmax/200, lmax]) on an FP16 copy of the "
+                       "Jacobi-scaled matrix D^-1/2 A D^-1/2 + FP64 Galerkin coarse correction on a 16x8x8 trilinear "
                        "box grid"),
     "plain": "plain FP64 Jacobi-PCG on the assembled 3x3 block matrix (the reference's algorithm)",
     "chebyshev": "FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (8 steps) on an FP32 SELL copy",
@@ -76,10 +77,10 @@ def parse():
     return ap.parse_args()
 
 
-def solver_options(method: str, tol: float):
-    from platoanalyze_b200.workloads import method_options
+def solver_options(method: str, tol: float, size: str = "large"):
+    from platoanalyze_b200.workloads import coarse_grid, method_options
 
-    return method_options(method, tol, COARSE)
+    return method_options(method, tol, coarse_grid(*SIZES[size]))
 
 
 def peaks():
@@ -460,7 +461,7 @@ def main():
     from platoanalyze_b200.problem import EllipticProblem
     from platoanalyze_b200.workloads import SEED_LARGE, cantilever, splitmix_uniform
 
-    spec = cantilever(*SIZES[args.size], solver_options(args.method, args.tol))
+    spec = cantilever(*SIZES[args.size], solver_options(args.method, args.tol, args.size))
     z = splitmix_uniform(spec.coords.shape[0], SEED_LARGE)
     prob = EllipticProblem(spec)
     zd = prob.to_dev(z)
@@ -563,12 +564,12 @@ def main():
     # the plain FP64 GPU method on the same problem, same run (comparison only)
     plain = None
     if args.method != "plain":
-        prob.set_solver(solver_options("plain", args.tol))
+        prob.set_solver(solver_options("plain", args.tol, args.size))
         step()
         ms_plain, _, pstats = timed_steps(2)
         plain = {"value": world * 2 / (ms_plain / 1e3), "ms_per_step": ms_plain / 2,
                  "pcg_iterations": [s["iterations"] for s in pstats]}
-        prob.set_solver(solver_options(args.method, args.tol))
+        prob.set_solver(solver_options(args.method, args.tol, args.size))
 
     # accuracy against the CPU oracle's own FP64 solve of the full problem (untimed); the same
     # oracle run is the CPU baseline (all host threads)

@@ -14,13 +14,13 @@
 // CTA stages batches of elements' coarse gradients in shared memory and accumulates its
 // share of the cell's symmetric 24x24 block in registers (as a rank-k update of the
 // gradients for the elements whose nodes are free or fully clamped, entry by entry for the
-// rest), then adds it to E.  E is
-// factored (blocked Cholesky, 32x32 tiles) and inverted explicitly (E^-1 = L^-T L^-1), so a
-// coarse solve in the iteration is one dense matrix-vector product.  Each diagonal tile's
-// inverse is formed as the tile is factored, so the panels and the inverse are tile products.
+// rest), then adds it to E.  E is factored (blocked Cholesky, 64x64 tiles; each diagonal
+// tile's inverse is formed as it is factored, so the panels are tile products) and L is
+// inverted by doubling (batched 64x64 tile products), so a coarse solve in the iteration is
+// two triangular matrix-vector products with X = L^-1 and its transpose.
 // Per preconditioner call: restriction in two deterministic passes (per-cell partial sums by
-// split CTAs, then a fixed-order sum per coarse dof), y_c = E^-1 r_c (warp per row),
-// prolongation (thread per fine node).
+// split CTAs, then a fixed-order sum per coarse dof), y_c = X^T (X r_c) with X = L^-1 (two
+// triangular matrix-vector products, warp per row), prolongation (thread per fine node).
 #include <mutex>
 
 #include <cub/cub.cuh>
@@ -33,7 +33,6 @@ GraphView graph_view(const plato_problem* h);
 
 namespace {
 
-constexpr int kTile = 32;
 constexpr int kBatch = 32;     // elements staged per Galerkin batch (8 threads each)
 constexpr int kThreadsPerCta = 256;
 
@@ -351,148 +350,228 @@ __global__ void k_regularize(int n, double* __restrict__ E) {
         if (!(E[(int64_t)k * n + k] > 0.0)) E[(int64_t)k * n + k] = 1.0;
 }
 
-// ---- blocked Cholesky (lower, in place) --------------------------------------------------
+// ---- dense SPD inverse: blocked Cholesky and L^-1 by doubling, 64 x 64 tiles -------------
+// E (n x n, row-major, stride n) is factored in place (lower), each diagonal tile's inverse
+// kept in D; then X = L^-1 by doubling and E^-1 = X^T X.  Every bulk step is a product of
+// 64 x 64 tiles (`tile_gemm`: 256 threads, 4 x 4 outputs each, operands staged 16 columns at a
+// time), so the O(n^3) work runs at tile-GEMM speed and the number of launches grows with n/64.
 
-// Factors the diagonal block kb in place (L_kk) and writes its inverse L_kk^-1 to D[kb]
-// (a 32 x 32 lower-triangular tile): the panel and the explicit inverse then need only tile
-// products, no substitution.
-__global__ void k_chol_diag(int n, double* __restrict__ A, int kb, double* __restrict__ D, int32_t* __restrict__ bad) {
-    __shared__ double T[kTile][kTile + 1];
-    __shared__ double W[kTile][kTile + 1];
-    const int r0 = kb * kTile, m = min(kTile, n - r0);
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    if (tx < m && ty < m) T[ty][tx] = A[(int64_t)(r0 + ty) * n + r0 + tx];
-    W[ty][tx] = (tx == ty) ? 1.0 : 0.0;
+constexpr int kNB = 64;   // tile edge
+constexpr int kKB = 16;   // k columns staged per pass
+
+// C(ti,tj) = beta C + alpha sum_{kt in [k0,k1)} opA(ti,kt) opB(kt,tj), tiles of kNB; opA(ti,kt)
+// is A's tile (ti,kt), or the transpose of its tile (kt,ti) with TA; opB likewise with TB.
+// Entries outside n read as 0 and are not stored.
+template <int TA, int TB>
+__device__ __forceinline__ void tile_gemm(int n, const double* __restrict__ A, const double* __restrict__ B,
+                                          double* __restrict__ C, int ti, int tj, int k0, int k1, double alpha,
+                                          double beta) {
+    __shared__ double As[kKB][kNB + 1];  // As[k][row]
+    __shared__ double Bs[kKB][kNB + 1];  // Bs[k][col]
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int r0 = ti * kNB, c0 = tj * kNB;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int kt = k0; kt < k1; ++kt) {
+        for (int kk = 0; kk < kNB; kk += kKB) {
+            const int kbase = kt * kNB + kk;
+            __syncthreads();
+            // 1024 values per operand: 4 per thread
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = tid + 256 * q;
+                if (TA == 0) {  // A[r0 + row][kbase + c]: c fastest
+                    const int c = e & 15, row = e >> 4;
+                    const int gr = r0 + row, gc = kbase + c;
+                    As[c][row] = (gr < n && gc < n) ? A[(int64_t)gr * n + gc] : 0.0;
+                } else {        // A[kbase + c][r0 + row]: row fastest
+                    const int row = e & 63, c = e >> 6;
+                    const int gr = kbase + c, gc = r0 + row;
+                    As[c][row] = (gr < n && gc < n) ? A[(int64_t)gr * n + gc] : 0.0;
+                }
+                if (TB == 0) {  // B[kbase + c][c0 + col]: col fastest
+                    const int col = e & 63, c = e >> 6;
+                    const int gr = kbase + c, gc = c0 + col;
+                    Bs[c][col] = (gr < n && gc < n) ? B[(int64_t)gr * n + gc] : 0.0;
+                } else {        // B[c0 + col][kbase + c]: c fastest
+                    const int c = e & 15, col = e >> 4;
+                    const int gr = c0 + col, gc = kbase + c;
+                    Bs[c][col] = (gr < n && gc < n) ? B[(int64_t)gr * n + gc] : 0.0;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kKB; ++k) {
+                double a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gr = r0 + ty + 16 * i;
+        if (gr >= n) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gc = c0 + tx + 16 * j;
+            if (gc >= n) continue;
+            double* cp = C + (int64_t)gr * n + gc;
+            *cp = (beta == 0.0 ? 0.0 : beta * *cp) + alpha * acc[i][j];
+        }
+    }
+}
+
+// Factors diagonal tile kb in place (lower, zeros above) and writes its inverse to D[kb]
+// (kNB x kNB, row-major).  One CTA of 256 threads.
+constexpr size_t kTwoTiles = sizeof(double) * 2 * kNB * (kNB + 1);  // dynamic shared memory of the next two
+
+__global__ void __launch_bounds__(256) k_chol_diag(int n, double* __restrict__ A, int kb, double* __restrict__ D,
+                                                  int32_t* __restrict__ bad) {
+    extern __shared__ double dyn[];
+    double (*T)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn);
+    double (*W)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn + kNB * (kNB + 1));
+    const int r0 = kb * kNB, m = min(kNB, n - r0);
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int i = e >> 6, j = e & 63;
+        T[i][j] = (i < m && j < m) ? A[(int64_t)(r0 + i) * n + r0 + j] : (i == j ? 1.0 : 0.0);
+    }
     __syncthreads();
+    // right-looking: thread (ty, tx) owns rows ty + 16a and columns tx + 16b of the tile
     for (int k = 0; k < m; ++k) {
-        if (tx == 0 && ty == 0) {
+        if (tid == 0) {
             const double d = T[k][k];
             if (!(d > 0.0)) { atomicExch(bad, 1); T[k][k] = 1.0; }
             else T[k][k] = sqrt(d);
         }
         __syncthreads();
-        if (tx == 0 && ty > k && ty < m) T[ty][k] /= T[k][k];
+        if (tid > k && tid < m) T[tid][k] /= T[k][k];
         __syncthreads();
-        if (ty > k && tx > k && tx <= ty && ty < m) T[ty][tx] -= T[ty][k] * T[tx][k];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = ty + 16 * a;
+            if (i <= k || i >= m) continue;
+            const double tik = T[i][k];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int j = tx + 16 * b;
+                if (j > k && j <= i) T[i][j] -= tik * T[j][k];
+            }
+        }
         __syncthreads();
     }
-    // W = L^-1 row by row: row r is final once divided by L_rr, then leaves the rows below
-    for (int r = 0; r < m; ++r) {
-        if (ty == r && tx <= r) W[r][tx] /= T[r][r];
-        __syncthreads();
-        if (ty > r && ty < m && tx <= r) W[ty][tx] -= T[ty][r] * W[r][tx];
-        __syncthreads();
+    // W = L^-1, thread j < m forms column j top-down; all threads read the same T[i][k]
+    if (tid < kNB) {
+        const int j = tid;
+        for (int i = 0; i < kNB; ++i) {
+            double v = 0.0;
+            if (i >= j && i < m) {
+                double s2 = (i == j) ? 1.0 : 0.0;
+                for (int k = j; k < i; ++k) s2 -= T[i][k] * W[k][j];
+                v = s2 / T[i][i];
+            }
+            W[i][j] = v;
+        }
     }
-    if (tx < m && ty < m) A[(int64_t)(r0 + ty) * n + r0 + tx] = (tx <= ty) ? T[ty][tx] : 0.0;
-    D[(int64_t)kb * kTile * kTile + ty * kTile + tx] = (tx < m && ty < m && tx <= ty) ? W[ty][tx] : 0.0;
-}
-
-// A[ib,kb] <- A[ib,kb] L_kk^-T for every block row ib > kb (one CTA per block row)
-__global__ void k_chol_panel(int n, double* __restrict__ A, int kb, const double* __restrict__ D) {
-    __shared__ double Dk[kTile][kTile + 1];
-    __shared__ double X[kTile][kTile + 1];
-    const int ib = kb + 1 + blockIdx.x;
-    const int r0 = ib * kTile, c0 = kb * kTile;
-    const int mr = min(kTile, n - r0), mc = min(kTile, n - c0);
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    Dk[ty][tx] = D[(int64_t)kb * kTile * kTile + ty * kTile + tx];
-    X[ty][tx] = (tx < mc && ty < mr) ? A[(int64_t)(r0 + ty) * n + c0 + tx] : 0.0;
     __syncthreads();
-    // (X L^-T)[ty][tx] = sum_{k <= tx} X[ty][k] Linv[tx][k]
-    double s = 0.0;
-    for (int k = 0; k <= tx; ++k) s += X[ty][k] * Dk[tx][k];
-    if (tx < mc && ty < mr) A[(int64_t)(r0 + ty) * n + c0 + tx] = s;
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int i = e >> 6, j = e & 63;
+        if (i < m && j < m) A[(int64_t)(r0 + i) * n + r0 + j] = (j <= i) ? T[i][j] : 0.0;
+        D[(int64_t)kb * kNB * kNB + e] = (i < m && j < m && j <= i) ? W[i][j] : 0.0;
+    }
 }
 
-// trailing update A[ib,jb] -= A[ib,kb] A[jb,kb]^T for kb < jb <= ib
-__global__ void k_chol_update(int n, double* __restrict__ A, int kb, int nblk) {
-    __shared__ double P[kTile][kTile + 1];
-    __shared__ double Q[kTile][kTile + 1];
+// Panel: A[ib,kb] <- A[ib,kb] L_kk^-T for every tile row ib > kb (one CTA per tile row).
+__global__ void __launch_bounds__(256) k_chol_panel(int n, double* __restrict__ A, int kb,
+                                                   const double* __restrict__ D) {
+    extern __shared__ double dyn[];
+    double (*Ds)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn);
+    double (*Ps)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn + kNB * (kNB + 1));
+    const int ib = kb + 1 + blockIdx.x;
+    const int r0 = ib * kNB, c0 = kb * kNB;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int i = e / kNB, j = e - kNB * i;
+        Ds[i][j] = D[(int64_t)kb * kNB * kNB + e];
+        Ps[i][j] = (r0 + i < n && c0 + j < n) ? A[(int64_t)(r0 + i) * n + c0 + j] : 0.0;
+    }
+    __syncthreads();
+    // (P L^-T)[i][j] = sum_{k <= j} P[i][k] Linv[j][k]
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int k = 0; k < kNB; ++k) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = Ps[ty + 16 * i][k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Ds[tx + 16 * j][k];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gr = r0 + ty + 16 * i, gc = c0 + tx + 16 * j;
+            if (gr < n && gc < n) A[(int64_t)gr * n + gc] = acc[i][j];
+        }
+}
+
+// Trailing update A[ib,jb] -= A[ib,kb] A[jb,kb]^T for kb < jb <= ib (blockIdx enumerates the
+// lower triangle of the trailing tiles).
+__global__ void __launch_bounds__(256) k_chol_update(int n, double* __restrict__ A, int kb, int nblk) {
     const int rem = nblk - kb - 1;
-    // blockIdx.x enumerates (ib, jb) with jb <= ib in the trailing triangle
     int idx = blockIdx.x, ib = 0;
     while (idx >= ib + 1) { idx -= ib + 1; ++ib; }
-    const int jb = idx;
     if (ib >= rem) return;
-    const int gi = kb + 1 + ib, gj = kb + 1 + jb;
-    const int r0 = gi * kTile, s0 = gj * kTile, c0 = kb * kTile;
-    const int mr = min(kTile, n - r0), ms = min(kTile, n - s0), mc = min(kTile, n - c0);
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    P[ty][tx] = (ty < mr && tx < mc) ? A[(int64_t)(r0 + ty) * n + c0 + tx] : 0.0;
-    Q[ty][tx] = (ty < ms && tx < mc) ? A[(int64_t)(s0 + ty) * n + c0 + tx] : 0.0;
-    __syncthreads();
-    if (ty < mr && tx < ms) {
-        double s = 0.0;
-        for (int k = 0; k < mc; ++k) s += P[ty][k] * Q[tx][k];
-        A[(int64_t)(r0 + ty) * n + s0 + tx] -= s;
+    const int gi = kb + 1 + ib, gj = kb + 1 + idx;
+    tile_gemm<0, 1>(n, A, A, A, gi, gj, kb, kb + 1, -1.0, 1.0);
+}
+
+// X = L^-1 by doubling: X starts as its diagonal tiles D[i] and zeros; level s joins blocks
+// of s tiles into blocks of 2s: X[B2,B1] = -X[B2,B2] L[B2,B1] X[B1,B1], in two batched passes:
+// mode 0: T[i,j] = sum_{k in B1, k >= j} L[i,k] X[k,j];  mode 1: X[i,j] = -sum_{k in B2, k <= i} X[i,k] T[k,j].
+__global__ void k_tri_init(int n, const double* __restrict__ D, double* __restrict__ X) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = int(e / n), c = int(e - (int64_t)r * n);
+        const int ib = r / kNB, jb = c / kNB;
+        X[e] = (ib == jb) ? D[(int64_t)ib * kNB * kNB + (r - ib * kNB) * kNB + (c - jb * kNB)] : 0.0;
     }
 }
 
-// X = L^-1 by doubling: with the inverses of two adjacent diagonal blocks B1 (above) and B2
-// known, X[B2,B1] = -X[B2,B2] L[B2,B1] X[B1,B1].  Level s joins blocks of s tiles into blocks
-// of 2s, so five levels of two batched tile-product launches cover 19 tiles, and no CTA
-// carries more than s tile products (the column-by-column substitution carried up to 171).
-// X starts as its diagonal tiles D[i] = L_ii^-1 and zeros.
-__global__ void k_tri_init(int n, int nblk, const double* __restrict__ D, double* __restrict__ X) {
-    const int ib = blockIdx.y, jb = blockIdx.x;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int r = ib * kTile + ty, c = jb * kTile + tx;
-    if (r >= n || c >= n) return;
-    X[(int64_t)r * n + c] = (ib == jb) ? D[(int64_t)ib * kTile * kTile + ty * kTile + tx] : 0.0;
-}
-
-// Level s, one CTA per output tile (pair p, row tile i of B2, column tile j of B1):
-// mode 0: T[i,j] = sum_{k in B1, k >= j} L[i,k] X[k,j];  mode 1: X[i,j] = -sum_{k in B2, k <= i} X[i,k] T[k,j]
-__global__ void k_tri_level(int n, int nblk, int s, int mode, const double* __restrict__ A, double* __restrict__ X,
-                            double* __restrict__ T) {
-    __shared__ double P[kTile][kTile + 1];
-    __shared__ double Q[kTile][kTile + 1];
+__global__ void __launch_bounds__(256) k_tri_level(int n, int nblk, int s, int mode, const double* __restrict__ L,
+                                                  double* __restrict__ X, double* __restrict__ T) {
     const int per_pair = s * s;
     const int pair = blockIdx.x / per_pair, rem = blockIdx.x - pair * per_pair;
-    const int b1 = pair * 2 * s, b2 = b1 + s;              // first tiles of B1 and B2
-    const int e1 = min(b2, nblk), e2 = min(b2 + s, nblk);  // ends
+    const int b1 = pair * 2 * s, b2 = b1 + s;
+    const int e1 = min(b2, nblk), e2 = min(b2 + s, nblk);
     const int i = b2 + rem / s, j = b1 + rem % s;
     if (b2 >= nblk || i >= e2 || j >= e1) return;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int r0 = i * kTile, c0 = j * kTile;
-    const int mr = min(kTile, n - r0), mc = min(kTile, n - c0);
-    const int k_lo = mode == 0 ? j : b2, k_hi = mode == 0 ? e1 : i + 1;
-    const double* left = mode == 0 ? A : X;
-    const double* right = mode == 0 ? X : T;
-    double acc = 0.0;
-    for (int kb = k_lo; kb < k_hi; ++kb) {
-        const int k0 = kb * kTile, mk = min(kTile, n - k0);
-        __syncthreads();
-        P[ty][tx] = (ty < mr && tx < mk) ? left[(int64_t)(r0 + ty) * n + k0 + tx] : 0.0;
-        Q[ty][tx] = (ty < mk && tx < mc) ? right[(int64_t)(k0 + ty) * n + c0 + tx] : 0.0;
-        __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < kTile; ++k) acc += P[ty][k] * Q[k][tx];
-    }
-    if (ty < mr && tx < mc) {
-        if (mode == 0) T[(int64_t)(r0 + ty) * n + c0 + tx] = acc;
-        else X[(int64_t)(r0 + ty) * n + c0 + tx] = -acc;
-    }
+    if (mode == 0) tile_gemm<0, 0>(n, L, X, T, i, j, j, e1, 1.0, 0.0);
+    else tile_gemm<0, 0>(n, X, T, X, i, j, b2, i + 1, -1.0, 0.0);
 }
 
-// Einv = X^T X for X = L^-1 (lower): Einv[ib,jb] = sum_{kb >= max(ib,jb)} X[kb,ib]^T X[kb,jb]
-__global__ void k_gram(int n, const double* __restrict__ X, double* __restrict__ Einv, int nblk) {
-    __shared__ double P[kTile][kTile + 1];
-    __shared__ double Q[kTile][kTile + 1];
-    const int ib = blockIdx.y, jb = blockIdx.x;
-    const int r0 = ib * kTile, s0 = jb * kTile;
-    const int mr = min(kTile, n - r0), ms = min(kTile, n - s0);
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    double acc = 0.0;
-    for (int kb = max(ib, jb); kb < nblk; ++kb) {
-        const int k0 = kb * kTile, mk = min(kTile, n - k0);
-        __syncthreads();
-        P[ty][tx] = (ty < mk && tx < mr) ? X[(int64_t)(k0 + ty) * n + r0 + tx] : 0.0;
-        Q[ty][tx] = (ty < mk && tx < ms) ? X[(int64_t)(k0 + ty) * n + s0 + tx] : 0.0;
-        __syncthreads();
-        for (int k = 0; k < mk; ++k) acc += P[k][ty] * Q[k][tx];
-    }
-    if (ty < mr && tx < ms) Einv[(int64_t)(r0 + ty) * n + s0 + tx] = acc;
+// Einv = X^T X for X = L^-1 (lower): Einv[i,j] = sum_{k >= max(i,j)} X[k,i]^T X[k,j]
+__global__ void __launch_bounds__(256) k_gram(int n, int nblk, const double* __restrict__ X,
+                                             double* __restrict__ Einv) {
+    const int i = blockIdx.y, j = blockIdx.x;
+    tile_gemm<1, 0>(n, X, X, Einv, i, j, max(i, j), nblk, 1.0, 0.0);
 }
 
 // ---- per-iteration kernels ----------------------------------------------------------------
@@ -567,18 +646,39 @@ __global__ void k_restrict_sum(CoarseView cv, int split, const double* __restric
     }
 }
 
-// yc = Einv rc (warp per row)
-__global__ void k_coarse_gemv(int n, const double* __restrict__ Einv, const double* __restrict__ rc,
-                              double* __restrict__ yc, const PcgScalars* S) {
+// out = M in for a triangular M (warp per row): LOWER uses columns <= row, else >= row.
+// The coarse solve is y = U (X r) with X = L^-1 and U = X^T (E^-1 = X^T X).
+template <bool LOWER>
+__global__ void k_coarse_trmv(int n, const double* __restrict__ M, const double* __restrict__ in,
+                              double* __restrict__ out, const PcgScalars* S) {
     if (S && S->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
+        const int c0 = LOWER ? 0 : row, c1 = LOWER ? row + 1 : n;
         double s = 0.0;
-        for (int c = lane; c < n; c += 32) s += Einv[(int64_t)row * n + c] * rc[c];
+        for (int c = c0 + lane; c < c1; c += 32) s += M[(int64_t)row * n + c] * in[c];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) yc[row] = s;
+        if (lane == 0) out[row] = s;
     }
 }
+
+// U = X^T on and above the diagonal (32 x 32 tiles through shared memory)
+__global__ void k_transpose_upper(int n, const double* __restrict__ X, double* __restrict__ U) {
+    __shared__ double t[32][33];
+    const int bi = blockIdx.y, bj = blockIdx.x;  // output tile (bi, bj) of U, bj >= bi
+    if (bj < bi) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const int gr = bj * 32 + r, gc = bi * 32 + tx;  // X row block bj, column block bi
+        t[r][tx] = (gr < n && gc < n) ? X[(int64_t)gr * n + gc] : 0.0;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int gr = bi * 32 + r, gc = bj * 32 + tx;
+        if (gr < n && gc < n) U[(int64_t)gr * n + gc] = t[tx][r];
+    }
+}
+
 
 // y[(p,d)] (+)= yscale[(p,d)] m_(p,d) sum_J phi_J(x_p) yc[(J,d)]  (yscale may be NULL: 1)
 __global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ coords, const uint8_t* __restrict__ mask,
@@ -690,8 +790,8 @@ int coarse_setup_mesh(plato_problem* h) {
     PLATO_CUDA(h, cudaMalloc(&c.Einv, sizeof(double) * nn));
     PLATO_CUDA(h, cudaMalloc(&c.X, sizeof(double) * nn));
     PLATO_CUDA(h, cudaMalloc(&c.T, sizeof(double) * nn));
-    const int nblk = (c.ndof + kTile - 1) / kTile;
-    PLATO_CUDA(h, cudaMalloc(&c.Dt, sizeof(double) * size_t(nblk) * kTile * kTile));
+    const int nblk = (c.ndof + kNB - 1) / kNB;
+    PLATO_CUDA(h, cudaMalloc(&c.Dt, sizeof(double) * size_t(nblk) * kNB * kNB));
     // splits of each coarse cell's node / element lists so that the restriction and the
     // Galerkin sum run about 8 CTAs per SM
     c.rsplit = clampi((148 * 8 + c.ncells - 1) / c.ncells, 1, 64);
@@ -699,6 +799,7 @@ int coarse_setup_mesh(plato_problem* h) {
     PLATO_CUDA(h, cudaMalloc(&c.rpart, sizeof(double) * 24 * c.ncells * c.rsplit));
     PLATO_CUDA(h, cudaMalloc(&c.rc, sizeof(double) * c.ndof));
     PLATO_CUDA(h, cudaMalloc(&c.yc, sizeof(double) * c.ndof));
+    PLATO_CUDA(h, cudaMalloc(&c.tc, sizeof(double) * c.ndof));
     PLATO_CUDA(h, cudaMalloc(&c.flag, sizeof(int32_t)));
     c.ready = 1;
     return PLATO_OK;
@@ -708,7 +809,7 @@ void coarse_release(plato_problem* h) {
     CoarseSpace& c = h->coarse;
     for (int32_t** p : {&c.node_ptr, &c.node_list, &c.elem_ptr, &c.elem_list, &c.flag})
         if (*p) { cudaFree(*p); *p = nullptr; }
-    for (double** p : {&c.E, &c.Einv, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.rpart})
+    for (double** p : {&c.E, &c.Einv, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.tc, &c.rpart})
         if (*p) { cudaFree(*p); *p = nullptr; }
     c.ready = 0;
 }
@@ -737,31 +838,38 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     PLATO_LAUNCH_CHECK(h);
     if (E_copy) PLATO_CUDA(h, cudaMemcpyAsync(E_copy, c.E, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
     PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
-    const int nblk = (n + kTile - 1) / kTile;
-    const dim3 tb(kTile, kTile);
-    // X = L^-1 and the inverse diagonal tiles D (scratch allocated with the coarse grid)
-    double *X = c.X, *D = c.Dt;
+    const int nblk = (n + kNB - 1) / kNB;
+    double *X = c.X, *D = c.Dt, *Tmp = c.T;  // scratch allocated with the coarse grid
+    static std::once_flag tiles_once;
+    cudaError_t attr2 = cudaSuccess;
+    std::call_once(tiles_once, [&] {
+        attr2 = cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTwoTiles));
+        if (attr2 == cudaSuccess)
+            attr2 = cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTwoTiles));
+    });
+    PLATO_CUDA(h, attr2);
     for (int kb = 0; kb < nblk; ++kb) {
-        k_chol_diag<<<1, tb, 0, s>>>(n, c.E, kb, D, c.flag);
+        k_chol_diag<<<1, 256, kTwoTiles, s>>>(n, c.E, kb, D, c.flag);
         const int rem = nblk - kb - 1;
         if (rem > 0) {
-            k_chol_panel<<<rem, tb, 0, s>>>(n, c.E, kb, D);
-            k_chol_update<<<rem * (rem + 1) / 2, tb, 0, s>>>(n, c.E, kb, nblk);
+            k_chol_panel<<<rem, 256, kTwoTiles, s>>>(n, c.E, kb, D);
+            k_chol_update<<<rem * (rem + 1) / 2, 256, 0, s>>>(n, c.E, kb, nblk);
         }
     }
     h->launches += 3 * nblk;
     PLATO_LAUNCH_CHECK(h);
-    double* Tmp = c.T;
-    k_tri_init<<<dim3(nblk, nblk), tb, 0, s>>>(n, nblk, D, X);
+    k_tri_init<<<grid_for(int64_t(n) * n, 256, 148 * 16), 256, 0, s>>>(n, D, X);
     PLATO_LAUNCH_CHECK(h);
     for (int lv = 1; lv < nblk; lv *= 2) {
         const int pairs = (nblk + 2 * lv - 1) / (2 * lv);
-        k_tri_level<<<pairs * lv * lv, tb, 0, s>>>(n, nblk, lv, 0, c.E, X, Tmp);
-        k_tri_level<<<pairs * lv * lv, tb, 0, s>>>(n, nblk, lv, 1, c.E, X, Tmp);
+        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 0, c.E, X, Tmp);
+        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 1, c.E, X, Tmp);
         h->launches += 1;
         PLATO_LAUNCH_CHECK(h);
     }
-    k_gram<<<dim3(nblk, nblk), tb, 0, s>>>(n, X, c.Einv, nblk);
+    // the coarse solve applies X then X^T: keep U = X^T (upper) in the Einv buffer
+    const int nt = (n + 31) / 32;
+    k_transpose_upper<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, X, c.Einv);
     PLATO_LAUNCH_CHECK(h);
     int32_t bad = 0;
     PLATO_CUDA(h, cudaMemcpyAsync(&bad, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -779,9 +887,11 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
     k_restrict_cells<<<c.ncells * c.rsplit, kThreadsPerCta, 0, s>>>(cv, c.rsplit, c.node_ptr, c.node_list, h->coords,
                                                                       h->bc_mask, v, sq, c.rpart, S);
     k_restrict_sum<<<grid_for(c.ndof, 256), 256, 0, s>>>(cv, c.rsplit, c.rpart, c.rc, S);
-    k_coarse_gemv<<<grid_for(int64_t(c.ndof) * 32, 256, 148 * 8), 256, 0, s>>>(c.ndof, c.Einv, c.rc, c.yc, S);
+    const int GB = grid_for(int64_t(c.ndof) * 32, 256, 148 * 8);
+    k_coarse_trmv<true><<<GB, 256, 0, s>>>(c.ndof, c.X, c.rc, c.tc, S);
+    k_coarse_trmv<false><<<GB, 256, 0, s>>>(c.ndof, c.Einv, c.tc, c.yc, S);
     k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, sq, y, accumulate, S);
-    h->launches += 3;
+    h->launches += 4;
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }
@@ -802,8 +912,12 @@ extern "C" int plato_coarse_operator(plato_problem* h, const double* z, int32_t*
     PLATO_CUDA(h, cudaMalloc(&Ed, sizeof(double) * nn));
     rc = coarse_setup_operator(h, z, Ed);
     if (!rc && E) rc = cudaMemcpy(E, Ed, sizeof(double) * nn, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : PLATO_CUDA_ERROR;
-    if (!rc && Einv)
-        rc = cudaMemcpy(Einv, h->coarse.Einv, sizeof(double) * nn, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : PLATO_CUDA_ERROR;
+    if (!rc && Einv) {  // E^-1 = X^T X, formed here only (the solver applies X and X^T)
+        const int nblk = (h->coarse.ndof + kNB - 1) / kNB;
+        k_gram<<<dim3(nblk, nblk), 256, 0, h->stream>>>(h->coarse.ndof, nblk, h->coarse.X, h->coarse.T);
+        rc = cudaGetLastError() == cudaSuccess ? 0 : PLATO_CUDA_ERROR;
+        if (!rc) rc = cudaMemcpy(Einv, h->coarse.T, sizeof(double) * nn, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : PLATO_CUDA_ERROR;
+    }
     cudaFree(Ed);
     return rc;
 }

@@ -67,14 +67,19 @@ struct PcgScalars {
 // Every iteration enqueued after convergence still launches its kernels (they return at
 // once), so near the end the chunks shrink to what the observed residual decay predicts:
 // polled state s (its iteration count and r.r), `in_flight` iterations already queued
-// behind it.  Early or irregular decay keeps the full chunk.
+// behind it; the first poll measures the decay from b.b (the start from x0 = 0; a better
+// initial guess only makes the estimate conservative).  Irregular decay keeps the full chunk.
 struct ChunkPlanner {
     int32_t full = 16;
     int32_t last_iter = -1;
     double  last_rr = 0.0;
     int32_t next(const PcgScalars& st, int32_t in_flight) {
         int32_t size = full;
-        if (last_iter >= 0 && st.iter > last_iter && st.rr > 0.0 && last_rr > 0.0 && st.tol2 > 0.0) {
+        if (last_iter < 0) {  // first poll: measure the decay from the start, r.r = b.b for x0 = 0
+            last_iter = 0;
+            last_rr = st.bb;
+        }
+        if (st.iter > last_iter && st.rr > 0.0 && last_rr > 0.0 && st.tol2 > 0.0) {
             const double rate = std::pow(st.rr / last_rr, 1.0 / double(st.iter - last_iter));
             if (rate > 0.0 && rate < 0.999) {
                 const double left = std::log(st.tol2 / st.rr) / std::log(rate);  // iterations still needed
@@ -138,7 +143,7 @@ struct CoarseSpace {
     int32_t* elem_ptr = nullptr;  // elements bucketed by coarse cell (CSR)
     int32_t* elem_list = nullptr;
     double*  E = nullptr;         // Galerkin operator, then its Cholesky factor (ndof^2)
-    double*  Einv = nullptr;      // explicit inverse (ndof^2)
+    double*  Einv = nullptr;      // U = (L^-1)^T, upper (ndof^2); E^-1 = U L^-1
     double*  X = nullptr;         // L^-1 while inverting (ndof^2)
     double*  T = nullptr;         // tile-product scratch of the inversion (ndof^2)
     double*  Dt = nullptr;        // inverse diagonal tiles of the Cholesky factor
@@ -146,6 +151,7 @@ struct CoarseSpace {
     double*  rpart = nullptr;     // restriction partial sums (ncells * rsplit * 24)
     double*  rc = nullptr;        // restricted residual
     double*  yc = nullptr;        // coarse correction
+    double*  tc = nullptr;        // L^-1 rc
     int32_t* flag = nullptr;
 };
 

@@ -22,10 +22,10 @@ def main(argv=None) -> int:
     import torch
 
     from .problem import EllipticProblem
-    from .workloads import SEED_LARGE, cantilever, method_options, splitmix_uniform
+    from .workloads import SEED_LARGE, cantilever, coarse_grid, method_options, splitmix_uniform
 
     nx, ny, nz = (int(v) for v in a.cells.split(","))
-    spec = cantilever(nx, ny, nz, method_options(a.method, a.tol))
+    spec = cantilever(nx, ny, nz, method_options(a.method, a.tol, coarse_grid(nx, ny, nz)))
     z = splitmix_uniform(spec.coords.shape[0], SEED_LARGE)
     prob = EllipticProblem(spec)
     zd = prob.to_dev(z)

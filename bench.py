@@ -561,6 +561,17 @@ def main():
                   "frac": asm_bytes / (asm_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
                   "algorithmic_bytes": asm_bytes, "avg_launch_ms": asm_ms, "launches_timed": inst["assembly_timed"]}
 
+    # two-level coarse operator, once per solve: the Galerkin product P^T A P and the dense FP64
+    # Cholesky + L^-1 (n^3/3 flops each for the n coarse dofs; FP64 mma.sync tiles)
+    coarse = None
+    if inst["coarse_galerkin_timed"]:
+        nc = 3 * int(np.prod([c + 1 for c in spec.solver.coarse_cells]))
+        inv_ms = inst["coarse_inverse_ms_total"] / inst["coarse_galerkin_timed"]
+        flops = 2.0 * nc ** 3 / 3.0
+        coarse = {"coarse_dofs": nc, "galerkin_ms": inst["coarse_galerkin_ms_total"] / inst["coarse_galerkin_timed"],
+                  "inverse_ms": inv_ms, "inverse_flops": flops, "inverse_tflops": flops / (inv_ms / 1e3) / 1e12,
+                  "setups_timed": inst["coarse_galerkin_timed"]}
+
     # the plain FP64 GPU method on the same problem, same run (comparison only)
     plain = None
     if args.method != "plain":
@@ -600,7 +611,8 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"plain": "f64", "bf16": "f64+bf16", "two-level-fp16": "f64+f32+f16"}.get(args.method, "f64+f32"),
             "data": "synthetic", "config": cfg, "accuracy": accuracy, "roofline": roofline,
-            "roofline_fp64_spmv": roofline_other, "roofline_assembly": rl_asm, "cpu_baseline": cpu,
+            "roofline_fp64_spmv": roofline_other, "roofline_assembly": rl_asm, "coarse_setup": coarse,
+            "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N,
                     "d2h_bytes_per_step": 8 * (3 * N + N) + 8},
             "gpu_launches": inst["launches"], "clocks": clk.summary()}

@@ -151,7 +151,9 @@ int plato_reset_instrumentation(plato_problem* h);
 /* Sampled CUDA-event time of one kernel class inside the solvers: kind 0 = the FP64 operator
  * apply of the Krylov loop, kind 1 = the first Chebyshev step of the low-precision
  * preconditioner (one step = one preconditioner-operator apply fused with its update),
- * kind 2 = the Jacobian assembly of each assembled solve. */
+ * kind 2 = the Jacobian assembly of each assembled solve, kind 3 = the Galerkin product of
+ * the two-level coarse operator, kind 4 = its dense factorization and inverse (kinds 3 and 4
+ * count coarse operator set-ups). */
 int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
 
 /* ---- block pattern ---------------------------------------------------------------------

@@ -135,6 +135,8 @@ int plato_destroy(plato_problem* h) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : h->asm_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->coarse_ev)
+        if (e) cudaEventDestroy(e);
     coarse_release(h);
     batch_release(h);
     if (h->ritz_scratch) cudaFree(h->ritz_scratch);
@@ -315,6 +317,8 @@ int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_tot
     if (kind == 0) { *ms_total = h->op_ms_total; *count = h->op_timed; }
     else if (kind == 1) { *ms_total = h->inner_ms_total; *count = h->inner_timed; }
     else if (kind == 2) { *ms_total = h->asm_ms_total; *count = h->asm_timed; }
+    else if (kind == 3) { *ms_total = h->coarse_gal_ms; *count = h->coarse_timed; }
+    else if (kind == 4) { *ms_total = h->coarse_inv_ms; *count = h->coarse_timed; }
     else return PLATO_BAD_INPUT;
     return PLATO_OK;
 }
@@ -328,6 +332,9 @@ int plato_reset_instrumentation(plato_problem* h) {
     h->inner_timed = 0;
     h->asm_ms_total = 0.0;
     h->asm_timed = 0;
+    h->coarse_gal_ms = 0.0;
+    h->coarse_inv_ms = 0.0;
+    h->coarse_timed = 0;
     return PLATO_OK;
 }
 

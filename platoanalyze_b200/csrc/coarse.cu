@@ -353,193 +353,298 @@ __global__ void k_regularize(int n, double* __restrict__ E) {
 // ---- dense SPD inverse: blocked Cholesky and L^-1 by doubling, 64 x 64 tiles -------------
 // E (n x n, row-major, stride n) is factored in place (lower), each diagonal tile's inverse
 // kept in D; then X = L^-1 by doubling and E^-1 = X^T X.  Every bulk step is a product of
-// 64 x 64 tiles (`tile_gemm`: 256 threads, 4 x 4 outputs each, operands staged 16 columns at a
-// time), so the O(n^3) work runs at tile-GEMM speed and the number of launches grows with n/64.
+// 64 x 64 tiles (`tile_gemm`: 8 warps of FP64 mma.sync m8n8k4, a 32 x 16 block per warp,
+// operands staged 16 columns at a time through two shared-memory buffers), so the O(n^3)
+// work runs at tile-GEMM speed and the number of launches grows with n/64.
 
 constexpr int kNB = 64;   // tile edge
 constexpr int kKB = 16;   // k columns staged per pass
+constexpr int kRowPad = kKB + 4;  // [row][k] staging stride: 4 (mod 16) doubles, conflict-free fragments
+constexpr int kColPad = kNB + 4;  // [k][row] staging stride: 4 (mod 16) doubles
+constexpr int kStage = kNB * kRowPad;  // doubles per staged operand (>= kKB * kColPad)
+
+__device__ __forceinline__ void mma_f64(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
 
 // C(ti,tj) = beta C + alpha sum_{kt in [k0,k1)} opA(ti,kt) opB(kt,tj), tiles of kNB; opA(ti,kt)
 // is A's tile (ti,kt), or the transpose of its tile (kt,ti) with TA; opB likewise with TB.
-// Entries outside n read as 0 and are not stored.
+// Entries outside n read as 0 and are not stored.  Each operand is staged in the layout its
+// global reads are contiguous in: [row][k] (stride kRowPad) for a row-major A or a transposed
+// B, [k][row] (stride kColPad) otherwise; both strides keep the m8n8k4 fragment reads (lane
+// l: row l/4, k l%4) on distinct banks.
 template <int TA, int TB>
 __device__ __forceinline__ void tile_gemm(int n, const double* __restrict__ A, const double* __restrict__ B,
                                           double* __restrict__ C, int ti, int tj, int k0, int k1, double alpha,
                                           double beta) {
-    __shared__ double As[kKB][kNB + 1];  // As[k][row]
-    __shared__ double Bs[kKB][kNB + 1];  // Bs[k][col]
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    __shared__ double As[2][kStage];
+    __shared__ double Bs[2][kStage];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;  // warp block: rows wm.., cols wn..
+    const int g = lane >> 2, q = lane & 3;
     const int r0 = ti * kNB, c0 = tj * kNB;
-    double acc[4][4];
+    const int nstage = (k1 - k0) * (kNB / kKB);
+    double acc[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    for (int kt = k0; kt < k1; ++kt) {
-        for (int kk = 0; kk < kNB; kk += kKB) {
-            const int kbase = kt * kNB + kk;
-            __syncthreads();
-            // 1024 values per operand: 4 per thread
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    double ra[4], rb[4];
+    // global -> registers for stage st (1024 values per operand, 4 per thread)
+    auto fetch = [&](int st) {
+        const int kbase = k0 * kNB + st * kKB;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int e = tid + 256 * q;
-                if (TA == 0) {  // A[r0 + row][kbase + c]: c fastest
-                    const int c = e & 15, row = e >> 4;
-                    const int gr = r0 + row, gc = kbase + c;
-                    As[c][row] = (gr < n && gc < n) ? A[(int64_t)gr * n + gc] : 0.0;
-                } else {        // A[kbase + c][r0 + row]: row fastest
-                    const int row = e & 63, c = e >> 6;
-                    const int gr = kbase + c, gc = r0 + row;
-                    As[c][row] = (gr < n && gc < n) ? A[(int64_t)gr * n + gc] : 0.0;
-                }
-                if (TB == 0) {  // B[kbase + c][c0 + col]: col fastest
-                    const int col = e & 63, c = e >> 6;
-                    const int gr = kbase + c, gc = c0 + col;
-                    Bs[c][col] = (gr < n && gc < n) ? B[(int64_t)gr * n + gc] : 0.0;
-                } else {        // B[c0 + col][kbase + c]: c fastest
-                    const int c = e & 15, col = e >> 4;
-                    const int gr = c0 + col, gc = kbase + c;
-                    Bs[c][col] = (gr < n && gc < n) ? B[(int64_t)gr * n + gc] : 0.0;
-                }
+        for (int u = 0; u < 4; ++u) {
+            const int e = tid + 256 * u;
+            if (TA == 0) {  // A[r0 + row][kbase + c]: c fastest
+                const int c = e & 15, row = e >> 4, gr = r0 + row, gc = kbase + c;
+                ra[u] = (gr < n && gc < n) ? A[(int64_t)gr * n + gc] : 0.0;
+            } else {        // A[kbase + c][r0 + row]: row fastest
+                const int row = e & 63, c = e >> 6, gr = kbase + c, gc = r0 + row;
+                ra[u] = (gr < n && gc < n) ? A[(int64_t)gr * n + gc] : 0.0;
             }
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < kKB; ++k) {
-                double a[4], b[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+            if (TB == 0) {  // B[kbase + c][c0 + col]: col fastest
+                const int col = e & 63, c = e >> 6, gr = kbase + c, gc = c0 + col;
+                rb[u] = (gr < n && gc < n) ? B[(int64_t)gr * n + gc] : 0.0;
+            } else {        // B[c0 + col][kbase + c]: c fastest
+                const int c = e & 15, col = e >> 4, gr = c0 + col, gc = kbase + c;
+                rb[u] = (gr < n && gc < n) ? B[(int64_t)gr * n + gc] : 0.0;
             }
         }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = tid + 256 * u;
+            if (TA == 0) As[buf][(e >> 4) * kRowPad + (e & 15)] = ra[u];
+            else As[buf][(e >> 6) * kColPad + (e & 63)] = ra[u];
+            if (TB == 0) Bs[buf][(e >> 6) * kColPad + (e & 63)] = rb[u];
+            else Bs[buf][(e >> 4) * kRowPad + (e & 15)] = rb[u];
+        }
+    };
+    // C's old values (beta != 0) are loaded all at once before the epilogue's stores: one
+    // round trip per CTA instead of one per read-modify-write
+    double cold[4][2][2];
+    auto fetch_c = [&]() {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int gr = r0 + wm + 8 * i + g;
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const int gc = c0 + wn + 8 * j + 2 * q + t;
+                    cold[i][j][t] = (beta != 0.0 && gr < n && gc < n) ? C[(int64_t)gr * n + gc] : 0.0;
+                }
+        }
+    };
+    fetch(0);
+    store(0);
+    __syncthreads();
+    for (int st = 0; st < nstage; ++st) {
+        const int buf = st & 1;
+        if (st + 1 < nstage) fetch(st + 1);  // in flight during the products below
+        const double* as = As[buf];
+        const double* bs = Bs[buf];
+#pragma unroll
+        for (int k4 = 0; k4 < kKB; k4 += 4) {
+            const int k = k4 + q;
+            double a[4], b[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int row = wm + 8 * i + g;
+                a[i] = TA == 0 ? as[row * kRowPad + k] : as[k * kColPad + row];
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int col = wn + 8 * j + g;
+                b[j] = TB == 0 ? bs[k * kColPad + col] : bs[col * kRowPad + k];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) mma_f64(acc[i][j], a[i], b[j]);
+        }
+        if (st + 1 < nstage) store(buf ^ 1);  // that buffer was last read before the previous barrier
+        __syncthreads();
     }
+    fetch_c();
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int gr = r0 + ty + 16 * i;
+        const int gr = r0 + wm + 8 * i + g;
         if (gr >= n) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gc = c0 + tx + 16 * j;
-            if (gc >= n) continue;
-            double* cp = C + (int64_t)gr * n + gc;
-            *cp = (beta == 0.0 ? 0.0 : beta * *cp) + alpha * acc[i][j];
-        }
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int gc = c0 + wn + 8 * j + 2 * q + t;
+                if (gc < n) C[(int64_t)gr * n + gc] = beta * cold[i][j][t] + alpha * acc[i][j][t];
+            }
     }
 }
 
 // Factors diagonal tile kb in place (lower, zeros above) and writes its inverse to D[kb]
-// (kNB x kNB, row-major).  One CTA of 256 threads.
-constexpr size_t kTwoTiles = sizeof(double) * 2 * kNB * (kNB + 1);  // dynamic shared memory of the next two
+// (kNB x kNB, row-major).  One CTA of 1024 threads: the 64 pivot steps are a serial chain,
+// so each step gives every thread at most four entries and 8 warps per scheduler to hide
+// the shared-memory and FP64 latencies between barriers.
+constexpr int kDiagThreads = 1024;
+constexpr size_t kTwoTiles = sizeof(double) * 2 * kNB * (kNB + 1);  // dynamic shared memory of k_chol_diag
 
-__global__ void __launch_bounds__(256) k_chol_diag(int n, double* __restrict__ A, int kb, double* __restrict__ D,
-                                                  int32_t* __restrict__ bad) {
+__global__ void __launch_bounds__(kDiagThreads) k_chol_diag(int n, double* __restrict__ A, int kb,
+                                                           double* __restrict__ D, int32_t* __restrict__ bad) {
     extern __shared__ double dyn[];
     double (*T)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn);
     double (*W)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn + kNB * (kNB + 1));
+    __shared__ double piv[kNB], pinv[kNB], rsq[kNB];
     const int r0 = kb * kNB, m = min(kNB, n - r0);
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    for (int e = tid; e < kNB * kNB; e += 256) {
-        const int i = e >> 6, j = e & 63;
-        T[i][j] = (i < m && j < m) ? A[(int64_t)(r0 + i) * n + r0 + j] : (i == j ? 1.0 : 0.0);
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    {
+        double v[kNB * kNB / kDiagThreads];
+#pragma unroll
+        for (int u = 0; u < kNB * kNB / kDiagThreads; ++u) {
+            const int e = tid + kDiagThreads * u, i = e >> 6, j = e & 63;
+            v[u] = (i < m && j < m) ? A[(int64_t)(r0 + i) * n + r0 + j] : (i == j ? 1.0 : 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kNB * kNB / kDiagThreads; ++u) {
+            const int e = tid + kDiagThreads * u, i = e >> 6, j = e & 63;
+            T[i][j] = v[u];
+            W[i][j] = (i == j) ? 1.0 : 0.0;
+            if (e == 0) {  // the first pivot; later ones come from the thread that finishes them
+                const double d = (v[u] > 0.0) ? v[u] : 1.0;
+                if (!(v[u] > 0.0)) atomicExch(bad, 1);
+                piv[0] = d;
+                pinv[0] = 1.0 / d;
+            }
+        }
     }
     __syncthreads();
-    // right-looking: thread (ty, tx) owns rows ty + 16a and columns tx + 16b of the tile
+    // Unscaled (LDL^T-form) elimination, one barrier per pivot: with d_k = T[k][k],
+    //   T[i][j] -= T[i][k] T[j][k] / d_k   (k < j <= i)   -> Schur complements, column k kept
+    //   W[i][j] -= T[i][k] W[k][j] / d_k   (j <= k < i)   -> W = L1^-1, L1 the unit factor
+    // Step k reads only column k of T and row k of W and writes neither, so the steps need no
+    // barrier inside.  Afterwards L[i][j] = T[i][j] / sqrt(d_j) and L^-1[i][j] = W[i][j] / sqrt(d_i).
+    // Thread (ty, tx) owns rows ty, ty + 32 and columns tx, tx + 32 of the tile; the owner of
+    // entry (k+1, k+1) finishes that pivot in step k and leaves d and 1/d for step k + 1, so the
+    // division is off the other threads' path.
     for (int k = 0; k < m; ++k) {
-        if (tid == 0) {
-            const double d = T[k][k];
-            if (!(d > 0.0)) { atomicExch(bad, 1); T[k][k] = 1.0; }
-            else T[k][k] = sqrt(d);
-        }
-        __syncthreads();
-        if (tid > k && tid < m) T[tid][k] /= T[k][k];
-        __syncthreads();
+        const double inv = pinv[k];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = ty + 16 * a;
+        for (int a = 0; a < 2; ++a) {
+            const int i = ty + 32 * a;
             if (i <= k || i >= m) continue;
-            const double tik = T[i][k];
+            const double c = T[i][k] * inv;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int j = tx + 16 * b;
-                if (j > k && j <= i) T[i][j] -= tik * T[j][k];
+            for (int b = 0; b < 2; ++b) {
+                const int j = tx + 32 * b;
+                if (j > i) continue;
+                if (j > k) {
+                    const double t = T[i][j] - c * T[j][k];
+                    T[i][j] = t;
+                    if (j == k + 1 && i == k + 1) {
+                        const double d = (t > 0.0) ? t : 1.0;
+                        if (!(t > 0.0)) atomicExch(bad, 1);
+                        piv[k + 1] = d;
+                        pinv[k + 1] = 1.0 / d;
+                    }
+                } else {
+                    W[i][j] -= c * W[k][j];
+                }
             }
         }
         __syncthreads();
     }
-    // W = L^-1, thread j < m forms column j top-down; all threads read the same T[i][k]
-    if (tid < kNB) {
-        const int j = tid;
-        for (int i = 0; i < kNB; ++i) {
-            double v = 0.0;
-            if (i >= j && i < m) {
-                double s2 = (i == j) ? 1.0 : 0.0;
-                for (int k = j; k < i; ++k) s2 -= T[i][k] * W[k][j];
-                v = s2 / T[i][i];
-            }
-            W[i][j] = v;
-        }
-    }
+    if (tid < m) rsq[tid] = 1.0 / sqrt(piv[tid]);
     __syncthreads();
-    for (int e = tid; e < kNB * kNB; e += 256) {
+    for (int e = tid; e < kNB * kNB; e += kDiagThreads) {
         const int i = e >> 6, j = e & 63;
-        if (i < m && j < m) A[(int64_t)(r0 + i) * n + r0 + j] = (j <= i) ? T[i][j] : 0.0;
-        D[(int64_t)kb * kNB * kNB + e] = (i < m && j < m && j <= i) ? W[i][j] : 0.0;
+        if (i < m && j < m)
+            A[(int64_t)(r0 + i) * n + r0 + j] = (j < i) ? T[i][j] * rsq[j] : (j == i ? sqrt(piv[i]) : 0.0);
+        D[(int64_t)kb * kNB * kNB + e] = (i < m && j < m && j <= i) ? W[i][j] * rsq[i] : 0.0;
     }
 }
 
-// Panel: A[ib,kb] <- A[ib,kb] L_kk^-T for every tile row ib > kb (one CTA per tile row).
+// Panel: A[ib,kb] <- A[ib,kb] L_kk^-T for every tile row ib > kb (one CTA per tile row): both
+// 64 x 64 operands staged whole ([row][k], stride kColPad), then the FP64 mma.sync product
+// (P L^-T)[i][j] = sum_k P[i][k] Linv[j][k] with the warp blocks of `tile_gemm`.
+constexpr size_t kPanelSmem = sizeof(double) * 2 * kNB * kColPad;
+
 __global__ void __launch_bounds__(256) k_chol_panel(int n, double* __restrict__ A, int kb,
                                                    const double* __restrict__ D) {
     extern __shared__ double dyn[];
-    double (*Ds)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn);
-    double (*Ps)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn + kNB * (kNB + 1));
+    double* Ps = dyn;
+    double* Ds = dyn + kNB * kColPad;
     const int ib = kb + 1 + blockIdx.x;
     const int r0 = ib * kNB, c0 = kb * kNB;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    for (int e = tid; e < kNB * kNB; e += 256) {
-        const int i = e / kNB, j = e - kNB * i;
-        Ds[i][j] = D[(int64_t)kb * kNB * kNB + e];
-        Ps[i][j] = (r0 + i < n && c0 + j < n) ? A[(int64_t)(r0 + i) * n + c0 + j] : 0.0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    const int g = lane >> 2, q = lane & 3;
+    {   // all 32 loads of a thread in flight at once, then the shared-memory stores
+        double dv[16], pv[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int e = tid + 256 * u, i = e >> 6, j = e & 63;
+            dv[u] = D[(int64_t)kb * kNB * kNB + e];
+            pv[u] = (r0 + i < n && c0 + j < n) ? A[(int64_t)(r0 + i) * n + c0 + j] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int e = tid + 256 * u, i = e >> 6, j = e & 63;
+            Ds[i * kColPad + j] = dv[u];
+            Ps[i * kColPad + j] = pv[u];
+        }
     }
     __syncthreads();
-    // (P L^-T)[i][j] = sum_{k <= j} P[i][k] Linv[j][k]
-    double acc[4][4];
+    double acc[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    for (int k = 0; k < kNB; ++k) {
-        double a[4], b[4];
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 4
+    for (int k4 = 0; k4 < kNB; k4 += 4) {
+        const int k = k4 + q;
+        double a[4], b[2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = Ps[ty + 16 * i][k];
+        for (int i = 0; i < 4; ++i) a[i] = Ps[(wm + 8 * i + g) * kColPad + k];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = Ds[tx + 16 * j][k];
+        for (int j = 0; j < 2; ++j) b[j] = Ds[(wn + 8 * j + g) * kColPad + k];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+            for (int j = 0; j < 2; ++j) mma_f64(acc[i][j], a[i], b[j]);
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i) {
+        const int gr = r0 + wm + 8 * i + g;
+        if (gr >= n) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gr = r0 + ty + 16 * i, gc = c0 + tx + 16 * j;
-            if (gr < n && gc < n) A[(int64_t)gr * n + gc] = acc[i][j];
-        }
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int gc = c0 + wn + 8 * j + 2 * q + t;
+                if (gc < n) A[(int64_t)gr * n + gc] = acc[i][j][t];
+            }
+    }
 }
 
-// Trailing update A[ib,jb] -= A[ib,kb] A[jb,kb]^T for kb < jb <= ib (blockIdx enumerates the
-// lower triangle of the trailing tiles).
+// Trailing update A[ib,jb] -= A[ib,kb] A[jb,kb]^T.  COL: the next tile column jb = kb + 1
+// (one CTA per tile, ib > kb); otherwise the tiles kb + 2 <= jb <= ib (blockIdx enumerates
+// that lower triangle).
+template <bool COL>
 __global__ void __launch_bounds__(256) k_chol_update(int n, double* __restrict__ A, int kb, int nblk) {
-    const int rem = nblk - kb - 1;
-    int idx = blockIdx.x, ib = 0;
-    while (idx >= ib + 1) { idx -= ib + 1; ++ib; }
-    if (ib >= rem) return;
-    const int gi = kb + 1 + ib, gj = kb + 1 + idx;
+    int gi, gj;
+    if (COL) {
+        gi = kb + 1 + blockIdx.x;
+        gj = kb + 1;
+    } else {
+        int idx = blockIdx.x, ib = 0;
+        while (idx >= ib + 1) { idx -= ib + 1; ++ib; }
+        gi = kb + 2 + ib;
+        gj = kb + 2 + idx;
+    }
+    if (gi >= nblk) return;
     tile_gemm<0, 1>(n, A, A, A, gi, gj, kb, kb + 1, -1.0, 1.0);
 }
 
@@ -811,6 +916,9 @@ void coarse_release(plato_problem* h) {
         if (*p) { cudaFree(*p); *p = nullptr; }
     for (double** p : {&c.E, &c.Einv, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.tc, &c.rpart})
         if (*p) { cudaFree(*p); *p = nullptr; }
+    for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
+        if (*e) { cudaEventDestroy(*e); *e = nullptr; }
+    if (c.side) { cudaStreamDestroy(c.side); c.side = nullptr; }
     c.ready = 0;
 }
 
@@ -821,6 +929,11 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     cudaStream_t s = h->stream;
     const int n = c.ndof;
     const size_t nn = size_t(n) * n;
+    if (h->timing) {
+        for (cudaEvent_t& e : h->coarse_ev)
+            if (!e) PLATO_CUDA(h, cudaEventCreate(&e));
+        PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[0], s));
+    }
     PLATO_CUDA(h, cudaMemsetAsync(c.E, 0, sizeof(double) * nn, s));
     static std::once_flag smem_once;  // per kernel and process; a driver round trip per call otherwise
     cudaError_t attr = cudaSuccess;
@@ -836,6 +949,7 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     PLATO_LAUNCH_CHECK(h);
     k_regularize<<<grid_for(n, 256), 256, 0, s>>>(n, c.E);
     PLATO_LAUNCH_CHECK(h);
+    if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[1], s));
     if (E_copy) PLATO_CUDA(h, cudaMemcpyAsync(E_copy, c.E, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
     PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
     const int nblk = (n + kNB - 1) / kNB;
@@ -845,18 +959,40 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     std::call_once(tiles_once, [&] {
         attr2 = cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTwoTiles));
         if (attr2 == cudaSuccess)
-            attr2 = cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTwoTiles));
+            attr2 = cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPanelSmem));
     });
     PLATO_CUDA(h, attr2);
+    if (!c.side) PLATO_CUDA(h, cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
+        if (!*e) PLATO_CUDA(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    // Right-looking blocked Cholesky with a look-ahead of one tile column.  Step kb on the main
+    // stream: diagonal tile, panel, then the update of column kb + 1 alone, which the next
+    // step's diagonal tile needs; the rest of the trailing update (columns >= kb + 2) runs on
+    // the side stream meanwhile.  The two write disjoint tile columns; the main stream waits
+    // for the side stream's step kb - 1 before it updates column kb + 1 (which that step also
+    // writes), and the side stream starts step kb after panel kb.
+    bool trail_pending = false;
     for (int kb = 0; kb < nblk; ++kb) {
-        k_chol_diag<<<1, 256, kTwoTiles, s>>>(n, c.E, kb, D, c.flag);
+        k_chol_diag<<<1, kDiagThreads, kTwoTiles, s>>>(n, c.E, kb, D, c.flag);
+        h->launches += 1;
         const int rem = nblk - kb - 1;
-        if (rem > 0) {
-            k_chol_panel<<<rem, 256, kTwoTiles, s>>>(n, c.E, kb, D);
-            k_chol_update<<<rem * (rem + 1) / 2, 256, 0, s>>>(n, c.E, kb, nblk);
+        if (rem == 0) break;
+        k_chol_panel<<<rem, 256, kPanelSmem, s>>>(n, c.E, kb, D);
+        h->launches += 1;
+        if (trail_pending) PLATO_CUDA(h, cudaStreamWaitEvent(s, c.ev_trail, 0));
+        trail_pending = false;
+        if (rem > 1) {
+            PLATO_CUDA(h, cudaEventRecord(c.ev_panel, s));
+            PLATO_CUDA(h, cudaStreamWaitEvent(c.side, c.ev_panel, 0));
+            k_chol_update<false><<<(rem - 1) * rem / 2, 256, 0, c.side>>>(n, c.E, kb, nblk);
+            PLATO_CUDA(h, cudaEventRecord(c.ev_trail, c.side));
+            trail_pending = true;
+            h->launches += 1;
         }
+        k_chol_update<true><<<rem, 256, 0, s>>>(n, c.E, kb, nblk);
+        h->launches += 1;
     }
-    h->launches += 3 * nblk;
+    if (trail_pending) PLATO_CUDA(h, cudaStreamWaitEvent(s, c.ev_trail, 0));
     PLATO_LAUNCH_CHECK(h);
     k_tri_init<<<grid_for(int64_t(n) * n, 256, 148 * 16), 256, 0, s>>>(n, D, X);
     PLATO_LAUNCH_CHECK(h);
@@ -871,9 +1007,18 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     const int nt = (n + 31) / 32;
     k_transpose_upper<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, X, c.Einv);
     PLATO_LAUNCH_CHECK(h);
+    if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[2], s));
     int32_t bad = 0;
     PLATO_CUDA(h, cudaMemcpyAsync(&bad, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));
+    if (h->timing) {
+        float ms[2] = {0.f, 0.f};
+        PLATO_CUDA(h, cudaEventElapsedTime(&ms[0], h->coarse_ev[0], h->coarse_ev[1]));
+        PLATO_CUDA(h, cudaEventElapsedTime(&ms[1], h->coarse_ev[1], h->coarse_ev[2]));
+        h->coarse_gal_ms += ms[0];
+        h->coarse_inv_ms += ms[1];
+        h->coarse_timed += 1;
+    }
     if (bad) return plato_fail(h, PLATO_NONFINITE, "coarse operator is not positive definite");
     return PLATO_OK;
 }

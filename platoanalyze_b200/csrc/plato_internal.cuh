@@ -153,6 +153,8 @@ struct CoarseSpace {
     double*  yc = nullptr;        // coarse correction
     double*  tc = nullptr;        // L^-1 rc
     int32_t* flag = nullptr;
+    cudaStream_t side = nullptr;  // trailing Cholesky updates, overlapped with the next panel
+    cudaEvent_t  ev_panel = nullptr, ev_trail = nullptr;
 };
 
 struct plato_problem {
@@ -255,6 +257,10 @@ struct plato_problem {
     cudaEvent_t asm_ev[2] = {nullptr, nullptr};  // Jacobian assembly of the solve path
     double  asm_ms_total = 0.0;
     int64_t asm_timed = 0;
+    cudaEvent_t coarse_ev[3] = {nullptr, nullptr, nullptr};  // coarse operator: Galerkin | dense inverse
+    double  coarse_gal_ms = 0.0;
+    double  coarse_inv_ms = 0.0;
+    int64_t coarse_timed = 0;
     BatchState batch{};
     // subspace initial guess (ritz.cu): columns set for the duration of one solution call
     const double* ritz_W = nullptr;

@@ -169,7 +169,7 @@ class EllipticProblem:
         n, ms, k = C.c_int64(), C.c_double(), C.c_int64()
         check(lib.plato_get_instrumentation(self.h, C.byref(n), C.byref(ms), C.byref(k)), self.h)
         out = {"launches": n.value, "op_ms_total": ms.value, "op_timed": k.value}
-        for kind, name in ((1, "inner"), (2, "assembly")):
+        for kind, name in ((1, "inner"), (2, "assembly"), (3, "coarse_galerkin"), (4, "coarse_inverse")):
             t, c = C.c_double(), C.c_int64()
             check(lib.plato_get_kernel_timing(self.h, kind, C.byref(t), C.byref(c)), self.h)
             out[name + "_ms_total"], out[name + "_timed"] = t.value, c.value

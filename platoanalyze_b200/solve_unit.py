@@ -1,6 +1,6 @@
 """Run solve+adjoint units of the SIMP cantilever on cuda:0 (for profilers and quick checks).
 
-    python -m platoanalyze_b200.solve_unit --cells 120,60,60 --method two-level [--repeat 1]
+    python -m platoanalyze_b200.solve_unit --cells 120,60,60 --method two-level [--repeat 1] [--coarse 16,8,8]
 
 One unit = Problem::solution (assembly, constraints, solve), compliance and dC/dz
 (self-adjoint), the bench's step.  Densities are nodal i.i.d. U[0.01, 1] from SplitMix64
@@ -17,6 +17,7 @@ def main(argv=None) -> int:
     ap.add_argument("--method", default="two-level")
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--coarse", default=None, help="coarse box cells x,y,z (default: chosen from --cells)")
     a = ap.parse_args(argv)
 
     import torch
@@ -25,7 +26,8 @@ def main(argv=None) -> int:
     from .workloads import SEED_LARGE, cantilever, coarse_grid, method_options, splitmix_uniform
 
     nx, ny, nz = (int(v) for v in a.cells.split(","))
-    spec = cantilever(nx, ny, nz, method_options(a.method, a.tol, coarse_grid(nx, ny, nz)))
+    cg = tuple(int(v) for v in a.coarse.split(",")) if a.coarse else coarse_grid(nx, ny, nz)
+    spec = cantilever(nx, ny, nz, method_options(a.method, a.tol, cg))
     z = splitmix_uniform(spec.coords.shape[0], SEED_LARGE)
     prob = EllipticProblem(spec)
     zd = prob.to_dev(z)

@@ -486,20 +486,30 @@ __device__ __forceinline__ void tile_gemm(int n, const double* __restrict__ A, c
 }
 
 // Factors diagonal tile kb in place (lower, zeros above) and writes its inverse to D[kb]
-// (kNB x kNB, row-major).  One CTA of 1024 threads: the 64 pivot steps are a serial chain,
-// so each step gives every thread at most four entries and 8 warps per scheduler to hide
-// the shared-memory and FP64 latencies between barriers.
-constexpr int kDiagThreads = 1024;
-constexpr size_t kTwoTiles = sizeof(double) * 2 * kNB * (kNB + 1);  // dynamic shared memory of k_chol_diag
+// (kNB x kNB, row-major).  One CTA of 256 threads, blocked by 8: for each 8-column block s,
+//   A: warp 0 factors the 8 x 8 diagonal block (L_ss) and inverts it (Li = L_ss^-1);
+//   B: the block column below, Lp = T[below, s] Li^T, and block row s of L^-1,
+//      Wr = Li R_s (R = the rows of [L | I] still to be eliminated, kept in W);
+//   C: the rank-8 trailing update T -= Lp Lp^T, the row elimination W[below] -= Lp Wr, and
+//      Lp, Wr copied into place.
+// 24 barriers in all; rows and columns past m are an identity block that factors to itself.
+constexpr int kDiagThreads = 256;
+constexpr int kDiagPad = kNB + 1;
+constexpr size_t kDiagSmem = sizeof(double) * (2 * kNB * kDiagPad + kNB * 9 + 8 * kDiagPad + 8 * 9 + 8 * 9);
+constexpr size_t kTwoTiles = kDiagSmem;
 
 __global__ void __launch_bounds__(kDiagThreads) k_chol_diag(int n, double* __restrict__ A, int kb,
                                                            double* __restrict__ D, int32_t* __restrict__ bad) {
     extern __shared__ double dyn[];
-    double (*T)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn);
-    double (*W)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(dyn + kNB * (kNB + 1));
-    __shared__ double piv[kNB], pinv[kNB], rsq[kNB];
+    double (*T)[kDiagPad] = reinterpret_cast<double (*)[kDiagPad]>(dyn);                  // L (lower)
+    double (*W)[kDiagPad] = reinterpret_cast<double (*)[kDiagPad]>(dyn + kNB * kDiagPad);  // L^-1
+    double (*Lp)[9] = reinterpret_cast<double (*)[9]>(dyn + 2 * kNB * kDiagPad);           // block column
+    double (*Wr)[kDiagPad] = reinterpret_cast<double (*)[kDiagPad]>(dyn + 2 * kNB * kDiagPad + kNB * 9);
+    double (*Li)[9] = reinterpret_cast<double (*)[9]>(dyn + 2 * kNB * kDiagPad + kNB * 9 + 8 * kDiagPad);
+    double (*W8)[9] = Li + 8;
     const int r0 = kb * kNB, m = min(kNB, n - r0);
-    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tx = tid & 15, ty = tid >> 4;  // phase C: rows ty + 16a, columns tx + 16b
     {
         double v[kNB * kNB / kDiagThreads];
 #pragma unroll
@@ -512,57 +522,124 @@ __global__ void __launch_bounds__(kDiagThreads) k_chol_diag(int n, double* __res
             const int e = tid + kDiagThreads * u, i = e >> 6, j = e & 63;
             T[i][j] = v[u];
             W[i][j] = (i == j) ? 1.0 : 0.0;
-            if (e == 0) {  // the first pivot; later ones come from the thread that finishes them
-                const double d = (v[u] > 0.0) ? v[u] : 1.0;
-                if (!(v[u] > 0.0)) atomicExch(bad, 1);
-                piv[0] = d;
-                pinv[0] = 1.0 / d;
-            }
         }
     }
     __syncthreads();
-    // Unscaled (LDL^T-form) elimination, one barrier per pivot: with d_k = T[k][k],
-    //   T[i][j] -= T[i][k] T[j][k] / d_k   (k < j <= i)   -> Schur complements, column k kept
-    //   W[i][j] -= T[i][k] W[k][j] / d_k   (j <= k < i)   -> W = L1^-1, L1 the unit factor
-    // Step k reads only column k of T and row k of W and writes neither, so the steps need no
-    // barrier inside.  Afterwards L[i][j] = T[i][j] / sqrt(d_j) and L^-1[i][j] = W[i][j] / sqrt(d_i).
-    // Thread (ty, tx) owns rows ty, ty + 32 and columns tx, tx + 32 of the tile; the owner of
-    // entry (k+1, k+1) finishes that pivot in step k and leaves d and 1/d for step k + 1, so the
-    // division is off the other threads' path.
-    for (int k = 0; k < m; ++k) {
-        const double inv = pinv[k];
+    for (int s = 0; s < kNB / 8; ++s) {
+        const int o = 8 * s, nb = kNB - o - 8;  // block offset, rows below the block
+        // A: unscaled elimination of the 8 x 8 block (lane: row lane/4, columns lane%4 and +4),
+        // W8 = the unit factor's inverse; then L_ss = T D^1/2 and Li = D^-1/2 W8
+        if (warp == 0) {
+            const int r = lane >> 2, c0 = lane & 3;
+            W8[r][c0] = (r == c0) ? 1.0 : 0.0;
+            W8[r][c0 + 4] = (r == c0 + 4) ? 1.0 : 0.0;
+            __syncwarp();
+            for (int k = 0; k < 8; ++k) {
+                double d = T[o + k][o + k];
+                if (!(d > 0.0)) d = 1.0;
+                const double inv = 1.0 / d;
+                if (r > k) {
+                    const double cr = T[o + r][o + k] * inv;
 #pragma unroll
-        for (int a = 0; a < 2; ++a) {
-            const int i = ty + 32 * a;
-            if (i <= k || i >= m) continue;
-            const double c = T[i][k] * inv;
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = c0 + 4 * h;
+                        if (c > k && c <= r) T[o + r][o + c] -= cr * T[o + c][o + k];
+                        else if (c <= k) W8[r][c] -= cr * W8[k][c];
+                    }
+                }
+                __syncwarp();
+            }
+            const double dr = T[o + r][o + r], dc0 = T[o + c0][o + c0], dc1 = T[o + c0 + 4][o + c0 + 4];
+            if (!(dr > 0.0) && c0 == 0) atomicExch(bad, 1);
+            const double sr = sqrt(dr > 0.0 ? dr : 1.0);
+            const double sc[2] = {sqrt(dc0 > 0.0 ? dc0 : 1.0), sqrt(dc1 > 0.0 ? dc1 : 1.0)};
+            __syncwarp();  // every lane has read the pivots before the block is overwritten
 #pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const int j = tx + 32 * b;
-                if (j > i) continue;
-                if (j > k) {
-                    const double t = T[i][j] - c * T[j][k];
-                    T[i][j] = t;
-                    if (j == k + 1 && i == k + 1) {
-                        const double d = (t > 0.0) ? t : 1.0;
-                        if (!(t > 0.0)) atomicExch(bad, 1);
-                        piv[k + 1] = d;
-                        pinv[k + 1] = 1.0 / d;
+            for (int h = 0; h < 2; ++h) {
+                const int c = c0 + 4 * h;
+                Li[r][c] = (c <= r) ? W8[r][c] / sr : 0.0;
+                if (c < r) T[o + r][o + c] /= sc[h];
+                else if (c == r) T[o + r][o + r] = sr;
+            }
+        }
+        __syncthreads();
+        // B: Lp[i][c] = sum_{t <= c} T[o+8+i][o+t] Li[c][t];  Wr[r][j] = sum_{t <= r} Li[r][t] W[o+t][j], j < o+8
+        const int nB1 = nb * 8, nB2 = 8 * (o + 8);
+        for (int e = tid; e < nB1 + nB2; e += kDiagThreads) {
+            if (e < nB1) {
+                const int i = e >> 3, c = e & 7;
+                double acc = 0.0;
+#pragma unroll
+                for (int t = 0; t < 8; ++t)
+                    if (t <= c) acc += T[o + 8 + i][o + t] * Li[c][t];
+                Lp[i][c] = acc;
+            } else {
+                const int f = e - nB1, rr = f / (o + 8), j = f - rr * (o + 8);
+                double acc = 0.0;
+#pragma unroll
+                for (int t = 0; t < 8; ++t)
+                    if (t <= rr) acc += Li[rr][t] * W[o + t][j];
+                Wr[rr][j] = acc;
+            }
+        }
+        __syncthreads();
+        // C: trailing update and row elimination on the owned entries, then the copies
+        if (nb > 0) {
+            double li[4][8];
+            bool ri[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int i = ty + 16 * a;
+                ri[a] = i >= o + 8;
+#pragma unroll
+                for (int t = 0; t < 8; ++t) li[a][t] = ri[a] ? Lp[i - o - 8][t] : 0.0;
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int j = tx + 16 * b;
+                double lj[8];
+                if (j >= o + 8) {
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) lj[t] = Lp[j - o - 8][t];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const int i = ty + 16 * a;
+                        if (!ri[a] || j > i) continue;
+                        double acc = 0.0;
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) acc += li[a][t] * lj[t];
+                        T[i][j] -= acc;
                     }
                 } else {
-                    W[i][j] -= c * W[k][j];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) lj[t] = Wr[t][j];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const int i = ty + 16 * a;
+                        if (!ri[a]) continue;
+                        double acc = 0.0;
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) acc += li[a][t] * lj[t];
+                        W[i][j] -= acc;
+                    }
                 }
+            }
+        }
+        for (int e = tid; e < nB1 + nB2; e += kDiagThreads) {
+            if (e < nB1) {
+                const int i = e >> 3, c = e & 7;
+                T[o + 8 + i][o + c] = Lp[i][c];
+            } else {
+                const int f = e - nB1, rr = f / (o + 8), j = f - rr * (o + 8);
+                W[o + rr][j] = Wr[rr][j];
             }
         }
         __syncthreads();
     }
-    if (tid < m) rsq[tid] = 1.0 / sqrt(piv[tid]);
-    __syncthreads();
     for (int e = tid; e < kNB * kNB; e += kDiagThreads) {
         const int i = e >> 6, j = e & 63;
-        if (i < m && j < m)
-            A[(int64_t)(r0 + i) * n + r0 + j] = (j < i) ? T[i][j] * rsq[j] : (j == i ? sqrt(piv[i]) : 0.0);
-        D[(int64_t)kb * kNB * kNB + e] = (i < m && j < m && j <= i) ? W[i][j] * rsq[i] : 0.0;
+        if (i < m && j < m) A[(int64_t)(r0 + i) * n + r0 + j] = (j <= i) ? T[i][j] : 0.0;
+        D[(int64_t)kb * kNB * kNB + e] = (i < m && j < m && j <= i) ? W[i][j] : 0.0;
     }
 }
 
@@ -751,28 +828,50 @@ __global__ void k_restrict_sum(CoarseView cv, int split, const double* __restric
     }
 }
 
-// out = M in for a triangular M (warp per row): LOWER uses columns <= row, else >= row.
-// The coarse solve is y = U (X r) with X = L^-1 and U = X^T (E^-1 = X^T X).
+// The coarse solve is y = U (X r) with X = L^-1 and U = X^T (E^-1 = X^T X); the factorization
+// and inversion run in FP64, the two products per preconditioner apply read FP32 copies.
+// out = M in for a triangular FP32 matrix (row stride ld, zeros outside the triangle and in
+// the padding columns), FP64 vectors and sums.  A warp per row, 16-byte loads from the row's
+// first 4-aligned column; the in[] reads past n are skipped.
 template <bool LOWER>
-__global__ void k_coarse_trmv(int n, const double* __restrict__ M, const double* __restrict__ in,
-                              double* __restrict__ out, const PcgScalars* S) {
+__global__ void __launch_bounds__(256) k_coarse_trmv(int n, int ld, const float* __restrict__ M,
+                                                     const double* __restrict__ in, double* __restrict__ out,
+                                                     const PcgScalars* S) {
     if (S && S->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
-        const int c0 = LOWER ? 0 : row, c1 = LOWER ? row + 1 : n;
+        const int q0 = LOWER ? 0 : (row >> 2), q1 = LOWER ? (row >> 2) + 1 : (n + 3) >> 2;
+        const float4* mp = reinterpret_cast<const float4*>(M + (int64_t)row * ld);
         double s = 0.0;
-        for (int c = c0 + lane; c < c1; c += 32) s += M[(int64_t)row * n + c] * in[c];
+#pragma unroll 4
+        for (int q = q0 + lane; q < q1; q += 32) {
+            const float4 v = __ldg(mp + q);
+            const int c = 4 * q;
+            s += double(v.x) * in[c];
+            if (c + 1 < n) s += double(v.y) * in[c + 1];
+            if (c + 2 < n) s += double(v.z) * in[c + 2];
+            if (c + 3 < n) s += double(v.w) * in[c + 3];
+        }
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) out[row] = s;
     }
 }
 
-// U = X^T on and above the diagonal (32 x 32 tiles through shared memory)
-__global__ void k_transpose_upper(int n, const double* __restrict__ X, double* __restrict__ U) {
+// Xf = L^-1 (lower) and Uf = its transpose (upper) in FP32, row stride ld, from X = L^-1 (FP64,
+// stride n); every entry of a row up to ld is written (zeros off the triangle and past n).
+// Block (bj, bi) of 32 x 32: Xf tile (bi, bj) when bj <= bi, Uf tile (bi, bj) when bj >= bi.
+__global__ void k_coarse_pack(int n, int ld, const double* __restrict__ X, float* __restrict__ Xf,
+                              float* __restrict__ Uf) {
     __shared__ double t[32][33];
-    const int bi = blockIdx.y, bj = blockIdx.x;  // output tile (bi, bj) of U, bj >= bi
-    if (bj < bi) return;
+    const int bi = blockIdx.y, bj = blockIdx.x;
     const int tx = threadIdx.x, ty = threadIdx.y;
+    if (bj <= bi) {
+        for (int r = ty; r < 32; r += 8) {
+            const int gr = bi * 32 + r, gc = bj * 32 + tx;
+            if (gr < n && gc < ld) Xf[(int64_t)gr * ld + gc] = (gc <= gr && gc < n) ? float(X[(int64_t)gr * n + gc]) : 0.f;
+        }
+    }
+    if (bj < bi) return;
     for (int r = ty; r < 32; r += 8) {
         const int gr = bj * 32 + r, gc = bi * 32 + tx;  // X row block bj, column block bi
         t[r][tx] = (gr < n && gc < n) ? X[(int64_t)gr * n + gc] : 0.0;
@@ -780,7 +879,7 @@ __global__ void k_transpose_upper(int n, const double* __restrict__ X, double* _
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
         const int gr = bi * 32 + r, gc = bj * 32 + tx;
-        if (gr < n && gc < n) U[(int64_t)gr * n + gc] = t[tx][r];
+        if (gr < n && gc < ld) Uf[(int64_t)gr * ld + gc] = (gc >= gr && gc < n) ? float(t[tx][r]) : 0.f;
     }
 }
 
@@ -892,7 +991,9 @@ int coarse_setup_mesh(plato_problem* h) {
                           "coarse grid does not align with the mesh: an element straddles two coarse cells");
     const size_t nn = size_t(c.ndof) * c.ndof;
     PLATO_CUDA(h, cudaMalloc(&c.E, sizeof(double) * nn));
-    PLATO_CUDA(h, cudaMalloc(&c.Einv, sizeof(double) * nn));
+    c.ldf = (c.ndof + 3) & ~3;
+    PLATO_CUDA(h, cudaMalloc(&c.Xf, sizeof(float) * 2 * size_t(c.ndof) * c.ldf));
+    c.Uf = c.Xf + size_t(c.ndof) * c.ldf;
     PLATO_CUDA(h, cudaMalloc(&c.X, sizeof(double) * nn));
     PLATO_CUDA(h, cudaMalloc(&c.T, sizeof(double) * nn));
     const int nblk = (c.ndof + kNB - 1) / kNB;
@@ -914,8 +1015,9 @@ void coarse_release(plato_problem* h) {
     CoarseSpace& c = h->coarse;
     for (int32_t** p : {&c.node_ptr, &c.node_list, &c.elem_ptr, &c.elem_list, &c.flag})
         if (*p) { cudaFree(*p); *p = nullptr; }
-    for (double** p : {&c.E, &c.Einv, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.tc, &c.rpart})
+    for (double** p : {&c.E, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.tc, &c.rpart})
         if (*p) { cudaFree(*p); *p = nullptr; }
+    if (c.Xf) { cudaFree(c.Xf); c.Xf = c.Uf = nullptr; }
     for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
         if (*e) { cudaEventDestroy(*e); *e = nullptr; }
     if (c.side) { cudaStreamDestroy(c.side); c.side = nullptr; }
@@ -1003,9 +1105,9 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
         h->launches += 1;
         PLATO_LAUNCH_CHECK(h);
     }
-    // the coarse solve applies X then X^T: keep U = X^T (upper) in the Einv buffer
+    // the coarse solve applies X then U = X^T: FP32 copies with 16-byte rows
     const int nt = (n + 31) / 32;
-    k_transpose_upper<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, X, c.Einv);
+    k_coarse_pack<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, c.ldf, X, c.Xf, c.Uf);
     PLATO_LAUNCH_CHECK(h);
     if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[2], s));
     int32_t bad = 0;
@@ -1033,8 +1135,8 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
                                                                       h->bc_mask, v, sq, c.rpart, S);
     k_restrict_sum<<<grid_for(c.ndof, 256), 256, 0, s>>>(cv, c.rsplit, c.rpart, c.rc, S);
     const int GB = grid_for(int64_t(c.ndof) * 32, 256, 148 * 8);
-    k_coarse_trmv<true><<<GB, 256, 0, s>>>(c.ndof, c.X, c.rc, c.tc, S);
-    k_coarse_trmv<false><<<GB, 256, 0, s>>>(c.ndof, c.Einv, c.tc, c.yc, S);
+    k_coarse_trmv<true><<<GB, 256, 0, s>>>(c.ndof, c.ldf, c.Xf, c.rc, c.tc, S);
+    k_coarse_trmv<false><<<GB, 256, 0, s>>>(c.ndof, c.ldf, c.Uf, c.tc, c.yc, S);
     k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, sq, y, accumulate, S);
     h->launches += 4;
     PLATO_LAUNCH_CHECK(h);

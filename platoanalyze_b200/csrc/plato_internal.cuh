@@ -143,7 +143,9 @@ struct CoarseSpace {
     int32_t* elem_ptr = nullptr;  // elements bucketed by coarse cell (CSR)
     int32_t* elem_list = nullptr;
     double*  E = nullptr;         // Galerkin operator, then its Cholesky factor (ndof^2)
-    double*  Einv = nullptr;      // U = (L^-1)^T, upper (ndof^2); E^-1 = U L^-1
+    float*   Xf = nullptr;        // L^-1 (lower) then its transpose U (upper), FP32, row stride ldf:
+    float*   Uf = nullptr;        // E^-1 = U L^-1, the per-iteration coarse solve (zeros elsewhere)
+    int32_t  ldf = 0;             // ndof rounded up to a multiple of 4 (16-byte rows)
     double*  X = nullptr;         // L^-1 while inverting (ndof^2)
     double*  T = nullptr;         // tile-product scratch of the inversion (ndof^2)
     double*  Dt = nullptr;        // inverse diagonal tiles of the Cholesky factor

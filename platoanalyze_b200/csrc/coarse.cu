@@ -492,7 +492,8 @@ __device__ __forceinline__ void tile_gemm(int n, const double* __restrict__ A, c
 //      Wr = Li R_s (R = the rows of [L | I] still to be eliminated, kept in W);
 //   C: the rank-8 trailing update T -= Lp Lp^T, the row elimination W[below] -= Lp Wr, and
 //      Lp, Wr copied into place.
-// 24 barriers in all; rows and columns past m are an identity block that factors to itself.
+// B and C are FP64 mma.sync tile products; 24 barriers in all; rows and columns past m are an
+// identity block that factors to itself.
 constexpr int kDiagThreads = 256;
 constexpr int kDiagPad = kNB + 1;
 constexpr size_t kDiagSmem = sizeof(double) * (2 * kNB * kDiagPad + kNB * 9 + 8 * kDiagPad + 8 * 9 + 8 * 9);
@@ -563,66 +564,49 @@ __global__ void __launch_bounds__(kDiagThreads) k_chol_diag(int n, double* __res
             }
         }
         __syncthreads();
-        // B: Lp[i][c] = sum_{t <= c} T[o+8+i][o+t] Li[c][t];  Wr[r][j] = sum_{t <= r} Li[r][t] W[o+t][j], j < o+8
-        const int nB1 = nb * 8, nB2 = 8 * (o + 8);
-        for (int e = tid; e < nB1 + nB2; e += kDiagThreads) {
-            if (e < nB1) {
-                const int i = e >> 3, c = e & 7;
-                double acc = 0.0;
+        // B and C on 8 x 8 tiles, one warp per tile, two FP64 m8n8k4 products per tile (lane l
+        // holds A[l/4][l%4], B[l%4][l/4] and C[l/4][2(l%4) + t]).  Li is zero above its
+        // diagonal, and a diagonal tile's upper half takes the trailing update too (never read).
+        const int nI = 7 - s;  // block rows below block s
+        const int g = lane >> 2, q = lane & 3;
+        // B: Lp = T[below, s] Li^T (tiles I < nI);  Wr = Li W[s, :] (tiles J <= s)
+        for (int tile = warp; tile < nI + s + 1; tile += kDiagThreads / 32) {
+            double acc[2] = {0.0, 0.0};
+            if (tile < nI) {
 #pragma unroll
-                for (int t = 0; t < 8; ++t)
-                    if (t <= c) acc += T[o + 8 + i][o + t] * Li[c][t];
-                Lp[i][c] = acc;
+                for (int kh = 0; kh < 2; ++kh)
+                    mma_f64(acc, T[o + 8 + 8 * tile + g][o + 4 * kh + q], Li[g][4 * kh + q]);
+                Lp[8 * tile + g][2 * q] = acc[0];
+                Lp[8 * tile + g][2 * q + 1] = acc[1];
             } else {
-                const int f = e - nB1, rr = f / (o + 8), j = f - rr * (o + 8);
-                double acc = 0.0;
+                const int J = tile - nI;
 #pragma unroll
-                for (int t = 0; t < 8; ++t)
-                    if (t <= rr) acc += Li[rr][t] * W[o + t][j];
-                Wr[rr][j] = acc;
+                for (int kh = 0; kh < 2; ++kh) mma_f64(acc, Li[g][4 * kh + q], W[o + 4 * kh + q][8 * J + g]);
+                Wr[g][8 * J + 2 * q] = acc[0];
+                Wr[g][8 * J + 2 * q + 1] = acc[1];
             }
         }
         __syncthreads();
-        // C: trailing update and row elimination on the owned entries, then the copies
-        if (nb > 0) {
-            double li[4][8];
-            bool ri[4];
+        const int nB1 = nb * 8, nB2 = 8 * (o + 8);
+        // C: T[I, J] -= Lp_I Lp_J^T (s < J <= I);  W[I, J] -= Lp_I Wr_J (J <= s < I)
+        const int t1 = nI * (nI + 1) / 2, t2 = nI * (s + 1);
+        for (int tile = warp; tile < t1 + t2; tile += kDiagThreads / 32) {
+            double acc[2] = {0.0, 0.0};
+            if (tile < t1) {
+                int I = 0, J = tile;
+                while (J >= I + 1) { J -= I + 1; ++I; }
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const int i = ty + 16 * a;
-                ri[a] = i >= o + 8;
+                for (int kh = 0; kh < 2; ++kh) mma_f64(acc, Lp[8 * I + g][4 * kh + q], Lp[8 * J + g][4 * kh + q]);
+                const int i = o + 8 + 8 * I + g, j = o + 8 + 8 * J + 2 * q;
+                T[i][j] -= acc[0];
+                T[i][j + 1] -= acc[1];
+            } else {
+                const int f = tile - t1, I = f / (s + 1), J = f - I * (s + 1);
 #pragma unroll
-                for (int t = 0; t < 8; ++t) li[a][t] = ri[a] ? Lp[i - o - 8][t] : 0.0;
-            }
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int j = tx + 16 * b;
-                double lj[8];
-                if (j >= o + 8) {
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) lj[t] = Lp[j - o - 8][t];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const int i = ty + 16 * a;
-                        if (!ri[a] || j > i) continue;
-                        double acc = 0.0;
-#pragma unroll
-                        for (int t = 0; t < 8; ++t) acc += li[a][t] * lj[t];
-                        T[i][j] -= acc;
-                    }
-                } else {
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) lj[t] = Wr[t][j];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const int i = ty + 16 * a;
-                        if (!ri[a]) continue;
-                        double acc = 0.0;
-#pragma unroll
-                        for (int t = 0; t < 8; ++t) acc += li[a][t] * lj[t];
-                        W[i][j] -= acc;
-                    }
-                }
+                for (int kh = 0; kh < 2; ++kh) mma_f64(acc, Lp[8 * I + g][4 * kh + q], Wr[4 * kh + q][8 * J + g]);
+                const int i = o + 8 + 8 * I + g, j = 8 * J + 2 * q;
+                W[i][j] -= acc[0];
+                W[i][j + 1] -= acc[1];
             }
         }
         for (int e = tid; e < nB1 + nB2; e += kDiagThreads) {

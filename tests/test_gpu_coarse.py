@@ -66,3 +66,28 @@ def test_galerkin_operator_and_inverse(cells, nc):
     assert np.abs(E - E.T).max() <= 1e-13 * np.abs(E).max()
     assert np.abs(Einv @ E - np.eye(nd.value)).max() <= 1e-9
     prob.close()
+
+
+def test_coarse_inverse_bench_grid():
+    """The bench's coarse grid (16x8x8 cells, 4131 coarse dofs: 65 tiles of 64, the last one
+    35 rows) on a small fine mesh: every step of the look-ahead chain and the ragged last tile.
+    Checked by the normwise residual of x = E^-1 b for random b, ||E x - b|| / (||E||_F ||x||): a
+    wrong tile gives O(1), rounding gives about n^1.5 eps whatever E's conditioning."""
+    m = box_mesh(48, 24, 24, 2.0, 1.0, 1.0)
+    opts = SolverOptions(precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=10, coarse_cells=(16, 8, 8))
+    prob = EllipticProblem(cantilever_spec(m, solver=opts))
+    zd = prob.to_dev(splitmix_uniform(m.num_nodes, 62))
+    nd = C.c_int32()
+    check(lib.plato_coarse_operator(prob.h, C.c_void_p(zd.data_ptr()), C.byref(nd), None, None), prob.h)
+    assert nd.value == 4131
+    E = np.empty((nd.value, nd.value))
+    Einv = np.empty_like(E)
+    check(lib.plato_coarse_operator(prob.h, C.c_void_p(zd.data_ptr()), C.byref(nd), E.ctypes.data_as(C.c_void_p),
+                                    Einv.ctypes.data_as(C.c_void_p)), prob.h)
+    assert np.abs(E - E.T).max() <= 1e-13 * np.abs(E).max()
+    rng = np.random.default_rng(7)
+    B = rng.standard_normal((nd.value, 4))
+    X = Einv @ B
+    backward = np.linalg.norm(E @ X - B, axis=0) / (np.linalg.norm(E) * np.linalg.norm(X, axis=0))
+    assert backward.max() <= 1e-10, backward
+    prob.close()

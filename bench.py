@@ -50,7 +50,7 @@ FP64_ITERATIONS = {"large": 3632, "medium": 1833, "small": None}
 METHOD_TEXT = {
     "two-level": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (10 steps on [lmax/200, lmax]) on an FP32 SELL copy + "
                   "FP64 Galerkin coarse correction on a 16x8x8 trilinear box grid"),
-    "two-level-fp16": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (10 steps on [lmax/200, lmax]) on an FP16 copy of the "
+    "two-level-fp16": ("FP64 flexible CG; preconditioner: FP32 Chebyshev-Jacobi (14 steps on [lmax/300, lmax]) on an FP16 copy of the "
                        "Jacobi-scaled matrix D^-1/2 A D^-1/2 + FP64 Galerkin coarse correction on a 16x8x8 trilinear "
                        "box grid"),
     "plain": "plain FP64 Jacobi-PCG on the assembled 3x3 block matrix (the reference's algorithm)",

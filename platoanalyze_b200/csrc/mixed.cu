@@ -205,6 +205,11 @@ k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__
           float* __restrict__ dnext, float* __restrict__ y, float c1, float c2, const PcgScalars* S) {
     if (S && S->done) return;
     const int64_t npairs = (((int64_t)A.num_rows + 31) & ~int64_t(31)) >> 1;
+    const uintptr_t vbits = reinterpret_cast<uintptr_t>(res) |
+                            (MODE == 0 ? reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dnext) |
+                                             reinterpret_cast<uintptr_t>(y)
+                                       : uintptr_t(0));
+    const bool vec2 = (vbits & 7) == 0;
     for (int64_t pr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pr < npairs;
          pr += (int64_t)gridDim.x * blockDim.x) {
         const int64_t sl = pr >> 4;
@@ -234,6 +239,26 @@ k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__
         }
         const int64_t r0 = 32 * sl + 2 * m;
         const float wv[6] = {a0, a1, a2, b0, b1, b2};
+        // both rows of the pair: their 6 entries start at 3 r0 = 6 (16 sl + m), 8-byte aligned
+        // when the vectors are, so the update runs on float2 (half the memory instructions)
+        if (MODE != 2 && vec2 && r0 + 1 < A.num_rows) {
+            float2* rp = reinterpret_cast<float2*>(res + 3 * r0);
+#pragma unroll
+            for (int u = 0; u < 3; ++u) {
+                const float2 rr = rp[u];
+                const float rs0 = rr.x - wv[2 * u], rs1 = rr.y - wv[2 * u + 1];
+                rp[u] = make_float2(rs0, rs1);
+                if (MODE == 0) {
+                    const float2 xx = reinterpret_cast<const float2*>(x + 3 * r0)[u];
+                    float2* yp = reinterpret_cast<float2*>(y + 3 * r0) + u;
+                    const float2 yy = *yp;
+                    const float d0 = c1 * xx.x + c2 * rs0, d1 = c1 * xx.y + c2 * rs1;
+                    reinterpret_cast<float2*>(dnext + 3 * r0)[u] = make_float2(d0, d1);
+                    *yp = make_float2(yy.x + d0, yy.y + d1);
+                }
+            }
+            continue;
+        }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             if (r0 + h >= A.num_rows) break;

@@ -18,6 +18,10 @@ throughput measured in the same run, and the accuracy of the timed solution agai
 CPU oracle's own FP64 solve.
 
     python bench.py [--gpus N --steps K --warmup W] [--method plain] [--impl reference]
+    python bench.py --profile-unit --cells 120,60,60 [--method two-level] [--repeat 1] [--coarse 16,8,8]
+
+--profile-unit runs untimed solve+adjoint units of the same cantilever on other meshes (the
+command the profiles' ncu captures run) and prints each unit's solver statistics.
 
 Prints one JSON line (rank 0).  Multi-GPU runs are independent replicas (weak scaling).
 """
@@ -71,6 +75,11 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations in the reference-arm sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-unit", action="store_true",
+                    help="run --repeat untimed solve+adjoint units on the --cells mesh (for profilers)")
+    ap.add_argument("--cells", default="80,40,40", help="--profile-unit: hexes along x,y,z (6 tets each)")
+    ap.add_argument("--repeat", type=int, default=1, help="--profile-unit: units to run")
+    ap.add_argument("--coarse", default=None, help="--profile-unit: coarse box cells x,y,z")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "helmholtz"],
                     help="batch: 64 independent GRF cantilevers n x n/2 x n/2, n in {16,24,32,48,64}, one batched "
                          "solve; helmholtz: the density filter's solution and chain rule on the --size mesh")
@@ -437,8 +446,36 @@ def run_helmholtz(args):
     return 0
 
 
+def run_profile_unit(args):
+    """Untimed solve+adjoint units (Problem::solution, compliance, self-adjoint dC/dz) of the
+    cantilever on the --cells mesh with nodal densities U[0.01, 1] (seed 0x5EED0002), for
+    profilers; prints the solver statistics and compliance of each unit."""
+    import torch
+
+    from platoanalyze_b200.problem import EllipticProblem
+    from platoanalyze_b200.workloads import SEED_LARGE, cantilever, coarse_grid, method_options, splitmix_uniform
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    nx, ny, nz = (int(v) for v in args.cells.split(","))
+    cg = tuple(int(v) for v in args.coarse.split(",")) if args.coarse else coarse_grid(nx, ny, nz)
+    spec = cantilever(nx, ny, nz, method_options(args.method, args.tol, cg))
+    z = splitmix_uniform(spec.coords.shape[0], SEED_LARGE)
+    prob = EllipticProblem(spec)
+    zd = prob.to_dev(z)
+    for _ in range(args.repeat):
+        u, st = prob.solution(zd)
+        f = prob.criterion_value(zd, u)
+        prob.criterion_gradient(zd, u)
+        torch.cuda.synchronize()
+        print({"cells": (nx, ny, nz), "method": args.method, "compliance": f} | st)
+    prob.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_unit:
+        return run_profile_unit(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":

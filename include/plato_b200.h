@@ -241,15 +241,19 @@ int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host
  * the implicit synchronisation of cudaMalloc/cudaFree).  No handle: connectivity
  * (num_cells*4 int32, 16-byte aligned), coords (num_nodes*3), u (num_nodes*3) and z
  * (num_nodes) are caller-owned [device] arrays; value is a [device] double written on
- * cuda_stream (NULL = legacy stream), readable after the caller synchronises that stream.
+ * cuda_stream (NULL = legacy stream).  The call waits for its kernel (it synchronises
+ * cuda_stream) so that its status reports what the kernel found: a connectivity id outside
+ * [0, num_nodes) gives PLATO_BAD_INPUT (such cells are skipped on the device, never read,
+ * and *value is NaN), a non-finite value gives PLATO_NONFINITE.  Material and penalty are
+ * checked as plato_create checks them.
  * The call allocates nothing: its reduction scratch is a static device array of 65,536 block
- * partial sums (512 KiB, held by every GPU that loads the library until exit), so num_cells is
- * limited to 16,777,216; larger meshes get PLATO_BAD_INPUT.  The first call on a device looks
- * up the scratch address on the current device; make that first call before any stream
- * capture.  Every call shares the one scratch array, which keeps the last call's contents:
- * calls whose kernels overlap on the GPU (different streams, or different host threads on
- * one device) race and must be serialised by the caller.  Errors read through
- * plato_last_error(NULL). */
+ * partial sums plus two counters (512 KiB, held by every GPU that loads the library until
+ * exit), so num_cells is limited to 16,777,216; larger meshes get PLATO_BAD_INPUT.  The first
+ * call on a device looks up the scratch address on the current device; make that first call
+ * before any stream capture.  Every call shares the one scratch array, which keeps the last
+ * call's contents (the counters are cleared at the start of each call): calls whose kernels
+ * overlap on the GPU (different streams, or different host threads on one device) race and
+ * must be serialised by the caller.  Errors read through plato_last_error(NULL). */
 int plato_sf_value_noalloc(int32_t num_nodes, int32_t num_cells, const int32_t* connectivity,
                            const double* coords, const double* u, const double* z,
                            const plato_material* material, const plato_penalty* penalty,

@@ -4,6 +4,10 @@
 #include <cstring>
 #include <vector>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "plato_internal.cuh"
 
 namespace plato {
@@ -57,6 +61,21 @@ int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const cha
     const int status = (e == cudaErrorMemoryAllocation) ? PLATO_OUT_OF_MEMORY : PLATO_CUDA_ERROR;
     return plato_fail(h, status, buf);
 }
+
+namespace plato {
+int ensure_smem_attribute(plato_problem* h, const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> granted;
+    int dev = 0;
+    PLATO_CUDA(h, cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    int& have = granted[{dev, kernel}];
+    if (bytes <= have) return PLATO_OK;
+    PLATO_CUDA(h, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    have = bytes;
+    return PLATO_OK;
+}
+}  // namespace plato
 
 namespace {
 

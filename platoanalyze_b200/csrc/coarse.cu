@@ -1021,12 +1021,7 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
         PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[0], s));
     }
     PLATO_CUDA(h, cudaMemsetAsync(c.E, 0, sizeof(double) * nn, s));
-    static std::once_flag smem_once;  // per kernel and process; a driver round trip per call otherwise
-    cudaError_t attr = cudaSuccess;
-    std::call_once(smem_once, [&] {
-        attr = cudaFuncSetAttribute(k_galerkin_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFastSmem));
-    });
-    PLATO_CUDA(h, attr);
+    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_galerkin_fast), int(kFastSmem)));
     k_galerkin_fast<<<c.ncells * c.gsplit, kThreadsPerCta, kFastSmem, s>>>(
         coarse_view(h), c.gsplit, c.elem_ptr, c.elem_list, h->conn, h->coords, z, h->material, h->bc_mask, n, c.E);
     PLATO_LAUNCH_CHECK(h);
@@ -1040,14 +1035,8 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
     const int nblk = (n + kNB - 1) / kNB;
     double *X = c.X, *D = c.Dt, *Tmp = c.T;  // scratch allocated with the coarse grid
-    static std::once_flag tiles_once;
-    cudaError_t attr2 = cudaSuccess;
-    std::call_once(tiles_once, [&] {
-        attr2 = cudaFuncSetAttribute(k_chol_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTwoTiles));
-        if (attr2 == cudaSuccess)
-            attr2 = cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPanelSmem));
-    });
-    PLATO_CUDA(h, attr2);
+    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_chol_diag), int(kTwoTiles)));
+    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_chol_panel), int(kPanelSmem)));
     if (!c.side) PLATO_CUDA(h, cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
         if (!*e) PLATO_CUDA(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));

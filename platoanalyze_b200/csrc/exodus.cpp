@@ -101,20 +101,28 @@ public:
         if (it == vars_.end()) throw DeckError("Exodus: variable '" + name + "' missing");
         return it->second;
     }
+    // element count of a variable; no variable holds more elements than the file has bytes,
+    // so a product beyond that is a corrupt header (and is stopped before it can overflow)
     uint64_t size(const NcVar& v) const {
         uint64_t n = 1;
-        for (int64_t d : v.dims) n *= dim_len_[size_t(d)];
+        for (int64_t d : v.dims) {
+            const uint64_t len = dim_len_[size_t(d)];
+            if (len != 0 && n > buf_.size() / len) throw DeckError("netCDF: variable larger than the file");
+            n *= len;
+        }
         return n;
     }
     // a fixed-size variable as doubles / int64 (any numeric type)
     std::vector<double> doubles(const std::string& name) const {
         const NcVar& v = var(name);
+        check_range(v, size(v));  // before the allocation: the size comes from the file
         std::vector<double> out(size(v));
         for (size_t i = 0; i < out.size(); ++i) out[i] = value(v, i);
         return out;
     }
     std::vector<int64_t> ints(const std::string& name) const {
         const NcVar& v = var(name);
+        check_range(v, size(v));
         std::vector<int64_t> out(size(v));
         for (size_t i = 0; i < out.size(); ++i) out[i] = int64_t(value(v, i));
         return out;
@@ -124,7 +132,7 @@ public:
         const NcVar& v = var(name);
         if (v.type != NC_CHAR || v.dims.size() != 2) throw DeckError("Exodus: '" + name + "' is not a name table");
         const uint64_t rows = dim_len_[size_t(v.dims[0])], len = dim_len_[size_t(v.dims[1])];
-        check_range(v, rows * len);
+        check_range(v, size(v));
         std::vector<std::string> out;
         for (uint64_t r = 0; r < rows; ++r) {
             const char* s = buf_.data() + v.begin + r * len;
@@ -139,7 +147,7 @@ public:
 
 private:
     void need(uint64_t n) const {
-        if (p_ + n > buf_.size()) throw DeckError("netCDF: header runs past the end of the file");
+        if (p_ > buf_.size() || n > buf_.size() - p_) throw DeckError("netCDF: header runs past the end of the file");
     }
     uint32_t u32() {
         need(4);
@@ -167,7 +175,8 @@ private:
             const std::string name = str();
             const int t = int(u32());
             const uint64_t m = count();
-            const uint64_t bytes = m * uint64_t(type_size(t));
+            if (m > buf_.size()) throw DeckError("netCDF: header runs past the end of the file");
+            const uint64_t bytes = m * uint64_t(type_size(t));  // at most 8 x the file size: no overflow
             need(bytes);
             if (text && t == NC_CHAR) (*text)[name] = buf_.substr(p_, m);
             p_ += (bytes + 3) & ~uint64_t(3);
@@ -175,7 +184,9 @@ private:
     }
     void check_range(const NcVar& v, uint64_t n) const {
         if (v.record) throw DeckError("Exodus: record variables are not read");
-        if (v.begin + n * uint64_t(type_size(v.type)) > buf_.size()) throw DeckError("netCDF: variable past the end of the file");
+        const uint64_t ts = uint64_t(type_size(v.type));
+        if (v.begin > buf_.size() || n > (buf_.size() - v.begin) / ts)
+            throw DeckError("netCDF: variable past the end of the file");
     }
     double value(const NcVar& v, uint64_t i) const {
         if (i == 0) check_range(v, size(v));

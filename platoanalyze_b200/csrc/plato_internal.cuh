@@ -301,11 +301,25 @@ constexpr int kEnergySplit = 32;  // CTAs per member in the batched criterion su
 int launch_energy_segments(plato_problem* h, const double* u, const double* z, double* values);
 }  // namespace plato
 int plato_cuda_fail(plato_problem* h, cudaError_t e, const char* what, const char* file, int line);
+namespace plato {
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the handle's current
+// device.  The attribute belongs to one device, so the granted size is remembered per
+// (device, kernel) under a lock (a driver call per launch otherwise); a failed attempt is
+// not remembered, so every later call retries and reports the same error.
+int ensure_smem_attribute(plato_problem* h, const void* kernel, int bytes);
+}  // namespace plato
 
 #define PLATO_CUDA(h, expr)                                                          \
     do {                                                                             \
         cudaError_t _e = (expr);                                                     \
         if (_e != cudaSuccess) return plato_cuda_fail((h), _e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+// Returns a non-zero plato_status of a call from the enclosing function.
+#define PLATO_RC(expr)                                                               \
+    do {                                                                             \
+        const int _rc = (expr);                                                      \
+        if (_rc) return _rc;                                                         \
     } while (0)
 
 #define PLATO_LAUNCH_CHECK(h)                                                        \

@@ -197,18 +197,9 @@ int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float
     const size_t smem = size_t(9) * P.max_slice_blocks * sizeof(double);
     const int grid = grid_for(P.nslices, 1, 148 * 16);
     if (smem <= 200 * 1024) {
-        // the attribute is per kernel and process; raise it only (a driver round trip per call otherwise)
-        static std::mutex mu;
-        static int granted = 0;
         const int want = int(smem > 48 * 1024 ? smem : 48 * 1024);
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            if (want > granted) {
-                PLATO_CUDA(h, cudaFuncSetAttribute(k_crs_to_sell<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   want));
-                granted = want;
-            }
-        }
+        const int rc = ensure_smem_attribute(h, reinterpret_cast<const void*>(k_crs_to_sell<true>), want);
+        if (rc) return rc;
         k_crs_to_sell<true><<<grid, kSliceThreads, smem, h->stream>>>(
             h->N, P.nslices, h->row_map, h->diag, P.width, P.ptr, crs, out64, out32,
             static_cast<__nv_bfloat16*>(out16), dinv, dinv32);

@@ -106,6 +106,13 @@ typedef struct plato_solver_opts {
                                  box (trilinear coarse space, Galerkin coarse operator);
                                  {0,0,0} = none.  Needs every element inside one coarse
                                  cell (box meshes with divisible cell counts)             */
+    int32_t fallback_max_iterations; /* when a flexible-CG method (precision != FP64, a
+                                 Chebyshev degree, a coarse grid or the matrix-free operator)
+                                 ends without meeting the tolerance or breaks down, the solve
+                                 is retried from a zero guess if a subspace guess seeded it,
+                                 then falls back to the plain FP64 Jacobi-PCG from a zero
+                                 guess; this caps the fallback's iterations (0: the same cap
+                                 as max_iterations, < 0: no fallback)                      */
 } plato_solver_opts;
 
 typedef struct plato_problem_desc {
@@ -124,6 +131,10 @@ typedef struct plato_solve_stats {
     double  relative_residual; /* FP64 ||b - A x|| / ||b|| at exit          */
     int32_t converged;
     int32_t status;            /* plato_status of the solve                */
+    int32_t fallback;          /* 0: the configured method converged; 1: it converged after a
+                                  retry from a zero guess (the subspace guess failed); 2: the
+                                  plain FP64 Jacobi-PCG fallback ran (iterations and residual
+                                  are the fallback's)                                     */
 } plato_solve_stats;
 
 /* ---- lifetime -------------------------------------------------------------------------

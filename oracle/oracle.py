@@ -62,10 +62,13 @@ def _load() -> C.CDLL:
         "oracle_apply_block_constraints": ([C.c_int32, vp, vp, vp, vp, C.c_int32, vp, vp, C.c_double], None),
         "oracle_matvec_plus": ([C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp], None),
         "oracle_pcg_jacobi": ([C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_int32, C.POINTER(OracleStats)], C.c_int),
+        "oracle_refine_solution": ([C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                    C.POINTER(OracleStats)], C.c_int),
         "oracle_problem_solution": ([P, vp, vp, C.c_double, C.c_int32, C.POINTER(OracleStats)], C.c_int),
         "oracle_problem_criterion_gradient": ([P, vp, vp, C.c_int32, C.c_double, C.c_int32, vp,
                                                C.POINTER(OracleStats)], C.c_int),
         "oracle_num_threads": ([], C.c_int),
+        "oracle_set_num_threads": ([C.c_int], None),
         "oracle_volume_value": ([P, vp, C.c_double, C.c_double], C.c_double),
         "oracle_volume_gradient_z": ([P, vp, C.c_double, C.c_double, vp], None),
         "oracle_helmholtz_value": ([P, H, vp, vp, vp], None),
@@ -206,6 +209,29 @@ class Oracle:
         return x, {"iterations": st.iterations, "relative_residual": st.relative_residual,
                    "converged": st.converged}
 
+    def refine(self, A, b, u, tol=1e-13, inner_tol=1e-5, max_rounds=6, max_it=1000000):
+        """Iterative refinement of A u = b from u (any float array) with a long double iterate
+        and long double residuals; returns (u as np.longdouble, stats)."""
+        rm, cols = self.graph()
+        x = np.array(u, dtype=np.longdouble)
+        st = OracleStats()
+        lib.oracle_refine_solution(self.N, _p(rm), _p(cols), _p(A), _p(np.ascontiguousarray(b, np.float64)), _p(x),
+                                   tol, inner_tol, max_rounds, max_it, C.byref(st))
+        return x, {"iterations": st.iterations, "relative_residual": st.relative_residual,
+                   "converged": st.converged}
+
+    def solution_refined(self, z, tol=1e-13, tol0=1e-10, max_it=1000000):
+        """Problem::solution to a long double relative residual <= tol: FP64 Jacobi-PCG to
+        tol0, then iterative refinement.  Returns (u as float64, u as np.longdouble, stats)."""
+        n = 3 * self.N
+        K = self.vf_gradient_u(np.zeros(n), z)
+        rhs = -self.vf_value(np.zeros(n), z)
+        self.apply_constraints(K, rhs, 1.0)
+        u0, st0 = self.pcg(K, rhs, tol=tol0, max_it=max_it)
+        uld, st = self.refine(K, rhs, u0, tol=tol, max_it=max_it)
+        st["iterations"] += st0["iterations"]
+        return uld.astype(np.float64), uld, st
+
     def solution(self, z, tol=1e-10, max_it=100000):
         u = np.empty(3 * self.N)
         st = OracleStats()
@@ -283,3 +309,7 @@ class Oracle:
     @staticmethod
     def num_threads() -> int:
         return lib.oracle_num_threads()
+
+    @staticmethod
+    def set_num_threads(n: int) -> None:
+        lib.oracle_set_num_threads(int(n))

@@ -85,6 +85,12 @@ void oracle_apply_block_constraints(int32_t num_node_rows, const int32_t* row_ma
 void oracle_matvec_plus(int32_t num_node_rows, int32_t rows_per_block, int32_t cols_per_block,
                         const int32_t* row_map, const int32_t* column_indices, const double* entries,
                         const double* x, double* y);
+/* Iterative refinement of A u = b with a long double iterate u (in/out), long double
+ * residuals and FP64 Jacobi-PCG corrections to inner_tol; stops at ||b - A u||/||b|| <= tol.
+ * stats->iterations counts the inner iterations, relative_residual is the long double one. */
+int oracle_refine_solution(int32_t N, const int32_t* row_map, const int32_t* cols, const double* A,
+                           const double* b, long double* u, double tol, double inner_tol, int32_t max_rounds,
+                           int32_t max_it, oracle_solve_stats* stats);
 int  oracle_pcg_jacobi(int32_t num_node_rows, const int32_t* row_map, const int32_t* column_indices,
                        const double* entries, const double* b, double* x, double tolerance,
                        int32_t max_iterations, oracle_solve_stats* stats);
@@ -121,6 +127,7 @@ int oracle_helmholtz_criterion_gradient(const oracle_problem* P, const oracle_he
                                         double* dfdcontrol, double tolerance, int32_t max_iterations,
                                         oracle_solve_stats* stats);
 int oracle_num_threads(void);
+void oracle_set_num_threads(int n); /* OpenMP threads of the later calls (n > 0) */
 
 #ifdef __cplusplus
 }

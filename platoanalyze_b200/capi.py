@@ -47,7 +47,8 @@ class EssentialBCs(C.Structure):
 class SolverOpts(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int32), ("operator_kind", C.c_int32),
                 ("precision", C.c_int32), ("self_adjoint", C.c_int32), ("chebyshev_ratio", C.c_double),
-                ("chebyshev_degree", C.c_int32), ("coarse_cells", C.c_int32 * 3)]
+                ("chebyshev_degree", C.c_int32), ("coarse_cells", C.c_int32 * 3),
+                ("fallback_max_iterations", C.c_int32)]
 
 
 class ProblemDesc(C.Structure):
@@ -64,7 +65,7 @@ class HelmholtzDesc(C.Structure):
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("refinements", C.c_int32), ("relative_residual", C.c_double),
-                ("converged", C.c_int32), ("status", C.c_int32)]
+                ("converged", C.c_int32), ("status", C.c_int32), ("fallback", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

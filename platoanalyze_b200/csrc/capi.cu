@@ -575,6 +575,42 @@ static bool plain_method(const plato_solver_opts& o) {
            o.chebyshev_degree <= 0 && o.coarse_cells[0] <= 0;
 }
 
+// The plain method is the fallback of the others.  When a flexible-CG solve (status
+// `failed`) did not meet the tolerance or broke down: if a subspace guess seeded it, the same
+// method is retried from a zero guess; if that fails too, or there was no such guess, the
+// plain FP64 Jacobi-PCG solves from a zero guess with fallback_max_iterations (0: the
+// max_iterations cap).  h->v_b holds the constrained right-hand side.  For the matrix-free
+// operator (z given) the constrained block matrix is assembled first.
+static int fallback_solve(plato_problem* h, double* x, plato_solve_stats* st, int failed,
+                          const double* z = nullptr) {
+    const int32_t cap = h->opts.fallback_max_iterations;
+    const size_t bytes = sizeof(double) * 3 * size_t(h->N);
+    if (h->ritz_W && h->ritz_k > 0) {
+        PLATO_CUDA(h, cudaMemsetAsync(x, 0, bytes, h->stream));
+        const int rc = fcg_poly(h, h->v_b, x, st);
+        if (rc != PLATO_NOT_CONVERGED && rc != PLATO_NONFINITE) {
+            st->fallback = 1;
+            return rc;
+        }
+        failed = rc;
+    }
+    if (cap < 0) return failed;
+    if (z) {  // matrix-free: the assembled constrained operator (right-hand side already built)
+        RC(dmalloc(h, &h->K, 9 * h->nblocks));
+        RC(launch_assemble_jacobian(h, z, h->K));
+        RC(launch_dirichlet(h, h->K, nullptr, 0.0));
+        RC(prepare_operator(h, h->K));
+    }
+    // the SELL FP64 copy and its Jacobi diagonal were made for the flexible CG's operator
+    const int32_t saved = h->opts.max_iterations;
+    if (cap > 0) h->opts.max_iterations = cap;
+    PLATO_CUDA(h, cudaMemsetAsync(x, 0, bytes, h->stream));
+    const int rc = pcg_fp64(h, h->v_b, x, st);
+    h->opts.max_iterations = saved;
+    st->fallback = 2;
+    return rc;
+}
+
 // Builds the constrained operator of control z and the right-hand side (rhs with the
 // Dirichlet rows/columns eliminated, values scaled by bc_scale), then solves into x (which
 // holds the initial guess).  Plain method: assembled block matrix + Jacobi-PCG.  Otherwise:
@@ -589,7 +625,9 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         RC(prepare_mixed(h, nullptr, z));
         RC(prepare_coarse(h, z));
         RC(matfree_rhs(h, h->v_b, bc_scale));
-        return fcg_poly(h, h->v_b, x, st);
+        const int rc = fcg_poly(h, h->v_b, x, st);
+        if (rc != PLATO_NOT_CONVERGED && rc != PLATO_NONFINITE) return rc;
+        return fallback_solve(h, x, st, rc, z);
     }
     RC(dmalloc(h, &h->K, 9 * h->nblocks));
     if (h->timing) {
@@ -613,6 +651,7 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         RC(prepare_coarse(h, z));
         RC(ritz_guess(h, h->v_b, x));
         rc = fcg_poly(h, h->v_b, x, st);
+        if (rc == PLATO_NOT_CONVERGED || rc == PLATO_NONFINITE) rc = fallback_solve(h, x, st, rc);
     }
     if (h->timing) {  // the solver has synchronised the stream
         float ms = 0.f;

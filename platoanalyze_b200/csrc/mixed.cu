@@ -49,6 +49,7 @@ namespace {
 
 constexpr int kChunk = 16;
 constexpr int kTimingStride = 8;
+constexpr int kMaxRestarts = 8;  // restarts from the true residual (see the plain PCG)
 
 enum InnerKind { INNER_SELL64 = 0, INNER_SELL32 = 1, INNER_SELL16 = 2, INNER_EBE32 = 3, INNER_EBE64 = 4,
                  INNER_SELL16S = 5 };
@@ -830,14 +831,13 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         if (rc) return rc;
         const double rel = fin.bb > 0.0 ? std::sqrt(rr / fin.bb) : 0.0;
         stats->relative_residual = rel;
-        // same acceptance as the plain PCG: recurrence met, true residual within 10x of tol
-        const bool recurrence_met = fin.rr <= fin.tol2;
-        if (fin.bb == 0.0 || rel <= tol || (recurrence_met && rel <= 10.0 * tol)) {
+        // same acceptance as the plain PCG: the recomputed FP64 residual meets the tolerance
+        if (fin.bb == 0.0 || rel <= tol) {
             stats->converged = 1;
             stats->status = PLATO_OK;
             return PLATO_OK;
         }
-        if (fin.iter >= max_it || restarts >= 3) {
+        if (fin.iter >= max_it || restarts >= kMaxRestarts) {
             stats->converged = 0;
             stats->status = PLATO_NOT_CONVERGED;
             return plato_fail(h, PLATO_NOT_CONVERGED, "flexible CG stopped before ||b - A x|| <= tol ||b||");
@@ -907,7 +907,7 @@ __device__ __forceinline__ void seg_mark_done(const BatchView& B) {
 }
 
 // r = b - A x (A x in r on entry), r.r and b.b per member; starts the preconditioner.
-// accept scales the stop test (1 on the first pass, the true-residual slack on restarts).
+// accept scales the stop test (1: the FP64 true residual must meet the tolerance).
 __global__ void __launch_bounds__(kThreads)
 k_bfcg_start(BatchView B, const double* __restrict__ b, double* __restrict__ r, const float* __restrict__ dinv32,
              float* __restrict__ res, float* __restrict__ d, float* __restrict__ y, float c0, double tol,
@@ -1189,8 +1189,7 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
     PcgScalars init{};
     PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
     PLATO_CUDA(h, cudaMemsetAsync(bt.S, 0, sizeof(SegScalars) * bt.nseg, s));
-    constexpr int kMaxPasses = 4;  // first pass + restarts from the true residual
-    constexpr double kSlack = 10.0;
+    constexpr int kMaxPasses = 1 + kMaxRestarts;  // first pass + restarts from the true residual
     int64_t precond_applies = 0;
     cudaEvent_t* ev = h->poll_ev;
     for (int e = 0; e < 2; ++e)
@@ -1203,7 +1202,7 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         rc = launch_sell_spmv(h, h->sell64, x, h->v_r);
         if (rc) return rc;
         k_bfcg_start<<<T, kThreads, 0, s>>>(BV, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, tol,
-                                             pass > 0 ? 1 : 0, pass > 0 ? kSlack : 1.0);
+                                             pass > 0 ? 1 : 0, 1.0);
         PLATO_LAUNCH_CHECK(h);
         PcgScalars* slots = h->scal_host;
         PLATO_CUDA(h, cudaMemcpyAsync(&slots[0], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
@@ -1255,8 +1254,7 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         st.iterations = S.iter;
         st.refinements = int32_t(precond_applies);
         st.relative_residual = S.bb > 0.0 ? std::sqrt(S.rr / S.bb) : 0.0;
-        const bool ok = !S.nonfinite && S.done && (S.bb == 0.0 || st.relative_residual <= kSlack * tol) &&
-                        (S.iter < max_it || st.relative_residual <= tol);
+        const bool ok = !S.nonfinite && S.done && (S.bb == 0.0 || st.relative_residual <= tol);
         st.converged = ok ? 1 : 0;
         st.status = S.nonfinite ? PLATO_NONFINITE : (ok ? PLATO_OK : PLATO_NOT_CONVERGED);
         agg.iterations = std::max(agg.iterations, st.iterations);

@@ -26,7 +26,10 @@ namespace {
 
 constexpr int kChunk = 32;
 constexpr int kTimingStride = 8;
-constexpr double kTrueResidualSlack = 10.0;
+// Restarts from the current iterate allowed when the iterated residual met the tolerance but
+// the recomputed b - A x did not (the recurrence drifts from the true residual over thousands
+// of iterations; each restart re-synchronises them).
+constexpr int kMaxRestarts = 8;
 
 // y = A x on the SELL copy; with S != nullptr also p.Ap (x = p, y = Ap) and alpha.
 // 6 blocks of 256 per SM (40 registers, no spills): more loads in flight than the default
@@ -394,17 +397,14 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
         if (rc) return rc;
         const double rel = fin.bb > 0.0 ? sqrt(rr / fin.bb) : 0.0;
         stats->relative_residual = rel;
-        // Converged when the recurrence met the tolerance (AztecOO's AZ_r0 test on the
-        // iterated residual) and the recomputed FP64 residual is within kTrueResidualSlack of
-        // it: b - A x cannot be evaluated in FP64 much below eps * ||A|| ||x|| / ||b||, which on
-        // stiff SIMP problems sits near 1e-10.
-        const bool recurrence_met = fin.rr <= fin.tol2;
-        if (fin.bb == 0.0 || rel <= tol || (recurrence_met && rel <= kTrueResidualSlack * tol)) {
+        // Converged only when the recomputed FP64 residual ||b - A x|| meets the tolerance; the
+        // iterated residual (AztecOO's AZ_r0 test) only decides when to recompute it.
+        if (fin.bb == 0.0 || rel <= tol) {
             stats->converged = 1;
             stats->status = PLATO_OK;
             return PLATO_OK;
         }
-        if (fin.iter >= max_it || restarts >= 3) {
+        if (fin.iter >= max_it || restarts >= kMaxRestarts) {
             stats->converged = 0;
             stats->status = PLATO_NOT_CONVERGED;
             return plato_fail(h, PLATO_NOT_CONVERGED, "PCG stopped before ||b - A x|| <= tol ||b||");

@@ -33,11 +33,12 @@ class SolverOptions:
     chebyshev_ratio: float = 30.0
     chebyshev_degree: int = 0
     coarse_cells: tuple = (0, 0, 0)
+    fallback_max_iterations: int = 0  # plain FP64 Jacobi-PCG fallback cap (0: max_iterations, < 0: none)
 
     def to_c(self) -> capi.SolverOpts:
         return capi.SolverOpts(self.tolerance, self.max_iterations, self.operator_kind, self.precision,
                                int(self.self_adjoint), self.chebyshev_ratio, self.chebyshev_degree,
-                               (C.c_int32 * 3)(*self.coarse_cells))
+                               (C.c_int32 * 3)(*self.coarse_cells), self.fallback_max_iterations)
 
 
 @dataclass

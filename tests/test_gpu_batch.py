@@ -111,7 +111,7 @@ def test_batched_solution_matches_oracle():
     uh = host(u)
     for s, sl in enumerate(bp.member_slices()):
         orc = Oracle.from_spec(specs[s])
-        uo, _ = orc.solution(zs[s], tol=1e-13)
+        uo, _, _ = orc.solution_refined(zs[s], tol=1e-13)
         assert rel_l2(uh[sl], uo) <= 1e-8, s
 
 

@@ -172,7 +172,7 @@ def test_solution_compliance_gradient(small):
     zd = prob.to_dev(z)
     u, st = prob.solution(zd)
     assert st["converged"] == 1 and st["relative_residual"] <= 1e-10, st
-    uo, sto = orc.solution(z, tol=1e-13)
+    uo, _, sto = orc.solution_refined(z, tol=1e-13)
     assert rel_l2(host(u), uo) <= 1e-8, rel_l2(host(u), uo)
     # criterion and sensitivity are functions of (u, z): compare on the GPU state at 1e-11
     uh = host(u)

@@ -138,7 +138,7 @@ def test_inhomogeneous_dirichlet_matrix_free_matches_assembled():
     spec.bc_values = np.linspace(-1e-3, 2e-3, spec.bc_dofs.size)
     z = splitmix_uniform(spec.coords.shape[0], 17)
     orc = Oracle.from_spec(spec)
-    uo, _ = orc.solution(z, tol=1e-13)
+    uo, _, _ = orc.solution_refined(z, tol=1e-13)
     for opts in (SolverOptions(tolerance=1e-11),
                  SolverOptions(tolerance=1e-11, operator_kind=capi.OPERATOR_MATRIX_FREE,
                                precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=6)):

@@ -56,12 +56,12 @@ def test_compliance_sensitivity_by_finite_differences(small):
     dz = np.sin(np.arange(orc.N) * 0.7) * 0.05
 
     def compliance(zz):
-        uu, _ = orc.solution(zz, tol=1e-13)
+        uu, _, _ = orc.solution_refined(zz, tol=1e-13)
         return orc.sf_value(uu, zz)
 
     eps = 1e-5
     fd = (compliance(z + eps * dz) - compliance(z - eps * dz)) / (2 * eps)
-    u, _ = orc.solution(z, tol=1e-13)
+    u, _, _ = orc.solution_refined(z, tol=1e-13)
     for self_adjoint in (True, False):
         g = orc.criterion_gradient(z, u, self_adjoint=self_adjoint, tol=1e-13)
         assert abs(g @ dz - fd) < 1e-6 * abs(fd), (self_adjoint, g @ dz, fd)
@@ -91,18 +91,43 @@ def test_linear_patch():
 
 
 def test_solution_matches_direct_factorisation():
-    """Config-1 sized cantilever: PCG (tol 1e-13) equals scipy's sparse direct solve."""
+    """Config-1 cantilever (z = 0.5): the FP64 PCG at 1e-10 and the refined solve at 1e-13 both
+    equal scipy's sparse direct solve; the PCG's stop test is the recomputed FP64 residual."""
     spec = cantilever(20, 10, 10)
     orc = Oracle.from_spec(spec)
     z = np.full(orc.N, 0.5)
-    u, st = orc.solution(z, tol=1e-13)
+    u, st = orc.solution(z, tol=1e-10)
     rm, cols = orc.graph()
     K = orc.vf_gradient_u(np.zeros(3 * orc.N), z)
     b = -orc.vf_value(np.zeros(3 * orc.N), z)
     orc.apply_constraints(K, b, 1.0)
     ud = spla.spsolve(bsr_to_scipy(rm, cols, K, orc.N).tocsc(), b)
-    assert st["converged"] == 1
-    assert rel_l2(u, ud) < 1e-10
+    assert st["converged"] == 1 and st["relative_residual"] <= 1e-10
+    r = b - orc.matvec_plus(3, 3, K, u, np.zeros(3 * orc.N))
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b)
+    assert rel_l2(u, ud) < 1e-7
+    ur, uld, st2 = orc.solution_refined(z, tol=1e-13)
+    assert st2["converged"] == 1 and st2["relative_residual"] <= 1e-13
+    assert rel_l2(ur, ud) < 1e-10
+
+
+def test_refinement_reaches_the_extended_precision_tolerance():
+    """The long double refinement lowers the residual floor of an FP64 iterate: from a 1e-10
+    solve it reaches <= 1e-13 (long double residual), and the refined iterate is closer to the
+    direct solution than the FP64 one."""
+    spec = cantilever(12, 6, 6)
+    orc = Oracle.from_spec(spec)
+    z = np.linspace(0.05, 1.0, orc.N)
+    n = 3 * orc.N
+    K = orc.vf_gradient_u(np.zeros(n), z)
+    b = -orc.vf_value(np.zeros(n), z)
+    orc.apply_constraints(K, b, 1.0)
+    u0, st0 = orc.pcg(K, b, tol=1e-10)
+    uld, st = orc.refine(K, b, u0, tol=1e-13, inner_tol=1e-4)
+    assert uld.dtype == np.longdouble and st["converged"] == 1 and st["relative_residual"] <= 1e-13
+    rm, cols = orc.graph()
+    ud = spla.spsolve(bsr_to_scipy(rm, cols, K, orc.N).tocsc(), b)
+    assert rel_l2(uld.astype(np.float64), ud) <= rel_l2(u0, ud)
 
 
 def test_volume_criterion():

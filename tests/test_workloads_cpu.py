@@ -34,3 +34,22 @@ def test_batch_workload_draw():
     specs2, zs2, ns2 = batch_workload(count=8, sizes=(4, 6))
     assert ns == ns2 and all(np.array_equal(a, b) for a, b in zip(zs, zs2))
     assert BATCH_SIZES == (16, 24, 32, 48, 64)
+
+
+def test_oracle_side_cantilever_equals_the_product_workload():
+    """The reference arm builds its problem without the product library (oracle/workload.py);
+    it must be the same problem, array for array."""
+    import workload as ow
+
+    from platoanalyze_b200.workloads import cantilever
+
+    for size in ((3, 2, 2), (8, 4, 4), (5, 3, 7)):
+        spec = cantilever(*size)
+        orc = ow.cantilever_oracle(*size)
+        assert np.array_equal(orc.coords, spec.coords)
+        assert np.array_equal(orc.conn, spec.connectivity)
+        assert np.array_equal(orc.bc_dofs, spec.bc_dofs)
+        cells, local, vec = spec.tractions[0]
+        assert np.array_equal(orc.fc, cells) and np.array_equal(orc.fl, local)
+        assert tuple(vec) == (0.0, -1.0, 0.0)
+    assert np.array_equal(ow.splitmix_uniform(4096, 0x5EED0002), splitmix_uniform(4096, 0x5EED0002))

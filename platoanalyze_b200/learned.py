@@ -262,13 +262,7 @@ def learned_subspace(net: UNet, zd, src_nodes, smooth_passes: int = 0):
 
 def subspace_solution(prob: EllipticProblem, zd, W):
     """plato_problem_solution_subspace from a zero guess; returns (u, stats, residual ratio)."""
-    torch = prob.torch
-    u = torch.zeros(prob.num_dofs, dtype=torch.float64, device="cuda")
-    st = capi.SolveStats()
-    ratio = C.c_double()
-    check(lib.plato_problem_solution_subspace(prob.h, prob._dev(zd), None, C.c_void_p(W.data_ptr()), W.shape[0],
-                                              prob._dev(u), C.byref(st), C.byref(ratio)), prob.h)
-    return u, st.as_dict(), ratio.value
+    return prob.solution_subspace(zd, W)
 
 
 def warm_start_solution(prob: EllipticProblem, net: UNet, zd, src_nodes, smooth_passes: int = 0):

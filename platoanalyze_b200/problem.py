@@ -290,6 +290,17 @@ class EllipticProblem:
             check(rc, self.h)
         return u, st.as_dict() | {"rc": rc}
 
+    def solution_subspace(self, z, W, u0=None):
+        """Problem::solution from the guess u0 (or zero) improved on span(P W), W a (k, 3N)
+        device array; returns (u, stats, residual ratio of the subspace correction)."""
+        u = self.zeros(self.num_dofs)
+        st = capi.SolveStats()
+        ratio = C.c_double()
+        check(lib.plato_problem_solution_subspace(self.h, self._dev(z), self._dev(u0) if u0 is not None else None,
+                                                  self._dev(W), int(W.shape[0]), self._dev(u), C.byref(st),
+                                                  C.byref(ratio)), self.h)
+        return u, st.as_dict(), ratio.value
+
     def criterion_value(self, z, u) -> float:
         v = C.c_double()
         check(lib.plato_problem_criterion_value(self.h, self._dev(z), self._dev(u), C.byref(v)), self.h)

@@ -1,0 +1,148 @@
+"""Parity on the stated benchmark configurations, through the C ABI.
+
+* Config 1 exactly: 20x10x10 cantilever (7,623 dofs), z = 0.5 everywhere, plain FP64
+  Jacobi-PCG to 1e-10.  Pattern bit-exact; R(0, z) (= -F), R(u, z), K(z) and the constrained
+  K within 1e-11 of the oracle; the solve meets the FP64-recomputed tolerance and its u is
+  within 1e-8 of the oracle refined to 1e-13; compliance and dC/dz within 1e-11 on the same
+  state.
+* Config 2 at full size: 160x80x80 (3,168,963 dofs), nodal densities U[0.01, 1] from seed
+  0x5EED0002.  Pattern bit-exact; R(u, z), every one of the 140 M Jacobian entries, the
+  compliance, dC/dz and (dR/dz)^T lambda on a smooth state within 1e-11 of the oracle.
+* Config 4 member sizes: n in {16, 24, 32, 48, 64} (n x n/2 x n/2 hexes, up to 212,355 dofs),
+  GRF densities and random end tractions from seed 0x5EED0004, one batched solve; every
+  member's u and dC/dz within 1e-8 of the oracle's solve refined to 1e-13.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+from oracle import Oracle
+from platoanalyze_b200.problem import EllipticProblem, SolverOptions, cantilever_spec
+from platoanalyze_b200.mesh import box_mesh
+from platoanalyze_b200.workloads import BATCH_SIZES, SEED_BATCH, SEED_LARGE, cantilever, grf_density, method_options
+from platoanalyze_b200.workloads import splitmix_uniform
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-11
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def close(gpu, ref, tol=TOL):
+    gpu = np.asarray(gpu, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    assert rel_l2(gpu, ref) <= tol, rel_l2(gpu, ref)
+    assert np.abs(gpu - ref).max() <= tol * np.abs(ref).max(), np.abs(gpu - ref).max() / np.abs(ref).max()
+
+
+def test_config1_exactly():
+    spec = cantilever(20, 10, 10, SolverOptions(tolerance=1e-10))
+    assert spec.coords.shape[0] == 2541 and spec.connectivity.shape[0] == 12000
+    prob, orc = EllipticProblem(spec), Oracle.from_spec(spec)
+    n = 3 * orc.N
+    z = np.full(orc.N, 0.5)
+    zd = prob.to_dev(z)
+    rm, cols = prob.pattern()
+    orm, ocols = orc.graph()
+    assert np.array_equal(host(rm), orm) and np.array_equal(host(cols), ocols)
+    assert ocols.size == 33621
+    zero = prob.to_dev(np.zeros(n))
+    close(host(prob.vf_value(zero, zd)), orc.vf_value(np.zeros(n), z))
+    us = np.sin(np.arange(n) * 0.37) * 1e-2
+    close(host(prob.vf_value(prob.to_dev(us), zd)), orc.vf_value(us, z))
+    K = prob.vf_gradient_u(zero, zd)
+    Ko = orc.vf_gradient_u(np.zeros(n), z)
+    close(host(K), Ko)
+    rhs = -prob.vf_value(zero, zd)
+    rhso = -orc.vf_value(np.zeros(n), z)
+    prob.apply_constraints(K, rhs, 1.0)
+    orc.apply_constraints(Ko, rhso, 1.0)
+    close(host(K), Ko)
+    close(host(rhs), rhso)
+    # Jacobi-PCG to 1e-10 on the recomputed FP64 residual
+    u, st = prob.solution(zd)
+    assert st["converged"] == 1 and st["relative_residual"] <= 1e-10 and st["fallback"] == 0, st
+    uh = host(u)
+    r = rhso - orc.matvec_plus(3, 3, Ko, uh, np.zeros(n))
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rhso)
+    uo, _, sto = orc.solution_refined(z, tol=1e-13)
+    assert sto["relative_residual"] <= 1e-13
+    assert rel_l2(uh, uo) <= 1e-8, rel_l2(uh, uo)
+    f = prob.criterion_value(zd, u)
+    fo = orc.sf_value(uh, z)
+    assert abs(f - fo) <= TOL * abs(fo)
+    g, _ = prob.criterion_gradient(zd, u)
+    close(host(g), orc.criterion_gradient(z, uh, self_adjoint=True))
+    prob.close()
+
+
+def test_config2_at_full_size():
+    spec = cantilever(160, 80, 80)
+    prob = EllipticProblem(spec)
+    orc = Oracle.from_spec(spec)
+    N = orc.N
+    assert 3 * N == 3_168_963 and orc.C == 6_144_000
+    z = splitmix_uniform(N, SEED_LARGE)
+    zd = prob.to_dev(z)
+    rm, cols = prob.pattern()
+    orm, ocols = orc.graph()
+    assert ocols.size == 15_584_961
+    assert np.array_equal(host(rm), orm) and np.array_equal(host(cols), ocols)
+    del rm, cols
+    # a smooth state of the size of the solution (cantilever bending plus a twist)
+    x = spec.coords
+    u = np.stack([-0.5 * x[:, 0] * (x[:, 1] - 0.5), -x[:, 0] ** 2 * (3.0 - x[:, 0]) * 0.5,
+                  0.1 * x[:, 0] * (x[:, 2] - 0.5)], axis=1).reshape(-1) * 10.0
+    ud = prob.to_dev(u)
+    close(host(prob.vf_value(ud, zd)), orc.vf_value(u, z))
+    K = host(prob.vf_gradient_u(ud, zd))
+    Ko = orc.vf_gradient_u(u, z)
+    close(K, Ko)
+    del K, Ko
+    f = prob.sf_value(ud, zd)
+    fo = orc.sf_value(u, z)
+    assert abs(f - fo) <= TOL * abs(fo)
+    g, _ = prob.criterion_gradient(zd, ud)
+    close(host(g), orc.criterion_gradient(z, u, self_adjoint=True))
+    lam = np.cos(np.arange(3 * N) * 1e-3)
+    out = prob.zeros(N)
+    prob.vf_gradient_z_apply(ud, zd, prob.to_dev(lam), out)
+    close(host(out), orc.matvec_plus(1, 3, orc.vf_gradient_z(u, z), lam, np.zeros(N)))
+    prob.close()
+
+
+def test_config4_member_sizes():
+    """One member of every config-4 size in one batch, solved to a 1e-10 residual so that the
+    error bar (1e-8 in u and dC/dz against u*) is met; the config's own 1e-8 residual
+    tolerance is checked on the same batch."""
+    rng = np.random.default_rng(SEED_BATCH)
+    specs, zs = [], []
+    for n in BATCH_SIZES:
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        mesh = box_mesh(n, n // 2, n // 2, 2.0, 1.0, 1.0)
+        specs.append(cantilever_spec(mesh, traction=tuple(float(v) for v in d), solver=method_options("chebyshev", 1e-10)))
+        zs.append(grf_density(n, n // 2, n // 2, rng=rng))
+    assert [3 * s.coords.shape[0] for s in specs] == [4131, 12675, 28611, 91875, 212355]
+    bp = EllipticProblem.batch(specs)
+    zd = bp.to_dev(np.concatenate(zs))
+    u, st = bp.solution(zd)
+    per = bp.batch_last_stats()
+    assert st["converged"] == 1 and all(m["relative_residual"] <= 1e-10 for m in per), per
+    g, _ = bp.criterion_gradient(zd, u)
+    uh, gh = host(u), host(g)
+    for s, sl in enumerate(bp.member_slices()):
+        orc = Oracle.from_spec(specs[s])
+        uo, _, sto = orc.solution_refined(zs[s], tol=1e-13)
+        assert sto["relative_residual"] <= 1e-13, (s, sto)
+        a, b = bp.node_offsets[s], bp.node_offsets[s + 1]
+        assert rel_l2(uh[sl], uo) <= 1e-8, (s, rel_l2(uh[sl], uo))
+        go = orc.criterion_gradient(zs[s], uo, self_adjoint=True)
+        assert rel_l2(gh[a:b], go) <= 1e-8, (s, rel_l2(gh[a:b], go))
+    # the config's own tolerance: every member's recomputed FP64 residual <= 1e-8
+    bp.set_solver(method_options("chebyshev", 1e-8))
+    u8, st8 = bp.solution(zd)
+    assert st8["converged"] == 1 and all(m["relative_residual"] <= 1e-8 for m in bp.batch_last_stats())
+    bp.close()

@@ -47,7 +47,7 @@ def setup():
     z = splitmix_uniform(spec.coords.shape[0], 0x5EED0003)
     prob = EllipticProblem(spec)
     orc = Oracle.from_spec(spec)
-    uo, _ = orc.solution(z, tol=1e-12)
+    uo, _, _ = orc.solution_refined(z, tol=1e-13)
     go = orc.criterion_gradient(z, uo)
     return spec, z, prob, orc, uo, go
 
@@ -147,3 +147,41 @@ def test_inhomogeneous_dirichlet_matrix_free_matches_assembled():
         u, st = prob.solution(prob.to_dev(z))
         assert st["converged"] == 1
         assert rel_l2(host(u), uo) <= 1e-8
+
+
+@pytest.mark.parametrize("kind", [capi.OPERATOR_ASSEMBLED, capi.OPERATOR_MATRIX_FREE])
+def test_failed_flexible_cg_falls_back_to_plain_fp64(setup, kind):
+    """A flexible-CG method that cannot meet the tolerance within its iteration cap hands the
+    solve to the plain FP64 Jacobi-PCG (from a zero guess, with its own cap); the answer is the
+    FP64 one.  With the fallback switched off the status is PLATO_NOT_CONVERGED."""
+    spec, z, prob, orc, uo, go = setup
+    zd = prob.to_dev(z)
+    opts = SolverOptions(tolerance=1e-10, max_iterations=2, operator_kind=kind,
+                         precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4, fallback_max_iterations=100000)
+    prob.set_solver(opts)
+    try:
+        u, st = prob.solution(zd)
+        assert st["converged"] == 1 and st["fallback"] == 2 and st["relative_residual"] <= 1e-10, st
+        assert rel_l2(host(u), uo) <= 1e-8
+        opts.fallback_max_iterations = -1
+        prob.set_solver(opts)
+        u, st = prob.solution(zd, raise_on_error=False)
+        assert st["rc"] == capi.NOT_CONVERGED and st["fallback"] == 0 and st["converged"] == 0
+    finally:
+        prob.set_solver(SolverOptions(tolerance=1e-10))
+
+
+def test_fallback_after_a_subspace_guess(setup):
+    """With a subspace (learned) guess the method is first retried from a zero guess; when that
+    fails too the plain FP64 method finishes the solve."""
+    spec, z, prob, orc, uo, go = setup
+    zd = prob.to_dev(z)
+    prob.set_solver(SolverOptions(tolerance=1e-10, max_iterations=2, precision=capi.PRECISION_MIXED_FP32,
+                                  chebyshev_degree=4, fallback_max_iterations=100000))
+    try:
+        W = np.stack([np.sin(np.arange(3 * orc.N) * 0.01 * (k + 1)) for k in range(3)])
+        u, st, _ = prob.solution_subspace(zd, prob.to_dev(W))
+        assert st["converged"] == 1 and st["fallback"] == 2, st
+        assert rel_l2(host(u), uo) <= 1e-8
+    finally:
+        prob.set_solver(SolverOptions(tolerance=1e-10))

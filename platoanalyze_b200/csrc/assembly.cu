@@ -1,4 +1,5 @@
-// Block-CRS assembly of the Jacobian K(z) (3x3 blocks) and of (dR/dz)^T (1x3 blocks), and
+// Block-CRS assembly of (dR/dz)^T (1x3 blocks), the warp-per-row Jacobian path for
+// high-valence rows (the thread-per-row kernel of assembly_rows.cu assembles the others), and
 // the symmetric Dirichlet elimination.
 //
 // The reference assembles cell by cell with one FP64 atomic per entry and finds each entry
@@ -77,16 +78,19 @@ __device__ __noinline__ void jacobian_row_atomic(const MeshView& m, const GraphV
     __syncwarp();
 }
 
+// Warp per block row over the rows in `rows` (count of them): the path for rows with more
+// blocks than the thread-per-row kernel (assembly_rows.cu) holds.
 __global__ void __launch_bounds__(kJacWarps * 32, 5)
 k_assemble_jacobian(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
-                    double* __restrict__ entries) {
+                    double* __restrict__ entries, const int32_t* __restrict__ rows, int32_t count) {
     __shared__ JacRowSmem sm[kJacWarps];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     JacRowSmem& S = sm[wib];
     const double c01 = mat.c01, c33 = mat.c33;
     const int64_t warps_total = (int64_t)gridDim.x * kJacWarps;
-    for (int64_t row = blockIdx.x * (int64_t)kJacWarps + wib; row < g.num_nodes; row += warps_total) {
+    for (int64_t it = blockIdx.x * (int64_t)kJacWarps + wib; it < count; it += warps_total) {
+        const int64_t row = rows[it];
         const int32_t rs = g.row_map[row];
         const int nbk = g.row_map[row + 1] - rs;
         const int32_t ks = g.n2c_ptr[row];
@@ -328,10 +332,12 @@ __global__ void k_matvec_plus(int32_t N, const int32_t* __restrict__ row_map,
 MeshView mesh_view(const plato_problem* h);
 GraphView graph_view(const plato_problem* h);
 
-int launch_assemble_jacobian(plato_problem* h, const double* z, double* entries) {
-    const int blocks = grid_for(h->N, kJacWarps, 148 * 5 * 8);
+int launch_assemble_jacobian_list(plato_problem* h, const double* z, double* entries, const int32_t* rows,
+                                  int32_t count) {
+    if (count <= 0) return PLATO_OK;
+    const int blocks = grid_for(count, kJacWarps, 148 * 5 * 8);
     k_assemble_jacobian<<<blocks, kJacWarps * 32, 0, h->stream>>>(mesh_view(h), graph_view(h), h->material, z,
-                                                                  entries);
+                                                                  entries, rows, count);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -23,7 +23,8 @@ int launch_dirichlet(plato_problem* h, double* A, double* rhs, double scale);
 int launch_matvec_plus(plato_problem* h, int rb, int cb, const double* A, const double* x, double* y);
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
 int build_sell_pattern(plato_problem* h);
-int prepare_operator(plato_problem* h, const double* crs);
+int prepare_operator(plato_problem* h, const double* crs, const double* z = nullptr);
+int assembly_direct_sell_ok(plato_problem* h, int* ok);
 int pcg_fp64(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
 int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* stats);
 int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* stats);
@@ -135,6 +136,7 @@ int plato_destroy(plato_problem* h) {
     cudaStreamSynchronize(h->stream);
     dfree(h->conn); dfree(h->coords); dfree(h->row_map); dfree(h->cols); dfree(h->diag);
     dfree(h->n2c_ptr); dfree(h->n2c); dfree(h->F); dfree(h->bc_dofs); dfree(h->bc_values);
+    dfree(h->asm_plan); dfree(h->asm_wide);
     dfree(h->bc_mask); dfree(h->K); dfree(h->KT); dfree(h->v_r); dfree(h->v_z); dfree(h->v_p);
     dfree(h->v_Ap); dfree(h->v_dinv); dfree(h->v_b); dfree(h->v_x); dfree(h->v_tmp);
     dfree(h->partials); dfree(h->cellbuf); dfree(h->scal); dfree(h->red_out); dfree(h->red_ticket);
@@ -462,7 +464,7 @@ int plato_apply_operator(plato_problem* h, const double* z, int32_t operator_kin
     RC(dmalloc(h, &h->K, 9 * h->nblocks));
     RC(launch_assemble_jacobian(h, z, h->K));
     RC(launch_dirichlet(h, h->K, nullptr, 0.0));
-    RC(prepare_operator(h, h->K));
+    RC(prepare_operator(h, h->K, z));
     return launch_sell_spmv(h, h->sell64, x, y);
 }
 
@@ -599,7 +601,7 @@ static int fallback_solve(plato_problem* h, double* x, plato_solve_stats* st, in
         RC(dmalloc(h, &h->K, 9 * h->nblocks));
         RC(launch_assemble_jacobian(h, z, h->K));
         RC(launch_dirichlet(h, h->K, nullptr, 0.0));
-        RC(prepare_operator(h, h->K));
+        RC(prepare_operator(h, h->K, z));
     }
     // the SELL FP64 copy and its Jacobi diagonal were made for the flexible CG's operator
     const int32_t saved = h->opts.max_iterations;
@@ -629,25 +631,35 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         if (rc != PLATO_NOT_CONVERGED && rc != PLATO_NONFINITE) return rc;
         return fallback_solve(h, x, st, rc, z);
     }
-    RC(dmalloc(h, &h->K, 9 * h->nblocks));
-    if (h->timing) {
+    // Homogeneous essential BCs and no high-valence rows: the solver's SELL copies are assembled
+    // straight from z with the constraints applied (no CRS copy); otherwise K is assembled into
+    // the block CRS, constrained there (lifting inhomogeneous values) and converted.
+    int direct = 0;
+    RC(assembly_direct_sell_ok(h, &direct));
+    if (h->timing)
         for (cudaEvent_t& e : h->asm_ev)
             if (!e) PLATO_CUDA(h, cudaEventCreate(&e));
-        PLATO_CUDA(h, cudaEventRecord(h->asm_ev[0], h->stream));
+    const double* crs = nullptr;
+    if (direct) {
+        RC(launch_dirichlet_rhs(h, h->v_b, bc_scale));
+    } else {
+        RC(dmalloc(h, &h->K, 9 * h->nblocks));
+        if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[0], h->stream));
+        RC(launch_assemble_jacobian(h, z, h->K));
+        if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[1], h->stream));
+        RC(launch_dirichlet(h, h->K, h->v_b, bc_scale));
+        crs = h->K;
     }
-    RC(launch_assemble_jacobian(h, z, h->K));
-    if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[1], h->stream));
-    RC(launch_dirichlet(h, h->K, h->v_b, bc_scale));
     int rc;
     if (h->batch.nseg > 0) {  // member-wise flexible CG over the union (Jacobi when no degree is set)
-        RC(prepare_mixed(h, h->K, z));
+        RC(prepare_mixed(h, crs, z));
         rc = fcg_batch(h, h->v_b, x, st);
     } else if (plain_method(h->opts)) {
-        RC(prepare_operator(h, h->K));
+        RC(prepare_operator(h, crs, z));
         RC(ritz_guess(h, h->v_b, x));
         rc = pcg_fp64(h, h->v_b, x, st);
     } else {
-        RC(prepare_mixed(h, h->K, z));
+        RC(prepare_mixed(h, crs, z));
         RC(prepare_coarse(h, z));
         RC(ritz_guess(h, h->v_b, x));
         rc = fcg_poly(h, h->v_b, x, st);

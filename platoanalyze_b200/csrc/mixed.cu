@@ -29,6 +29,9 @@
 
 namespace plato {
 
+int launch_assemble_sell(plato_problem* h, const double* z, double* v64, float* v32, void* v16, double* dinv,
+                         float* dinv32);
+
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
 int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, double* host_result);
 int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float* out32, void* out16,
@@ -578,8 +581,9 @@ static ChebCoef chebyshev(double lmax, double ratio, int degree) {
     return c;
 }
 
-// Prepares the operators for a polynomial-preconditioned solve with control z (assembled
-// path: h->K holds the constrained CRS matrix).
+// Prepares the operators for a polynomial-preconditioned solve with control z.  Assembled
+// operator: from the constrained CRS matrix crs, or -- crs == nullptr -- assembled straight
+// into the solver's SELL copies from z (thread-per-row assembly with the constraints applied).
 int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
     const int64_t n = 3 * (int64_t)h->N;
     for (float** v : {&h->f_res, &h->f_d0, &h->f_d1, &h->f_y, &h->f_w, &h->f_dinv})
@@ -601,12 +605,14 @@ int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
         if (!h->sell16s) PLATO_CUDA(h, cudaMalloc(&h->sell16s, sizeof(__half) * slots));
         for (float** v : {&h->f_sq, &h->f_isq})
             if (!*v) PLATO_CUDA(h, cudaMalloc(v, sizeof(float) * n));
-        int rc = launch_crs_to_sell(h, crs, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
+        int rc = crs ? launch_crs_to_sell(h, crs, h->sell64, nullptr, nullptr, h->v_dinv, nullptr)
+                     : launch_assemble_sell(h, z, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
         if (rc) return rc;
         // the Jacobi diagonal of the scaled matrix is 1: f_dinv = ones
         return launch_sell_scale16(h, h->sell64, h->v_dinv, h->sell16s, h->f_sq, h->f_isq, h->f_dinv);
     }
-    return launch_crs_to_sell(h, crs, h->sell64, o32, o16, h->v_dinv, h->f_dinv);
+    return crs ? launch_crs_to_sell(h, crs, h->sell64, o32, o16, h->v_dinv, h->f_dinv)
+               : launch_assemble_sell(h, z, h->sell64, o32, o16, h->v_dinv, h->f_dinv);
 }
 
 // Two-level preconditioner data for control z (mesh buckets once, Galerkin operator per solve).

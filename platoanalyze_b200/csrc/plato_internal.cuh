@@ -189,6 +189,11 @@ struct plato_problem {
     double   bbox_min[3] = {0, 0, 0};
     double   bbox_max[3] = {0, 0, 0};
     CoarseSpace coarse{};
+    // thread-per-row assembly plan (assembly_rows.cu, once per mesh): three 4-bit slots per
+    // n2c entry, and the rows with too many blocks for it
+    uint16_t* asm_plan = nullptr;
+    int32_t*  asm_wide = nullptr;  // [N + 1]: wide rows, then their count at [N]
+    int32_t   asm_nwide = 0;
     // assembled operator (allocated on first use)
     double* K = nullptr;           // 9*nblocks
     double* KT = nullptr;          // scratch for transposed / gradient_z matrices

@@ -21,6 +21,8 @@ namespace plato {
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
 int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float* out32, void* out16,
                        double* dinv, float* dinv32);
+int launch_assemble_sell(plato_problem* h, const double* z, double* v64, float* v32, void* v16, double* dinv,
+                         float* dinv32);
 
 namespace {
 
@@ -287,9 +289,11 @@ int launch_sell_spmv(plato_problem* h, const double* vals, const double* x, doub
     return PLATO_OK;
 }
 
-// Makes the SELL copy (and Jacobi diagonal) of a constrained CRS matrix.
-int prepare_operator(plato_problem* h, const double* crs) {
+// Makes the SELL copy (and Jacobi diagonal) of a constrained CRS matrix, or -- crs == nullptr
+// -- assembles it straight from the control z with the constraints applied.
+int prepare_operator(plato_problem* h, const double* crs, const double* z) {
     if (!h->sell64) PLATO_CUDA(h, cudaMalloc(&h->sell64, sizeof(double) * 9 * size_t(h->sell.total_slots)));
+    if (!crs) return launch_assemble_sell(h, z, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
     return launch_crs_to_sell(h, crs, h->sell64, nullptr, nullptr, h->v_dinv, nullptr);
 }
 

@@ -653,6 +653,18 @@ def main():
                  "pcg_iterations": [s["iterations"] for s in pstats]}
         prob.set_solver(solver_options(args.method, args.tol, args.size))
 
+    # secondary figure: Self-Adjoint = false, the adjoint K^T lambda = -df/du solved explicitly
+    # by the same method (Problem::criterionGradient, src/elliptic/Problem.hpp:428-448)
+    explicit_adjoint = None
+    o = solver_options(args.method, args.tol, args.size)
+    o.self_adjoint = False
+    prob.set_solver(o)
+    step()
+    ms_ea, (_, _, g_ea, _), _ = timed_steps(2)
+    prob.set_solver(solver_options(args.method, args.tol, args.size))
+    explicit_adjoint = {"value": world * 2 / (ms_ea / 1e3), "unit": UNIT, "ms_per_step": ms_ea / 2,
+                        "dcdz_rel_diff_vs_self_adjoint": float((g_ea - g).norm() / g.norm())}
+
     # accuracy against the oracle: its full FP64 solve of the problem (timed: the CPU baseline on
     # all host threads), refined with a long double iterate to a relative residual <= 1e-13
     # (untimed; u* and dC/dz* of the error definitions)
@@ -682,6 +694,7 @@ def main():
     if plain:
         cfg["plain_fp64_gpu"] = plain
         cfg["speedup_vs_plain_fp64_gpu"] = value / plain["value"]
+    cfg["explicit_adjoint"] = explicit_adjoint
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,

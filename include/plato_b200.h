@@ -148,6 +148,18 @@ const char* plato_last_error(const plato_problem* h);
 /* Bind the handle to a CUDA stream (cudaStream_t); NULL means the legacy default stream. */
 int plato_set_stream(plato_problem* h, void* cuda_stream);
 int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* opts);
+/* Control layout (no reference counterpart: the reference's control is nodal and each cell
+ * takes the mean of its nodes, ApplyWeighting, src/ApplyWeighting.hpp:55-64).
+ * PLATO_CONTROL_ELEMENT gives every cell its own density: from then on every entry point's
+ * control z has num_cells entries (cell order) and every control derivative (sf_gradient_z,
+ * vf_gradient_z_apply, problem_criterion_gradient, volume_gradient_z) has num_cells entries,
+ * d/dz_e of the cell's own terms.  The (dR/dz)^T block matrix (vf_gradient_z) and batches
+ * are nodal only (PLATO_NOT_SUPPORTED). */
+typedef enum plato_control_layout {
+    PLATO_CONTROL_NODAL   = 0,
+    PLATO_CONTROL_ELEMENT = 1
+} plato_control_layout;
+int plato_set_control_layout(plato_problem* h, int32_t layout);
 int plato_get_sizes(const plato_problem* h, int32_t* num_nodes, int32_t* num_cells,
                     int64_t* num_blocks);
 /* Instrumentation (no reference counterpart; the reference times phases with

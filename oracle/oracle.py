@@ -24,7 +24,7 @@ class OracleProblem(C.Structure):
                 ("penalty_exponent", C.c_double), ("penalty_minimum", C.c_double),
                 ("num_traction_faces", C.c_int32), ("face_cells", i32p), ("face_local_nodes", i32p),
                 ("traction", C.c_double * 3), ("num_bc_dofs", C.c_int32), ("bc_dofs", i32p),
-                ("bc_values", f64p)]
+                ("bc_values", f64p), ("cell_control", C.c_int32)]
 
 
 class OracleStats(C.Structure):
@@ -96,7 +96,7 @@ class Oracle:
     """FP64 CPU restatement of the reference path on one mesh + material + BCs."""
 
     def __init__(self, coords, connectivity, E=1.0, nu=0.3, p=3.0, rho_min=1e-9,
-                 traction_faces=None, traction=(0.0, 0.0, 0.0), bc_dofs=None, bc_values=None):
+                 traction_faces=None, traction=(0.0, 0.0, 0.0), bc_dofs=None, bc_values=None, cell_control=False):
         self.coords = np.ascontiguousarray(coords, dtype=np.float64)
         self.conn = np.ascontiguousarray(connectivity, dtype=np.int32)
         if traction_faces is None:
@@ -121,17 +121,19 @@ class Oracle:
         P.num_bc_dofs = self.bc_dofs.size
         P.bc_dofs = self.bc_dofs.ctypes.data_as(i32p)
         P.bc_values = self.bc_values.ctypes.data_as(f64p)
+        P.cell_control = int(bool(cell_control))
         self.P = P
         self.N = P.num_nodes
         self.C = P.num_cells
+        self.nz = self.C if cell_control else self.N  # control entries
         self._graph = None
 
     @classmethod
-    def from_spec(cls, spec) -> "Oracle":
+    def from_spec(cls, spec, cell_control=False) -> "Oracle":
         (fc, fl, vec) = spec.tractions[0] if spec.tractions else (None, None, (0.0, 0.0, 0.0))
         return cls(spec.coords, spec.connectivity, spec.youngs_modulus, spec.poissons_ratio,
                    spec.penalty_exponent, spec.penalty_minimum,
-                   (fc, fl) if fc is not None else None, vec, spec.bc_dofs, spec.bc_values)
+                   (fc, fl) if fc is not None else None, vec, spec.bc_dofs, spec.bc_values, cell_control)
 
     def cell_fields(self, u):
         u = np.ascontiguousarray(u, dtype=np.float64)
@@ -184,7 +186,7 @@ class Oracle:
         return g
 
     def sf_gradient_z(self, u, z):
-        g = np.empty(self.N)
+        g = np.empty(self.nz)
         lib.oracle_sf_gradient_z(C.byref(self.P), _p(np.ascontiguousarray(u, np.float64)),
                                  _p(np.ascontiguousarray(z, np.float64)), _p(g))
         return g
@@ -241,7 +243,7 @@ class Oracle:
                    "converged": st.converged}
 
     def criterion_gradient(self, z, u, self_adjoint=True, tol=1e-10, max_it=100000):
-        g = np.empty(self.N)
+        g = np.empty(self.nz)
         st = OracleStats()
         lib.oracle_problem_criterion_gradient(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)),
                                               _p(np.ascontiguousarray(u, np.float64)), int(self_adjoint), tol,
@@ -252,7 +254,7 @@ class Oracle:
         return lib.oracle_volume_value(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)), p, m)
 
     def volume_gradient_z(self, z, p=1.0, m=0.0):
-        g = np.empty(self.N)
+        g = np.empty(self.nz)
         lib.oracle_volume_gradient_z(C.byref(self.P), _p(np.ascontiguousarray(z, np.float64)), p, m, _p(g))
         return g
 

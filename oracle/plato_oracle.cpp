@@ -111,12 +111,16 @@ void stress_of(const double C[6][6], const double eps[6], double sig[6]) {
     }
 }
 
-/* ApplyWeighting cell density, src/ApplyWeighting.hpp:55-60. */
-double cell_density(const double* z, const int32_t* n) {
+/* ApplyWeighting cell density, src/ApplyWeighting.hpp:55-60: the mean of the cell's nodal
+ * control; with element control (no reference counterpart) the cell's own entry. */
+double cell_density(const oracle_problem* P, const double* z, int32_t c, const int32_t* n) {
+    if (P->cell_control) return z[c];
     double rho = 0.0;
     for (int a = 0; a < kNodesPerCell; ++a) rho += z[n[a]];
     return rho / kNodesPerCell;
 }
+/* d rho_c / d z: 1/4 per node of the cell, or 1 for the cell's own entry */
+double density_dz(const oracle_problem* P) { return P->cell_control ? 1.0 : 1.0 / kNodesPerCell; }
 
 /* MSIMP::operator(), src/Simp.hpp:130-134. */
 double msimp(const oracle_problem* P, double rho) {
@@ -159,7 +163,7 @@ void cell_residual(const oracle_problem* P, const double C[6][6], int32_t c, con
     gather_cell_state(u, n, ue);
     strain_of(G, ue, eps);
     stress_of(C, eps, sig);
-    const double s = msimp(P, cell_density(z, n));
+    const double s = msimp(P, cell_density(P, z, c, n));
     for (int v = 0; v < kVoigt; ++v) sig[v] *= s;
     for (int k = 0; k < 12; ++k) out[k] = 0.0;
     divergence_add(G, sig, out);
@@ -173,7 +177,7 @@ void cell_stiffness(const oracle_problem* P, const double C[6][6], int32_t c, co
     CellGeom G;
     cell_geometry(P, c, G);
     const int32_t* n = P->connectivity + 4 * (int64_t)c;
-    const double s = msimp(P, cell_density(z, n));
+    const double s = msimp(P, cell_density(P, z, c, n));
     for (int j = 0; j < kDofsPerCell; ++j) {
         double seed[12] = {0};
         seed[j] = 1.0;
@@ -407,7 +411,7 @@ void oracle_vf_gradient_z(const oracle_problem* P, const double* u, const double
         strain_of(G, ue, eps);
         stress_of(C, eps, sig);
         /* cell density rho = sum(z)/4 has d rho/d z_k = 1/4 for every local node k */
-        const double sdx = msimp_dx(P, cell_density(z, nd)) * (1.0 / kNodesPerCell);
+        const double sdx = msimp_dx(P, cell_density(P, z, c, nd)) * density_dz(P);
         double dsig[6], dres[12] = {0};
         for (int v = 0; v < 6; ++v) dsig[v] = sig[v] * sdx;
         divergence_add(G, dsig, dres);
@@ -436,7 +440,7 @@ double oracle_sf_value(const oracle_problem* P, const double* u, const double* z
         gather_cell_state(u, nd, ue);
         strain_of(G, ue, eps);
         stress_of(C, eps, sig);
-        const double s = msimp(P, cell_density(z, nd));
+        const double s = msimp(P, cell_density(P, z, c, nd));
         for (int v = 0; v < 6; ++v) sig[v] *= s;
         double inc = 0.0;
         for (int v = 0; v < 6; ++v) inc += sig[v] * eps[v];
@@ -460,7 +464,7 @@ void oracle_sf_gradient_u(const oracle_problem* P, const double* u, const double
         gather_cell_state(u, nd, ue);
         strain_of(G, ue, eps);
         stress_of(C, eps, sig);
-        const double s = msimp(P, cell_density(z, nd));
+        const double s = msimp(P, cell_density(P, z, c, nd));
         for (int v = 0; v < 6; ++v) sig[v] *= s;
         for (int j = 0; j < 12; ++j) {
             double seed[12] = {0};
@@ -481,7 +485,7 @@ void oracle_sf_gradient_u(const oracle_problem* P, const double* u, const double
 void oracle_sf_gradient_z(const oracle_problem* P, const double* u, const double* z, double* dfdz) {
     double C[6][6];
     material_matrix(P, C);
-    std::fill(dfdz, dfdz + (int64_t)P->num_nodes, 0.0);
+    std::fill(dfdz, dfdz + (int64_t)(P->cell_control ? P->num_cells : P->num_nodes), 0.0);
 #pragma omp parallel for schedule(static)
     for (int32_t c = 0; c < P->num_cells; ++c) {
         CellGeom G;
@@ -491,11 +495,13 @@ void oracle_sf_gradient_z(const oracle_problem* P, const double* u, const double
         gather_cell_state(u, nd, ue);
         strain_of(G, ue, eps);
         stress_of(C, eps, sig);
-        const double sdx = msimp_dx(P, cell_density(z, nd)) * (1.0 / kNodesPerCell);
+        const double sdx = msimp_dx(P, cell_density(P, z, c, nd)) * density_dz(P);
         double dinc = 0.0;
         for (int v = 0; v < 6; ++v) dinc += (sig[v] * sdx) * eps[v];
         const double val = 0.5 * dinc * G.vol;
-        for (int k = 0; k < 4; ++k) atomic_add(&dfdz[nd[k]], val);
+        if (P->cell_control) dfdz[c] = val;
+        else
+            for (int k = 0; k < 4; ++k) atomic_add(&dfdz[nd[k]], val);
     }
 }
 
@@ -522,7 +528,7 @@ double oracle_volume_value(const oracle_problem* P, const double* z, double p, d
 #pragma omp parallel for reduction(+ : total) schedule(static)
     for (int32_t c = 0; c < P->num_cells; ++c) {
         double v = cell_volume(P, c);
-        v *= msimp(&Q, cell_density(z, P->connectivity + 4 * (int64_t)c));
+        v *= msimp(&Q, cell_density(P, z, c, P->connectivity + 4 * (int64_t)c));
         total += v;
     }
     return total;
@@ -532,12 +538,14 @@ void oracle_volume_gradient_z(const oracle_problem* P, const double* z, double p
     oracle_problem Q = *P;
     Q.penalty_exponent = p;
     Q.penalty_minimum = m;
-    std::fill(dvdz, dvdz + (int64_t)P->num_nodes, 0.0);
+    std::fill(dvdz, dvdz + (int64_t)(P->cell_control ? P->num_cells : P->num_nodes), 0.0);
 #pragma omp parallel for schedule(static)
     for (int32_t c = 0; c < P->num_cells; ++c) {
         const int32_t* nd = P->connectivity + 4 * (int64_t)c;
-        const double val = cell_volume(P, c) * (msimp_dx(&Q, cell_density(z, nd)) * (1.0 / kNodesPerCell));
-        for (int k = 0; k < 4; ++k) atomic_add(&dvdz[nd[k]], val);
+        const double val = cell_volume(P, c) * (msimp_dx(&Q, cell_density(P, z, c, nd)) * density_dz(P));
+        if (P->cell_control) dvdz[c] = val;
+        else
+            for (int k = 0; k < 4; ++k) atomic_add(&dvdz[nd[k]], val);
     }
 }
 
@@ -869,6 +877,28 @@ int oracle_problem_criterion_gradient(const oracle_problem* P, const double* z, 
         oracle_solve_stats local;
         rc = oracle_pcg_jacobi(P->num_nodes, rm.data(), cols.data(), JT.data(), dfdu.data(),
                                lambda.data(), tol, max_it, st ? st : &local);
+    }
+    if (P->cell_control) {  /* (dR/dz_c)^T lambda = s'(rho_c) lambda_e . (K_e^0 u_e), per cell */
+        double C[6][6];
+        material_matrix(P, C);
+#pragma omp parallel for schedule(static)
+        for (int32_t c = 0; c < P->num_cells; ++c) {
+            CellGeom G;
+            cell_geometry(P, c, G);
+            const int32_t* nd = P->connectivity + 4 * (int64_t)c;
+            double ue[12], le[12], eps[6], sig[6], dres[12] = {0};
+            gather_cell_state(u, nd, ue);
+            gather_cell_state(lambda.data(), nd, le);
+            strain_of(G, ue, eps);
+            stress_of(C, eps, sig);
+            const double sdx = msimp_dx(P, cell_density(P, z, c, nd));
+            for (int v = 0; v < 6; ++v) sig[v] *= sdx;
+            divergence_add(G, sig, dres);
+            double t = 0.0;
+            for (int i = 0; i < 12; ++i) t += dres[i] * le[i];
+            dfdz[c] += t;
+        }
+        return rc;
     }
     std::vector<double> dRdz(3 * cols.size());
     oracle_vf_gradient_z(P, u, z, rm.data(), cols.data(), dRdz.data());

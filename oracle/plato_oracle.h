@@ -41,6 +41,8 @@ typedef struct oracle_problem {
     int32_t        num_bc_dofs;
     const int32_t* bc_dofs;
     const double*  bc_values;
+    int32_t        cell_control;      /* 0: nodal control (ApplyWeighting mean); 1: one density per
+                                         cell, z and dz have num_cells entries */
 } oracle_problem;
 
 typedef struct oracle_solve_stats {

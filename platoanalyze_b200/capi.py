@@ -10,6 +10,7 @@ from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libplato_b200.so"
 
+CONTROL_NODAL, CONTROL_ELEMENT = 0, 1
 OK, BAD_INPUT, NOT_CONVERGED, NONFINITE, DEVICE_TIMEOUT, CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED = range(8)
 LAYOUT_SCALAR_FIELD, LAYOUT_SCALAR_VALUE, LAYOUT_SCALAR_PARAMETER = range(3)
 STATUS_NAMES = ["OK", "BAD_INPUT", "NOT_CONVERGED", "NONFINITE", "DEVICE_TIMEOUT", "CUDA_ERROR",
@@ -89,6 +90,7 @@ def _load() -> C.CDLL:
         "plato_last_error": ([vp], C.c_char_p),
         "plato_set_stream": ([vp, vp], C.c_int),
         "plato_set_solver_opts": ([vp, C.POINTER(SolverOpts)], C.c_int),
+        "plato_set_control_layout": ([vp, C.c_int32], C.c_int),
         "plato_set_timing": ([vp, C.c_int32], C.c_int),
         "plato_get_instrumentation": ([vp, C.POINTER(C.c_int64), f64p, C.POINTER(C.c_int64)], C.c_int),
         "plato_reset_instrumentation": ([vp], C.c_int),

@@ -64,7 +64,7 @@ __device__ __noinline__ void jacobian_row_atomic(const MeshView& m, const GraphV
         load_cell_coords(m.coords, n, x);
         TetGeom<double> G;
         tet_geometry(x, G);
-        const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+        const double rho = cell_rho(mat, z, c, n);
         const double w = G.vol * simp(mat, rho);
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
@@ -118,7 +118,7 @@ k_assemble_jacobian(MeshView m, GraphView g, Material mat, const double* __restr
             load_cell_coords(m.coords, n, x);
             TetGeom<double> G;
             tet_geometry(x, G);
-            const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+            const double rho = cell_rho(mat, z, packed >> 2, n);
             const double w = G.vol * simp(mat, rho);
             double ga[3];
 #pragma unroll
@@ -235,7 +235,7 @@ k_assemble_dRdz_rows(MeshView m, GraphView g, Material mat, const double* __rest
             load_cell_coords(m.coords, n, x);
             TetGeom<double> G;
             tet_geometry(x, G);
-            const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+            const double rho = cell_rho(mat, z, c, n);
             double ue[4][3], e[6], s[6];
             const int ids[4] = {n.x, n.y, n.z, n.w};
 #pragma unroll
@@ -244,7 +244,7 @@ k_assemble_dRdz_rows(MeshView m, GraphView g, Material mat, const double* __rest
                 for (int d = 0; d < 3; ++d) ue[a][d] = __ldg(u + 3 * (int64_t)ids[a] + d);
             strain_voigt(G.g, ue, e);
             stress_voigt(mat, e, s);
-            const double w = G.vol * simp_dx(mat, rho) * 0.25;
+            const double w = G.vol * simp_dx(mat, rho) * rho_dz(mat);
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 double f[3];

@@ -124,7 +124,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 xr[0] = __ldg(m.coords + 3 * (int64_t)r);
                 xr[1] = __ldg(m.coords + 3 * (int64_t)r + 1);
                 xr[2] = __ldg(m.coords + 3 * (int64_t)r + 2);
-                zr = __ldg(z + r);
+                zr = mat.cell_control ? 0.0 : __ldg(z + r);
             } else {
                 nb = 0;  // wide row: assembled by the warp-per-row kernel
             }
@@ -168,7 +168,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 const double j11 = __ldg(c0) - xr[0], j21 = __ldg(c0 + 1) - xr[1], j31 = __ldg(c0 + 2) - xr[2];
                 const double j12 = __ldg(c1) - xr[0], j22 = __ldg(c1 + 1) - xr[1], j32 = __ldg(c1 + 2) - xr[2];
                 const double j13 = __ldg(c2) - xr[0], j23 = __ldg(c2 + 1) - xr[1], j33 = __ldg(c2 + 2) - xr[2];
-                const double rho = (__ldg(z + i0) + __ldg(z + i1) + __ldg(z + i2) + zr) * 0.25;
+                const double rho = mat.cell_control ? __ldg(z + (p >> 2)) : (__ldg(z + i0) + __ldg(z + i1) + __ldg(z + i2) + zr) * 0.25;
                 // ComputeGradientWorkset<3> (src/ImplicitFunctors.hpp:169-221) with x_3 = the row node
                 const double c11 = j22 * j33 - j23 * j32, c12 = j13 * j32 - j12 * j33, c13 = j12 * j23 - j13 * j22;
                 const double detj = j11 * c11 + j21 * c12 + j31 * c13;

@@ -309,6 +309,16 @@ int plato_set_stream(plato_problem* h, void* stream) {
     return PLATO_OK;
 }
 
+int plato_set_control_layout(plato_problem* h, int32_t layout) {
+    if (!h) return plato_fail(nullptr, PLATO_BAD_INPUT, "null handle");
+    if (layout != PLATO_CONTROL_NODAL && layout != PLATO_CONTROL_ELEMENT)
+        return plato_fail(h, PLATO_BAD_INPUT, "unknown control layout");
+    if (layout == PLATO_CONTROL_ELEMENT && (h->batch.nseg > 0 || h->physics != 0))
+        return plato_fail(h, PLATO_NOT_SUPPORTED, "element control is for single elastostatic problems");
+    h->material.cell_control = layout == PLATO_CONTROL_ELEMENT ? 1 : 0;
+    return PLATO_OK;
+}
+
 int plato_set_solver_opts(plato_problem* h, const plato_solver_opts* o) {
     NEED(h, o != nullptr, "null solver options");
     RC(check_opts(h, *o));
@@ -392,6 +402,8 @@ int plato_vf_gradient_u_T(plato_problem* h, const double* u, const double* z, do
 }
 
 int plato_vf_gradient_z(plato_problem* h, const double* u, const double* z, double* entries) {
+    if (h && h->material.cell_control)
+        return plato_fail(h, PLATO_NOT_SUPPORTED, "the (dR/dz)^T block matrix needs nodal control");
     NEED(h, u && z && entries, "null device pointer");
     return launch_assemble_gradient_z(h, u, z, entries);
 }
@@ -419,8 +431,9 @@ int plato_sf_gradient_z(plato_problem* h, const double* u, const double* z, doub
     return launch_nodal_control_derivative(h, 1, u, z, nullptr, h->cellbuf, dfdz, 0);
 }
 
-static Material volume_penalty(const plato_penalty* p) {
+static Material volume_penalty(const plato_penalty* p, const plato_problem* h) {
     Material m{};
+    m.cell_control = h->material.cell_control;
     m.p = p->exponent;
     m.rho_min = p->minimum_value;
     m.p_int = (p->exponent >= 0.0 && p->exponent <= 16.0 && std::floor(p->exponent) == p->exponent)
@@ -431,7 +444,7 @@ static Material volume_penalty(const plato_penalty* p) {
 int plato_volume_value(plato_problem* h, const double* z, const plato_penalty* penalty, double* value) {
     NEED(h, z && penalty && value, "null pointer");
     NEED(h, std::isfinite(penalty->exponent) && std::isfinite(penalty->minimum_value), "non-finite penalty");
-    RC(launch_volume(h, volume_penalty(penalty), z, h->red_out));
+    RC(launch_volume(h, volume_penalty(penalty, h), z, h->red_out));
     PLATO_CUDA(h, cudaMemcpyAsync(value, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
     return PLATO_OK;
@@ -440,7 +453,7 @@ int plato_volume_value(plato_problem* h, const double* z, const plato_penalty* p
 int plato_volume_gradient_z(plato_problem* h, const double* z, const plato_penalty* penalty, double* dvdz) {
     NEED(h, z && penalty && dvdz, "null pointer");
     NEED(h, std::isfinite(penalty->exponent) && std::isfinite(penalty->minimum_value), "non-finite penalty");
-    return launch_volume_gradient(h, volume_penalty(penalty), z, dvdz);
+    return launch_volume_gradient(h, volume_penalty(penalty, h), z, dvdz);
 }
 
 int plato_apply_constraints(plato_problem* h, double* entries, double* rhs, double scale) {
@@ -542,11 +555,14 @@ int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host
                                           plato_solve_stats* stats) {
     NEED(h, z_host != nullptr, "null control");
     const int64_t n = 3 * int64_t(h->N);
-    RC(dmalloc(h, &h->d_z_in, h->N));
+    // control entries: one per node, or one per cell with element control (buffers sized for both)
+    const int64_t nz = h->material.cell_control ? h->C : h->N;
+    const int64_t zcap = h->C > h->N ? h->C : h->N;
+    RC(dmalloc(h, &h->d_z_in, zcap));
     RC(dmalloc(h, &h->d_u_out, n));
-    RC(dmalloc(h, &h->d_g_out, h->N));
+    RC(dmalloc(h, &h->d_g_out, zcap));
     cudaStream_t s = h->stream;
-    PLATO_CUDA(h, cudaMemcpyAsync(h->d_z_in, z_host, sizeof(double) * h->N, cudaMemcpyHostToDevice, s));
+    PLATO_CUDA(h, cudaMemcpyAsync(h->d_z_in, z_host, sizeof(double) * nz, cudaMemcpyHostToDevice, s));
     const double* u0 = nullptr;
     if (u0_host) {
         PLATO_CUDA(h, cudaMemcpyAsync(h->d_u_out, u0_host, sizeof(double) * n, cudaMemcpyHostToDevice, s));
@@ -561,7 +577,7 @@ int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host
     if (dfdz_host) {
         plato_solve_stats adj{};
         RC(plato_problem_criterion_gradient(h, h->d_z_in, h->d_u_out, h->d_g_out, &adj));
-        PLATO_CUDA(h, cudaMemcpyAsync(dfdz_host, h->d_g_out, sizeof(double) * h->N, cudaMemcpyDeviceToHost, s));
+        PLATO_CUDA(h, cudaMemcpyAsync(dfdz_host, h->d_g_out, sizeof(double) * nz, cudaMemcpyDeviceToHost, s));
     }
     if (u_host) PLATO_CUDA(h, cudaMemcpyAsync(u_host, h->d_u_out, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));

@@ -158,12 +158,13 @@ k_galerkin_fast(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, 
     for (int base = e0; base < e1; base += kFastBatch) {
         const int nb = min(kFastBatch, e1 - base);
         if (tid < nb) {
-            const int4 nd = conn[elem_list[base + tid]];
+            const int32_t cell = elem_list[base + tid];
+            const int4 nd = conn[cell];
             double x[4][3];
             load_cell_coords(coords, nd, x);
             TetGeom<double> G;
             tet_geometry(x, G);
-            const double rho = (z[nd.x] + z[nd.y] + z[nd.z] + z[nd.w]) * 0.25;
+            const double rho = cell_rho(mat, z, cell, nd);
             double* row = Gs + tid * 25;
             row[0] = G.vol * simp(mat, rho);
             const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
@@ -280,12 +281,13 @@ k_galerkin(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, const
     const int k = threadIdx.x >> 3, J = threadIdx.x & 7;  // staging: element k of the batch, corner J
     for (int base = e0; base < e1; base += kBatch) {
         if (base + k < e1) {
-            const int4 nd = conn[elem_list[base + k]];
+            const int32_t cell = elem_list[base + k];
+            const int4 nd = conn[cell];
             double x[4][3];
             load_cell_coords(coords, nd, x);
             TetGeom<double> G;
             tet_geometry(x, G);
-            const double rho = (z[nd.x] + z[nd.y] + z[nd.z] + z[nd.w]) * 0.25;
+            const double rho = cell_rho(mat, z, cell, nd);
             const double w = G.vol * simp(mat, rho);
             const int ids[4] = {nd.x, nd.y, nd.z, nd.w};
             double wa[4];

@@ -15,13 +15,13 @@ struct CellState {
     double rho;  // mean nodal control, ApplyWeighting (src/ApplyWeighting.hpp:55-60)
 };
 
-__device__ __forceinline__ void load_cell(const MeshView& m, const double* __restrict__ z, int64_t c,
-                                          CellState& cs) {
+__device__ __forceinline__ void load_cell(const MeshView& m, const Material& mat, const double* __restrict__ z,
+                                          int64_t c, CellState& cs) {
     cs.n = m.conn[c];
     double x[4][3];
     load_cell_coords(m.coords, cs.n, x);
     tet_geometry(x, cs.G);
-    cs.rho = (__ldg(z + cs.n.x) + __ldg(z + cs.n.y) + __ldg(z + cs.n.z) + __ldg(z + cs.n.w)) * 0.25;
+    cs.rho = cell_rho(mat, z, c, cs.n);
 }
 
 __device__ __forceinline__ void gather_state(const double* __restrict__ u, int4 n, double ue[4][3]) {
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kThreads) k_internal_force(MeshView m, Materia
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < m.num_cells;
          c += (int64_t)gridDim.x * blockDim.x) {
         CellState cs;
-        load_cell(m, z, c, cs);
+        load_cell(m, mat, z, c, cs);
         double ue[4][3], e[6], s[6];
         gather_state(u, cs.n, ue);
         strain_voigt(cs.G.g, ue, e);
@@ -80,14 +80,14 @@ __device__ __forceinline__ double cell_quantity(const MeshView& m, const Materia
                                                 const double* __restrict__ z,
                                                 const double* __restrict__ lam, int64_t c) {
     CellState cs;
-    load_cell(m, z, c, cs);
+    load_cell(m, mat, z, c, cs);
     double ue[4][3], e[6], s[6];
     gather_state(u, cs.n, ue);
     strain_voigt(cs.G.g, ue, e);
     stress_voigt(mat, e, s);
     const double ese = s[0] * e[0] + s[1] * e[1] + s[2] * e[2] + s[3] * e[3] + s[4] * e[4] + s[5] * e[5];
     if (MODE == 0) return 0.5 * ese * cs.G.vol * simp(mat, cs.rho);
-    const double sdx = simp_dx(mat, cs.rho) * 0.25;
+    const double sdx = simp_dx(mat, cs.rho) * rho_dz(mat);
     if (MODE == 1) return 0.5 * ese * cs.G.vol * sdx;
     if (MODE == 2) return -0.5 * ese * cs.G.vol * sdx;
     double le[4][3], el[6];
@@ -98,15 +98,18 @@ __device__ __forceinline__ double cell_quantity(const MeshView& m, const Materia
     return (0.5 * ese + esl) * cs.G.vol * sdx;
 }
 
+// accumulate != 0 adds into out (the element-control gradient goes straight to its output).
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_cell_quantity(MeshView m, Material mat,
                                                             const double* __restrict__ u,
                                                             const double* __restrict__ z,
                                                             const double* __restrict__ lam,
-                                                            double* __restrict__ out) {
+                                                            double* __restrict__ out, int accumulate) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < m.num_cells;
-         c += (int64_t)gridDim.x * blockDim.x)
-        out[c] = cell_quantity<MODE>(m, mat, u, z, lam, c);
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const double q = cell_quantity<MODE>(m, mat, u, z, lam, c);
+        out[c] = accumulate ? out[c] + q : q;
+    }
 }
 
 // Nodal sum of a per-cell quantity over the node's incident cells, in incidence order
@@ -177,8 +180,8 @@ template <int GRAD>
 __device__ __forceinline__ double cell_volume_quantity(const MeshView& m, const Material& pen,
                                                        const double* __restrict__ z, int64_t c) {
     CellState cs;
-    load_cell(m, z, c, cs);
-    return GRAD ? cs.G.vol * simp_dx(pen, cs.rho) * 0.25 : cs.G.vol * simp(pen, cs.rho);
+    load_cell(m, pen, z, c, cs);
+    return GRAD ? cs.G.vol * simp_dx(pen, cs.rho) * rho_dz(pen) : cs.G.vol * simp(pen, cs.rho);
 }
 
 __global__ void __launch_bounds__(kThreads) k_volume_sum(MeshView m, Material pen, const double* __restrict__ z,
@@ -289,14 +292,19 @@ int launch_nodal_control_derivative(plato_problem* h, int mode, const double* u,
                                     const double* lam, double* cellbuf, double* out, int accumulate) {
     const MeshView m = mesh_view(h);
     const int G = grid_for(h->C, kThreads);
+    // element control: the per-cell quantity is the derivative itself
+    const bool cells = h->material.cell_control != 0;
+    double* dst = cells ? out : cellbuf;
+    const int acc = cells ? accumulate : 0;
     switch (mode) {
-        case 1: k_cell_quantity<1><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, cellbuf); break;
-        case 2: k_cell_quantity<2><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, cellbuf); break;
-        case 3: k_cell_quantity<3><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, cellbuf); break;
-        case 4: k_cell_quantity<4><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, cellbuf); break;
+        case 1: k_cell_quantity<1><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, dst, acc); break;
+        case 2: k_cell_quantity<2><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, dst, acc); break;
+        case 3: k_cell_quantity<3><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, dst, acc); break;
+        case 4: k_cell_quantity<4><<<G, kThreads, 0, h->stream>>>(m, h->material, u, z, lam, dst, acc); break;
         default: return plato_fail(h, PLATO_BAD_INPUT, "unknown control-derivative mode");
     }
     PLATO_LAUNCH_CHECK(h);
+    if (cells) return PLATO_OK;
     k_node_sum<<<grid_for(h->N, kThreads), kThreads, 0, h->stream>>>(graph_view(h), cellbuf, out, accumulate);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
@@ -311,8 +319,11 @@ int launch_volume(plato_problem* h, const Material& pen, const double* z, double
 }
 
 int launch_volume_gradient(plato_problem* h, const Material& pen, const double* z, double* dvdz) {
-    k_volume_cell_grad<<<grid_for(h->C, kThreads), kThreads, 0, h->stream>>>(mesh_view(h), pen, z, h->cellbuf);
+    const bool cells = pen.cell_control != 0;
+    k_volume_cell_grad<<<grid_for(h->C, kThreads), kThreads, 0, h->stream>>>(mesh_view(h), pen, z,
+                                                                              cells ? dvdz : h->cellbuf);
     PLATO_LAUNCH_CHECK(h);
+    if (cells) return PLATO_OK;
     k_node_sum<<<grid_for(h->N, kThreads), kThreads, 0, h->stream>>>(graph_view(h), h->cellbuf, dvdz, 0);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;

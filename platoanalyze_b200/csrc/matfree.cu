@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kThreads) k_cell_weights(int32_t C, const int4
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C;
          c += (int64_t)gridDim.x * blockDim.x) {
         const int4 n = conn[c];
-        const double rho = (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+        const double rho = cell_rho(mat, z, c, n);
         w[c] = T(simp(mat, rho));
     }
 }

@@ -23,6 +23,8 @@ struct Material {
     double c00, c01, c33;
     double p, rho_min;  // MSIMP exponent and minimum value (src/Simp.hpp:130-134)
     int    p_int;       // p when it is a small non-negative integer, else -1
+    int    cell_control;  // 0: nodal control, cell density = mean of its 4 nodes
+                          // (ApplyWeighting, src/ApplyWeighting.hpp:55-60); 1: one density per cell
 };
 
 // Device pointers and sizes the element kernels read.
@@ -391,6 +393,16 @@ __device__ __forceinline__ void load_cell_coords(const double* __restrict__ coor
         x[a][2] = __ldg(p + 2);
     }
 }
+
+// Density of cell c: the mean of its nodal control (ApplyWeighting, src/ApplyWeighting.hpp:
+// 55-60), or the cell's own entry with element control.
+__device__ __forceinline__ double cell_rho(const Material& m, const double* __restrict__ z, int64_t c, int4 n) {
+    if (m.cell_control) return __ldg(z + c);
+    return (__ldg(z + n.x) + __ldg(z + n.y) + __ldg(z + n.z) + __ldg(z + n.w)) * 0.25;
+}
+
+// d rho_e / d z: 1/4 for each of the cell's nodes, or 1 for the cell's own entry.
+__device__ __forceinline__ double rho_dz(const Material& m) { return m.cell_control ? 1.0 : 0.25; }
 
 __device__ __forceinline__ int node_of(int4 n, int a) {
     return a == 0 ? n.x : (a == 1 ? n.y : (a == 2 ? n.z : n.w));

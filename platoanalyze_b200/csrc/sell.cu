@@ -112,35 +112,45 @@ k_crs_to_sell(int32_t N, int32_t nslices, const int32_t* __restrict__ row_map, c
     }
 }
 
+// D^1/2, D^-1/2 (FP32) and the unit Jacobi diagonal of the scaled matrix, from dinv = 1/diag.
+__global__ void k_scale_vectors(int64_t n, const double* __restrict__ dinv, float* __restrict__ sq,
+                                float* __restrict__ isq, float* __restrict__ ones) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double di = dinv[i];
+        sq[i] = float(1.0 / sqrt(di));
+        isq[i] = float(sqrt(di));
+        ones[i] = 1.0f;
+    }
+}
+
 // FP16 copy of the Jacobi-scaled matrix: entry (a, b) of block k of row r, column node c,
-// becomes A * sqrt(dinv[3r+a]) * sqrt(dinv[3c+b]) (dinv = 1 / diag, FP64), same slots as
-// the FP64 SELL copy.  Also sq = D^1/2, isq = D^-1/2 and ones (the Jacobi diagonal of the
-// scaled matrix) in FP32.
-__global__ void k_sell_scale16(int32_t N, int32_t nslices, const int32_t* __restrict__ width,
-                               const int64_t* __restrict__ ptr, const int32_t* __restrict__ cols,
-                               const double* __restrict__ sell64, const double* __restrict__ dinv,
-                               __half* __restrict__ out16, float* __restrict__ sq, float* __restrict__ isq,
-                               float* __restrict__ ones) {
-    for (int64_t s = blockIdx.x; s < nslices; s += gridDim.x) {
-        const int w = width[s];
-        const int64_t base = ptr[s];
-        for (int t = threadIdx.x; t < 9 * 32 * w; t += blockDim.x) {
-            const int l = t & 31, kq = t >> 5;
-            const int k = kq / 9, q = kq - 9 * k, a = q / 3, b = q - 3 * a;
-            const int64_t r = 32 * s + l;
-            double v = 0.0;
-            if (r < N) {
-                const int64_t c = cols[base + 32 * k + l];
-                v = sell64[9 * base + t] * sqrt(dinv[3 * r + a]) * sqrt(dinv[3 * c + b]);
+// becomes A * isq[3r+a] * isq[3c+b] (isq = D^-1/2 in FP32, far finer than the FP16 result;
+// the diagonal rounds to exactly 1), same slots as the FP64 SELL copy.  A thread owns one
+// row of a slice: per block it loads the column once, the three isq of the column and the
+// nine entries (coalesced across the warp), and stores nine halves.
+__global__ void __launch_bounds__(256)
+k_sell_scale16(int32_t N, int32_t nslices, const int32_t* __restrict__ width, const int64_t* __restrict__ ptr,
+               const int32_t* __restrict__ cols, const double* __restrict__ sell64, const float* __restrict__ isq,
+               __half* __restrict__ out16) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; s < nslices;
+         s += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int w = __ldg(width + s);
+        const int64_t base = __ldg(ptr + s);
+        const int64_t r = 32 * s + lane;
+        float ir[3] = {0.f, 0.f, 0.f};
+        if (r < N)
+            for (int a = 0; a < 3; ++a) ir[a] = __ldg(isq + 3 * r + a);
+        for (int k = 0; k < w; ++k) {
+            const int64_t c = __ldg(cols + base + 32 * k + lane);
+            const float ic0 = __ldg(isq + 3 * c), ic1 = __ldg(isq + 3 * c + 1), ic2 = __ldg(isq + 3 * c + 2);
+            const double* v = sell64 + 9 * base + 32 * (9 * k) + lane;
+            __half* o = out16 + 9 * base + 32 * (9 * k) + lane;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                const float ic = (q % 3) == 0 ? ic0 : ((q % 3) == 1 ? ic1 : ic2);
+                o[32 * q] = __float2half_rn(float(__ldg(v + 32 * q)) * ir[q / 3] * ic);
             }
-            out16[9 * base + t] = __double2half(v);
-        }
-        if (threadIdx.x < 96 && 32 * s + threadIdx.x / 3 < N) {
-            const int64_t i = 96 * s + threadIdx.x;
-            const double di = dinv[i];
-            sq[i] = float(1.0 / sqrt(di));
-            isq[i] = float(sqrt(di));
-            ones[i] = 1.0f;
         }
     }
 }
@@ -215,8 +225,11 @@ int launch_crs_to_sell(plato_problem* h, const double* crs, double* out64, float
 int launch_sell_scale16(plato_problem* h, const double* sell64, const double* dinv, void* out16, float* sq,
                         float* isq, float* ones) {
     const SellPattern& P = h->sell;
-    k_sell_scale16<<<grid_for(P.nslices, 1, 148 * 16), kSliceThreads, 0, h->stream>>>(
-        h->N, P.nslices, P.width, P.ptr, P.cols, sell64, dinv, static_cast<__half*>(out16), sq, isq, ones);
+    const int64_t n = 3 * int64_t(h->N);
+    k_scale_vectors<<<grid_for(n, 256), 256, 0, h->stream>>>(n, dinv, sq, isq, ones);
+    PLATO_LAUNCH_CHECK(h);
+    k_sell_scale16<<<grid_for(int64_t(P.nslices) * 32, 256, 148 * 16), 256, 0, h->stream>>>(
+        h->N, P.nslices, P.width, P.ptr, P.cols, sell64, isq, static_cast<__half*>(out16));
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -124,6 +124,7 @@ class EllipticProblem:
         check(lib.plato_get_sizes(h, C.byref(nn), C.byref(nc), C.byref(nb)), h)
         self.num_nodes, self.num_cells, self.num_blocks = nn.value, nc.value, nb.value
         self.num_dofs = 3 * self.num_nodes
+        self.nz = self.num_nodes  # control entries (nodal layout)
         cnt = C.c_int32()
         check(lib.plato_batch_info(h, C.byref(cnt), None, None), h)
         self.count = cnt.value
@@ -154,6 +155,13 @@ class EllipticProblem:
         return v.cpu().numpy()
 
     # -- plumbing ------------------------------------------------------------------------
+    def set_control_layout(self, layout: str) -> None:
+        """'nodal' (the reference's: a cell takes the mean of its nodes) or 'element' (one
+        density per cell; control vectors and their gradients then have num_cells entries)."""
+        code = {"nodal": capi.CONTROL_NODAL, "element": capi.CONTROL_ELEMENT}[layout]
+        check(lib.plato_set_control_layout(self.h, code), self.h)
+        self.nz = self.num_cells if code == capi.CONTROL_ELEMENT else self.num_nodes
+
     def set_stream(self, stream) -> None:
         self.stream = stream
         check(lib.plato_set_stream(self.h, C.c_void_p(stream.cuda_stream)), self.h)
@@ -245,7 +253,7 @@ class EllipticProblem:
         return g
 
     def sf_gradient_z(self, u, z):
-        g = self.zeros(self.num_nodes)
+        g = self.zeros(self.nz)
         check(lib.plato_sf_gradient_z(self.h, self._dev(u), self._dev(z), self._dev(g)), self.h)
         return g
 
@@ -265,7 +273,7 @@ class EllipticProblem:
         return v.value
 
     def volume_gradient_z(self, z, exponent=1.0, minimum=0.0):
-        g, pen = self.zeros(self.num_nodes), capi.Penalty(exponent, minimum)
+        g, pen = self.zeros(self.nz), capi.Penalty(exponent, minimum)
         check(lib.plato_volume_gradient_z(self.h, self._dev(z), C.byref(pen), self._dev(g)), self.h)
         return g
 
@@ -307,7 +315,7 @@ class EllipticProblem:
         return v.value
 
     def criterion_gradient(self, z, u):
-        g = self.zeros(self.num_nodes)
+        g = self.zeros(self.nz)
         st = capi.SolveStats()
         check(lib.plato_problem_criterion_gradient(self.h, self._dev(z), self._dev(u), self._dev(g), C.byref(st)),
               self.h)
@@ -317,7 +325,7 @@ class EllipticProblem:
         """One optimisation step on host (numpy) buffers; returns (u, value, dfdz, stats)."""
         z = np.ascontiguousarray(z, dtype=np.float64)
         u = u_out if u_out is not None else np.empty(self.num_dofs)
-        g = g_out if g_out is not None else np.empty(self.num_nodes)
+        g = g_out if g_out is not None else np.empty(self.nz)
         v = C.c_double()
         st = capi.SolveStats()
         rc = lib.plato_problem_solve_and_gradient_host(self.h, _np_ptr(z), _np_ptr(u0) if u0 is not None else None,

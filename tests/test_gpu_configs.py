@@ -146,3 +146,46 @@ def test_config4_member_sizes():
     u8, st8 = bp.solution(zd)
     assert st8["converged"] == 1 and all(m["relative_residual"] <= 1e-8 for m in bp.batch_last_stats())
     bp.close()
+
+
+def test_element_control_parity():
+    """Element control (one density per cell, the per-element density of the 160x80x80
+    configuration's wording): residual, Jacobian, energy, its control derivative and the
+    compliance sensitivity (self-adjoint and explicit adjoint) at 1e-11 of the oracle in the
+    same layout; the solve within 1e-8 of the oracle's refined solve; a uniform field gives
+    the nodal layout's numbers."""
+    spec = cantilever(20, 10, 10, SolverOptions(tolerance=1e-10))
+    prob = EllipticProblem(spec)
+    prob.set_control_layout("element")
+    orc = Oracle.from_spec(spec, cell_control=True)
+    zc = splitmix_uniform(orc.C, SEED_LARGE)
+    zd = prob.to_dev(zc)
+    u = np.sin(np.arange(3 * orc.N) * 0.37) * 1e-2
+    ud = prob.to_dev(u)
+    close(host(prob.vf_value(ud, zd)), orc.vf_value(u, zc))
+    close(host(prob.vf_gradient_u(ud, zd)), orc.vf_gradient_u(u, zc))
+    assert abs(prob.sf_value(ud, zd) - orc.sf_value(u, zc)) <= TOL * abs(orc.sf_value(u, zc))
+    g = host(prob.sf_gradient_z(ud, zd))
+    assert g.shape == (orc.C,)
+    close(g, orc.sf_gradient_z(u, zc))
+    us, st = prob.solution(zd)
+    assert st["converged"] == 1 and st["relative_residual"] <= 1e-10
+    uo, _, _ = orc.solution_refined(zc, tol=1e-13)
+    assert rel_l2(host(us), uo) <= 1e-8
+    uh = host(us)
+    gs, _ = prob.criterion_gradient(zd, us)
+    close(host(gs), orc.criterion_gradient(zc, uh, self_adjoint=True))
+    prob.set_solver(SolverOptions(tolerance=1e-10, self_adjoint=False))
+    ga, _ = prob.criterion_gradient(zd, us)
+    assert rel_l2(host(ga), host(gs)) <= 1e-8
+    # the two-level FP16 method runs in the element layout too
+    prob.set_solver(method_options("two-level-fp16", 1e-10, (10, 5, 5)))
+    u2, st2 = prob.solution(zd)
+    assert st2["converged"] == 1 and rel_l2(host(u2), uo) <= 1e-8
+    nodal = EllipticProblem(spec)
+    z_uniform = 0.6
+    fe = prob.sf_value(ud, prob.to_dev(np.full(orc.C, z_uniform)))
+    fn = nodal.sf_value(nodal.to_dev(u), nodal.to_dev(np.full(orc.N, z_uniform)))
+    assert abs(fe - fn) <= 1e-14 * abs(fn)
+    nodal.close()
+    prob.close()

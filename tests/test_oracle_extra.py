@@ -143,3 +143,29 @@ def test_volume_criterion():
         assert abs(g @ dz - fd) < 1e-8 * np.linalg.norm(g) * np.linalg.norm(dz)
     # linear in z for p = 1: sum of the gradient is the total volume
     assert orc.volume_gradient_z(z, 1.0, 0.0).sum() == pytest.approx(1.0, rel=1e-13)
+
+
+def test_element_control_derivatives_by_finite_differences(small):
+    """Element control (one density per cell): the energy's and the compliance's control
+    derivatives per cell against central differences; a uniform field gives the nodal result."""
+    spec, _, _, u = small
+    orc = Oracle.from_spec(spec, cell_control=True)
+    zc = splitmix_uniform(orc.C, 23, 0.2, 0.9)
+    eps = 1e-6
+    dz = np.sin(np.arange(orc.C) * 0.4) * 0.05
+    fdz = (orc.sf_value(u, zc + eps * dz) - orc.sf_value(u, zc - eps * dz)) / (2 * eps)
+    g = orc.sf_gradient_z(u, zc)
+    assert g.shape == (orc.C,) and abs(g @ dz - fdz) < 1e-7 * abs(fdz)
+
+    def compliance(zz):
+        uu, _, _ = orc.solution_refined(zz, tol=1e-13)
+        return orc.sf_value(uu, zz)
+
+    fd = (compliance(zc + eps * dz) - compliance(zc - eps * dz)) / (2 * eps)
+    us, _, _ = orc.solution_refined(zc, tol=1e-13)
+    for self_adjoint in (True, False):
+        gc = orc.criterion_gradient(zc, us, self_adjoint=self_adjoint, tol=1e-13)
+        assert abs(gc @ dz - fd) < 1e-6 * abs(fd), (self_adjoint, gc @ dz, fd)
+    nodal = Oracle.from_spec(spec)
+    z_uniform = np.full(orc.N, 0.6)
+    assert abs(orc.sf_value(u, np.full(orc.C, 0.6)) - nodal.sf_value(u, z_uniform)) < 1e-14 * nodal.sf_value(u, z_uniform)

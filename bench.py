@@ -77,9 +77,10 @@ def parse():
     ap.add_argument("--cells", default="80,40,40", help="--profile-unit: hexes along x,y,z (6 tets each)")
     ap.add_argument("--repeat", type=int, default=1, help="--profile-unit: units to run")
     ap.add_argument("--coarse", default=None, help="--profile-unit: coarse box cells x,y,z")
-    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "helmholtz"],
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "helmholtz", "mixed"],
                     help="batch: 64 independent GRF cantilevers n x n/2 x n/2, n in {16,24,32,48,64}, one batched "
-                         "solve; helmholtz: the density filter's solution and chain rule on the --size mesh")
+                         "solve; helmholtz: the density filter's solution and chain rule on the --size mesh; "
+                         "mixed: the error report of every reduced-precision variant on the 20x10x10 mesh")
     return ap.parse_args()
 
 
@@ -506,6 +507,81 @@ def run_profile_unit(args):
     return 0
 
 
+MIXED_METRIC = "mixed-precision variants, 20x10x10 seeded cantilever, FP64-checked tol 1e-8: max relative error in u vs the FP64 oracle"
+
+
+def run_mixed(args):
+    """The mixed-precision error report: every reduced-precision variant solves the 20x10x10
+    cantilever with nodal densities U[0.01, 1] (seed 0x5EED0003) to the FP64-recomputed
+    relative residual 1e-8 (FP64 residuals, dot products and step lengths; the reduced
+    precision lives in the preconditioner's matrix, element kernels and sweep), and reports
+    its error in u, compliance and dC/dz against the oracle solved to a long double relative
+    residual <= 1e-13.  The plain FP64 method at the same tolerance is the first row."""
+    import torch
+
+    from platoanalyze_b200 import capi
+    from platoanalyze_b200.problem import EllipticProblem, SolverOptions
+    from platoanalyze_b200.workloads import cantilever, splitmix_uniform
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    tol = 1e-8
+    spec = cantilever(20, 10, 10)
+    z = splitmix_uniform(spec.coords.shape[0], 0x5EED0003)
+    ow, Oracle = _oracle_modules()
+    orc = ow.cantilever_oracle(20, 10, 10)
+    us, _, st_ref = orc.solution_refined(z, tol=1e-13)
+    fs = orc.sf_value(us, z)
+    gs = orc.criterion_gradient(z, us, self_adjoint=True)
+    variants = {
+        "fp64: plain Jacobi-PCG (reference algorithm)": SolverOptions(tolerance=tol, max_iterations=200000),
+        "fp32: Chebyshev(8)-Jacobi on an FP32 SELL copy, FP32 accumulation": SolverOptions(
+            tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=8),
+        "bf16-stored: Chebyshev(8)-Jacobi on a BF16 SELL copy, FP32 accumulation": SolverOptions(
+            tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_BF16, chebyshev_degree=8),
+        "fp16-scaled: Chebyshev(8) on FP16 D^-1/2 A D^-1/2, FP32 accumulation": SolverOptions(
+            tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8),
+        "fp32 element kernels: matrix-free FP32 element-by-element Chebyshev(8), FP64 matrix-free outer": SolverOptions(
+            tolerance=tol, max_iterations=200000, operator_kind=capi.OPERATOR_MATRIX_FREE,
+            precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=8),
+        "fp16-scaled two-level: Chebyshev(8) + Galerkin coarse space 10x5x5": SolverOptions(
+            tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8,
+            coarse_cells=(10, 5, 5)),
+    }
+    prob = EllipticProblem(spec)
+    zd = prob.to_dev(z)
+    rows = []
+    for name, opts in variants.items():
+        prob.set_solver(opts)
+        prob.solution(zd)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        u, st = prob.solution(zd)
+        f = prob.criterion_value(zd, u)
+        g, _ = prob.criterion_gradient(zd, u)
+        e1.record()
+        torch.cuda.synchronize()
+        uh, gh = u.cpu().numpy(), g.cpu().numpy()
+        rows.append({"variant": name, "iterations": st["iterations"], "relative_residual": st["relative_residual"],
+                     "fallback": st["fallback"], "ms_solve_adjoint": e0.elapsed_time(e1),
+                     "e_u": float(np.linalg.norm(uh - us) / np.linalg.norm(us)),
+                     "e_compliance": abs(f - fs) / abs(fs),
+                     "e_dcdz": float(np.linalg.norm(gh - gs) / np.linalg.norm(gs))})
+    prob.close()
+    worst = max(r["e_u"] for r in rows)
+    line = {"metric": MIXED_METRIC, "value": worst, "unit": "relative error", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+bf16+f16",
+            "data": "synthetic",
+            "config": {"workload": "SIMP cantilever 20x10x10 hexes x 6 tets, nodal densities U[0.01,1] seed 0x5EED0003",
+                       "tolerance": tol, "oracle": f"FP64 Jacobi-PCG refined with a long double iterate to relres "
+                                                   f"{st_ref['relative_residual']:.2e}",
+                       "variants": rows}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_unit:
@@ -516,6 +592,8 @@ def main():
         return run_batch(args)
     if args.workload == "helmholtz":
         return run_helmholtz(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
 
     import torch
     import torch.distributed as dist
@@ -632,6 +710,34 @@ def main():
                   "frac": asm_bytes / (asm_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
                   "algorithmic_bytes": asm_bytes, "avg_launch_ms": asm_ms, "launches_timed": inst["assembly_timed"]}
 
+    # element kernels: the energy sum and the fused self-adjoint dC/dz are inside every step; the
+    # residual R(u, z) = K(z) u - F (not part of the step) is timed on the step's solution.
+    # Algorithmic bytes: connectivity 16 C, coordinates 24 N, control 8 N, state 24 N, plus the
+    # output (R 24 N; dC/dz 8 N; the energy is a scalar).
+    prob.set_timing(True)
+    for _ in range(5):
+        prob.vf_value(u, zd)
+    torch.cuda.synchronize()
+    prob.set_timing(False)
+    inst_e = prob.instrumentation()
+    elem_in = 16 * prob.num_cells + 24 * N + 8 * N + 24 * N
+
+    def roof_line(kernel, nbytes, ms_total, count):
+        if not count:
+            return None
+        ms = ms_total / count
+        return {"bound": "hbm", "kernel": kernel, "achieved": nbytes / (ms / 1e3) / 1e9, "peak": peak,
+                "unit": "GB/s", "frac": nbytes / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                "traffic": None, "algorithmic_bytes": nbytes, "avg_launch_ms": ms, "launches_timed": count}
+
+    rl_elements = {
+        "residual": roof_line("k_internal_force (+ the load copy): R = K(z) u - F", elem_in + 24 * N,
+                              inst_e["residual_ms_total"], inst_e["residual_timed"]),
+        "energy": roof_line("k_energy_sum: compliance 1/2 u^T K(z) u", elem_in,
+                            inst["energy_ms_total"], inst["energy_timed"]),
+        "dcdz": roof_line("k_cell_quantity<2> + k_node_sum: self-adjoint dC/dz", elem_in + 8 * N,
+                          inst["dcdz_ms_total"], inst["dcdz_timed"])}
+
     # two-level coarse operator, once per solve: the Galerkin product P^T A P and the dense FP64
     # Cholesky + L^-1 (n^3/3 flops each for the n coarse dofs; FP64 mma.sync tiles)
     coarse = None
@@ -700,7 +806,8 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"plain": "f64", "bf16": "f64+bf16", "two-level-fp16": "f64+f32+f16"}.get(args.method, "f64+f32"),
             "data": "synthetic", "config": cfg, "accuracy": accuracy, "roofline": roofline,
-            "roofline_fp64_spmv": roofline_other, "roofline_assembly": rl_asm, "coarse_setup": coarse,
+            "roofline_fp64_spmv": roofline_other, "roofline_assembly": rl_asm, "roofline_elements": rl_elements,
+            "coarse_setup": coarse,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N,
                     "d2h_bytes_per_step": 8 * (3 * N + N) + 8},

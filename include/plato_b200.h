@@ -176,7 +176,10 @@ int plato_reset_instrumentation(plato_problem* h);
  * preconditioner (one step = one preconditioner-operator apply fused with its update),
  * kind 2 = the Jacobian assembly of each assembled solve, kind 3 = the Galerkin product of
  * the two-level coarse operator, kind 4 = its dense factorization and inverse (kinds 3 and 4
- * count coarse operator set-ups). */
+ * count coarse operator set-ups); kinds 5-7 time every call with timing on: 5 = the residual
+ * of plato_vf_value (load copy + element force kernel), 6 = the energy sum of plato_sf_value,
+ * 7 = the self-adjoint dC/dz of plato_problem_criterion_gradient (per-cell pass + nodal
+ * sums).  Reading kinds 5-7 waits for the last timed launch of that kind. */
 int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
 
 /* ---- block pattern ---------------------------------------------------------------------
@@ -315,6 +318,14 @@ int plato_batch_criterion_values(plato_problem* h, const double* z, const double
  * operator only. */
 int plato_problem_solution_subspace(plato_problem* h, const double* z, const double* u0, const double* W, int32_t k,
                                     double* u, plato_solve_stats* stats, double* residual_ratio);
+/* The same, with the subspace also deflating the Krylov iteration (no reference counterpart;
+ * the learned network's fields use it): after the Galerkin guess above, every search
+ * direction is made A-orthogonal to P W (deflated CG), so the solver never searches span(P W)
+ * again.  Plain Jacobi-PCG and the flexible-CG methods on the assembled operator; deflation is
+ * skipped (the plain solve runs) when the Gram matrix is not positive definite or the guess
+ * was dropped.  A failed deflated solve falls back like the others (fallback_max_iterations). */
+int plato_problem_solution_deflated(plato_problem* h, const double* z, const double* u0, const double* W,
+                                    int32_t k, double* u, plato_solve_stats* stats, double* residual_ratio);
 
 /* ---- learned warm start (no reference counterpart) -------------------------------------
  * A 3-level 3D U-Net (16-32-64 channels; 3x3x3 convolutions with ReLU, 2x2x2 average pooling,

@@ -122,6 +122,7 @@ def _load() -> C.CDLL:
         "plato_batch_last_stats": ([vp, C.POINTER(SolveStats)], C.c_int),
         "plato_batch_criterion_values": ([vp, vp, vp, vp], C.c_int),
         "plato_problem_solution_subspace": ([vp, vp, vp, vp, C.c_int32, vp, C.POINTER(SolveStats), f64p], C.c_int),
+        "plato_problem_solution_deflated": ([vp, vp, vp, vp, C.c_int32, vp, C.POINTER(SolveStats), f64p], C.c_int),
         "plato_unet_create": ([i32p, C.c_int32, C.POINTER(vp)], C.c_int),
         "plato_unet_destroy": ([vp], C.c_int),
         "plato_unet_set_stream": ([vp, vp], C.c_int),

@@ -136,7 +136,7 @@ int plato_destroy(plato_problem* h) {
     cudaStreamSynchronize(h->stream);
     dfree(h->conn); dfree(h->coords); dfree(h->row_map); dfree(h->cols); dfree(h->diag);
     dfree(h->n2c_ptr); dfree(h->n2c); dfree(h->F); dfree(h->bc_dofs); dfree(h->bc_values);
-    dfree(h->asm_plan); dfree(h->asm_wide);
+    dfree(h->asm_plan); dfree(h->asm_wide); dfree(h->ritz_small);
     dfree(h->bc_mask); dfree(h->K); dfree(h->KT); dfree(h->v_r); dfree(h->v_z); dfree(h->v_p);
     dfree(h->v_Ap); dfree(h->v_dinv); dfree(h->v_b); dfree(h->v_x); dfree(h->v_tmp);
     dfree(h->partials); dfree(h->cellbuf); dfree(h->scal); dfree(h->red_out); dfree(h->red_ticket);
@@ -343,8 +343,48 @@ int plato_get_instrumentation(const plato_problem* h, int64_t* launches, double*
     return PLATO_OK;
 }
 
-int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count) {
-    if (!h || !ms_total || !count) return PLATO_BAD_INPUT;
+// Element-kernel timing: begin/end bracket one launch group of kind k (0 residual, 1 energy,
+// 2 control derivative) on the handle's stream; a previous pair of the same kind is read
+// first (it has completed by then or is waited for).
+static int elem_time_flush(plato_problem* h, int k) {
+    auto& t = h->elem_timing[k];
+    if (!t.pending) return PLATO_OK;
+    PLATO_CUDA(h, cudaEventSynchronize(t.e1));
+    float ms = 0.f;
+    PLATO_CUDA(h, cudaEventElapsedTime(&ms, t.e0, t.e1));
+    t.ms += ms;
+    t.count += 1;
+    t.pending = 0;
+    return PLATO_OK;
+}
+
+static int elem_time_begin(plato_problem* h, int k) {
+    if (!h->timing) return PLATO_OK;
+    auto& t = h->elem_timing[k];
+    RC(elem_time_flush(h, k));
+    if (!t.e0) PLATO_CUDA(h, cudaEventCreate(&t.e0));
+    if (!t.e1) PLATO_CUDA(h, cudaEventCreate(&t.e1));
+    PLATO_CUDA(h, cudaEventRecord(t.e0, h->stream));
+    return PLATO_OK;
+}
+
+static int elem_time_end(plato_problem* h, int k) {
+    if (!h->timing) return PLATO_OK;
+    auto& t = h->elem_timing[k];
+    PLATO_CUDA(h, cudaEventRecord(t.e1, h->stream));
+    t.pending = 1;
+    return PLATO_OK;
+}
+
+int plato_get_kernel_timing(const plato_problem* hc, int32_t kind, double* ms_total, int64_t* count) {
+    if (!hc || !ms_total || !count) return PLATO_BAD_INPUT;
+    plato_problem* h = const_cast<plato_problem*>(hc);  // reading the totals completes pending pairs
+    if (kind >= 5 && kind <= 7) {
+        RC(elem_time_flush(h, kind - 5));
+        *ms_total = h->elem_timing[kind - 5].ms;
+        *count = h->elem_timing[kind - 5].count;
+        return PLATO_OK;
+    }
     if (kind == 0) { *ms_total = h->op_ms_total; *count = h->op_timed; }
     else if (kind == 1) { *ms_total = h->inner_ms_total; *count = h->inner_timed; }
     else if (kind == 2) { *ms_total = h->asm_ms_total; *count = h->asm_timed; }
@@ -363,6 +403,12 @@ int plato_reset_instrumentation(plato_problem* h) {
     h->inner_timed = 0;
     h->asm_ms_total = 0.0;
     h->asm_timed = 0;
+    for (auto& t : h->elem_timing) {
+        if (t.pending && t.e1) cudaEventSynchronize(t.e1);
+        t.pending = 0;
+        t.ms = 0.0;
+        t.count = 0;
+    }
     h->coarse_gal_ms = 0.0;
     h->coarse_inv_ms = 0.0;
     h->coarse_timed = 0;
@@ -386,7 +432,9 @@ int plato_jacobian_pattern(plato_problem* h, int32_t* row_map, int32_t* cols) {
 
 int plato_vf_value(plato_problem* h, const double* u, const double* z, double* R) {
     NEED(h, u && z && R, "null device pointer");
-    return launch_internal_force(h, u, z, R, -1.0);
+    RC(elem_time_begin(h, 0));
+    RC(launch_internal_force(h, u, z, R, -1.0));
+    return elem_time_end(h, 0);
 }
 
 int plato_vf_gradient_u(plato_problem* h, const double* u, const double* z, double* entries) {
@@ -415,7 +463,9 @@ int plato_vf_gradient_z_apply(plato_problem* h, const double* u, const double* z
 
 int plato_sf_value(plato_problem* h, const double* u, const double* z, double* value) {
     NEED(h, u && z && value, "null pointer");
+    RC(elem_time_begin(h, 1));
     RC(launch_energy(h, u, z, h->red_out));
+    RC(elem_time_end(h, 1));
     PLATO_CUDA(h, cudaMemcpyAsync(value, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
     return PLATO_OK;
@@ -528,6 +578,27 @@ int plato_problem_solution_subspace(plato_problem* h, const double* z, const dou
     return rc;
 }
 
+int plato_problem_solution_deflated(plato_problem* h, const double* z, const double* u0, const double* W, int32_t k,
+                                    double* u, plato_solve_stats* stats, double* residual_ratio) {
+    NEED(h, z && u, "null device pointer");
+    NEED(h, k >= 1 && k <= 8 && W, "deflation needs 1 <= k <= 8 columns");
+    if (h->batch.nseg > 0 || h->opts.operator_kind != PLATO_OPERATOR_ASSEMBLED)
+        return plato_fail(h, PLATO_NOT_SUPPORTED, "deflation needs a single problem on the assembled operator");
+    plato_solve_stats local{};
+    h->ritz_W = W;
+    h->ritz_k = k;
+    h->ritz_rel_gain = 1.0;
+    h->ritz_deflate = 1;
+    h->ritz_deflating = 0;
+    const int rc = solve_state(h, z, u0, u, stats ? stats : &local);
+    h->ritz_W = nullptr;
+    h->ritz_k = 0;
+    h->ritz_deflate = 0;
+    h->ritz_deflating = 0;
+    if (residual_ratio) *residual_ratio = h->ritz_rel_gain;
+    return rc;
+}
+
 int plato_problem_criterion_value(plato_problem* h, const double* z, const double* u, double* value) {
     return plato_sf_value(h, u, z, value);
 }
@@ -540,7 +611,9 @@ int plato_problem_criterion_gradient(plato_problem* h, const double* z, const do
     if (h->opts.self_adjoint) {
         // lambda = -u (src/elliptic/Problem.hpp:423-427): dfdz + (dR/dz)^T lambda fused per cell
         st->iterations = 0; st->refinements = 0; st->relative_residual = 0.0; st->converged = 1; st->status = 0;
-        return launch_nodal_control_derivative(h, 2, u, z, nullptr, h->cellbuf, dfdz, 0);
+        RC(elem_time_begin(h, 2));
+        RC(launch_nodal_control_derivative(h, 2, u, z, nullptr, h->cellbuf, dfdz, 0));
+        return elem_time_end(h, 2);
     }
     // adjoint: K^T lambda = -df/du with zero-valued constraints (Problem.hpp:429-441, 701-713)
     const int64_t n = 3 * int64_t(h->N);
@@ -603,6 +676,7 @@ static int fallback_solve(plato_problem* h, double* x, plato_solve_stats* st, in
                           const double* z = nullptr) {
     const int32_t cap = h->opts.fallback_max_iterations;
     const size_t bytes = sizeof(double) * 3 * size_t(h->N);
+    h->ritz_deflating = 0;  // deflation needs the Galerkin guess, which the retries drop
     if (h->ritz_W && h->ritz_k > 0) {
         PLATO_CUDA(h, cudaMemsetAsync(x, 0, bytes, h->stream));
         const int rc = fcg_poly(h, h->v_b, x, st);

@@ -756,6 +756,8 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 1);
         h->launches += 1;
         PLATO_LAUNCH_CHECK(h);
+        rc = deflate_direction(h, h->v_p, h->v_r, 1);
+        if (rc) return rc;
 
         PcgScalars* slots = h->scal_host;
         int64_t enqueued = 0;
@@ -798,6 +800,8 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 0);
                 h->launches += 1;
                 PLATO_LAUNCH_CHECK(h);
+                rc = deflate_direction(h, h->v_p, h->v_r, 1);
+                if (rc) return rc;
             }
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));

@@ -270,6 +270,15 @@ struct plato_problem {
     double  coarse_gal_ms = 0.0;
     double  coarse_inv_ms = 0.0;
     int64_t coarse_timed = 0;
+    // element kernels timed as one unit per call (kinds 5-7 of plato_get_kernel_timing): the
+    // residual (k_internal_force), the energy sum and the control derivative (per-cell pass +
+    // nodal sum); a pair is read when the same kind is timed again or the totals are read
+    struct TimedPair {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        int pending = 0;
+        double ms = 0.0;
+        int64_t count = 0;
+    } elem_timing[3];
     BatchState batch{};
     // subspace initial guess (ritz.cu): columns set for the duration of one solution call
     const double* ritz_W = nullptr;
@@ -277,6 +286,9 @@ struct plato_problem {
     double* ritz_scratch = nullptr;
     size_t  ritz_scratch_len = 0;
     double  ritz_rel_gain = 1.0;   // ||r|| after / before the last subspace correction (1: not used)
+    int32_t ritz_deflate = 0;      // the subspace also deflates the Krylov directions (this call)
+    int32_t ritz_deflating = 0;    // deflation set up for the running solve (Galerkin guess kept)
+    double* ritz_small = nullptr;  // G^-1 (k x k) and mu (k) of the deflation
     // Helmholtz density filter (helmholtz.cu): physics 1, one unknown per node
     int32_t physics = 0;           // 0 elastostatics, 1 Helmholtz filter
     double  helm_length = 0.0;     // length scale L
@@ -304,6 +316,7 @@ void coarse_release(plato_problem* h);
 void batch_release(plato_problem* h);
 int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
 int ritz_guess(plato_problem* h, const double* b, double* x);
+int deflate_direction(plato_problem* h, double* p, const double* r, int update_pr);
 constexpr int kEnergySplit = 32;  // CTAs per member in the batched criterion sum
 int launch_energy_segments(plato_problem* h, const double* u, const double* z, double* values);
 }  // namespace plato

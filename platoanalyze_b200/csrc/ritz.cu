@@ -10,6 +10,13 @@
 // initial guess - when G is not numerically positive definite or the new residual is not
 // finite or grows past kResidualGuard times the old one (a guess with node-scale noise has a
 // residual far above ||b|| and gains the solver nothing).
+//
+// Deflation (plato_problem_solution_deflated): after the Galerkin guess the residual is
+// orthogonal to span(P W), and the Krylov solver keeps it so by making every new search
+// direction A-orthogonal to P W (deflated CG: Saad, Yeung, Erhel, Guyomarc'h, SIAM J. Sci.
+// Comput. 21, 2000): p <- p - P W mu with mu = G^-1 (A P W)^T p, G = W^T P A P W.  Two launches
+// per iteration (the k dot products with mu in the last block; the update with the new p.r
+// for the flexible CG); W, A P W and G^-1 stay on the device for the solve.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -79,6 +86,69 @@ k_ritz_update(int64_t n, int k, const double* __restrict__ W, const double* __re
     }
     block_sum_n<1>(v, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+// mu = Ginv (Q^T p): block partials of the k dot products, finished by the last block.
+__global__ void __launch_bounds__(kThreads)
+k_deflate_mu(int64_t n, int k, const double* __restrict__ Q, const double* __restrict__ p,
+             const double* __restrict__ Ginv, double* __restrict__ mu, PcgScalars* S, double* partials) {
+    __shared__ double sh[kMaxRitz][32];
+    __shared__ bool last;
+    if (S->done) return;
+    double v[kMaxRitz];
+#pragma unroll
+    for (int j = 0; j < kMaxRitz; ++j) v[j] = 0.0;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+        const double pe = p[e];
+#pragma unroll
+        for (int j = 0; j < kMaxRitz; ++j)
+            if (j < k) v[j] += Q[j * n + e] * pe;
+    }
+    block_sum_n<kMaxRitz>(v, sh);
+    if (publish_partials<kMaxRitz>(v, partials, &S->ticket, &last)) {
+        double t[kMaxRitz];
+        final_sums<kMaxRitz>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < k; ++i) {
+                double m = 0.0;
+                for (int j = 0; j < k; ++j) m += Ginv[i * k + j] * t[j];
+                mu[i] = m;
+            }
+            S->ticket = 0u;
+        }
+    }
+}
+
+// p -= W mu; with update_pr also p.r into S->rz (the flexible CG's numerator of alpha).
+__global__ void __launch_bounds__(kThreads)
+k_deflate_apply(int64_t n, int k, const double* __restrict__ W, const double* __restrict__ mu, double* __restrict__ p,
+                const double* __restrict__ r, PcgScalars* S, double* partials, int update_pr) {
+    __shared__ double sh[1][32];
+    __shared__ bool last;
+    if (S->done) return;
+    double m[kMaxRitz];
+#pragma unroll
+    for (int j = 0; j < kMaxRitz; ++j) m[j] = j < k ? mu[j] : 0.0;
+    double v[1] = {0.0};
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+        double pe = p[e];
+#pragma unroll
+        for (int j = 0; j < kMaxRitz; ++j)
+            if (j < k) pe -= W[j * n + e] * m[j];
+        p[e] = pe;
+        if (update_pr) v[0] += pe * r[e];
+    }
+    if (!update_pr) return;
+    block_sum_n<1>(v, sh);
+    if (publish_partials<1>(v, partials, &S->ticket, &last)) {
+        double t[1];
+        final_sums<1>(t, partials, sh);
+        if (threadIdx.x == 0) {
+            S->rz = t[0];
+            if (!isfinite(t[0])) { S->nonfinite = 1; S->done = 1; }
+            S->ticket = 0u;
+        }
+    }
 }
 
 __global__ void k_residual(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax,
@@ -169,6 +239,7 @@ int ritz_guess(plato_problem* h, const double* b, double* x) {
         for (int bk = 0; bk < VB; ++bk) t += part[size_t(q) * VB + bk];
         c[i] = t;
     }
+    std::vector<double> Gram = G;
     if (!cholesky_solve(G, k, c)) return PLATO_OK;  // degenerate subspace: keep x
     double rr0 = 0.0;
     rc = launch_dot(h, r, r, n, &rr0);
@@ -184,10 +255,42 @@ int ritz_guess(plato_problem* h, const double* b, double* x) {
     double rr1 = 0.0;
     for (int bk = 0; bk < VB; ++bk) rr1 += host_rr[bk];
     h->ritz_rel_gain = rr0 > 0.0 ? std::sqrt(rr1 / rr0) : 1.0;
-    if (std::isfinite(rr1) && rr1 <= kResidualGuard * kResidualGuard * rr0)
+    const bool keep = std::isfinite(rr1) && rr1 <= kResidualGuard * kResidualGuard * rr0;
+    if (keep)
         PLATO_CUDA(h, cudaMemcpyAsync(x, h->v_tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     else
         h->ritz_rel_gain = 1.0;
+    // deflation needs the Galerkin guess (residual orthogonal to P W): G^-1 column by column
+    if (h->ritz_deflate && keep) {
+        std::vector<double> Ginv(size_t(k) * k);
+        for (int j = 0; j < k; ++j) {
+            std::vector<double> e(k, 0.0);
+            e[j] = 1.0;
+            if (!cholesky_solve(Gram, k, e)) return PLATO_OK;
+            for (int i = 0; i < k; ++i) Ginv[i * k + j] = e[i];
+        }
+        if (!h->ritz_small) PLATO_CUDA(h, cudaMalloc(&h->ritz_small, sizeof(double) * (kMaxRitz * kMaxRitz + kMaxRitz)));
+        PLATO_CUDA(h, cudaMemcpyAsync(h->ritz_small, Ginv.data(), sizeof(double) * k * k, cudaMemcpyHostToDevice, s));
+        PLATO_CUDA(h, cudaStreamSynchronize(s));
+        h->ritz_deflating = 1;
+    }
+    return PLATO_OK;
+}
+
+// One deflation of the search direction p (see the file comment); update_pr recomputes p.r.
+int deflate_direction(plato_problem* h, double* p, const double* r, int update_pr) {
+    if (!h->ritz_deflating) return PLATO_OK;
+    const int k = h->ritz_k;
+    const int64_t n = 3 * int64_t(h->N);
+    double* Wm = h->ritz_scratch;
+    double* Q = Wm + int64_t(k) * n;
+    const int VB = grid_for(n, kThreads, 148 * 8);
+    double* Ginv = h->ritz_small;
+    double* mu = h->ritz_small + kMaxRitz * kMaxRitz;
+    k_deflate_mu<<<VB, kThreads, 0, h->stream>>>(n, k, Q, p, Ginv, mu, h->scal, h->partials);
+    PLATO_LAUNCH_CHECK(h);
+    k_deflate_apply<<<VB, kThreads, 0, h->stream>>>(n, k, Wm, mu, p, r, h->scal, h->partials, update_pr);
+    PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }
 

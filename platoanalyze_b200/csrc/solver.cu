@@ -327,6 +327,10 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
         k_pcg_start<<<vec_blocks, kThreads, 0, s>>>(n, b, h->v_r, dinv, h->v_z, h->v_p, h->scal,
                                                      h->partials, tol, keep_bb ? 1 : 0);
         PLATO_LAUNCH_CHECK(h);
+        if (!p2) {
+            rc = deflate_direction(h, h->v_p, nullptr, 0);
+            if (rc) return rc;
+        }
         PcgScalars* slots = h->scal_host;
         int64_t enqueued = 0;
         std::vector<int64_t> timed_iters;
@@ -359,7 +363,11 @@ static int pcg_run(plato_problem* h, int64_t n, Apply apply, ApplyDir apply_dir,
                 if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
                 k_pcg_update<<<vec_blocks, kThreads, 0, s>>>(n, x, h->v_r, pbuf[pcur], h->v_Ap, dinv, h->v_z,
                                                              h->scal, h->partials, max_it);
-                if (!p2) k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
+                if (!p2) {
+                    k_pcg_direction<<<vec_blocks, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->scal);
+                    rc = deflate_direction(h, h->v_p, nullptr, 0);
+                    if (rc) return rc;
+                }
             }
             // the operator applies count themselves
             h->launches += (p2 ? chunk : 2 * chunk) - 1;

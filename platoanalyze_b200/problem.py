@@ -178,7 +178,8 @@ class EllipticProblem:
         n, ms, k = C.c_int64(), C.c_double(), C.c_int64()
         check(lib.plato_get_instrumentation(self.h, C.byref(n), C.byref(ms), C.byref(k)), self.h)
         out = {"launches": n.value, "op_ms_total": ms.value, "op_timed": k.value}
-        for kind, name in ((1, "inner"), (2, "assembly"), (3, "coarse_galerkin"), (4, "coarse_inverse")):
+        for kind, name in ((1, "inner"), (2, "assembly"), (3, "coarse_galerkin"), (4, "coarse_inverse"),
+                           (5, "residual"), (6, "energy"), (7, "dcdz")):
             t, c = C.c_double(), C.c_int64()
             check(lib.plato_get_kernel_timing(self.h, kind, C.byref(t), C.byref(c)), self.h)
             out[name + "_ms_total"], out[name + "_timed"] = t.value, c.value
@@ -305,6 +306,17 @@ class EllipticProblem:
         st = capi.SolveStats()
         ratio = C.c_double()
         check(lib.plato_problem_solution_subspace(self.h, self._dev(z), self._dev(u0) if u0 is not None else None,
+                                                  self._dev(W), int(W.shape[0]), self._dev(u), C.byref(st),
+                                                  C.byref(ratio)), self.h)
+        return u, st.as_dict(), ratio.value
+
+    def solution_deflated(self, z, W, u0=None):
+        """Problem::solution with the Galerkin guess on span(P W) and deflated Krylov directions
+        (W a (k, 3N) device array); returns (u, stats, residual ratio of the guess)."""
+        u = self.zeros(self.num_dofs)
+        st = capi.SolveStats()
+        ratio = C.c_double()
+        check(lib.plato_problem_solution_deflated(self.h, self._dev(z), self._dev(u0) if u0 is not None else None,
                                                   self._dev(W), int(W.shape[0]), self._dev(u), C.byref(st),
                                                   C.byref(ratio)), self.h)
         return u, st.as_dict(), ratio.value

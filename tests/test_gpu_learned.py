@@ -119,10 +119,37 @@ def test_trained_network_end_to_end():
     test = [design_density(n, rng.uniform(0.2, 0.6), rng) for _ in range(6)]
     trs = [v / np.linalg.norm(v) for v in rng.standard_normal((6, 3))]
     rows = evaluate(net, n, test, trs, "plain")
-    assert all(r["u_rel_diff"] <= 1e-4 for r in rows)
+    assert all(r["u_rel_diff"] <= 1e-4 and r["u_rel_diff_deflated"] <= 1e-4 for r in rows)
     assert all(0.0 <= r["energy_captured"] <= 1.0 + 1e-9 for r in rows)
     it0 = np.mean([r["iterations"] for r in rows])
     it1 = np.mean([r["iterations_learned"] for r in rows])
-    print(f"plain Jacobi-PCG on held-out 16x8x8 designs: {it0:.1f} iterations from zero, {it1:.1f} from the "
-          f"learned guess; energy captured {np.mean([r['energy_captured'] for r in rows]):.3f}")
-    assert it1 <= 1.05 * it0
+    it2 = np.mean([r["iterations_deflated"] for r in rows])
+    gain = {"iterations_zero_guess": it0, "iterations_learned_guess": it1, "iterations_learned_deflation": it2,
+            "energy_captured": float(np.mean([r["energy_captured"] for r in rows]))}
+    print(f"learned gain on held-out 16x8x8 designs (plain Jacobi-PCG to 1e-8): {gain}")
+    # what the network gains is measured, not assumed: the deflated solve reaches the same
+    # answer, and neither the guess nor the deflation may cost more than a few iterations
+    assert it1 <= it0 + 5 and it2 <= it0 + 5, gain
+
+
+def test_deflation_by_responses_of_a_nearby_design(small_cantilever):
+    """Deflated CG with the unit-load responses of a different (uniform) design: smooth global
+    bending modes.  The deflated solve reaches the plain solve's answer in fewer iterations
+    than both the zero guess and the Galerkin guess alone."""
+    prob, spec, zd, W, tr = small_cantilever
+    n = 16
+    opts = SolverOptions(tolerance=1e-10, max_iterations=20000)
+    probs = unit_load_problems(n, opts)
+    zu = probs[0].to_dev(np.full(prob.num_nodes, 0.5))
+    Wn = torch.stack([p.solution(zu)[0] for p in probs])
+    u_ref, st_ref = prob.solution(zd)
+    u_g, st_g, _ = subspace_solution(prob, zd, Wn)
+    u_d, st_d, _ = prob.solution_deflated(zd, Wn)
+    assert st_d["converged"] == 1 and rel_l2(u_d.cpu().numpy(), u_ref.cpu().numpy()) <= 1e-8
+    print(f"iterations: zero guess {st_ref['iterations']}, Galerkin guess {st_g['iterations']}, "
+          f"deflated {st_d['iterations']}")
+    assert st_d["iterations"] < st_ref["iterations"] and st_d["iterations"] <= st_g["iterations"]
+    # with the exact responses the deflated solve, like the guess, is done at once
+    u_e, st_e, _ = prob.solution_deflated(zd, W)
+    assert st_e["iterations"] <= st_ref["iterations"] // 10
+    assert rel_l2(u_e.cpu().numpy(), u_ref.cpu().numpy()) <= 1e-8

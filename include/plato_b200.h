@@ -307,6 +307,24 @@ int plato_batch_last_stats(const plato_problem* h, plato_solve_stats* stats);
  * each member) into values[count] [device]; synchronises the handle's stream */
 int plato_batch_criterion_values(plato_problem* h, const double* z, const double* u, double* values);
 
+/* Autotuner of the batched solve (no reference counterpart).  The batched Krylov kernels are
+ * persistent: a grid of ctas_per_sm x SMs CTAs walks the members' row tiles (tiles of
+ * tile_rows rows, never across two members, one row per thread), skipping converged members.
+ * plato_batch_autotune times every pair tile_rows in {128, 256, 512} x ctas_per_sm in
+ * {2, 4, 8, 16} on 8 flexible-CG iterations of this batch with control z [device] (the
+ * handle's solver options; the callers' vectors are untouched), keeps the fastest for the
+ * handle's later solves and reports all timings.  Without it a batch uses 256 x 8. */
+typedef struct plato_batch_tuning {
+    int32_t tile_rows;            /* chosen */
+    int32_t ctas_per_sm;          /* chosen */
+    int32_t candidates;           /* pairs timed */
+    int32_t iterations;           /* flexible-CG iterations per timing */
+    int32_t tile_rows_tried[16];
+    int32_t ctas_per_sm_tried[16];
+    double  ms_tried[16];         /* set-up + iterations of each pair (second of two runs) */
+} plato_batch_tuning;
+int plato_batch_autotune(plato_problem* h, const double* z, plato_batch_tuning* out);
+
 /* Problem::solution with an initial guess improved on a subspace (no reference counterpart;
  * the learned warm start uses it).  W holds k <= 8 columns of 3N values [device]; after the
  * operator is assembled and constrained, the iterate x (u0, or zero) becomes x + P W c with

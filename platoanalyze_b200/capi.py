@@ -72,6 +72,18 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("tile_rows", C.c_int32), ("ctas_per_sm", C.c_int32), ("candidates", C.c_int32),
+                ("iterations", C.c_int32), ("tile_rows_tried", C.c_int32 * 16), ("ctas_per_sm_tried", C.c_int32 * 16),
+                ("ms_tried", C.c_double * 16)]
+
+    def as_dict(self) -> dict:
+        k = self.candidates
+        return {"tile_rows": self.tile_rows, "ctas_per_sm": self.ctas_per_sm, "iterations": self.iterations,
+                "tried": [{"tile_rows": self.tile_rows_tried[i], "ctas_per_sm": self.ctas_per_sm_tried[i],
+                           "ms": self.ms_tried[i]} for i in range(k)]}
+
+
 class PlatoError(RuntimeError):
     def __init__(self, status: int, msg: str):
         name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
@@ -91,6 +103,7 @@ def _load() -> C.CDLL:
         "plato_set_stream": ([vp, vp], C.c_int),
         "plato_set_solver_opts": ([vp, C.POINTER(SolverOpts)], C.c_int),
         "plato_set_control_layout": ([vp, C.c_int32], C.c_int),
+        "plato_batch_autotune": ([vp, vp, C.POINTER(BatchTuning)], C.c_int),
         "plato_set_timing": ([vp, C.c_int32], C.c_int),
         "plato_get_instrumentation": ([vp, C.POINTER(C.c_int64), f64p, C.POINTER(C.c_int64)], C.c_int),
         "plato_reset_instrumentation": ([vp], C.c_int),

@@ -16,6 +16,8 @@
 
 namespace plato {
 
+int solve_state(plato_problem* h, const double* z, const double* u0, double* u, plato_solve_stats* st);
+
 void batch_release(plato_problem* h) {
     BatchState& b = h->batch;
     for (int32_t** p : {&b.cta_seg, &b.cta_row0, &b.cta_row1, &b.seg_cta0, &b.cell_off_d, &b.ndone})
@@ -29,19 +31,26 @@ void batch_release(plato_problem* h) {
 
 namespace {
 
-// Tiles of at most kTileRows rows that never straddle two members; inside a member the
-// tiles after the first start on multiples of kTileRows (aligned with the SELL slices).
-constexpr int kTileRows = 256;
+// Tiles of at most b.tile_rows rows that never straddle two members; inside a member the
+// tiles after the first start on multiples of tile_rows (aligned with the SELL slices).
+// Rebuilt when the autotuner changes the tile size.
+void free_tiles(BatchState& b) {
+    for (int32_t** p : {&b.cta_seg, &b.cta_row0, &b.cta_row1, &b.seg_cta0})
+        if (*p) { cudaFree(*p); *p = nullptr; }
+    if (b.partials) { cudaFree(b.partials); b.partials = nullptr; }
+}
 
 int setup_tiles(plato_problem* h) {
     BatchState& b = h->batch;
+    const int64_t T = b.tile_rows;
+    free_tiles(b);
     std::vector<int32_t> seg, r0, r1, first(b.nseg + 1, 0);
     for (int s = 0; s < b.nseg; ++s) {
         first[s] = int32_t(seg.size());
         int64_t a = b.node_off[s];
         const int64_t e = b.node_off[s + 1];
         while (a < e) {
-            const int64_t next = std::min<int64_t>(e, (a / kTileRows + 1) * kTileRows);
+            const int64_t next = std::min<int64_t>(e, (a / T + 1) * T);
             seg.push_back(s);
             r0.push_back(int32_t(a));
             r1.push_back(int32_t(next));
@@ -54,18 +63,20 @@ int setup_tiles(plato_problem* h) {
     PLATO_CUDA(h, cudaMalloc(&b.cta_row0, sizeof(int32_t) * b.ncta));
     PLATO_CUDA(h, cudaMalloc(&b.cta_row1, sizeof(int32_t) * b.ncta));
     PLATO_CUDA(h, cudaMalloc(&b.seg_cta0, sizeof(int32_t) * (b.nseg + 1)));
-    PLATO_CUDA(h, cudaMalloc(&b.cell_off_d, sizeof(int32_t) * (b.nseg + 1)));
-    PLATO_CUDA(h, cudaMalloc(&b.ndone, sizeof(int32_t)));
     PLATO_CUDA(h, cudaMalloc(&b.partials, sizeof(double) * 2 * b.ncta));
-    PLATO_CUDA(h, cudaMalloc(&b.values, sizeof(double) * size_t(b.nseg) * kEnergySplit));
-    PLATO_CUDA(h, cudaMalloc(&b.S, sizeof(SegScalars) * b.nseg));
-    PLATO_CUDA(h, cudaMallocHost(reinterpret_cast<void**>(&b.S_host), sizeof(SegScalars) * b.nseg));
+    if (!b.cell_off_d) PLATO_CUDA(h, cudaMalloc(&b.cell_off_d, sizeof(int32_t) * (b.nseg + 1)));
+    if (!b.ndone) PLATO_CUDA(h, cudaMalloc(&b.ndone, sizeof(int32_t)));
+    if (!b.values) PLATO_CUDA(h, cudaMalloc(&b.values, sizeof(double) * size_t(b.nseg) * kEnergySplit));
+    if (!b.S) {
+        PLATO_CUDA(h, cudaMalloc(&b.S, sizeof(SegScalars) * b.nseg));
+        PLATO_CUDA(h, cudaMemset(b.S, 0, sizeof(SegScalars) * b.nseg));
+    }
+    if (!b.S_host) PLATO_CUDA(h, cudaMallocHost(reinterpret_cast<void**>(&b.S_host), sizeof(SegScalars) * b.nseg));
     PLATO_CUDA(h, cudaMemcpy(b.cta_seg, seg.data(), sizeof(int32_t) * b.ncta, cudaMemcpyHostToDevice));
     PLATO_CUDA(h, cudaMemcpy(b.cta_row0, r0.data(), sizeof(int32_t) * b.ncta, cudaMemcpyHostToDevice));
     PLATO_CUDA(h, cudaMemcpy(b.cta_row1, r1.data(), sizeof(int32_t) * b.ncta, cudaMemcpyHostToDevice));
     PLATO_CUDA(h, cudaMemcpy(b.seg_cta0, first.data(), sizeof(int32_t) * (b.nseg + 1), cudaMemcpyHostToDevice));
     PLATO_CUDA(h, cudaMemcpy(b.cell_off_d, b.cell_off.data(), sizeof(int32_t) * (b.nseg + 1), cudaMemcpyHostToDevice));
-    PLATO_CUDA(h, cudaMemset(b.S, 0, sizeof(SegScalars) * b.nseg));
     return PLATO_OK;
 }
 
@@ -193,6 +204,68 @@ int plato_batch_last_stats(const plato_problem* h, plato_solve_stats* stats) {
         return plato_fail(const_cast<plato_problem*>(h), PLATO_BAD_INPUT, "no batched solve has run on this handle");
     std::copy(b.last.begin(), b.last.end(), stats);
     return PLATO_OK;
+}
+
+// The project's autotuner of the batched solve: every (tile rows, CTAs per SM) candidate runs
+// kAutotuneIterations flexible-CG iterations of this batch (assembly and preconditioner set-up
+// included, the same for every candidate) on a scratch state; the fastest pair is kept.
+int plato_batch_autotune(plato_problem* h, const double* z, plato_batch_tuning* out) {
+    if (!h) return PLATO_BAD_INPUT;
+    if (!z || !out) return plato_fail(h, PLATO_BAD_INPUT, "null pointer");
+    BatchState& b = h->batch;
+    if (b.nseg == 0) return plato_fail(h, PLATO_BAD_INPUT, "not a batch handle");
+    static const int32_t kRows[] = {128, 256, 512};
+    static const int32_t kCtas[] = {2, 4, 8, 16};
+    constexpr int32_t kAutotuneIterations = 8;
+    double* x = nullptr;
+    PLATO_CUDA(h, cudaMalloc(&x, sizeof(double) * 3 * size_t(h->N)));
+    const plato_solver_opts saved = h->opts;
+    h->opts.max_iterations = kAutotuneIterations;
+    h->opts.fallback_max_iterations = -1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = -1, k = 0, rc = PLATO_OK;
+    double best_ms = 0.0;
+    *out = plato_batch_tuning{};
+    for (int32_t rows : kRows)
+        for (int32_t ctas : kCtas) {
+            b.tile_rows = rows;
+            b.ctas_per_sm = ctas;
+            rc = setup_tiles(h);
+            if (rc) break;
+            plato_solve_stats st{};
+            float ms = 0.f;
+            // the first run of a candidate warms it up; the second is timed
+            for (int rep = 0; rep < 2 && rc == PLATO_OK; ++rep) {
+                cudaEventRecord(e0, h->stream);
+                const int r = solve_state(h, z, nullptr, x, &st);
+                cudaEventRecord(e1, h->stream);
+                if (r != PLATO_OK && r != PLATO_NOT_CONVERGED) rc = r;
+            }
+            if (rc) break;
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms, e0, e1);
+            out->tile_rows_tried[k] = rows;
+            out->ctas_per_sm_tried[k] = ctas;
+            out->ms_tried[k] = ms;
+            if (best < 0 || ms < best_ms) { best = k; best_ms = ms; }
+            ++k;
+        }
+    h->opts = saved;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(x);
+    h->last_error.clear();
+    if (rc) return rc;
+    out->candidates = k;
+    out->tile_rows = out->tile_rows_tried[best];
+    out->ctas_per_sm = out->ctas_per_sm_tried[best];
+    out->iterations = kAutotuneIterations;
+    b.tile_rows = out->tile_rows;
+    b.ctas_per_sm = out->ctas_per_sm;
+    b.tuned = 1;
+    return setup_tiles(h);
 }
 
 int plato_batch_criterion_values(plato_problem* h, const double* z, const double* u, double* values) {

@@ -875,23 +875,26 @@ namespace {
 
 struct BatchView {
     int32_t        nseg;
-    const int32_t* cta_seg;
-    const int32_t* cta_row0;
-    const int32_t* cta_row1;
-    const int32_t* seg_cta0;
+    int32_t        ntiles;
+    const int32_t* cta_seg;   // member of each tile
+    const int32_t* cta_row0;  // first row of each tile
+    const int32_t* cta_row1;  // one past its last row
+    const int32_t* seg_cta0;  // first tile of each member
     SegScalars*    S;
     PcgScalars*    G;
     int32_t*       ndone;
-    double*        partials;
+    double*        partials;  // NV per tile
 };
 
+// Block sums of tile t's values into its partials; true in the CTA that finishes the
+// member's last tile (its view of the member's partials is then complete).
 template <int NV>
-__device__ __forceinline__ bool seg_publish(const BatchView& B, int s, double (&v)[NV], double (*sh)[32],
+__device__ __forceinline__ bool seg_publish(const BatchView& B, int s, int t, double (&v)[NV], double (*sh)[32],
                                             bool* sh_last) {
     block_sum_n<NV>(v, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) B.partials[NV * blockIdx.x + q] = v[q];
+        for (int q = 0; q < NV; ++q) B.partials[NV * t + q] = v[q];
         __threadfence();
         const unsigned tiles = unsigned(B.seg_cta0[s + 1] - B.seg_cta0[s]);
         *sh_last = atomicAdd(&B.S[s].ticket, 1u) == tiles - 1u;
@@ -916,204 +919,219 @@ __device__ __forceinline__ void seg_mark_done(const BatchView& B) {
     if (atomicAdd(B.ndone, 1) + 1 == B.nseg) B.G->done = 1;
 }
 
+// Every batched kernel is persistent: a grid of (CTAs per SM) x SMs walks the member tiles
+// (tile t, then t + gridDim.x, ...), one row of the tile per thread (blockDim.x = the tile
+// rows the autotuner chose), skipping the tiles of members that are done.
+constexpr int kMaxTileRows = 512;
+
 // r = b - A x (A x in r on entry), r.r and b.b per member; starts the preconditioner.
 // accept scales the stop test (1: the FP64 true residual must meet the tolerance).
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxTileRows)
 k_bfcg_start(BatchView B, const double* __restrict__ b, double* __restrict__ r, const float* __restrict__ dinv32,
              float* __restrict__ res, float* __restrict__ d, float* __restrict__ y, float c0, double tol,
              int keep_bb, double accept) {
     __shared__ double sh[2][32];
     __shared__ bool last;
-    const int s = B.cta_seg[blockIdx.x];
-    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
-    double v[2] = {0.0, 0.0};
-    if (row < B.cta_row1[blockIdx.x]) {
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int s = B.cta_seg[t];
+        const int64_t row = B.cta_row0[t] + threadIdx.x;
+        double v[2] = {0.0, 0.0};
+        if (row < B.cta_row1[t]) {
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const int64_t k = 3 * row + i;
-            const double ri = b[k] - r[k];
-            r[k] = ri;
-            v[0] += ri * ri;
-            v[1] += b[k] * b[k];
-            const float rf = float(ri);
-            const float di = c0 * dinv32[k] * rf;
-            res[k] = rf;
-            d[k] = di;
-            y[k] = di;
-        }
-    }
-    if (seg_publish<2>(B, s, v, sh, &last)) {
-        double t[2];
-        seg_final<2>(B, s, t, sh);
-        if (threadIdx.x == 0) {
-            SegScalars& S = B.S[s];
-            S.rr = t[0];
-            if (!keep_bb) {
-                S.bb = t[1];
-                S.tol2 = tol * tol * t[1];
-                S.iter = 0;
+            for (int i = 0; i < 3; ++i) {
+                const int64_t k = 3 * row + i;
+                const double ri = b[k] - r[k];
+                r[k] = ri;
+                v[0] += ri * ri;
+                v[1] += b[k] * b[k];
+                const float rf = float(ri);
+                const float di = c0 * dinv32[k] * rf;
+                res[k] = rf;
+                d[k] = di;
+                y[k] = di;
             }
-            S.nonfinite = (!isfinite(t[0]) || !isfinite(t[1])) ? 1 : 0;
-            S.done = (t[0] <= accept * accept * S.tol2 || S.nonfinite) ? 1 : 0;
-            if (S.done) seg_mark_done(B);
-            S.ticket = 0u;
+        }
+        if (seg_publish<2>(B, s, t, v, sh, &last)) {
+            double tt[2];
+            seg_final<2>(B, s, tt, sh);
+            if (threadIdx.x == 0) {
+                SegScalars& S = B.S[s];
+                S.rr = tt[0];
+                if (!keep_bb) {
+                    S.bb = tt[1];
+                    S.tol2 = tol * tol * tt[1];
+                    S.iter = 0;
+                }
+                S.nonfinite = (!isfinite(tt[0]) || !isfinite(tt[1])) ? 1 : 0;
+                S.done = (tt[0] <= accept * accept * S.tol2 || S.nonfinite) ? 1 : 0;
+                if (S.done) seg_mark_done(B);
+                S.ticket = 0u;
+            }
         }
     }
 }
 
 // q = A p (FP64 SELL rows of the tile), p.q per member -> alpha = (p.r)/(p.q)
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxTileRows)
 k_bfcg_apply(BatchView B, SellView A, const double* __restrict__ vals, const double* __restrict__ p,
              double* __restrict__ q) {
     __shared__ double sh[1][32];
     __shared__ bool last;
-    const int s = B.cta_seg[blockIdx.x];
-    if (B.S[s].done) return;
-    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
-    double v[1] = {0.0};
-    if (row < B.cta_row1[blockIdx.x]) {
-        double a0, a1, a2;
-        sell_row<double>(A, vals, p, row, a0, a1, a2);
-        q[3 * row] = a0;
-        q[3 * row + 1] = a1;
-        q[3 * row + 2] = a2;
-        v[0] = p[3 * row] * a0 + p[3 * row + 1] * a1 + p[3 * row + 2] * a2;
-    }
-    if (seg_publish<1>(B, s, v, sh, &last)) {
-        double t[1];
-        seg_final<1>(B, s, t, sh);
-        if (threadIdx.x == 0) {
-            SegScalars& S = B.S[s];
-            S.pq = t[0];
-            S.alpha = S.pr / t[0];
-            if (!isfinite(S.alpha) || t[0] <= 0.0) {
-                S.nonfinite = 1;
-                S.done = 1;
-                seg_mark_done(B);
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int s = B.cta_seg[t];
+        if (B.S[s].done) continue;
+        const int64_t row = B.cta_row0[t] + threadIdx.x;
+        double v[1] = {0.0};
+        if (row < B.cta_row1[t]) {
+            double a0, a1, a2;
+            sell_row<double>(A, vals, p, row, a0, a1, a2);
+            q[3 * row] = a0;
+            q[3 * row + 1] = a1;
+            q[3 * row + 2] = a2;
+            v[0] = p[3 * row] * a0 + p[3 * row + 1] * a1 + p[3 * row + 2] * a2;
+        }
+        if (seg_publish<1>(B, s, t, v, sh, &last)) {
+            double tt[1];
+            seg_final<1>(B, s, tt, sh);
+            if (threadIdx.x == 0) {
+                SegScalars& S = B.S[s];
+                S.pq = tt[0];
+                S.alpha = S.pr / tt[0];
+                if (!isfinite(S.alpha) || tt[0] <= 0.0) {
+                    S.nonfinite = 1;
+                    S.done = 1;
+                    seg_mark_done(B);
+                }
+                S.ticket = 0u;
             }
-            S.ticket = 0u;
         }
     }
 }
 
 // x += alpha p; r -= alpha q; r.r and the member's stop test; starts the preconditioner.
 // Tiles of converged members clear their preconditioner vectors instead.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxTileRows)
 k_bfcg_update(BatchView B, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
               const double* __restrict__ q, const float* __restrict__ dinv32, float* __restrict__ res,
               float* __restrict__ d, float* __restrict__ y, float c0, int32_t max_it) {
     __shared__ double sh[1][32];
     __shared__ bool last;
-    const int s = B.cta_seg[blockIdx.x];
-    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
-    const bool in = row < B.cta_row1[blockIdx.x];
-    if (B.S[s].done) {
-        if (in)
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int s = B.cta_seg[t];
+        const int64_t row = B.cta_row0[t] + threadIdx.x;
+        const bool in = row < B.cta_row1[t];
+        if (B.S[s].done) {
+            if (in)
 #pragma unroll
-            for (int i = 0; i < 3; ++i) res[3 * row + i] = d[3 * row + i] = y[3 * row + i] = 0.f;
-        return;
-    }
-    const double alpha = B.S[s].alpha;
-    double v[1] = {0.0};
-    if (in) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const int64_t k = 3 * row + i;
-            x[k] += alpha * p[k];
-            const double ri = r[k] - alpha * q[k];
-            r[k] = ri;
-            v[0] += ri * ri;
-            const float rf = float(ri);
-            const float di = c0 * dinv32[k] * rf;
-            res[k] = rf;
-            d[k] = di;
-            y[k] = di;
+                for (int i = 0; i < 3; ++i) res[3 * row + i] = d[3 * row + i] = y[3 * row + i] = 0.f;
+            continue;
         }
-    }
-    if (seg_publish<1>(B, s, v, sh, &last)) {
-        double t[1];
-        seg_final<1>(B, s, t, sh);
-        if (threadIdx.x == 0) {
-            SegScalars& S = B.S[s];
-            S.rr = t[0];
-            S.iter += 1;
-            if (!isfinite(t[0])) S.nonfinite = 1;
-            if (S.nonfinite || t[0] <= S.tol2 || S.iter >= max_it) {
-                S.done = 1;
-                seg_mark_done(B);
+        const double alpha = B.S[s].alpha;
+        double v[1] = {0.0};
+        if (in) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int64_t k = 3 * row + i;
+                x[k] += alpha * p[k];
+                const double ri = r[k] - alpha * q[k];
+                r[k] = ri;
+                v[0] += ri * ri;
+                const float rf = float(ri);
+                const float di = c0 * dinv32[k] * rf;
+                res[k] = rf;
+                d[k] = di;
+                y[k] = di;
             }
-            S.ticket = 0u;
+        }
+        if (seg_publish<1>(B, s, t, v, sh, &last)) {
+            double tt[1];
+            seg_final<1>(B, s, tt, sh);
+            if (threadIdx.x == 0) {
+                SegScalars& S = B.S[s];
+                S.rr = tt[0];
+                S.iter += 1;
+                if (!isfinite(tt[0])) S.nonfinite = 1;
+                if (S.nonfinite || tt[0] <= S.tol2 || S.iter >= max_it) {
+                    S.done = 1;
+                    seg_mark_done(B);
+                }
+                S.ticket = 0u;
+            }
         }
     }
 }
 
 // z = y (widened); z.q per member -> beta = -(z.q)/(p.q).  first: only z = y.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxTileRows)
 k_bfcg_zq(BatchView B, const float* __restrict__ y, double* __restrict__ z, const double* __restrict__ q, int first) {
     __shared__ double sh[1][32];
     __shared__ bool last;
-    const int s = B.cta_seg[blockIdx.x];
-    if (B.S[s].done) return;
-    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
-    const bool in = row < B.cta_row1[blockIdx.x];
-    double v[1] = {0.0};
-    if (in)
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int s = B.cta_seg[t];
+        if (B.S[s].done) continue;
+        const int64_t row = B.cta_row0[t] + threadIdx.x;
+        const bool in = row < B.cta_row1[t];
+        double v[1] = {0.0};
+        if (in)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const int64_t k = 3 * row + i;
-            const double zi = double(y[k]);
-            z[k] = zi;
-            if (!first) v[0] += zi * q[k];
-        }
-    if (first) return;
-    if (seg_publish<1>(B, s, v, sh, &last)) {
-        double t[1];
-        seg_final<1>(B, s, t, sh);
-        if (threadIdx.x == 0) {
-            SegScalars& S = B.S[s];
-            S.zq = t[0];
-            S.beta = -t[0] / S.pq;
-            if (!isfinite(S.beta)) {
-                S.nonfinite = 1;
-                S.done = 1;
-                seg_mark_done(B);
+            for (int i = 0; i < 3; ++i) {
+                const int64_t k = 3 * row + i;
+                const double zi = double(y[k]);
+                z[k] = zi;
+                if (!first) v[0] += zi * q[k];
             }
-            S.ticket = 0u;
+        if (first) continue;
+        if (seg_publish<1>(B, s, t, v, sh, &last)) {
+            double tt[1];
+            seg_final<1>(B, s, tt, sh);
+            if (threadIdx.x == 0) {
+                SegScalars& S = B.S[s];
+                S.zq = tt[0];
+                S.beta = -tt[0] / S.pq;
+                if (!isfinite(S.beta)) {
+                    S.nonfinite = 1;
+                    S.done = 1;
+                    seg_mark_done(B);
+                }
+                S.ticket = 0u;
+            }
         }
     }
 }
 
 // p = z + beta p; p.r per member.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxTileRows)
 k_bfcg_direction(BatchView B, const double* __restrict__ z, double* __restrict__ p, const double* __restrict__ r,
                  int first) {
     __shared__ double sh[1][32];
     __shared__ bool last;
-    const int s = B.cta_seg[blockIdx.x];
-    if (B.S[s].done) return;
-    const double beta = first ? 0.0 : B.S[s].beta;
-    const int64_t row = B.cta_row0[blockIdx.x] + threadIdx.x;
-    double v[1] = {0.0};
-    if (row < B.cta_row1[blockIdx.x])
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int s = B.cta_seg[t];
+        if (B.S[s].done) continue;
+        const double beta = first ? 0.0 : B.S[s].beta;
+        const int64_t row = B.cta_row0[t] + threadIdx.x;
+        double v[1] = {0.0};
+        if (row < B.cta_row1[t])
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const int64_t k = 3 * row + i;
-            const double pi = z[k] + (first ? 0.0 : beta * p[k]);
-            p[k] = pi;
-            v[0] += pi * r[k];
-        }
-    if (seg_publish<1>(B, s, v, sh, &last)) {
-        double t[1];
-        seg_final<1>(B, s, t, sh);
-        if (threadIdx.x == 0) {
-            SegScalars& S = B.S[s];
-            S.pr = t[0];
-            if (!isfinite(t[0])) {
-                S.nonfinite = 1;
-                S.done = 1;
-                seg_mark_done(B);
+            for (int i = 0; i < 3; ++i) {
+                const int64_t k = 3 * row + i;
+                const double pi = z[k] + (first ? 0.0 : beta * p[k]);
+                p[k] = pi;
+                v[0] += pi * r[k];
             }
-            S.ticket = 0u;
+        if (seg_publish<1>(B, s, t, v, sh, &last)) {
+            double tt[1];
+            seg_final<1>(B, s, tt, sh);
+            if (threadIdx.x == 0) {
+                SegScalars& S = B.S[s];
+                S.pr = tt[0];
+                if (!isfinite(tt[0])) {
+                    S.nonfinite = 1;
+                    S.done = 1;
+                    seg_mark_done(B);
+                }
+                S.ticket = 0u;
+            }
         }
     }
 }
@@ -1121,32 +1139,34 @@ k_bfcg_direction(BatchView B, const double* __restrict__ z, double* __restrict__
 // One Chebyshev step over the tiles of members still iterating (converged members' rows
 // are skipped): w = A d_cur, res -= w, d_next = c1 d_cur + c2 Dinv res, y += d_next.
 template <int KIND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxTileRows)
 k_bcheb_sell(BatchView B, SellView A, const void* __restrict__ vals, const float* __restrict__ dinv32,
              float* __restrict__ res, const float* __restrict__ dcur, float* __restrict__ dnext, float* __restrict__ y,
              float c1, float c2) {
-    if (B.S[B.cta_seg[blockIdx.x]].done) return;
-    const int64_t r = B.cta_row0[blockIdx.x] + threadIdx.x;
-    if (r >= B.cta_row1[blockIdx.x]) return;
-    float w0, w1, w2;
-    if (KIND == INNER_SELL16)
-        sell_row_bf16(A, static_cast<const __nv_bfloat16*>(vals), dcur, r, w0, w1, w2);
-    else if (KIND == INNER_SELL32)
-        sell_row<float>(A, static_cast<const float*>(vals), dcur, r, w0, w1, w2);
-    else {
-        double a0, a1, a2;
-        sell_row<double>(A, static_cast<const double*>(vals), dcur, r, a0, a1, a2);
-        w0 = float(a0); w1 = float(a1); w2 = float(a2);
-    }
-    const float w[3] = {w0, w1, w2};
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        if (B.S[B.cta_seg[t]].done) continue;
+        const int64_t r = B.cta_row0[t] + threadIdx.x;
+        if (r >= B.cta_row1[t]) continue;
+        float w0, w1, w2;
+        if (KIND == INNER_SELL16)
+            sell_row_bf16(A, static_cast<const __nv_bfloat16*>(vals), dcur, r, w0, w1, w2);
+        else if (KIND == INNER_SELL32)
+            sell_row<float>(A, static_cast<const float*>(vals), dcur, r, w0, w1, w2);
+        else {
+            double a0, a1, a2;
+            sell_row<double>(A, static_cast<const double*>(vals), dcur, r, a0, a1, a2);
+            w0 = float(a0); w1 = float(a1); w2 = float(a2);
+        }
+        const float w[3] = {w0, w1, w2};
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const int64_t k = 3 * r + i;
-        const float rs = res[k] - w[i];
-        res[k] = rs;
-        const float dn = c1 * dcur[k] + c2 * dinv32[k] * rs;
-        dnext[k] = dn;
-        y[k] += dn;
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * r + i;
+            const float rs = res[k] - w[i];
+            res[k] = rs;
+            const float dn = c1 * dcur[k] + c2 * dinv32[k] * rs;
+            dnext[k] = dn;
+            y[k] += dn;
+        }
     }
 }
 
@@ -1167,8 +1187,13 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
     if (kind == INNER_SELL16S)
         return plato_fail(h, PLATO_NOT_SUPPORTED, "the FP16 scaled inner precision is built for single problems");
     const SellView V = sell_view(h);
-    const int T = bt.ncta;
-    const BatchView BV{bt.nseg, bt.cta_seg, bt.cta_row0, bt.cta_row1, bt.seg_cta0, bt.S, h->scal, bt.ndone,
+    // persistent grid: the autotuned CTAs per SM x SMs (never more CTAs than tiles), one row of
+    // a tile per thread
+    const int TR = bt.tile_rows;
+    int sms = 0;
+    PLATO_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    const int T = std::max(1, std::min(bt.ncta, bt.ctas_per_sm * sms));
+    const BatchView BV{bt.nseg, bt.ncta, bt.cta_seg, bt.cta_row0, bt.cta_row1, bt.seg_cta0, bt.S, h->scal, bt.ndone,
                        bt.partials};
 
     double lmax = 0.0;
@@ -1182,13 +1207,13 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         float* dnext = h->f_d1;
         for (int k = 1; k < degree; ++k) {
             if (kind == INNER_SELL16)
-                k_bcheb_sell<INNER_SELL16><<<T, kThreads, 0, s>>>(BV, V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
+                k_bcheb_sell<INNER_SELL16><<<T, TR, 0, s>>>(BV, V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
                                                                   h->f_y, cc.c1[k], cc.c2[k]);
             else if (kind == INNER_SELL32)
-                k_bcheb_sell<INNER_SELL32><<<T, kThreads, 0, s>>>(BV, V, h->sell32, h->f_dinv, h->f_res, dcur, dnext,
+                k_bcheb_sell<INNER_SELL32><<<T, TR, 0, s>>>(BV, V, h->sell32, h->f_dinv, h->f_res, dcur, dnext,
                                                                   h->f_y, cc.c1[k], cc.c2[k]);
             else
-                k_bcheb_sell<INNER_SELL64><<<T, kThreads, 0, s>>>(BV, V, h->sell64, h->f_dinv, h->f_res, dcur, dnext,
+                k_bcheb_sell<INNER_SELL64><<<T, TR, 0, s>>>(BV, V, h->sell64, h->f_dinv, h->f_res, dcur, dnext,
                                                                   h->f_y, cc.c1[k], cc.c2[k]);
             PLATO_LAUNCH_CHECK(h);
             std::swap(dcur, dnext);
@@ -1196,11 +1221,37 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         return PLATO_OK;
     };
 
+    int64_t precond_applies = 0;
+    // One chunk of kChunk iterations: every parameter of its launches (pointers, Chebyshev
+    // coefficients, grid) is fixed for the solve and every scalar lives on the device, so on a
+    // capturable stream the chunk is captured into a CUDA graph once and replayed.
+    auto enqueue_chunk = [&]() -> int {
+        for (int k = 0; k < kChunk; ++k) {
+            k_bfcg_apply<<<T, TR, 0, s>>>(BV, V, h->sell64, h->v_p, h->v_q);
+            k_bfcg_update<<<T, TR, 0, s>>>(BV, x, h->v_r, h->v_p, h->v_q, h->f_dinv, h->f_res, h->f_d0,
+                                           h->f_y, cc.c0, max_it);
+            h->launches += 2;
+            int r2 = chebyshev_steps();
+            if (r2) return r2;
+            k_bfcg_zq<<<T, TR, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 0);
+            k_bfcg_direction<<<T, TR, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 0);
+            h->launches += 2;
+            PLATO_LAUNCH_CHECK(h);
+            precond_applies += degree - 1;
+        }
+        return PLATO_OK;
+    };
+    struct ChunkGraph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+        ~ChunkGraph() { if (exec) cudaGraphExecDestroy(exec); }
+    } chunk;
+    const bool graphs = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
+
     PcgScalars init{};
     PLATO_CUDA(h, cudaMemcpyAsync(h->scal, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
     PLATO_CUDA(h, cudaMemsetAsync(bt.S, 0, sizeof(SegScalars) * bt.nseg, s));
     constexpr int kMaxPasses = 1 + kMaxRestarts;  // first pass + restarts from the true residual
-    int64_t precond_applies = 0;
     cudaEvent_t* ev = h->poll_ev;
     for (int e = 0; e < 2; ++e)
         if (!ev[e]) PLATO_CUDA(h, cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
@@ -1211,7 +1262,7 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         PLATO_CUDA(h, cudaMemsetAsync(&h->scal->done, 0, sizeof(int32_t), s));
         rc = launch_sell_spmv(h, h->sell64, x, h->v_r);
         if (rc) return rc;
-        k_bfcg_start<<<T, kThreads, 0, s>>>(BV, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, tol,
+        k_bfcg_start<<<T, TR, 0, s>>>(BV, b, h->v_r, h->f_dinv, h->f_res, h->f_d0, h->f_y, cc.c0, tol,
                                              pass > 0 ? 1 : 0, 1.0);
         PLATO_LAUNCH_CHECK(h);
         PcgScalars* slots = h->scal_host;
@@ -1221,25 +1272,38 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
         // z = M r, p = z, p.r
         rc = chebyshev_steps();
         if (rc) return rc;
-        k_bfcg_zq<<<T, kThreads, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 1);
-        k_bfcg_direction<<<T, kThreads, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 1);
+        k_bfcg_zq<<<T, TR, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 1);
+        k_bfcg_direction<<<T, TR, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 1);
         h->launches += 2;
         PLATO_LAUNCH_CHECK(h);
         int cur = 0;
         bool have_prev = false;
         for (;;) {
-            for (int k = 0; k < kChunk; ++k) {
-                k_bfcg_apply<<<T, kThreads, 0, s>>>(BV, V, h->sell64, h->v_p, h->v_q);
-                k_bfcg_update<<<T, kThreads, 0, s>>>(BV, x, h->v_r, h->v_p, h->v_q, h->f_dinv, h->f_res, h->f_d0,
-                                                      h->f_y, cc.c0, max_it);
-                h->launches += 2;
-                rc = chebyshev_steps();
+            if (!graphs) {
+                rc = enqueue_chunk();
                 if (rc) return rc;
-                k_bfcg_zq<<<T, kThreads, 0, s>>>(BV, h->f_y, h->v_z, h->v_q, 0);
-                k_bfcg_direction<<<T, kThreads, 0, s>>>(BV, h->v_z, h->v_p, h->v_r, 0);
-                h->launches += 2;
-                PLATO_LAUNCH_CHECK(h);
-                precond_applies += degree - 1;
+            } else {
+                if (!chunk.exec) {  // capture the chunk once per solve, replay it afterwards
+                    const int64_t l0 = h->launches;
+                    cudaGraph_t g = nullptr;
+                    PLATO_CUDA(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                    rc = enqueue_chunk();
+                    const cudaError_t ce = cudaStreamEndCapture(s, &g);
+                    if (rc || ce != cudaSuccess) {
+                        if (g) cudaGraphDestroy(g);
+                        cudaGetLastError();
+                        return rc ? rc : plato_cuda_fail(h, ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+                    }
+                    const cudaError_t ie = cudaGraphInstantiate(&chunk.exec, g, 0);
+                    cudaGraphDestroy(g);
+                    PLATO_CUDA(h, ie);
+                    chunk.launches = h->launches - l0;
+                    h->launches = l0;
+                    precond_applies -= int64_t(kChunk) * (degree - 1);
+                }
+                PLATO_CUDA(h, cudaGraphLaunch(chunk.exec, s));
+                h->launches += chunk.launches;
+                precond_applies += int64_t(kChunk) * (degree - 1);
             }
             PLATO_CUDA(h, cudaMemcpyAsync(&slots[cur], h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
             PLATO_CUDA(h, cudaEventRecord(ev[cur], s));

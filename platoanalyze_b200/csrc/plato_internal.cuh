@@ -118,7 +118,10 @@ struct SegScalars {
 struct BatchState {
     int32_t  nseg = 0;                 // 0 for a single problem
     std::vector<int32_t> node_off, cell_off;
-    int32_t  ncta = 0;
+    int32_t  ncta = 0;                 // tiles of at most tile_rows rows, never across two members
+    int32_t  tile_rows = 256;          // rows per tile = threads per CTA of the batched kernels
+    int32_t  ctas_per_sm = 8;          // persistent grid of the batched kernels
+    int32_t  tuned = 0;                // the pair above comes from plato_batch_autotune
     int32_t* cta_seg = nullptr;        // [ncta] member of each tile
     int32_t* cta_row0 = nullptr;       // [ncta] first row of each tile
     int32_t* cta_row1 = nullptr;       // [ncta] one past its last row

@@ -144,6 +144,12 @@ class EllipticProblem:
         o = self.node_offsets
         return [slice(dofs_per_node * int(o[s]), dofs_per_node * int(o[s + 1])) for s in range(self.count)]
 
+    def batch_autotune(self, z) -> dict:
+        """Times the batched solve's (tile rows, CTAs per SM) candidates and keeps the fastest."""
+        t = capi.BatchTuning()
+        check(lib.plato_batch_autotune(self.h, self._dev(z), C.byref(t)), self.h)
+        return t.as_dict()
+
     def batch_last_stats(self) -> list:
         st = (capi.SolveStats * self.count)()
         check(lib.plato_batch_last_stats(self.h, st), self.h)

@@ -5,6 +5,7 @@ residual and Jacobian entries, a solution converged to its own tolerance, its co
 dC/dz; members converge independently (their own iteration counts and stop tests).
 """
 import numpy as np
+import torch
 import pytest
 
 from helpers import rel_l2
@@ -178,3 +179,31 @@ def test_batch_workload_small_draw():
     u, st = bp.solution(bp.to_dev(np.concatenate(zs)))
     assert st["converged"] == 1
     assert len(bp.batch_last_stats()) == 6
+
+
+def test_autotuned_persistent_batch_with_graphs_matches_members():
+    """The autotuner times every (tile rows, CTAs per SM) pair and keeps the fastest; a batch
+    on a non-default stream (chunks captured as CUDA graphs) with the chosen tiling gives every
+    member the answer of its own handle."""
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        specs, zs = members([6, 10, 4, 8, 12, 6], 21)
+        bp = EllipticProblem.batch(specs, stream=stream)
+        zd = bp.to_dev(np.concatenate(zs))
+        tuning = bp.batch_autotune(zd)
+        assert tuning["tile_rows"] in (128, 256, 512) and tuning["ctas_per_sm"] in (2, 4, 8, 16)
+        assert len(tuning["tried"]) == 12 and all(t["ms"] > 0 for t in tuning["tried"])
+        assert min(t["ms"] for t in tuning["tried"]) == pytest.approx(
+            [t["ms"] for t in tuning["tried"] if t["tile_rows"] == tuning["tile_rows"]
+             and t["ctas_per_sm"] == tuning["ctas_per_sm"]][0])
+        u, st = bp.solution(zd)
+        assert st["converged"] == 1
+        uh = host(u)
+        for s, sl in enumerate(bp.member_slices()):
+            single = EllipticProblem(specs[s], stream=stream)
+            us, sts = single.solution(single.to_dev(zs[s]))
+            assert sts["converged"] == 1
+            assert rel_l2(uh[sl], host(us)) <= 1e-8, s
+            single.close()
+        bp.close()
+    torch.cuda.synchronize()

@@ -714,10 +714,12 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     h->coarse.active = 0;
     if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
+        RC(prepare_coarse(h, z));  // starts on its own stream, overlapping what follows
         RC(prepare_mixed(h, nullptr, z));
-        RC(prepare_coarse(h, z));
         RC(matfree_rhs(h, h->v_b, bc_scale));
-        const int rc = fcg_poly(h, h->v_b, x, st);
+        int rc = fcg_poly(h, h->v_b, x, st);
+        const int crc = coarse_finish(h);
+        if (crc && rc == PLATO_OK) rc = crc;
         if (rc != PLATO_NOT_CONVERGED && rc != PLATO_NONFINITE) return rc;
         return fallback_solve(h, x, st, rc, z);
     }
@@ -749,10 +751,12 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         RC(ritz_guess(h, h->v_b, x));
         rc = pcg_fp64(h, h->v_b, x, st);
     } else {
+        RC(prepare_coarse(h, z));  // starts on its own stream, overlapping the fine-level set-up
         RC(prepare_mixed(h, crs, z));
-        RC(prepare_coarse(h, z));
         RC(ritz_guess(h, h->v_b, x));
         rc = fcg_poly(h, h->v_b, x, st);
+        const int crc = coarse_finish(h);  // the overlapped coarse set-up: timing and its check
+        if (crc && rc == PLATO_OK) rc = crc;
         if (rc == PLATO_NOT_CONVERGED || rc == PLATO_NONFINITE) rc = fallback_solve(h, x, st, rc);
     }
     if (h->timing) {  // the solver has synchronised the stream

@@ -1004,17 +1004,29 @@ void coarse_release(plato_problem* h) {
     for (double** p : {&c.E, &c.X, &c.T, &c.Dt, &c.rc, &c.yc, &c.tc, &c.rpart})
         if (*p) { cudaFree(*p); *p = nullptr; }
     if (c.Xf) { cudaFree(c.Xf); c.Xf = c.Uf = nullptr; }
-    for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
+    if (c.pending && c.ev_ready) cudaEventSynchronize(c.ev_ready);
+    c.pending = 0;
+    for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail, &c.ev_start, &c.ev_ready})
         if (*e) { cudaEventDestroy(*e); *e = nullptr; }
     if (c.side) { cudaStreamDestroy(c.side); c.side = nullptr; }
+    if (c.cs) { cudaStreamDestroy(c.cs); c.cs = nullptr; }
+    if (c.flag_host) { cudaFreeHost(c.flag_host); c.flag_host = nullptr; }
     c.ready = 0;
 }
 
-// Per-solve setup: Galerkin operator of control z, Cholesky, explicit inverse.
-// E_copy (device, may be NULL) receives E before it is factored.
-int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
+// Per-solve setup: Galerkin operator of control z, Cholesky, explicit inverse, on the coarse
+// stream after the work already queued on the handle's stream.  E_copy (device, may be NULL)
+// receives E before it is factored.  deferred: return at once (coarse_wait before the first
+// use, coarse_finish after the solve); otherwise wait here.
+int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy, int deferred) {
     CoarseSpace& c = h->coarse;
-    cudaStream_t s = h->stream;
+    if (!c.cs) PLATO_CUDA(h, cudaStreamCreateWithFlags(&c.cs, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c.ev_start, &c.ev_ready})
+        if (!*e) PLATO_CUDA(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    if (!c.flag_host) PLATO_CUDA(h, cudaMallocHost(reinterpret_cast<void**>(&c.flag_host), sizeof(int32_t)));
+    PLATO_CUDA(h, cudaEventRecord(c.ev_start, h->stream));
+    PLATO_CUDA(h, cudaStreamWaitEvent(c.cs, c.ev_start, 0));
+    cudaStream_t s = c.cs;
     const int n = c.ndof;
     const size_t nn = size_t(n) * n;
     if (h->timing) {
@@ -1085,9 +1097,25 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
     k_coarse_pack<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, c.ldf, X, c.Xf, c.Uf);
     PLATO_LAUNCH_CHECK(h);
     if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[2], s));
-    int32_t bad = 0;
-    PLATO_CUDA(h, cudaMemcpyAsync(&bad, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    PLATO_CUDA(h, cudaStreamSynchronize(s));
+    PLATO_CUDA(h, cudaMemcpyAsync(c.flag_host, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    PLATO_CUDA(h, cudaEventRecord(c.ev_ready, s));
+    c.pending = 1;
+    if (deferred) return PLATO_OK;
+    PLATO_RC(coarse_wait(h));
+    return coarse_finish(h);
+}
+
+int coarse_wait(plato_problem* h) {
+    CoarseSpace& c = h->coarse;
+    if (c.pending) PLATO_CUDA(h, cudaStreamWaitEvent(h->stream, c.ev_ready, 0));
+    return PLATO_OK;
+}
+
+int coarse_finish(plato_problem* h) {
+    CoarseSpace& c = h->coarse;
+    if (!c.pending) return PLATO_OK;
+    PLATO_CUDA(h, cudaEventSynchronize(c.ev_ready));
+    c.pending = 0;
     if (h->timing) {
         float ms[2] = {0.f, 0.f};
         PLATO_CUDA(h, cudaEventElapsedTime(&ms[0], h->coarse_ev[0], h->coarse_ev[1]));
@@ -1096,7 +1124,7 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy) {
         h->coarse_inv_ms += ms[1];
         h->coarse_timed += 1;
     }
-    if (bad) return plato_fail(h, PLATO_NONFINITE, "coarse operator is not positive definite");
+    if (*c.flag_host) return plato_fail(h, PLATO_NONFINITE, "coarse operator is not positive definite");
     return PLATO_OK;
 }
 

@@ -620,7 +620,7 @@ int prepare_coarse(plato_problem* h, const double* z) {
     if (h->opts.coarse_cells[0] <= 0 || !z) return PLATO_OK;
     int rc = coarse_setup_mesh(h);
     if (rc) return rc;
-    rc = coarse_setup_operator(h, z);
+    rc = coarse_setup_operator(h, z, nullptr, 1);  // overlapped with the fine-level set-up
     if (rc) return rc;
     h->coarse.active = 1;
     return PLATO_OK;
@@ -654,6 +654,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     if (rc) return rc;
     const double safety = kind == INNER_SELL16 ? 1.15 : 1.10;
     const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree);
+    // the coarse set-up ran on its own stream meanwhile: the iterations wait for it here
+    rc = coarse_wait(h);
+    if (rc) return rc;
 
     auto outer_apply = [&](const double* in, double* out) -> int {
         if (mf) {

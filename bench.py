@@ -550,6 +550,10 @@ def run_mixed(args):
         "fp32 element kernels: matrix-free FP32 element-by-element Chebyshev(8), FP64 matrix-free outer": SolverOptions(
             tolerance=tol, max_iterations=200000, operator_kind=capi.OPERATOR_MATRIX_FREE,
             precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=8),
+        "fp32 element assembly: FP32 element kernels assemble the preconditioner's SELL matrix, "
+        "Chebyshev(8), FP64 matrix-free outer": SolverOptions(
+            tolerance=tol, max_iterations=200000, operator_kind=capi.OPERATOR_MATRIX_FREE,
+            precision=capi.PRECISION_MIXED_FP32_ASSEMBLED, chebyshev_degree=8),
         "fp16-scaled two-level: Chebyshev(8) + Galerkin coarse space 10x5x5": SolverOptions(
             tolerance=tol, max_iterations=200000, precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8,
             coarse_cells=(10, 5, 5)),

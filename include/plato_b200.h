@@ -48,10 +48,15 @@ typedef enum plato_precision {
     PLATO_PRECISION_FP64       = 0, /* plain FP64 Jacobi-PCG                                */
     PLATO_PRECISION_MIXED_FP32 = 1, /* FP32 inner PCG inside FP64 iterative refinement      */
     PLATO_PRECISION_MIXED_BF16 = 2, /* as MIXED_FP32 with the block CRS stored in BF16      */
-    PLATO_PRECISION_MIXED_FP16 = 3  /* as MIXED_FP32 with the Jacobi-scaled matrix
+    PLATO_PRECISION_MIXED_FP16 = 3, /* as MIXED_FP32 with the Jacobi-scaled matrix
                                        D^-1/2 A D^-1/2 stored in FP16 (unit diagonal, entries
                                        in [-1, 1]); the Chebyshev sweep runs in scaled
                                        variables (assembled operator only)                 */
+    PLATO_PRECISION_MIXED_FP32_ASSEMBLED = 4 /* matrix-free operator only: the FP64 outer
+                                       operator is the element-by-element apply and the
+                                       preconditioner's matrix is assembled by FP32 element
+                                       kernels (gradients, weights and sums in FP32) straight
+                                       into an FP32 SELL copy; no FP64 matrix exists        */
 } plato_precision;
 
 typedef struct plato_problem plato_problem; /* opaque handle */

@@ -18,6 +18,7 @@ STATUS_NAMES = ["OK", "BAD_INPUT", "NOT_CONVERGED", "NONFINITE", "DEVICE_TIMEOUT
 
 OPERATOR_ASSEMBLED, OPERATOR_MATRIX_FREE = 0, 1
 PRECISION_FP64, PRECISION_MIXED_FP32, PRECISION_MIXED_BF16, PRECISION_MIXED_FP16 = 0, 1, 2, 3
+PRECISION_MIXED_FP32_ASSEMBLED = 4  # FP32 element assembly of the preconditioner matrix (matrix-free outer)
 
 i32p = C.POINTER(C.c_int32)
 f64p = C.POINTER(C.c_double)

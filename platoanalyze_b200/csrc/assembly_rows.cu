@@ -99,21 +99,29 @@ __global__ void k_asm_plan(GraphView g, const int4* __restrict__ conn, uint16_t*
     }
 }
 
-// kSell = false: block CRS values (unconstrained) into crs[9 * nblocks].
-// kSell = true:  constrained SELL copy + inverse diagonal (+ optional copies) into `so`.
-template <bool kSell>
-__global__ void __launch_bounds__(kAsmWarps * 32, 1)
+// T = double, kSell = false: block CRS values (unconstrained) into crs[9 * nblocks].
+// T = double, kSell = true:  constrained SELL copy + inverse diagonal (+ optional FP32 / BF16
+//                            copies rounded from the FP64 values) into `so`.
+// T = float,  kSell = true:  FP32 element assembly -- gradients, weights and sums in FP32 -- of
+//                            the constrained SELL copy (so.v32) and its inverse diagonal
+//                            (so.dinv32), the preconditioner matrix of the mixed-precision solve
+//                            whose FP64 outer operator is the matrix-free element apply.
+// Shared memory is the same 207,360 bytes per CTA: 6 warps of FP64 or 12 warps of FP32 sums.
+template <bool kSell, typename T>
+__global__ void __launch_bounds__(kAsmWarps * 32 * (sizeof(T) == 8 ? 1 : 2), 1)
 k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
                 const uint16_t* __restrict__ plan, double* __restrict__ crs, SellOut so) {
-    extern __shared__ double smem[];
+    constexpr int kWarps = kAsmWarps * (sizeof(T) == 8 ? 1 : 2);
+    extern __shared__ double smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* acc = smem + warp * kAccPerWarp;
-    const double lam = mat.c01, mu = mat.c33;
+    T* acc = smem + warp * kAccPerWarp;
+    const T lam = T(mat.c01), mu = T(mat.c33);
     const int32_t nslices = (g.num_nodes + 31) >> 5;
-    for (int32_t s = blockIdx.x * kAsmWarps + warp; s < nslices; s += gridDim.x * kAsmWarps) {
+    for (int32_t s = blockIdx.x * kWarps + warp; s < nslices; s += gridDim.x * kWarps) {
         const int32_t r = 32 * s + lane;
         int32_t rs = 0, nb = 0, ks = 0, kc = 0, dslot = -1;
-        double xr[3] = {0.0, 0.0, 0.0}, zr = 0.0;
+        T xr[3] = {T(0), T(0), T(0)}, zr = T(0);
         if (r < g.num_nodes) {
             rs = g.row_map[r];
             nb = g.row_map[r + 1] - rs;
@@ -121,10 +129,10 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 ks = g.n2c_ptr[r];
                 kc = g.n2c_ptr[r + 1] - ks;
                 dslot = g.diag[r] - rs;
-                xr[0] = __ldg(m.coords + 3 * (int64_t)r);
-                xr[1] = __ldg(m.coords + 3 * (int64_t)r + 1);
-                xr[2] = __ldg(m.coords + 3 * (int64_t)r + 2);
-                zr = mat.cell_control ? 0.0 : __ldg(z + r);
+                xr[0] = T(__ldg(m.coords + 3 * (int64_t)r));
+                xr[1] = T(__ldg(m.coords + 3 * (int64_t)r + 1));
+                xr[2] = T(__ldg(m.coords + 3 * (int64_t)r + 2));
+                zr = mat.cell_control ? T(0) : T(__ldg(z + r));
             } else {
                 nb = 0;  // wide row: assembled by the warp-per-row kernel
             }
@@ -132,10 +140,10 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
         const int nbw = warp_max(nb);
         for (int k = 0; k < nbw; ++k)
 #pragma unroll
-            for (int q = 0; q < 9; ++q) acc[acc_index(k, q, lane)] = 0.0;
+            for (int q = 0; q < 9; ++q) acc[acc_index(k, q, lane)] = T(0);
         __syncwarp();
 
-        double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0, d4 = 0.0, d5 = 0.0;  // xx yy zz yz xz xy
+        T d0 = T(0), d1 = T(0), d2 = T(0), d3 = T(0), d4 = T(0), d5 = T(0);  // xx yy zz yz xz xy
         const int kmax = warp_max(kc);
         // one cell ahead: incidence entry, plan and connectivity of the next cell
         int32_t p_next = 0;
@@ -165,15 +173,16 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 const double* c0 = m.coords + 3 * (int64_t)i0;
                 const double* c1 = m.coords + 3 * (int64_t)i1;
                 const double* c2 = m.coords + 3 * (int64_t)i2;
-                const double j11 = __ldg(c0) - xr[0], j21 = __ldg(c0 + 1) - xr[1], j31 = __ldg(c0 + 2) - xr[2];
-                const double j12 = __ldg(c1) - xr[0], j22 = __ldg(c1 + 1) - xr[1], j32 = __ldg(c1 + 2) - xr[2];
-                const double j13 = __ldg(c2) - xr[0], j23 = __ldg(c2 + 1) - xr[1], j33 = __ldg(c2 + 2) - xr[2];
-                const double rho = mat.cell_control ? __ldg(z + (p >> 2)) : (__ldg(z + i0) + __ldg(z + i1) + __ldg(z + i2) + zr) * 0.25;
+                const T j11 = T(__ldg(c0)) - xr[0], j21 = T(__ldg(c0 + 1)) - xr[1], j31 = T(__ldg(c0 + 2)) - xr[2];
+                const T j12 = T(__ldg(c1)) - xr[0], j22 = T(__ldg(c1 + 1)) - xr[1], j32 = T(__ldg(c1 + 2)) - xr[2];
+                const T j13 = T(__ldg(c2)) - xr[0], j23 = T(__ldg(c2 + 1)) - xr[1], j33 = T(__ldg(c2 + 2)) - xr[2];
+                const T rho = mat.cell_control ? T(__ldg(z + (p >> 2)))
+                                               : (T(__ldg(z + i0)) + T(__ldg(z + i1)) + T(__ldg(z + i2)) + zr) * T(0.25);
                 // ComputeGradientWorkset<3> (src/ImplicitFunctors.hpp:169-221) with x_3 = the row node
-                const double c11 = j22 * j33 - j23 * j32, c12 = j13 * j32 - j12 * j33, c13 = j12 * j23 - j13 * j22;
-                const double detj = j11 * c11 + j21 * c12 + j31 * c13;
-                const double inv = 1.0 / detj;
-                double gb[3][3];
+                const T c11 = j22 * j33 - j23 * j32, c12 = j13 * j32 - j12 * j33, c13 = j12 * j23 - j13 * j22;
+                const T detj = j11 * c11 + j21 * c12 + j31 * c13;
+                const T inv = T(1) / detj;
+                T gb[3][3];
                 gb[0][0] = c11 * inv;
                 gb[0][1] = c12 * inv;
                 gb[0][2] = c13 * inv;
@@ -183,11 +192,11 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 gb[2][0] = (j21 * j32 - j22 * j31) * inv;
                 gb[2][1] = (j12 * j31 - j11 * j32) * inv;
                 gb[2][2] = (j11 * j22 - j12 * j21) * inv;
-                const double w = fabs(detj) * (1.0 / 6.0) * simp(mat, rho);
-                const double ga0 = -(gb[0][0] + gb[1][0] + gb[2][0]);
-                const double ga1 = -(gb[0][1] + gb[1][1] + gb[2][1]);
-                const double ga2 = -(gb[0][2] + gb[1][2] + gb[2][2]);
-                const double a0 = w * ga0, a1 = w * ga1, a2 = w * ga2;
+                const T w = fabs(detj) * (T(1) / T(6)) * simp(mat, rho);
+                const T ga0 = -(gb[0][0] + gb[1][0] + gb[2][0]);
+                const T ga1 = -(gb[0][1] + gb[1][1] + gb[2][1]);
+                const T ga2 = -(gb[0][2] + gb[1][2] + gb[2][2]);
+                const T a0 = w * ga0, a1 = w * ga1, a2 = w * ga2;
                 d0 = fma(a0, ga0, d0);
                 d1 = fma(a1, ga1, d1);
                 d2 = fma(a2, ga2, d2);
@@ -197,11 +206,11 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 #pragma unroll
                 for (int t = 0; t < 3; ++t) {
                     const int k = (pl >> (4 * t)) & 15;
-                    double* row = acc + 9 * 32 * k;
+                    T* row = acc + 9 * 32 * k;
 #pragma unroll
                     for (int q = 0; q < 9; ++q) {
-                        const double ai = q < 3 ? a0 : (q < 6 ? a1 : a2);
-                        double& v = row[q * 32 + (lane ^ q)];
+                        const T ai = q < 3 ? a0 : (q < 6 ? a1 : a2);
+                        T& v = row[q * 32 + (lane ^ q)];
                         v = fma(ai, gb[t][q % 3], v);
                     }
                 }
@@ -213,7 +222,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
         const int64_t pbase = kSell ? __ldg(so.ptr + s) : 0;  // first SELL slot of the slice
         const int64_t sbase = 9 * pbase;
         for (int k = 0; k < nbw; ++k) {
-            double S[9];
+            T S[9];
             if (k == dslot) {
                 S[0] = d0; S[4] = d1; S[8] = d2;
                 S[5] = S[7] = d3;
@@ -223,13 +232,13 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 #pragma unroll
                 for (int q = 0; q < 9; ++q) S[q] = acc[acc_index(k, q, lane)];
             }
-            const double tr = mu * (S[0] + S[4] + S[8]);
-            double K[9];
+            const T tr = mu * (S[0] + S[4] + S[8]);
+            T K[9];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int jj = 0; jj < 3; ++jj)
-                    K[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : 0.0);
+                    K[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : T(0));
             if (!kSell) {
 #pragma unroll
                 for (int q = 0; q < 9; ++q) acc[acc_index(k, q, lane)] = K[q];
@@ -239,19 +248,19 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 #pragma unroll
                 for (int q = 0; q < 9; ++q) {
                     const int i = q / 3, jj = q % 3;
-                    double v = real ? K[q] : 0.0;
+                    T v = real ? K[q] : T(0);
                     if (real) {
                         const bool mr = __ldg(so.bc_mask + 3 * (int64_t)r + i) != 0;
                         const bool mc = __ldg(so.bc_mask + 3 * (int64_t)c + jj) != 0;
-                        if (mr || mc) v = (c == r && i == jj) ? 1.0 : 0.0;
+                        if (mr || mc) v = (c == r && i == jj) ? T(1) : T(0);
                     }
                     const int64_t o = sbase + 32 * (9 * k + q) + lane;
-                    so.v64[o] = v;
+                    if (sizeof(T) == 8) so.v64[o] = double(v);
                     if (so.v32) so.v32[o] = float(v);
                     if (so.v16) so.v16[o] = __float2bfloat16_rn(float(v));
                     if (real && k == dslot && i == jj) {
-                        so.dinv[3 * (int64_t)r + i] = 1.0 / v;
-                        if (so.dinv32) so.dinv32[3 * (int64_t)r + i] = float(1.0 / v);
+                        if (sizeof(T) == 8) so.dinv[3 * (int64_t)r + i] = 1.0 / double(v);
+                        if (so.dinv32) so.dinv32[3 * (int64_t)r + i] = float(1.0 / double(v));
                     }
                 }
             }
@@ -265,7 +274,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 double* dst = crs + 9 * (int64_t)rs_l;
                 for (int e = lane; e < nv; e += 32) {
                     const int q = e % 9;
-                    dst[e] = acc[e * 32 + (l ^ q)];
+                    dst[e] = double(acc[e * 32 + (l ^ q)]);
                 }
             }
         }
@@ -295,12 +304,12 @@ int assembly_plan(plato_problem* h) {
     return PLATO_OK;
 }
 
-static int asm_grid(plato_problem* h, const void* kernel, int* grid) {
+static int asm_grid(plato_problem* h, const void* kernel, int* grid, int warps = kAsmWarps) {
     PLATO_RC(ensure_smem_attribute(h, kernel, int(kAsmSmem)));
     int sms = 0;
     PLATO_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     const int64_t nslices = (int64_t(h->N) + 31) / 32;
-    *grid = int(std::min<int64_t>(sms, (nslices + kAsmWarps - 1) / kAsmWarps));
+    *grid = int(std::min<int64_t>(sms, (nslices + warps - 1) / warps));
     if (*grid < 1) *grid = 1;
     return PLATO_OK;
 }
@@ -310,8 +319,8 @@ static int asm_grid(plato_problem* h, const void* kernel, int* grid) {
 int launch_assemble_jacobian(plato_problem* h, const double* z, double* entries) {
     PLATO_RC(assembly_plan(h));
     int grid = 0;
-    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<false>), &grid));
-    k_assemble_rows<false><<<grid, kAsmWarps * 32, kAsmSmem, h->stream>>>(mesh_view(h), graph_view(h), h->material,
+    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<false, double>), &grid));
+    k_assemble_rows<false, double><<<grid, kAsmWarps * 32, kAsmSmem, h->stream>>>(mesh_view(h), graph_view(h), h->material,
                                                                            z, h->asm_plan, entries, SellOut{});
     PLATO_LAUNCH_CHECK(h);
     if (h->asm_nwide > 0) PLATO_RC(launch_assemble_jacobian_list(h, z, entries, h->asm_wide, h->asm_nwide));
@@ -333,14 +342,29 @@ int launch_assemble_sell(plato_problem* h, const double* z, double* v64, float* 
     PLATO_RC(assembly_plan(h));
     if (h->asm_nwide > 0) return plato_fail(h, PLATO_NOT_SUPPORTED, "direct SELL assembly needs every row narrow");
     int grid = 0;
-    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<true>), &grid));
+    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<true, double>), &grid));
     SellOut so{h->sell.ptr, h->sell.cols, h->bc_mask, v64, v32, static_cast<__nv_bfloat16*>(v16), dinv, dinv32};
     // the solver's assembly timing (instrumentation) brackets this one kernel
     if (h->timing && h->asm_ev[0]) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[0], h->stream));
-    k_assemble_rows<true><<<grid, kAsmWarps * 32, kAsmSmem, h->stream>>>(mesh_view(h), graph_view(h), h->material,
+    k_assemble_rows<true, double><<<grid, kAsmWarps * 32, kAsmSmem, h->stream>>>(mesh_view(h), graph_view(h), h->material,
                                                                           z, h->asm_plan, nullptr, so);
     PLATO_LAUNCH_CHECK(h);
     if (h->timing && h->asm_ev[1]) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[1], h->stream));
+    return PLATO_OK;
+}
+
+// FP32 element assembly of the constrained SELL copy (values and inverse diagonal in FP32),
+// the preconditioner matrix when the FP64 outer operator is the matrix-free element apply.
+int launch_assemble_sell32(plato_problem* h, const double* z, float* v32, float* dinv32) {
+    PLATO_RC(assembly_plan(h));
+    if (h->asm_nwide > 0) return plato_fail(h, PLATO_NOT_SUPPORTED, "FP32 element assembly needs every row narrow");
+    if (h->bc_nonzero) return plato_fail(h, PLATO_NOT_SUPPORTED, "FP32 element assembly needs homogeneous essential BCs");
+    int grid = 0;
+    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<true, float>), &grid, 2 * kAsmWarps));
+    SellOut so{h->sell.ptr, h->sell.cols, h->bc_mask, nullptr, v32, nullptr, nullptr, dinv32};
+    k_assemble_rows<true, float><<<grid, 2 * kAsmWarps * 32, kAsmSmem, h->stream>>>(
+        mesh_view(h), graph_view(h), h->material, z, h->asm_plan, nullptr, so);
+    PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }
 

@@ -106,8 +106,10 @@ int check_opts(plato_problem* h, const plato_solver_opts& o) {
     if (o.max_iterations < 1) return plato_fail(h, PLATO_BAD_INPUT, "solver max_iterations must be >= 1");
     if (o.operator_kind != PLATO_OPERATOR_ASSEMBLED && o.operator_kind != PLATO_OPERATOR_MATRIX_FREE)
         return plato_fail(h, PLATO_BAD_INPUT, "unknown operator_kind");
-    if (o.precision < PLATO_PRECISION_FP64 || o.precision > PLATO_PRECISION_MIXED_FP16)
+    if (o.precision < PLATO_PRECISION_FP64 || o.precision > PLATO_PRECISION_MIXED_FP32_ASSEMBLED)
         return plato_fail(h, PLATO_BAD_INPUT, "unknown precision");
+    if (o.precision == PLATO_PRECISION_MIXED_FP32_ASSEMBLED && o.operator_kind != PLATO_OPERATOR_MATRIX_FREE)
+        return plato_fail(h, PLATO_BAD_INPUT, "FP32 element assembly pairs with the matrix-free FP64 operator");
     return PLATO_OK;
 }
 

@@ -31,6 +31,7 @@ namespace plato {
 
 int launch_assemble_sell(plato_problem* h, const double* z, double* v64, float* v32, void* v16, double* dinv,
                          float* dinv32);
+int launch_assemble_sell32(plato_problem* h, const double* z, float* v32, float* dinv32);
 
 int launch_axpby(plato_problem* h, int64_t n, double a, const double* x, double b, double* y);
 int launch_dot(plato_problem* h, const double* a, const double* b, int64_t n, double* host_result);
@@ -477,8 +478,10 @@ __global__ void k_power_init(int64_t n, float* __restrict__ v) {
 
 int inner_kind(const plato_problem* h) {
     const plato_solver_opts& o = h->opts;
-    if (o.operator_kind == PLATO_OPERATOR_MATRIX_FREE)
+    if (o.operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
+        if (o.precision == PLATO_PRECISION_MIXED_FP32_ASSEMBLED) return INNER_SELL32;  // FP32 element assembly
         return o.precision == PLATO_PRECISION_FP64 ? INNER_EBE64 : INNER_EBE32;
+    }
     if (o.precision == PLATO_PRECISION_MIXED_BF16) return INNER_SELL16;
     if (o.precision == PLATO_PRECISION_MIXED_FP16) return INNER_SELL16S;
     if (o.precision == PLATO_PRECISION_MIXED_FP32) return INNER_SELL32;
@@ -590,7 +593,13 @@ int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
         if (!*v) PLATO_CUDA(h, cudaMalloc(v, sizeof(float) * n));
     if (!h->v_q) PLATO_CUDA(h, cudaMalloc(&h->v_q, sizeof(double) * n));
     const int kind = inner_kind(h);
-    if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) return matfree_setup(h, z);
+    if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
+        int rc = matfree_setup(h, z);
+        if (rc || kind != INNER_SELL32) return rc;
+        // the preconditioner's matrix by FP32 element assembly (no FP64 matrix)
+        if (!h->sell32) PLATO_CUDA(h, cudaMalloc(&h->sell32, sizeof(float) * 9 * size_t(h->sell.total_slots)));
+        return launch_assemble_sell32(h, z, h->sell32, h->f_dinv);
+    }
     const size_t slots = 9 * size_t(h->sell.total_slots);
     if (!h->sell64) PLATO_CUDA(h, cudaMalloc(&h->sell64, sizeof(double) * slots));
     float* o32 = nullptr;
@@ -634,7 +643,8 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     const int32_t max_it = h->opts.max_iterations;
     const int degree = h->opts.chebyshev_degree < 1 ? 1 : (h->opts.chebyshev_degree > 64 ? 64 : h->opts.chebyshev_degree);
     const int kind = inner_kind(h);
-    const bool mf = h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE;
+    const bool mf = h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE;       // FP64 outer operator
+    const bool mf_inner = kind == INNER_EBE32 || kind == INNER_EBE64;          // preconditioner operator
     const int VB = grid_for(n, kThreads, 148 * 16);
     const int SB = spmv_blocks(h);
     const SellView V = sell_view(h);
@@ -672,7 +682,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     const float* res_scale = scaled ? h->f_isq : nullptr;
     // res -= A_inner xin (FP32)
     auto inner_apply_sub = [&](const float* xin) -> int {
-        if (mf) {
+        if (mf_inner) {
             int r2 = launch_ebe_apply32(h, xin, h->f_w, h->scal);
             if (r2) return r2;
             k_res_sub_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, xin, h->f_w, h->f_res, h->scal);
@@ -703,7 +713,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 timed_iters.push_back(inner_record);
                 PLATO_CUDA(h, cudaEventRecord(t0, s));
             }
-            if (mf) {
+            if (mf_inner) {
                 int r2 = launch_ebe_apply32(h, dcur, h->f_w, h->scal);
                 if (r2) return r2;
                 k_cheb_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, h->f_w, h->f_dinv, h->f_res, dcur, dnext, h->f_y,

@@ -31,6 +31,11 @@ CONFIGS = {
     "fp16s_cheb8": SolverOptions(precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8),
     "fp16s_cheb8_coarse": SolverOptions(precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8,
                                         coarse_cells=(10, 5, 5)),
+    "mf_fp32asm_cheb8": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE,
+                                      precision=capi.PRECISION_MIXED_FP32_ASSEMBLED, chebyshev_degree=8),
+    "mf_fp32asm_cheb4_coarse": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE,
+                                             precision=capi.PRECISION_MIXED_FP32_ASSEMBLED, chebyshev_degree=4,
+                                             coarse_cells=(10, 5, 5)),
     "mf_fp32_cheb4_coarse": SolverOptions(operator_kind=capi.OPERATOR_MATRIX_FREE,
                                           precision=capi.PRECISION_MIXED_FP32, chebyshev_degree=4,
                                           coarse_cells=(4, 2, 2)),
@@ -185,3 +190,21 @@ def test_fallback_after_a_subspace_guess(setup):
         assert rel_l2(host(u), uo) <= 1e-8
     finally:
         prob.set_solver(SolverOptions(tolerance=1e-10))
+
+
+def test_fp32_element_assembly_matches_the_fp64_matrix(setup):
+    """The FP32 element assembly of the preconditioner matrix: the solve with it reaches the
+    FP64 answer (the outer operator is the FP64 matrix-free apply), and its inverse diagonal
+    (the preconditioner's Jacobi scaling) agrees with the FP64 matrix's to FP32 accuracy."""
+    spec, z, prob, orc, uo, go = setup
+    zd = prob.to_dev(z)
+    prob.set_solver(SolverOptions(tolerance=1e-10, operator_kind=capi.OPERATOR_MATRIX_FREE,
+                                  precision=capi.PRECISION_MIXED_FP32_ASSEMBLED, chebyshev_degree=8))
+    try:
+        u, st = prob.solution(zd)
+        assert st["converged"] == 1 and st["fallback"] == 0 and rel_l2(host(u), uo) <= 1e-8
+    finally:
+        prob.set_solver(SolverOptions(tolerance=1e-10))
+    with pytest.raises(capi.PlatoError):  # only with the matrix-free FP64 operator
+        prob.set_solver(SolverOptions(precision=capi.PRECISION_MIXED_FP32_ASSEMBLED, chebyshev_degree=8))
+    prob.set_solver(SolverOptions(tolerance=1e-10))

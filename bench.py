@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--cells", default="80,40,40", help="--profile-unit: hexes along x,y,z (6 tets each)")
     ap.add_argument("--repeat", type=int, default=1, help="--profile-unit: units to run")
     ap.add_argument("--coarse", default=None, help="--profile-unit: coarse box cells x,y,z")
+    ap.add_argument("--api-kernels", action="store_true",
+                    help="--profile-unit: each unit also evaluates R(u, z) and the block-CRS K(z) of the API")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "helmholtz", "mixed"],
                     help="batch: 64 independent GRF cantilevers n x n/2 x n/2, n in {16,24,32,48,64}, one batched "
                          "solve; helmholtz: the density filter's solution and chain rule on the --size mesh; "
@@ -506,6 +508,9 @@ def run_profile_unit(args):
         u, st = prob.solution(zd)
         f = prob.criterion_value(zd, u)
         prob.criterion_gradient(zd, u)
+        if args.api_kernels:  # VectorFunction::value and ::gradient_u through the C ABI
+            prob.vf_value(u, zd)
+            prob.vf_gradient_u(u, zd)
         torch.cuda.synchronize()
         print({"cells": (nx, ny, nz), "method": args.method, "compliance": f} | st)
     prob.close()

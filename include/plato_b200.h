@@ -181,10 +181,11 @@ int plato_reset_instrumentation(plato_problem* h);
  * preconditioner (one step = one preconditioner-operator apply fused with its update),
  * kind 2 = the Jacobian assembly of each assembled solve, kind 3 = the Galerkin product of
  * the two-level coarse operator, kind 4 = its dense factorization and inverse (kinds 3 and 4
- * count coarse operator set-ups); kinds 5-7 time every call with timing on: 5 = the residual
+ * count coarse operator set-ups); kinds 5-8 time every call with timing on: 5 = the residual
  * of plato_vf_value (load copy + element force kernel), 6 = the energy sum of plato_sf_value,
  * 7 = the self-adjoint dC/dz of plato_problem_criterion_gradient (per-cell pass + nodal
- * sums).  Reading kinds 5-7 waits for the last timed launch of that kind. */
+ * sums), 8 = plato_problem_criterion_value_and_gradient's one pass (+ nodal sums).  Reading
+ * kinds 5-8 waits for the last timed launch of that kind. */
 int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
 
 /* ---- block pattern ---------------------------------------------------------------------
@@ -257,6 +258,11 @@ int plato_problem_criterion_value(plato_problem* h, const double* z, const doubl
 /* criterionGradient(z, u), :395-450 (self-adjoint shortcut or adjoint solve) */
 int plato_problem_criterion_gradient(plato_problem* h, const double* z, const double* u,
                                      double* dfdz, plato_solve_stats* stats);
+/* criterionValue and criterionGradient together (what an MPMD ComputeCriterion operation
+ * computes, src/Analyze_App.cpp:727-1014): with the self-adjoint shortcut one pass over the
+ * cells gives the compliance (*value, host) and dC/dz [device]; otherwise the two calls above. */
+int plato_problem_criterion_value_and_gradient(plato_problem* h, const double* z, const double* u,
+                                               double* value /*[host]*/, double* dfdz, plato_solve_stats* stats);
 /* One optimisation step on HOST buffers: z -> u, compliance value, dC/dz.  Host<->device
  * copies are part of the call (what an MPMD ComputeSolution + ComputeCriterion +
  * ComputeCriterionGradient sequence does, src/Analyze_App.cpp:727-1201). */

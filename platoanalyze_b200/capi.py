@@ -128,6 +128,7 @@ def _load() -> C.CDLL:
         "plato_problem_solution": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_problem_criterion_value": ([vp, vp, vp, f64p], C.c_int),
         "plato_problem_criterion_gradient": ([vp, vp, vp, vp, C.POINTER(SolveStats)], C.c_int),
+        "plato_problem_criterion_value_and_gradient": ([vp, vp, vp, f64p, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_problem_solve_and_gradient_host": ([vp, vp, vp, vp, f64p, vp, C.POINTER(SolveStats)], C.c_int),
         "plato_sf_value_noalloc": ([C.c_int32, C.c_int32, vp, vp, vp, vp, C.POINTER(Material), C.POINTER(Penalty),
                                     vp, vp], C.c_int),

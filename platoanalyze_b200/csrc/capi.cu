@@ -17,6 +17,7 @@ int launch_traction(plato_problem* h, int32_t nfaces, const int32_t* fcell, cons
 int launch_nodal_control_derivative(plato_problem* h, int mode, const double* u, const double* z,
                                     const double* lam, double* cellbuf, double* out, int accumulate);
 int launch_energy(plato_problem* h, const double* u, const double* z, double* result);
+int launch_energy_and_gradient(plato_problem* h, const double* u, const double* z, double* result, double* dfdz);
 int launch_assemble_jacobian(plato_problem* h, const double* z, double* entries);
 int launch_assemble_gradient_z(plato_problem* h, const double* u, const double* z, double* entries);
 int launch_dirichlet(plato_problem* h, double* A, double* rhs, double scale);
@@ -381,7 +382,7 @@ static int elem_time_end(plato_problem* h, int k) {
 int plato_get_kernel_timing(const plato_problem* hc, int32_t kind, double* ms_total, int64_t* count) {
     if (!hc || !ms_total || !count) return PLATO_BAD_INPUT;
     plato_problem* h = const_cast<plato_problem*>(hc);  // reading the totals completes pending pairs
-    if (kind >= 5 && kind <= 7) {
+    if (kind >= 5 && kind <= 8) {
         RC(elem_time_flush(h, kind - 5));
         *ms_total = h->elem_timing[kind - 5].ms;
         *count = h->elem_timing[kind - 5].count;
@@ -605,6 +606,23 @@ int plato_problem_criterion_value(plato_problem* h, const double* z, const doubl
     return plato_sf_value(h, u, z, value);
 }
 
+int plato_problem_criterion_value_and_gradient(plato_problem* h, const double* z, const double* u, double* value,
+                                               double* dfdz, plato_solve_stats* stats) {
+    NEED(h, z && u && value && dfdz, "null pointer");
+    if (!h->opts.self_adjoint || h->batch.nseg > 0) {  // the adjoint solve, or per-member values: two calls
+        RC(plato_problem_criterion_value(h, z, u, value));
+        return plato_problem_criterion_gradient(h, z, u, dfdz, stats);
+    }
+    if (stats) { stats->iterations = 0; stats->refinements = 0; stats->relative_residual = 0.0;
+                 stats->converged = 1; stats->status = 0; stats->fallback = 0; }
+    RC(elem_time_begin(h, 3));
+    RC(launch_energy_and_gradient(h, u, z, h->red_out, dfdz));
+    RC(elem_time_end(h, 3));
+    PLATO_CUDA(h, cudaMemcpyAsync(value, h->red_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PLATO_OK;
+}
+
 int plato_problem_criterion_gradient(plato_problem* h, const double* z, const double* u, double* dfdz,
                                      plato_solve_stats* stats) {
     NEED(h, z && u && dfdz, "null device pointer");
@@ -648,8 +666,13 @@ int plato_problem_solve_and_gradient_host(plato_problem* h, const double* z_host
     int rc = solve_state(h, h->d_z_in, u0, h->d_u_out, st);
     if (rc && rc != PLATO_NOT_CONVERGED) return rc;
     const int solve_rc = rc;
-    if (value_host) RC(plato_sf_value(h, h->d_u_out, h->d_z_in, value_host));
-    if (dfdz_host) {
+    if (value_host && dfdz_host) {  // ComputeCriterion: value and gradient together
+        plato_solve_stats adj{};
+        RC(plato_problem_criterion_value_and_gradient(h, h->d_z_in, h->d_u_out, value_host, h->d_g_out, &adj));
+        PLATO_CUDA(h, cudaMemcpyAsync(dfdz_host, h->d_g_out, sizeof(double) * nz, cudaMemcpyDeviceToHost, s));
+    } else if (value_host) {
+        RC(plato_sf_value(h, h->d_u_out, h->d_z_in, value_host));
+    } else if (dfdz_host) {
         plato_solve_stats adj{};
         RC(plato_problem_criterion_gradient(h, h->d_z_in, h->d_u_out, h->d_g_out, &adj));
         PLATO_CUDA(h, cudaMemcpyAsync(dfdz_host, h->d_g_out, sizeof(double) * nz, cudaMemcpyDeviceToHost, s));

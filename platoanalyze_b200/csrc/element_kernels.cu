@@ -173,6 +173,53 @@ __global__ void __launch_bounds__(kThreads) k_energy_sum(MeshView m, Material ma
     }
 }
 
+// Compliance and its self-adjoint sensitivity in one pass over the cells (the value and the
+// gradient that an MPMD ComputeCriterion operation asks for together, src/Analyze_App.cpp:
+// 727-1014): per cell ese = eps.C.eps once; the energy 1/2 vol s(rho) ese is summed as in
+// k_energy_sum (block partials, the last block adds them in block order) and the cell's
+// sensitivity -1/2 vol s'(rho) drho/dz ese goes to cellq (nodal control: summed per node by
+// k_node_sum afterwards; element control: the gradient itself).
+__global__ void __launch_bounds__(kThreads) k_energy_and_cell_grad(MeshView m, Material mat,
+                                                                   const double* __restrict__ u,
+                                                                   const double* __restrict__ z,
+                                                                   double* __restrict__ partials,
+                                                                   unsigned int* __restrict__ ticket,
+                                                                   double* __restrict__ result,
+                                                                   double* __restrict__ cellq) {
+    __shared__ double sh[32];
+    __shared__ bool last;
+    double v = 0.0;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < m.num_cells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        CellState cs;
+        load_cell(m, mat, z, c, cs);
+        double ue[4][3], e[6], s[6];
+        gather_state(u, cs.n, ue);
+        strain_voigt(cs.G.g, ue, e);
+        stress_voigt(mat, e, s);
+        const double ese = s[0] * e[0] + s[1] * e[1] + s[2] * e[2] + s[3] * e[3] + s[4] * e[4] + s[5] * e[5];
+        v += 0.5 * ese * cs.G.vol * simp(mat, cs.rho);
+        cellq[c] = -0.5 * ese * cs.G.vol * (simp_dx(mat, cs.rho) * rho_dz(mat));
+    }
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v;
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double t = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) t += partials[b];
+        t = block_sum(t, sh);
+        if (threadIdx.x == 0) {
+            *result = t;
+            *ticket = 0u;
+        }
+    }
+}
+
 // Geometric "Volume" criterion (src/geometric/Volume.hpp:83-110): cell volume |det J| / 6
 // weighted by the criterion's own penalty s_v(rho) (ApplyWeighting); GRAD = 1 gives the
 // derivative with respect to one nodal control, vol s_v'(rho) / 4.
@@ -359,6 +406,19 @@ int launch_energy(plato_problem* h, const double* u, const double* z, double* re
     const int G = grid_for(h->C, kThreads, h->partials_len);
     k_energy_sum<<<G, kThreads, 0, h->stream>>>(mesh_view(h), h->material, u, z, h->partials,
                                                  h->red_ticket, result);
+    PLATO_LAUNCH_CHECK(h);
+    return PLATO_OK;
+}
+
+// Compliance into *result (device scalar) and the self-adjoint dC/dz into dfdz, one pass.
+int launch_energy_and_gradient(plato_problem* h, const double* u, const double* z, double* result, double* dfdz) {
+    const int G = grid_for(h->C, kThreads, h->partials_len);
+    const bool cells = h->material.cell_control != 0;
+    k_energy_and_cell_grad<<<G, kThreads, 0, h->stream>>>(mesh_view(h), h->material, u, z, h->partials,
+                                                           h->red_ticket, result, cells ? dfdz : h->cellbuf);
+    PLATO_LAUNCH_CHECK(h);
+    if (cells) return PLATO_OK;
+    k_node_sum<<<grid_for(h->N, kThreads), kThreads, 0, h->stream>>>(graph_view(h), h->cellbuf, dfdz, 0);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

@@ -279,15 +279,16 @@ struct plato_problem {
     double  coarse_gal_ms = 0.0;
     double  coarse_inv_ms = 0.0;
     int64_t coarse_timed = 0;
-    // element kernels timed as one unit per call (kinds 5-7 of plato_get_kernel_timing): the
-    // residual (k_internal_force), the energy sum and the control derivative (per-cell pass +
-    // nodal sum); a pair is read when the same kind is timed again or the totals are read
+    // element kernels timed as one unit per call (kinds 5-8 of plato_get_kernel_timing): the
+    // residual (k_internal_force), the energy sum, the control derivative (per-cell pass +
+    // nodal sum) and the fused value + derivative; a pair is read when the same kind is timed
+    // again or the totals are read
     struct TimedPair {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         int pending = 0;
         double ms = 0.0;
         int64_t count = 0;
-    } elem_timing[3];
+    } elem_timing[4];
     BatchState batch{};
     // subspace initial guess (ritz.cu): columns set for the duration of one solution call
     const double* ritz_W = nullptr;

@@ -185,7 +185,7 @@ class EllipticProblem:
         check(lib.plato_get_instrumentation(self.h, C.byref(n), C.byref(ms), C.byref(k)), self.h)
         out = {"launches": n.value, "op_ms_total": ms.value, "op_timed": k.value}
         for kind, name in ((1, "inner"), (2, "assembly"), (3, "coarse_galerkin"), (4, "coarse_inverse"),
-                           (5, "residual"), (6, "energy"), (7, "dcdz")):
+                           (5, "residual"), (6, "energy"), (7, "dcdz"), (8, "criterion")):
             t, c = C.c_double(), C.c_int64()
             check(lib.plato_get_kernel_timing(self.h, kind, C.byref(t), C.byref(c)), self.h)
             out[name + "_ms_total"], out[name + "_timed"] = t.value, c.value
@@ -331,6 +331,16 @@ class EllipticProblem:
         v = C.c_double()
         check(lib.plato_problem_criterion_value(self.h, self._dev(z), self._dev(u), C.byref(v)), self.h)
         return v.value
+
+    def criterion_value_and_gradient(self, z, u):
+        """Compliance and dC/dz together (one pass over the cells with the self-adjoint
+        shortcut); returns (value, dC/dz, stats)."""
+        g = self.zeros(self.nz)
+        v = C.c_double()
+        st = capi.SolveStats()
+        check(lib.plato_problem_criterion_value_and_gradient(self.h, self._dev(z), self._dev(u), C.byref(v),
+                                                             self._dev(g), C.byref(st)), self.h)
+        return v.value, g, st.as_dict()
 
     def criterion_gradient(self, z, u):
         g = self.zeros(self.nz)

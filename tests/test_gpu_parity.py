@@ -298,3 +298,17 @@ def test_volume_criterion(small):
         assert abs(v - orc.volume_value(z, p, m)) <= TOL * abs(v)
         close(host(prob.volume_gradient_z(zd, p, m)), orc.volume_gradient_z(z, p, m))
     assert prob.volume_value(prob.to_dev(np.ones(orc.N)), 1.0, 0.0) == pytest.approx(2.0, rel=1e-13)
+
+
+def test_fused_criterion_value_and_gradient(small):
+    """plato_problem_criterion_value_and_gradient (one pass) gives exactly what the two calls
+    give: the same energy sum order and the same per-cell sensitivities."""
+    spec, prob, orc, z = small
+    u = np.cos(np.arange(3 * orc.N) * 0.11) * 1e-2
+    ud, zd = prob.to_dev(u), prob.to_dev(z)
+    f, g, st = prob.criterion_value_and_gradient(zd, ud)
+    assert f == prob.criterion_value(zd, ud)
+    g2, _ = prob.criterion_gradient(zd, ud)
+    assert np.array_equal(host(g), host(g2))
+    assert abs(f - orc.sf_value(u, z)) <= TOL * abs(f)
+    close(host(g), orc.criterion_gradient(z, u, self_adjoint=True))

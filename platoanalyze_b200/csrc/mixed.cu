@@ -457,9 +457,12 @@ k_power_step(int64_t n, const uint8_t* __restrict__ mask, const float* __restric
     }
 }
 
+// v_next = Dinv A v / rms(Dinv A v), the norm read from the previous step's device result
+// (no host round trip between the power steps).
 __global__ void k_power_next(int64_t n, const uint8_t* __restrict__ mask, const float* __restrict__ v,
-                             const float* __restrict__ w, const float* __restrict__ dinv32, float scale,
-                             float* __restrict__ vn) {
+                             const float* __restrict__ w, const float* __restrict__ dinv32,
+                             const double* __restrict__ norms, float* __restrict__ vn) {
+    const float scale = float(1.0 / sqrt(norms[2] / double(n)));
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float wi = (mask && mask[i]) ? v[i] : w[i];
         vn[i] = scale * dinv32[i] * wi;
@@ -545,25 +548,26 @@ static int estimate_lambda_max(plato_problem* h, int kind, int steps, double* lm
     const uint8_t* mask = (kind == INNER_EBE32 || kind == INNER_EBE64) ? h->bc_mask : nullptr;
     k_power_init<<<VB, kThreads, 0, h->stream>>>(n, h->f_d0);
     PLATO_LAUNCH_CHECK(h);
-    double host[3] = {0, 0, 0};
-    double lam = 0.0;
-    float scale = 1.0f;
+    // every step stays on the device (the normalisation reads the previous step's sums); the
+    // host reads the Rayleigh quotient of the last step once
     for (int it = 0; it < steps; ++it) {
         int rc = apply_inner_plain(h, kind, h->f_d0, h->f_w);
         if (rc) return rc;
         k_power_step<<<VB, kThreads, 0, h->stream>>>(n, mask, h->f_d0, h->f_w, h->f_dinv, h->partials, h->red_ticket,
                                                      h->red_out);
         PLATO_LAUNCH_CHECK(h);
-        PLATO_CUDA(h, cudaMemcpyAsync(host, h->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
-        lam = host[0] / host[1];
-        scale = float(1.0 / std::sqrt(host[2] / double(n)));
-        if (!std::isfinite(lam) || !std::isfinite(scale))
-            return plato_fail(h, PLATO_NONFINITE, "power iteration for the Chebyshev interval failed");
-        k_power_next<<<VB, kThreads, 0, h->stream>>>(n, mask, h->f_d0, h->f_w, h->f_dinv, scale, h->f_d1);
-        PLATO_LAUNCH_CHECK(h);
-        std::swap(h->f_d0, h->f_d1);
+        if (it + 1 < steps) {
+            k_power_next<<<VB, kThreads, 0, h->stream>>>(n, mask, h->f_d0, h->f_w, h->f_dinv, h->red_out, h->f_d1);
+            PLATO_LAUNCH_CHECK(h);
+            std::swap(h->f_d0, h->f_d1);
+        }
     }
+    double host[3] = {0, 0, 0};
+    PLATO_CUDA(h, cudaMemcpyAsync(host, h->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+    const double lam = host[0] / host[1];
+    if (!std::isfinite(lam) || !(lam > 0.0) || !std::isfinite(host[2]))
+        return plato_fail(h, PLATO_NONFINITE, "power iteration for the Chebyshev interval failed");
     *lmax = lam;
     return PLATO_OK;
 }

@@ -255,7 +255,9 @@ int ritz_guess(plato_problem* h, const double* b, double* x) {
     double rr1 = 0.0;
     for (int bk = 0; bk < VB; ++bk) rr1 += host_rr[bk];
     h->ritz_rel_gain = rr0 > 0.0 ? std::sqrt(rr1 / rr0) : 1.0;
-    const bool keep = std::isfinite(rr1) && rr1 <= kResidualGuard * kResidualGuard * rr0;
+    // the residual guard protects a plain guess; deflated CG needs the Galerkin guess (it lowers
+    // the energy error whatever the residual does), so with deflation only finiteness counts
+    const bool keep = std::isfinite(rr1) && (h->ritz_deflate || rr1 <= kResidualGuard * kResidualGuard * rr0);
     if (keep)
         PLATO_CUDA(h, cudaMemcpyAsync(x, h->v_tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     else

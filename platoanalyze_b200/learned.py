@@ -363,8 +363,10 @@ def main(argv=None) -> int:
         for method in ("plain", "two-level"):
             rows = evaluate(net, 64, test, trs, method, passes)
             print(f"64x32x32 {method} smooth={passes}: iterations "
-                  f"{np.mean([r['iterations'] for r in rows]):.1f} -> {np.mean([r['iterations_learned'] for r in rows]):.1f}; "
-                  f"ms {np.mean([r['ms'] for r in rows]):.2f} -> {np.mean([r['ms_learned'] for r in rows]):.2f}; "
+                  f"{np.mean([r['iterations'] for r in rows]):.1f} -> {np.mean([r['iterations_learned'] for r in rows]):.1f} "
+                  f"(guess), {np.mean([r['iterations_deflated'] for r in rows]):.1f} (deflation); "
+                  f"ms {np.mean([r['ms'] for r in rows]):.2f} -> {np.mean([r['ms_learned'] for r in rows]):.2f}, "
+                  f"{np.mean([r['ms_deflated'] for r in rows]):.2f}; "
                   f"energy captured {np.mean([r['energy_captured'] for r in rows]):.4f}; initial residual ratio "
                   f"{np.mean([r['initial_residual_ratio'] for r in rows]):.3f}", flush=True)
         if a.fine:
@@ -372,7 +374,8 @@ def main(argv=None) -> int:
             for method in ("plain", "two-level"):
                 rows = evaluate(net, f, fine, ftr, method, passes)
                 print(f"{f}x{f // 2}x{f // 2} {method} smooth={passes}: " + "; ".join(
-                    f"it {r['iterations']} -> {r['iterations_learned']}, ms {r['ms']:.1f} -> {r['ms_learned']:.1f}, "
+                    f"it {r['iterations']} -> {r['iterations_learned']} (guess), {r['iterations_deflated']} (deflation), "
+                    f"ms {r['ms']:.1f} -> {r['ms_learned']:.1f}, {r['ms_deflated']:.1f}, "
                     f"energy {r['energy_captured']:.4f}, ratio {r['initial_residual_ratio']:.3f}" for r in rows),
                     flush=True)
     return 0

@@ -48,11 +48,31 @@ struct JacRowSmem {
 };
 static_assert(9 * kFastBlocks <= 12 * kFastCells, "output staging must fit in the gradient area");
 
+// The row kernel of assembly_rows.cu writes only the upper blocks of a narrow row and leaves
+// its lower blocks to the rows that own them as upper blocks.  A wide row assembled here
+// (`wide` given) therefore also writes the transpose of each of its upper blocks into the
+// neighbour's row when that neighbour is narrow; a wide neighbour writes its own row.
+__device__ __forceinline__ void transpose_upper_blocks(const GraphView& g, const uint8_t* __restrict__ wide,
+                                                       double* __restrict__ entries, int64_t row, int lane) {
+    const int32_t rs = g.row_map[row], nbk = g.row_map[row + 1] - rs;
+    for (int k = g.diag[row] - rs + 1 + lane; k < nbk; k += 32) {
+        const int32_t c = g.cols[rs + k];
+        if (wide[c]) continue;
+        const int32_t cs = g.row_map[c];
+        const double* src = entries + 9 * ((int64_t)rs + k);
+        double* dst = entries + 9 * ((int64_t)cs + find_slot(g.cols + cs, g.row_map[c + 1] - cs, int32_t(row)));
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) dst[3 * i + j] = src[3 * j + i];
+    }
+}
+
 // Rows beyond the fast-path limits: every lane walks cells and adds its four blocks with
 // global FP64 atomics into the zeroed row (general meshes with high-valence nodes).
 __device__ __noinline__ void jacobian_row_atomic(const MeshView& m, const GraphView& g, const Material& mat,
                                                  const double* __restrict__ z, double* __restrict__ entries,
-                                                 int64_t row, int lane) {
+                                                 int64_t row, int lane, const uint8_t* __restrict__ wide) {
     const int32_t rs = g.row_map[row], nbk = g.row_map[row + 1] - rs;
     for (int64_t t = lane; t < (int64_t)nbk * 9; t += 32) entries[9 * (int64_t)rs + t] = 0.0;
     __syncwarp();
@@ -76,13 +96,15 @@ __device__ __noinline__ void jacobian_row_atomic(const MeshView& m, const GraphV
         }
     }
     __syncwarp();
+    if (wide) transpose_upper_blocks(g, wide, entries, row, lane);
 }
 
 // Warp per block row over the rows in `rows` (count of them): the path for rows with more
 // blocks than the thread-per-row kernel (assembly_rows.cu) holds.
 __global__ void __launch_bounds__(kJacWarps * 32, 5)
 k_assemble_jacobian(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
-                    double* __restrict__ entries, const int32_t* __restrict__ rows, int32_t count) {
+                    double* __restrict__ entries, const int32_t* __restrict__ rows, int32_t count,
+                    const uint8_t* __restrict__ wide) {
     __shared__ JacRowSmem sm[kJacWarps];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -96,7 +118,7 @@ k_assemble_jacobian(MeshView m, GraphView g, Material mat, const double* __restr
         const int32_t ks = g.n2c_ptr[row];
         const int ncell = g.n2c_ptr[row + 1] - ks;
         if (nbk > kFastBlocks || ncell > kFastCells) {  // warp-uniform
-            jacobian_row_atomic(m, g, mat, z, entries, row, lane);
+            jacobian_row_atomic(m, g, mat, z, entries, row, lane, wide);
             continue;
         }
         if (lane < nbk) {
@@ -193,6 +215,7 @@ k_assemble_jacobian(MeshView m, GraphView g, Material mat, const double* __restr
         double* dst = entries + 9 * (int64_t)rs;
         for (int q = lane; q < 9 * nbk; q += 32) dst[q] = out[q];
         __syncwarp();
+        if (wide) transpose_upper_blocks(g, wide, entries, row, lane);
     }
 }
 
@@ -332,12 +355,14 @@ __global__ void k_matvec_plus(int32_t N, const int32_t* __restrict__ row_map,
 MeshView mesh_view(const plato_problem* h);
 GraphView graph_view(const plato_problem* h);
 
+// The rows in `rows`, whole; with `wide` (the row kernel's wide-row flags) also the transposes
+// of their upper blocks into narrow neighbours.
 int launch_assemble_jacobian_list(plato_problem* h, const double* z, double* entries, const int32_t* rows,
-                                  int32_t count) {
+                                  int32_t count, const uint8_t* wide) {
     if (count <= 0) return PLATO_OK;
     const int blocks = grid_for(count, kJacWarps, 148 * 5 * 8);
     k_assemble_jacobian<<<blocks, kJacWarps * 32, 0, h->stream>>>(mesh_view(h), graph_view(h), h->material, z,
-                                                                  entries, rows, count);
+                                                                  entries, rows, count, wide);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

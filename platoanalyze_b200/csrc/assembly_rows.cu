@@ -9,19 +9,26 @@
 //
 // One thread owns one row and walks the row's incident cells (the node -> cell incidence
 // of the graph, sorted by cell): per cell it gathers the three other nodes' coordinates and
-// densities, forms the gradients with the row node as the reference vertex, and adds
-// w g_a g_b^T into the slot of each other node b.  The slot of each (row, cell, b) is looked
-// up once per mesh (the assembly plan: three 4-bit slot numbers per incidence entry), so the
-// hot loop has no search and no inter-thread reduction.  The diagonal block, which every
-// incident cell feeds, is accumulated in registers (6 symmetric components); the other
-// slots accumulate in shared memory, 9 doubles per slot per thread.  A warp owns the 32 rows
-// of one SELL slice and the layout of its accumulator is [slot][component][lane ^ component]:
-// in the accumulation every lane touches the same component at a time, so the 64-bit
-// accesses of a half warp hit 16 distinct bank pairs; in the row-major write-out (CRS) 16
-// consecutive entries of one row span at most 9 components, two to a bank pair.
+// densities, forms the gradients with the row node as the reference vertex, adds w g_a g_a^T
+// to the diagonal block (registers, 6 symmetric components) and w g_a g_b^T into the slot of
+// each other node b with a larger index -- the upper blocks only.  K is symmetric, so the
+// thread writes each upper block K_ab into its own row and its transpose K_ba into row b;
+// every lower block is written exactly once, by the row that owns it as an upper block.
+// That halves the shared-memory accumulator (9 values per upper block per thread) and the
+// slot updates, and doubles the warps an SM holds.  The slot of each (row, cell, b) and the
+// position of the row in each upper neighbour's row are looked up once per mesh (the
+// assembly plan: three 4-bit upper-slot numbers per incidence entry, 15 for a lower node;
+// one byte per upper block for the mirror slot), so the hot loop has no search and no
+// inter-thread reduction.  A warp owns the 32 rows of one SELL slice and the layout of its
+// accumulator is [slot][component][lane ^ component]: in the accumulation every lane
+// touches the same component at a time, so the 64-bit accesses of a half warp hit 16
+// distinct bank pairs; in the row-major write-out (CRS) 16 consecutive entries of one row
+// span at most 9 components, two to a bank pair.
 //
-// Rows with more than kAsmSlots blocks (high-valence nodes of general meshes) are skipped
-// here and assembled by the warp-per-row kernel of assembly.cu.
+// Rows with more than kAsmMaxUp upper blocks or more than 255 blocks (high-valence nodes of
+// general meshes) are "wide": skipped here and assembled whole, with the transposes of their
+// upper blocks, by the warp-per-row kernel of assembly.cu; narrow rows write no transpose
+// into a wide row.
 //
 // Outputs: the reference's block CRS (the API path), or -- for the solver -- the SELL-32
 // component-major copy of the constrained matrix directly (applyBlockConstraints with zero
@@ -40,17 +47,27 @@ GraphView graph_view(const plato_problem* h);
 
 namespace {
 
-constexpr int kAsmWarps = 6;                        // warps per CTA, one CTA per SM
-constexpr int kAsmSlots = 15;                       // blocks per row held in shared memory
-constexpr int kAccPerWarp = 9 * kAsmSlots * 32;     // doubles
-constexpr size_t kAsmSmem = size_t(kAsmWarps) * kAccPerWarp * sizeof(double);  // 207,360 B
+constexpr int kAsmMaxWarps = 14;         // warps per CTA, one CTA per SM
+constexpr int kAsmMaxUp = 15;            // upper blocks per row held in shared memory (4-bit codes)
+constexpr int kAsmMaxBlocks = 255;       // blocks per row with a one-byte mirror slot
+constexpr int kAsmSmemMax = 227 * 1024;  // dynamic shared memory per CTA
+constexpr uint8_t kNoMirror = 255;       // the upper neighbour is wide: it writes its own row
 
-__device__ __forceinline__ int acc_index(int k, int q, int lane) { return (9 * k + q) * 32 + (lane ^ q); }
+__device__ __forceinline__ int acc_index(int u, int q, int lane) { return (9 * u + q) * 32 + (lane ^ q); }
 
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
+}
+
+__device__ __forceinline__ int row_slot(const int32_t* cols, int n, int32_t node) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (cols[mid] < node) lo = mid + 1; else hi = mid;
+    }
+    return lo;
 }
 
 struct SellOut {
@@ -64,18 +81,31 @@ struct SellOut {
     float* dinv32;           // optional FP32 copy of it
 };
 
-// Per mesh: for every (row, incident cell) entry of n2c, the slots of the cell's three other
-// nodes (ascending local ordinal) in the row, 4 bits each.  Rows with more than kAsmSlots
-// blocks get no plan and are appended to the wide-row list.
-__global__ void k_asm_plan(GraphView g, const int4* __restrict__ conn, uint16_t* __restrict__ plan,
-                           int32_t* __restrict__ wide, int32_t* __restrict__ nwide) {
+// Per mesh, pass 1: the wide rows (list + flags) and the largest upper-block count of the others.
+__global__ void k_asm_flags(GraphView g, uint8_t* __restrict__ wide, int32_t* __restrict__ list,
+                            int32_t* __restrict__ nwide, int32_t* __restrict__ maxup) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < g.num_nodes;
          r += (int64_t)gridDim.x * blockDim.x) {
         const int32_t rs = g.row_map[r], nb = g.row_map[r + 1] - rs;
-        if (nb > kAsmSlots) {
-            wide[atomicAdd(nwide, 1)] = int32_t(r);
-            continue;
-        }
+        const int32_t nup = nb - (g.diag[r] - rs) - 1;
+        const bool w = nup > kAsmMaxUp || nb > kAsmMaxBlocks;
+        wide[r] = w ? 1 : 0;
+        if (w) list[atomicAdd(nwide, 1)] = int32_t(r);
+        else atomicMax(maxup, nup);
+    }
+}
+
+// Per mesh, pass 2 (narrow rows): for every (row, incident cell) entry of n2c, the upper slots
+// of the cell's three other nodes (ascending local ordinal), 4 bits each, 15 for a node with a
+// smaller index; for every upper block, the slot of the row in the neighbour's row
+// (kNoMirror when the neighbour is wide).
+__global__ void k_asm_plan(GraphView g, const int4* __restrict__ conn, const uint8_t* __restrict__ wide,
+                           uint16_t* __restrict__ plan, uint8_t* __restrict__ mirror) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < g.num_nodes;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        if (wide[r]) continue;
+        const int32_t rs = g.row_map[r], nb = g.row_map[r + 1] - rs;
+        const int dslot = g.diag[r] - rs;
         for (int32_t k = g.n2c_ptr[r]; k < g.n2c_ptr[r + 1]; ++k) {
             const int32_t packed = g.n2c[k];
             const int la = packed & 3;
@@ -85,18 +115,24 @@ __global__ void k_asm_plan(GraphView g, const int4* __restrict__ conn, uint16_t*
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 if (b == la) continue;
-                const int32_t node = node_of(n, b);
-                int lo = 0, hi = nb - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (g.cols[rs + mid] < node) lo = mid + 1; else hi = mid;
-                }
-                code |= uint32_t(lo) << (4 * t);
+                const int slot = row_slot(g.cols + rs, nb, node_of(n, b));
+                code |= uint32_t(slot > dslot ? slot - dslot - 1 : 15) << (4 * t);
                 ++t;
             }
             plan[k] = uint16_t(code);
         }
+        for (int k = dslot + 1; k < nb; ++k) {
+            const int32_t c = g.cols[rs + k];
+            const int32_t cs = g.row_map[c];
+            mirror[rs + k] = wide[c] ? kNoMirror : uint8_t(row_slot(g.cols + cs, g.row_map[c + 1] - cs, int32_t(r)));
+        }
     }
+}
+
+__device__ __forceinline__ void store_sell(const SellOut& so, int64_t o, double v) {
+    if (so.v64) so.v64[o] = v;
+    if (so.v32) so.v32[o] = float(v);
+    if (so.v16) so.v16[o] = __float2bfloat16_rn(float(v));
 }
 
 // T = double, kSell = false: block CRS values (unconstrained) into crs[9 * nblocks].
@@ -106,43 +142,43 @@ __global__ void k_asm_plan(GraphView g, const int4* __restrict__ conn, uint16_t*
 //                            the constrained SELL copy (so.v32) and its inverse diagonal
 //                            (so.dinv32), the preconditioner matrix of the mixed-precision solve
 //                            whose FP64 outer operator is the matrix-free element apply.
-// Shared memory is the same 207,360 bytes per CTA: 6 warps of FP64 or 12 warps of FP32 sums.
+// `up` is the largest upper-block count of the narrow rows: each warp's accumulator holds
+// 9 x 32 x up values and the CTA as many warps as the shared memory takes (at most 14).
 template <bool kSell, typename T>
-__global__ void __launch_bounds__(kAsmWarps * 32 * (sizeof(T) == 8 ? 1 : 2), 1)
+__global__ void __launch_bounds__(kAsmMaxWarps * 32, 1)
 k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict__ z,
-                const uint16_t* __restrict__ plan, double* __restrict__ crs, SellOut so) {
-    constexpr int kWarps = kAsmWarps * (sizeof(T) == 8 ? 1 : 2);
+                const uint16_t* __restrict__ plan, const uint8_t* __restrict__ mirror,
+                const uint8_t* __restrict__ wide, int up, double* __restrict__ crs, SellOut so) {
+    const int nwarps = blockDim.x >> 5;
     extern __shared__ double smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    T* acc = smem + warp * kAccPerWarp;
+    T* acc = smem + warp * (9 * 32 * up);
     const T lam = T(mat.c01), mu = T(mat.c33);
     const int32_t nslices = (g.num_nodes + 31) >> 5;
-    for (int32_t s = blockIdx.x * kWarps + warp; s < nslices; s += gridDim.x * kWarps) {
+    for (int32_t s = blockIdx.x * nwarps + warp; s < nslices; s += gridDim.x * nwarps) {
         const int32_t r = 32 * s + lane;
-        int32_t rs = 0, nb = 0, ks = 0, kc = 0, dslot = -1;
+        int32_t rs = 0, nb = 0, ks = 0, kc = 0, dslot = -1, nup = 0;
         T xr[3] = {T(0), T(0), T(0)}, zr = T(0);
         if (r < g.num_nodes) {
             rs = g.row_map[r];
             nb = g.row_map[r + 1] - rs;
-            if (nb <= kAsmSlots) {
+            if (!wide[r]) {
                 ks = g.n2c_ptr[r];
                 kc = g.n2c_ptr[r + 1] - ks;
                 dslot = g.diag[r] - rs;
+                nup = nb - dslot - 1;
                 xr[0] = T(__ldg(m.coords + 3 * (int64_t)r));
                 xr[1] = T(__ldg(m.coords + 3 * (int64_t)r + 1));
                 xr[2] = T(__ldg(m.coords + 3 * (int64_t)r + 2));
                 zr = mat.cell_control ? T(0) : T(__ldg(z + r));
-            } else {
-                nb = 0;  // wide row: assembled by the warp-per-row kernel
             }
         }
-        const int nbw = warp_max(nb);
-        for (int k = 0; k < nbw; ++k)
+        const int nupw = warp_max(nup);
+        for (int u = 0; u < nupw; ++u)
 #pragma unroll
-            for (int q = 0; q < 9; ++q) acc[acc_index(k, q, lane)] = T(0);
+            for (int q = 0; q < 9; ++q) acc[acc_index(u, q, lane)] = T(0);
         __syncwarp();
-
         T d0 = T(0), d1 = T(0), d2 = T(0), d3 = T(0), d4 = T(0), d5 = T(0);  // xx yy zz yz xz xy
         const int kmax = warp_max(kc);
         // one cell ahead: incidence entry, plan and connectivity of the next cell
@@ -205,8 +241,9 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                 d5 = fma(a0, ga1, d5);
 #pragma unroll
                 for (int t = 0; t < 3; ++t) {
-                    const int k = (pl >> (4 * t)) & 15;
-                    T* row = acc + 9 * 32 * k;
+                    const int u = (pl >> (4 * t)) & 15;
+                    if (u == 15) continue;  // a lower node: its row writes the block
+                    T* row = acc + 9 * 32 * u;
 #pragma unroll
                     for (int q = 0; q < 9; ++q) {
                         const T ai = q < 3 ? a0 : (q < 6 ? a1 : a2);
@@ -218,60 +255,111 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
         }
         __syncwarp();
 
-        // K = lambda S + mu S^T + mu tr(S) I per slot; nbw is also the SELL slice width
-        const int64_t pbase = kSell ? __ldg(so.ptr + s) : 0;  // first SELL slot of the slice
-        const int64_t sbase = 9 * pbase;
-        for (int k = 0; k < nbw; ++k) {
-            T S[9];
-            if (k == dslot) {
-                S[0] = d0; S[4] = d1; S[8] = d2;
-                S[5] = S[7] = d3;
-                S[2] = S[6] = d4;
-                S[1] = S[3] = d5;
-            } else {
-#pragma unroll
-                for (int q = 0; q < 9; ++q) S[q] = acc[acc_index(k, q, lane)];
-            }
-            const T tr = mu * (S[0] + S[4] + S[8]);
-            T K[9];
+        // K = lambda S + mu S^T + mu tr(S) I per block
+        T Kd[9];  // the diagonal block
+        {
+            const T tr = mu * (d0 + d1 + d2);
+            const T S[9] = {d0, d5, d4, d5, d1, d3, d4, d3, d2};
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int jj = 0; jj < 3; ++jj)
-                    K[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : T(0));
-            if (!kSell) {
+                    Kd[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : T(0));
+        }
+        if (kSell) {
+            // own row: slots k of the slice (width nbw); lower slots k < dslot are left to the
+            // transposes, slots k >= nb of the slice are zero padding
+            const int nbw = warp_max(nb);
+            const int64_t pbase = __ldg(so.ptr + s);
+            const int64_t sbase = 9 * pbase;
+            for (int k = 0; k < nbw; ++k) {
+                const bool diag = k == dslot, upper = k > dslot && k < nb, pad = k >= nb;
+                if (!(diag || upper || pad)) continue;
+                T K[9];
+                int32_t c = r;
+                if (upper) {
+                    const int u = k - dslot - 1;
+                    T S[9];
 #pragma unroll
-                for (int q = 0; q < 9; ++q) acc[acc_index(k, q, lane)] = K[q];
-            } else {
-                const bool real = k < nb;
-                const int32_t c = __ldg(so.cols + pbase + 32 * k + lane);  // column node of the slot
+                    for (int q = 0; q < 9; ++q) S[q] = acc[acc_index(u, q, lane)];
+                    const T tr = mu * (S[0] + S[4] + S[8]);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int jj = 0; jj < 3; ++jj)
+                            K[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : T(0));
+                    c = __ldg(so.cols + pbase + 32 * k + lane);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) K[q] = diag ? Kd[q] : T(0);
+                }
 #pragma unroll
                 for (int q = 0; q < 9; ++q) {
                     const int i = q / 3, jj = q % 3;
-                    T v = real ? K[q] : T(0);
-                    if (real) {
+                    double v = pad ? 0.0 : double(K[q]);
+                    if (!pad) {
                         const bool mr = __ldg(so.bc_mask + 3 * (int64_t)r + i) != 0;
                         const bool mc = __ldg(so.bc_mask + 3 * (int64_t)c + jj) != 0;
-                        if (mr || mc) v = (c == r && i == jj) ? T(1) : T(0);
+                        if (mr || mc) v = (diag && i == jj) ? 1.0 : 0.0;
                     }
-                    const int64_t o = sbase + 32 * (9 * k + q) + lane;
-                    if (sizeof(T) == 8) so.v64[o] = double(v);
-                    if (so.v32) so.v32[o] = float(v);
-                    if (so.v16) so.v16[o] = __float2bfloat16_rn(float(v));
-                    if (real && k == dslot && i == jj) {
-                        if (sizeof(T) == 8) so.dinv[3 * (int64_t)r + i] = 1.0 / double(v);
-                        if (so.dinv32) so.dinv32[3 * (int64_t)r + i] = float(1.0 / double(v));
+                    store_sell(so, sbase + 32 * (9 * k + q) + lane, v);
+                    if (diag && i == jj) {
+                        if (so.dinv) so.dinv[3 * (int64_t)r + i] = 1.0 / v;
+                        if (so.dinv32) so.dinv32[3 * (int64_t)r + i] = float(1.0 / v);
+                    }
+                }
+                if (upper) {  // the transpose into row c: K_cr[i][j] = K_rc[j][i]
+                    const uint8_t ms = __ldg(mirror + rs + k);
+                    if (ms != kNoMirror) {
+                        const int64_t cb = 9 * __ldg(so.ptr + (c >> 5)) + 32 * 9 * int64_t(ms) + (c & 31);
+#pragma unroll
+                        for (int q = 0; q < 9; ++q) {
+                            const int i = q / 3, jj = q % 3;
+                            const bool mr = __ldg(so.bc_mask + 3 * (int64_t)c + i) != 0;
+                            const bool mc = __ldg(so.bc_mask + 3 * (int64_t)r + jj) != 0;
+                            store_sell(so, cb + 32 * q, (mr || mc) ? 0.0 : double(K[3 * jj + i]));
+                        }
                     }
                 }
             }
-        }
-        if (!kSell) {
+        } else {
+            // upper blocks: K back into the accumulator, the transposes straight to row c
+            for (int u = 0; u < nup; ++u) {
+                T S[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) S[q] = acc[acc_index(u, q, lane)];
+                const T tr = mu * (S[0] + S[4] + S[8]);
+                T K[9];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj)
+                        K[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : T(0));
+#pragma unroll
+                for (int q = 0; q < 9; ++q) acc[acc_index(u, q, lane)] = K[q];
+                const int k = dslot + 1 + u;
+                const uint8_t ms = __ldg(mirror + rs + k);
+                if (ms != kNoMirror) {
+                    const int32_t c = __ldg(g.cols + rs + k);
+                    double* dst = crs + 9 * ((int64_t)__ldg(g.row_map + c) + ms);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int jj = 0; jj < 3; ++jj) dst[3 * i + jj] = double(K[3 * jj + i]);
+                }
+            }
+            if (dslot >= 0) {
+                double* dst = crs + 9 * ((int64_t)rs + dslot);
+#pragma unroll
+                for (int q = 0; q < 9; ++q) dst[q] = double(Kd[q]);
+            }
             __syncwarp();
-            // row-major write-out: the warp writes each row of the slice as one contiguous run
+            // row-major write-out of the upper blocks: one contiguous run per row
             for (int l = 0; l < 32; ++l) {
-                const int32_t rs_l = __shfl_sync(0xffffffffu, rs, l);
-                const int nv = 9 * __shfl_sync(0xffffffffu, nb, l);
-                double* dst = crs + 9 * (int64_t)rs_l;
+                const int nv = 9 * __shfl_sync(0xffffffffu, nup, l);
+                if (nv == 0) continue;
+                const int32_t st = __shfl_sync(0xffffffffu, rs + dslot + 1, l);
+                double* dst = crs + 9 * (int64_t)st;
                 for (int e = lane; e < nv; e += 32) {
                     const int q = e % 9;
                     dst[e] = double(acc[e * 32 + (l ^ q)]);
@@ -284,28 +372,40 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 
 }  // namespace
 
-int launch_assemble_jacobian_rows(plato_problem* h, const double* z, double* entries, int32_t* nwide_out);
 int launch_assemble_jacobian_list(plato_problem* h, const double* z, double* entries, const int32_t* rows,
-                                  int32_t count);
+                                  int32_t count, const uint8_t* wide);
 
-// Builds the assembly plan and the wide-row list once per mesh.
+// Builds the assembly plan, the mirror slots and the wide-row list once per mesh.
 int assembly_plan(plato_problem* h) {
     if (h->asm_plan) return PLATO_OK;
     cudaStream_t s = h->stream;
     const int64_t ninc = 4 * (int64_t)h->C;
     PLATO_CUDA(h, cudaMalloc(&h->asm_plan, sizeof(uint16_t) * (ninc > 0 ? ninc : 1)));
-    PLATO_CUDA(h, cudaMalloc(&h->asm_wide, sizeof(int32_t) * (h->N + 1)));
-    PLATO_CUDA(h, cudaMemsetAsync(h->asm_wide + h->N, 0, sizeof(int32_t), s));
-    k_asm_plan<<<grid_for(h->N, 128), 128, 0, s>>>(graph_view(h), h->conn, h->asm_plan, h->asm_wide,
-                                                   h->asm_wide + h->N);
+    PLATO_CUDA(h, cudaMalloc(&h->asm_mirror, sizeof(uint8_t) * (h->nblocks > 0 ? h->nblocks : 1)));
+    PLATO_CUDA(h, cudaMalloc(&h->asm_wideflag, sizeof(uint8_t) * (h->N > 0 ? h->N : 1)));
+    PLATO_CUDA(h, cudaMalloc(&h->asm_wide, sizeof(int32_t) * (h->N + 2)));
+    PLATO_CUDA(h, cudaMemsetAsync(h->asm_wide + h->N, 0, 2 * sizeof(int32_t), s));
+    k_asm_flags<<<grid_for(h->N, 128), 128, 0, s>>>(graph_view(h), h->asm_wideflag, h->asm_wide, h->asm_wide + h->N,
+                                                    h->asm_wide + h->N + 1);
     PLATO_LAUNCH_CHECK(h);
-    PLATO_CUDA(h, cudaMemcpyAsync(&h->asm_nwide, h->asm_wide + h->N, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    k_asm_plan<<<grid_for(h->N, 128), 128, 0, s>>>(graph_view(h), h->conn, h->asm_wideflag, h->asm_plan,
+                                                   h->asm_mirror);
+    PLATO_LAUNCH_CHECK(h);
+    int32_t counts[2] = {0, 0};
+    PLATO_CUDA(h, cudaMemcpyAsync(counts, h->asm_wide + h->N, sizeof(counts), cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));
+    h->asm_nwide = counts[0];
+    h->asm_maxup = counts[1] > 0 ? counts[1] : 1;
     return PLATO_OK;
 }
 
-static int asm_grid(plato_problem* h, const void* kernel, int* grid, int warps = kAsmWarps) {
-    PLATO_RC(ensure_smem_attribute(h, kernel, int(kAsmSmem)));
+// One CTA per SM with as many warps as the accumulators of `up` upper blocks let fit.
+static int asm_launch(plato_problem* h, const void* kernel, size_t elem, int* grid, int* threads, int* smem) {
+    const int per_warp = int(9 * 32 * h->asm_maxup * elem);
+    const int warps = std::min(kAsmMaxWarps, kAsmSmemMax / per_warp);
+    *threads = 32 * warps;
+    *smem = warps * per_warp;
+    PLATO_RC(ensure_smem_attribute(h, kernel, *smem));
     int sms = 0;
     PLATO_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     const int64_t nslices = (int64_t(h->N) + 31) / 32;
@@ -314,16 +414,19 @@ static int asm_grid(plato_problem* h, const void* kernel, int* grid, int warps =
     return PLATO_OK;
 }
 
-// K(z) into the block CRS `entries` (unconstrained): narrow rows here, wide rows by the
-// warp-per-row kernel.
+// K(z) into the block CRS `entries` (unconstrained): narrow rows here, wide rows (and the
+// transposes of their upper blocks) by the warp-per-row kernel.
 int launch_assemble_jacobian(plato_problem* h, const double* z, double* entries) {
     PLATO_RC(assembly_plan(h));
-    int grid = 0;
-    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<false, double>), &grid));
-    k_assemble_rows<false, double><<<grid, kAsmWarps * 32, kAsmSmem, h->stream>>>(mesh_view(h), graph_view(h), h->material,
-                                                                           z, h->asm_plan, entries, SellOut{});
+    int grid = 0, threads = 0, smem = 0;
+    PLATO_RC(asm_launch(h, reinterpret_cast<const void*>(k_assemble_rows<false, double>), sizeof(double), &grid,
+                        &threads, &smem));
+    k_assemble_rows<false, double><<<grid, threads, smem, h->stream>>>(mesh_view(h), graph_view(h), h->material, z,
+                                                                      h->asm_plan, h->asm_mirror, h->asm_wideflag,
+                                                                      h->asm_maxup, entries, SellOut{});
     PLATO_LAUNCH_CHECK(h);
-    if (h->asm_nwide > 0) PLATO_RC(launch_assemble_jacobian_list(h, z, entries, h->asm_wide, h->asm_nwide));
+    if (h->asm_nwide > 0)
+        PLATO_RC(launch_assemble_jacobian_list(h, z, entries, h->asm_wide, h->asm_nwide, h->asm_wideflag));
     return PLATO_OK;
 }
 
@@ -341,13 +444,15 @@ int launch_assemble_sell(plato_problem* h, const double* z, double* v64, float* 
                          float* dinv32) {
     PLATO_RC(assembly_plan(h));
     if (h->asm_nwide > 0) return plato_fail(h, PLATO_NOT_SUPPORTED, "direct SELL assembly needs every row narrow");
-    int grid = 0;
-    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<true, double>), &grid));
+    int grid = 0, threads = 0, smem = 0;
+    PLATO_RC(asm_launch(h, reinterpret_cast<const void*>(k_assemble_rows<true, double>), sizeof(double), &grid,
+                        &threads, &smem));
     SellOut so{h->sell.ptr, h->sell.cols, h->bc_mask, v64, v32, static_cast<__nv_bfloat16*>(v16), dinv, dinv32};
     // the solver's assembly timing (instrumentation) brackets this one kernel
     if (h->timing && h->asm_ev[0]) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[0], h->stream));
-    k_assemble_rows<true, double><<<grid, kAsmWarps * 32, kAsmSmem, h->stream>>>(mesh_view(h), graph_view(h), h->material,
-                                                                          z, h->asm_plan, nullptr, so);
+    k_assemble_rows<true, double><<<grid, threads, smem, h->stream>>>(mesh_view(h), graph_view(h), h->material, z,
+                                                                     h->asm_plan, h->asm_mirror, h->asm_wideflag,
+                                                                     h->asm_maxup, nullptr, so);
     PLATO_LAUNCH_CHECK(h);
     if (h->timing && h->asm_ev[1]) PLATO_CUDA(h, cudaEventRecord(h->asm_ev[1], h->stream));
     return PLATO_OK;
@@ -359,11 +464,13 @@ int launch_assemble_sell32(plato_problem* h, const double* z, float* v32, float*
     PLATO_RC(assembly_plan(h));
     if (h->asm_nwide > 0) return plato_fail(h, PLATO_NOT_SUPPORTED, "FP32 element assembly needs every row narrow");
     if (h->bc_nonzero) return plato_fail(h, PLATO_NOT_SUPPORTED, "FP32 element assembly needs homogeneous essential BCs");
-    int grid = 0;
-    PLATO_RC(asm_grid(h, reinterpret_cast<const void*>(k_assemble_rows<true, float>), &grid, 2 * kAsmWarps));
+    int grid = 0, threads = 0, smem = 0;
+    PLATO_RC(asm_launch(h, reinterpret_cast<const void*>(k_assemble_rows<true, float>), sizeof(float), &grid,
+                        &threads, &smem));
     SellOut so{h->sell.ptr, h->sell.cols, h->bc_mask, nullptr, v32, nullptr, nullptr, dinv32};
-    k_assemble_rows<true, float><<<grid, 2 * kAsmWarps * 32, kAsmSmem, h->stream>>>(
-        mesh_view(h), graph_view(h), h->material, z, h->asm_plan, nullptr, so);
+    k_assemble_rows<true, float><<<grid, threads, smem, h->stream>>>(mesh_view(h), graph_view(h), h->material, z,
+                                                                    h->asm_plan, h->asm_mirror, h->asm_wideflag,
+                                                                    h->asm_maxup, nullptr, so);
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;
 }

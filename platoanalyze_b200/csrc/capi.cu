@@ -139,7 +139,7 @@ int plato_destroy(plato_problem* h) {
     cudaStreamSynchronize(h->stream);
     dfree(h->conn); dfree(h->coords); dfree(h->row_map); dfree(h->cols); dfree(h->diag);
     dfree(h->n2c_ptr); dfree(h->n2c); dfree(h->F); dfree(h->bc_dofs); dfree(h->bc_values);
-    dfree(h->asm_plan); dfree(h->asm_wide); dfree(h->ritz_small);
+    dfree(h->asm_plan); dfree(h->asm_wide); dfree(h->asm_mirror); dfree(h->asm_wideflag); dfree(h->ritz_small);
     dfree(h->bc_mask); dfree(h->K); dfree(h->KT); dfree(h->v_r); dfree(h->v_z); dfree(h->v_p);
     dfree(h->v_Ap); dfree(h->v_dinv); dfree(h->v_b); dfree(h->v_x); dfree(h->v_tmp);
     dfree(h->partials); dfree(h->cellbuf); dfree(h->scal); dfree(h->red_out); dfree(h->red_ticket);

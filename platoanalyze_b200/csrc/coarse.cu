@@ -21,6 +21,7 @@
 // Per preconditioner call: restriction in two deterministic passes (per-cell partial sums by
 // split CTAs, then a fixed-order sum per coarse dof), y_c = X^T (X r_c) with X = L^-1 (two
 // triangular matrix-vector products, warp per row), prolongation (thread per fine node).
+#include <algorithm>
 #include <mutex>
 
 #include <cub/cub.cuh>
@@ -714,6 +715,8 @@ __global__ void __launch_bounds__(256) k_chol_update(int n, double* __restrict__
 // X = L^-1 by doubling: X starts as its diagonal tiles D[i] and zeros; level s joins blocks
 // of s tiles into blocks of 2s: X[B2,B1] = -X[B2,B2] L[B2,B1] X[B1,B1], in two batched passes:
 // mode 0: T[i,j] = sum_{k in B1, k >= j} L[i,k] X[k,j];  mode 1: X[i,j] = -sum_{k in B2, k <= i} X[i,k] T[k,j].
+// L is banded (tile (i,k) zero for i - k > tb), so T's rows i >= b2 + tb are zero: mode 0
+// forms only rows [b2, b2 + tb) over k >= i - tb, and mode 1 sums over k < b2 + tb.
 __global__ void k_tri_init(int n, const double* __restrict__ D, double* __restrict__ X) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n;
          e += (int64_t)gridDim.x * blockDim.x) {
@@ -723,16 +726,19 @@ __global__ void k_tri_init(int n, const double* __restrict__ D, double* __restri
     }
 }
 
-__global__ void __launch_bounds__(256) k_tri_level(int n, int nblk, int s, int mode, const double* __restrict__ L,
-                                                  double* __restrict__ X, double* __restrict__ T) {
-    const int per_pair = s * s;
+__device__ __forceinline__ int tri_rows(int mode, int s, int tb) { return mode == 0 ? min(s, tb) : s; }
+
+__global__ void __launch_bounds__(256) k_tri_level(int n, int nblk, int s, int mode, int tb,
+                                                  const double* __restrict__ L, double* __restrict__ X,
+                                                  double* __restrict__ T) {
+    const int per_pair = tri_rows(mode, s, tb) * s;
     const int pair = blockIdx.x / per_pair, rem = blockIdx.x - pair * per_pair;
     const int b1 = pair * 2 * s, b2 = b1 + s;
     const int e1 = min(b2, nblk), e2 = min(b2 + s, nblk);
     const int i = b2 + rem / s, j = b1 + rem % s;
     if (b2 >= nblk || i >= e2 || j >= e1) return;
-    if (mode == 0) tile_gemm<0, 0>(n, L, X, T, i, j, j, e1, 1.0, 0.0);
-    else tile_gemm<0, 0>(n, X, T, X, i, j, b2, i + 1, -1.0, 0.0);
+    if (mode == 0) tile_gemm<0, 0>(n, L, X, T, i, j, min(max(j, i - tb), e1), e1, 1.0, 0.0);
+    else tile_gemm<0, 0>(n, X, T, X, i, j, b2, min(i + 1, b2 + tb), -1.0, 0.0);
 }
 
 // Einv = X^T X for X = L^-1 (lower): Einv[i,j] = sum_{k >= max(i,j)} X[k,i]^T X[k,j]
@@ -975,6 +981,10 @@ int coarse_setup_mesh(plato_problem* h) {
     if (bad_h)
         return plato_fail(h, PLATO_BAD_INPUT,
                           "coarse grid does not align with the mesh: an element straddles two coarse cells");
+    // Every element lies in one coarse cell, so E couples only corners of a common cell: nodes
+    // at most (nc1+1)(nc2+1) + (nc2+1) + 1 apart in the x-major numbering, 3 dofs each.
+    c.band = 3 * ((c.nc[1] + 1) * (c.nc[2] + 1) + (c.nc[2] + 1) + 1) + 2;
+    c.tband = (c.band + kNB - 1) / kNB;
     const size_t nn = size_t(c.ndof) * c.ndof;
     PLATO_CUDA(h, cudaMalloc(&c.E, sizeof(double) * nn));
     c.ldf = (c.ndof + 3) & ~3;
@@ -1059,12 +1069,13 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy, int
     // step's diagonal tile needs; the rest of the trailing update (columns >= kb + 2) runs on
     // the side stream meanwhile.  The two write disjoint tile columns; the main stream waits
     // for the side stream's step kb - 1 before it updates column kb + 1 (which that step also
-    // writes), and the side stream starts step kb after panel kb.
+    // writes), and the side stream starts step kb after panel kb.  E is banded and the factor
+    // keeps its band (no fill outside it), so a step touches only the tb tile rows below kb.
     bool trail_pending = false;
     for (int kb = 0; kb < nblk; ++kb) {
         k_chol_diag<<<1, kDiagThreads, kTwoTiles, s>>>(n, c.E, kb, D, c.flag);
         h->launches += 1;
-        const int rem = nblk - kb - 1;
+        const int rem = std::min(nblk - kb - 1, c.tband);
         if (rem == 0) break;
         k_chol_panel<<<rem, 256, kPanelSmem, s>>>(n, c.E, kb, D);
         h->launches += 1;
@@ -1087,9 +1098,9 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy, int
     PLATO_LAUNCH_CHECK(h);
     for (int lv = 1; lv < nblk; lv *= 2) {
         const int pairs = (nblk + 2 * lv - 1) / (2 * lv);
-        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 0, c.E, X, Tmp);
-        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 1, c.E, X, Tmp);
-        h->launches += 1;
+        k_tri_level<<<pairs * std::min(lv, c.tband) * lv, 256, 0, s>>>(n, nblk, lv, 0, c.tband, c.E, X, Tmp);
+        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 1, c.tband, c.E, X, Tmp);
+        h->launches += 2;
         PLATO_LAUNCH_CHECK(h);
     }
     // the coarse solve applies X then U = X^T: FP32 copies with 16-byte rows

@@ -151,6 +151,8 @@ struct CoarseSpace {
     float*   Xf = nullptr;        // L^-1 (lower) then its transpose U (upper), FP32, row stride ldf:
     float*   Uf = nullptr;        // E^-1 = U L^-1, the per-iteration coarse solve (zeros elsewhere)
     int32_t  ldf = 0;             // ndof rounded up to a multiple of 4 (16-byte rows)
+    int32_t  band = 0;            // E[i][j] == 0 for |i - j| > band (structural, x-major node order)
+    int32_t  tband = 0;           // the same in 64 x 64 tiles: tile (ti, tj) == 0 for ti - tj > tband
     double*  X = nullptr;         // L^-1 while inverting (ndof^2)
     double*  T = nullptr;         // tile-product scratch of the inversion (ndof^2)
     double*  Dt = nullptr;        // inverse diagonal tiles of the Cholesky factor
@@ -203,8 +205,11 @@ struct plato_problem {
     // thread-per-row assembly plan (assembly_rows.cu, once per mesh): three 4-bit slots per
     // n2c entry, and the rows with too many blocks for it
     uint16_t* asm_plan = nullptr;
-    int32_t*  asm_wide = nullptr;  // [N + 1]: wide rows, then their count at [N]
+    uint8_t*  asm_mirror = nullptr;   // [nblocks]: slot of the row in each upper neighbour's row
+    uint8_t*  asm_wideflag = nullptr; // [N]: rows assembled by the warp-per-row kernel
+    int32_t*  asm_wide = nullptr;  // [N + 2]: wide rows, then their count at [N], max upper blocks at [N+1]
     int32_t   asm_nwide = 0;
+    int32_t   asm_maxup = 1;       // upper blocks of the widest narrow row
     // assembled operator (allocated on first use)
     double* K = nullptr;           // 9*nblocks
     double* KT = nullptr;          // scratch for transposed / gradient_z matrices

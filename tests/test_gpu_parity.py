@@ -259,10 +259,13 @@ def fan_mesh(k):
     return coords, np.asarray(cells, dtype=np.int32)
 
 
-@pytest.mark.parametrize("k", [12, 20, 40])
+@pytest.mark.parametrize("k", [12, 14, 20, 40])
 def test_high_valence_rows(k):
-    """Rows with more than 32 incident cells or blocks take the atomic assembly path; rows
-    below the limits the register path.  Both must match the oracle."""
+    """Node 0 has k + 2 upper blocks: up to 15 (k = 12) the thread-per-row kernel assembles it,
+    beyond that it is a wide row of the warp-per-row kernel, which also writes the transposes
+    of its upper blocks into the narrow ring rows -- in registers while the row has at most
+    32 incident cells and blocks (k = 14), with global atomics beyond (k = 20, 40).  All must
+    match the oracle."""
     coords, conn = fan_mesh(k)
     spec = ProblemSpec(coords, conn, 1.7, 0.31, 3.0, 1e-9)
     prob, orc = EllipticProblem(spec), Oracle.from_spec(spec)

@@ -508,9 +508,10 @@ def run_profile_unit(args):
         u, st = prob.solution(zd)
         f = prob.criterion_value(zd, u)
         prob.criterion_gradient(zd, u)
-        if args.api_kernels:  # VectorFunction::value and ::gradient_u through the C ABI
+        if args.api_kernels:  # VectorFunction::value and ::gradient_u, the fused criterion pass
             prob.vf_value(u, zd)
             prob.vf_gradient_u(u, zd)
+            prob.criterion_value_and_gradient(zd, u)
         torch.cuda.synchronize()
         print({"cells": (nx, ny, nz), "method": args.method, "compliance": f} | st)
     prob.close()
@@ -701,8 +702,10 @@ def main():
     roofline, roofline_other = rl_spmv, None
     if inst["inner_timed"]:
         if args.method == "two-level-fp16":  # FP16 entries, no Jacobi diagonal stream (unit diagonal)
-            cheb_bytes = 9 * B * 2 + B * 4 + (N + 1) * 4 + 6 * 3 * N * 4
-            cheb_name = "k_sell16s<0> (FP16 Jacobi-scaled SELL SpMV fused with one Chebyshev step)"
+            cb = prob.sell_info()["column_bytes"]  # 16-bit column offsets when the numbering allows
+            cheb_bytes = 9 * B * 2 + B * cb + (N + 1) * 4 + 6 * 3 * N * 4
+            cheb_name = (f"k_sell16s<0> (FP16 Jacobi-scaled SELL SpMV fused with one Chebyshev step, "
+                         f"{8 * cb}-bit column indices)")
         else:
             cheb_bytes = 9 * B * 4 + B * 4 + (N + 1) * 4 + 7 * 3 * N * 4
             cheb_name = "k_cheb_sell<FP32> (FP32 SELL SpMV fused with one Chebyshev step)"

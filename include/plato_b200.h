@@ -187,6 +187,10 @@ int plato_reset_instrumentation(plato_problem* h);
  * sums), 8 = plato_problem_criterion_value_and_gradient's one pass (+ nodal sums).  Reading
  * kinds 5-8 waits for the last timed launch of that kind. */
 int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
+/* The solver's SELL-32 layout of the block matrix: slots (blocks plus the padding of each
+ * 32-row slice to its widest row) and the bytes per column index the FP16 preconditioner
+ * sweep reads (2 when every column lies within 32767 of its slice's first row, else 4). */
+int plato_get_sell_info(const plato_problem* h, int64_t* total_slots, int32_t* column_bytes);
 
 /* ---- block pattern ---------------------------------------------------------------------
  * CreateBlockMatrix (src/ImplicitFunctors.hpp:932-1005) over the node-node graph

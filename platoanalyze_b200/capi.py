@@ -109,6 +109,7 @@ def _load() -> C.CDLL:
         "plato_get_instrumentation": ([vp, C.POINTER(C.c_int64), f64p, C.POINTER(C.c_int64)], C.c_int),
         "plato_reset_instrumentation": ([vp], C.c_int),
         "plato_get_kernel_timing": ([vp, C.c_int32, f64p, C.POINTER(C.c_int64)], C.c_int),
+        "plato_get_sell_info": ([vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)], C.c_int),
         "plato_get_sizes": ([vp, i32p, i32p, C.POINTER(C.c_int64)], C.c_int),
         "plato_jacobian_pattern": ([vp, vp, vp], C.c_int),
         "plato_vf_value": ([vp, vp, vp, vp], C.c_int),

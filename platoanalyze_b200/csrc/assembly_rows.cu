@@ -47,13 +47,20 @@ GraphView graph_view(const plato_problem* h);
 
 namespace {
 
-constexpr int kAsmMaxWarps = 14;         // warps per CTA, one CTA per SM
+constexpr int kAsmMaxWarps = 12;         // warps per CTA, one CTA per SM (170 registers each)
 constexpr int kAsmMaxUp = 15;            // upper blocks per row held in shared memory (4-bit codes)
 constexpr int kAsmMaxBlocks = 255;       // blocks per row with a one-byte mirror slot
 constexpr int kAsmSmemMax = 227 * 1024;  // dynamic shared memory per CTA
 constexpr uint8_t kNoMirror = 255;       // the upper neighbour is wide: it writes its own row
 
-__device__ __forceinline__ int acc_index(int u, int q, int lane) { return (9 * u + q) * 32 + (lane ^ q); }
+// Accumulator layout [upper slot][component][lane]: the SELL output reads a thread's own
+// entries back, so the lanes of one access are 32 consecutive doubles (conflict free per half
+// warp); the CRS output writes each row as one contiguous run, so there the lane index is
+// swizzled by the component (16 consecutive entries of a row then span 9 bank pairs).
+template <bool kSwizzle>
+__device__ __forceinline__ int acc_lane_t(int lane, int q) { return kSwizzle ? (lane ^ q) : lane; }
+template <bool kSell>
+__device__ __forceinline__ int acc_index(int u, int q, int lane) { return (9 * u + q) * 32 + acc_lane_t<!kSell>(lane, q); }
 
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
@@ -177,43 +184,70 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
         const int nupw = warp_max(nup);
         for (int u = 0; u < nupw; ++u)
 #pragma unroll
-            for (int q = 0; q < 9; ++q) acc[acc_index(u, q, lane)] = T(0);
+            for (int q = 0; q < 9; ++q) acc[acc_index<kSell>(u, q, lane)] = T(0);
         __syncwarp();
         T d0 = T(0), d1 = T(0), d2 = T(0), d3 = T(0), d4 = T(0), d5 = T(0);  // xx yy zz yz xz xy
         const int kmax = warp_max(kc);
-        // one cell ahead: incidence entry, plan and connectivity of the next cell
-        int32_t p_next = 0;
-        uint32_t pl_next = 0;
-        int4 n_next = make_int4(0, 0, 0, 0);
+        // Two-stage prefetch: the incidence entry, plan and connectivity two cells ahead, the
+        // three other nodes' coordinates and controls one cell ahead, so each cell's gathers are
+        // in flight during the previous cell's arithmetic.
+        int32_t pA = 0, pB = 0;  // cells j + 1 (connectivity loaded) and j (geometry loaded)
+        uint32_t plA = 0, plB = 0;
+        int4 nA = make_int4(0, 0, 0, 0);
+        double cx[9], cz[3];
+        auto load_geometry = [&](int32_t pk, int4 nk) {
+            const int la = pk & 3;  // the three other nodes in ascending local order
+            const int32_t i0 = la == 0 ? nk.y : nk.x;
+            const int32_t i1 = la <= 1 ? nk.z : nk.y;
+            const int32_t i2 = la <= 2 ? nk.w : nk.z;
+            const double* c0 = m.coords + 3 * (int64_t)i0;
+            const double* c1 = m.coords + 3 * (int64_t)i1;
+            const double* c2 = m.coords + 3 * (int64_t)i2;
+            cx[0] = __ldg(c0); cx[1] = __ldg(c0 + 1); cx[2] = __ldg(c0 + 2);
+            cx[3] = __ldg(c1); cx[4] = __ldg(c1 + 1); cx[5] = __ldg(c1 + 2);
+            cx[6] = __ldg(c2); cx[7] = __ldg(c2 + 1); cx[8] = __ldg(c2 + 2);
+            if (mat.cell_control) {
+                cz[0] = __ldg(z + (pk >> 2));
+                cz[1] = cz[2] = 0.0;
+            } else {
+                cz[0] = __ldg(z + i0);
+                cz[1] = __ldg(z + i1);
+                cz[2] = __ldg(z + i2);
+            }
+        };
         if (kc > 0) {
-            p_next = __ldg(g.n2c + ks);
-            pl_next = __ldg(plan + ks);
-            n_next = __ldg(m.conn + (p_next >> 2));
+            pB = __ldg(g.n2c + ks);
+            plB = __ldg(plan + ks);
+            load_geometry(pB, __ldg(m.conn + (pB >> 2)));
+        }
+        if (kc > 1) {
+            pA = __ldg(g.n2c + ks + 1);
+            plA = __ldg(plan + ks + 1);
+            nA = __ldg(m.conn + (pA >> 2));
         }
 #pragma unroll 1
         for (int j = 0; j < kmax; ++j) {
-            const int32_t p = p_next;
-            const uint32_t pl = pl_next;
-            const int4 n = n_next;
+            const uint32_t pl = plB;
+            double x9[9], z3[3];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) x9[e] = cx[e];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) z3[e] = cz[e];
             if (j + 1 < kc) {
-                p_next = __ldg(g.n2c + ks + j + 1);
-                pl_next = __ldg(plan + ks + j + 1);
-                n_next = __ldg(m.conn + (p_next >> 2));
+                pB = pA;
+                plB = plA;
+                load_geometry(pA, nA);
+            }
+            if (j + 2 < kc) {
+                pA = __ldg(g.n2c + ks + j + 2);
+                plA = __ldg(plan + ks + j + 2);
+                nA = __ldg(m.conn + (pA >> 2));
             }
             if (j < kc) {
-                // the three other nodes in ascending local order; the row node is vertex 3
-                const int la = p & 3;
-                const int32_t i0 = la == 0 ? n.y : n.x;
-                const int32_t i1 = la <= 1 ? n.z : n.y;
-                const int32_t i2 = la <= 2 ? n.w : n.z;
-                const double* c0 = m.coords + 3 * (int64_t)i0;
-                const double* c1 = m.coords + 3 * (int64_t)i1;
-                const double* c2 = m.coords + 3 * (int64_t)i2;
-                const T j11 = T(__ldg(c0)) - xr[0], j21 = T(__ldg(c0 + 1)) - xr[1], j31 = T(__ldg(c0 + 2)) - xr[2];
-                const T j12 = T(__ldg(c1)) - xr[0], j22 = T(__ldg(c1 + 1)) - xr[1], j32 = T(__ldg(c1 + 2)) - xr[2];
-                const T j13 = T(__ldg(c2)) - xr[0], j23 = T(__ldg(c2 + 1)) - xr[1], j33 = T(__ldg(c2 + 2)) - xr[2];
-                const T rho = mat.cell_control ? T(__ldg(z + (p >> 2)))
-                                               : (T(__ldg(z + i0)) + T(__ldg(z + i1)) + T(__ldg(z + i2)) + zr) * T(0.25);
+                const T j11 = T(x9[0]) - xr[0], j21 = T(x9[1]) - xr[1], j31 = T(x9[2]) - xr[2];
+                const T j12 = T(x9[3]) - xr[0], j22 = T(x9[4]) - xr[1], j32 = T(x9[5]) - xr[2];
+                const T j13 = T(x9[6]) - xr[0], j23 = T(x9[7]) - xr[1], j33 = T(x9[8]) - xr[2];
+                const T rho = mat.cell_control ? T(z3[0]) : (T(z3[0]) + T(z3[1]) + T(z3[2]) + zr) * T(0.25);
                 // ComputeGradientWorkset<3> (src/ImplicitFunctors.hpp:169-221) with x_3 = the row node
                 const T c11 = j22 * j33 - j23 * j32, c12 = j13 * j32 - j12 * j33, c13 = j12 * j23 - j13 * j22;
                 const T detj = j11 * c11 + j21 * c12 + j31 * c13;
@@ -247,7 +281,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 #pragma unroll
                     for (int q = 0; q < 9; ++q) {
                         const T ai = q < 3 ? a0 : (q < 6 ? a1 : a2);
-                        T& v = row[q * 32 + (lane ^ q)];
+                        T& v = row[q * 32 + acc_lane_t<!kSell>(lane, q)];
                         v = fma(ai, gb[t][q % 3], v);
                     }
                 }
@@ -281,7 +315,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                     const int u = k - dslot - 1;
                     T S[9];
 #pragma unroll
-                    for (int q = 0; q < 9; ++q) S[q] = acc[acc_index(u, q, lane)];
+                    for (int q = 0; q < 9; ++q) S[q] = acc[acc_index<kSell>(u, q, lane)];
                     const T tr = mu * (S[0] + S[4] + S[8]);
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
@@ -327,7 +361,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
             for (int u = 0; u < nup; ++u) {
                 T S[9];
 #pragma unroll
-                for (int q = 0; q < 9; ++q) S[q] = acc[acc_index(u, q, lane)];
+                for (int q = 0; q < 9; ++q) S[q] = acc[acc_index<kSell>(u, q, lane)];
                 const T tr = mu * (S[0] + S[4] + S[8]);
                 T K[9];
 #pragma unroll
@@ -336,7 +370,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
                     for (int jj = 0; jj < 3; ++jj)
                         K[3 * i + jj] = lam * S[3 * i + jj] + mu * S[3 * jj + i] + (i == jj ? tr : T(0));
 #pragma unroll
-                for (int q = 0; q < 9; ++q) acc[acc_index(u, q, lane)] = K[q];
+                for (int q = 0; q < 9; ++q) acc[acc_index<kSell>(u, q, lane)] = K[q];
                 const int k = dslot + 1 + u;
                 const uint8_t ms = __ldg(mirror + rs + k);
                 if (ms != kNoMirror) {

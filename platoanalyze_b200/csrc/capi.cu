@@ -31,6 +31,7 @@ int solve_state(plato_problem* h, const double* z, const double* u0, double* u, 
 int solve_adjoint(plato_problem* h, const double* z, const double* rhs, double* lam, plato_solve_stats* stats);
 int prepare_mixed(plato_problem* h, const double* crs, const double* z);
 int prepare_coarse(plato_problem* h, const double* z);
+int prepare_coarse_start(plato_problem* h);
 int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* stats);
 int matfree_rhs(plato_problem* h, double* b, double scale);
 int launch_dirichlet_rhs(plato_problem* h, double* rhs, double scale);
@@ -146,7 +147,7 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_r); dfree(h->f_z); dfree(h->f_p); dfree(h->f_Ap); dfree(h->f_x); dfree(h->f_dinv);
     dfree(h->f_K); dfree(h->h_K); dfree(h->f_coords); dfree(h->f_z_ctrl); dfree(h->d_z_ctrl);
     dfree(h->d_z_in); dfree(h->d_u_out); dfree(h->d_g_out);
-    dfree(h->sell.width); dfree(h->sell.ptr); dfree(h->sell.cols);
+    dfree(h->sell.width); dfree(h->sell.ptr); dfree(h->sell.cols); dfree(h->sell.dcols);
     dfree(h->sell64); dfree(h->sell32);
     if (h->sell16) cudaFree(h->sell16);
     if (h->sell16s) cudaFree(h->sell16s);
@@ -394,6 +395,13 @@ int plato_get_kernel_timing(const plato_problem* hc, int32_t kind, double* ms_to
     else if (kind == 3) { *ms_total = h->coarse_gal_ms; *count = h->coarse_timed; }
     else if (kind == 4) { *ms_total = h->coarse_inv_ms; *count = h->coarse_timed; }
     else return PLATO_BAD_INPUT;
+    return PLATO_OK;
+}
+
+int plato_get_sell_info(const plato_problem* h, int64_t* total_slots, int32_t* column_bytes) {
+    if (!h || !total_slots || !column_bytes) return PLATO_BAD_INPUT;
+    *total_slots = h->sell.total_slots;
+    *column_bytes = h->sell.dcols ? 2 : 4;
     return PLATO_OK;
 }
 
@@ -739,6 +747,7 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         PLATO_CUDA(h, cudaMemcpyAsync(h->v_b, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     h->coarse.active = 0;
     if (h->opts.operator_kind == PLATO_OPERATOR_MATRIX_FREE) {
+        RC(prepare_coarse_start(h));
         RC(prepare_coarse(h, z));  // starts on its own stream, overlapping what follows
         RC(prepare_mixed(h, nullptr, z));
         RC(matfree_rhs(h, h->v_b, bc_scale));
@@ -776,8 +785,11 @@ static int solve_constrained(plato_problem* h, const double* z, const double* rh
         RC(ritz_guess(h, h->v_b, x));
         rc = pcg_fp64(h, h->v_b, x, st);
     } else {
-        RC(prepare_coarse(h, z));  // starts on its own stream, overlapping the fine-level set-up
+        // the fine-level set-up is queued first (a few launches), then the coarse set-up on its
+        // own stream, overlapping it from the point where z is final
+        RC(prepare_coarse_start(h));
         RC(prepare_mixed(h, crs, z));
+        RC(prepare_coarse(h, z));
         RC(ritz_guess(h, h->v_b, x));
         rc = fcg_poly(h, h->v_b, x, st);
         const int crc = coarse_finish(h);  // the overlapped coarse set-up: timing and its check

@@ -1016,12 +1016,112 @@ void coarse_release(plato_problem* h) {
     if (c.Xf) { cudaFree(c.Xf); c.Xf = c.Uf = nullptr; }
     if (c.pending && c.ev_ready) cudaEventSynchronize(c.ev_ready);
     c.pending = 0;
+    c.start_marked = 0;
     for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail, &c.ev_start, &c.ev_ready})
         if (*e) { cudaEventDestroy(*e); *e = nullptr; }
+    if (c.chain) { cudaGraphExecDestroy(c.chain); c.chain = nullptr; }
     if (c.side) { cudaStreamDestroy(c.side); c.side = nullptr; }
     if (c.cs) { cudaStreamDestroy(c.cs); c.cs = nullptr; }
     if (c.flag_host) { cudaFreeHost(c.flag_host); c.flag_host = nullptr; }
     c.ready = 0;
+}
+
+// The coarse set-up is a chain of small dependent kernels running beside the fine-level
+// work: its streams take the highest priority, so each of its CTAs is scheduled as soon as an
+// SM has room rather than behind the queued fine-level CTAs.
+static int coarse_stream(plato_problem* h, cudaStream_t* st) {
+    int least = 0, greatest = 0;
+    PLATO_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    PLATO_CUDA(h, cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, greatest));
+    return PLATO_OK;
+}
+
+// Enqueues on the coarse stream (being captured) the banded blocked Cholesky of E, the
+// doubling inverse X = L^-1 and the FP32 packing of X and X^T.
+static int enqueue_factorization(plato_problem* h, int* launches) {
+    CoarseSpace& c = h->coarse;
+    cudaStream_t s = c.cs;
+    const int n = c.ndof;
+    const int nblk = (n + kNB - 1) / kNB;
+    double *X = c.X, *D = c.Dt, *Tmp = c.T;  // scratch allocated with the coarse grid
+    int nl = 0;
+    PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
+    // Right-looking blocked Cholesky with a look-ahead of one tile column.  Step kb on the
+    // coarse stream: diagonal tile, panel, then the update of column kb + 1 alone, which the
+    // next step's diagonal tile needs; the rest of the trailing update (columns >= kb + 2)
+    // runs on the side stream meanwhile.  The two write disjoint tile columns; the coarse
+    // stream waits for the side stream's step kb - 1 before it updates column kb + 1 (which
+    // that step also writes), and the side stream starts step kb after panel kb.  E is banded
+    // and the factor keeps its band (no fill outside it), so a step touches only the tband
+    // tile rows below kb.
+    bool trail_pending = false;
+    for (int kb = 0; kb < nblk; ++kb) {
+        k_chol_diag<<<1, kDiagThreads, kTwoTiles, s>>>(n, c.E, kb, D, c.flag);
+        ++nl;
+        const int rem = std::min(nblk - kb - 1, c.tband);
+        if (rem == 0) break;
+        k_chol_panel<<<rem, 256, kPanelSmem, s>>>(n, c.E, kb, D);
+        ++nl;
+        if (trail_pending) PLATO_CUDA(h, cudaStreamWaitEvent(s, c.ev_trail, 0));
+        trail_pending = false;
+        if (rem > 1) {
+            PLATO_CUDA(h, cudaEventRecord(c.ev_panel, s));
+            PLATO_CUDA(h, cudaStreamWaitEvent(c.side, c.ev_panel, 0));
+            k_chol_update<false><<<(rem - 1) * rem / 2, 256, 0, c.side>>>(n, c.E, kb, nblk);
+            PLATO_CUDA(h, cudaEventRecord(c.ev_trail, c.side));
+            trail_pending = true;
+            ++nl;
+        }
+        k_chol_update<true><<<rem, 256, 0, s>>>(n, c.E, kb, nblk);
+        ++nl;
+    }
+    if (trail_pending) PLATO_CUDA(h, cudaStreamWaitEvent(s, c.ev_trail, 0));
+    PLATO_LAUNCH_CHECK(h);
+    k_tri_init<<<grid_for(int64_t(n) * n, 256, 148 * 16), 256, 0, s>>>(n, D, X);
+    ++nl;
+    PLATO_LAUNCH_CHECK(h);
+    for (int lv = 1; lv < nblk; lv *= 2) {
+        const int pairs = (nblk + 2 * lv - 1) / (2 * lv);
+        k_tri_level<<<pairs * std::min(lv, c.tband) * lv, 256, 0, s>>>(n, nblk, lv, 0, c.tband, c.E, X, Tmp);
+        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 1, c.tband, c.E, X, Tmp);
+        nl += 2;
+        PLATO_LAUNCH_CHECK(h);
+    }
+    // the coarse solve applies X then U = X^T: FP32 copies with 16-byte rows
+    const int nt = (n + 31) / 32;
+    k_coarse_pack<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, c.ldf, X, c.Xf, c.Uf);
+    ++nl;
+    PLATO_LAUNCH_CHECK(h);
+    *launches = nl;
+    return PLATO_OK;
+}
+
+// Captures enqueue_factorization into c.chain (once per coarse grid).
+static int capture_factorization(plato_problem* h) {
+    CoarseSpace& c = h->coarse;
+    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_chol_diag), int(kTwoTiles)));
+    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_chol_panel), int(kPanelSmem)));
+    if (!c.side) PLATO_RC(coarse_stream(h, &c.side));
+    for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
+        if (!*e) PLATO_CUDA(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    PLATO_CUDA(h, cudaStreamBeginCapture(c.cs, cudaStreamCaptureModeThreadLocal));
+    int launches = 0;
+    const int rc = enqueue_factorization(h, &launches);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(c.cs, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) return plato_fail(h, PLATO_CUDA_ERROR, cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&c.chain, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        c.chain = nullptr;
+        return plato_fail(h, PLATO_CUDA_ERROR, cudaGetErrorString(ie));
+    }
+    c.chain_launches = launches;
+    return PLATO_OK;
 }
 
 // Per-solve setup: Galerkin operator of control z, Cholesky, explicit inverse, on the coarse
@@ -1030,11 +1130,12 @@ void coarse_release(plato_problem* h) {
 // use, coarse_finish after the solve); otherwise wait here.
 int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy, int deferred) {
     CoarseSpace& c = h->coarse;
-    if (!c.cs) PLATO_CUDA(h, cudaStreamCreateWithFlags(&c.cs, cudaStreamNonBlocking));
+    if (!c.cs) PLATO_RC(coarse_stream(h, &c.cs));
     for (cudaEvent_t* e : {&c.ev_start, &c.ev_ready})
         if (!*e) PLATO_CUDA(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     if (!c.flag_host) PLATO_CUDA(h, cudaMallocHost(reinterpret_cast<void**>(&c.flag_host), sizeof(int32_t)));
-    PLATO_CUDA(h, cudaEventRecord(c.ev_start, h->stream));
+    if (!c.start_marked) PLATO_CUDA(h, cudaEventRecord(c.ev_start, h->stream));
+    c.start_marked = 0;
     PLATO_CUDA(h, cudaStreamWaitEvent(c.cs, c.ev_start, 0));
     cudaStream_t s = c.cs;
     const int n = c.ndof;
@@ -1056,57 +1157,12 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy, int
     PLATO_LAUNCH_CHECK(h);
     if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[1], s));
     if (E_copy) PLATO_CUDA(h, cudaMemcpyAsync(E_copy, c.E, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
-    PLATO_CUDA(h, cudaMemsetAsync(c.flag, 0, sizeof(int32_t), s));
-    const int nblk = (n + kNB - 1) / kNB;
-    double *X = c.X, *D = c.Dt, *Tmp = c.T;  // scratch allocated with the coarse grid
-    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_chol_diag), int(kTwoTiles)));
-    PLATO_RC(ensure_smem_attribute(h, reinterpret_cast<const void*>(k_chol_panel), int(kPanelSmem)));
-    if (!c.side) PLATO_CUDA(h, cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&c.ev_panel, &c.ev_trail})
-        if (!*e) PLATO_CUDA(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    // Right-looking blocked Cholesky with a look-ahead of one tile column.  Step kb on the main
-    // stream: diagonal tile, panel, then the update of column kb + 1 alone, which the next
-    // step's diagonal tile needs; the rest of the trailing update (columns >= kb + 2) runs on
-    // the side stream meanwhile.  The two write disjoint tile columns; the main stream waits
-    // for the side stream's step kb - 1 before it updates column kb + 1 (which that step also
-    // writes), and the side stream starts step kb after panel kb.  E is banded and the factor
-    // keeps its band (no fill outside it), so a step touches only the tb tile rows below kb.
-    bool trail_pending = false;
-    for (int kb = 0; kb < nblk; ++kb) {
-        k_chol_diag<<<1, kDiagThreads, kTwoTiles, s>>>(n, c.E, kb, D, c.flag);
-        h->launches += 1;
-        const int rem = std::min(nblk - kb - 1, c.tband);
-        if (rem == 0) break;
-        k_chol_panel<<<rem, 256, kPanelSmem, s>>>(n, c.E, kb, D);
-        h->launches += 1;
-        if (trail_pending) PLATO_CUDA(h, cudaStreamWaitEvent(s, c.ev_trail, 0));
-        trail_pending = false;
-        if (rem > 1) {
-            PLATO_CUDA(h, cudaEventRecord(c.ev_panel, s));
-            PLATO_CUDA(h, cudaStreamWaitEvent(c.side, c.ev_panel, 0));
-            k_chol_update<false><<<(rem - 1) * rem / 2, 256, 0, c.side>>>(n, c.E, kb, nblk);
-            PLATO_CUDA(h, cudaEventRecord(c.ev_trail, c.side));
-            trail_pending = true;
-            h->launches += 1;
-        }
-        k_chol_update<true><<<rem, 256, 0, s>>>(n, c.E, kb, nblk);
-        h->launches += 1;
-    }
-    if (trail_pending) PLATO_CUDA(h, cudaStreamWaitEvent(s, c.ev_trail, 0));
-    PLATO_LAUNCH_CHECK(h);
-    k_tri_init<<<grid_for(int64_t(n) * n, 256, 148 * 16), 256, 0, s>>>(n, D, X);
-    PLATO_LAUNCH_CHECK(h);
-    for (int lv = 1; lv < nblk; lv *= 2) {
-        const int pairs = (nblk + 2 * lv - 1) / (2 * lv);
-        k_tri_level<<<pairs * std::min(lv, c.tband) * lv, 256, 0, s>>>(n, nblk, lv, 0, c.tband, c.E, X, Tmp);
-        k_tri_level<<<pairs * lv * lv, 256, 0, s>>>(n, nblk, lv, 1, c.tband, c.E, X, Tmp);
-        h->launches += 2;
-        PLATO_LAUNCH_CHECK(h);
-    }
-    // the coarse solve applies X then U = X^T: FP32 copies with 16-byte rows
-    const int nt = (n + 31) / 32;
-    k_coarse_pack<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(n, c.ldf, X, c.Xf, c.Uf);
-    PLATO_LAUNCH_CHECK(h);
+    // The factorization and inversion chain is the same launch sequence every solve (its
+    // kernels read only E and the coarse scratch): captured once into a CUDA graph and replayed,
+    // so the host does not spend a launch per tile step while the fine-level set-up waits.
+    if (!c.chain) PLATO_RC(capture_factorization(h));
+    PLATO_CUDA(h, cudaGraphLaunch(c.chain, s));
+    h->launches += c.chain_launches;
     if (h->timing) PLATO_CUDA(h, cudaEventRecord(h->coarse_ev[2], s));
     PLATO_CUDA(h, cudaMemcpyAsync(c.flag_host, c.flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaEventRecord(c.ev_ready, s));
@@ -1114,6 +1170,16 @@ int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy, int
     if (deferred) return PLATO_OK;
     PLATO_RC(coarse_wait(h));
     return coarse_finish(h);
+}
+
+// Marks the point of the handle's stream after which the next coarse set-up may start (its
+// control is final there), so that fine-level work queued in between does not delay it.
+int coarse_mark_start(plato_problem* h) {
+    CoarseSpace& c = h->coarse;
+    if (!c.ev_start) PLATO_CUDA(h, cudaEventCreateWithFlags(&c.ev_start, cudaEventDisableTiming));
+    PLATO_CUDA(h, cudaEventRecord(c.ev_start, h->stream));
+    c.start_marked = 1;
+    return PLATO_OK;
 }
 
 int coarse_wait(plato_problem* h) {
@@ -1169,6 +1235,7 @@ extern "C" int plato_coarse_operator(plato_problem* h, const double* z, int32_t*
     if (!E && !Einv) return PLATO_OK;
     if (!z) return plato_fail(h, PLATO_BAD_INPUT, "null control");
     const size_t nn = size_t(h->coarse.ndof) * h->coarse.ndof;
+    h->coarse.start_marked = 0;  // z is final at this point of the stream
     double* Ed = nullptr;
     PLATO_CUDA(h, cudaMalloc(&Ed, sizeof(double) * nn));
     rc = coarse_setup_operator(h, z, Ed);

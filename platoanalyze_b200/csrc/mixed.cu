@@ -204,7 +204,9 @@ k_cheb_sell(SellView A, const void* __restrict__ vals, const float* __restrict__
 // this latency-bound loop).  Entry (k, q) of the pair at (9 ptr_s) / 2 + 16 (9k + q) + m.
 // MODE 0: Chebyshev step in scaled variables (unit diagonal): w = A^ d, res -= w,
 //         d_next = c1 d + c2 res, y += d_next;  MODE 1: res -= A^ x;  MODE 2: out = A^ x.
-template <int MODE>
+// kShort: the pair's two column indices come as 16-bit offsets from the slice's first row
+// (one 4-byte load instead of 8; 20 instead of 22 bytes per block pair entry).
+template <int MODE, bool kShort>
 __global__ void __launch_bounds__(kThreads, 4)
 k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__ x, float* __restrict__ res,
           float* __restrict__ dnext, float* __restrict__ y, float c1, float c2, const PcgScalars* S) {
@@ -222,11 +224,19 @@ k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__
         const int w = __ldg(A.width + sl);
         const int64_t base = __ldg(A.ptr + sl);
         const int2* __restrict__ cp = reinterpret_cast<const int2*>(A.cols + base) + m;
+        const short2* __restrict__ dp = reinterpret_cast<const short2*>(A.dcols + base) + m;
+        const int32_t row0 = int32_t(32 * sl);
         const __half2* __restrict__ vp = reinterpret_cast<const __half2*>(vals + 9 * base) + m;
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
 #pragma unroll 4
         for (int k = 0; k < w; ++k) {
-            const int2 c = __ldg(cp + 16 * k);
+            int2 c;
+            if (kShort) {
+                const short2 d = __ldg(dp + 16 * k);
+                c = make_int2(row0 + d.x, row0 + d.y);
+            } else {
+                c = __ldg(cp + 16 * k);
+            }
             const float x0 = __ldg(x + 3 * (int64_t)c.x), x1 = __ldg(x + 3 * (int64_t)c.x + 1),
                         x2 = __ldg(x + 3 * (int64_t)c.x + 2);
             const float z0 = __ldg(x + 3 * (int64_t)c.y), z1 = __ldg(x + 3 * (int64_t)c.y + 1),
@@ -532,8 +542,12 @@ static int apply_inner_plain(plato_problem* h, int kind, const float* x, float* 
     const void* vals = inner_vals(h, kind);
     const int B = spmv_blocks(h);
     if (kind == INNER_SELL16S)
-        k_sell16s<2><<<B, kThreads, 0, h->stream>>>(V, static_cast<const __half*>(vals), x, nullptr, nullptr, y, 0.f,
-                                                    0.f, nullptr);
+        if (V.dcols)
+            k_sell16s<2, true><<<B, kThreads, 0, h->stream>>>(V, static_cast<const __half*>(vals), x, nullptr, nullptr,
+                                                              y, 0.f, 0.f, nullptr);
+        else
+            k_sell16s<2, false><<<B, kThreads, 0, h->stream>>>(V, static_cast<const __half*>(vals), x, nullptr, nullptr,
+                                                               y, 0.f, 0.f, nullptr);
     else if (kind == INNER_SELL16) k_sell_apply32<INNER_SELL16><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
     else if (kind == INNER_SELL32) k_sell_apply32<INNER_SELL32><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
     else k_sell_apply32<INNER_SELL64><<<B, kThreads, 0, h->stream>>>(V, vals, x, y);
@@ -628,6 +642,14 @@ int prepare_mixed(plato_problem* h, const double* crs, const double* z) {
                : launch_assemble_sell(h, z, h->sell64, o32, o16, h->v_dinv, h->f_dinv);
 }
 
+// Mesh-level coarse data (once per grid) and the start mark of the next per-solve set-up.
+int prepare_coarse_start(plato_problem* h) {
+    if (h->opts.coarse_cells[0] <= 0) return PLATO_OK;
+    int rc = coarse_setup_mesh(h);
+    if (rc) return rc;
+    return coarse_mark_start(h);
+}
+
 // Two-level preconditioner data for control z (mesh buckets once, Galerkin operator per solve).
 int prepare_coarse(plato_problem* h, const double* z) {
     if (h->opts.coarse_cells[0] <= 0 || !z) return PLATO_OK;
@@ -659,7 +681,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     if (kind == INNER_SELL16S) {
         int sms = 0, per_sm = 0;
         PLATO_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-        PLATO_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sell16s<0>, kThreads, 0));
+        PLATO_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sell16s<0, false>, kThreads, 0));
         CB = std::min(SB, std::max(1, per_sm) * std::max(1, sms));
     }
 
@@ -668,9 +690,10 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     if (rc) return rc;
     const double safety = kind == INNER_SELL16 ? 1.15 : 1.10;
     const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree);
-    // the coarse set-up ran on its own stream meanwhile: the iterations wait for it here
-    rc = coarse_wait(h);
-    if (rc) return rc;
+    // The coarse set-up runs on its own stream meanwhile; the handle's stream waits for it only
+    // at the first coarse solve (after the first residual and Chebyshev sweep), so the set-up
+    // overlaps that work too.
+    bool coarse_waited = false;
 
     auto outer_apply = [&](const double* in, double* out) -> int {
         if (mf) {
@@ -691,8 +714,12 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             if (r2) return r2;
             k_res_sub_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, xin, h->f_w, h->f_res, h->scal);
         } else if (kind == INNER_SELL16S) {
-            k_sell16s<1><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), xin, h->f_res, nullptr,
-                                                 nullptr, 0.f, 0.f, h->scal);
+            if (V.dcols)
+                k_sell16s<1, true><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), xin, h->f_res,
+                                                           nullptr, nullptr, 0.f, 0.f, h->scal);
+            else
+                k_sell16s<1, false><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), xin, h->f_res,
+                                                            nullptr, nullptr, 0.f, 0.f, h->scal);
         } else if (kind == INNER_SELL16) {
             k_res_sub_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, xin, h->f_res, h->scal);
         } else if (kind == INNER_SELL32) {
@@ -723,8 +750,12 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                 k_cheb_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, h->f_w, h->f_dinv, h->f_res, dcur, dnext, h->f_y,
                                                    cc.c1[k], cc.c2[k], h->scal);
             } else if (kind == INNER_SELL16S) {
-                k_sell16s<0><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), dcur, h->f_res, dnext,
-                                                     h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                if (V.dcols)
+                    k_sell16s<0, true><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), dcur,
+                                                               h->f_res, dnext, h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                else
+                    k_sell16s<0, false><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), dcur,
+                                                                h->f_res, dnext, h->f_y, cc.c1[k], cc.c2[k], h->scal);
             } else if (kind == INNER_SELL16) {
                 k_cheb_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
                                                                   h->f_y, cc.c1[k], cc.c2[k], h->scal);
@@ -752,6 +783,11 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         if (r2 || !coarse) return r2;
         r2 = inner_apply_sub(dlast);  // the sweep left res = r - A (s - d_last)
         if (r2) return r2;
+        if (!coarse_waited) {
+            r2 = coarse_wait(h);
+            if (r2) return r2;
+            coarse_waited = true;
+        }
         return coarse_apply(h, h->f_res, h->f_y, 1, h->scal, scaled ? h->f_sq : nullptr);
     };
 

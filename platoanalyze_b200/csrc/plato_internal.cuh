@@ -163,11 +163,14 @@ struct CoarseSpace {
     double*  tc = nullptr;        // L^-1 rc
     int32_t* flag = nullptr;
     cudaStream_t side = nullptr;  // trailing Cholesky updates, overlapped with the next panel
+    cudaGraphExec_t chain = nullptr;  // the captured factorization + inversion chain
+    int          chain_launches = 0;
     cudaEvent_t  ev_panel = nullptr, ev_trail = nullptr;
     // the per-solve set-up runs on a stream of its own, overlapped with the fine-level set-up
     // (assembly, SELL copies, spectrum estimate) on the handle's stream
     cudaStream_t cs = nullptr;
     cudaEvent_t  ev_start = nullptr, ev_ready = nullptr;
+    int          start_marked = 0;    // ev_start already recorded for the next set-up
     int32_t*     flag_host = nullptr; // pinned copy of flag (factorization failure)
     int          pending = 0;         // a set-up is in flight: wait for ev_ready before use
 };
@@ -325,6 +328,7 @@ int plato_fail(plato_problem* h, int status, const std::string& msg);
 namespace plato {
 int coarse_setup_mesh(plato_problem* h);
 int coarse_setup_operator(plato_problem* h, const double* z, double* E_copy = nullptr, int deferred = 0);
+int coarse_mark_start(plato_problem* h);  // ev_start: where the next set-up may begin
 int coarse_wait(plato_problem* h);    // the handle's stream waits for the set-up (no host wait)
 int coarse_finish(plato_problem* h);  // host wait, timing, factorization check
 int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, const PcgScalars* S,

@@ -67,6 +67,27 @@ __global__ void k_sell_cols(int32_t N, int32_t nslices, const int32_t* __restric
     }
 }
 
+// Column offsets from the slice's first row, 16 bits each, for the FP16 sweep (whose
+// column indices are otherwise 18 % of its bytes); `bad` counts offsets that do not fit.  The
+// padding lanes past the last row (zero entries) point at the slice's first row.
+__global__ void k_sell_dcols(int32_t N, int32_t nslices, const int64_t* __restrict__ ptr,
+                             const int32_t* __restrict__ cols, int16_t* __restrict__ dcols,
+                             int32_t* __restrict__ bad) {
+    for (int64_t s = blockIdx.x; s < nslices; s += gridDim.x) {
+        const int64_t base = ptr[s], end = ptr[s + 1];
+        for (int64_t t = base + threadIdx.x; t < end; t += blockDim.x) {
+            const int64_t r = 32 * s + ((t - base) & 31);
+            const int64_t d = r < N ? int64_t(cols[t]) - 32 * s : 0;
+            if (d < -32768 || d > 32767) {
+                atomicAdd(bad, 1);
+                dcols[t] = 0;
+            } else {
+                dcols[t] = int16_t(d);
+            }
+        }
+    }
+}
+
 // Per-slice transpose CRS -> SELL (+ Jacobi diagonal, + optional FP32 / BF16 copies).
 template <bool kSmem>
 __global__ void __launch_bounds__(kSliceThreads)
@@ -192,12 +213,23 @@ int build_sell_pattern(plato_problem* h) {
     PLATO_CUDA(h, cudaMalloc(&P.cols, sizeof(int32_t) * (P.total_slots > 0 ? P.total_slots : 1)));
     k_sell_cols<<<grid_for(ns, 1, 148 * 64), 256, 0, s>>>(N, ns, h->row_map, h->cols, P.width, P.ptr, P.cols);
     PLATO_LAUNCH_CHECK(h);
+    // the 16-bit column offsets (kept only when every column is within 32767 of its slice)
+    PLATO_CUDA(h, cudaMalloc(&P.dcols, sizeof(int16_t) * (P.total_slots > 0 ? P.total_slots : 1)));
+    PLATO_CUDA(h, cudaMemsetAsync(d_max, 0, sizeof(int32_t), s));
+    k_sell_dcols<<<grid_for(ns, 1, 148 * 64), 256, 0, s>>>(N, ns, P.ptr, P.cols, P.dcols, d_max);
+    PLATO_LAUNCH_CHECK(h);
+    int32_t bad = 0;
+    PLATO_CUDA(h, cudaMemcpyAsync(&bad, d_max, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PLATO_CUDA(h, cudaFreeAsync(tmp, s));
     PLATO_CUDA(h, cudaFreeAsync(tmp2, s));
     PLATO_CUDA(h, cudaFreeAsync(d_max, s));
     PLATO_CUDA(h, cudaFreeAsync(slots, s));
     PLATO_CUDA(h, cudaFreeAsync(slice_nnz, s));
     PLATO_CUDA(h, cudaStreamSynchronize(s));
+    if (bad) {
+        PLATO_CUDA(h, cudaFree(P.dcols));
+        P.dcols = nullptr;
+    }
     return PLATO_OK;
 }
 

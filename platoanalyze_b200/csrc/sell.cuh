@@ -12,6 +12,7 @@ struct SellPattern {
     int32_t* width = nullptr;       // [nslices] blocks per row in the slice (max over its rows)
     int64_t* ptr = nullptr;         // [nslices+1] first slot of each slice
     int32_t* cols = nullptr;        // [total_slots] column node of each slot
+    int16_t* dcols = nullptr;       // [total_slots] column - 32 * slice, when every one fits in 16 bits
     int64_t  total_slots = 0;
     int32_t  max_slice_blocks = 0;  // max CRS blocks in one slice (transpose tile size)
 };
@@ -21,6 +22,7 @@ struct SellView {
     const int32_t* width;
     const int64_t* ptr;
     const int32_t* cols;
+    const int16_t* dcols;  // nullptr unless the mesh numbering keeps every column within 16 bits
 };
 
 __device__ __forceinline__ float to_float(float v) { return v; }

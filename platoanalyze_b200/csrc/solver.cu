@@ -232,7 +232,9 @@ k_dot(int64_t n, const double* __restrict__ a, const double* __restrict__ b, dou
 
 }  // namespace
 
-SellView sell_view(const plato_problem* h) { return SellView{h->N, h->sell.width, h->sell.ptr, h->sell.cols}; }
+SellView sell_view(const plato_problem* h) {
+    return SellView{h->N, h->sell.width, h->sell.ptr, h->sell.cols, h->sell.dcols};
+}
 
 int spmv_blocks(const plato_problem* h) {
     const int64_t padded = ((int64_t)h->N + 31) & ~int64_t(31);

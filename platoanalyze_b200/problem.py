@@ -191,6 +191,13 @@ class EllipticProblem:
             out[name + "_ms_total"], out[name + "_timed"] = t.value, c.value
         return out
 
+    def sell_info(self) -> dict:
+        """The solver's SELL-32 layout: slots (with slice padding) and the bytes per column
+        index the FP16 preconditioner sweep reads."""
+        slots, cb = C.c_int64(), C.c_int32()
+        check(lib.plato_get_sell_info(self.h, C.byref(slots), C.byref(cb)), self.h)
+        return {"total_slots": slots.value, "column_bytes": cb.value}
+
     def reset_instrumentation(self) -> None:
         check(lib.plato_reset_instrumentation(self.h), self.h)
 

@@ -208,3 +208,37 @@ def test_fp32_element_assembly_matches_the_fp64_matrix(setup):
     with pytest.raises(capi.PlatoError):  # only with the matrix-free FP64 operator
         prob.set_solver(SolverOptions(precision=capi.PRECISION_MIXED_FP32_ASSEMBLED, chebyshev_degree=8))
     prob.set_solver(SolverOptions(tolerance=1e-10))
+
+
+def test_fp16_sweep_column_offsets_and_their_fallback():
+    """The FP16 sweep reads 16-bit column offsets when the numbering keeps every column within
+    32767 of its slice and 32-bit columns otherwise (a randomly relabelled 70,785-node mesh).
+    Both layouts solve the same problem to the same answer."""
+    from platoanalyze_b200.workloads import coarse_grid, method_options
+    cells = (64, 32, 32)
+    opts = method_options("two-level-fp16", 1e-11, coarse_grid(*cells))
+    spec = cantilever(*cells, opts)
+    N = spec.coords.shape[0]
+    rng = np.random.default_rng(11)
+    perm = rng.permutation(N).astype(np.int32)
+    coords = np.empty_like(spec.coords)
+    coords[perm] = spec.coords
+    bc = 3 * perm[spec.bc_dofs // 3] + spec.bc_dofs % 3
+    spec_p = ProblemSpec(coords, perm[spec.connectivity].astype(np.int32), spec.youngs_modulus,
+                         spec.poissons_ratio, spec.penalty_exponent, spec.penalty_minimum, spec.tractions,
+                         bc.astype(np.int32), spec.bc_values, opts)
+    a, b = EllipticProblem(spec), EllipticProblem(spec_p)
+    assert a.sell_info()["column_bytes"] == 2
+    assert b.sell_info()["column_bytes"] == 4
+    z = splitmix_uniform(N, 0x5EED0002)
+    zp = np.empty_like(z)
+    zp[perm] = z
+    ua, sa = a.solution(a.to_dev(z))
+    ub, sb = b.solution(b.to_dev(zp))
+    assert sa["converged"] == 1 and sb["converged"] == 1
+    assert sa["relative_residual"] <= 1e-11 and sb["relative_residual"] <= 1e-11
+    uah = host(ua).reshape(-1, 3)
+    ubh = host(ub).reshape(-1, 3)[perm]
+    assert rel_l2(ubh, uah) <= 1e-8, rel_l2(ubh, uah)
+    a.close()
+    b.close()

@@ -47,6 +47,22 @@ SIZES = {"large": (160, 80, 80), "medium": (80, 40, 40), "small": (20, 10, 10)}
 # coarse box grid of the two-level method: coarse cells of 10^3 hexes (16x8x8 on 160x80x80,
 # 4131 coarse dofs), see workloads.coarse_grid
 SEED_LARGE = 0x5EED0002  # nodal densities of the workload (SplitMix64 stream)
+# DRAM bytes per algorithmic byte of each roofline kernel: ncu's dram__bytes_read.sum +
+# dram__bytes_write.sum per launch on the 120x60x60 cantilever (450,241 nodes, 2,592,000 cells,
+# 6,606,721 blocks; inputs above L2) divided by that launch's algorithmic bytes.  Every stream
+# of these kernels grows with the mesh, so the bench line's traffic is this ratio times the
+# algorithmic bytes of its own launch.  Ratios near 1: no re-reads; the dC/dz pair reads the
+# cell values and the node -> cell incidence a second time (nodal sums after the cell pass).
+TRAFFIC_RATIO = {
+    "sweep": 152.3 / 166.35,        # k_sell16s<0> (16-bit columns)
+    "fp64_spmv": 533.8 / 525.52,    # k_fcg_sell_apply
+    "assembly": 595.5 / 559.79,     # k_assemble_rows<SELL>
+    "residual": 79.58 / 77.49,      # k_internal_force
+    "energy": 67.58 / 66.69,        # k_energy_sum
+    "dcdz": 135.35 / 70.29,         # k_cell_quantity<2> + k_node_sum
+    "criterion": 135.34 / 70.29,    # k_energy_and_cell_grad + k_node_sum
+}
+TRAFFIC_NOTE = "ncu DRAM bytes per launch on the 120x60x60 cantilever, scaled by the algorithmic bytes"
 
 
 METHOD_TEXT = {
@@ -697,7 +713,8 @@ def main():
     spmv_ms = inst["op_ms_total"] / max(1, inst["op_timed"])
     rl_spmv = {"bound": "hbm", "kernel": "k_sell_spmv / k_fcg_sell_apply (FP64 SELL-32 SpMV + p.Ap)",
                "achieved": spmv_bytes / (spmv_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-               "frac": spmv_bytes / (spmv_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+               "frac": spmv_bytes / (spmv_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+               "traffic": TRAFFIC_RATIO["fp64_spmv"] * spmv_bytes, "traffic_source": TRAFFIC_NOTE,
                "algorithmic_bytes": spmv_bytes, "avg_launch_ms": spmv_ms, "launches_timed": inst["op_timed"]}
     roofline, roofline_other = rl_spmv, None
     if inst["inner_timed"]:
@@ -712,7 +729,9 @@ def main():
         cheb_ms = inst["inner_ms_total"] / inst["inner_timed"]
         rl_cheb = {"bound": "hbm", "kernel": cheb_name,
                    "achieved": cheb_bytes / (cheb_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                   "frac": cheb_bytes / (cheb_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+                   "frac": cheb_bytes / (cheb_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                   "traffic": TRAFFIC_RATIO["sweep"] * cheb_bytes if args.method == "two-level-fp16" and cb == 2 else None,
+                   "traffic_source": TRAFFIC_NOTE,
                    "algorithmic_bytes": cheb_bytes, "avg_launch_ms": cheb_ms, "launches_timed": inst["inner_timed"]}
         roofline, roofline_other = rl_cheb, rl_spmv
 
@@ -724,7 +743,8 @@ def main():
         rl_asm = {"bound": "hbm", "kernel": "k_assemble_rows<SELL> (K(z) straight into the constrained SELL copy: "
                                            "thread per block row, upper blocks and their transposes)",
                   "achieved": asm_bytes / (asm_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                  "frac": asm_bytes / (asm_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+                  "frac": asm_bytes / (asm_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                  "traffic": TRAFFIC_RATIO["assembly"] * asm_bytes, "traffic_source": TRAFFIC_NOTE,
                   "algorithmic_bytes": asm_bytes, "avg_launch_ms": asm_ms, "launches_timed": inst["assembly_timed"]}
 
     # element kernels: the energy sum and the fused self-adjoint dC/dz are inside every step; the
@@ -741,24 +761,26 @@ def main():
     inst_e = prob.instrumentation()
     elem_in = 16 * prob.num_cells + 24 * N + 8 * N + 24 * N
 
-    def roof_line(kernel, nbytes, ms_total, count):
+    def roof_line(kernel, nbytes, ms_total, count, ratio):
         if not count:
             return None
         ms = ms_total / count
         return {"bound": "hbm", "kernel": kernel, "achieved": nbytes / (ms / 1e3) / 1e9, "peak": peak,
                 "unit": "GB/s", "frac": nbytes / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes": nbytes, "avg_launch_ms": ms, "launches_timed": count}
+                "traffic": ratio * nbytes, "traffic_source": TRAFFIC_NOTE, "algorithmic_bytes": nbytes,
+                "avg_launch_ms": ms, "launches_timed": count}
 
     rl_elements = {
         "residual": roof_line("k_internal_force (+ the load copy): R = K(z) u - F", elem_in + 24 * N,
-                              inst_e["residual_ms_total"], inst_e["residual_timed"]),
+                              inst_e["residual_ms_total"], inst_e["residual_timed"], TRAFFIC_RATIO["residual"]),
         "energy": roof_line("k_energy_sum: compliance 1/2 u^T K(z) u", elem_in,
-                            inst_e["energy_ms_total"], inst_e["energy_timed"]),
+                            inst_e["energy_ms_total"], inst_e["energy_timed"], TRAFFIC_RATIO["energy"]),
         "dcdz": roof_line("k_cell_quantity<2> + k_node_sum: self-adjoint dC/dz", elem_in + 8 * N,
-                          inst_e["dcdz_ms_total"], inst_e["dcdz_timed"]),
+                          inst_e["dcdz_ms_total"], inst_e["dcdz_timed"], TRAFFIC_RATIO["dcdz"]),
         "criterion_in_step": roof_line("k_energy_and_cell_grad + k_node_sum: compliance and dC/dz in one pass "
                                        "(the step's ComputeCriterion)", elem_in + 8 * N,
-                                       inst["criterion_ms_total"], inst["criterion_timed"])}
+                                       inst["criterion_ms_total"], inst["criterion_timed"],
+                                       TRAFFIC_RATIO["criterion"])}
 
     # two-level coarse operator, once per solve: the Galerkin product P^T A P, then the banded
     # FP64 Cholesky (the coarse operator couples only corners of a common coarse cell) and the

@@ -2,6 +2,8 @@
 // control derivatives.  Every kernel gathers connectivity (one int4 per cell), nodal
 // coordinates, control and state straight from the global arrays (no worksets) and
 // recomputes the tet kinematics in registers.
+#include <algorithm>
+
 #include "plato_internal.cuh"
 
 namespace plato {
@@ -142,7 +144,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return r;  // valid in thread 0
 }
 
-__global__ void __launch_bounds__(kThreads) k_energy_sum(MeshView m, Material mat,
+__global__ void __launch_bounds__(kThreads, 4) k_energy_sum(MeshView m, Material mat,
                                                          const double* __restrict__ u,
                                                          const double* __restrict__ z,
                                                          double* __restrict__ partials,
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(kThreads) k_energy_sum(MeshView m, Material ma
 // k_energy_sum (block partials, the last block adds them in block order) and the cell's
 // sensitivity -1/2 vol s'(rho) drho/dz ese goes to cellq (nodal control: summed per node by
 // k_node_sum afterwards; element control: the gradient itself).
-__global__ void __launch_bounds__(kThreads) k_energy_and_cell_grad(MeshView m, Material mat,
+__global__ void __launch_bounds__(kThreads, 4) k_energy_and_cell_grad(MeshView m, Material mat,
                                                                    const double* __restrict__ u,
                                                                    const double* __restrict__ z,
                                                                    double* __restrict__ partials,
@@ -401,9 +403,18 @@ __global__ void k_sum_pieces(int32_t nseg, const double* __restrict__ pieces, do
     }
 }
 
+// The energy sums run one resident wave (4 CTAs of 256 threads per SM at 64 registers): each
+// thread accumulates several cells before the block sums, so the per-block reduction and the
+// partial written per block are paid once per CTA rather than once per 256 cells.
+static int energy_grid(plato_problem* h) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess || sms < 1) sms = 148;
+    return grid_for(h->C, kThreads, std::min(h->partials_len, 4 * sms));
+}
+
 // Internal elastic energy into *result (device scalar).
 int launch_energy(plato_problem* h, const double* u, const double* z, double* result) {
-    const int G = grid_for(h->C, kThreads, h->partials_len);
+    const int G = energy_grid(h);
     k_energy_sum<<<G, kThreads, 0, h->stream>>>(mesh_view(h), h->material, u, z, h->partials,
                                                  h->red_ticket, result);
     PLATO_LAUNCH_CHECK(h);
@@ -412,7 +423,7 @@ int launch_energy(plato_problem* h, const double* u, const double* z, double* re
 
 // Compliance into *result (device scalar) and the self-adjoint dC/dz into dfdz, one pass.
 int launch_energy_and_gradient(plato_problem* h, const double* u, const double* z, double* result, double* dfdz) {
-    const int G = grid_for(h->C, kThreads, h->partials_len);
+    const int G = energy_grid(h);
     const bool cells = h->material.cell_control != 0;
     k_energy_and_cell_grad<<<G, kThreads, 0, h->stream>>>(mesh_view(h), h->material, u, z, h->partials,
                                                            h->red_ticket, result, cells ? dfdz : h->cellbuf);

@@ -118,6 +118,18 @@ typedef struct plato_solver_opts {
                                  then falls back to the plain FP64 Jacobi-PCG from a zero
                                  guess; this caps the fallback's iterations (0: the same cap
                                  as max_iterations, < 0: no fallback)                      */
+    int32_t chebyshev_kind;   /* polynomial of the Chebyshev preconditioner: 0 or 1 = first
+                                 kind on [lambda_max/ratio, lambda_max]; 4 = fourth kind on
+                                 (0, lambda_max] (Lottes, Numer. Linear Algebra Appl. 2023;
+                                 chebyshev_ratio unused), which damps the upper part of the
+                                 spectrum more and leaves the lowest modes to the coarse space */
+    int32_t sweep_steps;      /* FP16 scaled sweep (PLATO_PRECISION_MIXED_FP16): Chebyshev steps
+                                 per launch.  0 or 1 = one launch per step; 2..16 = that many
+                                 steps in one launch, each (step, 512-row tile) task waiting only
+                                 for the tiles of the step before that its columns reach, so the
+                                 matrix can be re-read from L2 (needs 16-bit column offsets)  */
+    int32_t sweep_lag;        /* multi-step sweep: tiles of 512 rows by which each step trails the
+                                 one before beyond the column reach (0 = 600 / sweep_steps)  */
 } plato_solver_opts;
 
 typedef struct plato_problem_desc {
@@ -185,8 +197,20 @@ int plato_reset_instrumentation(plato_problem* h);
  * of plato_vf_value (load copy + element force kernel), 6 = the energy sum of plato_sf_value,
  * 7 = the self-adjoint dC/dz of plato_problem_criterion_gradient (per-cell pass + nodal
  * sums), 8 = plato_problem_criterion_value_and_gradient's one pass (+ nodal sums).  Reading
- * kinds 5-8 waits for the last timed launch of that kind. */
+ * kinds 5-8 waits for the last timed launch of that kind.  With the multi-step FP16 sweep
+ * (sweep_steps) kind 1 times the first launch of the sampled preconditioner calls and counts
+ * it as its number of steps, so ms_total / count stays the time per step. */
 int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
+/* The FP16 sweep of the last flexible-CG solve: Chebyshev steps per launch (1 = one launch
+ * per step; > 1 = the multi-step sweep) and its column reach in tiles of 512 rows (-1 when
+ * not measured). */
+int plato_get_sweep_info(const plato_problem* h, int32_t* steps_per_launch, int32_t* halo_tiles);
+/* Test hook for the bounded device waits (no reference counterpart): the next multi-step sweep
+ * launch of this handle waits for a completion stamp that none of its tasks writes, so its
+ * first dependency wait gives up after its poll limit (about a second).  The launch then ends,
+ * the solve reports the timeout to the host, the multi-step sweep is switched off for the
+ * handle and the plain FP64 Jacobi-PCG fallback finishes the solve (fallback_max_iterations). */
+int plato_test_stall_next_sweep(plato_problem* h);
 /* The solver's SELL-32 layout of the block matrix: slots (blocks plus the padding of each
  * 32-row slice to its widest row) and the bytes per column index the FP16 preconditioner
  * sweep reads (2 when every column lies within 32767 of its slice's first row, else 4). */

@@ -50,7 +50,8 @@ class SolverOpts(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int32), ("operator_kind", C.c_int32),
                 ("precision", C.c_int32), ("self_adjoint", C.c_int32), ("chebyshev_ratio", C.c_double),
                 ("chebyshev_degree", C.c_int32), ("coarse_cells", C.c_int32 * 3),
-                ("fallback_max_iterations", C.c_int32)]
+                ("fallback_max_iterations", C.c_int32), ("chebyshev_kind", C.c_int32),
+                ("sweep_steps", C.c_int32), ("sweep_lag", C.c_int32)]
 
 
 class ProblemDesc(C.Structure):
@@ -110,6 +111,8 @@ def _load() -> C.CDLL:
         "plato_reset_instrumentation": ([vp], C.c_int),
         "plato_get_kernel_timing": ([vp, C.c_int32, f64p, C.POINTER(C.c_int64)], C.c_int),
         "plato_get_sell_info": ([vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)], C.c_int),
+        "plato_get_sweep_info": ([vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "plato_test_stall_next_sweep": ([vp], C.c_int),
         "plato_get_sizes": ([vp, i32p, i32p, C.POINTER(C.c_int64)], C.c_int),
         "plato_jacobian_pattern": ([vp, vp, vp], C.c_int),
         "plato_vf_value": ([vp, vp, vp, vp], C.c_int),

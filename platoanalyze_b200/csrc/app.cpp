@@ -300,6 +300,9 @@ plato_solver_opts read_solver(const ParamList& deck) {
         throw AppError(PLATO_BAD_INPUT, "Linear Solver: unknown Method '" + ls.get_string("Method") + "'");
     }
     o.chebyshev_ratio = ls.get_double("Chebyshev Ratio", o.chebyshev_ratio);
+    o.chebyshev_kind = ls.get_int("Chebyshev Kind", 1);
+    if (o.chebyshev_kind != 1 && o.chebyshev_kind != 4)
+        throw AppError(PLATO_BAD_INPUT, "Linear Solver: 'Chebyshev Kind' must be 1 or 4");
     return o;
 }
 

@@ -112,6 +112,10 @@ int check_opts(plato_problem* h, const plato_solver_opts& o) {
         return plato_fail(h, PLATO_BAD_INPUT, "unknown precision");
     if (o.precision == PLATO_PRECISION_MIXED_FP32_ASSEMBLED && o.operator_kind != PLATO_OPERATOR_MATRIX_FREE)
         return plato_fail(h, PLATO_BAD_INPUT, "FP32 element assembly pairs with the matrix-free FP64 operator");
+    if (o.chebyshev_kind != 0 && o.chebyshev_kind != 1 && o.chebyshev_kind != 4)
+        return plato_fail(h, PLATO_BAD_INPUT, "chebyshev_kind must be 0 or 1 (first kind) or 4 (fourth kind)");
+    if (o.sweep_steps < 0 || o.sweep_steps > 16) return plato_fail(h, PLATO_BAD_INPUT, "sweep_steps must be in 0..16");
+    if (o.sweep_lag < 0) return plato_fail(h, PLATO_BAD_INPUT, "sweep_lag must be >= 0");
     return PLATO_OK;
 }
 
@@ -154,6 +158,8 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_sq); dfree(h->f_isq);
     dfree(h->mf_w64); dfree(h->mf_w32); dfree(h->v_q);
     dfree(h->f_res); dfree(h->f_d0); dfree(h->f_d1); dfree(h->f_y); dfree(h->f_w);
+    dfree(h->wave_flags); dfree(h->wave_ctl);
+    for (int32_t*& o : h->wave_order) dfree(o);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->poll_ev)
@@ -395,6 +401,19 @@ int plato_get_kernel_timing(const plato_problem* hc, int32_t kind, double* ms_to
     else if (kind == 3) { *ms_total = h->coarse_gal_ms; *count = h->coarse_timed; }
     else if (kind == 4) { *ms_total = h->coarse_inv_ms; *count = h->coarse_timed; }
     else return PLATO_BAD_INPUT;
+    return PLATO_OK;
+}
+
+int plato_test_stall_next_sweep(plato_problem* h) {
+    if (!h) return PLATO_BAD_INPUT;
+    h->wave_stall = 1;
+    return PLATO_OK;
+}
+
+int plato_get_sweep_info(const plato_problem* h, int32_t* steps_per_launch, int32_t* halo_tiles) {
+    if (!h || !steps_per_launch || !halo_tiles) return PLATO_BAD_INPUT;
+    *steps_per_launch = h->sweep_steps_used > 0 ? h->sweep_steps_used : 1;
+    *halo_tiles = h->wave_halo >= 0 ? h->wave_halo : -1;
     return PLATO_OK;
 }
 

@@ -202,10 +202,103 @@ k_cheb_sell(SellView A, const void* __restrict__ vals, const float* __restrict__
 // slice share each (k, q) entry pair as one __half2 and their column indices as one int2,
 // so a thread loads 4 bytes per entry load (2-byte loads would halve the bytes in flight of
 // this latency-bound loop).  Entry (k, q) of the pair at (9 ptr_s) / 2 + 16 (9k + q) + m.
-// MODE 0: Chebyshev step in scaled variables (unit diagonal): w = A^ d, res -= w,
-//         d_next = c1 d + c2 res, y += d_next;  MODE 1: res -= A^ x;  MODE 2: out = A^ x.
 // kShort: the pair's two column indices come as 16-bit offsets from the slice's first row
 // (one 4-byte load instead of 8; 20 instead of 22 bytes per block pair entry).
+// kConstX: x is read-only for the whole kernel (read through the non-coherent path); the
+// multi-step sweep reads directions written by other CTAs of the same launch with plain
+// loads instead, ordered after its acquire of their completion flags.
+template <bool kShort, bool kConstX>
+__device__ __forceinline__ void sell16s_pair(const SellView& A, const __half* __restrict__ vals, const float* x,
+                                             int64_t pr, float (&wv)[6]) {
+    const int64_t sl = pr >> 4;
+    const int m = int(pr & 15);
+    const int w = __ldg(A.width + sl);
+    const int64_t base = __ldg(A.ptr + sl);
+    const int2* __restrict__ cp = reinterpret_cast<const int2*>(A.cols + base) + m;
+    const short2* __restrict__ dp = reinterpret_cast<const short2*>(A.dcols + base) + m;
+    const int32_t row0 = int32_t(32 * sl);
+    const __half2* __restrict__ vp = reinterpret_cast<const __half2*>(vals + 9 * base) + m;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < w; ++k) {
+        int2 c;
+        if (kShort) {
+            const short2 d = __ldg(dp + 16 * k);
+            c = make_int2(row0 + d.x, row0 + d.y);
+        } else {
+            c = __ldg(cp + 16 * k);
+        }
+        const float* xa = x + 3 * (int64_t)c.x;
+        const float* xb = x + 3 * (int64_t)c.y;
+        const float x0 = kConstX ? __ldg(xa) : xa[0], x1 = kConstX ? __ldg(xa + 1) : xa[1],
+                    x2 = kConstX ? __ldg(xa + 2) : xa[2];
+        const float z0 = kConstX ? __ldg(xb) : xb[0], z1 = kConstX ? __ldg(xb + 1) : xb[1],
+                    z2 = kConstX ? __ldg(xb + 2) : xb[2];
+        const __half2* vk = vp + 144 * k;
+        float2 e[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) e[q] = __half22float2(vk[16 * q]);
+        a0 += e[0].x * x0 + e[1].x * x1 + e[2].x * x2;
+        a1 += e[3].x * x0 + e[4].x * x1 + e[5].x * x2;
+        a2 += e[6].x * x0 + e[7].x * x1 + e[8].x * x2;
+        b0 += e[0].y * z0 + e[1].y * z1 + e[2].y * z2;
+        b1 += e[3].y * z0 + e[4].y * z1 + e[5].y * z2;
+        b2 += e[6].y * z0 + e[7].y * z1 + e[8].y * z2;
+    }
+    wv[0] = a0; wv[1] = a1; wv[2] = a2; wv[3] = b0; wv[4] = b1; wv[5] = b2;
+}
+
+// The pair's vector update after w = A^ x.  MODE 0: Chebyshev step in scaled variables (unit
+// diagonal): res -= w, d_next = c1 x + c2 res, y += d_next;  MODE 1: res -= w;  MODE 2: y = w.
+template <int MODE>
+__device__ __forceinline__ void sell16s_update(int64_t num_rows, int64_t pr, const float (&wv)[6],
+                                               const float* __restrict__ x, float* __restrict__ res,
+                                               float* __restrict__ dnext, float* __restrict__ y, float c1, float c2,
+                                               bool vec2) {
+    const int64_t r0 = 32 * (pr >> 4) + 2 * (pr & 15);
+    // both rows of the pair: their 6 entries start at 3 r0 = 6 (16 sl + m), 8-byte aligned
+    // when the vectors are, so the update runs on float2 (half the memory instructions)
+    if (MODE != 2 && vec2 && r0 + 1 < num_rows) {
+        float2* rp = reinterpret_cast<float2*>(res + 3 * r0);
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const float2 rr = rp[u];
+            const float rs0 = rr.x - wv[2 * u], rs1 = rr.y - wv[2 * u + 1];
+            rp[u] = make_float2(rs0, rs1);
+            if (MODE == 0) {
+                const float2 xx = reinterpret_cast<const float2*>(x + 3 * r0)[u];
+                float2* yp = reinterpret_cast<float2*>(y + 3 * r0) + u;
+                const float2 yy = *yp;
+                const float d0 = c1 * xx.x + c2 * rs0, d1 = c1 * xx.y + c2 * rs1;
+                reinterpret_cast<float2*>(dnext + 3 * r0)[u] = make_float2(d0, d1);
+                *yp = make_float2(yy.x + d0, yy.y + d1);
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        if (r0 + h >= num_rows) break;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * (r0 + h) + i;
+            const float wi = wv[3 * h + i];
+            if (MODE == 0) {
+                const float rs = res[k] - wi;
+                res[k] = rs;
+                const float dn = c1 * x[k] + c2 * rs;
+                dnext[k] = dn;
+                y[k] += dn;
+            } else if (MODE == 1) {
+                res[k] -= wi;
+            } else {
+                y[k] = wi;
+            }
+        }
+    }
+}
+
+// One application of the FP16 scaled matrix per launch (sell16s_pair + sell16s_update).
 template <int MODE, bool kShort>
 __global__ void __launch_bounds__(kThreads, 4)
 k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__ x, float* __restrict__ res,
@@ -219,82 +312,153 @@ k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__
     const bool vec2 = (vbits & 7) == 0;
     for (int64_t pr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pr < npairs;
          pr += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t sl = pr >> 4;
-        const int m = int(pr & 15);
-        const int w = __ldg(A.width + sl);
-        const int64_t base = __ldg(A.ptr + sl);
-        const int2* __restrict__ cp = reinterpret_cast<const int2*>(A.cols + base) + m;
-        const short2* __restrict__ dp = reinterpret_cast<const short2*>(A.dcols + base) + m;
-        const int32_t row0 = int32_t(32 * sl);
-        const __half2* __restrict__ vp = reinterpret_cast<const __half2*>(vals + 9 * base) + m;
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
-#pragma unroll 4
-        for (int k = 0; k < w; ++k) {
-            int2 c;
-            if (kShort) {
-                const short2 d = __ldg(dp + 16 * k);
-                c = make_int2(row0 + d.x, row0 + d.y);
-            } else {
-                c = __ldg(cp + 16 * k);
-            }
-            const float x0 = __ldg(x + 3 * (int64_t)c.x), x1 = __ldg(x + 3 * (int64_t)c.x + 1),
-                        x2 = __ldg(x + 3 * (int64_t)c.x + 2);
-            const float z0 = __ldg(x + 3 * (int64_t)c.y), z1 = __ldg(x + 3 * (int64_t)c.y + 1),
-                        z2 = __ldg(x + 3 * (int64_t)c.y + 2);
-            const __half2* vk = vp + 144 * k;
-            float2 e[9];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) e[q] = __half22float2(vk[16 * q]);
-            a0 += e[0].x * x0 + e[1].x * x1 + e[2].x * x2;
-            a1 += e[3].x * x0 + e[4].x * x1 + e[5].x * x2;
-            a2 += e[6].x * x0 + e[7].x * x1 + e[8].x * x2;
-            b0 += e[0].y * z0 + e[1].y * z1 + e[2].y * z2;
-            b1 += e[3].y * z0 + e[4].y * z1 + e[5].y * z2;
-            b2 += e[6].y * z0 + e[7].y * z1 + e[8].y * z2;
+        float wv[6];
+        sell16s_pair<kShort, true>(A, vals, x, pr, wv);
+        sell16s_update<MODE>(A.num_rows, pr, wv, x, res, dnext, y, c1, c2, vec2);
+    }
+}
+
+// ---- multi-step sweep: several Chebyshev steps per launch, the matrix re-read from L2 ------
+//
+// Step g of a preconditioner call reads the whole FP16 matrix (280 MB on the 160x80x80 mesh)
+// to apply it to d_(g-1).  A row of step g needs d_(g-1) only at its columns, which lie within
+// the row's tile +- `halo` tiles (tiles of kWaveRows consecutive rows; halo from the mesh's
+// numbering, 14 tiles of 512 rows on the bench mesh), so step g can start on a tile as soon as
+// step g-1 has finished that neighbourhood.  One launch runs `nsteps` consecutive steps as
+// tasks (step, tile) issued in the order of tile + lag * step (lag = halo + 1 + slack): step g
+// trails step g-1 by `lag` tiles, so the rows a step reads were read by the step before a few
+// tens of MB earlier and are still in the 126 MB L2 -- the matrix comes from HBM once per
+// launch instead of once per step.  Each CTA takes the next task from a ticket counter (only
+// running CTAs take tickets, and every task depends only on tasks issued before it, so the
+// launch cannot deadlock whatever the residency), waits until the completion stamps of its
+// dependencies -- step g-1 on tiles t-halo..t+halo -- carry this launch's epoch (acquire:
+// the SM's L1 holds no stale line of the direction vector after it), runs the same row-pair
+// arithmetic as k_sell16s, and stamps its own completion (release).  d_g alternates between
+// two buffers: step g overwrites d_(g-2) on tile t only after step g-1 finished every tile
+// that reads it.  Every wait is bounded: after kWavePolls polls the CTA raises `abort`, the
+// others stop taking tasks and stop waiting, the launch ends, and `fail` stays set for the
+// host.  The last CTA to leave resets the ticket counters for the next launch.
+constexpr int kWaveRows = 2 * kThreads;  // rows per tile: one row pair per thread
+constexpr int kWaveMaxSteps = 16;        // steps per launch
+constexpr uint32_t kWavePolls = 1u << 21;
+
+struct WaveCtl {
+    uint32_t ticket;  // next task
+    uint32_t exits;   // CTAs that left the task loop
+    int32_t  abort;   // a wait ran out during this launch
+    int32_t  fail;    // sticky for the host: some launch aborted
+};
+
+struct WaveStep {
+    float c1[kWaveMaxSteps], c2[kWaveMaxSteps];
+    int32_t first;     // global step number of local step 0 (d_(first-1) is the launch's input)
+    int32_t nsteps;    // steps in this launch
+    int32_t nupdate;   // local steps < nupdate are Chebyshev steps, the rest residual-only (MODE 1)
+};
+
+__device__ __forceinline__ int32_t ld_acquire_s32(const int32_t* p) {
+    int32_t v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_s32(int32_t* p, int32_t v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <bool kShort>
+__global__ void __launch_bounds__(kThreads, 4)
+k_sell16s_wave(SellView A, const __half* __restrict__ vals, float* __restrict__ res, float* d_even, float* d_odd,
+               float* __restrict__ y, WaveStep st, const int32_t* __restrict__ order, int32_t ntasks, int32_t ntiles,
+               int32_t halo, int32_t epoch, int32_t wait_epoch, int32_t* flags, WaveCtl* ctl,
+               const PcgScalars* S) {
+    if (S && S->done) return;
+    __shared__ uint32_t sh_task, sh_next;
+    const int64_t npairs = (((int64_t)A.num_rows + 31) & ~int64_t(31)) >> 1;
+    const uintptr_t vbits = reinterpret_cast<uintptr_t>(res) | reinterpret_cast<uintptr_t>(d_even) |
+                            reinterpret_cast<uintptr_t>(d_odd) | reinterpret_cast<uintptr_t>(y);
+    const bool vec2 = (vbits & 7) == 0;
+    if (threadIdx.x == 0) sh_next = atomicAdd(&ctl->ticket, 1u);
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sh_task = sh_next;  // take the next ticket now, so its latency hides behind this task
+            const bool stop = sh_task >= uint32_t(ntasks) || *reinterpret_cast<volatile int32_t*>(&ctl->abort);
+            sh_next = stop ? uint32_t(ntasks) : atomicAdd(&ctl->ticket, 1u);
+            if (stop) sh_task = uint32_t(ntasks);
         }
-        const int64_t r0 = 32 * sl + 2 * m;
-        const float wv[6] = {a0, a1, a2, b0, b1, b2};
-        // both rows of the pair: their 6 entries start at 3 r0 = 6 (16 sl + m), 8-byte aligned
-        // when the vectors are, so the update runs on float2 (half the memory instructions)
-        if (MODE != 2 && vec2 && r0 + 1 < A.num_rows) {
-            float2* rp = reinterpret_cast<float2*>(res + 3 * r0);
-#pragma unroll
-            for (int u = 0; u < 3; ++u) {
-                const float2 rr = rp[u];
-                const float rs0 = rr.x - wv[2 * u], rs1 = rr.y - wv[2 * u + 1];
-                rp[u] = make_float2(rs0, rs1);
-                if (MODE == 0) {
-                    const float2 xx = reinterpret_cast<const float2*>(x + 3 * r0)[u];
-                    float2* yp = reinterpret_cast<float2*>(y + 3 * r0) + u;
-                    const float2 yy = *yp;
-                    const float d0 = c1 * xx.x + c2 * rs0, d1 = c1 * xx.y + c2 * rs1;
-                    reinterpret_cast<float2*>(dnext + 3 * r0)[u] = make_float2(d0, d1);
-                    *yp = make_float2(yy.x + d0, yy.y + d1);
+        __syncthreads();
+        const uint32_t task = sh_task;
+        if (task >= uint32_t(ntasks)) break;
+        const int32_t code = __ldg(order + task);
+        const int j = code >> 24, t = code & 0xFFFFFF;  // local step, tile
+        if (j > 0) {
+            // step j-1 finished on tiles t-halo .. t+halo (a thread per tile)
+            int ok = 1;
+            for (int q = max(0, t - halo) + int(threadIdx.x); ok && q <= min(ntiles - 1, t + halo);
+                 q += blockDim.x) {
+                const int32_t* f = flags + (int64_t)(j - 1) * ntiles + q;
+                uint32_t polls = 0;
+                while (ld_acquire_s32(f) < wait_epoch) {
+                    if (++polls > kWavePolls || *reinterpret_cast<volatile int32_t*>(&ctl->abort)) {
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(128);
                 }
             }
-            continue;
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (r0 + h >= A.num_rows) break;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const int64_t k = 3 * (r0 + h) + i;
-                const float wi = wv[3 * h + i];
-                if (MODE == 0) {
-                    const float rs = res[k] - wi;
-                    res[k] = rs;
-                    const float dn = c1 * x[k] + c2 * rs;
-                    dnext[k] = dn;
-                    y[k] += dn;
-                } else if (MODE == 1) {
-                    res[k] -= wi;
-                } else {
-                    y[k] = wi;
-                }
+            if (!__syncthreads_and(ok)) {
+                if (threadIdx.x == 0) atomicExch(&ctl->abort, 1);
+                break;
             }
+        }
+        const int g = st.first + j;  // global step: reads d_(g-1), writes d_g
+        const float* x = ((g - 1) & 1) ? d_odd : d_even;
+        float* dn = (g & 1) ? d_odd : d_even;
+        const int64_t pr = (int64_t)t * kThreads + threadIdx.x;
+        if (pr < npairs) {
+            float wv[6];
+            if (kShort) sell16s_pair<true, false>(A, vals, x, pr, wv);
+            else sell16s_pair<false, false>(A, vals, x, pr, wv);
+            if (j < st.nupdate)
+                sell16s_update<0>(A.num_rows, pr, wv, x, res, dn, y, st.c1[j], st.c2[j], vec2);
+            else
+                sell16s_update<1>(A.num_rows, pr, wv, x, res, nullptr, nullptr, 0.f, 0.f, vec2);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_s32(flags + (int64_t)j * ntiles + t, epoch);
         }
     }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl->exits, 1u) == gridDim.x - 1) {
+            if (ctl->abort) ctl->fail = 1;
+            ctl->abort = 0;
+            ctl->ticket = 0u;
+            ctl->exits = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// Largest distance in tiles between a row and one of its columns (padding lanes excluded).
+__global__ void k_wave_halo(SellView A, int32_t* __restrict__ out) {
+    int32_t m = 0;
+    const int32_t nslices = (A.num_rows + 31) >> 5;
+    for (int64_t sl = blockIdx.x; sl < nslices; sl += gridDim.x) {
+        const int64_t base = A.ptr[sl];
+        const int w = A.width[sl];
+        for (int e = threadIdx.x; e < 32 * w; e += blockDim.x) {
+            const int32_t r = int32_t(32 * sl + (e & 31));
+            if (r >= A.num_rows) continue;
+            const int32_t c = A.cols[base + e];
+            const int32_t d = abs(c / kWaveRows - r / kWaveRows);
+            m = max(m, d);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 // Chebyshev step after a matrix-free apply (w holds P A P d_cur; constrained rows are identity).
@@ -586,9 +750,21 @@ static int estimate_lambda_max(plato_problem* h, int kind, int steps, double* lm
     return PLATO_OK;
 }
 
-// Chebyshev coefficients for `degree` steps on [lmax/ratio, lmax].
-static ChebCoef chebyshev(double lmax, double ratio, int degree) {
+// Chebyshev coefficients for `degree` steps on [lmax/ratio, lmax] (first kind), or -- kind
+// 4 -- the fourth-kind polynomial on (0, lmax] (Lottes, "Optimal polynomial smoothers for
+// multigrid V-cycles", Numer. Linear Algebra Appl. 2023): d_0 = 4/(3 lmax) Dinv r,
+// d_k = (2k-1)/(2k+3) d_(k-1) + (8k+4)/((2k+3) lmax) Dinv r_k, whose error polynomial E
+// satisfies max sqrt(lambda/lmax) |E(lambda)| = 1/(2 degree + 1) on (0, lmax].
+static ChebCoef chebyshev(double lmax, double ratio, int degree, int kind) {
     ChebCoef c{};
+    if (kind == 4) {
+        c.c0 = float(4.0 / (3.0 * lmax));
+        for (int k = 1; k < degree && k < 64; ++k) {
+            c.c1[k] = float((2.0 * k - 1.0) / (2.0 * k + 3.0));
+            c.c2[k] = float((8.0 * k + 4.0) / ((2.0 * k + 3.0) * lmax));
+        }
+        return c;
+    }
     const double lmin = lmax / ratio;
     const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
     double rho = 1.0 / sigma;
@@ -661,6 +837,104 @@ int prepare_coarse(plato_problem* h, const double* z) {
     return PLATO_OK;
 }
 
+// Multi-step sweep set-up (once per handle and launch length): the column reach in tiles, the
+// stamp and counter arrays, and the task order of an `nsteps`-step launch; *steps = the steps
+// per launch to use (0: one launch per step).  Measured on the 160x80x80 bench mesh (halo 13
+// tiles, 592 CTAs in flight): a step trails the one before by at least (592 / steps) tiles or
+// the tasks serialise on their waits (2 steps, slack 0: 223 us per step; 4 steps: 514 us);
+// with that slack the rows between the first and the last front approach half the matrix, so
+// little of the L2 reuse survives: 7 steps per launch, slack 130: 81 us per step against 88 us
+// with one launch per step, 41.8 against 42.4 ms per solve+adjoint.  The sweep is bound by
+// load latency rather than HBM bandwidth, so automatic mode (sweep_steps 0) keeps one launch
+// per step and the multi-step form is an option.
+constexpr int kWaveSlackCtas = 600;  // default slack: this many tasks between a task and its deps
+
+int wave_steps(plato_problem* h, int* steps, int* lag) {
+    *steps = 0;
+    if (h->opts.sweep_steps <= 1 || h->wave_halo == -2 || !h->sell.dcols) return PLATO_OK;
+    const int32_t nslices = h->sell.nslices;
+    const int32_t tiles = int32_t((int64_t(nslices) * 16 + kThreads - 1) / kThreads);
+    if (h->wave_halo == -1 || h->wave_tiles != tiles) {
+        int32_t* d = nullptr;
+        PLATO_CUDA(h, cudaMallocAsync(&d, sizeof(int32_t), h->stream));
+        PLATO_CUDA(h, cudaMemsetAsync(d, 0, sizeof(int32_t), h->stream));
+        k_wave_halo<<<grid_for(nslices, 1, 148 * 8), 256, 0, h->stream>>>(sell_view(h), d);
+        PLATO_LAUNCH_CHECK(h);
+        int32_t halo = 0;
+        PLATO_CUDA(h, cudaMemcpyAsync(&halo, d, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        PLATO_CUDA(h, cudaFreeAsync(d, h->stream));
+        PLATO_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (h->wave_flags) PLATO_CUDA(h, cudaFree(h->wave_flags));
+        h->wave_flags = nullptr;
+        for (int k = 0; k <= kWaveMaxSteps; ++k) {
+            if (h->wave_order[k]) PLATO_CUDA(h, cudaFree(h->wave_order[k]));
+            h->wave_order[k] = nullptr;
+        }
+        PLATO_CUDA(h, cudaMalloc(&h->wave_flags, sizeof(int32_t) * kWaveMaxSteps * size_t(tiles)));
+        PLATO_CUDA(h, cudaMemset(h->wave_flags, 0, sizeof(int32_t) * kWaveMaxSteps * size_t(tiles)));
+        if (!h->wave_ctl) {
+            PLATO_CUDA(h, cudaMalloc(&h->wave_ctl, sizeof(WaveCtl)));
+            PLATO_CUDA(h, cudaMemset(h->wave_ctl, 0, sizeof(WaveCtl)));
+        }
+        h->wave_epoch = 0;
+        h->wave_tiles = tiles;
+        h->wave_halo = halo;
+    }
+    const int S = h->opts.sweep_steps;
+    *lag = h->wave_halo + 1 + (h->opts.sweep_lag > 0 ? h->opts.sweep_lag : (kWaveSlackCtas + S - 1) / S);
+    if (h->wave_tiles < 2 * (h->wave_halo + 1)) return PLATO_OK;  // too few tiles to pipeline
+    *steps = S;
+    return PLATO_OK;
+}
+
+int wave_order(plato_problem* h, int nsteps, int lag) {
+    if (h->wave_order[nsteps] && h->wave_order_lag[nsteps] == lag) return PLATO_OK;
+    const int32_t tiles = h->wave_tiles;
+    std::vector<std::pair<int64_t, int32_t>> key;
+    key.reserve(size_t(nsteps) * tiles);
+    for (int j = 0; j < nsteps; ++j)
+        for (int32_t t = 0; t < tiles; ++t)
+            key.push_back({(int64_t(t) + int64_t(lag) * j) * 64 + (63 - j), (j << 24) | t});
+    std::sort(key.begin(), key.end());
+    std::vector<int32_t> codes(key.size());
+    for (size_t i = 0; i < key.size(); ++i) codes[i] = key[i].second;
+    if (h->wave_order[nsteps]) PLATO_CUDA(h, cudaFree(h->wave_order[nsteps]));
+    h->wave_order[nsteps] = nullptr;
+    PLATO_CUDA(h, cudaMalloc(&h->wave_order[nsteps], sizeof(int32_t) * codes.size()));
+    PLATO_CUDA(h, cudaMemcpy(h->wave_order[nsteps], codes.data(), sizeof(int32_t) * codes.size(),
+                             cudaMemcpyHostToDevice));
+    h->wave_order_lag[nsteps] = lag;
+    return PLATO_OK;
+}
+
+// Global steps [first, first + nsteps) of a preconditioner call in one launch; steps below
+// `cheb_end` are Chebyshev steps (coefficients cc), the others residual-only.
+int wave_launch(plato_problem* h, const ChebCoef& cc, int first, int nsteps, int cheb_end, int lag, int grid) {
+    int rc = wave_order(h, nsteps, lag);
+    if (rc) return rc;
+    WaveStep st{};
+    st.first = first;
+    st.nsteps = nsteps;
+    st.nupdate = std::max(0, std::min(nsteps, cheb_end - first));
+    for (int j = 0; j < nsteps && first + j < 64; ++j) {
+        st.c1[j] = cc.c1[first + j];
+        st.c2[j] = cc.c2[first + j];
+    }
+    const int32_t ntasks = nsteps * h->wave_tiles;
+    const int32_t epoch = ++h->wave_epoch;
+    // test hook (plato_test_stall_next_sweep): the launch waits for a later epoch than its
+    // tasks stamp, so its first dependency wait runs out
+    const int32_t wait_epoch = h->wave_stall ? epoch + 1 : epoch;
+    h->wave_stall = 0;
+    k_sell16s_wave<true><<<std::min(grid, ntasks), kThreads, 0, h->stream>>>(
+        sell_view(h), static_cast<const __half*>(h->sell16s), h->f_res, h->f_d0, h->f_d1, h->f_y, st,
+        h->wave_order[nsteps], ntasks, h->wave_tiles, h->wave_halo, epoch, wait_epoch, h->wave_flags,
+        reinterpret_cast<WaveCtl*>(h->wave_ctl), h->scal);
+    PLATO_LAUNCH_CHECK(h);
+    h->launches += 1;
+    return PLATO_OK;
+}
+
 // Flexible CG with the Chebyshev preconditioner: A x = b, x holds the initial guess.
 int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* stats) {
     const int64_t n = 3 * (int64_t)h->N;
@@ -684,12 +958,26 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         PLATO_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sell16s<0, false>, kThreads, 0));
         CB = std::min(SB, std::max(1, per_sm) * std::max(1, sms));
     }
+    // multi-step sweep (FP16 scaled matrix, numbering with a short column reach)
+    int wave_S = 0, wave_lag = 0, wave_grid = 0;
+    if (kind == INNER_SELL16S) {
+        const int wrc = wave_steps(h, &wave_S, &wave_lag);
+        if (wrc) return wrc;
+        if (wave_S > 0) {
+            int sms = 0, per_sm = 0;
+            PLATO_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+            PLATO_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sell16s_wave<true>, kThreads, 0));
+            wave_grid = std::max(1, per_sm) * std::max(1, sms);
+        }
+    }
+    h->sweep_steps_used = wave_S > 0 ? wave_S : 1;
 
     double lmax = 0.0;
     int rc = estimate_lambda_max(h, kind, 20, &lmax);
     if (rc) return rc;
     const double safety = kind == INNER_SELL16 ? 1.15 : 1.10;
-    const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree);
+    const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree,
+                                   h->opts.chebyshev_kind);
     // The coarse set-up runs on its own stream meanwhile; the handle's stream waits for it only
     // at the first coarse solve (after the first residual and Chebyshev sweep), so the set-up
     // overlaps that work too.
@@ -731,9 +1019,36 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         return PLATO_OK;
     };
     float* dlast = h->f_d0;
+    int wave_first_len = 0;  // steps in the first launch of a multi-step sweep (timing)
     std::vector<int64_t> timed_iters;  // timing records of the current pass (see collect_timing)
     int64_t inner_record = -1;  // >= 0: time the first step of this sweep (record 2*iter+1)
+    // The multi-step sweep runs the Chebyshev steps 1 .. degree-1 and, with a coarse space, the
+    // residual step res -= A^ d_(degree-1) of the two-level form as step `degree`, in launches
+    // of at most wave_S steps of as even a length as possible.
+    auto wave_sweep = [&]() -> int {
+        const int total = (degree - 1) + (coarse ? 1 : 0);
+        const int launches_n = (total + wave_S - 1) / wave_S;
+        int first = 1;
+        for (int L = 0; L < launches_n; ++L) {
+            const int len = (total - (first - 1) + (launches_n - L) - 1) / (launches_n - L);
+            cudaEvent_t t0 = nullptr, t1 = nullptr;
+            if (L == 0 && inner_record >= 0) {
+                int r2 = timing_events(h, &t0, &t1);
+                if (r2) return r2;
+                timed_iters.push_back(inner_record);
+                PLATO_CUDA(h, cudaEventRecord(t0, s));
+            }
+            int r2 = wave_launch(h, cc, first, len, degree, wave_lag, wave_grid);
+            if (r2) return r2;
+            if (t1) PLATO_CUDA(h, cudaEventRecord(t1, s));
+            if (L == 0) wave_first_len = len;
+            first += len;
+        }
+        dlast = ((degree - 1) & 1) ? h->f_d1 : h->f_d0;
+        return PLATO_OK;
+    };
     auto chebyshev_steps = [&]() -> int {
+        if (wave_S > 0) return wave_sweep();
         float* dcur = h->f_d0;
         float* dnext = h->f_d1;
         for (int k = 1; k < degree; ++k) {
@@ -781,8 +1096,10 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     auto precondition = [&](float) -> int {
         int r2 = chebyshev_steps();
         if (r2 || !coarse) return r2;
-        r2 = inner_apply_sub(dlast);  // the sweep left res = r - A (s - d_last)
-        if (r2) return r2;
+        if (wave_S == 0) {
+            r2 = inner_apply_sub(dlast);  // the sweep left res = r - A (s - d_last)
+            if (r2) return r2;
+        }
         if (!coarse_waited) {
             r2 = coarse_wait(h);
             if (r2) return r2;
@@ -870,6 +1187,22 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         PLATO_CUDA(h, cudaStreamSynchronize(s));
         PcgScalars fin;
         PLATO_CUDA(h, cudaMemcpy(&fin, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
+        if (wave_S > 0) {
+            WaveCtl ctl{};
+            PLATO_CUDA(h, cudaMemcpy(&ctl, h->wave_ctl, sizeof(WaveCtl), cudaMemcpyDeviceToHost));
+            if (ctl.fail) {
+                // a dependency wait ran out: no further multi-step launches on this handle; the
+                // caller's fallback (plain FP64 Jacobi-PCG) redoes the solve
+                PLATO_CUDA(h, cudaMemset(h->wave_ctl, 0, sizeof(WaveCtl)));
+                h->wave_halo = -2;
+                h->ev_used = 0;
+                stats->converged = 0;
+                stats->status = PLATO_NOT_CONVERGED;
+                return plato_fail(h, PLATO_NOT_CONVERGED,
+                                  "multi-step sweep: a bounded wait for a neighbouring tile ran out");
+            }
+        }
+        h->inner_record_steps = wave_S > 0 ? wave_first_len : 1;
         rc = collect_timing(h, timed_iters, fin.iter - iter_base);
         if (rc) return rc;
         precond_applies += int64_t(fin.iter - iter_base + 1) * (degree - 1);
@@ -1253,7 +1586,8 @@ int fcg_batch(plato_problem* h, const double* b, double* x, plato_solve_stats* s
     int rc = estimate_lambda_max(h, kind, 20, &lmax);
     if (rc) return rc;
     const double safety = kind == INNER_SELL16 ? 1.15 : 1.10;
-    const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree);
+    const ChebCoef cc = chebyshev(lmax * safety, h->opts.chebyshev_ratio > 1.0 ? h->opts.chebyshev_ratio : 30.0, degree,
+                                   h->opts.chebyshev_kind);
 
     auto chebyshev_steps = [&]() -> int {
         float* dcur = h->f_d0;

@@ -269,6 +269,17 @@ struct plato_problem {
     float*  f_d1 = nullptr;
     float*  f_y = nullptr;         // preconditioner output
     float*  f_w = nullptr;         // inner operator output
+    // multi-step FP16 sweep (k_sell16s_wave in mixed.cu): completion stamps of (step, tile),
+    // ticket counters, and the task order for each launch length
+    int32_t* wave_flags = nullptr; // [16][wave_tiles] epoch of the last completion
+    int32_t* wave_ctl = nullptr;   // ticket, exits, abort, fail
+    int32_t* wave_order[17] = {};  // per steps-per-launch: task codes (step << 24 | tile)
+    int32_t  wave_order_lag[17] = {};
+    int32_t  wave_tiles = 0;
+    int32_t  wave_halo = -1;       // column reach in tiles (-1: not measured, -2: disabled)
+    int32_t  wave_epoch = 0;
+    int32_t  sweep_steps_used = 0; // steps per launch of the last flexible-CG solve's sweep
+    int32_t  wave_stall = 0;       // test hook: the next launch waits for a stamp nobody writes
     // instrumentation: kernel launches issued, and sampled CUDA-event timings of the
     // solver's operator apply (every kTimingStride-th apply, events on the handle's stream)
     int64_t launches = 0;
@@ -279,7 +290,8 @@ struct plato_problem {
     double  op_ms_total = 0.0;
     int64_t op_timed = 0;
     double  inner_ms_total = 0.0;  // preconditioner operator step (mixed-precision solver)
-    int64_t inner_timed = 0;
+    int64_t inner_timed = 0;       // steps timed
+    int32_t inner_record_steps = 1;  // steps in one timed preconditioner launch
     cudaEvent_t asm_ev[2] = {nullptr, nullptr};  // Jacobian assembly of the solve path
     double  asm_ms_total = 0.0;
     int64_t asm_timed = 0;

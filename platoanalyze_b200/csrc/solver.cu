@@ -265,7 +265,7 @@ int collect_timing(plato_problem* h, const std::vector<int64_t>& iters, int64_t 
         PLATO_CUDA(h, cudaEventElapsedTime(&ms, h->ev_pool[2 * k], h->ev_pool[2 * k + 1]));
         if (iters[k] & 1) {
             h->inner_ms_total += ms;
-            h->inner_timed += 1;
+            h->inner_timed += h->inner_record_steps;
         } else {
             h->op_ms_total += ms;
             h->op_timed += 1;

@@ -34,11 +34,15 @@ class SolverOptions:
     chebyshev_degree: int = 0
     coarse_cells: tuple = (0, 0, 0)
     fallback_max_iterations: int = 0  # plain FP64 Jacobi-PCG fallback cap (0: max_iterations, < 0: none)
+    chebyshev_kind: int = 1  # 1: first kind on [lmax/ratio, lmax]; 4: fourth kind on (0, lmax]
+    sweep_steps: int = 0  # FP16 sweep: Chebyshev steps per launch (0 or 1: one per launch)
+    sweep_lag: int = 0  # multi-step sweep: extra tiles between consecutive steps (0: 600 / steps)
 
     def to_c(self) -> capi.SolverOpts:
         return capi.SolverOpts(self.tolerance, self.max_iterations, self.operator_kind, self.precision,
                                int(self.self_adjoint), self.chebyshev_ratio, self.chebyshev_degree,
-                               (C.c_int32 * 3)(*self.coarse_cells), self.fallback_max_iterations)
+                               (C.c_int32 * 3)(*self.coarse_cells), self.fallback_max_iterations,
+                               self.chebyshev_kind, self.sweep_steps, self.sweep_lag)
 
 
 @dataclass
@@ -197,6 +201,13 @@ class EllipticProblem:
         slots, cb = C.c_int64(), C.c_int32()
         check(lib.plato_get_sell_info(self.h, C.byref(slots), C.byref(cb)), self.h)
         return {"total_slots": slots.value, "column_bytes": cb.value}
+
+    def sweep_info(self) -> dict:
+        """The FP16 sweep of the last flexible-CG solve: Chebyshev steps per launch (1: one
+        launch per step) and the column reach in tiles of 512 rows (-1: not measured)."""
+        steps, halo = C.c_int32(), C.c_int32()
+        check(lib.plato_get_sweep_info(self.h, C.byref(steps), C.byref(halo)), self.h)
+        return {"steps_per_launch": steps.value, "halo_tiles": halo.value}
 
     def reset_instrumentation(self) -> None:
         check(lib.plato_reset_instrumentation(self.h), self.h)

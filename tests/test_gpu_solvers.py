@@ -242,3 +242,58 @@ def test_fp16_sweep_column_offsets_and_their_fallback():
     assert rel_l2(ubh, uah) <= 1e-8, rel_l2(ubh, uah)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("cells", [(20, 10, 10), (40, 20, 20)])
+def test_multistep_sweep_matches_one_launch_per_step(cells):
+    """The multi-step FP16 sweep (several Chebyshev steps per launch, each step waiting only
+    for its neighbouring tiles of the step before) does the same arithmetic per row as one
+    launch per step: the same iterations and the same solution, for launch lengths that do and
+    do not divide the degree and for a one-tile lag."""
+    spec = cantilever(*cells, SolverOptions(tolerance=1e-10))
+    z = splitmix_uniform(spec.coords.shape[0], 0x5EED0003)
+    prob = EllipticProblem(spec)
+    orc = Oracle.from_spec(spec)
+    uo, _, _ = orc.solution_refined(z, tol=1e-13)
+    zd = prob.to_dev(z)
+    coarse = (cells[0] // 10, cells[1] // 10, cells[2] // 10)
+    results = {}
+    for steps, lag in ((1, 0), (2, 0), (3, 0), (4, 0), (7, 1), (16, 0), (0, 0), (5, 300)):
+        prob.set_solver(SolverOptions(tolerance=1e-10, precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=9,
+                                      chebyshev_ratio=100.0, coarse_cells=coarse, sweep_steps=steps,
+                                      sweep_lag=lag))
+        u, st = prob.solution(zd)
+        info = prob.sweep_info()
+        assert st["converged"] == 1 and st["fallback"] == 0, (steps, st)
+        assert info["steps_per_launch"] == max(1, steps)
+        assert rel_l2(host(u), uo) <= 1e-8
+        results[(steps, lag)] = (st["iterations"], host(u))
+    it1, u1 = results[(1, 0)]
+    for key, (it, u) in results.items():
+        assert it == it1, (key, it, it1)
+        assert rel_l2(u, u1) <= 1e-14, key
+    prob.close()
+
+
+def test_multistep_sweep_wait_runs_out_and_falls_back(setup):
+    """A multi-step sweep launch whose dependency wait can never be met (the test hook makes it
+    wait for a stamp no task writes) gives up after its bounded wait, the host reads the
+    timeout, the solve is finished by the plain FP64 fallback with the oracle's answer, later
+    solves on the handle run one launch per step, and the device stays usable."""
+    from platoanalyze_b200.problem import lib
+
+    spec, z, _, orc, uo, _ = setup
+    prob = EllipticProblem(spec)
+    zd = prob.to_dev(z)
+    prob.set_solver(SolverOptions(tolerance=1e-10, precision=capi.PRECISION_MIXED_FP16, chebyshev_degree=8,
+                                  coarse_cells=(10, 5, 5), sweep_steps=4))
+    u, st = prob.solution(zd)
+    assert st["converged"] == 1 and st["fallback"] == 0 and prob.sweep_info()["steps_per_launch"] == 4
+    assert lib.plato_test_stall_next_sweep(prob.h) == 0
+    u, st = prob.solution(zd)
+    assert st["converged"] == 1 and st["fallback"] == 2, st
+    assert rel_l2(host(u), uo) <= 1e-8
+    u, st = prob.solution(zd)
+    assert st["converged"] == 1 and st["fallback"] == 0 and prob.sweep_info()["steps_per_launch"] == 1
+    assert rel_l2(host(u), uo) <= 1e-8
+    prob.close()

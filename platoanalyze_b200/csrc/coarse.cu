@@ -759,6 +759,8 @@ k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
                  const uint8_t* __restrict__ mask, const float* __restrict__ v, const float* __restrict__ vscale,
                  double* __restrict__ part, const PcgScalars* S) {
     __shared__ double sh[kThreadsPerCta / 32][24];
+    pdl_wait();
+    pdl_trigger();
     if (S && S->done) return;
     const int cell = blockIdx.x / split, piece = blockIdx.x - cell * split;
     const int cz = cell % cv.nc2, cy = (cell / cv.nc2) % cv.nc1, cx = cell / (cv.nc1 * cv.nc2);
@@ -804,6 +806,8 @@ k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
 // and over their splits, in a fixed order.
 __global__ void k_restrict_sum(CoarseView cv, int split, const double* __restrict__ part, double* __restrict__ rc,
                                const PcgScalars* S) {
+    pdl_wait();
+    pdl_trigger();
     if (S && S->done) return;
     const int ncn = (cv.nc0 + 1) * (cv.nc1 + 1) * (cv.nc2 + 1);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * ncn; t += gridDim.x * blockDim.x) {
@@ -829,6 +833,8 @@ template <bool LOWER>
 __global__ void __launch_bounds__(256) k_coarse_trmv(int n, int ld, const float* __restrict__ M,
                                                      const double* __restrict__ in, double* __restrict__ out,
                                                      const PcgScalars* S) {
+    pdl_wait();
+    pdl_trigger();
     if (S && S->done) return;
     const int lane = threadIdx.x & 31;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
@@ -880,6 +886,8 @@ __global__ void k_coarse_pack(int n, int ld, const double* __restrict__ X, float
 __global__ void k_prolong(int32_t N, CoarseView cv, const double* __restrict__ coords, const uint8_t* __restrict__ mask,
                           const double* __restrict__ yc, const float* __restrict__ yscale, float* __restrict__ y,
                           int accumulate, const PcgScalars* S) {
+    pdl_wait();
+    pdl_trigger();
     if (S && S->done) return;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
         const double x = coords[3 * p], yy = coords[3 * p + 1], zz = coords[3 * p + 2];
@@ -1211,13 +1219,19 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
     CoarseSpace& c = h->coarse;
     cudaStream_t s = h->stream;
     const CoarseView cv = coarse_view(h);
-    k_restrict_cells<<<c.ncells * c.rsplit, kThreadsPerCta, 0, s>>>(cv, c.rsplit, c.node_ptr, c.node_list, h->coords,
-                                                                      h->bc_mask, v, sq, c.rpart, S);
-    k_restrict_sum<<<grid_for(c.ndof, 256), 256, 0, s>>>(cv, c.rsplit, c.rpart, c.rc, S);
+    // programmatic dependent launches (see launch_pdl): each kernel waits for its predecessor
+    PLATO_CUDA(h, launch_pdl(k_restrict_cells, c.ncells * c.rsplit, kThreadsPerCta, s, cv, c.rsplit,
+                             (const int32_t*)c.node_ptr, (const int32_t*)c.node_list, (const double*)h->coords,
+                             (const uint8_t*)h->bc_mask, v, sq, c.rpart, S));
+    PLATO_CUDA(h, launch_pdl(k_restrict_sum, grid_for(c.ndof, 256), 256, s, cv, c.rsplit, (const double*)c.rpart,
+                             c.rc, S));
     const int GB = grid_for(int64_t(c.ndof) * 32, 256, 148 * 8);
-    k_coarse_trmv<true><<<GB, 256, 0, s>>>(c.ndof, c.ldf, c.Xf, c.rc, c.tc, S);
-    k_coarse_trmv<false><<<GB, 256, 0, s>>>(c.ndof, c.ldf, c.Uf, c.tc, c.yc, S);
-    k_prolong<<<grid_for(h->N, 256), 256, 0, s>>>(h->N, cv, h->coords, h->bc_mask, c.yc, sq, y, accumulate, S);
+    PLATO_CUDA(h, launch_pdl(k_coarse_trmv<true>, GB, 256, s, c.ndof, c.ldf, (const float*)c.Xf, (const double*)c.rc,
+                             c.tc, S));
+    PLATO_CUDA(h, launch_pdl(k_coarse_trmv<false>, GB, 256, s, c.ndof, c.ldf, (const float*)c.Uf, (const double*)c.tc,
+                             c.yc, S));
+    PLATO_CUDA(h, launch_pdl(k_prolong, grid_for(h->N, 256), 256, s, h->N, cv, (const double*)h->coords,
+                             (const uint8_t*)h->bc_mask, (const double*)c.yc, sq, y, accumulate, S));
     h->launches += 4;
     PLATO_LAUNCH_CHECK(h);
     return PLATO_OK;

@@ -77,6 +77,8 @@ k_fcg_sell_apply(SellView A, const double* __restrict__ vals, const double* __re
                  PcgScalars* S, double* partials) {
     __shared__ double sh[1][32];
     __shared__ bool last;
+    pdl_wait();
+    pdl_trigger();
     if (S->done) return;
     double dot = 0.0;
     const int64_t padded = ((int64_t)A.num_rows + 31) & ~int64_t(31);
@@ -135,6 +137,8 @@ k_fcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r, const do
              double* partials, int32_t max_it) {
     __shared__ double sh[1][32];
     __shared__ bool last;
+    pdl_wait();
+    pdl_trigger();
     if (S->done) return;
     const double alpha = S->alpha;
     double v[1] = {0.0};
@@ -303,6 +307,8 @@ template <int MODE, bool kShort>
 __global__ void __launch_bounds__(kThreads, 4)
 k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__ x, float* __restrict__ res,
           float* __restrict__ dnext, float* __restrict__ y, float c1, float c2, const PcgScalars* S) {
+    pdl_wait();
+    pdl_trigger();
     if (S && S->done) return;
     const int64_t npairs = (((int64_t)A.num_rows + 31) & ~int64_t(31)) >> 1;
     const uintptr_t vbits = reinterpret_cast<uintptr_t>(res) |
@@ -519,6 +525,8 @@ k_fcg_zq(int64_t n, const float* __restrict__ y, const float* __restrict__ z_sca
          const double* __restrict__ q, PcgScalars* S, double* partials, int first) {
     __shared__ double sh[1][32];
     __shared__ bool last;
+    pdl_wait();
+    pdl_trigger();
     if (S->done) return;
     if (first) {  // initial direction: only widen z = y
         for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -549,6 +557,8 @@ k_fcg_direction(int64_t n, const double* __restrict__ z, double* __restrict__ p,
                 PcgScalars* S, double* partials, int first) {
     __shared__ double sh[1][32];
     __shared__ bool last;
+    pdl_wait();
+    pdl_trigger();
     if (S->done) return;
     const double beta = first ? 0.0 : S->beta;
     double v[1] = {0.0};
@@ -1003,11 +1013,11 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             k_res_sub_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, xin, h->f_w, h->f_res, h->scal);
         } else if (kind == INNER_SELL16S) {
             if (V.dcols)
-                k_sell16s<1, true><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), xin, h->f_res,
-                                                           nullptr, nullptr, 0.f, 0.f, h->scal);
+                PLATO_CUDA(h, launch_pdl(k_sell16s<1, true>, CB, kThreads, s, V, static_cast<const __half*>(h->sell16s),
+                                         xin, h->f_res, nullptr, nullptr, 0.f, 0.f, (const PcgScalars*)h->scal));
             else
-                k_sell16s<1, false><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), xin, h->f_res,
-                                                            nullptr, nullptr, 0.f, 0.f, h->scal);
+                PLATO_CUDA(h, launch_pdl(k_sell16s<1, false>, CB, kThreads, s, V, static_cast<const __half*>(h->sell16s),
+                                         xin, h->f_res, nullptr, nullptr, 0.f, 0.f, (const PcgScalars*)h->scal));
         } else if (kind == INNER_SELL16) {
             k_res_sub_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, xin, h->f_res, h->scal);
         } else if (kind == INNER_SELL32) {
@@ -1066,11 +1076,13 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                                                    cc.c1[k], cc.c2[k], h->scal);
             } else if (kind == INNER_SELL16S) {
                 if (V.dcols)
-                    k_sell16s<0, true><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), dcur,
-                                                               h->f_res, dnext, h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                    PLATO_CUDA(h, launch_pdl(k_sell16s<0, true>, CB, kThreads, s, V,
+                                             static_cast<const __half*>(h->sell16s), (const float*)dcur, h->f_res, dnext,
+                                             h->f_y, cc.c1[k], cc.c2[k], (const PcgScalars*)h->scal));
                 else
-                    k_sell16s<0, false><<<CB, kThreads, 0, s>>>(V, static_cast<const __half*>(h->sell16s), dcur,
-                                                                h->f_res, dnext, h->f_y, cc.c1[k], cc.c2[k], h->scal);
+                    PLATO_CUDA(h, launch_pdl(k_sell16s<0, false>, CB, kThreads, s, V,
+                                             static_cast<const __half*>(h->sell16s), (const float*)dcur, h->f_res, dnext,
+                                             h->f_y, cc.c1[k], cc.c2[k], (const PcgScalars*)h->scal));
             } else if (kind == INNER_SELL16) {
                 k_cheb_sell<INNER_SELL16><<<SB, kThreads, 0, s>>>(V, h->sell16, h->f_dinv, h->f_res, dcur, dnext,
                                                                   h->f_y, cc.c1[k], cc.c2[k], h->scal);
@@ -1156,18 +1168,22 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                     if (rc) return rc;
                     k_fcg_mask_dot<<<VB, kThreads, 0, s>>>(n, h->bc_mask, h->v_p, h->v_q, h->scal, h->partials);
                 } else {
-                    k_fcg_sell_apply<<<SB, kThreads, 0, s>>>(V, h->sell64, h->v_p, h->v_q, h->scal, h->partials);
+                    PLATO_CUDA(h, launch_pdl(k_fcg_sell_apply, SB, kThreads, s, V, (const double*)h->sell64,
+                                             (const double*)h->v_p, h->v_q, h->scal, h->partials));
                 }
                 if (timed) PLATO_CUDA(h, cudaEventRecord(e1, s));
-                k_fcg_update<<<VB, kThreads, 0, s>>>(n, x, h->v_r, h->v_p, h->v_q, h->f_dinv, res_scale, h->f_res, h->f_d0,
-                                                     h->f_y, cc.c0, h->scal, h->partials, max_it);
+                PLATO_CUDA(h, launch_pdl(k_fcg_update, VB, kThreads, s, n, x, h->v_r, (const double*)h->v_p,
+                                         (const double*)h->v_q, (const float*)h->f_dinv, res_scale, h->f_res, h->f_d0,
+                                         h->f_y, cc.c0, h->scal, h->partials, max_it));
                 h->launches += 2;
                 inner_record = timed ? 2 * enqueued + 1 : -1;
                 rc = precondition(cc.c0);
                 inner_record = -1;
                 if (rc) return rc;
-                k_fcg_zq<<<VB, kThreads, 0, s>>>(n, h->f_y, res_scale, h->v_z, h->v_q, h->scal, h->partials, 0);
-                k_fcg_direction<<<VB, kThreads, 0, s>>>(n, h->v_z, h->v_p, h->v_r, h->scal, h->partials, 0);
+                PLATO_CUDA(h, launch_pdl(k_fcg_zq, VB, kThreads, s, n, (const float*)h->f_y, res_scale, h->v_z,
+                                         (const double*)h->v_q, h->scal, h->partials, 0));
+                PLATO_CUDA(h, launch_pdl(k_fcg_direction, VB, kThreads, s, n, (const double*)h->v_z, h->v_p,
+                                         (const double*)h->v_r, h->scal, h->partials, 0));
                 h->launches += 1;
                 PLATO_LAUNCH_CHECK(h);
                 rc = deflate_direction(h, h->v_p, h->v_r, 1);

@@ -393,6 +393,31 @@ inline int grid_for(int64_t n, int threads, int64_t max_blocks = 148 * 32) {
     return int(b);
 }
 
+// Programmatic dependent launch (sm_90 and later).  The Krylov loop's kernels are launched with
+// launch_pdl: each may be scheduled onto SMs that the kernel before it in the stream has left,
+// while that kernel's last CTAs still run, instead of after its completion has reached the
+// host-side launch queue.  Every such kernel starts with pdl_wait(), which returns once the
+// previous kernel has completed and its memory operations are visible, before it touches any
+// memory; pdl_trigger() then lets the next kernel be scheduled.  Launched without the
+// attribute, both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // ---------------------------------------------------------------------------------------
 // device element arithmetic
 

@@ -393,7 +393,18 @@ int plato_problem_solution_deflated(plato_problem* h, const double* z, const dou
  * FP32 parameters trained with Adam.  All array arguments are [device]; work is issued on the
  * network's stream; errors read through plato_unet_last_error(). */
 typedef struct plato_unet plato_unet;
+typedef enum plato_unet_conv_kernel {
+    PLATO_UNET_CONV_TCGEN05  = 0, /* default: tcgen05.mma from shared-memory descriptors, FP32
+                                     accumulator in tensor memory, 128 voxels x all output
+                                     channels per CTA, two cp.async-filled stages per tap     */
+    PLATO_UNET_CONV_MMA_SYNC = 1  /* warp-level mma.sync.m16n8k16 tiles, register accumulators */
+} plato_unet_conv_kernel;
 int plato_unet_create(const int32_t nodes[3], int32_t max_batch, plato_unet** out);
+/* the kernel family of the forward and data-gradient convolutions (plato_unet_conv_kernel) */
+int plato_unet_set_conv_kernel(plato_unet* net, int32_t kind);
+/* waits for the network's stream; PLATO_DEVICE_TIMEOUT when a tensor-core convolution's bounded
+ * wait for its MMAs ran out since the last check (its outputs were then not written) */
+int plato_unet_check(plato_unet* net);
 int plato_unet_destroy(plato_unet* net);
 int plato_unet_set_stream(plato_unet* net, void* cuda_stream);
 const char* plato_unet_last_error(void);

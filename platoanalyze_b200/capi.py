@@ -145,6 +145,8 @@ def _load() -> C.CDLL:
         "plato_unet_create": ([i32p, C.c_int32, C.POINTER(vp)], C.c_int),
         "plato_unet_destroy": ([vp], C.c_int),
         "plato_unet_set_stream": ([vp, vp], C.c_int),
+        "plato_unet_set_conv_kernel": ([vp, C.c_int32], C.c_int),
+        "plato_unet_check": ([vp], C.c_int),
         "plato_unet_last_error": ([], C.c_char_p),
         "plato_unet_num_params": ([vp, C.POINTER(C.c_int64)], C.c_int),
         "plato_unet_set_params": ([vp, vp], C.c_int),

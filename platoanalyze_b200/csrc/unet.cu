@@ -185,6 +185,253 @@ k_conv(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TV
         }
 }
 
+// ---- convolution on the 5th-generation tensor cores (tcgen05, TMEM accumulator) -----------
+// The same implicit GEMM as k_conv: a CTA of 4 warps owns 128 consecutive voxels (UMMA M = 128)
+// and every output channel (N = COUTP, a multiple of 16, at most 96 here); the FP32 accumulator
+// lives in tensor memory, 128 lanes x N columns.  K runs over taps x input channels: per tap
+// all threads gather the 128 voxels' shifted input rows (cp.async, 16 bytes = 8 channels, zero
+// fill past the last voxel) and the tap's weights [COUTP][CIN] into shared memory in the
+// canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk c
+// at c * LBO + (r / 8) * 128 + (r % 8) * 16), then one thread issues CIN / 16 tcgen05.mma
+// (kind::f16: BF16 A and B, FP32 accumulate) with shared-memory descriptors of both operands and
+// commits them to the stage's mbarrier.  Two stages: tap t + 1 is gathered while the tensor core
+// works on tap t; a stage is refilled only after the mbarrier shows its MMAs complete.  The
+// epilogue loads the accumulator with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31, the
+// rows of its 32 voxels), adds the bias, applies ReLU and stores.  Every mbarrier wait is
+// bounded: on a timeout the CTA stops issuing, waits (bounded) for what it issued, raises *err,
+// skips the stores and still frees its tensor memory.
+constexpr int kTcRows = 128;             // voxels per CTA (UMMA M)
+constexpr uint32_t kTcPolls = 1u << 22;  // bounded mbarrier polls (about half a second)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle; start, leading (K) and stride (M/N)
+// byte offsets in 16-byte units, descriptor version 1 (bits 46-47)
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B (bits
+// 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+template <int N>
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_f32() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// waits for the completion of the phase with the given parity; false when the poll bound ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t i = 0; i < kTcPolls; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+
+template <int COUTP>
+constexpr int tc_tmem_cols() {
+    return COUTP <= 32 ? 32 : (COUTP <= 64 ? 64 : (COUTP <= 128 ? 128 : 256));
+}
+
+template <int CIN, int COUTP>
+constexpr uint32_t tc_stage_bytes() {
+    return uint32_t(kTcRows) * CIN * 2 + uint32_t(COUTP) * CIN * 2;
+}
+
+// Dynamic shared memory per CTA: the two stages, raised so that no more CTAs fit on an SM than
+// its 512 TMEM columns hold (an allocation beyond them would wait for another CTA's release).
+template <int CIN, int COUTP>
+constexpr uint32_t tc_smem_bytes() {
+    constexpr uint32_t stages = 2 * tc_stage_bytes<CIN, COUTP>();
+    constexpr uint32_t per_cta = (227u * 1024u) / (512u / tc_tmem_cols<COUTP>()) + 1024u;
+    return stages > per_cta ? stages : per_cta;
+}
+
+template <int CIN, int COUT, int TAPS, bool RELU, bool OUT_F32, bool ACCUM>
+__global__ void __launch_bounds__(128)
+k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TView out, int64_t nvox,
+          int* __restrict__ err) {
+    constexpr int COUTP = (COUT + 15) / 16 * 16;
+    static_assert(CIN % 16 == 0 && COUTP <= 256, "UMMA shape");
+    constexpr int TMEM_COLS = tc_tmem_cols<COUTP>();
+    constexpr uint32_t A_BYTES = uint32_t(kTcRows) * CIN * 2;
+    constexpr uint32_t STAGE = tc_stage_bytes<CIN, COUTP>();
+    constexpr uint32_t LBO_A = (kTcRows / 8) * 128;  // bytes between the K-chunks of A
+    constexpr uint32_t LBO_B = (COUTP / 8) * 128;
+    constexpr uint32_t IDESC = umma_idesc_bf16_f32<COUTP>();
+    extern __shared__ __align__(128) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t bar[3];  // MMA completion of stage 0, of stage 1; all MMAs
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const int64_t v = int64_t(blockIdx.x) * kTcRows + tid;  // this thread's voxel row
+    const bool row_ok = v < nvox;
+    const bf16* __restrict__ ip = static_cast<const bf16*>(in.p);
+    const int64_t hrow = row_ok ? halo_index(in, v) : 0;
+    const int64_t sy = in.W + 2, sz = int64_t(in.H + 2) * (in.W + 2);
+    const uint32_t sbase = smem_u32(tc_smem);
+    bool ok = true;
+    int issued = 0;
+    for (int t = 0; t < TAPS; ++t) {
+        const int st = t & 1;
+        if (t >= 2) {  // the MMAs of tap t - 2 have finished reading this stage
+            bool w = true;
+            if (tid == 0) w = mbar_wait(&bar[st], uint32_t((t - 2) >> 1) & 1u);
+            ok = __syncthreads_and(w) != 0;
+            if (!ok) break;
+        }
+        const uint32_t a_s = sbase + uint32_t(st) * STAGE, b_s = a_s + A_BYTES;
+        int64_t o = 0;
+        if (TAPS == 27) o = (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1);
+        const bf16* src = row_ok ? ip + (hrow + o) * in.ld + in.c0 : ip;
+        const uint32_t arow = uint32_t(tid >> 3) * 128u + uint32_t(tid & 7) * 16u;
+#pragma unroll
+        for (int c8 = 0; c8 < CIN / 8; ++c8)
+            cp_async16(a_s + uint32_t(c8) * LBO_A + arow, row_ok ? src + 8 * c8 : ip, row_ok ? 16u : 0u);
+        const bf16* wt = Wt + int64_t(t) * COUTP * CIN;
+        for (int q = tid; q < COUTP * (CIN / 8); q += 128) {
+            const int n = q / (CIN / 8), c8 = q - n * (CIN / 8);
+            cp_async16(b_s + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u, wt + n * CIN + 8 * c8,
+                       16u);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int kc = 0; kc < CIN / 16; ++kc)
+                umma_bf16(tmem, umma_smem_desc(a_s + 2u * kc * LBO_A, LBO_A, 128u),
+                          umma_smem_desc(b_s + 2u * kc * LBO_B, LBO_B, 128u), IDESC, (t > 0 || kc > 0) ? 1u : 0u);
+            umma_commit(&bar[st]);
+        }
+        ++issued;
+    }
+    // all issued MMAs complete (bounded even after a timeout above)
+    bool fin = true;
+    if (tid == 0) {
+        if (issued > 0) umma_commit(&bar[2]);
+        fin = issued == 0 || mbar_wait(&bar[2], 0u);
+    }
+    const bool good = __syncthreads_and(ok && fin) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (good) {
+        const int64_t obase = row_ok ? halo_index(out, v) * out.ld + out.c0 : 0;
+#pragma unroll
+        for (int c0 = 0; c0 < COUTP; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + (uint32_t(32 * warp) << 16) + uint32_t(c0), r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (!row_ok) continue;
+            float y[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int c = c0 + j;
+                y[j] = __uint_as_float(r[j]);
+                if (bias && c < COUT) y[j] += bias[c];
+                if (RELU) y[j] = fmaxf(y[j], 0.f);
+            }
+            if (OUT_F32) {
+                float* op = static_cast<float*>(out.p) + obase + c0;
+                if (c0 + 16 <= COUT) {
+#pragma unroll
+                    for (int j = 0; j < 16; j += 4) {
+                        float4 w4 = make_float4(y[j], y[j + 1], y[j + 2], y[j + 3]);
+                        if (ACCUM) {
+                            const float4 o4 = *reinterpret_cast<const float4*>(op + j);
+                            w4.x += o4.x; w4.y += o4.y; w4.z += o4.z; w4.w += o4.w;
+                        }
+                        *reinterpret_cast<float4*>(op + j) = w4;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (c0 + j < COUT) op[j] = ACCUM ? op[j] + y[j] : y[j];
+                }
+            } else {
+                bf16* op = static_cast<bf16*>(out.p) + obase + c0;
+                if (c0 + 16 <= COUT) {
+                    uint4 lo, hi;
+                    lo.x = pack_bf16(y[0], y[1]); lo.y = pack_bf16(y[2], y[3]);
+                    lo.z = pack_bf16(y[4], y[5]); lo.w = pack_bf16(y[6], y[7]);
+                    hi.x = pack_bf16(y[8], y[9]); hi.y = pack_bf16(y[10], y[11]);
+                    hi.z = pack_bf16(y[12], y[13]); hi.w = pack_bf16(y[14], y[15]);
+                    reinterpret_cast<uint4*>(op)[0] = lo;
+                    reinterpret_cast<uint4*>(op)[1] = hi;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (c0 + j < COUT) op[j] = __float2bfloat16_rn(y[j]);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
 // ---- weight gradient --------------------------------------------------------------------
 // dW[t][co][ci] += sum_v dy[v][co] x[v + o_t][ci]; grid (voxel chunks, TAPS).
 constexpr int kWgVox = 64;    // voxels per shared-memory tile
@@ -583,6 +830,8 @@ struct plato_unet {
     float* out = nullptr;
     float *dx0a = nullptr, *dcat0 = nullptr, *dp1 = nullptr, *dx1a = nullptr, *dcat1 = nullptr, *dp2 = nullptr,
           *dx2a = nullptr, *dx2b = nullptr, *dx1c = nullptr, *dx1d = nullptr, *dx0c = nullptr, *dx0d = nullptr;
+    int conv_kind = PLATO_UNET_CONV_TCGEN05;
+    int* conv_err = nullptr;     // raised by a tcgen05 convolution whose bounded wait ran out
     bf16* mbuf = nullptr;        // masked output gradient (BF16), also the head's gradient
     double* loss_d = nullptr;
     std::vector<void*> allocs;
@@ -602,36 +851,53 @@ int alloc(plato_unet* u, T** p, int64_t count) {
     return PLATO_OK;
 }
 
+// The convolution kernel family of a network: tcgen05 (default) or the warp-level mma.sync form.
+struct ConvPath {
+    int kind;  // PLATO_UNET_CONV_TCGEN05 or PLATO_UNET_CONV_MMA_SYNC
+    int* err;  // device flag raised by a tcgen05 CTA whose bounded wait ran out
+};
+
 // launch helpers (dispatch on the layer's channel counts)
 template <int CIN, int COUT, int TAPS, bool RELU, bool F32, bool ACC>
-int conv_launch(cudaStream_t s, TView in, const bf16* w, const float* b, TView out, int64_t nvox) {
+int conv_launch(cudaStream_t s, const ConvPath& P, TView in, const bf16* w, const float* b, TView out, int64_t nvox) {
+    if (P.kind == PLATO_UNET_CONV_TCGEN05) {
+        constexpr int COUTP = (COUT + 15) / 16 * 16;
+        constexpr uint32_t smem = tc_smem_bytes<CIN, COUTP>();
+        auto kernel = k_conv_tc<CIN, COUT, TAPS, RELU, F32, ACC>;
+        UCUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        kernel<<<int((nvox + kTcRows - 1) / kTcRows), 128, smem, s>>>(in, w, b, out, nvox, P.err);
+        ULAUNCH();
+        return PLATO_OK;
+    }
     const int64_t per = kConvWarps * 16 * kMT;
     k_conv<CIN, COUT, TAPS, RELU, F32, ACC><<<int((nvox + per - 1) / per), kConvWarps * 32, 0, s>>>(in, w, b, out, nvox);
     ULAUNCH();
     return PLATO_OK;
 }
 
-int conv_forward(cudaStream_t s, const Layer& L, TView in, TView out, const float* bias, int64_t nvox) {
+int conv_forward(cudaStream_t s, const ConvPath& P, const Layer& L, TView in, TView out, const float* bias,
+                 int64_t nvox) {
     const int c = L.cin, o = L.cout;
-    if (L.taps == 1) return conv_launch<16, 9, 1, false, true, false>(s, in, L.wf, bias, out, nvox);
+    if (L.taps == 1) return conv_launch<16, 9, 1, false, true, false>(s, P, in, L.wf, bias, out, nvox);
 #define FWD(CI, CO) \
-    if (c == CI && o == CO) return conv_launch<CI, CO, 27, true, false, false>(s, in, L.wf, bias, out, nvox);
+    if (c == CI && o == CO) return conv_launch<CI, CO, 27, true, false, false>(s, P, in, L.wf, bias, out, nvox);
     FWD(16, 16) FWD(16, 32) FWD(32, 32) FWD(32, 64) FWD(64, 64) FWD(96, 32) FWD(48, 16)
 #undef FWD
     return fail(PLATO_NOT_SUPPORTED, "no forward convolution for these channel counts");
 }
 
 // data gradient into an FP32 tensor (write, or accumulate)
-int conv_data_grad(cudaStream_t s, const Layer& L, TView dy, TView dx, int64_t nvox, bool accumulate) {
+int conv_data_grad(cudaStream_t s, const ConvPath& P, const Layer& L, TView dy, TView dx, int64_t nvox,
+                   bool accumulate) {
     const int c = L.cout, o = L.cin;  // roles swap
     if (L.taps == 1) {
-        if (accumulate) return conv_launch<16, 16, 1, false, true, true>(s, dy, L.wb, nullptr, dx, nvox);
-        return conv_launch<16, 16, 1, false, true, false>(s, dy, L.wb, nullptr, dx, nvox);
+        if (accumulate) return conv_launch<16, 16, 1, false, true, true>(s, P, dy, L.wb, nullptr, dx, nvox);
+        return conv_launch<16, 16, 1, false, true, false>(s, P, dy, L.wb, nullptr, dx, nvox);
     }
-#define BWD(CI, CO)                                                                                       \
-    if (c == CI && o == CO) {                                                                             \
-        if (accumulate) return conv_launch<CI, CO, 27, false, true, true>(s, dy, L.wb, nullptr, dx, nvox); \
-        return conv_launch<CI, CO, 27, false, true, false>(s, dy, L.wb, nullptr, dx, nvox);               \
+#define BWD(CI, CO)                                                                                          \
+    if (c == CI && o == CO) {                                                                                \
+        if (accumulate) return conv_launch<CI, CO, 27, false, true, true>(s, P, dy, L.wb, nullptr, dx, nvox); \
+        return conv_launch<CI, CO, 27, false, true, false>(s, P, dy, L.wb, nullptr, dx, nvox);               \
     }
     BWD(16, 16) BWD(32, 16) BWD(32, 32) BWD(64, 32) BWD(64, 64) BWD(32, 96) BWD(16, 48)
 #undef BWD
@@ -682,29 +948,30 @@ int forward(plato_unet* u, int B, const float* input) {
     const int64_t n0 = int64_t(B) * G0[0] * G0[1] * G0[2], n1 = int64_t(B) * G1[0] * G1[1] * G1[2],
                   n2 = int64_t(B) * G2[0] * G2[1] * G2[2];
     const std::vector<Layer>& L = u->layers;
+    const ConvPath P{u->conv_kind, u->conv_err};
     auto bias = [&](int k) { return u->params + L[k].b_off; };
     const int64_t nn = int64_t(B) * u->n[0] * u->n[1] * u->n[2];
     k_pack_input<<<blocks_for(nn * 8, 256), 256, 0, s>>>(input, u->n[0], u->n[1], u->n[2], tv(u->in, 16, 0, B, G0));
     ULAUNCH();
-    URC(conv_forward(s, L[0], tv(u->in, 16, 0, B, G0), tv(u->x0a, 16, 0, B, G0), bias(0), n0));
-    URC(conv_forward(s, L[1], tv(u->x0a, 16, 0, B, G0), tv(u->cat0, 48, 32, B, G0), bias(1), n0));
+    URC(conv_forward(s, P, L[0], tv(u->in, 16, 0, B, G0), tv(u->x0a, 16, 0, B, G0), bias(0), n0));
+    URC(conv_forward(s, P, L[1], tv(u->x0a, 16, 0, B, G0), tv(u->cat0, 48, 32, B, G0), bias(1), n0));
     k_pool<<<blocks_for(n1 * 16, 256), 256, 0, s>>>(tv(u->cat0, 48, 32, B, G0), tv(u->p1, 16, 0, B, G1), 16);
     ULAUNCH();
-    URC(conv_forward(s, L[2], tv(u->p1, 16, 0, B, G1), tv(u->x1a, 32, 0, B, G1), bias(2), n1));
-    URC(conv_forward(s, L[3], tv(u->x1a, 32, 0, B, G1), tv(u->cat1, 96, 64, B, G1), bias(3), n1));
+    URC(conv_forward(s, P, L[2], tv(u->p1, 16, 0, B, G1), tv(u->x1a, 32, 0, B, G1), bias(2), n1));
+    URC(conv_forward(s, P, L[3], tv(u->x1a, 32, 0, B, G1), tv(u->cat1, 96, 64, B, G1), bias(3), n1));
     k_pool<<<blocks_for(n2 * 32, 256), 256, 0, s>>>(tv(u->cat1, 96, 64, B, G1), tv(u->p2, 32, 0, B, G2), 32);
     ULAUNCH();
-    URC(conv_forward(s, L[4], tv(u->p2, 32, 0, B, G2), tv(u->x2a, 64, 0, B, G2), bias(4), n2));
-    URC(conv_forward(s, L[5], tv(u->x2a, 64, 0, B, G2), tv(u->x2b, 64, 0, B, G2), bias(5), n2));
+    URC(conv_forward(s, P, L[4], tv(u->p2, 32, 0, B, G2), tv(u->x2a, 64, 0, B, G2), bias(4), n2));
+    URC(conv_forward(s, P, L[5], tv(u->x2a, 64, 0, B, G2), tv(u->x2b, 64, 0, B, G2), bias(5), n2));
     k_upsample<<<blocks_for(n1 * 64, 256), 256, 0, s>>>(tv(u->x2b, 64, 0, B, G2), tv(u->cat1, 96, 0, B, G1), 64);
     ULAUNCH();
-    URC(conv_forward(s, L[6], tv(u->cat1, 96, 0, B, G1), tv(u->x1c, 32, 0, B, G1), bias(6), n1));
-    URC(conv_forward(s, L[7], tv(u->x1c, 32, 0, B, G1), tv(u->x1d, 32, 0, B, G1), bias(7), n1));
+    URC(conv_forward(s, P, L[6], tv(u->cat1, 96, 0, B, G1), tv(u->x1c, 32, 0, B, G1), bias(6), n1));
+    URC(conv_forward(s, P, L[7], tv(u->x1c, 32, 0, B, G1), tv(u->x1d, 32, 0, B, G1), bias(7), n1));
     k_upsample<<<blocks_for(n0 * 32, 256), 256, 0, s>>>(tv(u->x1d, 32, 0, B, G1), tv(u->cat0, 48, 0, B, G0), 32);
     ULAUNCH();
-    URC(conv_forward(s, L[8], tv(u->cat0, 48, 0, B, G0), tv(u->x0c, 16, 0, B, G0), bias(8), n0));
-    URC(conv_forward(s, L[9], tv(u->x0c, 16, 0, B, G0), tv(u->x0d, 16, 0, B, G0), bias(9), n0));
-    URC(conv_forward(s, L[10], tv(u->x0d, 16, 0, B, G0), tv(u->out, 16, 0, B, G0), bias(10), n0));
+    URC(conv_forward(s, P, L[8], tv(u->cat0, 48, 0, B, G0), tv(u->x0c, 16, 0, B, G0), bias(8), n0));
+    URC(conv_forward(s, P, L[9], tv(u->x0c, 16, 0, B, G0), tv(u->x0d, 16, 0, B, G0), bias(9), n0));
+    URC(conv_forward(s, P, L[10], tv(u->x0d, 16, 0, B, G0), tv(u->out, 16, 0, B, G0), bias(10), n0));
     return PLATO_OK;
 }
 
@@ -714,6 +981,7 @@ int layer_backward(plato_unet* u, int k, TView dy, TView y, TView x, TView dx, b
                    int64_t nvox) {
     cudaStream_t s = u->stream;
     const Layer& L = u->layers[k];
+    const ConvPath P{u->conv_kind, u->conv_err};
     const int C = L.coutp() < 16 ? 16 : L.coutp();
     const int gdims[3] = {y.D, y.H, y.W};
     TView m = tv(u->mbuf, C, 0, y.B, gdims);
@@ -726,7 +994,7 @@ int layer_backward(plato_unet* u, int k, TView dy, TView y, TView x, TView dx, b
     URC(conv_weight_grad(s, L, x, m, u->grads + L.w_off, nvox));
     k_bias_grad<<<256, 128, 0, s>>>(u->mbuf, m, C, L.cout, u->grads + L.b_off, nvox);
     ULAUNCH();
-    if (write_dx) URC(conv_data_grad(s, L, m, dx, nvox, accumulate));
+    if (write_dx) URC(conv_data_grad(s, P, L, m, dx, nvox, accumulate));
     return PLATO_OK;
 }
 
@@ -860,6 +1128,7 @@ int plato_unet_create(const int32_t nodes[3], int32_t max_batch, plato_unet** ou
     CA(u->dx0d, halo_elems(G0, B, 16));
     CA(u->mbuf, halo_elems(G0, B, 64) > halo_elems(G1, B, 64) ? halo_elems(G0, B, 64) : halo_elems(G1, B, 64));
     CA(u->loss_d, 1);
+    CA(u->conv_err, 1);
 #undef CA
     *out = u;
     return PLATO_OK;
@@ -870,6 +1139,26 @@ int plato_unet_destroy(plato_unet* u) {
     if (u->stream) cudaStreamSynchronize(u->stream);
     for (void* p : u->allocs) cudaFree(p);
     delete u;
+    return PLATO_OK;
+}
+
+int plato_unet_set_conv_kernel(plato_unet* u, int32_t kind) {
+    if (!u) return fail(PLATO_BAD_INPUT, "null network");
+    if (kind != PLATO_UNET_CONV_TCGEN05 && kind != PLATO_UNET_CONV_MMA_SYNC)
+        return fail(PLATO_BAD_INPUT, "unknown convolution kernel kind");
+    u->conv_kind = kind;
+    return PLATO_OK;
+}
+
+int plato_unet_check(plato_unet* u) {
+    if (!u) return fail(PLATO_BAD_INPUT, "null network");
+    int err = 0;
+    UCUDA(cudaMemcpyAsync(&err, u->conv_err, sizeof(int), cudaMemcpyDeviceToHost, u->stream));
+    UCUDA(cudaStreamSynchronize(u->stream));
+    if (err) {
+        UCUDA(cudaMemsetAsync(u->conv_err, 0, sizeof(int), u->stream));
+        return fail(PLATO_DEVICE_TIMEOUT, "a tensor-core convolution gave up waiting for its MMAs");
+    }
     return PLATO_OK;
 }
 
@@ -927,7 +1216,7 @@ int plato_unet_loss_and_gradients(plato_unet* u, int32_t batch, const float* inp
         UCUDA(cudaMemcpyAsync(grads, u->grads, sizeof(float) * size_t(u->nparams), cudaMemcpyDeviceToDevice, s));
     if (loss) {
         UCUDA(cudaMemcpyAsync(loss, u->loss_d, sizeof(double), cudaMemcpyDeviceToHost, s));
-        UCUDA(cudaStreamSynchronize(s));
+        return plato_unet_check(u);  // synchronises the stream
     }
     return PLATO_OK;
 }

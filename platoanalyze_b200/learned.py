@@ -48,7 +48,9 @@ def _i3(v):
 class UNet:
     """The warm-start network on a fixed node grid (device parameters, FP32 + BF16 copies)."""
 
-    def __init__(self, nodes=NET_NODES, max_batch: int = 8, stream=None):
+    CONV_TCGEN05, CONV_MMA_SYNC = 0, 1
+
+    def __init__(self, nodes=NET_NODES, max_batch: int = 8, stream=None, conv_kernel: int = 0):
         import torch
 
         self.torch = torch
@@ -58,10 +60,15 @@ class UNet:
         _ucheck(lib.plato_unet_create(_i3(self.nodes), max_batch, C.byref(self.h)))
         self.stream = stream if stream is not None else torch.cuda.current_stream()
         _ucheck(lib.plato_unet_set_stream(self.h, C.c_void_p(self.stream.cuda_stream)))
+        _ucheck(lib.plato_unet_set_conv_kernel(self.h, conv_kernel))
         n = C.c_int64()
         _ucheck(lib.plato_unet_num_params(self.h, C.byref(n)))
         self.num_params = n.value
         self.num_nodes = int(np.prod(self.nodes))
+
+    def check(self):
+        """Waits for the network's stream; raises when a tensor-core convolution timed out."""
+        _ucheck(lib.plato_unet_check(self.h))
 
     def close(self):
         if getattr(self, "h", None):

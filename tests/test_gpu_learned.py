@@ -22,11 +22,13 @@ def layer_slices():
     return out
 
 
+@pytest.mark.parametrize("conv_kernel", [UNet.CONV_TCGEN05, UNet.CONV_MMA_SYNC])
 @pytest.mark.parametrize("nodes,batch", [((9, 5, 5), 2), ((6, 7, 5), 1)])
-def test_network_matches_oracle(nodes, batch):
+def test_network_matches_oracle(nodes, batch, conv_kernel):
     """Forward output, loss and every layer's weight and bias gradient within BF16-level
-    tolerance of the oracle, which rounds to BF16 where the GPU stores BF16."""
-    net = UNet(nodes, batch)
+    tolerance of the oracle, which rounds to BF16 where the GPU stores BF16, with the tcgen05
+    (TMEM accumulator) and the mma.sync convolutions."""
+    net = UNet(nodes, batch, conv_kernel=conv_kernel)
     assert net.num_params == num_params()
     rng = np.random.default_rng(4)
     p = init_params(net.num_params, 3) + (0.05 * rng.standard_normal(net.num_params)).astype(np.float32)
@@ -47,6 +49,32 @@ def test_network_matches_oracle(nodes, batch):
     for k, (ws, bs) in enumerate(layer_slices()):
         assert rel_l2(g[ws], g_o[ws]) <= 5e-2, (k, rel_l2(g[ws], g_o[ws]))
         assert rel_l2(g[bs], g_o[bs]) <= 5e-2, (k, rel_l2(g[bs], g_o[bs]))
+
+
+def test_tcgen05_and_mma_sync_convolutions_agree():
+    """The two convolution kernel families on one network, a grid whose voxel count is not a
+    multiple of the 128-voxel tile at any level and a batch of 3: forward outputs and parameter
+    gradients agree to FP32 summation order (BF16 activations rounded alike), and no
+    tensor-core wait ran out."""
+    nodes = (13, 7, 9)
+    rng = np.random.default_rng(8)
+    nn = int(np.prod(nodes))
+    inp = torch.tensor(rng.uniform(-1, 1, (3, nn, 8)).astype(np.float32)).cuda()
+    tgt = torch.tensor(rng.standard_normal((3, nn, 9)).astype(np.float32)).cuda()
+    outs, grads, p = [], [], None
+    for kind in (UNet.CONV_TCGEN05, UNet.CONV_MMA_SYNC):
+        net = UNet(nodes, 3, conv_kernel=kind)
+        if p is None:
+            p = init_params(net.num_params, 5) + (0.05 * rng.standard_normal(net.num_params)).astype(np.float32)
+        net.set_params(p)
+        outs.append(net.forward(inp).cpu().numpy())
+        _, g = net.loss_and_gradients(inp, tgt, want_grads=True)
+        net.check()
+        grads.append(g.cpu().numpy())
+        net.close()
+    assert np.all(np.isfinite(outs[0])) and np.abs(outs[0]).max() > 0
+    assert rel_l2(outs[0], outs[1]) <= 5e-3, rel_l2(outs[0], outs[1])
+    assert rel_l2(grads[0], grads[1]) <= 1e-2, rel_l2(grads[0], grads[1])
 
 
 def test_adam_first_step():

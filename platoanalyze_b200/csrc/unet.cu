@@ -194,8 +194,9 @@ k_conv(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TV
 // canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk c
 // at c * LBO + (r / 8) * 128 + (r % 8) * 16), then one thread issues CIN / 16 tcgen05.mma
 // (kind::f16: BF16 A and B, FP32 accumulate) with shared-memory descriptors of both operands and
-// commits them to the stage's mbarrier.  Two stages: tap t + 1 is gathered while the tensor core
-// works on tap t; a stage is refilled only after the mbarrier shows its MMAs complete.  The
+// commits them to the stage's mbarrier.  Up to four stages, the MMAs of a tap issued two taps
+// after its gathers (so later taps' gathers are in flight while the tensor core works); a stage
+// is refilled only after its mbarrier shows the MMAs that read it complete.  The
 // epilogue loads the accumulator with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31, the
 // rows of its 32 voxels), adds the bias, applies ReLU and stores.  Every mbarrier wait is
 // bounded: on a timeout the CTA stops issuing, waits (bounded) for what it issued, raises *err,
@@ -280,11 +281,19 @@ constexpr uint32_t tc_stage_bytes() {
     return uint32_t(kTcRows) * CIN * 2 + uint32_t(COUTP) * CIN * 2;
 }
 
-// Dynamic shared memory per CTA: the two stages, raised so that no more CTAs fit on an SM than
-// its 512 TMEM columns hold (an allocation beyond them would wait for another CTA's release).
+// Pipeline depth: up to 4 shared-memory stages (3 or 2 for the widest layers) and the MMAs of a
+// tap issued kTcLag(S) taps after its gathers, so that many taps' gathers are in flight.
+template <int CIN, int COUTP>
+constexpr int tc_stages() {
+    return tc_stage_bytes<CIN, COUTP>() <= 16u * 1024u ? 4 : (tc_stage_bytes<CIN, COUTP>() <= 24u * 1024u ? 3 : 2);
+}
+constexpr int tc_lag(int stages) { return stages / 2; }
+
+// Dynamic shared memory per CTA: the stages, raised so that no more CTAs fit on an SM than its
+// 512 TMEM columns hold (an allocation beyond them would wait for another CTA's release).
 template <int CIN, int COUTP>
 constexpr uint32_t tc_smem_bytes() {
-    constexpr uint32_t stages = 2 * tc_stage_bytes<CIN, COUTP>();
+    constexpr uint32_t stages = uint32_t(tc_stages<CIN, COUTP>()) * tc_stage_bytes<CIN, COUTP>();
     constexpr uint32_t per_cta = (227u * 1024u) / (512u / tc_tmem_cols<COUTP>()) + 1024u;
     return stages > per_cta ? stages : per_cta;
 }
@@ -296,13 +305,14 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     constexpr int COUTP = (COUT + 15) / 16 * 16;
     static_assert(CIN % 16 == 0 && COUTP <= 256, "UMMA shape");
     constexpr int TMEM_COLS = tc_tmem_cols<COUTP>();
+    constexpr int S = tc_stages<CIN, COUTP>(), LAG = tc_lag(S);
     constexpr uint32_t A_BYTES = uint32_t(kTcRows) * CIN * 2;
     constexpr uint32_t STAGE = tc_stage_bytes<CIN, COUTP>();
     constexpr uint32_t LBO_A = (kTcRows / 8) * 128;  // bytes between the K-chunks of A
     constexpr uint32_t LBO_B = (COUTP / 8) * 128;
     constexpr uint32_t IDESC = umma_idesc_bf16_f32<COUTP>();
     extern __shared__ __align__(128) uint8_t tc_smem[];
-    __shared__ __align__(8) uint64_t bar[3];  // MMA completion of stage 0, of stage 1; all MMAs
+    __shared__ __align__(8) uint64_t bar[S + 1];  // MMA completion per stage; all MMAs
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
     if (warp == 0) {
@@ -312,9 +322,7 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_init(&bar[2], 1);
+        for (int q = 0; q <= S; ++q) mbar_init(&bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -327,49 +335,59 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     const int64_t hrow = row_ok ? halo_index(in, v) : 0;
     const int64_t sy = in.W + 2, sz = int64_t(in.H + 2) * (in.W + 2);
     const uint32_t sbase = smem_u32(tc_smem);
+    const uint32_t arow = uint32_t(tid >> 3) * 128u + uint32_t(tid & 7) * 16u;
     bool ok = true;
     int issued = 0;
-    for (int t = 0; t < TAPS; ++t) {
-        const int st = t & 1;
-        if (t >= 2) {  // the MMAs of tap t - 2 have finished reading this stage
-            bool w = true;
-            if (tid == 0) w = mbar_wait(&bar[st], uint32_t((t - 2) >> 1) & 1u);
-            ok = __syncthreads_and(w) != 0;
-            if (!ok) break;
-        }
-        const uint32_t a_s = sbase + uint32_t(st) * STAGE, b_s = a_s + A_BYTES;
-        int64_t o = 0;
-        if (TAPS == 27) o = (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1);
-        const bf16* src = row_ok ? ip + (hrow + o) * in.ld + in.c0 : ip;
-        const uint32_t arow = uint32_t(tid >> 3) * 128u + uint32_t(tid & 7) * 16u;
+    // iteration i gathers tap i (when i < TAPS) and issues the MMAs of tap i - LAG
+    for (int i = 0; i < TAPS + LAG; ++i) {
+        if (i < TAPS) {
+            const int st = i % S;
+            if (i >= S) {  // the MMAs of tap i - S (issued LAG iterations after it) have read this stage
+                bool w = true;
+                if (tid == 0) w = mbar_wait(&bar[st], uint32_t((i - S) / S) & 1u);
+                ok = __syncthreads_and(w) != 0;
+                if (!ok) break;
+            }
+            const uint32_t a_s = sbase + uint32_t(st) * STAGE, b_s = a_s + A_BYTES;
+            int64_t o = 0;
+            if (TAPS == 27) o = (i / 9 - 1) * sz + ((i / 3) % 3 - 1) * sy + (i % 3 - 1);
+            const bf16* src = row_ok ? ip + (hrow + o) * in.ld + in.c0 : ip;
 #pragma unroll
-        for (int c8 = 0; c8 < CIN / 8; ++c8)
-            cp_async16(a_s + uint32_t(c8) * LBO_A + arow, row_ok ? src + 8 * c8 : ip, row_ok ? 16u : 0u);
-        const bf16* wt = Wt + int64_t(t) * COUTP * CIN;
-        for (int q = tid; q < COUTP * (CIN / 8); q += 128) {
-            const int n = q / (CIN / 8), c8 = q - n * (CIN / 8);
-            cp_async16(b_s + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u, wt + n * CIN + 8 * c8,
-                       16u);
+            for (int c8 = 0; c8 < CIN / 8; ++c8)  // L1-allocating: neighbouring taps re-read these rows
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(a_s + uint32_t(c8) * LBO_A + arow),
+                             "l"(row_ok ? src + 8 * c8 : ip), "r"(row_ok ? 16u : 0u)
+                             : "memory");
+            const bf16* wt = Wt + int64_t(i) * COUTP * CIN;
+            for (int q = tid; q < COUTP * (CIN / 8); q += 128) {
+                const int n = q / (CIN / 8), c8 = q - n * (CIN / 8);
+                cp_async16(b_s + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u,
+                           wt + n * CIN + 8 * c8, 16u);
+            }
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");  // one group per iteration (empty past TAPS)
+        if (i >= LAG) {
+            const int tm = i - LAG;  // the groups of the last LAG iterations may stay in flight
+            asm volatile("cp.async.wait_group %0;" ::"n"(LAG) : "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core
+            __syncthreads();
+            if (tid == 0) {
+                const uint32_t a_s = sbase + uint32_t(tm % S) * STAGE, b_s = a_s + A_BYTES;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-            for (int kc = 0; kc < CIN / 16; ++kc)
-                umma_bf16(tmem, umma_smem_desc(a_s + 2u * kc * LBO_A, LBO_A, 128u),
-                          umma_smem_desc(b_s + 2u * kc * LBO_B, LBO_B, 128u), IDESC, (t > 0 || kc > 0) ? 1u : 0u);
-            umma_commit(&bar[st]);
+                for (int kc = 0; kc < CIN / 16; ++kc)
+                    umma_bf16(tmem, umma_smem_desc(a_s + 2u * kc * LBO_A, LBO_A, 128u),
+                              umma_smem_desc(b_s + 2u * kc * LBO_B, LBO_B, 128u), IDESC, (tm > 0 || kc > 0) ? 1u : 0u);
+                umma_commit(&bar[tm % S]);
+            }
+            ++issued;
         }
-        ++issued;
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into shared memory outlives the loop
     // all issued MMAs complete (bounded even after a timeout above)
     bool fin = true;
     if (tid == 0) {
-        if (issued > 0) umma_commit(&bar[2]);
-        fin = issued == 0 || mbar_wait(&bar[2], 0u);
+        if (issued > 0) umma_commit(&bar[S]);
+        fin = issued == 0 || mbar_wait(&bar[S], 0u);
     }
     const bool good = __syncthreads_and(ok && fin) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -543,14 +561,22 @@ __global__ void k_grad_mask(TView dy, TView y, int relu, bf16* __restrict__ m, i
     }
 }
 
-// db[c] += sum_v m[v][c] for c < count (m haloed, ld channels per voxel)
-__global__ void k_bias_grad(const bf16* __restrict__ m, TView shape, int ld, int count, float* __restrict__ db,
-                            int64_t nvox) {
-    for (int c = threadIdx.x; c < count; c += blockDim.x) {
-        float s = 0.f;
-        for (int64_t v = blockIdx.x; v < nvox; v += gridDim.x) s += __bfloat162float(m[halo_index(shape, v) * ld + c]);
-        atomicAdd(db + c, s);
-    }
+// db[c] += sum over every haloed position p of m[p][c] for c < count (m: C channels per position,
+// C in {16, 32, 64}; its halo holds zeros, so the sum over all positions is the interior sum).
+// Every thread sums one channel (blockDim and the grid stride are multiples of C) over a strided
+// range, the block combines per channel in shared memory, and one atomic per channel and block
+// adds to db.
+__global__ void __launch_bounds__(256) k_bias_grad(const bf16* __restrict__ m, int64_t total, int C, int count,
+                                                   float* __restrict__ db) {
+    __shared__ float sh[64];
+    if (threadIdx.x < 64) sh[threadIdx.x] = 0.f;
+    __syncthreads();
+    float s = 0.f;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x)
+        s += __bfloat162float(m[i]);
+    atomicAdd(&sh[threadIdx.x % C], s);
+    __syncthreads();
+    if (threadIdx.x < count) atomicAdd(db + threadIdx.x, sh[threadIdx.x]);
 }
 
 // 2x2x2 average pooling: out (extents of the coarse grid) from in (twice as fine)
@@ -992,7 +1018,8 @@ int layer_backward(plato_unet* u, int k, TView dy, TView y, TView x, TView dx, b
         ULAUNCH();
     }
     URC(conv_weight_grad(s, L, x, m, u->grads + L.w_off, nvox));
-    k_bias_grad<<<256, 128, 0, s>>>(u->mbuf, m, C, L.cout, u->grads + L.b_off, nvox);
+    const int64_t mtotal = halo_elems(gdims, y.B, C);
+    k_bias_grad<<<blocks_for(mtotal, 256, 148 * 8), 256, 0, s>>>(u->mbuf, mtotal, C, L.cout, u->grads + L.b_off);
     ULAUNCH();
     if (write_dx) URC(conv_data_grad(s, P, L, m, dx, nvox, accumulate));
     return PLATO_OK;

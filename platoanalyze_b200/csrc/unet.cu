@@ -281,19 +281,30 @@ constexpr uint32_t tc_stage_bytes() {
     return uint32_t(kTcRows) * CIN * 2 + uint32_t(COUTP) * CIN * 2;
 }
 
-// Pipeline depth: up to 4 shared-memory stages (3 or 2 for the widest layers) and the MMAs of a
-// tap issued kTcLag(S) taps after its gathers, so that many taps' gathers are in flight.
-template <int CIN, int COUTP>
+// Taps per pipeline stage: 3 when three taps' operands take at most 18 KB (the narrow layers, where
+// one tap is too little work per barrier), else 1; a single-tap (1x1x1) convolution uses 1.
+template <int CIN, int COUTP, int TAPS>
+constexpr int tc_group() {
+    return (TAPS % 3 == 0 && 3u * tc_stage_bytes<CIN, COUTP>() <= 18u * 1024u) ? 3 : 1;
+}
+
+// Pipeline depth: up to 4 shared-memory stages (3 or 2 for the widest ones) and the MMAs of a
+// stage issued tc_lag(S) stages after its gathers, so that several stages' gathers are in flight.
+template <int CIN, int COUTP, int TAPS>
 constexpr int tc_stages() {
-    return tc_stage_bytes<CIN, COUTP>() <= 16u * 1024u ? 4 : (tc_stage_bytes<CIN, COUTP>() <= 24u * 1024u ? 3 : 2);
+    return tc_group<CIN, COUTP, TAPS>() > 1 ? 2
+           : uint32_t(tc_group<CIN, COUTP, TAPS>()) * tc_stage_bytes<CIN, COUTP>() <= 18u * 1024u
+               ? 4
+               : (uint32_t(tc_group<CIN, COUTP, TAPS>()) * tc_stage_bytes<CIN, COUTP>() <= 24u * 1024u ? 3 : 2);
 }
 constexpr int tc_lag(int stages) { return stages / 2; }
 
 // Dynamic shared memory per CTA: the stages, raised so that no more CTAs fit on an SM than its
 // 512 TMEM columns hold (an allocation beyond them would wait for another CTA's release).
-template <int CIN, int COUTP>
+template <int CIN, int COUTP, int TAPS>
 constexpr uint32_t tc_smem_bytes() {
-    constexpr uint32_t stages = uint32_t(tc_stages<CIN, COUTP>()) * tc_stage_bytes<CIN, COUTP>();
+    constexpr uint32_t stages = uint32_t(tc_stages<CIN, COUTP, TAPS>()) * uint32_t(tc_group<CIN, COUTP, TAPS>()) *
+                                tc_stage_bytes<CIN, COUTP>();
     constexpr uint32_t per_cta = (227u * 1024u) / (512u / tc_tmem_cols<COUTP>()) + 1024u;
     return stages > per_cta ? stages : per_cta;
 }
@@ -305,9 +316,11 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     constexpr int COUTP = (COUT + 15) / 16 * 16;
     static_assert(CIN % 16 == 0 && COUTP <= 256, "UMMA shape");
     constexpr int TMEM_COLS = tc_tmem_cols<COUTP>();
-    constexpr int S = tc_stages<CIN, COUTP>(), LAG = tc_lag(S);
+    constexpr int G = tc_group<CIN, COUTP, TAPS>(), NG = TAPS / G;  // taps per stage, stages' worth of taps
+    constexpr int S = tc_stages<CIN, COUTP, TAPS>(), LAG = tc_lag(S);
     constexpr uint32_t A_BYTES = uint32_t(kTcRows) * CIN * 2;
-    constexpr uint32_t STAGE = tc_stage_bytes<CIN, COUTP>();
+    constexpr uint32_t TAPB = tc_stage_bytes<CIN, COUTP>();  // one tap's A and B
+    constexpr uint32_t STAGE = G * TAPB;
     constexpr uint32_t LBO_A = (kTcRows / 8) * 128;  // bytes between the K-chunks of A
     constexpr uint32_t LBO_B = (COUTP / 8) * 128;
     constexpr uint32_t IDESC = umma_idesc_bf16_f32<COUTP>();
@@ -338,46 +351,55 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     const uint32_t arow = uint32_t(tid >> 3) * 128u + uint32_t(tid & 7) * 16u;
     bool ok = true;
     int issued = 0;
-    // iteration i gathers tap i (when i < TAPS) and issues the MMAs of tap i - LAG
-    for (int i = 0; i < TAPS + LAG; ++i) {
-        if (i < TAPS) {
+    // iteration i gathers tap group i (taps G i .. G i + G - 1, when i < NG) and issues the MMAs
+    // of group i - LAG
+    for (int i = 0; i < NG + LAG; ++i) {
+        if (i < NG) {
             const int st = i % S;
-            if (i >= S) {  // the MMAs of tap i - S (issued LAG iterations after it) have read this stage
+            if (i >= S) {  // the MMAs of group i - S (issued LAG iterations after it) have read this stage
                 bool w = true;
                 if (tid == 0) w = mbar_wait(&bar[st], uint32_t((i - S) / S) & 1u);
                 ok = __syncthreads_and(w) != 0;
                 if (!ok) break;
             }
-            const uint32_t a_s = sbase + uint32_t(st) * STAGE, b_s = a_s + A_BYTES;
-            int64_t o = 0;
-            if (TAPS == 27) o = (i / 9 - 1) * sz + ((i / 3) % 3 - 1) * sy + (i % 3 - 1);
-            const bf16* src = row_ok ? ip + (hrow + o) * in.ld + in.c0 : ip;
 #pragma unroll
-            for (int c8 = 0; c8 < CIN / 8; ++c8)  // L1-allocating: neighbouring taps re-read these rows
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(a_s + uint32_t(c8) * LBO_A + arow),
-                             "l"(row_ok ? src + 8 * c8 : ip), "r"(row_ok ? 16u : 0u)
-                             : "memory");
-            const bf16* wt = Wt + int64_t(i) * COUTP * CIN;
-            for (int q = tid; q < COUTP * (CIN / 8); q += 128) {
-                const int n = q / (CIN / 8), c8 = q - n * (CIN / 8);
-                cp_async16(b_s + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u,
-                           wt + n * CIN + 8 * c8, 16u);
+            for (int gq = 0; gq < G; ++gq) {
+                const int t = G * i + gq;
+                const uint32_t a_s = sbase + uint32_t(st) * STAGE + uint32_t(gq) * TAPB, b_s = a_s + A_BYTES;
+                int64_t o = 0;
+                if (TAPS == 27) o = (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1);
+                const bf16* src = row_ok ? ip + (hrow + o) * in.ld + in.c0 : ip;
+#pragma unroll
+                for (int c8 = 0; c8 < CIN / 8; ++c8)  // L1-allocating: neighbouring taps re-read these rows
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(a_s + uint32_t(c8) * LBO_A + arow),
+                                 "l"(row_ok ? src + 8 * c8 : ip), "r"(row_ok ? 16u : 0u)
+                                 : "memory");
+                const bf16* wt = Wt + int64_t(t) * COUTP * CIN;
+                for (int q = tid; q < COUTP * (CIN / 8); q += 128) {
+                    const int n = q / (CIN / 8), c8 = q - n * (CIN / 8);
+                    cp_async16(b_s + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u,
+                               wt + n * CIN + 8 * c8, 16u);
+                }
             }
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");  // one group per iteration (empty past TAPS)
+        asm volatile("cp.async.commit_group;" ::: "memory");  // one group per iteration (empty past NG)
         if (i >= LAG) {
-            const int tm = i - LAG;  // the groups of the last LAG iterations may stay in flight
+            const int gm = i - LAG;  // the groups of the last LAG iterations may stay in flight
             asm volatile("cp.async.wait_group %0;" ::"n"(LAG) : "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core
             __syncthreads();
             if (tid == 0) {
-                const uint32_t a_s = sbase + uint32_t(tm % S) * STAGE, b_s = a_s + A_BYTES;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-                for (int kc = 0; kc < CIN / 16; ++kc)
-                    umma_bf16(tmem, umma_smem_desc(a_s + 2u * kc * LBO_A, LBO_A, 128u),
-                              umma_smem_desc(b_s + 2u * kc * LBO_B, LBO_B, 128u), IDESC, (tm > 0 || kc > 0) ? 1u : 0u);
-                umma_commit(&bar[tm % S]);
+                for (int gq = 0; gq < G; ++gq) {
+                    const uint32_t a_s = sbase + uint32_t(gm % S) * STAGE + uint32_t(gq) * TAPB, b_s = a_s + A_BYTES;
+#pragma unroll
+                    for (int kc = 0; kc < CIN / 16; ++kc)
+                        umma_bf16(tmem, umma_smem_desc(a_s + 2u * kc * LBO_A, LBO_A, 128u),
+                                  umma_smem_desc(b_s + 2u * kc * LBO_B, LBO_B, 128u), IDESC,
+                                  (gm > 0 || gq > 0 || kc > 0) ? 1u : 0u);
+                }
+                umma_commit(&bar[gm % S]);
             }
             ++issued;
         }
@@ -888,7 +910,7 @@ template <int CIN, int COUT, int TAPS, bool RELU, bool F32, bool ACC>
 int conv_launch(cudaStream_t s, const ConvPath& P, TView in, const bf16* w, const float* b, TView out, int64_t nvox) {
     if (P.kind == PLATO_UNET_CONV_TCGEN05) {
         constexpr int COUTP = (COUT + 15) / 16 * 16;
-        constexpr uint32_t smem = tc_smem_bytes<CIN, COUTP>();
+        constexpr uint32_t smem = tc_smem_bytes<CIN, COUTP, TAPS>();
         auto kernel = k_conv_tc<CIN, COUT, TAPS, RELU, F32, ACC>;
         UCUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         kernel<<<int((nvox + kTcRows - 1) / kTcRows), 128, smem, s>>>(in, w, b, out, nvox, P.err);

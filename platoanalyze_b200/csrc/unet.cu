@@ -21,6 +21,7 @@
 //    are element-wise kernels.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -475,7 +476,8 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
 // ---- weight gradient --------------------------------------------------------------------
 // dW[t][co][ci] += sum_v dy[v][co] x[v + o_t][ci]; grid (voxel chunks, TAPS).
 constexpr int kWgVox = 64;    // voxels per shared-memory tile
-constexpr int kWgTiles = 8;   // tiles per CTA
+constexpr int kWgCtasX = 48;  // CTAs per tap: each sums a long run of voxel tiles, so few CTAs
+                              // add their partial weight gradients to the same entries
 
 __device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const bf16* p) {
     const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -490,7 +492,7 @@ __device__ __forceinline__ void ldsm_x2_t(uint32_t& r0, uint32_t& r1, const bf16
 
 template <int CIN, int COUT, int TAPS>
 __global__ void __launch_bounds__(128)
-k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t nvox) {
+k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t nvox, int tiles) {
     static_assert(COUT % 16 == 0 && CIN % 8 == 0, "channel counts");
     constexpr int LDY = COUT + 8, LDX = CIN + 8;  // padded rows: 16-byte aligned, no bank conflicts
     constexpr int TILES = (COUT / 16) * (CIN / 8);
@@ -508,8 +510,8 @@ k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t n
         for (int q = 0; q < 4; ++q) acc[k][q] = 0.f;
     const bf16* __restrict__ yp = static_cast<const bf16*>(dy.p);
     const bf16* __restrict__ xp = static_cast<const bf16*>(x.p);
-    for (int tile = 0; tile < kWgTiles; ++tile) {
-        const int64_t v0 = (int64_t(blockIdx.x) * kWgTiles + tile) * kWgVox;
+    for (int tile = 0; tile < tiles; ++tile) {
+        const int64_t v0 = (int64_t(blockIdx.x) * tiles + tile) * kWgVox;
         if (v0 >= nvox) break;
         // stage: 16-byte vectors of 8 channels
         for (int q = threadIdx.x; q < kWgVox * (COUT / 8); q += blockDim.x) {
@@ -572,14 +574,28 @@ k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t n
 
 // masked output gradient (BF16, plain ld = C): m = dy * [y > 0] (relu) or dy
 __global__ void k_grad_mask(TView dy, TView y, int relu, bf16* __restrict__ m, int C, int64_t nvox) {
-    const int64_t total = nvox * C;
+    // one thread per (voxel, 4 channels): C, the views' ld and c0 are multiples of 4
+    const int C4 = C / 4;
+    const int64_t total = nvox * C4;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C;
-        const int c = int(i - v * C);
+        const int64_t v = i / C4;
+        const int c = 4 * int(i - v * C4);
         const int64_t hv = halo_index(dy, v);
-        float val = static_cast<const float*>(dy.p)[hv * dy.ld + dy.c0 + c];
-        if (relu && !(__bfloat162float(static_cast<const bf16*>(y.p)[hv * y.ld + y.c0 + c]) > 0.f)) val = 0.f;
-        m[hv * C + c] = __float2bfloat16(val);
+        const float4 d = *reinterpret_cast<const float4*>(static_cast<const float*>(dy.p) + hv * dy.ld + dy.c0 + c);
+        float val[4] = {d.x, d.y, d.z, d.w};
+        if (relu) {
+            const uint2 yy = *reinterpret_cast<const uint2*>(static_cast<const bf16*>(y.p) + hv * y.ld + y.c0 + c);
+            const __nv_bfloat162 y01 = *reinterpret_cast<const __nv_bfloat162*>(&yy.x);
+            const __nv_bfloat162 y23 = *reinterpret_cast<const __nv_bfloat162*>(&yy.y);
+            if (!(__low2float(y01) > 0.f)) val[0] = 0.f;
+            if (!(__high2float(y01) > 0.f)) val[1] = 0.f;
+            if (!(__low2float(y23) > 0.f)) val[2] = 0.f;
+            if (!(__high2float(y23) > 0.f)) val[3] = 0.f;
+        }
+        uint2 o;
+        o.x = pack_bf16(val[0], val[1]);
+        o.y = pack_bf16(val[2], val[3]);
+        *reinterpret_cast<uint2*>(m + hv * C + c) = o;
     }
 }
 
@@ -634,15 +650,17 @@ __global__ void k_pool_grad(TView dout, TView din, int C) {
 
 // nearest upsampling: out[fine] = in[coarse]
 __global__ void k_upsample(TView in, TView out, int C) {
+    // one thread per (fine voxel, 8 channels): a 16-byte copy (C, ld and c0 are multiples of 8)
+    const int C8 = C / 8;
     const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C;
-        const int c = int(i - v * C);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C8; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = i / C8;
+        const int c = 8 * int(i - v * C8);
         const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
         const int64_t b = v / (int64_t(out.W) * out.H * out.D);
         const int64_t cv = ((b * in.D + z / 2) * in.H + y / 2) * in.W + x / 2;
-        static_cast<bf16*>(out.p)[halo_index(out, v) * out.ld + out.c0 + c] =
-            static_cast<const bf16*>(in.p)[halo_index(in, cv) * in.ld + in.c0 + c];
+        *reinterpret_cast<uint4*>(static_cast<bf16*>(out.p) + halo_index(out, v) * out.ld + out.c0 + c) =
+            *reinterpret_cast<const uint4*>(static_cast<const bf16*>(in.p) + halo_index(in, cv) * in.ld + in.c0 + c);
     }
 }
 
@@ -954,9 +972,10 @@ int conv_data_grad(cudaStream_t s, const ConvPath& P, const Layer& L, TView dy, 
 
 template <int CIN, int COUT, int TAPS>
 int wgrad_launch(cudaStream_t s, TView x, TView dy, float* dW, int cout_real, int64_t nvox) {
-    const int64_t per = int64_t(kWgVox) * kWgTiles;
-    const dim3 grid(unsigned((nvox + per - 1) / per), TAPS);
-    k_conv_wgrad<CIN, COUT, TAPS><<<grid, 128, 0, s>>>(x, dy, dW, cout_real, nvox);
+    const int64_t ntiles = (nvox + kWgVox - 1) / kWgVox;
+    const int tiles = int(std::max<int64_t>(8, (ntiles + kWgCtasX - 1) / kWgCtasX));
+    const dim3 grid(unsigned((ntiles + tiles - 1) / tiles), TAPS);
+    k_conv_wgrad<CIN, COUT, TAPS><<<grid, 128, 0, s>>>(x, dy, dW, cout_real, nvox, tiles);
     ULAUNCH();
     return PLATO_OK;
 }

@@ -333,6 +333,42 @@ def evaluate(net: UNet, n: int, designs, tractions, method: str = "two-level", s
     return rows
 
 
+def time_kernels(batch: int = 8, steps: int = 10, nodes=NET_NODES) -> int:
+    """Forward and training-step (loss, backward) times of the network on random inputs with
+    the tcgen05 and the mma.sync convolutions, CUDA events on the network's stream, 3 warm-up
+    repetitions; prints one JSON line per kernel family."""
+    import json
+
+    import torch
+
+    rng = np.random.default_rng(0)
+    nn = int(np.prod(nodes))
+    inp = torch.tensor(rng.uniform(-1, 1, (batch, nn, 8)).astype(np.float32)).cuda()
+    tgt = torch.tensor(rng.standard_normal((batch, nn, 9)).astype(np.float32)).cuda()
+    for kind, name in ((UNet.CONV_TCGEN05, "tcgen05"), (UNet.CONV_MMA_SYNC, "mma.sync")):
+        net = UNet(nodes, batch, conv_kernel=kind)
+        net.set_params(init_params(net.num_params, 1))
+        for _ in range(3):
+            net.forward(inp)
+            net.loss_and_gradients(inp, tgt)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(net.stream)
+        for _ in range(steps):
+            net.forward(inp)
+        ev[1].record(net.stream)
+        for _ in range(steps):
+            net.loss_and_gradients(inp, tgt)
+        ev[2].record(net.stream)
+        torch.cuda.synchronize()
+        net.check()
+        print(json.dumps({"conv_kernel": name, "nodes": list(nodes), "batch": batch,
+                          "forward_ms": ev[0].elapsed_time(ev[1]) / steps,
+                          "train_step_ms": ev[1].elapsed_time(ev[2]) / steps}), flush=True)
+        net.close()
+    return 0
+
+
 def main(argv=None) -> int:
     import argparse
 
@@ -348,8 +384,14 @@ def main(argv=None) -> int:
     ap.add_argument("--load", default="", help="evaluate saved weights instead of training")
     ap.add_argument("--fine", type=int, default=160, help="also evaluate on the fine x fine/2 x fine/2 mesh (0: skip)")
     ap.add_argument("--smooth", default="0", help="comma-separated smoothing passes to evaluate")
+    ap.add_argument("--time-kernels", action="store_true",
+                    help="time the network alone (forward and training step on random data, both convolution "
+                         "kernel families) and exit")
+    ap.add_argument("--steps", type=int, default=10, help="--time-kernels: timed repetitions")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
+    if a.time_kernels:
+        return time_kernels(a.batch, a.steps)
     if a.load:
         net = UNet.load(a.load, a.batch)
     else:

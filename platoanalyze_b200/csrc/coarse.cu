@@ -786,14 +786,45 @@ k_restrict_cells(CoarseView cv, int split, const int32_t* __restrict__ node_ptr,
             for (int d = 0; d < 3; ++d) s[3 * b + d] += wgt * val[d];
         }
     }
-#pragma unroll
-    for (int t = 0; t < 24; ++t)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s[t] += __shfl_xor_sync(0xffffffffu, s[t], o);
+    // warp sums of the 24 values by halving: each exchange hands half of a lane's values to its
+    // partner, so after offsets 16, 8, 4 a lane holds 3 of the 24 sums (which 3 set by lane bits
+    // 4..2) and offsets 2, 1 finish them -- 27 shuffles instead of 24 x 5
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
+    double t12[12], t6[6], t3[3];
+    {
+        const bool hi = (lane & 16) != 0;
 #pragma unroll
-        for (int t = 0; t < 24; ++t) sh[wid][t] = s[t];
+        for (int i = 0; i < 12; ++i) {
+            const double send = hi ? s[i] : s[12 + i];
+            t12[i] = (hi ? s[12 + i] : s[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    }
+    {
+        const bool hi = (lane & 8) != 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const double send = hi ? t12[i] : t12[6 + i];
+            t6[i] = (hi ? t12[6 + i] : t12[i]) + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+    }
+    {
+        const bool hi = (lane & 4) != 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double send = hi ? t6[i] : t6[3 + i];
+            t3[i] = (hi ? t6[3 + i] : t6[i]) + __shfl_xor_sync(0xffffffffu, send, 4);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        t3[i] += __shfl_xor_sync(0xffffffffu, t3[i], 2);
+        t3[i] += __shfl_xor_sync(0xffffffffu, t3[i], 1);
+    }
+    if ((lane & 3) == 0) {
+        const int base = ((lane & 16) ? 12 : 0) + ((lane & 8) ? 6 : 0) + ((lane & 4) ? 3 : 0);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) sh[wid][base + i] = t3[i];
+    }
     __syncthreads();
     if (threadIdx.x < 24) {
         double t = 0.0;
@@ -827,22 +858,25 @@ __global__ void k_restrict_sum(CoarseView cv, int split, const double* __restric
 // The coarse solve is y = U (X r) with X = L^-1 and U = X^T (E^-1 = X^T X); the factorization
 // and inversion run in FP64, the two products per preconditioner apply read FP32 copies.
 // out = M in for a triangular FP32 matrix (row stride ld, zeros outside the triangle and in
-// the padding columns), FP64 vectors and sums.  A warp per row, 16-byte loads from the row's
-// first 4-aligned column; the in[] reads past n are skipped.
+// the padding columns), FP64 vectors and sums.  A CTA of 4 warps per row (the longest rows hold
+// n/4 16-byte groups, so one warp per row left the product waiting on their load latency);
+// 16-byte loads from the row's first 4-aligned column, the in[] reads past n skipped; the four
+// warp sums are added in a fixed order.
 template <bool LOWER>
-__global__ void __launch_bounds__(256) k_coarse_trmv(int n, int ld, const float* __restrict__ M,
+__global__ void __launch_bounds__(128) k_coarse_trmv(int n, int ld, const float* __restrict__ M,
                                                      const double* __restrict__ in, double* __restrict__ out,
                                                      const PcgScalars* S) {
     pdl_wait();
     pdl_trigger();
     if (S && S->done) return;
-    const int lane = threadIdx.x & 31;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
+    __shared__ double part[4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int row = blockIdx.x; row < n; row += gridDim.x) {
         const int q0 = LOWER ? 0 : (row >> 2), q1 = LOWER ? (row >> 2) + 1 : (n + 3) >> 2;
         const float4* mp = reinterpret_cast<const float4*>(M + (int64_t)row * ld);
         double s = 0.0;
 #pragma unroll 4
-        for (int q = q0 + lane; q < q1; q += 32) {
+        for (int q = q0 + threadIdx.x; q < q1; q += 128) {
             const float4 v = __ldg(mp + q);
             const int c = 4 * q;
             s += double(v.x) * in[c];
@@ -851,7 +885,10 @@ __global__ void __launch_bounds__(256) k_coarse_trmv(int n, int ld, const float*
             if (c + 3 < n) s += double(v.w) * in[c + 3];
         }
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) out[row] = s;
+        if (lane == 0) part[warp] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) out[row] = (part[0] + part[1]) + (part[2] + part[3]);
+        __syncthreads();
     }
 }
 
@@ -1225,10 +1262,10 @@ int coarse_apply(plato_problem* h, const float* v, float* y, int accumulate, con
                              (const uint8_t*)h->bc_mask, v, sq, c.rpart, S));
     PLATO_CUDA(h, launch_pdl(k_restrict_sum, grid_for(c.ndof, 256), 256, s, cv, c.rsplit, (const double*)c.rpart,
                              c.rc, S));
-    const int GB = grid_for(int64_t(c.ndof) * 32, 256, 148 * 8);
-    PLATO_CUDA(h, launch_pdl(k_coarse_trmv<true>, GB, 256, s, c.ndof, c.ldf, (const float*)c.Xf, (const double*)c.rc,
+    const int GB = std::min(c.ndof, 148 * 16);  // a CTA per row
+    PLATO_CUDA(h, launch_pdl(k_coarse_trmv<true>, GB, 128, s, c.ndof, c.ldf, (const float*)c.Xf, (const double*)c.rc,
                              c.tc, S));
-    PLATO_CUDA(h, launch_pdl(k_coarse_trmv<false>, GB, 256, s, c.ndof, c.ldf, (const float*)c.Uf, (const double*)c.tc,
+    PLATO_CUDA(h, launch_pdl(k_coarse_trmv<false>, GB, 128, s, c.ndof, c.ldf, (const float*)c.Uf, (const double*)c.tc,
                              c.yc, S));
     PLATO_CUDA(h, launch_pdl(k_prolong, grid_for(h->N, 256), 256, s, h->N, cv, (const double*)h->coords,
                              (const uint8_t*)h->bc_mask, (const double*)c.yc, sq, y, accumulate, S));

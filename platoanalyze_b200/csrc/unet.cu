@@ -476,8 +476,8 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
 // ---- weight gradient --------------------------------------------------------------------
 // dW[t][co][ci] += sum_v dy[v][co] x[v + o_t][ci]; grid (voxel chunks, TAPS).
 constexpr int kWgVox = 64;    // voxels per shared-memory tile
-constexpr int kWgCtasX = 48;  // CTAs per tap: each sums a long run of voxel tiles, so few CTAs
-                              // add their partial weight gradients to the same entries
+constexpr int kWgCtas = 148 * 16;  // CTAs over all taps: each sums a long run of voxel tiles, so
+                                   // few CTAs add their partial weight gradients to one entry
 
 __device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const bf16* p) {
     const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -496,11 +496,16 @@ k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t n
     static_assert(COUT % 16 == 0 && CIN % 8 == 0, "channel counts");
     constexpr int LDY = COUT + 8, LDX = CIN + 8;  // padded rows: 16-byte aligned, no bank conflicts
     constexpr int TILES = (COUT / 16) * (CIN / 8);
-    constexpr int PER = (TILES + 3) / 4;
+    // with only two 16 x 8 output tiles (16 -> 16 channels), pairs of warps share a tile and split
+    // its k-steps (even / odd), so all four warps work; each adds its own partial sums
+    constexpr int KSPLIT = TILES <= 2 ? 2 : 1;
+    constexpr int WPT = 4 / KSPLIT;  // warps per k-group
+    constexpr int PER = (TILES + WPT - 1) / WPT;
     __shared__ __align__(16) bf16 sy[kWgVox * LDY];
     __shared__ __align__(16) bf16 sx[kWgVox * LDX];
     const int t = blockIdx.y;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wt = warp % WPT, kg = warp / WPT;
     const int64_t sz = int64_t(x.H + 2) * (x.W + 2), syy = x.W + 2;
     const int64_t o = TAPS == 27 ? ((t / 9 - 1) * sz + ((t / 3) % 3 - 1) * syy + (t % 3 - 1)) : 0;
     float acc[PER][4];
@@ -532,9 +537,10 @@ k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t n
         __syncthreads();
 #pragma unroll
         for (int ks = 0; ks < kWgVox / 16; ++ks) {
+            if (ks % KSPLIT != kg) continue;
 #pragma unroll
             for (int k = 0; k < PER; ++k) {
-                const int tid = warp + 4 * k;
+                const int tid = wt + WPT * k;
                 if (tid >= TILES) break;
                 const int m0 = 16 * (tid / (CIN / 8)), n0 = 8 * (tid % (CIN / 8));
                 // A = dy^T (rows co, cols voxel): matrices (m0, k0), (m0+8, k0), (m0, k0+8), (m0+8, k0+8)
@@ -555,7 +561,7 @@ k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t n
     const int g = lane >> 2, tig = lane & 3;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-        const int tid = warp + 4 * k;
+        const int tid = wt + WPT * k;
         if (tid >= TILES) break;
         const int m0 = 16 * (tid / (CIN / 8)), n0 = 8 * (tid % (CIN / 8));
         float* w = dW + int64_t(t) * cout_real * CIN;  // rows past the real output channels are padding
@@ -973,7 +979,8 @@ int conv_data_grad(cudaStream_t s, const ConvPath& P, const Layer& L, TView dy, 
 template <int CIN, int COUT, int TAPS>
 int wgrad_launch(cudaStream_t s, TView x, TView dy, float* dW, int cout_real, int64_t nvox) {
     const int64_t ntiles = (nvox + kWgVox - 1) / kWgVox;
-    const int tiles = int(std::max<int64_t>(8, (ntiles + kWgCtasX - 1) / kWgCtasX));
+    const int64_t per_tap = std::max(1, kWgCtas / TAPS);
+    const int tiles = int(std::max<int64_t>(8, (ntiles + per_tap - 1) / per_tap));
     const dim3 grid(unsigned((ntiles + tiles - 1) / tiles), TAPS);
     k_conv_wgrad<CIN, COUT, TAPS><<<grid, 128, 0, s>>>(x, dy, dW, cout_real, nvox, tiles);
     ULAUNCH();

@@ -189,8 +189,9 @@ int plato_get_instrumentation(const plato_problem* h, int64_t* launches, double*
                               int64_t* op_timed);
 int plato_reset_instrumentation(plato_problem* h);
 /* Sampled CUDA-event time of one kernel class inside the solvers: kind 0 = the FP64 operator
- * apply of the Krylov loop, kind 1 = the first Chebyshev step of the low-precision
- * preconditioner (one step = one preconditioner-operator apply fused with its update),
+ * apply of the Krylov loop, kind 1 = the Chebyshev steps of the low-precision preconditioner
+ * (one step = one preconditioner-operator apply fused with its update; a sampled call is timed
+ * over its whole run of step launches and counts as its number of steps),
  * kind 2 = the Jacobian assembly of each assembled solve, kind 3 = the Galerkin product of
  * the two-level coarse operator, kind 4 = its dense factorization and inverse (kinds 3 and 4
  * count coarse operator set-ups); kinds 5-8 time every call with timing on: 5 = the residual
@@ -199,7 +200,7 @@ int plato_reset_instrumentation(plato_problem* h);
  * sums), 8 = plato_problem_criterion_value_and_gradient's one pass (+ nodal sums).  Reading
  * kinds 5-8 waits for the last timed launch of that kind.  With the multi-step FP16 sweep
  * (sweep_steps) kind 1 times the first launch of the sampled preconditioner calls and counts
- * it as its number of steps, so ms_total / count stays the time per step. */
+ * it as its number of steps; either way ms_total / count is the time per step. */
 int plato_get_kernel_timing(const plato_problem* h, int32_t kind, double* ms_total, int64_t* count);
 /* The FP16 sweep of the last flexible-CG solve: Chebyshev steps per launch (1 = one launch
  * per step; > 1 = the multi-step sweep) and its column reach in tiles of 512 rows (-1 when

@@ -1061,8 +1061,10 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
         if (wave_S > 0) return wave_sweep();
         float* dcur = h->f_d0;
         float* dnext = h->f_d1;
+        // a sampled call times its whole run of degree - 1 consecutive step launches between one
+        // event pair (collect_timing counts it as that many steps)
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
         for (int k = 1; k < degree; ++k) {
-            cudaEvent_t t0 = nullptr, t1 = nullptr;
             if (k == 1 && inner_record >= 0) {
                 int r2 = timing_events(h, &t0, &t1);
                 if (r2) return r2;
@@ -1094,7 +1096,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                                                                   h->f_y, cc.c1[k], cc.c2[k], h->scal);
             }
             PLATO_LAUNCH_CHECK(h);
-            if (t1) PLATO_CUDA(h, cudaEventRecord(t1, s));
+            if (t1 && k == degree - 1) PLATO_CUDA(h, cudaEventRecord(t1, s));
             std::swap(dcur, dnext);
         }
         dlast = dcur;
@@ -1218,7 +1220,7 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                                   "multi-step sweep: a bounded wait for a neighbouring tile ran out");
             }
         }
-        h->inner_record_steps = wave_S > 0 ? wave_first_len : 1;
+        h->inner_record_steps = wave_S > 0 ? wave_first_len : std::max(1, degree - 1);
         rc = collect_timing(h, timed_iters, fin.iter - iter_base);
         if (rc) return rc;
         precond_applies += int64_t(fin.iter - iter_base + 1) * (degree - 1);

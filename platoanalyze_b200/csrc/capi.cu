@@ -158,7 +158,7 @@ int plato_destroy(plato_problem* h) {
     dfree(h->f_sq); dfree(h->f_isq);
     dfree(h->mf_w64); dfree(h->mf_w32); dfree(h->v_q);
     dfree(h->f_res); dfree(h->f_d0); dfree(h->f_d1); dfree(h->f_y); dfree(h->f_w);
-    dfree(h->wave_flags); dfree(h->wave_ctl);
+    dfree(h->wave_flags); dfree(h->wave_ctl); dfree(h->lanczos);
     for (int32_t*& o : h->wave_order) dfree(o);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -275,7 +275,7 @@ int plato_create(const plato_problem_desc* d, plato_problem** out) {
     CRC(dmalloc(h, &h->partials, 4 * int64_t(h->partials_len)));
     CRC(dmalloc(h, &h->cellbuf, h->C));
     CRC(dmalloc(h, &h->scal, 1));
-    CRC(dmalloc(h, &h->red_out, 4));  // up to 4 reduction results (power iteration uses 3)
+    CRC(dmalloc(h, &h->red_out, 4));  // up to 4 reduction results
     CRC(dmalloc(h, &h->red_ticket, 1));
     CCUDA(cudaMemset(h->red_ticket, 0, sizeof(uint32_t)));
     CCUDA(cudaMemset(h->scal, 0, sizeof(PcgScalars)));

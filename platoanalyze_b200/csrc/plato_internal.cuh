@@ -273,6 +273,7 @@ struct plato_problem {
     // ticket counters, and the task order for each launch length
     int32_t* wave_flags = nullptr; // [16][wave_tiles] epoch of the last completion
     int32_t* wave_ctl = nullptr;   // ticket, exits, abort, fail
+    double* lanczos = nullptr;     // Lanczos coefficients of the Chebyshev interval estimate
     int32_t* wave_order[17] = {};  // per steps-per-launch: task codes (step << 24 | tile)
     int32_t  wave_order_lag[17] = {};
     int32_t  wave_tiles = 0;

@@ -132,7 +132,7 @@ __device__ __forceinline__ void upper_entry(int t, int& r, int& c) {
 constexpr int kFastBatch = 256;
 constexpr int kSlices = 25;
 
-__global__ void __launch_bounds__(kThreadsPerCta)
+__global__ void __launch_bounds__(kThreadsPerCta, 2)
 k_galerkin_fast(CoarseView cv, int split, const int32_t* __restrict__ elem_ptr, const int32_t* __restrict__ elem_list,
                 const int4* __restrict__ conn, const double* __restrict__ coords, const double* __restrict__ z,
                 Material mat, const uint8_t* __restrict__ mask, int n, double* __restrict__ E) {

@@ -187,22 +187,26 @@ k_conv(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TV
 }
 
 // ---- convolution on the 5th-generation tensor cores (tcgen05, TMEM accumulator) -----------
-// The same implicit GEMM as k_conv: a CTA of 4 warps owns 128 consecutive voxels (UMMA M = 128)
-// and every output channel (N = COUTP, a multiple of 16, at most 96 here); the FP32 accumulator
-// lives in tensor memory, 128 lanes x N columns.  K runs over taps x input channels: per tap
-// all threads gather the 128 voxels' shifted input rows (cp.async, 16 bytes = 8 channels, zero
-// fill past the last voxel) and the tap's weights [COUTP][CIN] into shared memory in the
-// canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk c
-// at c * LBO + (r / 8) * 128 + (r % 8) * 16), then one thread issues CIN / 16 tcgen05.mma
-// (kind::f16: BF16 A and B, FP32 accumulate) with shared-memory descriptors of both operands and
-// commits them to the stage's mbarrier.  Up to four stages, the MMAs of a tap issued two taps
-// after its gathers (so later taps' gathers are in flight while the tensor core works); a stage
-// is refilled only after its mbarrier shows the MMAs that read it complete.  The
-// epilogue loads the accumulator with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31, the
-// rows of its 32 voxels), adds the bias, applies ReLU and stores.  Every mbarrier wait is
-// bounded: on a timeout the CTA stops issuing, waits (bounded) for what it issued, raises *err,
-// skips the stores and still frees its tensor memory.
-constexpr int kTcRows = 128;             // voxels per CTA (UMMA M)
+// The same implicit GEMM as k_conv, tiled over HALOED positions: a CTA of 4 warps owns 128
+// consecutive positions p0 .. p0 + 127 of the zero-haloed channels-last input (UMMA M = 128) and
+// every output channel (N = COUTP, a multiple of 16); the FP32 accumulator lives in tensor
+// memory, 128 lanes x N columns.  Tap (dz, dy, dx) of output row m reads the input at position
+// p0 + m + dz sz + dy sy + dx (sy = W + 2, sz = (H + 2) sy), so for one dz the 9 taps' A operands
+// are 128-row windows, dy sy + dx rows apart, of ONE slab of 128 + 2 (sy + 1) consecutive input
+// rows.  Per dz all threads copy that slab (cp.async, 16 bytes = 8 channels, zero fill outside
+// the tensor) and the 9 taps' weights [tap][COUTP][CIN] into shared memory in the canonical
+// K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk c at
+// c * LBO + r * 16, so a window starting at any row is again such a matrix), then one thread
+// issues 9 x CIN / 16 tcgen05.mma (kind::f16: BF16 A and B, FP32 accumulate) whose A descriptors
+// start at the tap's row, and commits them to the buffer's mbarrier: 3 slabs instead of 27
+// gathered tap tiles.  Two buffers: slab i + 1 is copied while the MMAs of slab i run; a buffer is
+// refilled only after its mbarrier shows the MMAs that read it complete.  A 1x1x1 convolution
+// is one slab of 128 rows.  Outputs at halo positions are computed and discarded.  The epilogue
+// loads the accumulator with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31, the rows of its
+// 32 positions), adds the bias, applies ReLU and stores the interior positions.  Every mbarrier
+// wait is bounded: on a timeout the CTA stops issuing, waits (bounded) for what it issued,
+// raises *err, skips the stores and still frees its tensor memory.
+constexpr int kTcRows = 128;             // haloed positions per CTA (UMMA M)
 constexpr uint32_t kTcPolls = 1u << 22;  // bounded mbarrier polls (about half a second)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -277,157 +281,95 @@ constexpr int tc_tmem_cols() {
     return COUTP <= 32 ? 32 : (COUTP <= 64 ? 64 : (COUTP <= 128 ? 128 : 256));
 }
 
-template <int CIN, int COUTP>
-constexpr uint32_t tc_stage_bytes() {
-    return uint32_t(kTcRows) * CIN * 2 + uint32_t(COUTP) * CIN * 2;
+// Row stride of a staged slab: at least its rows, chosen modulo 8 so that the 16-byte chunks
+// that 8 consecutive threads copy (a row's CIN / 8 chunks, then the next row's) fall in distinct
+// 128-byte bank groups.
+inline int tc_row_stride(int nrows, int cin8) {
+    const int want = cin8 == 2 ? 4 : (cin8 == 4 ? 2 : 7);
+    return nrows + ((want - nrows % 8) + 8) % 8;
 }
 
-// Taps per pipeline stage: 3 when three taps' operands take at most 18 KB (the narrow layers, where
-// one tap is too little work per barrier), else 1; a single-tap (1x1x1) convolution uses 1.
-template <int CIN, int COUTP, int TAPS>
-constexpr int tc_group() {
-    return (TAPS % 3 == 0 && 3u * tc_stage_bytes<CIN, COUTP>() <= 18u * 1024u) ? 3 : 1;
-}
-
-// Pipeline depth: up to 4 shared-memory stages (3 or 2 for the widest ones) and the MMAs of a
-// stage issued tc_lag(S) stages after its gathers, so that several stages' gathers are in flight.
-template <int CIN, int COUTP, int TAPS>
-constexpr int tc_stages() {
-    return tc_group<CIN, COUTP, TAPS>() > 1 ? 2
-           : uint32_t(tc_group<CIN, COUTP, TAPS>()) * tc_stage_bytes<CIN, COUTP>() <= 18u * 1024u
-               ? 4
-               : (uint32_t(tc_group<CIN, COUTP, TAPS>()) * tc_stage_bytes<CIN, COUTP>() <= 24u * 1024u ? 3 : 2);
-}
-constexpr int tc_lag(int stages) { return stages / 2; }
-
-// Dynamic shared memory per CTA: the stages, raised so that no more CTAs fit on an SM than its
-// 512 TMEM columns hold (an allocation beyond them would wait for another CTA's release).
-template <int CIN, int COUTP, int TAPS>
-constexpr uint32_t tc_smem_bytes() {
-    constexpr uint32_t stages = uint32_t(tc_stages<CIN, COUTP, TAPS>()) * uint32_t(tc_group<CIN, COUTP, TAPS>()) *
-                                tc_stage_bytes<CIN, COUTP>();
-    constexpr uint32_t per_cta = (227u * 1024u) / (512u / tc_tmem_cols<COUTP>()) + 1024u;
-    return stages > per_cta ? stages : per_cta;
-}
+// Launch geometry of k_conv_tc, chosen on the host.  Positions are haloed indices of the input
+// (and output) grid, below 2^31.
+struct TcGeom {
+    int32_t pfirst, plast, ptotal;  // first and last interior position, all positions
+    int32_t ntiles;                 // 128-position tiles from pfirst to plast
+    int32_t rows;                   // slab row stride (>= the rows one slab gathers)
+    int32_t nbuf;                   // slab buffers in the pipeline (2 to 4)
+    int32_t wres;                   // 1: all taps' weights stay in shared memory; 0: staged per slab
+    uint32_t w_bytes;               // shared memory of the resident weights (0 when staged)
+    uint32_t buf_bytes;             // one slab buffer (with its taps' weights when staged)
+};
 
 template <int CIN, int COUT, int TAPS, bool RELU, bool OUT_F32, bool ACCUM>
 __global__ void __launch_bounds__(128)
-k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TView out, int64_t nvox,
+k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TView out, TcGeom g,
           int* __restrict__ err) {
     constexpr int COUTP = (COUT + 15) / 16 * 16;
     static_assert(CIN % 16 == 0 && COUTP <= 256, "UMMA shape");
-    constexpr int TMEM_COLS = tc_tmem_cols<COUTP>();
-    constexpr int G = tc_group<CIN, COUTP, TAPS>(), NG = TAPS / G;  // taps per stage, stages' worth of taps
-    constexpr int S = tc_stages<CIN, COUTP, TAPS>(), LAG = tc_lag(S);
-    constexpr uint32_t A_BYTES = uint32_t(kTcRows) * CIN * 2;
-    constexpr uint32_t TAPB = tc_stage_bytes<CIN, COUTP>();  // one tap's A and B
-    constexpr uint32_t STAGE = G * TAPB;
-    constexpr uint32_t LBO_A = (kTcRows / 8) * 128;  // bytes between the K-chunks of A
+    constexpr int NDZ = TAPS == 27 ? 3 : 1, TPD = TAPS / NDZ;  // slabs (z offsets) per tile, taps per slab
+    constexpr int ACC_COLS = tc_tmem_cols<COUTP>();            // one accumulator; two are allocated
+    constexpr uint32_t BTAP = uint32_t(COUTP) * CIN * 2;       // one tap's weights
     constexpr uint32_t LBO_B = (COUTP / 8) * 128;
     constexpr uint32_t IDESC = umma_idesc_bf16_f32<COUTP>();
+    const uint32_t LBO_A = uint32_t(g.rows) * 16u;  // bytes between the 8-channel chunks of a slab row
+    const uint32_t A_BYTES = uint32_t(g.rows) * CIN * 2;
     extern __shared__ __align__(128) uint8_t tc_smem[];
-    __shared__ __align__(8) uint64_t bar[S + 1];  // MMA completion per stage; all MMAs
+    // mbarriers: MMA completion per slab buffer (4), per accumulator (2), all MMAs (1)
+    __shared__ __align__(8) uint64_t bar[7];
     __shared__ uint32_t tmem_slot;
+    __shared__ float sbias[COUTP];
     const int tid = threadIdx.x, warp = tid >> 5;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(TMEM_COLS)
+                     "r"(2 * ACC_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int q = 0; q <= S; ++q) mbar_init(&bar[q], 1);
+        for (int q = 0; q < 7; ++q) mbar_init(&bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int c = tid; c < COUTP; c += 128) sbias[c] = (bias && c < COUT) ? bias[c] : 0.f;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const int64_t v = int64_t(blockIdx.x) * kTcRows + tid;  // this thread's voxel row
-    const bool row_ok = v < nvox;
+    const int32_t sy = in.W + 2, sz = (in.H + 2) * sy;
+    const int halo = TAPS == 27 ? sy + 1 : 0;
+    const int nrows = kTcRows + 2 * halo;  // slab rows gathered
+    const int nbuf = g.nbuf, lag = g.nbuf - 1;
+    const int my_tiles = (g.ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x);
+    const int nslabs = my_tiles * NDZ;
     const bf16* __restrict__ ip = static_cast<const bf16*>(in.p);
-    const int64_t hrow = row_ok ? halo_index(in, v) : 0;
-    const int64_t sy = in.W + 2, sz = int64_t(in.H + 2) * (in.W + 2);
-    const uint32_t sbase = smem_u32(tc_smem);
-    const uint32_t arow = uint32_t(tid >> 3) * 128u + uint32_t(tid & 7) * 16u;
-    bool ok = true;
-    int issued = 0;
-    // iteration i gathers tap group i (taps G i .. G i + G - 1, when i < NG) and issues the MMAs
-    // of group i - LAG
-    for (int i = 0; i < NG + LAG; ++i) {
-        if (i < NG) {
-            const int st = i % S;
-            if (i >= S) {  // the MMAs of group i - S (issued LAG iterations after it) have read this stage
-                bool w = true;
-                if (tid == 0) w = mbar_wait(&bar[st], uint32_t((i - S) / S) & 1u);
-                ok = __syncthreads_and(w) != 0;
-                if (!ok) break;
-            }
-#pragma unroll
-            for (int gq = 0; gq < G; ++gq) {
-                const int t = G * i + gq;
-                const uint32_t a_s = sbase + uint32_t(st) * STAGE + uint32_t(gq) * TAPB, b_s = a_s + A_BYTES;
-                int64_t o = 0;
-                if (TAPS == 27) o = (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1);
-                const bf16* src = row_ok ? ip + (hrow + o) * in.ld + in.c0 : ip;
-#pragma unroll
-                for (int c8 = 0; c8 < CIN / 8; ++c8)  // L1-allocating: neighbouring taps re-read these rows
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(a_s + uint32_t(c8) * LBO_A + arow),
-                                 "l"(row_ok ? src + 8 * c8 : ip), "r"(row_ok ? 16u : 0u)
-                                 : "memory");
-                const bf16* wt = Wt + int64_t(t) * COUTP * CIN;
-                for (int q = tid; q < COUTP * (CIN / 8); q += 128) {
-                    const int n = q / (CIN / 8), c8 = q - n * (CIN / 8);
-                    cp_async16(b_s + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u,
-                               wt + n * CIN + 8 * c8, 16u);
-                }
-            }
+    const uint32_t sbase = smem_u32(tc_smem), wbase = sbase, bbase = sbase + g.w_bytes;
+
+    // epilogue of the k-th tile of this CTA from accumulator k & 1: bias, ReLU, store the
+    // interior positions (all threads; thread t owns TMEM lane t = the tile's row t)
+    auto epilogue = [&](int k) {
+        const int32_t p = g.pfirst + (int(blockIdx.x) + k * int(gridDim.x)) * kTcRows + tid;
+        bool row_ok = p <= g.plast;
+        if (row_ok) {
+            uint32_t t = uint32_t(p);
+            const uint32_t x = t % uint32_t(sy);
+            t /= uint32_t(sy);
+            const uint32_t y = t % uint32_t(in.H + 2);
+            t /= uint32_t(in.H + 2);
+            const uint32_t z = t % uint32_t(in.D + 2);
+            row_ok = x >= 1u && x <= uint32_t(in.W) && y >= 1u && y <= uint32_t(in.H) && z >= 1u && z <= uint32_t(in.D);
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");  // one group per iteration (empty past NG)
-        if (i >= LAG) {
-            const int gm = i - LAG;  // the groups of the last LAG iterations may stay in flight
-            asm volatile("cp.async.wait_group %0;" ::"n"(LAG) : "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core
-            __syncthreads();
-            if (tid == 0) {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-                for (int gq = 0; gq < G; ++gq) {
-                    const uint32_t a_s = sbase + uint32_t(gm % S) * STAGE + uint32_t(gq) * TAPB, b_s = a_s + A_BYTES;
-#pragma unroll
-                    for (int kc = 0; kc < CIN / 16; ++kc)
-                        umma_bf16(tmem, umma_smem_desc(a_s + 2u * kc * LBO_A, LBO_A, 128u),
-                                  umma_smem_desc(b_s + 2u * kc * LBO_B, LBO_B, 128u), IDESC,
-                                  (gm > 0 || gq > 0 || kc > 0) ? 1u : 0u);
-                }
-                umma_commit(&bar[gm % S]);
-            }
-            ++issued;
-        }
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into shared memory outlives the loop
-    // all issued MMAs complete (bounded even after a timeout above)
-    bool fin = true;
-    if (tid == 0) {
-        if (issued > 0) umma_commit(&bar[S]);
-        fin = issued == 0 || mbar_wait(&bar[S], 0u);
-    }
-    const bool good = __syncthreads_and(ok && fin) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (good) {
-        const int64_t obase = row_ok ? halo_index(out, v) * out.ld + out.c0 : 0;
+        const int64_t obase = int64_t(p) * out.ld + out.c0;
+        const uint32_t acc = tmem + (uint32_t(32 * warp) << 16) + uint32_t((k & 1) * ACC_COLS);
 #pragma unroll
         for (int c0 = 0; c0 < COUTP; c0 += 16) {
             uint32_t r[16];
-            tmem_ld16(tmem + (uint32_t(32 * warp) << 16) + uint32_t(c0), r);
+            tmem_ld16(acc + uint32_t(c0), r);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (!row_ok) continue;
             float y[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-                const int c = c0 + j;
-                y[j] = __uint_as_float(r[j]);
-                if (bias && c < COUT) y[j] += bias[c];
+                y[j] = __uint_as_float(r[j]) + sbias[c0 + j];
                 if (RELU) y[j] = fmaxf(y[j], 0.f);
             }
             if (OUT_F32) {
@@ -464,13 +406,102 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
                 }
             }
         }
+        // the accumulator is rewritten two tiles later, by MMAs issued after a barrier
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    };
+
+    bool ok = true;
+    int issued = 0;
+    // iteration i copies slab i (tile i / NDZ of this CTA, z offset i % NDZ - 1) into buffer
+    // i % nbuf and issues the MMAs of slab i - lag (lag = nbuf - 1); a buffer is refilled once the
+    // MMAs of the slab it held, issued in the previous iteration, have completed
+    for (int i = 0; i < nslabs + lag; ++i) {
+        if (i < nslabs) {
+            const int b = i % nbuf;
+            if (i >= nbuf) {
+                bool w = true;
+                if (tid == 0) w = mbar_wait(&bar[b], uint32_t((i - nbuf) / nbuf) & 1u);
+                ok = __syncthreads_and(w) != 0;
+                if (!ok) break;
+            }
+            const int k = i / NDZ, dzi = i - k * NDZ;
+            const int32_t p0 = g.pfirst + (int(blockIdx.x) + k * int(gridDim.x)) * kTcRows;
+            const int32_t r0 = p0 + (NDZ == 3 ? (dzi - 1) * sz : 0) - halo;  // position of slab row 0
+            const uint32_t a_s = bbase + uint32_t(b) * g.buf_bytes;
+            for (int q = tid; q < nrows * (CIN / 8); q += 128) {  // consecutive threads: one row's chunks
+                const int r = q / (CIN / 8), c8 = q - r * (CIN / 8);
+                const int32_t pos = r0 + r;
+                const bool inside = pos >= 0 && pos < g.ptotal;  // rows outside feed discarded outputs only
+                cp_async16(a_s + uint32_t(c8) * LBO_A + uint32_t(r) * 16u,
+                           inside ? ip + int64_t(pos) * in.ld + in.c0 + 8 * c8 : ip, inside ? 16u : 0u);
+            }
+            // weights [tap][COUTP][CIN]: every tap once (resident), or this slab's taps per buffer
+            const int wt0 = g.wres ? 0 : dzi * TPD, nw = g.wres ? (i == 0 ? TAPS : 0) : TPD;
+            const uint32_t w_s = g.wres ? wbase : a_s + A_BYTES;
+            for (int q = tid; q < nw * COUTP * (CIN / 8); q += 128) {
+                const int j = q / (COUTP * (CIN / 8)), rem = q - j * (COUTP * (CIN / 8));
+                const int n = rem / (CIN / 8), c8 = rem - n * (CIN / 8);
+                cp_async16(w_s + uint32_t(j) * BTAP + uint32_t(c8) * LBO_B + uint32_t(n >> 3) * 128u + uint32_t(n & 7) * 16u,
+                           Wt + (int64_t(wt0 + j) * COUTP + n) * CIN + 8 * c8, 16u);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");  // one group per iteration (empty past the last slab)
+        if (i >= lag) {
+            const int s = i - lag, b = s % nbuf, k = s / NDZ, dzi = s - k * NDZ;
+            // slab s is in; the lag - 1 later ones may still be in flight
+            if (lag == 1) asm volatile("cp.async.wait_group 0;" ::: "memory");
+            else if (lag == 2) asm volatile("cp.async.wait_group 1;" ::: "memory");
+            else asm volatile("cp.async.wait_group 2;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_s = bbase + uint32_t(b) * g.buf_bytes;
+                const uint32_t w_s = g.wres ? wbase + uint32_t(dzi * TPD) * BTAP : a_s + A_BYTES;
+                const uint32_t d = tmem + uint32_t((k & 1) * ACC_COLS);
+#pragma unroll 1
+                for (int j = 0; j < TPD; ++j) {
+                    // tap (dz, dy, dx): its 128 rows start dy sy + dx rows from the slab's centre window
+                    const int dy = TPD == 9 ? j / 3 - 1 : 0, dx = TPD == 9 ? j % 3 - 1 : 0;
+                    const uint32_t a_t = a_s + uint32_t(halo + dy * sy + dx) * 16u;
+#pragma unroll
+                    for (int kc = 0; kc < CIN / 16; ++kc)
+                        umma_bf16(d, umma_smem_desc(a_t + 2u * kc * LBO_A, LBO_A, 128u),
+                                  umma_smem_desc(w_s + uint32_t(j) * BTAP + 2u * kc * LBO_B, LBO_B, 128u), IDESC,
+                                  (dzi > 0 || j > 0 || kc > 0) ? 1u : 0u);
+                }
+                umma_commit(&bar[b]);
+                if (dzi == NDZ - 1) umma_commit(&bar[4 + (k & 1)]);  // tile k's accumulator is complete
+            }
+            ++issued;
+            if (dzi == 0 && k >= 1) {  // tile k's first MMAs are queued: store tile k - 1 meanwhile
+                bool w = true;
+                if (tid == 0) w = mbar_wait(&bar[4 + ((k - 1) & 1)], uint32_t((k - 1) >> 1) & 1u);
+                ok = __syncthreads_and(w) != 0;
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                epilogue(k - 1);
+            }
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into shared memory outlives the loop
+    // all issued MMAs complete (bounded even after a timeout above)
+    bool fin = true;
+    if (tid == 0) {
+        if (issued > 0) umma_commit(&bar[6]);
+        fin = issued == 0 || mbar_wait(&bar[6], 0u);
+    }
+    const bool good = __syncthreads_and(ok && fin) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (good) {
+        if (my_tiles > 0) epilogue(my_tiles - 1);
     } else if (tid == 0) {
         atomicExch(err, 1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACC_COLS) : "memory");
 }
 
 // ---- weight gradient --------------------------------------------------------------------
@@ -929,17 +960,82 @@ struct ConvPath {
     int* err;  // device flag raised by a tcgen05 CTA whose bounded wait ran out
 };
 
+int sm_count() {
+    static const int n = [] {
+        int dev = 0, v = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            v = 148;
+        return v;
+    }();
+    return n;
+}
+
+// Shared memory and pipeline of a k_conv_tc launch with slab row stride `rows`: every tap's
+// weights stay resident when they fit beside two slab buffers (else each buffer carries its
+// slab's 9 taps); then the buffer count (2 to 4) that keeps the most slab copies in flight per
+// SM, resident CTAs x (buffers - 1), fewer buffers on a tie.  The dynamic shared memory is
+// raised so that no more CTAs fit on an SM than its 512 TMEM columns hold (a CTA beyond them
+// would wait in tcgen05.alloc for a persistent CTA to end).  False when no form fits.
+template <int CIN, int COUTP, int TAPS>
+bool tc_plan(int rows, TcGeom& g, uint32_t& smem, int& ctas_per_sm) {
+    constexpr int TPD = TAPS == 27 ? 9 : 1;
+    constexpr uint32_t BTAP = uint32_t(COUTP) * CIN * 2;
+    constexpr uint32_t kMaxDyn = 227u * 1024u - 1280u;  // the opt-in limit less the static mbarriers and bias
+    constexpr uint32_t kSmPerSm = 228u * 1024u, kPerCtaExtra = 1024u + 1280u;  // reserved + static per CTA
+    constexpr int tmem_ctas = 512 / (2 * tc_tmem_cols<COUTP>());
+    auto r128 = [](uint32_t v) { return (v + 127u) & ~127u; };
+    const uint32_t a = r128(uint32_t(rows) * CIN * 2), wall = r128(uint32_t(TAPS) * BTAP);
+    const bool wres = wall + 2u * a <= kMaxDyn;
+    const uint32_t wb = wres ? wall : 0u, buf = wres ? a : r128(a + uint32_t(TPD) * BTAP);
+    const uint32_t guard = (227u * 1024u) / uint32_t(tmem_ctas) + 1024u;
+    int best = 0;
+    for (int nb = 2; nb <= 4; ++nb) {
+        const uint32_t need = std::max(wb + uint32_t(nb) * buf, guard);
+        if (need > kMaxDyn) break;
+        const int occ = std::min<int>(tmem_ctas, int(kSmPerSm / (need + kPerCtaExtra)));
+        if (occ * (nb - 1) > best) {
+            best = occ * (nb - 1);
+            g.nbuf = nb;
+            smem = need;
+            ctas_per_sm = occ;
+        }
+    }
+    if (best == 0) return false;
+    g.rows = rows;
+    g.wres = wres ? 1 : 0;
+    g.w_bytes = wb;
+    g.buf_bytes = buf;
+    return true;
+}
+
 // launch helpers (dispatch on the layer's channel counts)
 template <int CIN, int COUT, int TAPS, bool RELU, bool F32, bool ACC>
 int conv_launch(cudaStream_t s, const ConvPath& P, TView in, const bf16* w, const float* b, TView out, int64_t nvox) {
+    if (nvox <= 0) return PLATO_OK;
+    if (in.B != out.B || in.D != out.D || in.H != out.H || in.W != out.W)
+        return fail(PLATO_BAD_INPUT, "convolution input and output grids differ");
     if (P.kind == PLATO_UNET_CONV_TCGEN05) {
         constexpr int COUTP = (COUT + 15) / 16 * 16;
-        constexpr uint32_t smem = tc_smem_bytes<CIN, COUTP, TAPS>();
-        auto kernel = k_conv_tc<CIN, COUT, TAPS, RELU, F32, ACC>;
-        UCUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        kernel<<<int((nvox + kTcRows - 1) / kTcRows), 128, smem, s>>>(in, w, b, out, nvox, P.err);
-        ULAUNCH();
-        return PLATO_OK;
+        const int64_t sy = in.W + 2, sz = int64_t(in.H + 2) * sy;
+        const int64_t ptotal = int64_t(in.B) * (in.D + 2) * sz;
+        const int nrows = kTcRows + (TAPS == 27 ? 2 * int(sy + 1) : 0);
+        TcGeom g{};
+        uint32_t smem = 0;
+        int ctas_per_sm = 0;
+        // positions index in 32 bits; a slab too long for shared memory (a grid row of more than
+        // about 140 voxels on the widest layers) takes the mma.sync kernel
+        if (ptotal < (int64_t(1) << 31) && tc_plan<CIN, COUTP, TAPS>(tc_row_stride(nrows, CIN / 8), g, smem, ctas_per_sm)) {
+            g.pfirst = int32_t(sz + sy + 1);
+            g.plast = int32_t(halo_index(in, nvox - 1));
+            g.ptotal = int32_t(ptotal);
+            g.ntiles = (g.plast - g.pfirst) / kTcRows + 1;
+            auto kernel = k_conv_tc<CIN, COUT, TAPS, RELU, F32, ACC>;
+            UCUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+            const int grid = int(std::min<int64_t>(g.ntiles, int64_t(sm_count()) * ctas_per_sm));
+            kernel<<<grid, 128, smem, s>>>(in, w, b, out, g, P.err);
+            ULAUNCH();
+            return PLATO_OK;
+        }
     }
     const int64_t per = kConvWarps * 16 * kMT;
     k_conv<CIN, COUT, TAPS, RELU, F32, ACC><<<int((nvox + per - 1) / per), kConvWarps * 32, 0, s>>>(in, w, b, out, nvox);

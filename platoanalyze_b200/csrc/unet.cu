@@ -505,10 +505,18 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
 }
 
 // ---- weight gradient --------------------------------------------------------------------
-// dW[t][co][ci] += sum_v dy[v][co] x[v + o_t][ci]; grid (voxel chunks, TAPS).
-constexpr int kWgVox = 64;    // voxels per shared-memory tile
-constexpr int kWgCtas = 148 * 16;  // CTAs over all taps: each sums a long run of voxel tiles, so
-                                   // few CTAs add their partial weight gradients to one entry
+// dW[t][co][ci] += sum_p dy[p][co] x[p + o_t][ci] over the interior haloed positions p (dy is
+// read as zero elsewhere; x's halo holds zeros).  Grid (CTAs per tap group, G tap groups): a CTA
+// owns TAPS / G consecutive taps and loops over 128-position tiles (tile = blockIdx.x + k gridDim.x).
+// Per tile it stages the tile's dy rows and, per z offset of its taps, one slab of x rows that
+// every tap of that z offset reads at a shifted row (cp.async, double-buffered: the next tile's
+// copies are in flight while this tile's MMAs run).  Warps own output tiles (tap, 16 co, 8 ci)
+// and keep their sums in registers over all of the CTA's tiles: mma.sync m16n8k16 with A = dy^T
+// and B = x, both through ldmatrix.trans (one A fragment per k-step serves every tap).  One
+// atomic add per output element and CTA at the end.  (The tensor-core MMA of tcgen05 needs M >= 64
+// rows of one operand at a uniform shared-memory stride; here M is 16 output channels, and the
+// taps that would fill it read the slab at non-uniform shifts.)
+constexpr int kWgRows = 128;  // positions per tile (8 k-steps)
 
 __device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const bf16* p) {
     const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -521,24 +529,64 @@ __device__ __forceinline__ void ldsm_x2_t(uint32_t& r0, uint32_t& r1, const bf16
     asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(a));
 }
 
+// tap groups of a weight-gradient launch: the fewest (1, 3, 9 or 27) that leave each warp at most
+// 18 output tiles (72 FP32 sums in registers)
 template <int CIN, int COUT, int TAPS>
+constexpr int wg_groups() {
+    if (TAPS == 1) return 1;
+    constexpr int per_tap = (COUT / 16) * (CIN / 8);
+    return (27 * per_tap + 3) / 4 <= 18 ? 1 : (9 * per_tap + 3) / 4 <= 18 ? 3 : (3 * per_tap + 3) / 4 <= 18 ? 9 : 27;
+}
+
+// offset of tap t of a 3x3x3 stencil in haloed positions
+__host__ __device__ __forceinline__ int wg_tap_offset(int t, int sy, int sz) {
+    return (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1);
+}
+
+// half-width (rows) of the x slab of a tap group: all 9 taps of a z offset, 3 taps of a row, one tap
+template <int TAPS, int G>
+__host__ __device__ __forceinline__ int wg_halfwidth(int sy) {
+    return TAPS == 1 ? 0 : (G <= 3 ? sy + 1 : (G == 9 ? 1 : 0));
+}
+
+template <int CIN, int COUT, int TAPS, int G>
 __global__ void __launch_bounds__(128)
-k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t nvox, int tiles) {
-    static_assert(COUT % 16 == 0 && CIN % 8 == 0, "channel counts");
-    constexpr int LDY = COUT + 8, LDX = CIN + 8;  // padded rows: 16-byte aligned, no bank conflicts
-    constexpr int TILES = (COUT / 16) * (CIN / 8);
-    // with only two 16 x 8 output tiles (16 -> 16 channels), pairs of warps share a tile and split
-    // its k-steps (even / odd), so all four warps work; each adds its own partial sums
-    constexpr int KSPLIT = TILES <= 2 ? 2 : 1;
-    constexpr int WPT = 4 / KSPLIT;  // warps per k-group
-    constexpr int PER = (TILES + WPT - 1) / WPT;
-    __shared__ __align__(16) bf16 sy[kWgVox * LDY];
-    __shared__ __align__(16) bf16 sx[kWgVox * LDX];
-    const int t = blockIdx.y;
+k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int32_t pfirst, int32_t plast, int32_t ptotal,
+             int32_t ntiles, int rows_pad, uint32_t stage_elems) {
+    static_assert(COUT % 16 == 0 && CIN % 16 == 0, "channel counts");
+    constexpr int TPG = TAPS / G;                         // taps of this CTA
+    constexpr int NSL = (TAPS == 27 && G == 1) ? 3 : 1;   // x slabs per tile (one per z offset)
+    constexpr int LDY = COUT + 8, LDX = CIN + 8;          // padded rows: 16-byte aligned, no ldmatrix conflicts
+    constexpr int T = TPG * (COUT / 16) * (CIN / 8);      // output tiles of 16 x 8
+    // with at most two output tiles (the 1x1x1 head), pairs of warps share a tile and split its
+    // k-steps (even / odd), so all four warps work; each adds its own partial sums
+    constexpr int KSPLIT = T <= 2 ? 2 : 1;
+    constexpr int WPT = 4 / KSPLIT;
+    constexpr int PER = (T + WPT - 1) / WPT;
+    extern __shared__ __align__(16) bf16 wg_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wt = warp % WPT, kg = warp / WPT;
-    const int64_t sz = int64_t(x.H + 2) * (x.W + 2), syy = x.W + 2;
-    const int64_t o = TAPS == 27 ? ((t / 9 - 1) * sz + ((t / 3) % 3 - 1) * syy + (t % 3 - 1)) : 0;
+    const int g = blockIdx.y;
+    const int32_t sy = x.W + 2, sz = (x.H + 2) * sy;
+    const int hw = wg_halfwidth<TAPS, G>(sy);
+    const int srows = kWgRows + 2 * hw;  // rows of one slab (rows_pad >= srows is their stride)
+    // slab centre offsets: the middle tap of each z offset (G = 1), else of the group
+    int32_t centre[NSL];
+#pragma unroll
+    for (int sl = 0; sl < NSL; ++sl)
+        centre[sl] = TAPS == 1 ? 0 : wg_tap_offset(NSL == 3 ? 9 * sl + 4 : g * TPG + TPG / 2, sy, sz);
+    // this warp's output tiles: element offset of its B rows (k-step 0, lane's row) and its A block
+    int boff[PER], mtile[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int id = wt + WPT * k;
+        const int j = id / ((COUT / 16) * (CIN / 8)), rem = id - j * ((COUT / 16) * (CIN / 8));
+        const int mt = rem / (CIN / 8), nt = rem - mt * (CIN / 8);
+        const int sl = NSL == 3 ? j / 9 : 0;
+        const int rel = TAPS == 1 ? 0 : wg_tap_offset(g * TPG + j, sy, sz) - centre[sl];
+        boff[k] = (kWgRows * LDY) + (sl * rows_pad + hw + rel + (lane & 7) + ((lane >> 3) & 1) * 8) * LDX + 8 * nt;
+        mtile[k] = mt;
+    }
     float acc[PER][4];
 #pragma unroll
     for (int k = 0; k < PER; ++k)
@@ -546,63 +594,87 @@ k_conv_wgrad(TView x, TView dy, float* __restrict__ dW, int cout_real, int64_t n
         for (int q = 0; q < 4; ++q) acc[k][q] = 0.f;
     const bf16* __restrict__ yp = static_cast<const bf16*>(dy.p);
     const bf16* __restrict__ xp = static_cast<const bf16*>(x.p);
-    for (int tile = 0; tile < tiles; ++tile) {
-        const int64_t v0 = (int64_t(blockIdx.x) * tiles + tile) * kWgVox;
-        if (v0 >= nvox) break;
-        // stage: 16-byte vectors of 8 channels
-        for (int q = threadIdx.x; q < kWgVox * (COUT / 8); q += blockDim.x) {
-            const int r = q / (COUT / 8), c8 = q % (COUT / 8);
-            const int64_t v = v0 + r;
-            uint4 val = make_uint4(0, 0, 0, 0);
-            if (v < nvox) val = *reinterpret_cast<const uint4*>(yp + halo_index(dy, v) * dy.ld + dy.c0 + 8 * c8);
-            *reinterpret_cast<uint4*>(sy + r * LDY + 8 * c8) = val;
+    const int my_tiles = (ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x);
+    const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(wg_smem));
+
+    // copies of tile k into stage buf: dy rows (zero outside the interior), then the x slabs
+    auto stage = [&](int k, int buf) {
+        const int32_t p0 = pfirst + (int(blockIdx.x) + k * int(gridDim.x)) * kWgRows;
+        const uint32_t st = sbase + uint32_t(buf) * stage_elems * 2u;
+        for (int q = threadIdx.x; q < kWgRows * (COUT / 8); q += 128) {
+            const int r = q / (COUT / 8), c8 = q - r * (COUT / 8);
+            const int32_t p = p0 + r;
+            bool in = p <= plast;
+            if (in) {
+                uint32_t t = uint32_t(p);
+                const uint32_t xx = t % uint32_t(sy);
+                t /= uint32_t(sy);
+                const uint32_t yy = t % uint32_t(x.H + 2);
+                t /= uint32_t(x.H + 2);
+                const uint32_t zz = t % uint32_t(x.D + 2);
+                in = xx >= 1u && xx <= uint32_t(x.W) && yy >= 1u && yy <= uint32_t(x.H) && zz >= 1u && zz <= uint32_t(x.D);
+            }
+            cp_async16(st + uint32_t(r * LDY + 8 * c8) * 2u, in ? yp + int64_t(p) * dy.ld + dy.c0 + 8 * c8 : yp,
+                       in ? 16u : 0u);
         }
-        for (int q = threadIdx.x; q < kWgVox * (CIN / 8); q += blockDim.x) {
-            const int r = q / (CIN / 8), c8 = q % (CIN / 8);
-            const int64_t v = v0 + r;
-            uint4 val = make_uint4(0, 0, 0, 0);
-            if (v < nvox)
-                val = *reinterpret_cast<const uint4*>(xp + (halo_index(x, v) + o) * x.ld + x.c0 + 8 * c8);
-            *reinterpret_cast<uint4*>(sx + r * LDX + 8 * c8) = val;
-        }
-        __syncthreads();
 #pragma unroll
-        for (int ks = 0; ks < kWgVox / 16; ++ks) {
-            if (ks % KSPLIT != kg) continue;
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int tid = wt + WPT * k;
-                if (tid >= TILES) break;
-                const int m0 = 16 * (tid / (CIN / 8)), n0 = 8 * (tid % (CIN / 8));
-                // A = dy^T (rows co, cols voxel): matrices (m0, k0), (m0+8, k0), (m0, k0+8), (m0+8, k0+8)
-                const int mat = lane >> 3, rr = lane & 7;
-                const int krow = 16 * ks + rr + ((mat & 2) ? 8 : 0);
-                const int mcol = m0 + ((mat & 1) ? 8 : 0);
-                uint32_t a[4];
-                ldsm_x4_t(a, sy + krow * LDY + mcol);
-                // B = x (rows voxel, cols ci): matrices (k0, n0), (k0+8, n0)
-                const int krow2 = 16 * ks + (lane & 7) + ((lane >> 3) & 1) * 8;
-                uint32_t b0, b1;
-                ldsm_x2_t(b0, b1, sx + krow2 * LDX + n0);
-                mma16816(acc[k], a, b0, b1);
+        for (int sl = 0; sl < NSL; ++sl) {
+            const int32_t r0 = p0 + centre[sl] - hw;
+            const uint32_t xs = st + uint32_t(kWgRows * LDY + sl * rows_pad * LDX) * 2u;
+            for (int q = threadIdx.x; q < srows * (CIN / 8); q += 128) {
+                const int r = q / (CIN / 8), c8 = q - r * (CIN / 8);
+                const int32_t pos = r0 + r;
+                const bool in = pos >= 0 && pos < ptotal;
+                cp_async16(xs + uint32_t(r * LDX + 8 * c8) * 2u, in ? xp + int64_t(pos) * x.ld + x.c0 + 8 * c8 : xp,
+                           in ? 16u : 0u);
             }
         }
+    };
+
+    if (my_tiles > 0) stage(0, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int k = 0; k < my_tiles; ++k) {
+        if (k + 1 < my_tiles) stage(k + 1, (k + 1) & 1);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");  // tile k is in; tile k + 1 may be in flight
         __syncthreads();
-    }
-    const int g = lane >> 2, tig = lane & 3;
+        const bf16* sb = wg_smem + size_t(k & 1) * stage_elems;
 #pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int tid = wt + WPT * k;
-        if (tid >= TILES) break;
-        const int m0 = 16 * (tid / (CIN / 8)), n0 = 8 * (tid % (CIN / 8));
-        float* w = dW + int64_t(t) * cout_real * CIN;  // rows past the real output channels are padding
-        if (m0 + g < cout_real) {
-            atomicAdd(w + (m0 + g) * CIN + n0 + 2 * tig, acc[k][0]);
-            atomicAdd(w + (m0 + g) * CIN + n0 + 2 * tig + 1, acc[k][1]);
+        for (int ks = 0; ks < kWgRows / 16; ++ks) {
+            if (ks % KSPLIT != kg) continue;
+            // A = dy^T (rows co, cols position): matrices (m0, k0), (m0+8, k0), (m0, k0+8), (m0+8, k0+8)
+            uint32_t a[COUT / 16][4];
+            const int mat = lane >> 3, rr = lane & 7;
+#pragma unroll
+            for (int mt = 0; mt < COUT / 16; ++mt)
+                ldsm_x4_t(a[mt], sb + (16 * ks + rr + ((mat & 2) ? 8 : 0)) * LDY + 16 * mt + ((mat & 1) ? 8 : 0));
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                if (wt + WPT * q >= T) break;
+                // B = x (rows position, cols ci) at the tap's shifted slab rows
+                uint32_t b0, b1;
+                ldsm_x2_t(b0, b1, sb + boff[q] + 16 * ks * LDX);
+                mma16816(acc[q], a[mtile[q]], b0, b1);
+            }
         }
-        if (m0 + g + 8 < cout_real) {
-            atomicAdd(w + (m0 + g + 8) * CIN + n0 + 2 * tig, acc[k][2]);
-            atomicAdd(w + (m0 + g + 8) * CIN + n0 + 2 * tig + 1, acc[k][3]);
+        __syncthreads();  // stage k & 1 is refilled by the next iteration's copies
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    const int gq = lane >> 2, tig = lane & 3;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int id = wt + WPT * q;
+        if (id >= T) break;
+        const int j = id / ((COUT / 16) * (CIN / 8)), rem = id - j * ((COUT / 16) * (CIN / 8));
+        const int m0 = 16 * (rem / (CIN / 8)), n0 = 8 * (rem % (CIN / 8));
+        float* w = dW + int64_t(g * TPG + j) * cout_real * CIN;  // rows past the real output channels are padding
+        if (m0 + gq < cout_real) {
+            atomicAdd(w + (m0 + gq) * CIN + n0 + 2 * tig, acc[q][0]);
+            atomicAdd(w + (m0 + gq) * CIN + n0 + 2 * tig + 1, acc[q][1]);
+        }
+        if (m0 + gq + 8 < cout_real) {
+            atomicAdd(w + (m0 + gq + 8) * CIN + n0 + 2 * tig, acc[q][2]);
+            atomicAdd(w + (m0 + gq + 8) * CIN + n0 + 2 * tig + 1, acc[q][3]);
         }
     }
 }
@@ -1074,11 +1146,28 @@ int conv_data_grad(cudaStream_t s, const ConvPath& P, const Layer& L, TView dy, 
 
 template <int CIN, int COUT, int TAPS>
 int wgrad_launch(cudaStream_t s, TView x, TView dy, float* dW, int cout_real, int64_t nvox) {
-    const int64_t ntiles = (nvox + kWgVox - 1) / kWgVox;
-    const int64_t per_tap = std::max(1, kWgCtas / TAPS);
-    const int tiles = int(std::max<int64_t>(8, (ntiles + per_tap - 1) / per_tap));
-    const dim3 grid(unsigned((ntiles + tiles - 1) / tiles), TAPS);
-    k_conv_wgrad<CIN, COUT, TAPS><<<grid, 128, 0, s>>>(x, dy, dW, cout_real, nvox, tiles);
+    if (nvox <= 0) return PLATO_OK;
+    if (x.B != dy.B || x.D != dy.D || x.H != dy.H || x.W != dy.W)
+        return fail(PLATO_BAD_INPUT, "weight gradient: input and output grids differ");
+    constexpr int G = wg_groups<CIN, COUT, TAPS>();
+    constexpr int NSL = (TAPS == 27 && G == 1) ? 3 : 1;
+    const int64_t sy = x.W + 2, sz = int64_t(x.H + 2) * sy;
+    const int64_t ptotal = int64_t(x.B) * (x.D + 2) * sz;
+    if (ptotal >= (int64_t(1) << 31)) return fail(PLATO_NOT_SUPPORTED, "weight gradient: grid above 2^31 positions");
+    const int srows = kWgRows + 2 * wg_halfwidth<TAPS, G>(int(sy));
+    const int rows_pad = srows;
+    const uint32_t stage_elems = uint32_t(kWgRows * (COUT + 8) + NSL * rows_pad * (CIN + 8));
+    const uint32_t smem = 2u * stage_elems * 2u;
+    if (smem > 227u * 1024u) return fail(PLATO_NOT_SUPPORTED, "weight gradient: grid rows too long for shared memory");
+    auto kernel = k_conv_wgrad<CIN, COUT, TAPS, G>;
+    UCUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int occ = 0;
+    UCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 128, smem));
+    const int32_t pfirst = int32_t(sz + sy + 1), plast = int32_t(halo_index(x, nvox - 1));
+    const int32_t ntiles = (plast - pfirst) / kWgRows + 1;
+    const int gx = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count()) * std::max(occ, 1) / G)));
+    kernel<<<dim3(unsigned(gx), unsigned(G)), 128, smem, s>>>(x, dy, dW, cout_real, pfirst, plast, int32_t(ptotal), ntiles,
+                                                               rows_pad, stage_elems);
     ULAUNCH();
     return PLATO_OK;
 }

@@ -73,6 +73,25 @@ __host__ __device__ __forceinline__ int64_t halo_index(const TView& t, int64_t v
     return ((b * (t.D + 2) + z + 1) * (t.H + 2) + y + 1) * (t.W + 2) + x + 1;
 }
 
+// voxel coordinates of plain interior index v of a view, and the haloed position of a voxel, in
+// 32-bit arithmetic (a network's grids hold fewer than 2^31 positions, checked at creation)
+struct Vox {
+    int b, z, y, x;
+};
+__device__ __forceinline__ Vox vox_of(const TView& t, uint32_t v) {
+    Vox r;
+    r.x = int(v % uint32_t(t.W));
+    v /= uint32_t(t.W);
+    r.y = int(v % uint32_t(t.H));
+    v /= uint32_t(t.H);
+    r.z = int(v % uint32_t(t.D));
+    r.b = int(v / uint32_t(t.D));
+    return r;
+}
+__device__ __forceinline__ int32_t hpos(const TView& t, int b, int z, int y, int x) {
+    return ((b * (t.D + 2) + z + 1) * (t.H + 2) + y + 1) * (t.W + 2) + x + 1;
+}
+
 __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -687,9 +706,10 @@ __global__ void k_grad_mask(TView dy, TView y, int relu, bf16* __restrict__ m, i
     const int C4 = C / 4;
     const int64_t total = nvox * C4;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C4;
-        const int c = 4 * int(i - v * C4);
-        const int64_t hv = halo_index(dy, v);
+        const uint32_t v = uint32_t(i / C4);
+        const int c = 4 * int(i - int64_t(v) * C4);
+        const Vox q = vox_of(dy, v);
+        const int64_t hv = hpos(dy, q.b, q.z, q.y, q.x);
         const float4 d = *reinterpret_cast<const float4*>(static_cast<const float*>(dy.p) + hv * dy.ld + dy.c0 + c);
         float val[4] = {d.x, d.y, d.z, d.w};
         if (relu) {
@@ -726,80 +746,131 @@ __global__ void __launch_bounds__(256) k_bias_grad(const bf16* __restrict__ m, i
     if (threadIdx.x < count) atomicAdd(db + threadIdx.x, sh[threadIdx.x]);
 }
 
-// 2x2x2 average pooling: out (extents of the coarse grid) from in (twice as fine)
+// 2x2x2 average pooling: out (extents of the coarse grid) from in (twice as fine); one thread
+// per (coarse voxel, 8 channels): eight 16-byte loads, one 16-byte store (C, ld and c0 are
+// multiples of 8).  Index arithmetic in 32 bits: every grid holds fewer than 2^31 positions.
 __global__ void k_pool(TView in, TView out, int C) {
-    const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C;
-        const int c = int(i - v * C);
-        const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
-        const int64_t b = v / (int64_t(out.W) * out.H * out.D);
-        float s = 0.f;
-        for (int q = 0; q < 8; ++q) {
-            const int64_t fv = ((b * in.D + 2 * z + (q >> 2)) * in.H + 2 * y + ((q >> 1) & 1)) * in.W + 2 * x + (q & 1);
-            s += __bfloat162float(static_cast<const bf16*>(in.p)[halo_index(in, fv) * in.ld + in.c0 + c]);
-        }
-        static_cast<bf16*>(out.p)[halo_index(out, v) * out.ld + out.c0 + c] = __float2bfloat16(0.125f * s);
-    }
-}
-
-// pooling gradient: din[fine] += dout[coarse] / 8 (FP32 gradients)
-__global__ void k_pool_grad(TView dout, TView din, int C) {
-    const int64_t nv = int64_t(din.B) * din.D * din.H * din.W;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C;
-        const int c = int(i - v * C);
-        const int x = int(v % din.W), y = int((v / din.W) % din.H), z = int((v / (int64_t(din.W) * din.H)) % din.D);
-        const int64_t b = v / (int64_t(din.W) * din.H * din.D);
-        const int64_t cv = ((b * dout.D + z / 2) * dout.H + y / 2) * dout.W + x / 2;
-        static_cast<float*>(din.p)[halo_index(din, v) * din.ld + din.c0 + c] +=
-            0.125f * static_cast<const float*>(dout.p)[halo_index(dout, cv) * dout.ld + dout.c0 + c];
-    }
-}
-
-// nearest upsampling: out[fine] = in[coarse]
-__global__ void k_upsample(TView in, TView out, int C) {
-    // one thread per (fine voxel, 8 channels): a 16-byte copy (C, ld and c0 are multiples of 8)
     const int C8 = C / 8;
-    const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C8; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C8;
-        const int c = 8 * int(i - v * C8);
-        const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
-        const int64_t b = v / (int64_t(out.W) * out.H * out.D);
-        const int64_t cv = ((b * in.D + z / 2) * in.H + y / 2) * in.W + x / 2;
-        *reinterpret_cast<uint4*>(static_cast<bf16*>(out.p) + halo_index(out, v) * out.ld + out.c0 + c) =
-            *reinterpret_cast<const uint4*>(static_cast<const bf16*>(in.p) + halo_index(in, cv) * in.ld + in.c0 + c);
-    }
-}
-
-// upsampling gradient: din[coarse] = sum of the 8 fine dout
-__global__ void k_upsample_grad(TView dout, TView din, int C) {
-    const int64_t nv = int64_t(din.B) * din.D * din.H * din.W;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * C; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / C;
-        const int c = int(i - v * C);
-        const int x = int(v % din.W), y = int((v / din.W) % din.H), z = int((v / (int64_t(din.W) * din.H)) % din.D);
-        const int64_t b = v / (int64_t(din.W) * din.H * din.D);
-        float s = 0.f;
-        for (int q = 0; q < 8; ++q) {
-            const int64_t fv = ((b * dout.D + 2 * z + (q >> 2)) * dout.H + 2 * y + ((q >> 1) & 1)) * dout.W + 2 * x + (q & 1);
-            s += static_cast<const float*>(dout.p)[halo_index(dout, fv) * dout.ld + dout.c0 + c];
+    const int64_t total = int64_t(out.B) * out.D * out.H * out.W * C8;
+    const int32_t fy = in.W + 2, fz = (in.H + 2) * fy;
+    const bf16* __restrict__ ip = static_cast<const bf16*>(in.p);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t v = uint32_t(i / C8);
+        const int c = 8 * int(i - int64_t(v) * C8);
+        const Vox q = vox_of(out, v);
+        const int32_t f = hpos(in, q.b, 2 * q.z, 2 * q.y, 2 * q.x);
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int32_t p = f + (k >> 2) * fz + ((k >> 1) & 1) * fy + (k & 1);
+            const uint4 u = *reinterpret_cast<const uint4*>(ip + int64_t(p) * in.ld + in.c0 + c);
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&w[j]);
+                s[2 * j] += __low2float(h);
+                s[2 * j + 1] += __high2float(h);
+            }
         }
-        static_cast<float*>(din.p)[halo_index(din, v) * din.ld + din.c0 + c] = s;
+        uint4 o;
+        o.x = pack_bf16(0.125f * s[0], 0.125f * s[1]);
+        o.y = pack_bf16(0.125f * s[2], 0.125f * s[3]);
+        o.z = pack_bf16(0.125f * s[4], 0.125f * s[5]);
+        o.w = pack_bf16(0.125f * s[6], 0.125f * s[7]);
+        *reinterpret_cast<uint4*>(static_cast<bf16*>(out.p) + int64_t(hpos(out, q.b, q.z, q.y, q.x)) * out.ld + out.c0 + c) = o;
     }
 }
 
-// network input: plain FP32 [B][n0][n1][n2][8] nodes -> haloed BF16 (16 channels, 8..15 zero)
+// pooling gradient: din[fine] += dout[coarse] / 8 (FP32 gradients); one thread per (coarse
+// voxel, 4 channels), one float4 read and eight float4 read-modify-writes
+__global__ void k_pool_grad(TView dout, TView din, int C) {
+    const int C4 = C / 4;
+    const int64_t total = int64_t(dout.B) * dout.D * dout.H * dout.W * C4;
+    const int32_t fy = din.W + 2, fz = (din.H + 2) * fy;
+    float* __restrict__ dp = static_cast<float*>(din.p);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t v = uint32_t(i / C4);
+        const int c = 4 * int(i - int64_t(v) * C4);
+        const Vox q = vox_of(dout, v);
+        const float4 g = *reinterpret_cast<const float4*>(static_cast<const float*>(dout.p) +
+                                                          int64_t(hpos(dout, q.b, q.z, q.y, q.x)) * dout.ld + dout.c0 + c);
+        const int32_t f = hpos(din, q.b, 2 * q.z, 2 * q.y, 2 * q.x);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int32_t p = f + (k >> 2) * fz + ((k >> 1) & 1) * fy + (k & 1);
+            float4* o = reinterpret_cast<float4*>(dp + int64_t(p) * din.ld + din.c0 + c);
+            float4 a = *o;
+            a.x += 0.125f * g.x; a.y += 0.125f * g.y; a.z += 0.125f * g.z; a.w += 0.125f * g.w;
+            *o = a;
+        }
+    }
+}
+
+// nearest upsampling: out[fine] = in[coarse]; one thread per (coarse voxel, 8 channels), one
+// 16-byte load and eight 16-byte stores
+__global__ void k_upsample(TView in, TView out, int C) {
+    const int C8 = C / 8;
+    const int64_t total = int64_t(in.B) * in.D * in.H * in.W * C8;
+    const int32_t fy = out.W + 2, fz = (out.H + 2) * fy;
+    bf16* __restrict__ op = static_cast<bf16*>(out.p);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t v = uint32_t(i / C8);
+        const int c = 8 * int(i - int64_t(v) * C8);
+        const Vox q = vox_of(in, v);
+        const uint4 u = *reinterpret_cast<const uint4*>(static_cast<const bf16*>(in.p) +
+                                                        int64_t(hpos(in, q.b, q.z, q.y, q.x)) * in.ld + in.c0 + c);
+        const int32_t f = hpos(out, q.b, 2 * q.z, 2 * q.y, 2 * q.x);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int32_t p = f + (k >> 2) * fz + ((k >> 1) & 1) * fy + (k & 1);
+            *reinterpret_cast<uint4*>(op + int64_t(p) * out.ld + out.c0 + c) = u;
+        }
+    }
+}
+
+// upsampling gradient: din[coarse] = sum of the 8 fine dout; one thread per (coarse voxel,
+// 4 channels), eight float4 loads summed in the fine voxels' order
+__global__ void k_upsample_grad(TView dout, TView din, int C) {
+    const int C4 = C / 4;
+    const int64_t total = int64_t(din.B) * din.D * din.H * din.W * C4;
+    const int32_t fy = dout.W + 2, fz = (dout.H + 2) * fy;
+    const float* __restrict__ gp = static_cast<const float*>(dout.p);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t v = uint32_t(i / C4);
+        const int c = 4 * int(i - int64_t(v) * C4);
+        const Vox q = vox_of(din, v);
+        const int32_t f = hpos(dout, q.b, 2 * q.z, 2 * q.y, 2 * q.x);
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int32_t p = f + (k >> 2) * fz + ((k >> 1) & 1) * fy + (k & 1);
+            const float4 a = *reinterpret_cast<const float4*>(gp + int64_t(p) * dout.ld + dout.c0 + c);
+            s.x += a.x; s.y += a.y; s.z += a.z; s.w += a.w;
+        }
+        *reinterpret_cast<float4*>(static_cast<float*>(din.p) + int64_t(hpos(din, q.b, q.z, q.y, q.x)) * din.ld + din.c0 + c) = s;
+    }
+}
+
+// network input: plain FP32 [B][n0][n1][n2][8] nodes -> haloed BF16 (16 channels, 8..15 zero);
+// one thread per node: two float4 loads, one 16-byte store
 __global__ void k_pack_input(const float* __restrict__ src, int n0, int n1, int n2, TView in) {
     const int64_t nv = int64_t(in.B) * n0 * n1 * n2;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * 8; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / 8;
-        const int c = int(i - v * 8);
-        const int x = int(v % n2), y = int((v / n2) % n1), z = int((v / (int64_t(n2) * n1)) % n0);
-        const int64_t b = v / (int64_t(n2) * n1 * n0);
-        const int64_t pv = ((b * in.D + z) * in.H + y) * in.W + x;
-        static_cast<bf16*>(in.p)[halo_index(in, pv) * in.ld + c] = __float2bfloat16(src[i]);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += int64_t(gridDim.x) * blockDim.x) {
+        uint32_t v = uint32_t(i);
+        const int x = int(v % uint32_t(n2));
+        v /= uint32_t(n2);
+        const int y = int(v % uint32_t(n1));
+        v /= uint32_t(n1);
+        const int z = int(v % uint32_t(n0));
+        const int b = int(v / uint32_t(n0));
+        const float4 a = reinterpret_cast<const float4*>(src)[2 * i];
+        const float4 c = reinterpret_cast<const float4*>(src)[2 * i + 1];
+        uint4 o;
+        o.x = pack_bf16(a.x, a.y);
+        o.y = pack_bf16(a.z, a.w);
+        o.z = pack_bf16(c.x, c.y);
+        o.w = pack_bf16(c.z, c.w);
+        *reinterpret_cast<uint4*>(static_cast<bf16*>(in.p) + int64_t(hpos(in, b, z, y, x)) * in.ld) = o;
     }
 }
 
@@ -807,35 +878,57 @@ __global__ void k_pack_input(const float* __restrict__ src, int n0, int n1, int 
 __global__ void k_unpack_output(TView out, int n0, int n1, int n2, float* __restrict__ dst) {
     const int64_t nv = int64_t(out.B) * n0 * n1 * n2;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * 9; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / 9;
-        const int c = int(i - v * 9);
-        const int x = int(v % n2), y = int((v / n2) % n1), z = int((v / (int64_t(n2) * n1)) % n0);
-        const int64_t b = v / (int64_t(n2) * n1 * n0);
-        const int64_t pv = ((b * out.D + z) * out.H + y) * out.W + x;
-        dst[i] = static_cast<const float*>(out.p)[halo_index(out, pv) * out.ld + c];
+        uint32_t v = uint32_t(i / 9);
+        const int c = int(i - int64_t(v) * 9);
+        const int x = int(v % uint32_t(n2));
+        v /= uint32_t(n2);
+        const int y = int(v % uint32_t(n1));
+        v /= uint32_t(n1);
+        const int z = int(v % uint32_t(n0));
+        const int b = int(v / uint32_t(n0));
+        dst[i] = static_cast<const float*>(out.p)[int64_t(hpos(out, b, z, y, x)) * out.ld + c];
     }
 }
 
-// mean squared error over the node region and its gradient (zero on padding voxels)
+// mean squared error over the node region and its gradient (zero on padding voxels); one
+// thread per voxel of the padded grid: the 16-channel output row in four float4 loads, the
+// BF16 gradient row in two 16-byte stores
 __global__ void k_loss(TView out, const float* __restrict__ tgt, int n0, int n1, int n2, TView dout,
                        double* __restrict__ loss) {
     const int64_t nv = int64_t(out.B) * out.D * out.H * out.W;
     const double inv = 1.0 / (double(out.B) * n0 * n1 * n2 * 9);
+    const float g2 = float(2.0 * inv);
     double local = 0.0;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv * 16; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = i / 16;
-        const int c = int(i - v * 16);
-        const int x = int(v % out.W), y = int((v / out.W) % out.H), z = int((v / (int64_t(out.W) * out.H)) % out.D);
-        const int64_t b = v / (int64_t(out.W) * out.H * out.D);
-        const int64_t hv = halo_index(out, v);
-        float gval = 0.f;
-        if (c < 9 && z < n0 && y < n1 && x < n2) {
-            const float d = static_cast<const float*>(out.p)[hv * out.ld + c] -
-                            tgt[(((b * n0 + z) * n1 + y) * n2 + x) * 9 + c];
-            local += double(d) * d;
-            gval = float(2.0 * inv) * d;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += int64_t(gridDim.x) * blockDim.x) {
+        const Vox q = vox_of(out, uint32_t(i));
+        const int32_t hv = hpos(out, q.b, q.z, q.y, q.x);
+        float gval[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) gval[c] = 0.f;
+        if (q.z < n0 && q.y < n1 && q.x < n2) {
+            const float4* orow = reinterpret_cast<const float4*>(static_cast<const float*>(out.p) + int64_t(hv) * out.ld);
+            float o[12];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float4 a = orow[k];
+                o[4 * k] = a.x; o[4 * k + 1] = a.y; o[4 * k + 2] = a.z; o[4 * k + 3] = a.w;
+            }
+            const float* t = tgt + ((((int64_t(q.b) * n0 + q.z) * n1 + q.y) * n2 + q.x) * 9);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                const float d = o[c] - t[c];
+                local += double(d) * d;
+                gval[c] = g2 * d;
+            }
         }
-        static_cast<bf16*>(dout.p)[hv * dout.ld + c] = __float2bfloat16(gval);
+        uint4 lo, hi;
+        lo.x = pack_bf16(gval[0], gval[1]); lo.y = pack_bf16(gval[2], gval[3]);
+        lo.z = pack_bf16(gval[4], gval[5]); lo.w = pack_bf16(gval[6], gval[7]);
+        hi.x = pack_bf16(gval[8], gval[9]); hi.y = pack_bf16(gval[10], gval[11]);
+        hi.z = pack_bf16(gval[12], gval[13]); hi.w = pack_bf16(gval[14], gval[15]);
+        uint4* drow = reinterpret_cast<uint4*>(static_cast<bf16*>(dout.p) + int64_t(hv) * dout.ld);
+        drow[0] = lo;
+        drow[1] = hi;
     }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * inv);
@@ -1210,23 +1303,23 @@ int forward(plato_unet* u, int B, const float* input) {
     const ConvPath P{u->conv_kind, u->conv_err};
     auto bias = [&](int k) { return u->params + L[k].b_off; };
     const int64_t nn = int64_t(B) * u->n[0] * u->n[1] * u->n[2];
-    k_pack_input<<<blocks_for(nn * 8, 256), 256, 0, s>>>(input, u->n[0], u->n[1], u->n[2], tv(u->in, 16, 0, B, G0));
+    k_pack_input<<<blocks_for(nn, 256), 256, 0, s>>>(input, u->n[0], u->n[1], u->n[2], tv(u->in, 16, 0, B, G0));
     ULAUNCH();
     URC(conv_forward(s, P, L[0], tv(u->in, 16, 0, B, G0), tv(u->x0a, 16, 0, B, G0), bias(0), n0));
     URC(conv_forward(s, P, L[1], tv(u->x0a, 16, 0, B, G0), tv(u->cat0, 48, 32, B, G0), bias(1), n0));
-    k_pool<<<blocks_for(n1 * 16, 256), 256, 0, s>>>(tv(u->cat0, 48, 32, B, G0), tv(u->p1, 16, 0, B, G1), 16);
+    k_pool<<<blocks_for(n1 * 2, 256), 256, 0, s>>>(tv(u->cat0, 48, 32, B, G0), tv(u->p1, 16, 0, B, G1), 16);
     ULAUNCH();
     URC(conv_forward(s, P, L[2], tv(u->p1, 16, 0, B, G1), tv(u->x1a, 32, 0, B, G1), bias(2), n1));
     URC(conv_forward(s, P, L[3], tv(u->x1a, 32, 0, B, G1), tv(u->cat1, 96, 64, B, G1), bias(3), n1));
-    k_pool<<<blocks_for(n2 * 32, 256), 256, 0, s>>>(tv(u->cat1, 96, 64, B, G1), tv(u->p2, 32, 0, B, G2), 32);
+    k_pool<<<blocks_for(n2 * 4, 256), 256, 0, s>>>(tv(u->cat1, 96, 64, B, G1), tv(u->p2, 32, 0, B, G2), 32);
     ULAUNCH();
     URC(conv_forward(s, P, L[4], tv(u->p2, 32, 0, B, G2), tv(u->x2a, 64, 0, B, G2), bias(4), n2));
     URC(conv_forward(s, P, L[5], tv(u->x2a, 64, 0, B, G2), tv(u->x2b, 64, 0, B, G2), bias(5), n2));
-    k_upsample<<<blocks_for(n1 * 64, 256), 256, 0, s>>>(tv(u->x2b, 64, 0, B, G2), tv(u->cat1, 96, 0, B, G1), 64);
+    k_upsample<<<blocks_for(n2 * 8, 256), 256, 0, s>>>(tv(u->x2b, 64, 0, B, G2), tv(u->cat1, 96, 0, B, G1), 64);
     ULAUNCH();
     URC(conv_forward(s, P, L[6], tv(u->cat1, 96, 0, B, G1), tv(u->x1c, 32, 0, B, G1), bias(6), n1));
     URC(conv_forward(s, P, L[7], tv(u->x1c, 32, 0, B, G1), tv(u->x1d, 32, 0, B, G1), bias(7), n1));
-    k_upsample<<<blocks_for(n0 * 32, 256), 256, 0, s>>>(tv(u->x1d, 32, 0, B, G1), tv(u->cat0, 48, 0, B, G0), 32);
+    k_upsample<<<blocks_for(n1 * 4, 256), 256, 0, s>>>(tv(u->x1d, 32, 0, B, G1), tv(u->cat0, 48, 0, B, G0), 32);
     ULAUNCH();
     URC(conv_forward(s, P, L[8], tv(u->cat0, 48, 0, B, G0), tv(u->x0c, 16, 0, B, G0), bias(8), n0));
     URC(conv_forward(s, P, L[9], tv(u->x0c, 16, 0, B, G0), tv(u->x0d, 16, 0, B, G0), bias(9), n0));
@@ -1274,25 +1367,25 @@ int backward(plato_unet* u, int B) {
                        tv(u->dx0c, 16, 0, B, G0), true, false, n0));
     URC(layer_backward(u, 8, tv(u->dx0c, 16, 0, B, G0), tv(u->x0c, 16, 0, B, G0), tv(u->cat0, 48, 0, B, G0),
                        tv(u->dcat0, 48, 0, B, G0), true, false, n0));
-    k_upsample_grad<<<blocks_for(n1 * 32, 256), 256, 0, s>>>(tv(u->dcat0, 48, 0, B, G0), tv(u->dx1d, 32, 0, B, G1), 32);
+    k_upsample_grad<<<blocks_for(n1 * 8, 256), 256, 0, s>>>(tv(u->dcat0, 48, 0, B, G0), tv(u->dx1d, 32, 0, B, G1), 32);
     ULAUNCH();
     URC(layer_backward(u, 7, tv(u->dx1d, 32, 0, B, G1), tv(u->x1d, 32, 0, B, G1), tv(u->x1c, 32, 0, B, G1),
                        tv(u->dx1c, 32, 0, B, G1), true, false, n1));
     URC(layer_backward(u, 6, tv(u->dx1c, 32, 0, B, G1), tv(u->x1c, 32, 0, B, G1), tv(u->cat1, 96, 0, B, G1),
                        tv(u->dcat1, 96, 0, B, G1), true, false, n1));
-    k_upsample_grad<<<blocks_for(n2 * 64, 256), 256, 0, s>>>(tv(u->dcat1, 96, 0, B, G1), tv(u->dx2b, 64, 0, B, G2), 64);
+    k_upsample_grad<<<blocks_for(n2 * 16, 256), 256, 0, s>>>(tv(u->dcat1, 96, 0, B, G1), tv(u->dx2b, 64, 0, B, G2), 64);
     ULAUNCH();
     URC(layer_backward(u, 5, tv(u->dx2b, 64, 0, B, G2), tv(u->x2b, 64, 0, B, G2), tv(u->x2a, 64, 0, B, G2),
                        tv(u->dx2a, 64, 0, B, G2), true, false, n2));
     URC(layer_backward(u, 4, tv(u->dx2a, 64, 0, B, G2), tv(u->x2a, 64, 0, B, G2), tv(u->p2, 32, 0, B, G2),
                        tv(u->dp2, 32, 0, B, G2), true, false, n2));
-    k_pool_grad<<<blocks_for(n1 * 32, 256), 256, 0, s>>>(tv(u->dp2, 32, 0, B, G2), tv(u->dcat1, 96, 64, B, G1), 32);
+    k_pool_grad<<<blocks_for(n2 * 8, 256), 256, 0, s>>>(tv(u->dp2, 32, 0, B, G2), tv(u->dcat1, 96, 64, B, G1), 32);
     ULAUNCH();
     URC(layer_backward(u, 3, tv(u->dcat1, 96, 64, B, G1), tv(u->cat1, 96, 64, B, G1), tv(u->x1a, 32, 0, B, G1),
                        tv(u->dx1a, 32, 0, B, G1), true, false, n1));
     URC(layer_backward(u, 2, tv(u->dx1a, 32, 0, B, G1), tv(u->x1a, 32, 0, B, G1), tv(u->p1, 16, 0, B, G1),
                        tv(u->dp1, 16, 0, B, G1), true, false, n1));
-    k_pool_grad<<<blocks_for(n0 * 16, 256), 256, 0, s>>>(tv(u->dp1, 16, 0, B, G1), tv(u->dcat0, 48, 32, B, G0), 16);
+    k_pool_grad<<<blocks_for(n1 * 4, 256), 256, 0, s>>>(tv(u->dp1, 16, 0, B, G1), tv(u->dcat0, 48, 32, B, G0), 16);
     ULAUNCH();
     URC(layer_backward(u, 1, tv(u->dcat0, 48, 32, B, G0), tv(u->cat0, 48, 32, B, G0), tv(u->x0a, 16, 0, B, G0),
                        tv(u->dx0a, 16, 0, B, G0), true, false, n0));
@@ -1318,6 +1411,10 @@ int plato_unet_create(const int32_t nodes[3], int32_t max_batch, plato_unet** ou
     for (int d = 0; d < 3; ++d) {
         u->n[d] = nodes[d];
         u->g0[d] = (nodes[d] + 3) / 4 * 4;
+    }
+    if (halo_elems(u->g0, max_batch, 1) >= (int64_t(1) << 31)) {
+        delete u;
+        return fail(PLATO_BAD_INPUT, "node grid x max_batch too large (2^31 haloed positions at most)");
     }
     // layers: {cin, cout, taps, relu}
     const int spec[11][4] = {{16, 16, 27, 1}, {16, 16, 27, 1}, {16, 32, 27, 1}, {32, 32, 27, 1}, {32, 64, 27, 1},
@@ -1468,7 +1565,7 @@ int plato_unet_loss_and_gradients(plato_unet* u, int32_t batch, const float* inp
     UCUDA(cudaMemsetAsync(u->loss_d, 0, sizeof(double), s));
     UCUDA(cudaMemsetAsync(u->mbuf, 0, sizeof(bf16) * size_t(halo_elems(u->g0, batch, 16)), s));
     const int64_t n0 = int64_t(batch) * u->g0[0] * u->g0[1] * u->g0[2];
-    k_loss<<<blocks_for(n0 * 16, 256), 256, 0, s>>>(tv(u->out, 16, 0, batch, u->g0), target, u->n[0], u->n[1], u->n[2],
+    k_loss<<<blocks_for(n0, 256), 256, 0, s>>>(tv(u->out, 16, 0, batch, u->g0), target, u->n[0], u->n[1], u->n[2],
                                                    tv(u->mbuf, 16, 0, batch, u->g0), u->loss_d);
     ULAUNCH();
     URC(backward(u, batch));

@@ -206,25 +206,28 @@ k_conv(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TV
 }
 
 // ---- convolution on the 5th-generation tensor cores (tcgen05, TMEM accumulator) -----------
-// The same implicit GEMM as k_conv, tiled over HALOED positions: a CTA of 4 warps owns 128
-// consecutive positions p0 .. p0 + 127 of the zero-haloed channels-last input (UMMA M = 128) and
-// every output channel (N = COUTP, a multiple of 16); the FP32 accumulator lives in tensor
-// memory, 128 lanes x N columns.  Tap (dz, dy, dx) of output row m reads the input at position
-// p0 + m + dz sz + dy sy + dx (sy = W + 2, sz = (H + 2) sy), so for one dz the 9 taps' A operands
-// are 128-row windows, dy sy + dx rows apart, of ONE slab of 128 + 2 (sy + 1) consecutive input
-// rows.  Per dz all threads copy that slab (cp.async, 16 bytes = 8 channels, zero fill outside
-// the tensor) and the 9 taps' weights [tap][COUTP][CIN] into shared memory in the canonical
-// K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk c at
-// c * LBO + r * 16, so a window starting at any row is again such a matrix), then one thread
+// The same implicit GEMM as k_conv, tiled over HALOED positions: a tile is 128 consecutive
+// positions p0 .. p0 + 127 of the zero-haloed channels-last input (UMMA M = 128) with every output
+// channel (N = COUTP, a multiple of 16); its FP32 accumulator lives in tensor memory, 128 lanes x
+// N columns.  Tap (dz, dy, dx) of output row m reads the input at position p0 + m + dz sz +
+// dy sy + dx (sy = W + 2, sz = (H + 2) sy), so for one dz the 9 taps' A operands are 128-row
+// windows, dy sy + dx rows apart, of ONE slab of 128 + 2 (sy + 1) consecutive input rows.  All
+// threads copy a slab with cp.async (16 bytes = 8 channels, zero fill outside the tensor) into
+// the canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk
+// c at c * LBO + r * 16, so a window starting at any row is again such a matrix); one thread then
 // issues 9 x CIN / 16 tcgen05.mma (kind::f16: BF16 A and B, FP32 accumulate) whose A descriptors
-// start at the tap's row, and commits them to the buffer's mbarrier: 3 slabs instead of 27
-// gathered tap tiles.  Two buffers: slab i + 1 is copied while the MMAs of slab i run; a buffer is
-// refilled only after its mbarrier shows the MMAs that read it complete.  A 1x1x1 convolution
-// is one slab of 128 rows.  Outputs at halo positions are computed and discarded.  The epilogue
-// loads the accumulator with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31, the rows of its
-// 32 positions), adds the bias, applies ReLU and stores the interior positions.  Every mbarrier
-// wait is bounded: on a timeout the CTA stops issuing, waits (bounded) for what it issued,
-// raises *err, skips the stores and still frees its tensor memory.
+// start at the tap's row and commits them to the buffer's mbarrier: 3 slabs per tile instead of
+// 27 gathered tap tiles.  The CTAs are persistent (tile = blockIdx.x + k gridDim.x): every tap's
+// weights stay in shared memory when they fit (else each buffer carries its slab's 9 taps), the
+// slabs run through 2 to 4 buffers with later slabs' copies in flight while the tensor core works,
+// and two accumulators alternate so that tile k - 1's epilogue runs after tile k's first MMAs are
+// queued.  A 1x1x1 convolution is one slab of 128 rows per tile.  Outputs at halo positions are
+// computed and discarded.  The epilogue loads an accumulator with tcgen05.ld (warp w reads TMEM
+// lanes 32w .. 32w + 31, the rows of its 32 positions), adds the bias, applies ReLU and stores
+// the interior positions.  Every mbarrier wait is bounded: on a timeout the CTA stops issuing,
+// waits (bounded) for what it issued, raises *err, skips the stores and still frees its tensor
+// memory.  With 16 output channels the MMAs are bound by reading the 4 KB A window from shared
+// memory (128 x 16 x 16 per instruction), not by the tensor core's arithmetic.
 constexpr int kTcRows = 128;             // haloed positions per CTA (UMMA M)
 constexpr uint32_t kTcPolls = 1u << 22;  // bounded mbarrier polls (about half a second)
 
@@ -315,6 +318,7 @@ struct TcGeom {
     int32_t ntiles;                 // 128-position tiles from pfirst to plast
     int32_t rows;                   // slab row stride (>= the rows one slab gathers)
     int32_t nbuf;                   // slab buffers in the pipeline (2 to 4)
+    int32_t lag;                    // MMAs of slab i issued in iteration i + lag (1 <= lag < nbuf)
     int32_t wres;                   // 1: all taps' weights stay in shared memory; 0: staged per slab
     uint32_t w_bytes;               // shared memory of the resident weights (0 when staged)
     uint32_t buf_bytes;             // one slab buffer (with its taps' weights when staged)
@@ -357,7 +361,7 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     const int32_t sy = in.W + 2, sz = (in.H + 2) * sy;
     const int halo = TAPS == 27 ? sy + 1 : 0;
     const int nrows = kTcRows + 2 * halo;  // slab rows gathered
-    const int nbuf = g.nbuf, lag = g.nbuf - 1;
+    const int nbuf = g.nbuf, lag = g.lag;
     const int my_tiles = (g.ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x);
     const int nslabs = my_tiles * NDZ;
     const bf16* __restrict__ ip = static_cast<const bf16*>(in.p);
@@ -432,8 +436,8 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     bool ok = true;
     int issued = 0;
     // iteration i copies slab i (tile i / NDZ of this CTA, z offset i % NDZ - 1) into buffer
-    // i % nbuf and issues the MMAs of slab i - lag (lag = nbuf - 1); a buffer is refilled once the
-    // MMAs of the slab it held, issued in the previous iteration, have completed
+    // i % nbuf and issues the MMAs of slab i - lag (lag < nbuf); a buffer is refilled once the
+    // MMAs of the slab it held, issued in iteration i - nbuf + lag, have completed
     for (int i = 0; i < nslabs + lag; ++i) {
         if (i < nslabs) {
             const int b = i % nbuf;
@@ -1158,9 +1162,12 @@ bool tc_plan(int rows, TcGeom& g, uint32_t& smem, int& ctas_per_sm) {
         const uint32_t need = std::max(wb + uint32_t(nb) * buf, guard);
         if (need > kMaxDyn) break;
         const int occ = std::min<int>(tmem_ctas, int(kSmPerSm / (need + kPerCtaExtra)));
-        if (occ * (nb - 1) > best) {
-            best = occ * (nb - 1);
+        const int lag = nb - 1;  // measured alike with lag nb - 2 (one iteration of MMA slack)
+        const int score = occ * lag;
+        if (score > best) {
+            best = score;
             g.nbuf = nb;
+            g.lag = lag;
             smem = need;
             ctas_per_sm = occ;
         }

@@ -306,6 +306,11 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
             const int nbw = warp_max(nb);
             const int64_t pbase = __ldg(so.ptr + s);
             const int64_t sbase = 9 * pbase;
+            // constrained components of the row, read once (a padding lane has nb = 0)
+            bool mrow[3] = {false, false, false};
+            if (nb > 0)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) mrow[i] = __ldg(so.bc_mask + 3 * (int64_t)r + i) != 0;
             for (int k = 0; k < nbw; ++k) {
                 const bool diag = k == dslot, upper = k > dslot && k < nb, pad = k >= nb;
                 if (!(diag || upper || pad)) continue;
@@ -327,15 +332,17 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 #pragma unroll
                     for (int q = 0; q < 9; ++q) K[q] = diag ? Kd[q] : T(0);
                 }
+                // constrained components of the column node, read once per block and reused
+                // for the transpose
+                bool mcol[3] = {false, false, false};
+                if (!pad)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) mcol[jj] = __ldg(so.bc_mask + 3 * (int64_t)c + jj) != 0;
 #pragma unroll
                 for (int q = 0; q < 9; ++q) {
                     const int i = q / 3, jj = q % 3;
                     double v = pad ? 0.0 : double(K[q]);
-                    if (!pad) {
-                        const bool mr = __ldg(so.bc_mask + 3 * (int64_t)r + i) != 0;
-                        const bool mc = __ldg(so.bc_mask + 3 * (int64_t)c + jj) != 0;
-                        if (mr || mc) v = (diag && i == jj) ? 1.0 : 0.0;
-                    }
+                    if (!pad && (mrow[i] || mcol[jj])) v = (diag && i == jj) ? 1.0 : 0.0;
                     store_sell(so, sbase + 32 * (9 * k + q) + lane, v);
                     if (diag && i == jj) {
                         if (so.dinv) so.dinv[3 * (int64_t)r + i] = 1.0 / v;
@@ -349,9 +356,7 @@ k_assemble_rows(MeshView m, GraphView g, Material mat, const double* __restrict_
 #pragma unroll
                         for (int q = 0; q < 9; ++q) {
                             const int i = q / 3, jj = q % 3;
-                            const bool mr = __ldg(so.bc_mask + 3 * (int64_t)c + i) != 0;
-                            const bool mc = __ldg(so.bc_mask + 3 * (int64_t)r + jj) != 0;
-                            store_sell(so, cb + 32 * q, (mr || mc) ? 0.0 : double(K[3 * jj + i]));
+                            store_sell(so, cb + 32 * q, (mcol[i] || mrow[jj]) ? 0.0 : double(K[3 * jj + i]));
                         }
                     }
                 }

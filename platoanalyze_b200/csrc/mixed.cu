@@ -324,6 +324,116 @@ k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__
     }
 }
 
+// Staged form of k_sell16s (16-bit column offsets): each warp covers two slices (lanes 0-15
+// and 16-31, two rows per lane as above) and streams their FP16 entries and column offsets
+// through shared memory in chunks of kStK slots: cp.async copies chunk c + 1 (16-byte pieces;
+// a slice's slots are contiguous, 576 B of entries and 64 B of offsets per slot) while the lanes
+// compute chunk c from shared memory.  The direction gathers then wait only on L2 (the offsets
+// are already on chip) instead of on a DRAM round trip followed by an L2 round trip.
+// Measured on the 160x80x80 bench mesh (sweep launch): 74.4 us with 2 slots x 2 stages (43 KB
+// per CTA, 4 CTAs per SM), 77.2 us with 3 stages (3 CTAs per SM), 79.0 us with 4 slots x 2
+// stages (2 CTAs per SM), 80.3 us for the register-fed k_sell16s.
+constexpr int kStK = 2;       // slots per chunk
+constexpr int kStStages = 2;  // chunks in the ring (kStStages - 1 in flight)
+// one slice's chunk: entries, then offsets; padded by 64 B so that the two half-warps' regions
+// start 16 banks apart
+constexpr int kStHalfBytes = kStK * (576 + 64) + 64;
+constexpr int kStWarpBytes = kStStages * 2 * kStHalfBytes;
+constexpr int kStSmem = (kThreads / 32) * kStWarpBytes;
+
+__device__ __forceinline__ void sweep_cp16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 4)
+k_sell16s_st(SellView A, const __half* __restrict__ vals, const float* __restrict__ x, float* __restrict__ res,
+             float* __restrict__ dnext, float* __restrict__ y, float c1, float c2, const PcgScalars* S) {
+    extern __shared__ __align__(16) uint8_t st_smem[];
+    pdl_wait();
+    pdl_trigger();
+    if (S && S->done) return;
+    const int64_t npairs = (((int64_t)A.num_rows + 31) & ~int64_t(31)) >> 1;
+    const uintptr_t vbits = reinterpret_cast<uintptr_t>(res) |
+                            (MODE == 0 ? reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dnext) |
+                                             reinterpret_cast<uintptr_t>(y)
+                                       : uintptr_t(0));
+    const bool vec2 = (vbits & 7) == 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, half = lane >> 4, m = lane & 15;
+    const uint8_t* wsm = st_smem + warp * kStWarpBytes;
+    const uint32_t wsm_s = static_cast<uint32_t>(__cvta_generic_to_shared(wsm));
+    // a warp's 32 pairs are 32 consecutive pairs starting at a multiple of 32: two whole slices
+    for (int64_t pb = blockIdx.x * (int64_t)blockDim.x + 32 * warp; pb < npairs;
+         pb += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pr = pb + lane;
+        const bool active = pr < npairs;  // npairs is a multiple of 16: half-warps are all or none
+        const int64_t sl = pr >> 4;
+        int w = 0;
+        int64_t base = 0;
+        if (active) {
+            w = __ldg(A.width + sl);
+            base = __ldg(A.ptr + sl);
+        }
+        int wmax = w;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+        const int nch = (wmax + kStK - 1) / kStK;
+        const uint8_t* gv = reinterpret_cast<const uint8_t*>(vals + 9 * base);  // 576 B per slot
+        const uint8_t* gc = reinterpret_cast<const uint8_t*>(A.dcols + base);  // 64 B per slot
+        // chunk c of this half-warp's slice into ring stage stg (nothing past the slice's width)
+        auto copy = [&](int c, int stg) {
+            const int k0 = c * kStK, kn = min(kStK, w - k0);
+            if (kn > 0) {
+                const uint32_t dst = wsm_s + uint32_t((stg * 2 + half) * kStHalfBytes);
+                for (int u = m; u < kn * 36; u += 16) sweep_cp16(dst + 16u * u, gv + 576 * int64_t(k0) + 16 * u);
+                for (int u = m; u < kn * 4; u += 16)
+                    sweep_cp16(dst + uint32_t(kStK * 576) + 16u * u, gc + 64 * int64_t(k0) + 16 * u);
+            }
+        };
+        const int32_t row0 = int32_t(32 * sl);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+#pragma unroll
+        for (int c = 0; c < kStStages - 1; ++c) {
+            if (c < nch) copy(c, c);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        for (int c = 0; c < nch; ++c) {
+            if (c + kStStages - 1 < nch) copy(c + kStStages - 1, (c + kStStages - 1) % kStStages);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group %0;" ::"n"(kStStages - 1) : "memory");  // chunk c is in
+            __syncwarp();
+            const uint8_t* sv = wsm + ((c % kStStages) * 2 + half) * kStHalfBytes;
+            const __half2* sh = reinterpret_cast<const __half2*>(sv) + m;
+            const short2* sd = reinterpret_cast<const short2*>(sv + kStK * 576) + m;
+#pragma unroll
+            for (int kk = 0; kk < kStK; ++kk) {
+                if (c * kStK + kk < w) {
+                    const short2 d = sd[16 * kk];
+                    const float* xa = x + 3 * (int64_t)(row0 + d.x);
+                    const float* xb = x + 3 * (int64_t)(row0 + d.y);
+                    const float x0 = __ldg(xa), x1 = __ldg(xa + 1), x2 = __ldg(xa + 2);
+                    const float z0 = __ldg(xb), z1 = __ldg(xb + 1), z2 = __ldg(xb + 2);
+                    float2 e[9];
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) e[q] = __half22float2(sh[144 * kk + 16 * q]);
+                    a0 += e[0].x * x0 + e[1].x * x1 + e[2].x * x2;
+                    a1 += e[3].x * x0 + e[4].x * x1 + e[5].x * x2;
+                    a2 += e[6].x * x0 + e[7].x * x1 + e[8].x * x2;
+                    b0 += e[0].y * z0 + e[1].y * z1 + e[2].y * z2;
+                    b1 += e[3].y * z0 + e[4].y * z1 + e[5].y * z2;
+                    b2 += e[6].y * z0 + e[7].y * z1 + e[8].y * z2;
+                }
+            }
+            __syncwarp();  // every lane has read stage c before a later copy refills it
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if (active) {
+            const float wv[6] = {a0, a1, a2, b0, b1, b2};
+            sell16s_update<MODE>(A.num_rows, pr, wv, x, res, dnext, y, c1, c2, vec2);
+        }
+    }
+}
+
 // ---- multi-step sweep: several Chebyshev steps per launch, the matrix re-read from L2 ------
 //
 // Step g of a preconditioner call reads the whole FP16 matrix (280 MB on the 160x80x80 mesh)
@@ -1043,12 +1153,19 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
     // The FP16 sweep runs as one resident wave that strides over the row pairs (every CTA
     // takes 3-4 pairs per thread on the bench mesh): 8 % faster per step than a grid of one
     // pair per thread, whose last partial wave leaves SMs idle.
-    int CB = SB;
+    int CB = SB, CBst = SB;
     if (kind == INNER_SELL16S) {
         int sms = 0, per_sm = 0;
         PLATO_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
         PLATO_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sell16s<0, false>, kThreads, 0));
         CB = std::min(SB, std::max(1, per_sm) * std::max(1, sms));
+        if (V.dcols) {  // the staged form, one resident wave as well
+            int per_st = 0;
+            PLATO_CUDA(h, cudaFuncSetAttribute(k_sell16s_st<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStSmem));
+            PLATO_CUDA(h, cudaFuncSetAttribute(k_sell16s_st<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStSmem));
+            PLATO_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_st, k_sell16s_st<0>, kThreads, kStSmem));
+            CBst = std::min(SB, std::max(1, per_st) * std::max(1, sms));
+        }
     }
     // multi-step sweep (FP16 scaled matrix, numbering with a short column reach)
     int wave_S = 0, wave_lag = 0, wave_grid = 0;
@@ -1095,8 +1212,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
             k_res_sub_vec<<<VB, kThreads, 0, s>>>(n, h->bc_mask, xin, h->f_w, h->f_res, h->scal);
         } else if (kind == INNER_SELL16S) {
             if (V.dcols)
-                PLATO_CUDA(h, launch_pdl(k_sell16s<1, true>, CB, kThreads, s, V, static_cast<const __half*>(h->sell16s),
-                                         xin, h->f_res, nullptr, nullptr, 0.f, 0.f, (const PcgScalars*)h->scal));
+                PLATO_CUDA(h, launch_pdl_smem(k_sell16s_st<1>, CBst, kThreads, size_t(kStSmem), s, V,
+                                              static_cast<const __half*>(h->sell16s), xin, h->f_res, nullptr, nullptr,
+                                              0.f, 0.f, (const PcgScalars*)h->scal));
             else
                 PLATO_CUDA(h, launch_pdl(k_sell16s<1, false>, CB, kThreads, s, V, static_cast<const __half*>(h->sell16s),
                                          xin, h->f_res, nullptr, nullptr, 0.f, 0.f, (const PcgScalars*)h->scal));
@@ -1160,9 +1278,9 @@ int fcg_poly(plato_problem* h, const double* b, double* x, plato_solve_stats* st
                                                    cc.c1[k], cc.c2[k], h->scal);
             } else if (kind == INNER_SELL16S) {
                 if (V.dcols)
-                    PLATO_CUDA(h, launch_pdl(k_sell16s<0, true>, CB, kThreads, s, V,
-                                             static_cast<const __half*>(h->sell16s), (const float*)dcur, h->f_res, dnext,
-                                             h->f_y, cc.c1[k], cc.c2[k], (const PcgScalars*)h->scal));
+                    PLATO_CUDA(h, launch_pdl_smem(k_sell16s_st<0>, CBst, kThreads, size_t(kStSmem), s, V,
+                                                  static_cast<const __half*>(h->sell16s), (const float*)dcur, h->f_res,
+                                                  dnext, h->f_y, cc.c1[k], cc.c2[k], (const PcgScalars*)h->scal));
                 else
                     PLATO_CUDA(h, launch_pdl(k_sell16s<0, false>, CB, kThreads, s, V,
                                              static_cast<const __half*>(h->sell16s), (const float*)dcur, h->f_res, dnext,

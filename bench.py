@@ -54,7 +54,7 @@ SEED_LARGE = 0x5EED0002  # nodal densities of the workload (SplitMix64 stream)
 # algorithmic bytes of its own launch.  Ratios near 1: no re-reads; the dC/dz pair reads the
 # cell values and the node -> cell incidence a second time (nodal sums after the cell pass).
 TRAFFIC_RATIO = {
-    "sweep": 152.3 / 166.35,        # k_sell16s<0> (16-bit columns)
+    "sweep": (150.34 + 3.67) / 166.35,  # k_sell16s_st<0> (16-bit columns)
     "fp64_spmv": 533.8 / 525.52,    # k_fcg_sell_apply
     "assembly": 595.5 / 559.79,     # k_assemble_rows<SELL>
     "residual": 79.58 / 77.49,      # k_internal_force
@@ -721,8 +721,9 @@ def main():
         if args.method == "two-level-fp16":  # FP16 entries, no Jacobi diagonal stream (unit diagonal)
             cb = prob.sell_info()["column_bytes"]  # 16-bit column offsets when the numbering allows
             cheb_bytes = 9 * B * 2 + B * cb + (N + 1) * 4 + 6 * 3 * N * 4
-            cheb_name = (f"k_sell16s<0> (FP16 Jacobi-scaled SELL SpMV fused with one Chebyshev step, "
-                         f"{8 * cb}-bit column indices)")
+            cheb_name = ("k_sell16s_st<0> (FP16 Jacobi-scaled SELL SpMV fused with one Chebyshev step; entries and "
+                         "16-bit column offsets staged through shared memory)" if cb == 2 else
+                         "k_sell16s<0> (FP16 Jacobi-scaled SELL SpMV fused with one Chebyshev step, 32-bit column indices)")
         else:
             cheb_bytes = 9 * B * 4 + B * 4 + (N + 1) * 4 + 7 * 3 * N * 4
             cheb_name = "k_cheb_sell<FP32> (FP32 SELL SpMV fused with one Chebyshev step)"

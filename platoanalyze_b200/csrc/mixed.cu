@@ -332,7 +332,8 @@ k_sell16s(SellView A, const __half* __restrict__ vals, const float* __restrict__
 // are already on chip) instead of on a DRAM round trip followed by an L2 round trip.
 // Measured on the 160x80x80 bench mesh (sweep launch): 74.4 us with 2 slots x 2 stages (43 KB
 // per CTA, 4 CTAs per SM), 77.2 us with 3 stages (3 CTAs per SM), 79.0 us with 4 slots x 2
-// stages (2 CTAs per SM), 80.3 us for the register-fed k_sell16s.
+// stages (2 CTAs per SM), 77.1 us with 1 slot x 3 stages, 78.7 us with 5 CTAs per SM (launch
+// bound 5; 78.4 us with 1 slot x 3 stages), 80.3 us for the register-fed k_sell16s.
 constexpr int kStK = 2;       // slots per chunk
 constexpr int kStStages = 2;  // chunks in the ring (kStStages - 1 in flight)
 // one slice's chunk: entries, then offsets; padded by 64 B so that the two half-warps' regions

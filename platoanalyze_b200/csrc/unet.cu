@@ -214,7 +214,8 @@ k_conv(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias, TV
 // windows, dy sy + dx rows apart, of ONE slab of 128 + 2 (sy + 1) consecutive input rows.  All
 // threads copy a slab with cp.async (16 bytes = 8 channels, zero fill outside the tensor) into
 // the canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes: row r of K-chunk
-// c at c * LBO + r * 16, so a window starting at any row is again such a matrix); one thread then
+// c at c * LBO + r * 16, so a window starting at any row is again such a matrix) -- or, with 16
+// input channels, rows of 32 bytes in the 32-byte swizzle (2.7 % faster forward); one thread then
 // issues 9 x CIN / 16 tcgen05.mma (kind::f16: BF16 A and B, FP32 accumulate) whose A descriptors
 // start at the tap's row and commits them to the buffer's mbarrier: 3 slabs per tile instead of
 // 27 gathered tap tiles.  The CTAs are persistent (tile = blockIdx.x + k gridDim.x): every tap's
@@ -240,6 +241,16 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
            (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// K-major SWIZZLE_32B descriptor (layout type 6 at bits 61-63) of a 16-channel slab window: rows
+// of 32 bytes, 8-row groups 256 B apart (stride offset), leading offset 16 B (unused within
+// the swizzle width), base offset 0.  The data is stored with its 16-byte chunk index XOR bit 7
+// of the row's shared-memory address, so a window may start at any row.  (Measured: with the
+// base offset set from the start address instead, the products came out wrong.)
+__device__ __forceinline__ uint64_t umma_smem_desc_sw32(uint32_t saddr) {
+    return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t(1) << 16) | (uint64_t(256 >> 4) << 32) | (uint64_t(1) << 46) |
+           (uint64_t(6) << 61);
 }
 
 // instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B (bits
@@ -331,6 +342,7 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
     constexpr int COUTP = (COUT + 15) / 16 * 16;
     static_assert(CIN % 16 == 0 && COUTP <= 256, "UMMA shape");
     constexpr int NDZ = TAPS == 27 ? 3 : 1, TPD = TAPS / NDZ;  // slabs (z offsets) per tile, taps per slab
+    constexpr bool SW = CIN == 16;  // 16-channel slabs: rows of 32 B in the 32-byte swizzle
     constexpr int ACC_COLS = tc_tmem_cols<COUTP>();            // one accumulator; two are allocated
     constexpr uint32_t BTAP = uint32_t(COUTP) * CIN * 2;       // one tap's weights
     constexpr uint32_t LBO_B = (COUTP / 8) * 128;
@@ -455,8 +467,12 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
                 const int r = q / (CIN / 8), c8 = q - r * (CIN / 8);
                 const int32_t pos = r0 + r;
                 const bool inside = pos >= 0 && pos < g.ptotal;  // rows outside feed discarded outputs only
-                cp_async16(a_s + uint32_t(c8) * LBO_A + uint32_t(r) * 16u,
-                           inside ? ip + int64_t(pos) * in.ld + in.c0 + 8 * c8 : ip, inside ? 16u : 0u);
+                uint32_t dst = a_s + uint32_t(c8) * LBO_A + uint32_t(r) * 16u;
+                if (SW) {
+                    const uint32_t row = a_s + 32u * uint32_t(r);
+                    dst = row + 16u * (uint32_t(c8) ^ ((row >> 7) & 1u));
+                }
+                cp_async16(dst, inside ? ip + int64_t(pos) * in.ld + in.c0 + 8 * c8 : ip, inside ? 16u : 0u);
             }
             // weights [tap][COUTP][CIN]: every tap once (resident), or this slab's taps per buffer
             const int wt0 = g.wres ? 0 : dzi * TPD, nw = g.wres ? (i == 0 ? TAPS : 0) : TPD;
@@ -486,10 +502,10 @@ k_conv_tc(TView in, const bf16* __restrict__ Wt, const float* __restrict__ bias,
                 for (int j = 0; j < TPD; ++j) {
                     // tap (dz, dy, dx): its 128 rows start dy sy + dx rows from the slab's centre window
                     const int dy = TPD == 9 ? j / 3 - 1 : 0, dx = TPD == 9 ? j % 3 - 1 : 0;
-                    const uint32_t a_t = a_s + uint32_t(halo + dy * sy + dx) * 16u;
+                    const uint32_t a_t = a_s + uint32_t(halo + dy * sy + dx) * (SW ? 32u : 16u);
 #pragma unroll
                     for (int kc = 0; kc < CIN / 16; ++kc)
-                        umma_bf16(d, umma_smem_desc(a_t + 2u * kc * LBO_A, LBO_A, 128u),
+                        umma_bf16(d, SW ? umma_smem_desc_sw32(a_t) : umma_smem_desc(a_t + 2u * kc * LBO_A, LBO_A, 128u),
                                   umma_smem_desc(w_s + uint32_t(j) * BTAP + 2u * kc * LBO_B, LBO_B, 128u), IDESC,
                                   (dzi > 0 || j > 0 || kc > 0) ? 1u : 0u);
                 }
